@@ -1,0 +1,368 @@
+#!/usr/bin/env python3
+"""Benchmark of the BioFVM 3-D diffusion-decay LOD step with cell sources.
+
+Metric: voxel*substrate updates per second per LOD step (N*S*steps / time).
+Workload (one GPU): config2 -- 200^3 voxels, dx=10 um, 4 substrates with
+log-uniform D in [1e2,1e5] and decay in [1e-3,1] (substrate 0 Dirichlet 38
+on all faces), 100,000 agents with uptake in [0,10] and secretion in [0,1],
+FP64, dt=0.01 min.  One bench step = one LOD step: agent sources fused into
+the x sweep, then the y and z sweeps (three kernels).
+
+  value  whole-job updates/s with the field resident in HBM (CUDA events on
+         the solve's stream, max over ranks).  The field is 256 MB, larger
+         than the 126 MB L2, so no flush is needed between steps.
+  e2e    the same metric through the C ABI with host buffers: every step
+         uploads the agent list (voxel + c1/c2/e2 from pinned host memory),
+         re-bins it on the device, runs the LOD step and reads the densities
+         at every agent's voxel back to the host.
+
+Multi-GPU: one process per GPU, each advancing its own replica of the
+workload (the solve does not shard; replicas only), value summed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "physicell-x_b200"))
+
+METRIC = "voxel·substrate updates/s per LOD step"
+UNIT = "voxel·substrate updates/s"
+WORKLOAD = ("config2: 200x200x200 voxels (dx=10 um), 4 substrates, 100000 agents, FP64, dt=0.01 min; "
+            "one LOD step = fused agent sources + x/y/z Thomas sweeps with Dirichlet pins")
+
+# DRAM bytes per launch of each sweep kernel from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) on this workload; see
+# profiles/sweeps_config2_fp64.md for the command and the raw figures.
+NCU_TRAFFIC = {}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            pk = json.load(fh)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_sample(wl, steps=2):
+    """Time the reference's own CPU path (oracle/_ref, all host threads) on a
+    bounded sample of the workload; the C restatement if the reference build
+    is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    threads = pyoracle.max_threads()
+    if pyoracle.Reference.available():
+        ref = pyoracle.Reference(wl, threads=threads)
+        ref.run(1, solver=0, threads=threads, sources_threads=threads, fetch=False)  # first call: factorization
+        t0 = time.perf_counter()
+        ref.run(steps, solver=0, threads=threads, sources_threads=threads, fetch=False)
+        dt = time.perf_counter() - t0
+        ref.close()
+        kind = "reference"
+    else:
+        field = wl.field0.copy()
+        c1, c2, e2 = pyoracle.Port.workload_constants(wl)
+        dv = wl.dirichlet_values
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            pyoracle.Port.sources(field, wl.S, wl.agent_voxel, c1, c2, e2)
+            pyoracle.Port.lod_step(field, wl.shape, wl.D, wl.decay, wl.dt, wl.dx, wl.dirichlet_active, dv, threads)
+        dt = time.perf_counter() - t0
+        kind = "port"
+    return {"value": wl.n_values * steps / dt, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{steps} LOD steps of config2 (sources + _BLOCKING sweeps, OpenMP {threads} threads), "
+                      f"{dt:.2f} s"}
+
+
+def run_reference_arm(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    from bfvm import workloads as W
+
+    wl = W.config2()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    threads = pyoracle.max_threads()
+    kind = "reference" if pyoracle.Reference.available() else "port"
+    if kind == "reference":
+        ref = pyoracle.Reference(wl, threads=threads)
+        step = lambda: ref.run(1, solver=0, threads=threads, sources_threads=threads, fetch=False)  # noqa: E731
+    else:
+        field = wl.field0.copy()
+        c1, c2, e2 = pyoracle.Port.workload_constants(wl)
+        dv = wl.dirichlet_values
+
+        def step():
+            pyoracle.Port.sources(field, wl.S, wl.agent_voxel, c1, c2, e2)
+            pyoracle.Port.lod_step(field, wl.shape, wl.D, wl.decay, wl.dt, wl.dx, wl.dirichlet_active, dv, threads)
+    for _ in range(max(1, args.warmup)):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = wl.n_values * args.steps / dt
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "solver": "diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING",
+                       "sources": f"simulate_cell_sources_and_sinks, OpenMP {threads} threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"{args.steps} timed LOD steps of config2 after {max(1, args.warmup)} warm-up"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    rank, world, local = dist_env()
+    import torch
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA GPU")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from bfvm import Microenvironment, kernel_launches
+    from bfvm import workloads as W
+
+    wl = W.config2()
+    me = Microenvironment.from_workload(wl, precision=args.precision, device=local)
+    stream = torch.cuda.ExternalStream(me.stream, device=torch.device("cuda", local))
+    N, S, A = wl.n_voxels, wl.S, wl.n_agents
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- warm-up ---------------------------------------------------------
+    me.simulate_diffusion_decay(max(3, args.warmup), sources=True)
+    me.synchronize()
+
+    # ---- timed region (resident field) -------------------------------------
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches0 = kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        me.timing_enable(True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            me.simulate_diffusion_decay(1, sources=True)
+        ev1.record(stream)
+        me.synchronize()
+        torch.cuda.synchronize()
+        me.timing_enable(False)
+    barrier()
+    launches = kernel_launches() - launches0
+    ms_total = ev0.elapsed_time(ev1)
+    ms_xyz, nrec = me.timing_read()
+    ms_step = ms_total / args.steps
+    if dist is not None:
+        t = torch.tensor([ms_step], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = world * N * S / (ms_step * 1e-3)
+
+    # ---- roofline of the dominant kernel -------------------------------------
+    eb = 8 if args.precision == "fp64" else 4
+    per_kernel_ms = ms_xyz / max(1, nrec)
+    names = ["sweep_x (+sources, pins)", "sweep_y (+pins)", "sweep_z (+pins)"]
+    field_bytes = 2 * N * S * eb
+    coef_bytes = [3 * wl.nx * S * 8, 3 * wl.ny * S * 8, 3 * wl.nz * S * 8]
+    agent_bytes = A * (4 + 3 * S * 8) + (wl.ny * wl.nz + 1) * 4
+    alg = [field_bytes + coef_bytes[0] + agent_bytes, field_bytes + coef_bytes[1], field_bytes + coef_bytes[2]]
+    dom = int(np.argmax(per_kernel_ms))
+    peak, peak_kind = load_peaks()
+    achieved = alg[dom] / (per_kernel_ms[dom] * 1e-3) / 1e9
+    traffic = NCU_TRAFFIC.get((args.precision, dom))
+    step_bytes = sum(alg)
+    roofline = {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": alg[dom],
+                "per_kernel": [{"kernel": names[k], "ms": per_kernel_ms[k],
+                                "GB/s": alg[k] / (per_kernel_ms[k] * 1e-3) / 1e9} for k in range(3)],
+                "step_frac": (step_bytes / (ms_step * 1e-3) / 1e9) / peak}
+
+    # ---- e2e through the C ABI with host buffers -----------------------------
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    c1, c2, e2 = _agent_constants(wl)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    h_vox, h_c1, h_c2, h_e2 = pin(wl.agent_voxel), pin(c1), pin(c2), pin(e2)
+    h_out = pin(np.zeros((A, S)))
+    from bfvm import _lib
+    import ctypes as C
+
+    L = me.L
+    vp = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+
+    def e2e_step():
+        _lib.check(L.bfvm_set_agents(me.h, A, vp(h_vox), None, vp(h_c1), vp(h_c2), vp(h_e2)), "bfvm_set_agents")
+        _lib.check(L.bfvm_step(me.h, 1, _lib.BFVM_STEP_SOURCES), "bfvm_step")
+        _lib.check(L.bfvm_sample_agents(me.h, vp(h_out)), "bfvm_sample_agents")
+
+    e2e_steps = args.e2e_steps or args.steps
+    for _ in range(3):
+        e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = A * 4 + 3 * A * S * 8
+    d2h = A * S * 8
+    e2e = {"value": world * N * S / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "ms_per_step": e2e_s * 1e3,
+           "path": "bfvm_set_agents (pinned host) + bfvm_step + bfvm_sample_agents (to pinned host)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_sample(wl)
+        except Exception as exc:  # report, do not fail the GPU measurement
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "unavailable", "sample": repr(exc)}
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}",
+                           "l2": "inputs larger than L2 (256 MB field per GPU), no flush",
+                           "voxels": N, "substrates": S, "agents": A},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def _agent_constants(wl):
+    """The agents' (c1, c2, e2) for the e2e upload, computed by the library on
+    the device with the arithmetic of Basic_Agent::set_internal_uptake_constants."""
+    import ctypes as C
+
+    import torch
+    from bfvm import _lib
+
+    n, S = wl.n_agents, wl.S
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t_vol = torch.from_numpy(np.ascontiguousarray(wl.agent_volume, np.float64)).to(dev)
+    t_r = [torch.from_numpy(np.ascontiguousarray(r, np.float64)).to(dev)
+           for r in (wl.secretion, wl.uptake, wl.saturation, wl.net_export)]
+    t_out = torch.empty((3, n, S), dtype=torch.float64, device=dev)
+    rc = _lib.lib().bfvm_agent_constants_device(n, S, wl.dt, wl.dx ** 3, C.c_void_p(t_vol.data_ptr()),
+                                                *[C.c_void_p(t.data_ptr()) for t in t_r],
+                                                *[C.c_void_p(t_out[k].data_ptr()) for k in range(3)], None)
+    _lib.check(rc, "bfvm_agent_constants_device")
+    torch.cuda.synchronize()
+    o = t_out.cpu().numpy()
+    return o[0].copy(), o[1].copy(), o[2].copy()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,199 @@
+/*
+ * biofvm_b200.h -- C ABI of the B200 implementation of BioFVM's 3-D
+ * diffusion-decay LOD step with cell sources/sinks (PhysiCell-X 1.14.0).
+ *
+ * Plain C: opaque handles, pointers and sizes, int status codes.  Every
+ * function returns BFVM_OK (0) or a negative BFVM_ERR_* code and leaves the
+ * solve's state unchanged on failure.  One handle is one microenvironment
+ * resident on one GPU; calls on one handle must not overlap, calls on
+ * different handles may come from different threads.
+ *
+ * Conventions shared with the reference (so a PhysiCell-X caller can pass its
+ * own buffers unchanged):
+ *   - a field is a flat double array in the reference layout, index
+ *     ((i*ny + j)*nz + k)*S + d  (Cartesian_Mesh::voxel_index,
+ *     BioFVM/BioFVM_mesh.cpp:1149-1158; Microenvironment::density_vector,
+ *     BioFVM/BioFVM_microenvironment.cpp:1123-1130);
+ *   - a voxel index is ((i*ny + j)*nz + k);
+ *   - per-agent arrays are [n][S] rows in agent-list order, the order of the
+ *     reference's all_basic_agents (BioFVM/BioFVM_basic_agent.h:187).
+ *
+ * The drop-in for the reference's own C++ API (the 4-argument
+ * diffusion_decay_solver__constant_coefficients_LOD_3D, BioFVM_solvers.h:66)
+ * is physicell-x_b200/host/biofvm_b200_dropin.cpp, built on these calls.
+ */
+#ifndef BIOFVM_B200_H
+#define BIOFVM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define BFVM_OK 0
+#define BFVM_ERR_ARG (-1)      /* bad argument (null pointer, size, index)   */
+#define BFVM_ERR_CUDA (-2)     /* a CUDA call failed                          */
+#define BFVM_ERR_OOM (-3)      /* device memory (or the HBM budget) exhausted */
+#define BFVM_ERR_SHAPE (-4)    /* grid not supported (extent, shared memory)  */
+#define BFVM_ERR_NODEVICE (-5) /* no usable CUDA device                       */
+#define BFVM_ERR_TIMEOUT (-6)  /* a bounded device-side wait gave up          */
+#define BFVM_ERR_STATE (-7)    /* call not valid in the current state         */
+
+/* ---- precision ---------------------------------------------------------- */
+#define BFVM_FP64 0 /* FP64 sweeps and storage: the reference's arithmetic    */
+#define BFVM_FP32 1 /* FP32 sweeps and storage; FP64-factored coefficients,   */
+                    /* FP64 agent updates                                      */
+
+/* ---- bfvm_step flags ----------------------------------------------------- */
+#define BFVM_STEP_SOURCES 1 /* apply the agents' sources/sinks ahead of each  */
+                            /* step, fused into the x sweep                    */
+
+/* Dirichlet faces, in the order the reference's setup writes them
+ * (BioFVM/BioFVM_microenvironment.cpp:2647-2760). */
+#define BFVM_FACE_XMIN 0
+#define BFVM_FACE_XMAX 1
+#define BFVM_FACE_YMIN 2
+#define BFVM_FACE_YMAX 3
+#define BFVM_FACE_ZMIN 4
+#define BFVM_FACE_ZMAX 5
+
+typedef struct bfvm_ctx bfvm_ctx;
+
+typedef struct bfvm_config {
+  int nx, ny, nz;                       /* voxels per axis                     */
+  int n_substrates;                     /* S                                   */
+  double dx;                            /* voxel edge; the mesh must be uniform */
+  double dt;                            /* diffusion time step                 */
+  const double* diffusion_coefficients; /* [S]                                 */
+  const double* decay_rates;            /* [S]                                 */
+  int precision;                        /* BFVM_FP64 or BFVM_FP32              */
+  int device;                           /* CUDA device ordinal                 */
+} bfvm_config;
+
+/* Create a resident solve.  Replaces the first-call setup inside
+ * diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING
+ * (BioFVM/BioFVM_solvers.cpp:125-337): the Thomas factorization of all three
+ * axes is computed here in FP64 with the reference's arithmetic and kept on
+ * the device.  The field starts at zero (Microenvironment::resize_space,
+ * BioFVM_microenvironment.cpp:610-638).  As in the reference
+ * (Microenvironment::resize_densities, :645-700), every substrate starts with
+ * Dirichlet activation on and value 1.0 on all six faces. */
+int bfvm_create(const bfvm_config* cfg, bfvm_ctx** out);
+int bfvm_destroy(bfvm_ctx* ctx);
+
+/* Per-substrate Dirichlet activation [S] (0/1).  Replaces
+ * Microenvironment::set_substrate_dirichlet_activation(int,bool)
+ * (BioFVM_microenvironment.cpp:265-273); the 3-D solvers read only this
+ * per-substrate flag (apply_dirichlet_boundaries_conditions, :348-446). */
+int bfvm_set_dirichlet_activation(bfvm_ctx* ctx, const unsigned char* active);
+
+/* Dirichlet values of every voxel on one face, as the reference's
+ * dirichlet_value_vectors hold them (update_dirichlet_node,
+ * BioFVM_microenvironment.cpp:228-244): x faces take [ny][nz][S], y faces
+ * [nx][nz][S], z faces [nx][ny][S], in reference index order.  A voxel on
+ * several faces must carry the same value in each (the value of its voxel). */
+int bfvm_set_dirichlet_face(bfvm_ctx* ctx, int face, const double* values);
+
+/* The same value vector [S] on every voxel of all six faces. */
+int bfvm_set_dirichlet_uniform(bfvm_ctx* ctx, const double* values);
+
+/* Copy a whole field in (host memory, reference layout).  Replaces writing
+ * the densities through Microenvironment::density_vector (:1123-1130). */
+int bfvm_upload_field(bfvm_ctx* ctx, const double* field);
+/* Copy the whole field out (host memory, reference layout). */
+int bfvm_download_field(bfvm_ctx* ctx, double* field);
+/* Same two calls with device pointers (reference layout in device memory). */
+int bfvm_upload_field_device(bfvm_ctx* ctx, const double* d_field);
+int bfvm_download_field_device(bfvm_ctx* ctx, double* d_field);
+
+/* Agent list from precomputed constants: voxel [n] (reference voxel index,
+ * <0 = outside), active [n] or NULL, and c1, c2, e2 [n][S] -- the agent's
+ * cell_source_sink_solver_temp1, _temp2 and _temp_export2
+ * (BioFVM/BioFVM_basic_agent.h:61-72).  The list is stably binned by voxel
+ * on the device, so agents sharing a voxel are applied in list order, as
+ * the single-threaded Microenvironment::simulate_cell_sources_and_sinks
+ * (BioFVM_microenvironment.cpp:1370-1379) applies them.  Host pointers. */
+int bfvm_set_agents(bfvm_ctx* ctx, int n, const int* voxel, const unsigned char* active, const double* c1,
+                    const double* c2, const double* e2);
+
+/* Agent list from rates: volume [n] and secretion, uptake, saturation and
+ * net-export rates [n][S]; the constants are computed on the device with the
+ * arithmetic of Basic_Agent::set_internal_uptake_constants
+ * (BioFVM/BioFVM_basic_agent.cpp:224-274) for this solve's dt and dx^3. */
+int bfvm_set_agents_from_rates(bfvm_ctx* ctx, int n, const int* voxel, const unsigned char* active,
+                               const double* volume, const double* secretion, const double* uptake,
+                               const double* saturation, const double* net_export);
+
+/* Basic_Agent::set_internal_uptake_constants (BioFVM_basic_agent.cpp:224-274)
+ * for a whole agent list, with no solve attached: every pointer is device
+ * memory -- volume [n], rates [n][S], outputs c1, c2, e2 [n][S] -- and
+ * stream is a cudaStream_t (NULL: the default stream).  Asynchronous. */
+int bfvm_agent_constants_device(int n, int S, double dt, double voxel_volume, const double* volume,
+                                const double* secretion, const double* uptake, const double* saturation,
+                                const double* net_export, double* c1, double* c2, double* e2, void* stream);
+
+/* Advance nsteps LOD steps.  Each step is the reference's
+ * [simulate_cell_sources_and_sinks (if flags & BFVM_STEP_SOURCES);
+ *  diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING]
+ * (BioFVM_microenvironment.cpp:1370-1384; BioFVM_solvers.cpp:102-780):
+ * Dirichlet pin, x sweep, pin, y sweep, pin, z sweep, pin.  Asynchronous on
+ * the solve's stream. */
+int bfvm_step(bfvm_ctx* ctx, int nsteps, int flags);
+
+/* The source/sink stage alone (one call of
+ * Microenvironment::simulate_cell_sources_and_sinks(dt), :1381-1384). */
+int bfvm_apply_sources(bfvm_ctx* ctx);
+
+/* Densities at each agent's voxel, [n][S] host doubles, in agent-list order
+ * (what Basic_Agent::nearest_density_vector returns to each agent,
+ * BioFVM/BioFVM_basic_agent.cpp:389-392). */
+int bfvm_sample_agents(bfvm_ctx* ctx, double* out);
+
+/* Per-substrate sums over all voxels, computed in FP64 on the device [S]
+ * (the mass-balance check; multiply by dx^3 for total substrate). */
+int bfvm_field_sums(bfvm_ctx* ctx, double* out);
+
+/* Wait for the solve's stream; returns BFVM_ERR_TIMEOUT if a device-side
+ * wait gave up since the last check, BFVM_ERR_CUDA on a CUDA error. */
+int bfvm_synchronize(bfvm_ctx* ctx);
+
+/* The cudaStream_t the solve runs on (as void*), for event timing. */
+void* bfvm_stream(bfvm_ctx* ctx);
+/* Run the solve on a caller-owned stream (NULL: back to its own stream). */
+int bfvm_set_stream(bfvm_ctx* ctx, void* stream);
+
+/* Device field pointer and row pitch (elements) of the device layout
+ * f[S][nz][ny][pitch], x fastest -- for callers that keep data on the GPU. */
+int bfvm_device_field(bfvm_ctx* ctx, void** ptr, int* pitch, int* elem_bytes);
+
+/* Bytes of device memory the solve holds (field, coefficients, agents). */
+size_t bfvm_device_bytes(bfvm_ctx* ctx);
+
+/* Launch shape of the sweeps: lines per CTA in the x sweep, x extent per CTA
+ * and rows per TMA box in the y/z sweeps.  The defaults fit all extents up to
+ * 256 in FP64; bfvm_set_launch re-encodes the TMA descriptors. */
+int bfvm_get_launch(bfvm_ctx* ctx, int* x_lines, int* yz_tile, int* yz_chunk);
+int bfvm_set_launch(bfvm_ctx* ctx, int x_lines, int yz_tile, int yz_chunk);
+
+/* Number of this library's kernels launched by the calls so far (counted on
+ * the host at each launch). */
+long long bfvm_kernel_launches(void);
+
+/* Per-kernel timing, the device counterpart of the reference's per-step
+ * timers (tests/mpi/diffusion/main.cpp:197-214): while enabled, every step
+ * records CUDA events on the solve's stream around the x, y and z sweep
+ * kernels.  bfvm_timing_read waits for the stream and returns the summed
+ * durations [3] (ms: x, y, z) and the number of steps recorded, then clears
+ * them.  At most 4096 steps are recorded between reads. */
+int bfvm_timing_enable(bfvm_ctx* ctx, int on);
+int bfvm_timing_read(bfvm_ctx* ctx, double* ms_xyz, int* steps);
+
+const char* bfvm_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BIOFVM_B200_H */

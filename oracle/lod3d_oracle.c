@@ -1,0 +1,201 @@
+/*
+ * lod3d_oracle.c -- TEST INFRASTRUCTURE: plain-C restatement of the
+ * reference's BioFVM 3-D LOD step and agent sources (see lod3d_oracle.h).
+ *
+ * Arithmetic contract.  The reference is C++ built by g++ -O3 with FMA
+ * available, and g++ contracts `y += a*x` into one fused multiply-add and
+ * `y -= a*x` into one fused negative multiply-add.  This file is compiled
+ * with -ffp-contract=off and writes every such contraction as an explicit
+ * fma(), so each value below is the one the reference computes, operation
+ * by operation:
+ *   forward  p[i] = fma(c1, p[i-1], p[i]);  p[i] = p[i] / denom[i]
+ *   backward p[i] = fma(-cupper[i], p[i+1], p[i])
+ * (BioFVM/BioFVM_solvers.cpp:365-376, 693-726, 742-775).
+ */
+#include "lod3d_oracle.h"
+
+#include <math.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <stdlib.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+void orc_thomas_axis(int n, int S, const double* D, const double* decay, double dt, double dx,
+                     double* denom, double* cupper, double* c1) {
+  for (int d = 0; d < S; ++d) {
+    /* BioFVM_solvers.cpp:196-218: constant1 = D; *= dt; /= dx; /= dx.
+       constant1a = constant1 * -1.0; constant2 = lambda*dt/3;
+       constant3 = ((1 + c1) + c1) + c2; constant3a = (1 + c1) + c2. */
+    double k1 = D[d];
+    k1 *= dt;
+    k1 /= dx;
+    k1 /= dx;
+    double k1a = k1 * -1.0;
+    double k2 = decay[d];
+    k2 *= dt;
+    k2 /= 3.0;
+    double k3 = 1.0;
+    k3 += k1;
+    k3 += k1;
+    k3 += k2;
+    double k3a = 1.0;
+    k3a += k1;
+    k3a += k2;
+    c1[d] = k1;
+    /* :226-245 (x, one rank) and :297-312 / :314-329 (y, z): identical. */
+    for (int i = 0; i < n; ++i) {
+      cupper[(size_t)i * S + d] = k1a;
+      denom[(size_t)i * S + d] = k3;
+    }
+    denom[d] = k3a;
+    denom[(size_t)(n - 1) * S + d] = k3a;
+    if (n == 1) {
+      double v = 1.0;
+      v += k2;
+      denom[d] = v;
+    }
+    cupper[d] /= denom[d];
+    for (int i = 1; i < n; ++i) {
+      /* axpy(&denom[i], constant1, c[i-1])  (BioFVM_vector.cpp:333-340) */
+      denom[(size_t)i * S + d] = fma(k1, cupper[(size_t)(i - 1) * S + d], denom[(size_t)i * S + d]);
+      cupper[(size_t)i * S + d] /= denom[(size_t)i * S + d];
+    }
+  }
+}
+
+void orc_apply_dirichlet(double* field, int nx, int ny, int nz, int S, const unsigned char* active,
+                         const double* dv) {
+  /* Every face voxel is set from its own entry of dv, so the order in which
+     the reference visits faces (x, then y, then z) cannot change the result. */
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        if (!(i == 0 || i == nx - 1 || j == 0 || j == ny - 1 || k == 0 || k == nz - 1)) continue;
+        size_t v = ((size_t)i * ny + j) * nz + k;
+        for (int d = 0; d < S; ++d)
+          if (active[d]) field[v * S + d] = dv[v * S + d];
+      }
+}
+
+void orc_lod3d_step(double* p, int nx, int ny, int nz, int S, const double* D, const double* decay,
+                    double dt, double dx, const unsigned char* active, const double* dv, int threads) {
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#else
+  (void)threads;
+#endif
+  double* coef = (double*)malloc(sizeof(double) * (2 * ((size_t)nx + ny + nz) * S + S));
+  double *dnx = coef, *cx = dnx + (size_t)nx * S, *dny = cx + (size_t)nx * S, *cy = dny + (size_t)ny * S;
+  double *dnz = cy + (size_t)ny * S, *cz = dnz + (size_t)nz * S, *c1 = cz + (size_t)nz * S;
+  orc_thomas_axis(nx, S, D, decay, dt, dx, dnx, cx, c1);
+  orc_thomas_axis(ny, S, D, decay, dt, dx, dny, cy, c1);
+  orc_thomas_axis(nz, S, D, decay, dt, dx, dnz, cz, c1);
+  const size_t jx = (size_t)ny * nz * S; /* thomas_i_jump */
+  const size_t jy = (size_t)nz * S;      /* thomas_j_jump */
+  const size_t jz = (size_t)S;           /* thomas_k_jump */
+
+  orc_apply_dirichlet(p, nx, ny, nz, S, active, dv);
+
+  /* x sweep (BioFVM_solvers.cpp:352-680 with one rank): lines over (j,k,d). */
+#pragma omp parallel for schedule(static)
+  for (long long jk = 0; jk < (long long)ny * nz; ++jk) {
+    for (int d = 0; d < S; ++d) {
+      double* q = p + (size_t)jk * S + d;
+      q[0] /= dnx[d];
+      for (int i = 1; i < nx; ++i) {
+        q[i * jx] = fma(c1[d], q[(i - 1) * jx], q[i * jx]);
+        q[i * jx] /= dnx[(size_t)i * S + d];
+      }
+      for (int i = nx - 2; i >= 0; --i) q[i * jx] = fma(-cx[(size_t)i * S + d], q[(i + 1) * jx], q[i * jx]);
+    }
+  }
+  orc_apply_dirichlet(p, nx, ny, nz, S, active, dv);
+
+  /* y sweep (:684-729): lines over (i,k,d). */
+#pragma omp parallel for schedule(static)
+  for (long long ik = 0; ik < (long long)nx * nz; ++ik) {
+    const size_t i = (size_t)(ik / nz), k = (size_t)(ik % nz);
+    for (int d = 0; d < S; ++d) {
+      double* q = p + i * jx + k * jz + d;
+      q[0] /= dny[d];
+      for (int j = 1; j < ny; ++j) {
+        q[j * jy] = fma(c1[d], q[(j - 1) * jy], q[j * jy]);
+        q[j * jy] /= dny[(size_t)j * S + d];
+      }
+      for (int j = ny - 2; j >= 0; --j) q[j * jy] = fma(-cy[(size_t)j * S + d], q[(j + 1) * jy], q[j * jy]);
+    }
+  }
+  orc_apply_dirichlet(p, nx, ny, nz, S, active, dv);
+
+  /* z sweep (:733-777): lines over (i,j,d). */
+#pragma omp parallel for schedule(static)
+  for (long long ij = 0; ij < (long long)nx * ny; ++ij) {
+    for (int d = 0; d < S; ++d) {
+      double* q = p + (size_t)ij * (size_t)nz * S + d;
+      q[0] /= dnz[d];
+      for (int k = 1; k < nz; ++k) {
+        q[k * jz] = fma(c1[d], q[(k - 1) * jz], q[k * jz]);
+        q[k * jz] /= dnz[(size_t)k * S + d];
+      }
+      for (int k = nz - 2; k >= 0; --k) q[k * jz] = fma(-cz[(size_t)k * S + d], q[(k + 1) * jz], q[k * jz]);
+    }
+  }
+  orc_apply_dirichlet(p, nx, ny, nz, S, active, dv);
+  free(coef);
+}
+
+void orc_agent_constants(int S, double dt, double V, double Vvox, const double* sec, const double* upt,
+                         const double* sat, const double* exp_, double* c1, double* c2, double* e2) {
+  /* BioFVM_basic_agent.cpp:238: dt * volume / voxel_volume, left to right. */
+  double k = dt * V / Vvox;
+  for (int d = 0; d < S; ++d) {
+    /* temp1 = 0; += S; *= T; *= k  (:241-244) */
+    double t1 = 0.0;
+    t1 += sec[d];
+    t1 *= sat[d];
+    t1 *= k;
+    /* temp2 = 1; axpy(temp2, k, S); axpy(temp2, k, U)  (:249-251) */
+    double t2 = 1.0;
+    t2 = fma(k, sec[d], t2);
+    t2 = fma(k, upt[d], t2);
+    /* export1 = E * dt; export2 = export1 / voxel_volume  (:258-262) */
+    double x1 = exp_[d];
+    x1 *= dt;
+    double x2 = x1;
+    x2 /= Vvox;
+    c1[d] = t1;
+    c2[d] = t2;
+    e2[d] = x2;
+  }
+}
+
+void orc_sources(double* field, int S, int n, const int* voxel, const unsigned char* active, const double* c1,
+                 const double* c2, const double* e2) {
+  for (int a = 0; a < n; ++a) {
+    if ((active && !active[a]) || voxel[a] < 0) continue;
+    double* rho = field + (size_t)voxel[a] * S;
+    /* BioFVM_basic_agent.cpp:538-552: += c1; /= c2; += e2 */
+    for (int d = 0; d < S; ++d) rho[d] += c1[(size_t)a * S + d];
+    for (int d = 0; d < S; ++d) rho[d] /= c2[(size_t)a * S + d];
+    for (int d = 0; d < S; ++d) rho[d] += e2[(size_t)a * S + d];
+  }
+}
+
+int orc_nearest_voxel(double x, double y, double z, double x0, double y0, double z0, double dx, int nx,
+                      int ny, int nz) {
+  /* Positions outside [x0, x0+n*dx] are rejected by the reference before
+     indexing (General_Mesh::is_position_valid, BioFVM_mesh.cpp:242-251). */
+  if (x < x0 || x > x0 + nx * dx || y < y0 || y > y0 + ny * dx || z < z0 || z > z0 + nz * dx) return -1;
+  long long i = (long long)floor((x - x0) / dx);
+  long long j = (long long)floor((y - y0) / dx);
+  long long k = (long long)floor((z - z0) / dx);
+  if (i >= nx) i = nx - 1;
+  if (j >= ny) j = ny - 1;
+  if (k >= nz) k = nz - 1;
+  if (i < 0) i = 0;
+  if (j < 0) j = 0;
+  if (k < 0) k = 0;
+  return (int)((i * ny + j) * nz + k);
+}

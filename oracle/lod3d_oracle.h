@@ -1,0 +1,72 @@
+/*
+ * lod3d_oracle.h -- TEST INFRASTRUCTURE: the CPU oracle (plain C restatement)
+ * of PhysiCell-X's BioFVM 3-D LOD diffusion-decay step and cell
+ * sources/sinks.  Only tests, smoke() and bench.py's CPU-baseline leg may
+ * call it; it is the checker, never the product.
+ *
+ * Layout is the reference's: one flat array, index ((i*ny + j)*nz + k)*S + d
+ * (Cartesian_Mesh::voxel_index, BioFVM/BioFVM_mesh.cpp:1149-1158, times the
+ * substrate count as in Microenvironment::density_vector,
+ * BioFVM/BioFVM_microenvironment.cpp:1123-1130).
+ *
+ * Parity status: pinned against the reference itself.  The reference ships
+ * no golden vectors for this path, so tests/test_oracle.py compares this
+ * restatement bit for bit with the reference's own solver built from its
+ * sources (oracle/_ref/libbiofvm_ref.so), and tests/golden/ holds fixtures
+ * generated from that build.
+ */
+#ifndef BFVM_LOD3D_ORACLE_H
+#define BFVM_LOD3D_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Thomas coefficients of one axis with n voxels, for S substrates.
+ * Outputs denom[n*S], cupper[n*S] (index i*S+d) and c1[S].
+ * Restates BioFVM/BioFVM_solvers.cpp:196-329 (one rank). */
+void orc_thomas_axis(int n, int S, const double* D, const double* decay, double dt, double dx,
+                     double* denom, double* cupper, double* c1);
+
+/* The Dirichlet pin: every voxel on the six outer faces takes its value from
+ * dirichlet_values (same layout as the field) for each substrate d with
+ * active[d] != 0.  Restates Microenvironment::apply_dirichlet_boundaries_conditions
+ * BioFVM/BioFVM_microenvironment.cpp:348-446 (rank 0 of 1). */
+void orc_apply_dirichlet(double* field, int nx, int ny, int nz, int S, const unsigned char* active,
+                         const double* dirichlet_values);
+
+/* One diffusion-decay LOD step: pin; x sweep; pin; y sweep; pin; z sweep; pin.
+ * Restates diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING,
+ * BioFVM/BioFVM_solvers.cpp:102-780 with one rank.  threads<=0 uses the
+ * OpenMP default; the result does not depend on the thread count. */
+void orc_lod3d_step(double* field, int nx, int ny, int nz, int S, const double* D,
+                    const double* decay, double dt, double dx, const unsigned char* active,
+                    const double* dirichlet_values, int threads);
+
+/* Per-agent implicit source/sink constants for one time step.
+ * Restates Basic_Agent::set_internal_uptake_constants,
+ * BioFVM/BioFVM_basic_agent.cpp:224-274.  Outputs c1,c2,e2 [S]. */
+void orc_agent_constants(int S, double dt, double agent_volume, double voxel_volume,
+                         const double* secretion, const double* uptake, const double* saturation,
+                         const double* net_export, double* c1, double* c2, double* e2);
+
+/* Apply agents in list order to their voxels (one thread, the reference's
+ * deterministic order).  voxel[a] is the reference linear voxel index; agents
+ * with active[a]==0 or voxel[a]<0 are skipped.  c1,c2,e2 are [n][S].
+ * Restates Basic_Agent::simulate_secretion_and_uptake,
+ * BioFVM/BioFVM_basic_agent.cpp:509-559, driven as in
+ * Microenvironment::simulate_cell_sources_and_sinks (:1370-1379). */
+void orc_sources(double* field, int S, int n_agents, const int* voxel, const unsigned char* active,
+                 const double* c1, const double* c2, const double* e2);
+
+/* Cartesian_Mesh::nearest_voxel_index for a one-rank mesh whose box starts
+ * at (x0,y0,z0) (BioFVM/BioFVM_mesh.cpp:1825-1843): floor((p-x0)/dx), clamped
+ * to [0,n-1].  Returns the reference linear index. */
+int orc_nearest_voxel(double x, double y, double z, double x0, double y0, double z0, double dx,
+                      int nx, int ny, int nz);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

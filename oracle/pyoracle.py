@@ -1,0 +1,268 @@
+"""ctypes bindings for the CPU oracle -- TEST INFRASTRUCTURE.
+
+Only tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+(and its ``--impl reference`` arm) import this module, always as the checker
+or the timed CPU reference, never as the product path.
+
+Two oracles share one numpy-facing interface:
+
+* :class:`Port` wraps ``oracle/liboracle_lod3d.so``, the plain-C restatement
+  (``oracle/lod3d_oracle.c``), which needs no reference sources.
+* :class:`Reference` wraps ``oracle/_ref/libbiofvm_ref.so``, the reference's
+  own BioFVM + DistPhy sources compiled by ``oracle/Makefile`` against a
+  single-rank MPI shim, driven through ``oracle/ref_driver.cpp``.
+
+Both take and return fields in the reference layout: a flat float64 array
+indexed ``((i*ny + j)*nz + k)*S + d`` (BioFVM/BioFVM_mesh.cpp:1149-1158).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "liboracle_lod3d.so")
+REF_LIB = os.path.join(HERE, "_ref", "libbiofvm_ref.so")
+DROPIN_LIB = os.path.join(HERE, "_ref", "libbiofvm_dropin.so")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_bp = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Port:
+    """The plain-C restatement of the reference path."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not os.path.exists(PORT_LIB):
+                raise FileNotFoundError(f"{PORT_LIB} missing: run `make -C oracle port`")
+            L = C.CDLL(PORT_LIB)
+            L.orc_thomas_axis.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_double, _dp, _dp, _dp]
+            L.orc_apply_dirichlet.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_int, _bp, _dp]
+            L.orc_lod3d_step.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_double,
+                                         C.c_double, _bp, _dp, C.c_int]
+            L.orc_agent_constants.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp,
+                                              _dp, _dp, _dp, _dp]
+            L.orc_sources.argtypes = [_dp, C.c_int, C.c_int, _ip, C.c_void_p, _dp, _dp, _dp]
+            L.orc_nearest_voxel.argtypes = [C.c_double] * 7 + [C.c_int] * 3
+            L.orc_nearest_voxel.restype = C.c_int
+            cls._lib = L
+        return cls._lib
+
+    @classmethod
+    def thomas_axis(cls, n, D, decay, dt, dx):
+        S = len(D)
+        denom = np.zeros(n * S)
+        cup = np.zeros(n * S)
+        c1 = np.zeros(S)
+        cls.lib().orc_thomas_axis(n, S, _f64(D), _f64(decay), dt, dx, denom, cup, c1)
+        return denom.reshape(n, S), cup.reshape(n, S), c1
+
+    @classmethod
+    def apply_dirichlet(cls, field, shape, active, dvals):
+        nx, ny, nz, S = shape
+        cls.lib().orc_apply_dirichlet(field, nx, ny, nz, S, np.ascontiguousarray(active, np.uint8), _f64(dvals))
+
+    @classmethod
+    def lod_step(cls, field, shape, D, decay, dt, dx, active, dvals, threads=0):
+        """One LOD diffusion-decay step, in place on ``field`` (float64, reference layout)."""
+        nx, ny, nz, S = shape
+        cls.lib().orc_lod3d_step(field, nx, ny, nz, S, _f64(D), _f64(decay), dt, dx,
+                                 np.ascontiguousarray(active, np.uint8), _f64(dvals), threads)
+
+    @classmethod
+    def agent_constants(cls, dt, volume, voxel_volume, sec, upt, sat, exp_):
+        """Per-agent (c1, c2, e2) rows for arrays of shape [n, S]."""
+        sec, upt, sat, exp_ = (np.atleast_2d(_f64(a)) for a in (sec, upt, sat, exp_))
+        n, S = sec.shape
+        vol = np.broadcast_to(np.asarray(volume, np.float64), (n,))
+        c1 = np.zeros((n, S))
+        c2 = np.zeros((n, S))
+        e2 = np.zeros((n, S))
+        L = cls.lib()
+        o1, o2, o3 = np.zeros(S), np.zeros(S), np.zeros(S)
+        for a in range(n):
+            L.orc_agent_constants(S, dt, float(vol[a]), voxel_volume, _f64(sec[a]), _f64(upt[a]),
+                                  _f64(sat[a]), _f64(exp_[a]), o1, o2, o3)
+            c1[a], c2[a], e2[a] = o1, o2, o3
+        return c1, c2, e2
+
+    @classmethod
+    def sources(cls, field, S, voxel, c1, c2, e2, active=None):
+        voxel = np.ascontiguousarray(voxel, np.int32)
+        act = None
+        if active is not None:
+            act_arr = np.ascontiguousarray(active, np.uint8)
+            act = act_arr.ctypes.data
+        cls.lib().orc_sources(field, S, len(voxel), voxel, act, _f64(c1).ravel(), _f64(c2).ravel(),
+                              _f64(e2).ravel())
+
+    @classmethod
+    def nearest_voxel(cls, pos, origin, dx, dims):
+        L = cls.lib()
+        out = np.empty(len(pos), np.int32)
+        for a, (x, y, z) in enumerate(pos):
+            out[a] = L.orc_nearest_voxel(x, y, z, origin[0], origin[1], origin[2], dx, *dims)
+        return out
+
+    @classmethod
+    def run(cls, wl, nsteps=None, threads=0):
+        """Run a workload (see physicell-x_b200/bfvm/workloads.py) for nsteps of
+        [agent sources ; LOD diffusion step], returning the final field."""
+        nsteps = wl.steps if nsteps is None else nsteps
+        field = wl.field0.copy()
+        c1, c2, e2 = cls.workload_constants(wl)
+        dv = wl.dirichlet_values
+        for _ in range(nsteps):
+            if wl.n_agents:
+                cls.sources(field, wl.S, wl.agent_voxel, c1, c2, e2)
+            cls.lod_step(field, wl.shape, wl.D, wl.decay, wl.dt, wl.dx, wl.dirichlet_active, dv, threads)
+        return field
+
+    @classmethod
+    def workload_constants(cls, wl):
+        """(c1, c2, e2) of every agent of a workload, [n, S] each."""
+        if wl.n_agents == 0:
+            z = np.zeros((0, wl.S))
+            return z, z, z
+        return cls.agent_constants(wl.dt, wl.agent_volume, wl.voxel_volume, wl.secretion, wl.uptake,
+                                   wl.saturation, wl.net_export)
+
+
+class Reference:
+    """The reference's own BioFVM solver and agents, built from its sources."""
+
+    _libs: dict = {}
+
+    def __init__(self, wl, threads=0, dropin=False):
+        self.L = self.lib(dropin)
+        self.wl = wl
+        nx, ny, nz, S = wl.shape
+        self.h = self.L.ref_env_create(nx, ny, nz, wl.dx, wl.origin[0], wl.origin[1], wl.origin[2], S,
+                                       _f64(wl.D), _f64(wl.decay))
+        if not self.h:
+            raise RuntimeError("reference mesh creation failed")
+        for d in range(S):
+            self.L.ref_env_set_dirichlet_activation(self.h, d, int(wl.dirichlet_active[d]))
+        self.L.ref_env_set_dirichlet_face_values(self.h, _f64(wl.dirichlet_values))
+        self.L.ref_env_set_field(self.h, _f64(wl.field0))
+        self.agent_index = []
+        for a in range(wl.n_agents):
+            idx = self.L.ref_env_add_agent(self.h, *map(float, wl.agent_pos[a]), float(wl.agent_volume[a]),
+                                           _f64(wl.secretion[a]), _f64(wl.uptake[a]), _f64(wl.saturation[a]),
+                                           _f64(wl.net_export[a]))
+            self.agent_index.append(idx)
+        self.threads = threads
+
+    @classmethod
+    def available(cls, dropin=False):
+        return os.path.exists(DROPIN_LIB if dropin else REF_LIB)
+
+    @classmethod
+    def lib(cls, dropin=False):
+        path = DROPIN_LIB if dropin else REF_LIB
+        if path not in cls._libs:
+            if not os.path.exists(path):
+                raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` (needs the reference sources)")
+            L = C.CDLL(path)
+            vp = C.c_void_p
+            L.ref_env_create.restype = vp
+            L.ref_env_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                         C.c_int, _dp, _dp]
+            L.ref_env_destroy.argtypes = [vp]
+            L.ref_env_set_field.argtypes = [vp, _dp]
+            L.ref_env_get_field.argtypes = [vp, _dp]
+            L.ref_env_set_dirichlet_activation.argtypes = [vp, C.c_int, C.c_int]
+            L.ref_env_set_dirichlet_face_values.argtypes = [vp, _dp]
+            L.ref_env_apply_dirichlet.argtypes = [vp]
+            L.ref_env_add_agent.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp, _dp]
+            L.ref_env_add_agent.restype = C.c_int
+            L.ref_env_num_agents.argtypes = [vp]
+            L.ref_env_agent_voxel.argtypes = [vp, C.c_int]
+            L.ref_env_agent_constants.argtypes = [vp, C.c_int, C.c_double, _dp, _dp, _dp]
+            L.ref_env_sources.argtypes = [vp, C.c_double, C.c_int]
+            L.ref_env_diffusion.argtypes = [vp, C.c_double, C.c_int, C.c_int]
+            L.ref_env_diffusion.restype = C.c_int
+            L.ref_env_run.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]
+            L.ref_env_run.restype = C.c_int
+            L.ref_max_threads.restype = C.c_int
+            if dropin:
+                L.ref_env_dropin_fuse_sources.argtypes = [vp, C.c_int, C.c_double]
+                L.ref_env_dropin_fuse_sources.restype = C.c_int
+            cls._libs[path] = L
+        return cls._libs[path]
+
+    def close(self):
+        if self.h:
+            self.L.ref_env_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def field(self):
+        out = np.empty(int(np.prod(self.wl.shape)), np.float64)
+        self.L.ref_env_get_field(self.h, out)
+        return out
+
+    def set_field(self, f):
+        self.L.ref_env_set_field(self.h, _f64(f))
+
+    def agent_voxels(self):
+        return np.array([self.L.ref_env_agent_voxel(self.h, a) for a in range(self.L.ref_env_num_agents(self.h))],
+                        np.int32)
+
+    def agent_constants(self, dt):
+        S = self.wl.S
+        n = self.L.ref_env_num_agents(self.h)
+        c1, c2, e2 = np.zeros((n, S)), np.zeros((n, S)), np.zeros((n, S))
+        o1, o2, o3 = np.zeros(S), np.zeros(S), np.zeros(S)
+        for a in range(n):
+            self.L.ref_env_agent_constants(self.h, a, dt, o1, o2, o3)
+            c1[a], c2[a], e2[a] = o1, o2, o3
+        return c1, c2, e2
+
+    def sources(self, threads=1):
+        self.L.ref_env_sources(self.h, self.wl.dt, threads)
+
+    def diffusion(self, solver=0, threads=None):
+        rc = self.L.ref_env_diffusion(self.h, self.wl.dt, solver, self.threads if threads is None else threads)
+        if rc != 0:
+            raise RuntimeError(f"ref_env_diffusion solver={solver} rc={rc}")
+
+    def apply_dirichlet(self):
+        self.L.ref_env_apply_dirichlet(self.h)
+
+    def run(self, nsteps=None, solver=0, threads=None, sources_threads=1, fetch=True):
+        nsteps = self.wl.steps if nsteps is None else nsteps
+        rc = self.L.ref_env_run(self.h, self.wl.dt, nsteps, solver, self.threads if threads is None else threads,
+                                sources_threads)
+        if rc != 0:
+            raise RuntimeError(f"ref_env_run rc={rc}")
+        return self.field() if fetch else None
+
+
+def max_threads():
+    if Reference.available():
+        return int(Reference.lib().ref_max_threads())
+    return os.cpu_count() or 1
+
+
+def timed(fn, *a, **k):
+    t0 = time.perf_counter()
+    r = fn(*a, **k)
+    return r, time.perf_counter() - t0

@@ -1,0 +1,270 @@
+/*
+ * ref_driver.cpp -- TEST INFRASTRUCTURE (part of the oracle).
+ *
+ * A small extern "C" driver around the reference BioFVM public API, compiled
+ * together with the unmodified reference sources (BioFVM/*.cpp, DistPhy/*.cpp)
+ * and the single-rank MPI shim (oracle/mpi_shim/mpi.h) into
+ * oracle/_ref/libbiofvm_ref.so by oracle/Makefile.  Only the tests, smoke()
+ * and bench.py's CPU-baseline leg load that library, as the checker.
+ *
+ * What it drives (all reference code, nothing re-implemented here):
+ *   - Microenvironment::resize_space(..., world, cart)   BioFVM_microenvironment.cpp:584-607
+ *   - set_density / add_density                           BioFVM_microenvironment.cpp
+ *   - update_dirichlet_node / set_substrate_dirichlet_activation  :224-282
+ *   - apply_dirichlet_boundaries_conditions(rank,size)    :348-446
+ *   - diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING  BioFVM_solvers.cpp:102-780
+ *   - diffusion_decay_solver__constant_coefficients_LOD_3D_AVX256D   BioFVM_solvers.cpp:796-1665
+ *   - Microenvironment::simulate_cell_sources_and_sinks(list, dt)     :1370-1379
+ *       -> Basic_Agent::simulate_secretion_and_uptake      BioFVM_basic_agent.cpp:509-559
+ *       -> Basic_Agent::set_internal_uptake_constants      BioFVM_basic_agent.cpp:224-274
+ *   - Basic_Agent::assign_position / update_voxel_index    BioFVM_basic_agent.cpp:159-186
+ *
+ * With -DBFVM_WITH_DROPIN the same driver can also route a step through the
+ * project's drop-in definition of the 4-argument
+ * diffusion_decay_solver__constant_coefficients_LOD_3D (declared at
+ * BioFVM_solvers.h:66, friend at BioFVM_microenvironment.h:349), which is how
+ * the drop-in is tested inside the reference's own Microenvironment.
+ */
+#include <omp.h>
+
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "BioFVM.h"
+#include "BioFVM_agent_container.h"
+#include "BioFVM_solvers.h"
+#include "DistPhy/DistPhy_Cartesian.h"
+#include "DistPhy/DistPhy_Environment.h"
+
+using namespace BioFVM;
+using DistPhy::mpi::mpi_Cartesian;
+using DistPhy::mpi::mpi_Environment;
+
+#ifdef BFVM_WITH_DROPIN
+namespace BioFVM {
+/* Provided by physicell-x_b200/host/biofvm_b200_dropin.cpp. */
+void bfvm_b200_release(Microenvironment& M);
+int bfvm_b200_set_fused_sources(Microenvironment& M, std::vector<Basic_Agent*>* agents, double dt);
+}
+#endif
+
+namespace {
+
+mpi_Environment g_world;
+mpi_Cartesian g_cart;
+bool g_mpi_ready = false;
+
+void ensure_world() {
+  if (g_mpi_ready) return;
+  g_world.Initialize();
+  g_cart.Build_Cartesian_Topology(g_world);
+  g_cart.Find_Cartesian_Coordinates(g_world);
+  g_cart.Find_Left_Right_Neighbours(g_world);
+  g_mpi_ready = true;
+}
+
+struct RefEnv {
+  Microenvironment* M = nullptr;
+  std::vector<Basic_Agent*> agents;
+  int nx = 0, ny = 0, nz = 0, S = 0;
+};
+
+}  // namespace
+
+extern "C" {
+
+/* Create a uniform nx*ny*nz grid of edge dx starting at (x0,y0,z0), with S
+ * substrates of the given diffusion coefficients and decay rates.  Returns
+ * NULL if the reference mesh does not come out with the requested shape. */
+void* ref_env_create(int nx, int ny, int nz, double dx, double x0, double y0, double z0, int S,
+                     const double* D, const double* decay) {
+  ensure_world();
+  RefEnv* e = new RefEnv();
+  e->M = new Microenvironment("oracle");
+  e->M->agent_container = new Agent_Container();
+  Microenvironment& M = *e->M;
+  M.set_density(0, "s0", "none", D[0], decay[0]);
+  for (int d = 1; d < S; ++d) {
+    char name[32];
+    std::snprintf(name, sizeof(name), "s%d", d);
+    M.add_density(name, "none", D[d], decay[d]);
+  }
+  M.resize_space(x0, x0 + nx * dx, y0, y0 + ny * dx, z0, z0 + nz * dx, dx, dx, dx, g_world, g_cart);
+  M.diffusion_decay_solver_mpi = diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING;
+  if ((int)M.mesh.x_coordinates.size() != nx || (int)M.mesh.y_coordinates.size() != ny ||
+      (int)M.mesh.z_coordinates.size() != nz || (int)M.number_of_densities() != S) {
+    std::fprintf(stderr, "ref_env_create: mesh came out %zu x %zu x %zu (S=%u)\n",
+                 M.mesh.x_coordinates.size(), M.mesh.y_coordinates.size(),
+                 M.mesh.z_coordinates.size(), M.number_of_densities());
+    delete e->M;
+    delete e;
+    return nullptr;
+  }
+  e->nx = nx;
+  e->ny = ny;
+  e->nz = nz;
+  e->S = S;
+  return e;
+}
+
+void ref_env_destroy(void* h) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  if (!e) return;
+#ifdef BFVM_WITH_DROPIN
+  bfvm_b200_release(*e->M);
+#endif
+  for (Basic_Agent* a : e->agents) delete a;
+  delete e->M->agent_container;
+  delete e->M;
+  delete e;
+}
+
+long long ref_env_num_values(void* h) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  return (long long)e->nx * e->ny * e->nz * e->S;
+}
+
+/* Field in the reference layout: flat [x][y][z][substrate]. */
+void ref_env_set_field(void* h, const double* aos) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  std::memcpy(e->M->p_density_vectors->data(), aos, sizeof(double) * ref_env_num_values(h));
+}
+
+void ref_env_get_field(void* h, double* aos) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  std::memcpy(aos, e->M->p_density_vectors->data(), sizeof(double) * ref_env_num_values(h));
+}
+
+void ref_env_set_dirichlet_activation(void* h, int substrate, int on) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  e->M->set_substrate_dirichlet_activation(substrate, on != 0);
+}
+
+/* Dirichlet values for every voxel on the six outer faces, read from a full
+ * grid in the reference layout (interior entries are ignored). */
+void ref_env_set_dirichlet_face_values(void* h, const double* aos) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  const int nx = e->nx, ny = e->ny, nz = e->nz, S = e->S;
+  std::vector<double> v(S);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        if (!(i == 0 || i == nx - 1 || j == 0 || j == ny - 1 || k == 0 || k == nz - 1)) continue;
+        int vox = e->M->voxel_index(i, j, k);
+        for (int d = 0; d < S; ++d) v[d] = aos[(long long)vox * S + d];
+        e->M->update_dirichlet_node(vox, v);
+      }
+}
+
+void ref_env_apply_dirichlet(void* h) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  e->M->apply_dirichlet_boundaries_conditions(0, 1);
+}
+
+/* Add one agent through the reference API.  Rates are [S] arrays.  Returns
+ * the agent's index in this environment's list, or -1 if the reference
+ * rejects the position. */
+int ref_env_add_agent(void* h, double x, double y, double z, double volume, const double* secretion,
+                      const double* uptake, const double* saturation, const double* net_export) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  Basic_Agent* a = new Basic_Agent();
+  a->register_microenvironment(e->M);
+  if (!a->assign_position(x, y, z)) {
+    delete a;
+    return -1;
+  }
+  for (int d = 0; d < e->S; ++d) {
+    (*a->secretion_rates)[d] = secretion[d];
+    (*a->uptake_rates)[d] = uptake[d];
+    (*a->saturation_densities)[d] = saturation[d];
+    (*a->net_export_rates)[d] = net_export[d];
+  }
+  a->set_total_volume(volume);
+  e->agents.push_back(a);
+  return (int)e->agents.size() - 1;
+}
+
+int ref_env_num_agents(void* h) { return (int)static_cast<RefEnv*>(h)->agents.size(); }
+
+int ref_env_agent_voxel(void* h, int a) {
+  return static_cast<RefEnv*>(h)->agents[a]->get_current_voxel_index();
+}
+
+/* The agent's implicit source/sink constants for time step dt, as the
+ * reference computes them (set_internal_uptake_constants). */
+void ref_env_agent_constants(void* h, int a, double dt, double* c1, double* c2, double* e2) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  Basic_Agent* ag = e->agents[a];
+  ag->set_internal_uptake_constants(dt);
+  for (int d = 0; d < e->S; ++d) {
+    c1[d] = ag->get_cell_source_sink_solver_temp1()[d];
+    c2[d] = ag->get_cell_source_sink_solver_temp2()[d];
+    e2[d] = ag->get_cell_source_sink_solver_temp_export2()[d];
+  }
+}
+
+/* simulate_cell_sources_and_sinks over this environment's agents with the
+ * given OpenMP thread count (1 = the deterministic oracle mode). */
+void ref_env_sources(void* h, double dt, int threads) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  omp_set_num_threads(threads > 0 ? threads : 1);
+  e->M->simulate_cell_sources_and_sinks(e->agents, dt);
+}
+
+/* One diffusion-decay step.  solver: 0 = _BLOCKING (what
+ * initialize_microenvironment(world,cart) installs), 1 = _AVX256D (constructor
+ * default; it has no final Dirichlet pin), 2 = the project's drop-in (only in
+ * the drop-in build).  Returns 0, or -1 for an unknown solver. */
+int ref_env_diffusion(void* h, double dt, int solver, int threads) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  omp_set_num_threads(threads > 0 ? threads : 1);
+  switch (solver) {
+    case 0:
+      e->M->diffusion_decay_solver_mpi = diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING;
+      break;
+    case 1:
+      e->M->diffusion_decay_solver_mpi = diffusion_decay_solver__constant_coefficients_LOD_3D_AVX256D;
+      break;
+#ifdef BFVM_WITH_DROPIN
+    case 2:
+      e->M->diffusion_decay_solver_mpi = diffusion_decay_solver__constant_coefficients_LOD_3D;
+      break;
+#endif
+    default:
+      return -1;
+  }
+  e->M->simulate_diffusion_decay(dt, g_world, g_cart);
+  return 0;
+}
+
+/* nsteps of [sources (sources_threads) ; diffusion (solver, threads)]. */
+int ref_env_run(void* h, double dt, int nsteps, int solver, int threads, int sources_threads) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  for (int s = 0; s < nsteps; ++s) {
+    if (!e->agents.empty()) ref_env_sources(h, dt, sources_threads);
+    if (ref_env_diffusion(h, dt, solver, threads) != 0) return -1;
+  }
+  return 0;
+}
+
+int ref_has_dropin(void) {
+#ifdef BFVM_WITH_DROPIN
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+#ifdef BFVM_WITH_DROPIN
+/* Route this environment's agents through the drop-in's fused GPU source
+ * stage on every following drop-in step (pass enable=0 to turn it off). */
+int ref_env_dropin_fuse_sources(void* h, int enable, double dt) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  return bfvm_b200_set_fused_sources(*e->M, enable ? &e->agents : nullptr, dt);
+}
+#endif
+
+int ref_max_threads(void) { return omp_get_max_threads(); }
+
+}  // extern "C"

@@ -1,0 +1,221 @@
+"""Python mirror of the reference's Microenvironment interface for the
+diffusion-decay path, over the C ABI.
+
+Names follow the reference API so that a test reads like the reference's
+own calls:
+
+=====================================================  ==========================================
+reference (BioFVM, PhysiCell-X 1.14.0)                 here
+=====================================================  ==========================================
+``Microenvironment::resize_space`` + ``set_density``   ``Microenvironment(nx, ny, nz, dx, dt, D, decay)``
+``set_substrate_dirichlet_activation(d, bool)``        ``set_substrate_dirichlet_activation(d, on)``
+``update_dirichlet_node`` on face voxels               ``set_dirichlet_face`` / ``set_dirichlet_uniform``
+``density_vector`` writes / reads                      ``upload_field`` / ``download_field``
+``simulate_diffusion_decay(dt, world, cart)``          ``simulate_diffusion_decay(nsteps=1)``
+``simulate_cell_sources_and_sinks(dt)``                ``simulate_cell_sources_and_sinks()``
+``Basic_Agent::nearest_density_vector``                ``sample_agents()``
+=====================================================  ==========================================
+
+Errors raise :class:`bfvm._lib.BfvmError` carrying the C status code; the
+solve is left unchanged on failure, as the reference prints and returns
+(BioFVM/BioFVM_solvers.cpp:116-121).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import BFVM_FP32, BFVM_FP64, BFVM_STEP_SOURCES, FACES, check
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Microenvironment:
+    """One microenvironment resident on one GPU."""
+
+    def __init__(self, nx, ny, nz, dx, dt, diffusion_coefficients, decay_rates, precision="fp64", device=0):
+        self.L = _lib.lib()
+        D = _f64(diffusion_coefficients).ravel()
+        lam = _f64(decay_rates).ravel()
+        if D.shape != lam.shape:
+            raise ValueError("diffusion_coefficients and decay_rates differ in length")
+        self.shape = (int(nx), int(ny), int(nz), int(D.size))
+        self.dx, self.dt = float(dx), float(dt)
+        self.precision = precision
+        cfg = _lib.bfvm_config(int(nx), int(ny), int(nz), int(D.size), float(dx), float(dt),
+                               D.ctypes.data_as(C.POINTER(C.c_double)), lam.ctypes.data_as(C.POINTER(C.c_double)),
+                               BFVM_FP64 if precision == "fp64" else BFVM_FP32, int(device))
+        h = C.c_void_p()
+        check(self.L.bfvm_create(C.byref(cfg), C.byref(h)), "bfvm_create")
+        self.h = h
+        self.n_agents = 0
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bfvm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def S(self):
+        return self.shape[3]
+
+    @property
+    def n_values(self):
+        nx, ny, nz, S = self.shape
+        return nx * ny * nz * S
+
+    # -- Dirichlet ----------------------------------------------------------
+    def set_dirichlet_activation(self, active):
+        a = np.ascontiguousarray(active, np.uint8).ravel()
+        if a.size != self.S:
+            raise ValueError("activation needs one flag per substrate")
+        check(self.L.bfvm_set_dirichlet_activation(self.h, _ptr(a)), "bfvm_set_dirichlet_activation")
+
+    def set_substrate_dirichlet_activation(self, substrate, on):
+        act = getattr(self, "_active", np.ones(self.S, np.uint8)).copy()
+        act[substrate] = 1 if on else 0
+        self.set_dirichlet_activation(act)
+        self._active = act
+
+    def set_dirichlet_uniform(self, values):
+        v = _f64(values).ravel()
+        check(self.L.bfvm_set_dirichlet_uniform(self.h, _ptr(v)), "bfvm_set_dirichlet_uniform")
+
+    def set_dirichlet_face(self, face, plane):
+        f = FACES[face] if isinstance(face, str) else int(face)
+        p = _f64(plane)
+        check(self.L.bfvm_set_dirichlet_face(self.h, f, _ptr(p)), "bfvm_set_dirichlet_face")
+
+    # -- field --------------------------------------------------------------
+    def upload_field(self, field):
+        f = _f64(field).ravel()
+        if f.size != self.n_values:
+            raise ValueError(f"field has {f.size} values, expected {self.n_values}")
+        check(self.L.bfvm_upload_field(self.h, _ptr(f)), "bfvm_upload_field")
+
+    def download_field(self, out=None):
+        out = np.empty(self.n_values, np.float64) if out is None else out
+        check(self.L.bfvm_download_field(self.h, _ptr(out)), "bfvm_download_field")
+        return out
+
+    def upload_field_device(self, ptr):
+        check(self.L.bfvm_upload_field_device(self.h, C.c_void_p(int(ptr))), "bfvm_upload_field_device")
+
+    def download_field_device(self, ptr):
+        check(self.L.bfvm_download_field_device(self.h, C.c_void_p(int(ptr))), "bfvm_download_field_device")
+
+    # -- agents -------------------------------------------------------------
+    def set_agents(self, voxel, c1, c2, e2, active=None):
+        v = np.ascontiguousarray(voxel, np.int32).ravel()
+        n = v.size
+        c1, c2, e2 = (_f64(x).reshape(n, self.S) for x in (c1, c2, e2))
+        act = None if active is None else np.ascontiguousarray(active, np.uint8).ravel()
+        check(self.L.bfvm_set_agents(self.h, n, _ptr(v), _ptr(act), _ptr(c1), _ptr(c2), _ptr(e2)),
+              "bfvm_set_agents")
+        self.n_agents = n
+
+    def set_agents_from_rates(self, voxel, volume, secretion, uptake, saturation, net_export, active=None):
+        v = np.ascontiguousarray(voxel, np.int32).ravel()
+        n = v.size
+        vol = _f64(np.broadcast_to(np.asarray(volume, np.float64), (n,)))
+        rates = [_f64(x).reshape(n, self.S) for x in (secretion, uptake, saturation, net_export)]
+        act = None if active is None else np.ascontiguousarray(active, np.uint8).ravel()
+        check(self.L.bfvm_set_agents_from_rates(self.h, n, _ptr(v), _ptr(act), _ptr(vol), *[_ptr(r) for r in rates]),
+              "bfvm_set_agents_from_rates")
+        self.n_agents = n
+
+    def sample_agents(self):
+        out = np.empty((self.n_agents, self.S), np.float64)
+        check(self.L.bfvm_sample_agents(self.h, _ptr(out)), "bfvm_sample_agents")
+        return out
+
+    # -- stepping -----------------------------------------------------------
+    def simulate_diffusion_decay(self, nsteps=1, sources=False):
+        """nsteps LOD steps; with sources=True each step first applies the agents
+        (fused into the x sweep)."""
+        check(self.L.bfvm_step(self.h, int(nsteps), BFVM_STEP_SOURCES if sources else 0), "bfvm_step")
+
+    def simulate_cell_sources_and_sinks(self):
+        check(self.L.bfvm_apply_sources(self.h), "bfvm_apply_sources")
+
+    def synchronize(self):
+        check(self.L.bfvm_synchronize(self.h), "bfvm_synchronize")
+
+    def field_sums(self):
+        out = np.empty(self.S, np.float64)
+        check(self.L.bfvm_field_sums(self.h, _ptr(out)), "bfvm_field_sums")
+        return out
+
+    # -- introspection --------------------------------------------------------
+    @property
+    def stream(self):
+        return int(self.L.bfvm_stream(self.h) or 0)
+
+    def set_stream(self, stream_ptr):
+        check(self.L.bfvm_set_stream(self.h, C.c_void_p(int(stream_ptr) if stream_ptr else None)), "bfvm_set_stream")
+
+    def device_field(self):
+        p, pitch, eb = C.c_void_p(), C.c_int(), C.c_int()
+        check(self.L.bfvm_device_field(self.h, C.byref(p), C.byref(pitch), C.byref(eb)), "bfvm_device_field")
+        return int(p.value or 0), int(pitch.value), int(eb.value)
+
+    def device_bytes(self):
+        return int(self.L.bfvm_device_bytes(self.h))
+
+    def timing_enable(self, on=True):
+        check(self.L.bfvm_timing_enable(self.h, 1 if on else 0), "bfvm_timing_enable")
+
+    def timing_read(self):
+        """(ms_x, ms_y, ms_z) summed over the recorded steps, and the step count."""
+        ms = np.zeros(3, np.float64)
+        n = C.c_int()
+        check(self.L.bfvm_timing_read(self.h, _ptr(ms), C.byref(n)), "bfvm_timing_read")
+        return ms, int(n.value)
+
+    def get_launch(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(self.L.bfvm_get_launch(self.h, C.byref(a), C.byref(b), C.byref(c)), "bfvm_get_launch")
+        return a.value, b.value, c.value
+
+    def set_launch(self, x_lines, yz_tile, yz_chunk):
+        check(self.L.bfvm_set_launch(self.h, int(x_lines), int(yz_tile), int(yz_chunk)), "bfvm_set_launch")
+
+    # -- convenience ----------------------------------------------------------
+    @classmethod
+    def from_workload(cls, wl, precision="fp64", device=0, agents="rates", upload=True):
+        """Build a solve from a :class:`bfvm.workloads.Workload`: coefficients,
+        Dirichlet activation and per-face values, initial field and agents."""
+        me = cls(wl.nx, wl.ny, wl.nz, wl.dx, wl.dt, wl.D, wl.decay, precision=precision, device=device)
+        me.set_dirichlet_activation(wl.dirichlet_active)
+        if wl.uniform_faces():
+            me.set_dirichlet_uniform(wl.face_values[0])
+        else:
+            for f, plane in enumerate(wl.face_planes()):
+                me.set_dirichlet_face(f, plane)
+        if upload:
+            me.upload_field(wl.field0)
+        if wl.n_agents and agents == "rates":
+            me.set_agents_from_rates(wl.agent_voxel, wl.agent_volume, wl.secretion, wl.uptake, wl.saturation,
+                                     wl.net_export)
+        return me

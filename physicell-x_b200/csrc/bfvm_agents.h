@@ -1,0 +1,49 @@
+// bfvm_agents.h -- device agent list: constants, stable voxel sort, line CSR,
+// standalone source/sink stage and density sampling.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+namespace bfvm {
+
+struct AgentBuild {
+  int n;                       // agents in the list (active or not)
+  int S, nx, ny, nz;
+  const int* voxel;            // [n] reference voxel index, <0 = none
+  const unsigned char* active; // [n] or nullptr (all active)
+  const double* c1;            // [n][S] constants in agent-list order
+  const double* c2;
+  const double* e2;
+  void* scratch;               // agent_scratch_bytes(n) bytes of device memory
+  // outputs
+  unsigned* dev_voxel;         // [n] device voxel id per agent (list order); nx*ny*nz = none
+  unsigned* sorted_keys;       // [n] device voxel ids, ascending (stable)
+  int* sorted_vals;            // [n] agent index per sorted position
+  int* line_off;               // [ny*nz + 1] CSR over x-lines (line = k*ny + j)
+  int* a_i;                    // [n] x index per sorted position
+  double* ac1;                 // [S][n] constants per sorted position
+  double* ac2;
+  double* ae2;
+  int* n_valid;                // device scalar: agents with a voxel
+};
+
+size_t agent_scratch_bytes(int n);
+
+cudaError_t agents_compute_constants(int n, int S, double dt, double voxel_volume, const double* volume,
+                                     const double* sec, const double* upt, const double* sat, const double* exp_,
+                                     double* c1, double* c2, double* e2, cudaStream_t st);
+
+// Sorts and bins the list; *launches receives the number of kernels launched.
+cudaError_t agents_build(const AgentBuild& b, cudaStream_t st, int* launches);
+
+template <typename T>
+cudaError_t agents_apply_sources(int n, const unsigned* sorted_keys, int S, int nx, int ny, int nz, int nxp,
+                                 const double* ac1, const double* ac2, const double* ae2, T* f, cudaStream_t st);
+
+template <typename T>
+cudaError_t agents_sample(int n, const unsigned* dev_voxel, int S, int nx, int ny, int nz, int nxp, const T* f,
+                          double* out, cudaStream_t st);
+
+}  // namespace bfvm

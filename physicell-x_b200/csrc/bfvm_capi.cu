@@ -1,0 +1,847 @@
+// bfvm_capi.cu -- the C ABI (include/biofvm_b200.h): one resident
+// microenvironment solve per handle.
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "../../include/biofvm_b200.h"
+#include "bfvm_agents.h"
+#include "bfvm_internal.h"
+
+using namespace bfvm;
+
+namespace bfvm {
+
+static std::atomic<long long> g_launches{0};
+void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Thomas factorization of one axis, FP64, operation by operation as in
+// diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING
+// (BioFVM/BioFVM_solvers.cpp:196-329, one rank): outputs [n][S] like the
+// reference's thomas_denom*/thomas_c* and c1[S] = thomas_constant1.
+// Contractions are written out with std::fma (this file is compiled with
+// -ffp-contract=off), matching the reference's g++ FMA contraction of axpy.
+void thomas_axis_host(int n, int S, const double* D, const double* decay, double dt, double dx, double* denom,
+                      double* cup, double* c1) {
+  for (int d = 0; d < S; ++d) {
+    double k1 = D[d];
+    k1 *= dt;
+    k1 /= dx;
+    k1 /= dx;
+    const double k1a = k1 * -1.0;
+    double k2 = decay[d];
+    k2 *= dt;
+    k2 /= 3.0;
+    double k3 = 1.0;
+    k3 += k1;
+    k3 += k1;
+    k3 += k2;
+    double k3a = 1.0;
+    k3a += k1;
+    k3a += k2;
+    c1[d] = k1;
+    for (int i = 0; i < n; ++i) {
+      cup[static_cast<size_t>(i) * S + d] = k1a;
+      denom[static_cast<size_t>(i) * S + d] = k3;
+    }
+    denom[d] = k3a;
+    denom[static_cast<size_t>(n - 1) * S + d] = k3a;
+    if (n == 1) {
+      double v = 1.0;
+      v += k2;
+      denom[d] = v;
+    }
+    cup[d] /= denom[d];
+    for (int i = 1; i < n; ++i) {
+      const size_t a = static_cast<size_t>(i) * S + d, b = static_cast<size_t>(i - 1) * S + d;
+      denom[a] = std::fma(k1, cup[b], denom[a]);
+      cup[a] /= denom[a];
+    }
+  }
+}
+
+}  // namespace bfvm
+
+struct bfvm_ctx {
+  int device = 0;
+  int nx = 0, ny = 0, nz = 0, S = 0, nxp = 0, prec = BFVM_FP64, eb = 8;
+  double dx = 0, dt = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  void* f = nullptr;           // field, device layout
+  size_t field_bytes = 0;
+  // coefficients: per axis denom (f64) [S][n], rcp (T) [S][n], cup (T) [S][n]; c1 (T) [S]
+  double* d_denom = nullptr;   // x | y | z
+  void* d_rcp = nullptr;       // x | y | z
+  void* d_cup = nullptr;       // x | y | z
+  void* d_c1 = nullptr;
+  int* d_active = nullptr;
+  double* d_faces = nullptr;   // xface | yface | zface
+  int* d_status = nullptr;
+  double* d_sums = nullptr;    // partial sums + result
+  FieldMaps maps{};
+  SweepConfig cfg{};
+  // agents
+  int n_agents = 0, cap_agents = 0;
+  int* d_voxel = nullptr;
+  unsigned char* d_agent_active = nullptr;
+  double* d_c = nullptr;       // c1 | c2 | e2, [n][S] each
+  double* d_rates = nullptr;   // volume [n] | sec | upt | sat | exp [n][S]
+  unsigned* d_dev_voxel = nullptr;
+  unsigned* d_sorted_keys = nullptr;
+  int* d_sorted_vals = nullptr;
+  int* d_line_off = nullptr;
+  int* d_a_i = nullptr;
+  double* d_ac = nullptr;      // ac1 | ac2 | ae2, [S][n] each
+  int* d_nvalid = nullptr;
+  void* d_agent_scratch = nullptr;
+  double* d_sample = nullptr;
+  // host-side mirrors
+  std::vector<unsigned char> active;
+  size_t device_bytes = 0;
+  double* d_staging = nullptr; // reference-layout field, for host uploads/downloads
+  // per-kernel timing: 4 events per recorded step
+  bool timing = false;
+  int timed_steps = 0;
+  std::vector<cudaEvent_t> events;
+};
+
+namespace {
+
+#define BFVM_CUDA(call)                                                                                      \
+  do {                                                                                                       \
+    cudaError_t e__ = (call);                                                                                \
+    if (e__ != cudaSuccess) {                                                                                \
+      std::fprintf(stderr, "biofvm_b200: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e__), __FILE__, \
+                   __LINE__);                                                                                \
+      return e__ == cudaErrorMemoryAllocation ? BFVM_ERR_OOM : BFVM_ERR_CUDA;                                \
+    }                                                                                                        \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+int dalloc(bfvm_ctx* c, void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return e == cudaErrorMemoryAllocation ? BFVM_ERR_OOM : BFVM_ERR_CUDA;
+  }
+  c->device_bytes += bytes;
+  return BFVM_OK;
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+template <typename T>
+SweepParams<T> make_params(bfvm_ctx* c, bool sources) {
+  SweepParams<T> p{};
+  p.f = static_cast<T*>(c->f);
+  p.nx = c->nx;
+  p.ny = c->ny;
+  p.nz = c->nz;
+  p.S = c->S;
+  p.nxp = c->nxp;
+  p.c1 = static_cast<const T*>(c->d_c1);
+  p.active = c->d_active;
+  const size_t S = c->S;
+  p.xface = c->d_faces;
+  p.yface = p.xface + 2 * S * c->nz * c->ny;
+  p.zface = p.yface + 2 * S * c->nz * c->nx;
+  const T* rcp = static_cast<const T*>(c->d_rcp);
+  const T* cup = static_cast<const T*>(c->d_cup);
+  const size_t ox = 0, oy = S * c->nx, oz = oy + S * c->ny;
+  p.ax = {c->d_denom + ox, rcp + ox, cup + ox};
+  p.ay = {c->d_denom + oy, rcp + oy, cup + oy};
+  p.az = {c->d_denom + oz, rcp + oz, cup + oz};
+  if (sources && c->n_agents > 0) {
+    p.line_off = c->d_line_off;
+    p.a_i = c->d_a_i;
+    p.ac1 = c->d_ac;
+    p.ac2 = c->d_ac + S * c->n_agents;
+    p.ae2 = c->d_ac + 2 * S * c->n_agents;
+    p.n_sorted = c->n_agents;
+  }
+  p.status = c->d_status;
+  return p;
+}
+
+constexpr int kMaxTimedSteps = 4096;
+
+template <typename T>
+int run_steps(bfvm_ctx* c, int nsteps, bool sources) {
+  const SweepParams<T> p = make_params<T>(c, sources);
+  for (int s = 0; s < nsteps; ++s) {
+    cudaEvent_t* ev = nullptr;
+    if (c->timing && c->timed_steps < kMaxTimedSteps) {
+      const size_t need = 4 * static_cast<size_t>(c->timed_steps + 1);
+      while (c->events.size() < need) {
+        cudaEvent_t e;
+        BFVM_CUDA(cudaEventCreate(&e));
+        c->events.push_back(e);
+      }
+      ev = &c->events[4 * static_cast<size_t>(c->timed_steps)];
+      ++c->timed_steps;
+    }
+    if (ev) BFVM_CUDA(cudaEventRecord(ev[0], c->stream));
+    BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, c->stream));
+    if (ev) BFVM_CUDA(cudaEventRecord(ev[1], c->stream));
+    BFVM_CUDA(launch_sweep_y<T>(c->maps, p, c->cfg, c->stream));
+    if (ev) BFVM_CUDA(cudaEventRecord(ev[2], c->stream));
+    BFVM_CUDA(launch_sweep_z<T>(c->maps, p, c->cfg, c->stream));
+    if (ev) BFVM_CUDA(cudaEventRecord(ev[3], c->stream));
+    note_launches(3);
+  }
+  return BFVM_OK;
+}
+
+bool config_fits(int eb, int nx, int ny, int nz, const SweepConfig& cfg) {
+  const size_t lim = 227 * 1024;
+  return sweep_x_smem(eb, nx, cfg) <= lim && sweep_yz_smem(eb, ny, cfg) <= lim && sweep_yz_smem(eb, nz, cfg) <= lim;
+}
+
+// Default launch shape: 32 lines / 32 x-columns per CTA, shrunk (keeping the
+// TMA x-coordinate alignment) until the staged lines fit in shared memory.
+bool pick_config(int eb, int nx, int ny, int nz, SweepConfig* cfg) {
+  SweepConfig c;
+  c.x_lines = 32;
+  c.yz_tile = 32;
+  c.yz_chunk = 32;
+  const int min_tile = 16 / eb * 2;  // >= 16 bytes per TMA row and an even warp split
+  while (!config_fits(eb, nx, ny, nz, c)) {
+    bool changed = false;
+    if (sweep_x_smem(eb, nx, c) > 227 * 1024 && c.x_lines > 8) {
+      c.x_lines /= 2;
+      changed = true;
+    }
+    if ((sweep_yz_smem(eb, ny, c) > 227 * 1024 || sweep_yz_smem(eb, nz, c) > 227 * 1024) && c.yz_tile > min_tile) {
+      c.yz_tile /= 2;
+      changed = true;
+    }
+    if (!changed) return false;
+  }
+  *cfg = c;
+  return true;
+}
+
+int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
+  const int S = c->S;
+  const int n_axis[3] = {c->nx, c->ny, c->nz};
+  const size_t tot = static_cast<size_t>(S) * (c->nx + c->ny + c->nz);
+  std::vector<double> denom(tot), rcp64(tot), cup64(tot), c1(S);
+  size_t off = 0;
+  for (int ax = 0; ax < 3; ++ax) {
+    const int n = n_axis[ax];
+    std::vector<double> dn(static_cast<size_t>(n) * S), cu(static_cast<size_t>(n) * S);
+    thomas_axis_host(n, S, D, decay, c->dt, c->dx, dn.data(), cu.data(), c1.data());
+    for (int s = 0; s < S; ++s)
+      for (int i = 0; i < n; ++i) {
+        const double d = dn[static_cast<size_t>(i) * S + s];
+        denom[off + static_cast<size_t>(s) * n + i] = d;
+        rcp64[off + static_cast<size_t>(s) * n + i] = 1.0 / d;
+        cup64[off + static_cast<size_t>(s) * n + i] = cu[static_cast<size_t>(i) * S + s];
+      }
+    off += static_cast<size_t>(S) * n;
+  }
+  BFVM_CUDA(cudaMemcpy(c->d_denom, denom.data(), tot * 8, cudaMemcpyHostToDevice));
+  if (c->prec == BFVM_FP64) {
+    BFVM_CUDA(cudaMemcpy(c->d_rcp, rcp64.data(), tot * 8, cudaMemcpyHostToDevice));
+    BFVM_CUDA(cudaMemcpy(c->d_cup, cup64.data(), tot * 8, cudaMemcpyHostToDevice));
+    BFVM_CUDA(cudaMemcpy(c->d_c1, c1.data(), S * 8, cudaMemcpyHostToDevice));
+  } else {
+    // FP32 form: the FP64 factorization rounded once.
+    std::vector<float> r32(tot), c32(tot), k32(S);
+    for (size_t q = 0; q < tot; ++q) {
+      r32[q] = static_cast<float>(rcp64[q]);
+      c32[q] = static_cast<float>(cup64[q]);
+    }
+    for (int s = 0; s < S; ++s) k32[s] = static_cast<float>(c1[s]);
+    BFVM_CUDA(cudaMemcpy(c->d_rcp, r32.data(), tot * 4, cudaMemcpyHostToDevice));
+    BFVM_CUDA(cudaMemcpy(c->d_cup, c32.data(), tot * 4, cudaMemcpyHostToDevice));
+    BFVM_CUDA(cudaMemcpy(c->d_c1, k32.data(), S * 4, cudaMemcpyHostToDevice));
+  }
+  return BFVM_OK;
+}
+
+size_t face_elems(const bfvm_ctx* c) {
+  return 2ull * c->S * (static_cast<size_t>(c->nz) * c->ny + static_cast<size_t>(c->nz) * c->nx +
+                        static_cast<size_t>(c->ny) * c->nx);
+}
+
+int free_agents(bfvm_ctx* c) {
+  dfree(c->d_voxel);
+  dfree(c->d_agent_active);
+  dfree(c->d_c);
+  dfree(c->d_rates);
+  dfree(c->d_dev_voxel);
+  dfree(c->d_sorted_keys);
+  dfree(c->d_sorted_vals);
+  dfree(c->d_a_i);
+  dfree(c->d_ac);
+  dfree(c->d_agent_scratch);
+  dfree(c->d_sample);
+  c->d_voxel = nullptr;
+  c->d_agent_active = nullptr;
+  c->d_c = c->d_rates = c->d_ac = c->d_sample = nullptr;
+  c->d_dev_voxel = c->d_sorted_keys = nullptr;
+  c->d_sorted_vals = c->d_a_i = nullptr;
+  c->d_agent_scratch = nullptr;
+  c->cap_agents = 0;
+  return BFVM_OK;
+}
+
+int ensure_agent_capacity(bfvm_ctx* c, int n) {
+  if (n <= c->cap_agents && c->d_voxel != nullptr) return BFVM_OK;
+  free_agents(c);
+  const int cap = n < 1024 ? 1024 : n;
+  const size_t S = c->S;
+  int rc = BFVM_OK;
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_voxel), sizeof(int) * cap);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_agent_active), cap);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_c), sizeof(double) * 3 * S * cap);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_rates), sizeof(double) * (1 + 4 * S) * cap);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_dev_voxel), sizeof(unsigned) * cap);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_sorted_keys), sizeof(unsigned) * cap);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_sorted_vals), sizeof(int) * cap);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_a_i), sizeof(int) * cap);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_ac), sizeof(double) * 3 * S * cap);
+  if (rc == BFVM_OK) rc = dalloc(c, &c->d_agent_scratch, agent_scratch_bytes(cap));
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_sample), sizeof(double) * S * cap);
+  if (rc != BFVM_OK) {
+    free_agents(c);
+    return rc;
+  }
+  c->cap_agents = cap;
+  return BFVM_OK;
+}
+
+int build_agents(bfvm_ctx* c, int n) {
+  AgentBuild b{};
+  b.n = n;
+  b.S = c->S;
+  b.nx = c->nx;
+  b.ny = c->ny;
+  b.nz = c->nz;
+  b.voxel = c->d_voxel;
+  b.active = c->d_agent_active;
+  const size_t S = c->S;
+  b.c1 = c->d_c;
+  b.c2 = c->d_c + S * n;
+  b.e2 = c->d_c + 2 * S * n;
+  b.scratch = c->d_agent_scratch;
+  b.dev_voxel = c->d_dev_voxel;
+  b.sorted_keys = c->d_sorted_keys;
+  b.sorted_vals = c->d_sorted_vals;
+  b.line_off = c->d_line_off;
+  b.a_i = c->d_a_i;
+  b.ac1 = c->d_ac;
+  b.ac2 = c->d_ac + S * n;
+  b.ae2 = c->d_ac + 2 * S * n;
+  b.n_valid = c->d_nvalid;
+  int launches = 0;
+  BFVM_CUDA(agents_build(b, c->stream, &launches));
+  note_launches(launches);
+  c->n_agents = n;
+  return BFVM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bfvm_status_string(int s) {
+  switch (s) {
+    case BFVM_OK: return "ok";
+    case BFVM_ERR_ARG: return "invalid argument";
+    case BFVM_ERR_CUDA: return "CUDA error";
+    case BFVM_ERR_OOM: return "out of device memory";
+    case BFVM_ERR_SHAPE: return "unsupported grid shape";
+    case BFVM_ERR_NODEVICE: return "no CUDA device";
+    case BFVM_ERR_TIMEOUT: return "device wait timed out";
+    case BFVM_ERR_STATE: return "invalid state";
+    default: return "unknown status";
+  }
+}
+
+long long bfvm_kernel_launches(void) { return g_launches.load(); }
+
+int bfvm_create(const bfvm_config* cfg, bfvm_ctx** out) {
+  if (!cfg || !out || !cfg->diffusion_coefficients || !cfg->decay_rates) return BFVM_ERR_ARG;
+  *out = nullptr;
+  if (cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1 || cfg->n_substrates < 1 || cfg->n_substrates > kMaxSubstrates ||
+      !(cfg->dx > 0) || !(cfg->dt > 0) || (cfg->precision != BFVM_FP64 && cfg->precision != BFVM_FP32))
+    return BFVM_ERR_ARG;
+  const long long nvox = 1LL * cfg->nx * cfg->ny * cfg->nz;
+  if (nvox >= (1LL << 31) || cfg->nx > 65535 || cfg->ny > 65535 || cfg->nz > 65535) return BFVM_ERR_SHAPE;
+  for (int s = 0; s < cfg->n_substrates; ++s)
+    if (!(cfg->diffusion_coefficients[s] >= 0) || !(cfg->decay_rates[s] >= 0)) return BFVM_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return BFVM_ERR_NODEVICE;
+  }
+  if (cfg->device < 0 || cfg->device >= ndev) return BFVM_ERR_NODEVICE;
+  DeviceGuard g(cfg->device);
+  bfvm_ctx* c = new (std::nothrow) bfvm_ctx();
+  if (!c) return BFVM_ERR_OOM;
+  c->device = cfg->device;
+  c->nx = cfg->nx;
+  c->ny = cfg->ny;
+  c->nz = cfg->nz;
+  c->S = cfg->n_substrates;
+  c->prec = cfg->precision;
+  c->eb = c->prec == BFVM_FP64 ? 8 : 4;
+  c->dx = cfg->dx;
+  c->dt = cfg->dt;
+  const int row_align = 128 / c->eb;
+  c->nxp = (c->nx + row_align - 1) / row_align * row_align;
+  if (!pick_config(c->eb, c->nx, c->ny, c->nz, &c->cfg)) {
+    delete c;
+    return BFVM_ERR_SHAPE;
+  }
+  auto fail = [&](int rc) {
+    bfvm_destroy(c);
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(BFVM_ERR_CUDA);
+  c->stream = c->own_stream;
+  const size_t S = c->S;
+  c->field_bytes = static_cast<size_t>(c->nxp) * c->ny * c->nz * S * c->eb;
+  const size_t tot = S * (c->nx + c->ny + c->nz);
+  int rc = BFVM_OK;
+  if (rc == BFVM_OK) rc = dalloc(c, &c->f, c->field_bytes);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_denom), tot * 8);
+  if (rc == BFVM_OK) rc = dalloc(c, &c->d_rcp, tot * c->eb);
+  if (rc == BFVM_OK) rc = dalloc(c, &c->d_cup, tot * c->eb);
+  if (rc == BFVM_OK) rc = dalloc(c, &c->d_c1, S * c->eb);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_active), S * sizeof(int));
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_faces), face_elems(c) * 8);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_status), sizeof(int));
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_nvalid), sizeof(int));
+  if (rc == BFVM_OK)
+    rc = dalloc(c, reinterpret_cast<void**>(&c->d_line_off), sizeof(int) * (static_cast<size_t>(c->ny) * c->nz + 1));
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_sums), sizeof(double) * (S * 1024 + S));
+  if (rc != BFVM_OK) return fail(rc);
+  if (cudaMemset(c->f, 0, c->field_bytes) != cudaSuccess || cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess)
+    return fail(BFVM_ERR_CUDA);
+  if ((rc = upload_coefficients(c, cfg->diffusion_coefficients, cfg->decay_rates)) != BFVM_OK) return fail(rc);
+  // Reference defaults: activation on, value 1.0 on every face voxel.
+  c->active.assign(S, 1);
+  std::vector<int> act(S, 1);
+  std::vector<double> ones(face_elems(c), 1.0);
+  if (cudaMemcpy(c->d_active, act.data(), S * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_faces, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(BFVM_ERR_CUDA);
+  if (encode_field_maps(&c->maps, c->f, c->eb, c->nx, c->ny, c->nz, c->S, c->nxp, c->cfg) != 0)
+    return fail(BFVM_ERR_CUDA);
+  *out = c;
+  return BFVM_OK;
+}
+
+int bfvm_destroy(bfvm_ctx* c) {
+  if (!c) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_agents(c);
+  dfree(c->f);
+  dfree(c->d_denom);
+  dfree(c->d_rcp);
+  dfree(c->d_cup);
+  dfree(c->d_c1);
+  dfree(c->d_active);
+  dfree(c->d_faces);
+  dfree(c->d_status);
+  dfree(c->d_nvalid);
+  dfree(c->d_line_off);
+  dfree(c->d_sums);
+  dfree(c->d_staging);
+  for (cudaEvent_t e : c->events) cudaEventDestroy(e);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return BFVM_OK;
+}
+
+int bfvm_set_dirichlet_activation(bfvm_ctx* c, const unsigned char* active) {
+  if (!c || !active) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  std::vector<int> act(c->S);
+  for (int s = 0; s < c->S; ++s) act[s] = active[s] ? 1 : 0;
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  BFVM_CUDA(cudaMemcpy(c->d_active, act.data(), c->S * sizeof(int), cudaMemcpyHostToDevice));
+  c->active.assign(active, active + c->S);
+  return BFVM_OK;
+}
+
+int bfvm_set_dirichlet_face(bfvm_ctx* c, int face, const double* values) {
+  if (!c || !values || face < 0 || face > 5) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  const int S = c->S, nx = c->nx, ny = c->ny, nz = c->nz;
+  const int side = face & 1;
+  // Transpose the reference-oriented plane into the device face layout.
+  std::vector<double> plane;
+  size_t dst_off = 0;
+  if (face < 2) {  // [ny][nz][S] -> xface[side][s][k][j]
+    plane.resize(static_cast<size_t>(S) * nz * ny);
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k)
+        for (int s = 0; s < S; ++s)
+          plane[(static_cast<size_t>(s) * nz + k) * ny + j] = values[(static_cast<size_t>(j) * nz + k) * S + s];
+    dst_off = static_cast<size_t>(side) * S * nz * ny;
+  } else if (face < 4) {  // [nx][nz][S] -> yface[side][s][k][i]
+    plane.resize(static_cast<size_t>(S) * nz * nx);
+    for (int i = 0; i < nx; ++i)
+      for (int k = 0; k < nz; ++k)
+        for (int s = 0; s < S; ++s)
+          plane[(static_cast<size_t>(s) * nz + k) * nx + i] = values[(static_cast<size_t>(i) * nz + k) * S + s];
+    dst_off = 2ull * S * nz * ny + static_cast<size_t>(side) * S * nz * nx;
+  } else {  // [nx][ny][S] -> zface[side][s][j][i]
+    plane.resize(static_cast<size_t>(S) * ny * nx);
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j)
+        for (int s = 0; s < S; ++s)
+          plane[(static_cast<size_t>(s) * ny + j) * nx + i] = values[(static_cast<size_t>(i) * ny + j) * S + s];
+    dst_off = 2ull * S * nz * ny + 2ull * S * nz * nx + static_cast<size_t>(side) * S * ny * nx;
+  }
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  BFVM_CUDA(cudaMemcpy(c->d_faces + dst_off, plane.data(), plane.size() * 8, cudaMemcpyHostToDevice));
+  return BFVM_OK;
+}
+
+int bfvm_set_dirichlet_uniform(bfvm_ctx* c, const double* values) {
+  if (!c || !values) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  const int S = c->S, nx = c->nx, ny = c->ny, nz = c->nz;
+  std::vector<double> all(face_elems(c));
+  size_t o = 0;
+  for (int side = 0; side < 2; ++side)
+    for (int s = 0; s < S; ++s)
+      for (size_t q = 0; q < static_cast<size_t>(nz) * ny; ++q) all[o++] = values[s];
+  for (int side = 0; side < 2; ++side)
+    for (int s = 0; s < S; ++s)
+      for (size_t q = 0; q < static_cast<size_t>(nz) * nx; ++q) all[o++] = values[s];
+  for (int side = 0; side < 2; ++side)
+    for (int s = 0; s < S; ++s)
+      for (size_t q = 0; q < static_cast<size_t>(ny) * nx; ++q) all[o++] = values[s];
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  BFVM_CUDA(cudaMemcpy(c->d_faces, all.data(), all.size() * 8, cudaMemcpyHostToDevice));
+  return BFVM_OK;
+}
+
+static int ensure_staging(bfvm_ctx* c) {
+  if (c->d_staging) return BFVM_OK;
+  return dalloc(c, reinterpret_cast<void**>(&c->d_staging),
+                sizeof(double) * static_cast<size_t>(c->nx) * c->ny * c->nz * c->S);
+}
+
+static int pack_from_device_aos(bfvm_ctx* c, const double* d_aos) {
+  if (c->prec == BFVM_FP64)
+    BFVM_CUDA(launch_pack<double>(d_aos, static_cast<double*>(c->f), c->nx, c->ny, c->nz, c->S, c->nxp, c->stream));
+  else
+    BFVM_CUDA(launch_pack<float>(d_aos, static_cast<float*>(c->f), c->nx, c->ny, c->nz, c->S, c->nxp, c->stream));
+  note_launches(1);
+  return BFVM_OK;
+}
+
+static int unpack_to_device_aos(bfvm_ctx* c, double* d_aos) {
+  if (c->prec == BFVM_FP64)
+    BFVM_CUDA(launch_unpack<double>(static_cast<const double*>(c->f), d_aos, c->nx, c->ny, c->nz, c->S, c->nxp,
+                                    c->stream));
+  else
+    BFVM_CUDA(
+        launch_unpack<float>(static_cast<const float*>(c->f), d_aos, c->nx, c->ny, c->nz, c->S, c->nxp, c->stream));
+  note_launches(1);
+  return BFVM_OK;
+}
+
+int bfvm_upload_field(bfvm_ctx* c, const double* field) {
+  if (!c || !field) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  int rc = ensure_staging(c);
+  if (rc != BFVM_OK) return rc;
+  const size_t bytes = sizeof(double) * static_cast<size_t>(c->nx) * c->ny * c->nz * c->S;
+  BFVM_CUDA(cudaMemcpyAsync(c->d_staging, field, bytes, cudaMemcpyHostToDevice, c->stream));
+  return pack_from_device_aos(c, c->d_staging);
+}
+
+int bfvm_download_field(bfvm_ctx* c, double* field) {
+  if (!c || !field) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  int rc = ensure_staging(c);
+  if (rc != BFVM_OK) return rc;
+  if ((rc = unpack_to_device_aos(c, c->d_staging)) != BFVM_OK) return rc;
+  const size_t bytes = sizeof(double) * static_cast<size_t>(c->nx) * c->ny * c->nz * c->S;
+  BFVM_CUDA(cudaMemcpyAsync(field, c->d_staging, bytes, cudaMemcpyDeviceToHost, c->stream));
+  return bfvm_synchronize(c);
+}
+
+int bfvm_upload_field_device(bfvm_ctx* c, const double* d_field) {
+  if (!c || !d_field) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  return pack_from_device_aos(c, d_field);
+}
+
+int bfvm_download_field_device(bfvm_ctx* c, double* d_field) {
+  if (!c || !d_field) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  return unpack_to_device_aos(c, d_field);
+}
+
+static int set_agents_common(bfvm_ctx* c, int n, const int* voxel, const unsigned char* active) {
+  int rc = ensure_agent_capacity(c, n);
+  if (rc != BFVM_OK) return rc;
+  if (n > 0) {
+    BFVM_CUDA(cudaMemcpyAsync(c->d_voxel, voxel, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+    if (active) {
+      BFVM_CUDA(cudaMemcpyAsync(c->d_agent_active, active, n, cudaMemcpyHostToDevice, c->stream));
+    } else {
+      BFVM_CUDA(cudaMemsetAsync(c->d_agent_active, 1, n, c->stream));
+    }
+  }
+  return BFVM_OK;
+}
+
+int bfvm_set_agents(bfvm_ctx* c, int n, const int* voxel, const unsigned char* active, const double* c1,
+                    const double* c2, const double* e2) {
+  if (!c || n < 0 || (n > 0 && (!voxel || !c1 || !c2 || !e2))) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  int rc = set_agents_common(c, n, voxel, active);
+  if (rc != BFVM_OK) return rc;
+  const size_t row = sizeof(double) * c->S * static_cast<size_t>(n);
+  if (n > 0) {
+    BFVM_CUDA(cudaMemcpyAsync(c->d_c, c1, row, cudaMemcpyHostToDevice, c->stream));
+    BFVM_CUDA(cudaMemcpyAsync(c->d_c + static_cast<size_t>(c->S) * n, c2, row, cudaMemcpyHostToDevice, c->stream));
+    BFVM_CUDA(cudaMemcpyAsync(c->d_c + 2ull * c->S * n, e2, row, cudaMemcpyHostToDevice, c->stream));
+  }
+  return build_agents(c, n);
+}
+
+int bfvm_set_agents_from_rates(bfvm_ctx* c, int n, const int* voxel, const unsigned char* active, const double* volume,
+                               const double* sec, const double* upt, const double* sat, const double* exp_) {
+  if (!c || n < 0 || (n > 0 && (!voxel || !volume || !sec || !upt || !sat || !exp_))) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  int rc = set_agents_common(c, n, voxel, active);
+  if (rc != BFVM_OK) return rc;
+  if (n > 0) {
+    const size_t row = sizeof(double) * c->S * static_cast<size_t>(n);
+    double* vol = c->d_rates;
+    double* r = c->d_rates + n;
+    const size_t SN = static_cast<size_t>(c->S) * n;
+    BFVM_CUDA(cudaMemcpyAsync(vol, volume, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    BFVM_CUDA(cudaMemcpyAsync(r, sec, row, cudaMemcpyHostToDevice, c->stream));
+    BFVM_CUDA(cudaMemcpyAsync(r + SN, upt, row, cudaMemcpyHostToDevice, c->stream));
+    BFVM_CUDA(cudaMemcpyAsync(r + 2 * SN, sat, row, cudaMemcpyHostToDevice, c->stream));
+    BFVM_CUDA(cudaMemcpyAsync(r + 3 * SN, exp_, row, cudaMemcpyHostToDevice, c->stream));
+    const double vvox = c->dx * c->dx * c->dx;
+    BFVM_CUDA(agents_compute_constants(n, c->S, c->dt, vvox, vol, r, r + SN, r + 2 * SN, r + 3 * SN, c->d_c,
+                                       c->d_c + SN, c->d_c + 2 * SN, c->stream));
+    note_launches(1);
+  }
+  return build_agents(c, n);
+}
+
+int bfvm_agent_constants_device(int n, int S, double dt, double voxel_volume, const double* volume,
+                                const double* sec, const double* upt, const double* sat, const double* exp_,
+                                double* c1, double* c2, double* e2, void* stream) {
+  if (n < 0 || S < 1 || S > kMaxSubstrates || !(dt > 0) || !(voxel_volume > 0)) return BFVM_ERR_ARG;
+  if (n > 0 && (!volume || !sec || !upt || !sat || !exp_ || !c1 || !c2 || !e2)) return BFVM_ERR_ARG;
+  BFVM_CUDA(agents_compute_constants(n, S, dt, voxel_volume, volume, sec, upt, sat, exp_, c1, c2, e2,
+                                     static_cast<cudaStream_t>(stream)));
+  if (n > 0) note_launches(1);
+  return BFVM_OK;
+}
+
+int bfvm_step(bfvm_ctx* c, int nsteps, int flags) {
+  if (!c || nsteps < 0) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  const bool src = (flags & BFVM_STEP_SOURCES) != 0;
+  return c->prec == BFVM_FP64 ? run_steps<double>(c, nsteps, src) : run_steps<float>(c, nsteps, src);
+}
+
+int bfvm_apply_sources(bfvm_ctx* c) {
+  if (!c) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  if (c->n_agents == 0) return BFVM_OK;
+  const size_t SN = static_cast<size_t>(c->S) * c->n_agents;
+  if (c->prec == BFVM_FP64)
+    BFVM_CUDA(agents_apply_sources<double>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
+                                           c->d_ac + SN, c->d_ac + 2 * SN, static_cast<double*>(c->f), c->stream));
+  else
+    BFVM_CUDA(agents_apply_sources<float>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
+                                          c->d_ac + SN, c->d_ac + 2 * SN, static_cast<float*>(c->f), c->stream));
+  note_launches(1);
+  return BFVM_OK;
+}
+
+int bfvm_sample_agents(bfvm_ctx* c, double* out) {
+  if (!c || (!out && c->n_agents > 0)) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  if (c->n_agents == 0) return BFVM_OK;
+  if (c->prec == BFVM_FP64)
+    BFVM_CUDA(agents_sample<double>(c->n_agents, c->d_dev_voxel, c->S, c->nx, c->ny, c->nz, c->nxp,
+                                    static_cast<const double*>(c->f), c->d_sample, c->stream));
+  else
+    BFVM_CUDA(agents_sample<float>(c->n_agents, c->d_dev_voxel, c->S, c->nx, c->ny, c->nz, c->nxp,
+                                   static_cast<const float*>(c->f), c->d_sample, c->stream));
+  note_launches(1);
+  BFVM_CUDA(cudaMemcpyAsync(out, c->d_sample, sizeof(double) * c->S * static_cast<size_t>(c->n_agents),
+                            cudaMemcpyDeviceToHost, c->stream));
+  return bfvm_synchronize(c);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Deterministic per-substrate sums: fixed block partials, then one block adds
+// the partials in order.
+template <typename T>
+__global__ void field_partial_sums(const T* __restrict__ f, int nx, int rows_per_s, int nxp, double* partial) {
+  __shared__ double red[256];
+  const int s = blockIdx.y;
+  const long long n = static_cast<long long>(rows_per_s) * nx;
+  double acc = 0.0;
+  for (long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; q < n;
+       q += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long r = q / nx, i = q % nx;
+    acc += static_cast<double>(f[(static_cast<size_t>(s) * rows_per_s + r) * nxp + i]);
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[static_cast<size_t>(s) * gridDim.x + blockIdx.x] = red[0];
+}
+
+__global__ void field_final_sums(const double* partial, int nparts, int S, double* out) {
+  const int s = threadIdx.x;
+  if (s >= S) return;
+  double acc = 0.0;
+  for (int b = 0; b < nparts; ++b) acc += partial[static_cast<size_t>(s) * nparts + b];
+  out[s] = acc;
+}
+
+}  // namespace
+
+extern "C" int bfvm_field_sums(bfvm_ctx* c, double* out) {
+  if (!c || !out) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  const int nparts = 1024;
+  dim3 grid(nparts, c->S);
+  double* partial = c->d_sums;
+  double* res = c->d_sums + static_cast<size_t>(c->S) * nparts;
+  if (c->prec == BFVM_FP64)
+    field_partial_sums<double><<<grid, 256, 0, c->stream>>>(static_cast<const double*>(c->f), c->nx, c->ny * c->nz,
+                                                            c->nxp, partial);
+  else
+    field_partial_sums<float><<<grid, 256, 0, c->stream>>>(static_cast<const float*>(c->f), c->nx, c->ny * c->nz,
+                                                           c->nxp, partial);
+  BFVM_CUDA(cudaGetLastError());
+  field_final_sums<<<1, 64, 0, c->stream>>>(partial, nparts, c->S, res);
+  BFVM_CUDA(cudaGetLastError());
+  note_launches(2);
+  BFVM_CUDA(cudaMemcpyAsync(out, res, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->stream));
+  return bfvm_synchronize(c);
+}
+
+extern "C" int bfvm_synchronize(bfvm_ctx* c) {
+  if (!c) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  int st = 0;
+  BFVM_CUDA(cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st != 0) {
+    cudaMemset(c->d_status, 0, sizeof(int));
+    return BFVM_ERR_TIMEOUT;
+  }
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_timing_enable(bfvm_ctx* c, int on) {
+  if (!c) return BFVM_ERR_ARG;
+  c->timing = on != 0;
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_timing_read(bfvm_ctx* c, double* ms_xyz, int* steps) {
+  if (!c || !ms_xyz) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  double acc[3] = {0, 0, 0};
+  for (int s = 0; s < c->timed_steps; ++s) {
+    const cudaEvent_t* ev = &c->events[4 * static_cast<size_t>(s)];
+    for (int k = 0; k < 3; ++k) {
+      float ms = 0.f;
+      BFVM_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      acc[k] += ms;
+    }
+  }
+  for (int k = 0; k < 3; ++k) ms_xyz[k] = acc[k];
+  if (steps) *steps = c->timed_steps;
+  c->timed_steps = 0;
+  return BFVM_OK;
+}
+
+extern "C" void* bfvm_stream(bfvm_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+extern "C" int bfvm_set_stream(bfvm_ctx* c, void* stream) {
+  if (!c) return BFVM_ERR_ARG;
+  c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_device_field(bfvm_ctx* c, void** ptr, int* pitch, int* elem_bytes) {
+  if (!c) return BFVM_ERR_ARG;
+  if (ptr) *ptr = c->f;
+  if (pitch) *pitch = c->nxp;
+  if (elem_bytes) *elem_bytes = c->eb;
+  return BFVM_OK;
+}
+
+extern "C" size_t bfvm_device_bytes(bfvm_ctx* c) { return c ? c->device_bytes : 0; }
+
+extern "C" int bfvm_get_launch(bfvm_ctx* c, int* x_lines, int* yz_tile, int* yz_chunk) {
+  if (!c) return BFVM_ERR_ARG;
+  if (x_lines) *x_lines = c->cfg.x_lines;
+  if (yz_tile) *yz_tile = c->cfg.yz_tile;
+  if (yz_chunk) *yz_chunk = c->cfg.yz_chunk;
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_set_launch(bfvm_ctx* c, int x_lines, int yz_tile, int yz_chunk) {
+  if (!c) return BFVM_ERR_ARG;
+  SweepConfig cfg;
+  cfg.x_lines = x_lines;
+  cfg.yz_tile = yz_tile;
+  cfg.yz_chunk = yz_chunk;
+  // x_lines: multiple of 8 (1024-byte swizzle atoms); yz_tile: a whole number
+  // of 16-byte units per row (TMA x alignment); both at most 256 (box limit).
+  if (x_lines < 8 || x_lines > 256 || x_lines % 8 != 0) return BFVM_ERR_ARG;
+  if (yz_tile < 1 || yz_tile > 256 || (yz_tile * c->eb) % 16 != 0) return BFVM_ERR_ARG;
+  if (yz_chunk < 1 || yz_chunk > 256) return BFVM_ERR_ARG;
+  if (!config_fits(c->eb, c->nx, c->ny, c->nz, cfg)) return BFVM_ERR_SHAPE;
+  DeviceGuard g(c->device);
+  FieldMaps maps;
+  if (encode_field_maps(&maps, c->f, c->eb, c->nx, c->ny, c->nz, c->S, c->nxp, cfg) != 0) return BFVM_ERR_CUDA;
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  c->maps = maps;
+  c->cfg = cfg;
+  return BFVM_OK;
+}

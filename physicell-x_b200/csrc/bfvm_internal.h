@@ -1,0 +1,96 @@
+// bfvm_internal.h -- device-side data of one microenvironment solve and the
+// kernel launchers shared by the C-ABI translation units.
+//
+// Device layout (chosen for the sweeps, not inherited from the reference):
+//   field   T f[S][nz][ny][nxp]   x fastest, rows padded to nxp elements
+//                                 (128-byte rows), one plane per substrate.
+// The reference layout is [x][y][z][S] with z fastest
+// (BioFVM/BioFVM_mesh.cpp:1149-1158); pack/unpack kernels convert at the
+// host boundary.  With x fastest, the y and z sweeps read whole 128-byte row
+// segments across consecutive x, and the x sweep is the one that stages its
+// lines through shared memory (swizzled TMA tiles).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+namespace bfvm {
+
+constexpr int kMaxSubstrates = 64;
+
+// Thomas coefficients of one axis for all substrates, index [s][i].
+template <typename T>
+struct AxisCoefs {
+  const double* denom;  // modified diagonal (FP64 always)
+  const T* rcp;         // RN(1/denom) in T
+  const T* cup;         // modified upper diagonal in T
+};
+
+template <typename T>
+struct SweepParams {
+  T* f;                  // field base
+  int nx, ny, nz, S, nxp;
+  const T* c1;           // [S] dt*D/dx^2
+  const int* active;     // [S] Dirichlet activation
+  // Face planes (resolved Dirichlet value of each face voxel), FP64:
+  //   xface[side][s][k][j], yface[side][s][k][i], zface[side][s][j][i]
+  const double* xface;
+  const double* yface;
+  const double* zface;
+  AxisCoefs<T> ax, ay, az;
+  // Agents (optional): sorted by device voxel id, CSR over x-lines
+  // (line = k*ny + j).  a_i: x index; ac1/ac2/ae2: [S][n_sorted] FP64.
+  const int* line_off;   // [ny*nz + 1] or nullptr when no sources this step
+  const int* a_i;
+  const double* ac1;
+  const double* ac2;
+  const double* ae2;
+  int n_sorted;
+  int* status;           // device status word
+};
+
+// Kernel launch configuration chosen by the host (autotuned per shape).
+struct SweepConfig {
+  int x_lines = 32;   // lines per CTA in the x sweep (multiple of 8, <= 256)
+  int yz_tile = 32;   // consecutive x per CTA in the y/z sweeps (multiple of 16 fp64 / 32 fp32... see launcher)
+  int yz_chunk = 32;  // rows per TMA box along the line in the y/z sweeps (<= 256)
+};
+
+// The three tensor maps the sweeps use, built once per context.
+struct FieldMaps {
+  CUtensorMap x;   // box {16 or 32 (128 B), x_lines, 1, 1}, 128B swizzle
+  CUtensorMap y;   // box {yz_tile, yz_chunk, 1, 1}
+  CUtensorMap z;   // box {yz_tile, 1, yz_chunk, 1}
+};
+
+// Host-side count of this library's kernel launches (bfvm_kernel_launches).
+void note_launches(int n);
+
+int encode_field_maps(FieldMaps* maps, void* f, int elem_bytes, int nx, int ny, int nz, int S, int nxp,
+                      const SweepConfig& cfg);
+
+template <typename T>
+cudaError_t launch_sweep_x(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st);
+template <typename T>
+cudaError_t launch_sweep_y(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st);
+template <typename T>
+cudaError_t launch_sweep_z(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st);
+
+// Shared-memory bytes one CTA of each sweep needs (0 if the shape is not
+// supported by that configuration).
+size_t sweep_x_smem(int elem_bytes, int nx, const SweepConfig& cfg);
+size_t sweep_yz_smem(int elem_bytes, int n_line, const SweepConfig& cfg);
+
+// Layout conversion between the reference AoS [x][y][z][S] (double) and the
+// device SoA [S][z][y][nxp] (T).
+template <typename T>
+cudaError_t launch_pack(const double* aos, T* f, int nx, int ny, int nz, int S, int nxp, cudaStream_t st);
+template <typename T>
+cudaError_t launch_unpack(const T* f, double* aos, int nx, int ny, int nz, int S, int nxp, cudaStream_t st);
+
+}  // namespace bfvm

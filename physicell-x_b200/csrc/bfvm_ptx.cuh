@@ -1,0 +1,123 @@
+// bfvm_ptx.cuh -- small inline-PTX helpers for sm_100a: mbarriers with
+// bounded waits, plain (non-multicast) TMA tensor loads/stores, and the exact
+// FP64 quotient used by the Thomas forward sweep.
+#pragma once
+
+#include <cstdint>
+#include <cuda.h>
+
+namespace bfvm {
+
+// Device status codes written to the context's status word (host-visible).
+enum : int {
+  kDevOk = 0,
+  kDevTimeout = 1,  // an mbarrier wait gave up (TMA copy never completed)
+};
+
+// Upper bound on any single wait in these kernels, in globaltimer ns.  A
+// healthy TMA copy completes in microseconds; the bound exists so that a
+// broken copy can never hang the GPU.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Wait for phase `parity` of the barrier; false if the wait limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (global_ns() - t0 > kWaitLimitNs) return false;
+  }
+  return true;
+}
+
+// 4-D tiled TMA load (no multicast) into this CTA's shared memory,
+// completing `bytes` on the barrier.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1,
+                                            int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+      : "memory");
+}
+
+// 4-D tiled TMA store from shared memory (elements outside the tensor are
+// not written).
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, uint32_t src, int c0, int c1, int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4, %5}], [%1];" ::"l"(
+          reinterpret_cast<uint64_t>(map)),
+      "r"(src), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_store_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// Wait until every committed bulk store has finished READING shared memory.
+__device__ __forceinline__ void tma_store_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// Make this thread's generic-proxy shared-memory writes visible to the TMA
+// (async proxy) before a bulk store reads them.
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+// Correctly rounded t / d given r = RN(1/d) (computed once on the host in
+// IEEE double).  Markstein's correction step: q0 = RN(t*r) is within one ulp
+// of t/d; the remainder e = t - q0*d is exact under an FMA, and
+// RN(q0 + e*r) is the correctly rounded quotient (P. Markstein, "Computation
+// of elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990; Theorem 4.x in Muller et al., Handbook of Floating-Point
+// Arithmetic).  The theorem needs the remainder not to underflow; for a
+// nonzero |t| < 2^-960 the plain IEEE division is used instead (never on
+// realistic densities, but it keeps the result exact for every input).  A
+// zero numerator returns q0 = t*r, which carries the sign of t as IEEE
+// division does.  The sweep denominators are all >= 1, so t*r cannot
+// overflow.
+__device__ __forceinline__ double div_exact(double t, double d, double r) {
+  const double q0 = t * r;
+  const double e = __fma_rn(-q0, d, t);
+  double q = __fma_rn(e, r, q0);
+  q = (t == 0.0) ? q0 : q;
+  if (fabs(t) < 0x1p-960 && t != 0.0) q = t / d;
+  return q;
+}
+
+}  // namespace bfvm

@@ -1,0 +1,69 @@
+"""CPU tests of the C ABI library: it loads, exports every function that
+include/biofvm_b200.h declares, and reports a missing device instead of
+failing silently.  No compute call is made here."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from bfvm import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(bfvm_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_function():
+    L = _lib.lib()
+    names = _declared("biofvm_b200.h")
+    assert "bfvm_create" in names and "bfvm_step" in names
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_python_signatures_cover_the_header():
+    names = _declared("biofvm_b200.h")
+    assert sorted(n for n in names if n in _lib._SIGS) == names
+
+
+def test_status_strings():
+    assert _lib.status_string(0) == "ok"
+    assert _lib.status_string(_lib.BFVM_ERR_TIMEOUT) == "device wait timed out"
+
+
+def _cuda_available():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_cuda_available(), reason="checks the no-device path")
+def test_create_without_device_reports_nodevice():
+    L = _lib.lib()
+    D = (C.c_double * 1)(1e5)
+    lam = (C.c_double * 1)(0.1)
+    cfg = _lib.bfvm_config(4, 4, 4, 1, 20.0, 0.01, D, lam, _lib.BFVM_FP64, 0)
+    h = C.c_void_p()
+    assert L.bfvm_create(C.byref(cfg), C.byref(h)) == _lib.BFVM_ERR_NODEVICE
+    assert not h.value
+
+
+def test_create_rejects_bad_arguments():
+    L = _lib.lib()
+    D = (C.c_double * 1)(1e5)
+    lam = (C.c_double * 1)(0.1)
+    h = C.c_void_p()
+    for bad in (dict(nx=0), dict(dx=-1.0), dict(dt=0.0), dict(precision=7)):
+        kw = dict(nx=4, ny=4, nz=4, S=1, dx=20.0, dt=0.01, precision=_lib.BFVM_FP64)
+        kw.update(bad)
+        cfg = _lib.bfvm_config(kw["nx"], kw["ny"], kw["nz"], kw["S"], kw["dx"], kw["dt"], D, lam, kw["precision"], 0)
+        assert L.bfvm_create(C.byref(cfg), C.byref(h)) == _lib.BFVM_ERR_ARG
+    assert L.bfvm_create(None, C.byref(h)) == _lib.BFVM_ERR_ARG

@@ -1,0 +1,70 @@
+"""The C++ drop-in inside the reference's own Microenvironment.
+
+oracle/_ref/libbiofvm_dropin.so is the reference BioFVM built from its
+sources plus physicell-x_b200/host/biofvm_b200_dropin.cpp, which defines the
+reference's declared friend entry point
+diffusion_decay_solver__constant_coefficients_LOD_3D(M, dt, world, cart).
+The tests install it in the solver slot (diffusion_decay_solver_mpi) and call
+Microenvironment::simulate_diffusion_decay(dt, world, cart) exactly as
+PhysiCell-X does, then compare with the reference's _BLOCKING solver on an
+identical Microenvironment.
+"""
+import numpy as np
+import pytest
+
+from bfvm import workloads as W
+from pyoracle import Reference
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not Reference.available(dropin=True), reason="drop-in library not built")]
+
+
+def _pair(wl):
+    cpu = Reference(wl, threads=4, dropin=True)
+    gpu = Reference(wl, threads=4, dropin=True)
+    return cpu, gpu
+
+
+@pytest.mark.parametrize("seed", [401, 402, 403])
+def test_dropin_solver_slot_bitwise(seed):
+    """Host-side sources (the reference's own agent loop), GPU diffusion through
+    the solver pointer, field mirrored to the host every step."""
+    wl = W.small_random(seed, steps=4, stack=True)
+    cpu, gpu = _pair(wl)
+    a = cpu.run(wl.steps, solver=0, sources_threads=1)
+    b = gpu.run(wl.steps, solver=2, sources_threads=1)
+    assert np.array_equal(a, b)
+
+
+def test_dropin_fused_sources_bitwise():
+    """Agents gathered from the reference's Basic_Agent list and applied on the
+    GPU fused ahead of the sweep; the host agent loop is not called."""
+    wl = W.small_random(404, nx=30, ny=22, nz=26, S=3, n_agents=500, steps=5, stack=True)
+    cpu, gpu = _pair(wl)
+    a = cpu.run(wl.steps, solver=0, sources_threads=1)
+    assert gpu.L.ref_env_dropin_fuse_sources(gpu.h, 1, wl.dt) == 0
+    for _ in range(wl.steps):
+        gpu.diffusion(solver=2)
+    assert np.array_equal(a, gpu.field())
+
+
+def test_dropin_config1_hundred_steps():
+    wl = W.config1(steps=100)
+    cpu, gpu = _pair(wl)
+    a = cpu.run(wl.steps, solver=0, sources_threads=1)
+    b = gpu.run(wl.steps, solver=2, sources_threads=1)
+    assert np.array_equal(a, b)
+
+
+def test_dropin_follows_dirichlet_changes_between_steps():
+    wl = W.small_random(405, steps=2)
+    cpu, gpu = _pair(wl)
+    for ref in (cpu, gpu):
+        ref.run(2, solver=0 if ref is cpu else 2)
+        for d in range(wl.S):
+            ref.L.ref_env_set_dirichlet_activation(ref.h, d, 1)
+        dv = wl.dirichlet_values * 0.5
+        ref.L.ref_env_set_dirichlet_face_values(ref.h, dv)
+    a = cpu.run(3, solver=0)
+    b = gpu.run(3, solver=2)
+    assert np.array_equal(a, b)

@@ -1,0 +1,242 @@
+"""GPU parity tests: the sm_100a path through the C ABI against the oracle.
+
+FP64 bar: bit-identical to the reference (its golden fixtures, and the C
+restatement on fresh seeded inputs).  FP32 bar: normwise relative L-inf
+error per substrate, max|g - r| / max|r| <= 1e-5, against the FP64 oracle.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from bfvm import Microenvironment, kernel_launches
+from bfvm import workloads as W
+from pyoracle import Port
+
+pytestmark = pytest.mark.gpu
+
+FP32_TOL = 1e-5
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def _load(golden_dir, name):
+    return np.load(os.path.join(golden_dir, name + ".npz"), allow_pickle=False)
+
+
+def _fixture_solve(g, precision="fp64"):
+    nx, ny, nz, S = (int(v) for v in g["shape"])
+    wl = W.Workload(name="fx", nx=nx, ny=ny, nz=nz, S=S, dx=float(g["dx"]), dt=float(g["dt"]), steps=int(g["steps"]),
+                    D=g["D"], decay=g["decay"], dirichlet_active=g["active"], face_values=g["face_values"],
+                    origin=(0, 0, 0), seed=0, agent_pos=np.zeros((0, 3)), agent_volume=np.zeros(0),
+                    secretion=np.zeros((0, S)), uptake=np.zeros((0, S)), saturation=np.zeros((0, S)),
+                    net_export=np.zeros((0, S)))
+    me = Microenvironment.from_workload(wl, precision=precision, upload=False)
+    me.upload_field(g["field0"])
+    if g["voxel"].size:
+        me.set_agents(g["voxel"], g["c1"], g["c2"], g["e2"])
+    return me, int(g["steps"])
+
+
+def _normwise(got, ref, S):
+    g = got.reshape(-1, S)
+    r = ref.reshape(-1, S)
+    return np.max(np.abs(g - r), axis=0) / np.maximum(np.max(np.abs(r), axis=0), 1e-300)
+
+
+def test_small_goldens_bitwise(golden_dir):
+    names = [n for n in json.load(open(os.path.join(golden_dir, "MANIFEST.json")))["cases"] if n.startswith("small_")]
+    for name in names:
+        g = _load(golden_dir, name)
+        me, steps = _fixture_solve(g)
+        me.simulate_diffusion_decay(steps, sources=True)
+        out = me.download_field()
+        me.close()
+        bad = np.flatnonzero(out != g["final"])
+        assert bad.size == 0, f"{name}: {bad.size} values differ, first {bad[:5]}"
+
+
+def test_config1_full_run_matches_reference_hash(golden_dir):
+    """config1 (50^3 x 2 substrates, 2000 agents), all 1000 LOD steps with fused
+    sources: the final field is bit-identical to the reference's."""
+    g = _load(golden_dir, "config1_1000")
+    wl = W.config1(steps=1000)
+    assert _sha(wl.field0) == str(g["field0_sha"])
+    me = Microenvironment.from_workload(wl)
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    out = me.download_field()
+    assert np.array_equal(out[g["sample_idx"]], g["sample_val"])
+    assert _sha(out) == str(g["final_sha"])
+
+
+def test_config2_and_config4_env_match_reference_hash(golden_dir):
+    for name, wl in (("config2_10", W.config2(steps=10)), ("config4_env_50", W.config4_env(index=7, steps=50))):
+        g = _load(golden_dir, name)
+        assert _sha(wl.field0) == str(g["field0_sha"])
+        me = Microenvironment.from_workload(wl)
+        me.simulate_diffusion_decay(wl.steps, sources=True)
+        out = me.download_field()
+        me.close()
+        assert np.array_equal(out[g["sample_idx"]], g["sample_val"]), name
+        assert _sha(out) == str(g["final_sha"]), name
+
+
+@pytest.mark.parametrize("seed", list(range(200, 212)))
+def test_random_cases_bitwise_against_port(seed):
+    wl = W.small_random(seed, steps=4, stack=(seed % 2 == 0), agent_mode="gauss" if seed % 3 == 0 else "uniform")
+    expect = Port.run(wl)
+    me = Microenvironment.from_workload(wl)
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    assert np.array_equal(me.download_field(), expect)
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1, 1), (1, 7, 3, 2), (256, 3, 5, 1), (3, 256, 4, 2), (5, 4, 256, 1),
+                                   (129, 65, 33, 3), (200, 200, 8, 4)])
+def test_edge_shapes_bitwise(shape):
+    nx, ny, nz, S = shape
+    wl = W.small_random(7, nx=nx, ny=ny, nz=nz, S=S, n_agents=min(500, nx * ny * nz), steps=2, stack=True)
+    expect = Port.run(wl)
+    me = Microenvironment.from_workload(wl)
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    assert np.array_equal(me.download_field(), expect)
+
+
+def test_constants_from_rates_equal_precomputed():
+    wl = W.small_random(31, n_agents=300, steps=3, stack=True)
+    c1, c2, e2 = Port.workload_constants(wl)
+    a = Microenvironment.from_workload(wl)  # constants computed on the device
+    b = Microenvironment.from_workload(wl, agents="none")
+    b.set_agents(wl.agent_voxel, c1, c2, e2)
+    for me in (a, b):
+        me.simulate_diffusion_decay(wl.steps, sources=True)
+    assert np.array_equal(a.download_field(), b.download_field())
+
+
+def test_standalone_sources_then_diffusion_equals_fused():
+    wl = W.small_random(32, n_agents=400, steps=3, stack=True)
+    expect = Port.run(wl)
+    me = Microenvironment.from_workload(wl)
+    for _ in range(wl.steps):
+        me.simulate_cell_sources_and_sinks()
+        me.simulate_diffusion_decay(1, sources=False)
+    assert np.array_equal(me.download_field(), expect)
+
+
+def test_sources_only_matches_port_and_sampling():
+    wl = W.small_random(33, n_agents=250, steps=1, stack=True)
+    c1, c2, e2 = Port.workload_constants(wl)
+    field = wl.field0.copy()
+    Port.sources(field, wl.S, wl.agent_voxel, c1, c2, e2)
+    me = Microenvironment.from_workload(wl)
+    me.simulate_cell_sources_and_sinks()
+    got = me.download_field()
+    assert np.array_equal(got, field)
+    samp = me.sample_agents()
+    expect = field.reshape(-1, wl.S)[wl.agent_voxel]
+    assert np.array_equal(samp, expect)
+
+
+def test_inactive_and_outside_agents_are_skipped():
+    wl = W.small_random(34, n_agents=100, steps=2)
+    c1, c2, e2 = Port.workload_constants(wl)
+    vox = wl.agent_voxel.copy()
+    vox[::7] = -1
+    active = np.ones(wl.n_agents, np.uint8)
+    active[::5] = 0
+    field = wl.field0.copy()
+    dv = wl.dirichlet_values
+    for _ in range(wl.steps):
+        Port.sources(field, wl.S, vox, c1, c2, e2, active=active)
+        Port.lod_step(field, wl.shape, wl.D, wl.decay, wl.dt, wl.dx, wl.dirichlet_active, dv)
+    me = Microenvironment.from_workload(wl, agents="none")
+    me.set_agents(vox, c1, c2, e2, active=active)
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    assert np.array_equal(me.download_field(), field)
+
+
+def test_runs_are_deterministic_and_launch_shape_independent():
+    wl = W.small_random(35, nx=70, ny=45, nz=90, S=2, n_agents=3000, steps=3, agent_mode="gauss")
+    outs = []
+    for launch in (None, (8, 16, 7), (64, 64, 64), (32, 32, 256)):
+        me = Microenvironment.from_workload(wl)
+        if launch:
+            me.set_launch(*launch)
+        me.simulate_diffusion_decay(wl.steps, sources=True)
+        outs.append(me.download_field())
+        me.close()
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+
+
+def test_upload_download_roundtrip_and_sums():
+    wl = W.small_random(36, nx=37, ny=41, nz=29, S=3, n_agents=0)
+    for prec in ("fp64", "fp32"):
+        me = Microenvironment.from_workload(wl, precision=prec)
+        back = me.download_field()
+        if prec == "fp64":
+            assert np.array_equal(back, wl.field0)
+        else:
+            assert np.array_equal(back, wl.field0.astype(np.float32).astype(np.float64))
+        sums = me.field_sums()
+        np.testing.assert_allclose(sums, back.reshape(-1, wl.S).sum(axis=0), rtol=1e-12)
+
+
+def test_device_pointer_upload_matches_host_upload():
+    import torch
+
+    wl = W.small_random(37, n_agents=50, steps=2)
+    a = Microenvironment.from_workload(wl)
+    b = Microenvironment.from_workload(wl, upload=False)
+    d = torch.from_numpy(wl.field0).cuda()
+    b.upload_field_device(d.data_ptr())
+    for me in (a, b):
+        me.simulate_diffusion_decay(wl.steps, sources=True)
+    out = torch.empty_like(d)
+    b.download_field_device(out.data_ptr())
+    b.synchronize()
+    assert np.array_equal(a.download_field(), out.cpu().numpy())
+
+
+def test_kat_uniform_field_at_config2_size():
+    """Size-independent property at the full config2 grid (200^3 x 4): a
+    uniform zero-flux field divides by (1 + dt*lambda/3)^3 per step."""
+    wl = W.config2(n_agents=0, steps=3)
+    me = Microenvironment(wl.nx, wl.ny, wl.nz, wl.dx, wl.dt, wl.D, wl.decay)
+    me.set_dirichlet_activation(np.zeros(wl.S, np.uint8))
+    me.upload_field(np.full(wl.n_values, 5.0))
+    me.simulate_diffusion_decay(wl.steps)
+    f = me.download_field().reshape(-1, wl.S)
+    for d in range(wl.S):
+        np.testing.assert_allclose(f[:, d], 5.0 / (1 + wl.dt * wl.decay[d] / 3) ** (3 * wl.steps), rtol=1e-12)
+
+
+@pytest.mark.parametrize("seed", [300, 301, 302])
+def test_fp32_within_tolerance_small(seed):
+    wl = W.small_random(seed, steps=20, n_agents=200, stack=True)
+    ref = Port.run(wl)
+    me = Microenvironment.from_workload(wl, precision="fp32")
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    err = _normwise(me.download_field(), ref, wl.S)
+    assert np.all(err <= FP32_TOL), err
+
+
+def test_fp32_config1_full_run_within_tolerance():
+    wl = W.config1(steps=1000)
+    ref = Port.run(wl)
+    me = Microenvironment.from_workload(wl, precision="fp32")
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    err = _normwise(me.download_field(), ref, wl.S)
+    assert np.all(err <= FP32_TOL), err
+
+
+def test_kernel_launch_counter_moves():
+    before = kernel_launches()
+    wl = W.small_random(38, steps=2)
+    me = Microenvironment.from_workload(wl)
+    me.simulate_diffusion_decay(2, sources=True)
+    me.synchronize()
+    assert kernel_launches() - before >= 6

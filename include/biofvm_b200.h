@@ -165,8 +165,14 @@ void* bfvm_stream(bfvm_ctx* ctx);
 int bfvm_set_stream(bfvm_ctx* ctx, void* stream);
 
 /* Device field pointer and row pitch (elements) of the device layout
- * f[S][nz][ny][pitch], x fastest -- for callers that keep data on the GPU. */
+ * f[S][nz][ny][pitch], x fastest -- for callers that keep data on the GPU.
+ * An FP32 solve stores rho - offset[s] (see bfvm_field_offsets). */
 int bfvm_device_field(bfvm_ctx* ctx, void** ptr, int* pitch, int* elem_bytes);
+
+/* Per-substrate offsets [S] of the stored field: 0 for FP64; for FP32 the
+ * mean Dirichlet face value of each activated substrate (else 0), chosen at
+ * the last field upload.  Uploads, downloads, sampling and sums apply them. */
+int bfvm_field_offsets(bfvm_ctx* ctx, double* offsets);
 
 /* Bytes of device memory the solve holds (field, coefficients, agents). */
 size_t bfvm_device_bytes(bfvm_ctx* ctx);

@@ -193,7 +193,8 @@ __global__ void agent_csr_kernel(int n, const unsigned* __restrict__ sk, const i
 template <typename T>
 __global__ void agent_sources_kernel(int n, const unsigned* __restrict__ sk, unsigned sentinel, int S, int nx, int ny,
                                      int nz, int nxp, const double* __restrict__ ac1, const double* __restrict__ ac2,
-                                     const double* __restrict__ ae2, T* __restrict__ f) {
+                                     const double* __restrict__ ae2, const double* __restrict__ off,
+                                     T* __restrict__ f) {
   const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (idx >= static_cast<long long>(n) * S) return;
   const int s = static_cast<int>(idx / n);
@@ -205,11 +206,13 @@ __global__ void agent_sources_kernel(int n, const unsigned* __restrict__ sk, uns
   const int jk = key / nx;
   T* rho = f + (static_cast<size_t>(s) * nz * ny + jk) * nxp + i;
   double r = static_cast<double>(*rho);
+  if (off) r += off[s];
   for (int q = p; q < n && sk[q] == key; ++q) {
     r += ac1[static_cast<size_t>(s) * n + q];
     r /= ac2[static_cast<size_t>(s) * n + q];
     r += ae2[static_cast<size_t>(s) * n + q];
   }
+  if (off) r -= off[s];
   *rho = static_cast<T>(r);
   (void)ny;
 }
@@ -218,7 +221,8 @@ __global__ void agent_sources_kernel(int n, const unsigned* __restrict__ sk, uns
 // (what Basic_Agent::nearest_density_vector exposes to the agent).
 template <typename T>
 __global__ void agent_sample_kernel(int n, const unsigned* __restrict__ dev_voxel, unsigned sentinel, int S, int nx,
-                                    int ny, int nz, int nxp, const T* __restrict__ f, double* __restrict__ out) {
+                                    int ny, int nz, int nxp, const T* __restrict__ f, const double* __restrict__ off,
+                                    double* __restrict__ out) {
   const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (idx >= static_cast<long long>(n) * S) return;
   const int a = static_cast<int>(idx / S), s = static_cast<int>(idx % S);
@@ -228,6 +232,7 @@ __global__ void agent_sample_kernel(int n, const unsigned* __restrict__ dev_voxe
     const int i = key % nx;
     const int jk = key / nx;
     v = static_cast<double>(f[(static_cast<size_t>(s) * nz * ny + jk) * nxp + i]);
+    if (off) v += off[s];
   }
   out[idx] = v;
   (void)ny;
@@ -293,33 +298,34 @@ cudaError_t agents_build(const AgentBuild& b, cudaStream_t st, int* launches) {
 
 template <typename T>
 cudaError_t agents_apply_sources(int n, const unsigned* sorted_keys, int S, int nx, int ny, int nz, int nxp,
-                                 const double* ac1, const double* ac2, const double* ae2, T* f, cudaStream_t st) {
+                                 const double* ac1, const double* ac2, const double* ae2, const double* off, T* f,
+                                 cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   const unsigned sentinel = static_cast<unsigned>(nx) * ny * nz;
   const long long total = static_cast<long long>(n) * S;
   agent_sources_kernel<T><<<static_cast<unsigned>((total + 255) / 256), 256, 0, st>>>(
-      n, sorted_keys, sentinel, S, nx, ny, nz, nxp, ac1, ac2, ae2, f);
+      n, sorted_keys, sentinel, S, nx, ny, nz, nxp, ac1, ac2, ae2, off, f);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t agents_sample(int n, const unsigned* dev_voxel, int S, int nx, int ny, int nz, int nxp, const T* f,
-                          double* out, cudaStream_t st) {
+                          const double* off, double* out, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   const unsigned sentinel = static_cast<unsigned>(nx) * ny * nz;
   const long long total = static_cast<long long>(n) * S;
   agent_sample_kernel<T><<<static_cast<unsigned>((total + 255) / 256), 256, 0, st>>>(n, dev_voxel, sentinel, S, nx,
-                                                                                      ny, nz, nxp, f, out);
+                                                                                      ny, nz, nxp, f, off, out);
   return cudaGetLastError();
 }
 
 template cudaError_t agents_apply_sources<double>(int, const unsigned*, int, int, int, int, int, const double*,
-                                                  const double*, const double*, double*, cudaStream_t);
+                                                  const double*, const double*, const double*, double*, cudaStream_t);
 template cudaError_t agents_apply_sources<float>(int, const unsigned*, int, int, int, int, int, const double*,
-                                                 const double*, const double*, float*, cudaStream_t);
-template cudaError_t agents_sample<double>(int, const unsigned*, int, int, int, int, int, const double*, double*,
-                                           cudaStream_t);
-template cudaError_t agents_sample<float>(int, const unsigned*, int, int, int, int, int, const float*, double*,
-                                          cudaStream_t);
+                                                 const double*, const double*, const double*, float*, cudaStream_t);
+template cudaError_t agents_sample<double>(int, const unsigned*, int, int, int, int, int, const double*,
+                                           const double*, double*, cudaStream_t);
+template cudaError_t agents_sample<float>(int, const unsigned*, int, int, int, int, int, const float*, const double*,
+                                          double*, cudaStream_t);
 
 }  // namespace bfvm

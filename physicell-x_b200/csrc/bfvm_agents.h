@@ -38,12 +38,14 @@ cudaError_t agents_compute_constants(int n, int S, double dt, double voxel_volum
 // Sorts and bins the list; *launches receives the number of kernels launched.
 cudaError_t agents_build(const AgentBuild& b, cudaStream_t st, int* launches);
 
+// off: [S] field offsets of an FP32 solve (the field holds rho - off), or null.
 template <typename T>
 cudaError_t agents_apply_sources(int n, const unsigned* sorted_keys, int S, int nx, int ny, int nz, int nxp,
-                                 const double* ac1, const double* ac2, const double* ae2, T* f, cudaStream_t st);
+                                 const double* ac1, const double* ac2, const double* ae2, const double* off, T* f,
+                                 cudaStream_t st);
 
 template <typename T>
 cudaError_t agents_sample(int n, const unsigned* dev_voxel, int S, int nx, int ny, int nz, int nxp, const T* f,
-                          double* out, cudaStream_t st);
+                          const double* off, double* out, cudaStream_t st);
 
 }  // namespace bfvm

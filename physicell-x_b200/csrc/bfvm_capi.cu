@@ -1,5 +1,6 @@
 // bfvm_capi.cu -- the C ABI (include/biofvm_b200.h): one resident
 // microenvironment solve per handle.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -78,7 +79,9 @@ struct bfvm_ctx {
   double* d_denom = nullptr;   // x | y | z
   void* d_rcp = nullptr;       // x | y | z
   void* d_cup = nullptr;       // x | y | z
-  void* d_c1 = nullptr;
+  void* d_c1 = nullptr;         // c1 hi [S] (| lo [S] in FP32)
+  double* d_off = nullptr;      // FP32: per-substrate field offsets [S]
+  void* d_shift = nullptr;      // FP32: RN32(c2 * off) [S]
   int* d_active = nullptr;
   double* d_faces = nullptr;   // xface | yface | zface
   int* d_status = nullptr;
@@ -102,6 +105,9 @@ struct bfvm_ctx {
   double* d_sample = nullptr;
   // host-side mirrors
   std::vector<unsigned char> active;
+  std::vector<double> faces;    // same layout as d_faces
+  std::vector<double> c2;       // dt*decay/3 per substrate (thomas_constant2)
+  std::vector<double> off;      // FP32 offsets currently applied to the field
   size_t device_bytes = 0;
   double* d_staging = nullptr; // reference-layout field, for host uploads/downloads
   // per-kernel timing: 4 events per recorded step
@@ -158,18 +164,25 @@ SweepParams<T> make_params(bfvm_ctx* c, bool sources) {
   p.nz = c->nz;
   p.S = c->S;
   p.nxp = c->nxp;
-  p.c1 = static_cast<const T*>(c->d_c1);
-  p.active = c->d_active;
   const size_t S = c->S;
+  const bool f32 = sizeof(T) == 4;
+  p.c1 = static_cast<const T*>(c->d_c1);
+  p.c1_lo = f32 ? p.c1 + S : nullptr;
+  p.off = f32 ? c->d_off : nullptr;
+  p.shift = f32 ? static_cast<const T*>(c->d_shift) : nullptr;
+  p.active = c->d_active;
   p.xface = c->d_faces;
   p.yface = p.xface + 2 * S * c->nz * c->ny;
   p.zface = p.yface + 2 * S * c->nz * c->nx;
   const T* rcp = static_cast<const T*>(c->d_rcp);
   const T* cup = static_cast<const T*>(c->d_cup);
   const size_t ox = 0, oy = S * c->nx, oz = oy + S * c->ny;
-  p.ax = {c->d_denom + ox, rcp + ox, cup + ox};
-  p.ay = {c->d_denom + oy, rcp + oy, cup + oy};
-  p.az = {c->d_denom + oz, rcp + oz, cup + oz};
+  const size_t tot = S * (c->nx + c->ny + c->nz);
+  const T* rlo = f32 ? rcp + tot : nullptr;
+  const T* clo = f32 ? cup + tot : nullptr;
+  p.ax = {c->d_denom + ox, rcp + ox, cup + ox, f32 ? rlo + ox : nullptr, f32 ? clo + ox : nullptr};
+  p.ay = {c->d_denom + oy, rcp + oy, cup + oy, f32 ? rlo + oy : nullptr, f32 ? clo + oy : nullptr};
+  p.az = {c->d_denom + oz, rcp + oz, cup + oz, f32 ? rlo + oz : nullptr, f32 ? clo + oz : nullptr};
   if (sources && c->n_agents > 0) {
     p.line_off = c->d_line_off;
     p.a_i = c->d_a_i;
@@ -223,7 +236,7 @@ bool pick_config(int eb, int nx, int ny, int nz, SweepConfig* cfg) {
   c.x_lines = 32;
   c.yz_tile = 32;
   c.yz_chunk = 32;
-  const int min_tile = 16 / eb * 2;  // >= 16 bytes per TMA row and an even warp split
+  const int min_tile = 128 / eb;  // keeps every TMA chunk 128-byte aligned in shared memory
   while (!config_fits(eb, nx, ny, nz, c)) {
     bool changed = false;
     if (sweep_x_smem(eb, nx, c) > 227 * 1024 && c.x_lines > 8) {
@@ -265,16 +278,29 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
     BFVM_CUDA(cudaMemcpy(c->d_cup, cup64.data(), tot * 8, cudaMemcpyHostToDevice));
     BFVM_CUDA(cudaMemcpy(c->d_c1, c1.data(), S * 8, cudaMemcpyHostToDevice));
   } else {
-    // FP32 form: the FP64 factorization rounded once.
-    std::vector<float> r32(tot), c32(tot), k32(S);
+    // FP32 form: each FP64 coefficient rounded once into a float pair
+    // hi = RN32(x), lo = RN32(x - hi); arrays are [hi | lo].
+    std::vector<float> r32(2 * tot), c32(2 * tot), k32(2 * S);
+    auto split = [](double x, float* hi, float* lo) {
+      *hi = static_cast<float>(x);
+      *lo = static_cast<float>(x - static_cast<double>(*hi));
+    };
     for (size_t q = 0; q < tot; ++q) {
-      r32[q] = static_cast<float>(rcp64[q]);
-      c32[q] = static_cast<float>(cup64[q]);
+      split(rcp64[q], &r32[q], &r32[tot + q]);
+      split(cup64[q], &c32[q], &c32[tot + q]);
     }
-    for (int s = 0; s < S; ++s) k32[s] = static_cast<float>(c1[s]);
-    BFVM_CUDA(cudaMemcpy(c->d_rcp, r32.data(), tot * 4, cudaMemcpyHostToDevice));
-    BFVM_CUDA(cudaMemcpy(c->d_cup, c32.data(), tot * 4, cudaMemcpyHostToDevice));
-    BFVM_CUDA(cudaMemcpy(c->d_c1, k32.data(), S * 4, cudaMemcpyHostToDevice));
+    for (int s = 0; s < S; ++s) split(c1[s], &k32[s], &k32[S + s]);
+    BFVM_CUDA(cudaMemcpy(c->d_rcp, r32.data(), 2 * tot * 4, cudaMemcpyHostToDevice));
+    BFVM_CUDA(cudaMemcpy(c->d_cup, c32.data(), 2 * tot * 4, cudaMemcpyHostToDevice));
+    BFVM_CUDA(cudaMemcpy(c->d_c1, k32.data(), 2 * S * 4, cudaMemcpyHostToDevice));
+  }
+  // thomas_constant2 = decay; *= dt; /= 3 (BioFVM_solvers.cpp:208-209)
+  c->c2.assign(S, 0.0);
+  for (int s = 0; s < S; ++s) {
+    double k2 = decay[s];
+    k2 *= c->dt;
+    k2 /= 3.0;
+    c->c2[s] = k2;
   }
   return BFVM_OK;
 }
@@ -427,9 +453,12 @@ int bfvm_create(const bfvm_config* cfg, bfvm_ctx** out) {
   int rc = BFVM_OK;
   if (rc == BFVM_OK) rc = dalloc(c, &c->f, c->field_bytes);
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_denom), tot * 8);
-  if (rc == BFVM_OK) rc = dalloc(c, &c->d_rcp, tot * c->eb);
-  if (rc == BFVM_OK) rc = dalloc(c, &c->d_cup, tot * c->eb);
-  if (rc == BFVM_OK) rc = dalloc(c, &c->d_c1, S * c->eb);
+  const size_t parts = c->prec == BFVM_FP32 ? 2 : 1;  // FP32 keeps hi and lo parts
+  if (rc == BFVM_OK) rc = dalloc(c, &c->d_rcp, parts * tot * c->eb);
+  if (rc == BFVM_OK) rc = dalloc(c, &c->d_cup, parts * tot * c->eb);
+  if (rc == BFVM_OK) rc = dalloc(c, &c->d_c1, parts * S * c->eb);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_off), S * sizeof(double));
+  if (rc == BFVM_OK) rc = dalloc(c, &c->d_shift, S * sizeof(float));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_active), S * sizeof(int));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_faces), face_elems(c) * 8);
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_status), sizeof(int));
@@ -444,9 +473,13 @@ int bfvm_create(const bfvm_config* cfg, bfvm_ctx** out) {
   // Reference defaults: activation on, value 1.0 on every face voxel.
   c->active.assign(S, 1);
   std::vector<int> act(S, 1);
-  std::vector<double> ones(face_elems(c), 1.0);
+  c->faces.assign(face_elems(c), 1.0);
+  c->off.assign(S, 0.0);
+  std::vector<float> zero32(S, 0.f);
   if (cudaMemcpy(c->d_active, act.data(), S * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(c->d_faces, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+      cudaMemcpy(c->d_faces, c->faces.data(), c->faces.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_off, c->off.data(), S * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_shift, zero32.data(), S * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(BFVM_ERR_CUDA);
   if (encode_field_maps(&c->maps, c->f, c->eb, c->nx, c->ny, c->nz, c->S, c->nxp, c->cfg) != 0)
     return fail(BFVM_ERR_CUDA);
@@ -464,6 +497,8 @@ int bfvm_destroy(bfvm_ctx* c) {
   dfree(c->d_rcp);
   dfree(c->d_cup);
   dfree(c->d_c1);
+  dfree(c->d_off);
+  dfree(c->d_shift);
   dfree(c->d_active);
   dfree(c->d_faces);
   dfree(c->d_status);
@@ -520,6 +555,7 @@ int bfvm_set_dirichlet_face(bfvm_ctx* c, int face, const double* values) {
   }
   BFVM_CUDA(cudaStreamSynchronize(c->stream));
   BFVM_CUDA(cudaMemcpy(c->d_faces + dst_off, plane.data(), plane.size() * 8, cudaMemcpyHostToDevice));
+  std::copy(plane.begin(), plane.end(), c->faces.begin() + dst_off);
   return BFVM_OK;
 }
 
@@ -540,6 +576,7 @@ int bfvm_set_dirichlet_uniform(bfvm_ctx* c, const double* values) {
       for (size_t q = 0; q < static_cast<size_t>(ny) * nx; ++q) all[o++] = values[s];
   BFVM_CUDA(cudaStreamSynchronize(c->stream));
   BFVM_CUDA(cudaMemcpy(c->d_faces, all.data(), all.size() * 8, cudaMemcpyHostToDevice));
+  c->faces = all;
   return BFVM_OK;
 }
 
@@ -549,11 +586,52 @@ static int ensure_staging(bfvm_ctx* c) {
                 sizeof(double) * static_cast<size_t>(c->nx) * c->ny * c->nz * c->S);
 }
 
+// FP32 solves store each substrate as a deviation from an FP64 offset: the
+// mean Dirichlet face value of an activated substrate, else 0.  Values near
+// the boundary value then keep more significant bits, and the sweeps stay
+// exact in structure (a constant solves the zero-flux system up to the
+// factor 1 + c2, which the right-hand-side shift accounts for).  The offsets
+// are chosen when a field is uploaded.
+static int choose_offsets(bfvm_ctx* c) {
+  if (c->prec != BFVM_FP32) return BFVM_OK;
+  const int S = c->S, nx = c->nx, ny = c->ny, nz = c->nz;
+  std::vector<double> off(S, 0.0);
+  std::vector<float> shift(S, 0.f);
+  const size_t px = static_cast<size_t>(nz) * ny, py = static_cast<size_t>(nz) * nx,
+               pz = static_cast<size_t>(ny) * nx;
+  for (int s = 0; s < S; ++s) {
+    if (!c->active[s]) continue;
+    double acc = 0.0;
+    size_t cnt = 0;
+    for (int side = 0; side < 2; ++side) {
+      const double* a = c->faces.data() + (static_cast<size_t>(side) * S + s) * px;
+      for (size_t q = 0; q < px; ++q) acc += a[q];
+      const double* b = c->faces.data() + 2 * S * px + (static_cast<size_t>(side) * S + s) * py;
+      for (size_t q = 0; q < py; ++q) acc += b[q];
+      const double* z = c->faces.data() + 2 * S * px + 2 * S * py + (static_cast<size_t>(side) * S + s) * pz;
+      for (size_t q = 0; q < pz; ++q) acc += z[q];
+      cnt += px + py + pz;
+    }
+    off[s] = acc / static_cast<double>(cnt);
+    shift[s] = static_cast<float>(c->c2[s] * off[s]);
+  }
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  BFVM_CUDA(cudaMemcpy(c->d_off, off.data(), S * sizeof(double), cudaMemcpyHostToDevice));
+  BFVM_CUDA(cudaMemcpy(c->d_shift, shift.data(), S * sizeof(float), cudaMemcpyHostToDevice));
+  c->off = off;
+  return BFVM_OK;
+}
+
 static int pack_from_device_aos(bfvm_ctx* c, const double* d_aos) {
-  if (c->prec == BFVM_FP64)
-    BFVM_CUDA(launch_pack<double>(d_aos, static_cast<double*>(c->f), c->nx, c->ny, c->nz, c->S, c->nxp, c->stream));
-  else
-    BFVM_CUDA(launch_pack<float>(d_aos, static_cast<float*>(c->f), c->nx, c->ny, c->nz, c->S, c->nxp, c->stream));
+  if (c->prec == BFVM_FP64) {
+    BFVM_CUDA(launch_pack<double>(d_aos, static_cast<double*>(c->f), c->nx, c->ny, c->nz, c->S, c->nxp, nullptr,
+                                  c->stream));
+  } else {
+    const int rc = choose_offsets(c);
+    if (rc != BFVM_OK) return rc;
+    BFVM_CUDA(launch_pack<float>(d_aos, static_cast<float*>(c->f), c->nx, c->ny, c->nz, c->S, c->nxp, c->d_off,
+                                 c->stream));
+  }
   note_launches(1);
   return BFVM_OK;
 }
@@ -561,10 +639,10 @@ static int pack_from_device_aos(bfvm_ctx* c, const double* d_aos) {
 static int unpack_to_device_aos(bfvm_ctx* c, double* d_aos) {
   if (c->prec == BFVM_FP64)
     BFVM_CUDA(launch_unpack<double>(static_cast<const double*>(c->f), d_aos, c->nx, c->ny, c->nz, c->S, c->nxp,
-                                    c->stream));
+                                    nullptr, c->stream));
   else
-    BFVM_CUDA(
-        launch_unpack<float>(static_cast<const float*>(c->f), d_aos, c->nx, c->ny, c->nz, c->S, c->nxp, c->stream));
+    BFVM_CUDA(launch_unpack<float>(static_cast<const float*>(c->f), d_aos, c->nx, c->ny, c->nz, c->S, c->nxp,
+                                   c->d_off, c->stream));
   note_launches(1);
   return BFVM_OK;
 }
@@ -680,10 +758,12 @@ int bfvm_apply_sources(bfvm_ctx* c) {
   const size_t SN = static_cast<size_t>(c->S) * c->n_agents;
   if (c->prec == BFVM_FP64)
     BFVM_CUDA(agents_apply_sources<double>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
-                                           c->d_ac + SN, c->d_ac + 2 * SN, static_cast<double*>(c->f), c->stream));
+                                           c->d_ac + SN, c->d_ac + 2 * SN, nullptr, static_cast<double*>(c->f),
+                                           c->stream));
   else
     BFVM_CUDA(agents_apply_sources<float>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
-                                          c->d_ac + SN, c->d_ac + 2 * SN, static_cast<float*>(c->f), c->stream));
+                                          c->d_ac + SN, c->d_ac + 2 * SN, c->d_off, static_cast<float*>(c->f),
+                                          c->stream));
   note_launches(1);
   return BFVM_OK;
 }
@@ -694,10 +774,10 @@ int bfvm_sample_agents(bfvm_ctx* c, double* out) {
   if (c->n_agents == 0) return BFVM_OK;
   if (c->prec == BFVM_FP64)
     BFVM_CUDA(agents_sample<double>(c->n_agents, c->d_dev_voxel, c->S, c->nx, c->ny, c->nz, c->nxp,
-                                    static_cast<const double*>(c->f), c->d_sample, c->stream));
+                                    static_cast<const double*>(c->f), nullptr, c->d_sample, c->stream));
   else
     BFVM_CUDA(agents_sample<float>(c->n_agents, c->d_dev_voxel, c->S, c->nx, c->ny, c->nz, c->nxp,
-                                   static_cast<const float*>(c->f), c->d_sample, c->stream));
+                                   static_cast<const float*>(c->f), c->d_off, c->d_sample, c->stream));
   note_launches(1);
   BFVM_CUDA(cudaMemcpyAsync(out, c->d_sample, sizeof(double) * c->S * static_cast<size_t>(c->n_agents),
                             cudaMemcpyDeviceToHost, c->stream));
@@ -758,7 +838,18 @@ extern "C" int bfvm_field_sums(bfvm_ctx* c, double* out) {
   BFVM_CUDA(cudaGetLastError());
   note_launches(2);
   BFVM_CUDA(cudaMemcpyAsync(out, res, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->stream));
-  return bfvm_synchronize(c);
+  const int rc = bfvm_synchronize(c);
+  if (rc == BFVM_OK && c->prec == BFVM_FP32) {
+    const double nv = static_cast<double>(c->nx) * c->ny * c->nz;
+    for (int s = 0; s < c->S; ++s) out[s] += c->off[s] * nv;
+  }
+  return rc;
+}
+
+extern "C" int bfvm_field_offsets(bfvm_ctx* c, double* out) {
+  if (!c || !out) return BFVM_ERR_ARG;
+  for (int s = 0; s < c->S; ++s) out[s] = c->off[s];
+  return BFVM_OK;
 }
 
 extern "C" int bfvm_synchronize(bfvm_ctx* c) {
@@ -831,10 +922,11 @@ extern "C" int bfvm_set_launch(bfvm_ctx* c, int x_lines, int yz_tile, int yz_chu
   cfg.x_lines = x_lines;
   cfg.yz_tile = yz_tile;
   cfg.yz_chunk = yz_chunk;
-  // x_lines: multiple of 8 (1024-byte swizzle atoms); yz_tile: a whole number
-  // of 16-byte units per row (TMA x alignment); both at most 256 (box limit).
+  // x_lines: multiple of 8 (1024-byte swizzle atoms); yz_tile: whole 128-byte
+  // rows, so every TMA chunk starts 128-byte aligned in shared memory and
+  // every box's x coordinate is 16-byte aligned; both at most 256 (box limit).
   if (x_lines < 8 || x_lines > 256 || x_lines % 8 != 0) return BFVM_ERR_ARG;
-  if (yz_tile < 1 || yz_tile > 256 || (yz_tile * c->eb) % 16 != 0) return BFVM_ERR_ARG;
+  if (yz_tile < 1 || yz_tile > 256 || (yz_tile * c->eb) % 128 != 0) return BFVM_ERR_ARG;
   if (yz_chunk < 1 || yz_chunk > 256) return BFVM_ERR_ARG;
   if (!config_fits(c->eb, c->nx, c->ny, c->nz, cfg)) return BFVM_ERR_SHAPE;
   DeviceGuard g(c->device);

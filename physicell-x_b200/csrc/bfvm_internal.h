@@ -24,18 +24,30 @@ namespace bfvm {
 constexpr int kMaxSubstrates = 64;
 
 // Thomas coefficients of one axis for all substrates, index [s][i].
+// The FP32 form keeps each FP64 coefficient as a float pair hi + lo
+// (hi = RN32(x), lo = RN32(x - hi)), so the fixed coefficients carry no
+// FP32 rounding bias from step to step; the FP64 form leaves the lo arrays
+// null.
 template <typename T>
 struct AxisCoefs {
   const double* denom;  // modified diagonal (FP64 always)
-  const T* rcp;         // RN(1/denom) in T
-  const T* cup;         // modified upper diagonal in T
+  const T* rcp;         // RN(1/denom) in T (hi part in FP32)
+  const T* cup;         // modified upper diagonal in T (hi part in FP32)
+  const T* rcp_lo;      // FP32 only: low parts
+  const T* cup_lo;
 };
 
 template <typename T>
 struct SweepParams {
   T* f;                  // field base
   int nx, ny, nz, S, nxp;
-  const T* c1;           // [S] dt*D/dx^2
+  const T* c1;           // [S] dt*D/dx^2 (hi part in FP32)
+  const T* c1_lo;        // [S] FP32 only: low part of c1
+  // FP32 only: the field holds rho - off[s]; each sweep's right-hand side is
+  // shifted by shift[s] = RN32(dt*decay/3 * off[s]) to match (the constant
+  // off[s] solves the zero-flux system with factor 1 + dt*decay/3).
+  const double* off;     // [S] or null (FP64)
+  const T* shift;        // [S] or null (FP64)
   const int* active;     // [S] Dirichlet activation
   // Face planes (resolved Dirichlet value of each face voxel), FP64:
   //   xface[side][s][k][j], yface[side][s][k][i], zface[side][s][j][i]
@@ -88,9 +100,12 @@ size_t sweep_yz_smem(int elem_bytes, int n_line, const SweepConfig& cfg);
 
 // Layout conversion between the reference AoS [x][y][z][S] (double) and the
 // device SoA [S][z][y][nxp] (T).
+// off: [S] offsets subtracted on pack / added on unpack (FP32), or null.
 template <typename T>
-cudaError_t launch_pack(const double* aos, T* f, int nx, int ny, int nz, int S, int nxp, cudaStream_t st);
+cudaError_t launch_pack(const double* aos, T* f, int nx, int ny, int nz, int S, int nxp, const double* off,
+                        cudaStream_t st);
 template <typename T>
-cudaError_t launch_unpack(const T* f, double* aos, int nx, int ny, int nz, int S, int nxp, cudaStream_t st);
+cudaError_t launch_unpack(const T* f, double* aos, int nx, int ny, int nz, int S, int nxp, const double* off,
+                          cudaStream_t st);
 
 }  // namespace bfvm

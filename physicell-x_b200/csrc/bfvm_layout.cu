@@ -14,16 +14,21 @@ namespace bfvm {
 
 namespace {
 
+// FP32 fields hold rho - off[s] (off null for FP64, where values are exact).
 template <typename T>
 __global__ void pack_kernel(const double* __restrict__ aos, T* __restrict__ f, int nx, int ny, int nz, int S,
-                            int nxp) {
+                            int nxp, const double* __restrict__ off) {
   __shared__ double tile[32][33];
   const int k0 = blockIdx.x * 32, i0 = blockIdx.y * 32, j = blockIdx.z;
   const int tx = threadIdx.x, ty = threadIdx.y;
   for (int s = 0; s < S; ++s) {
+    const double o = off ? off[s] : 0.0;
     for (int r = ty; r < 32; r += 8) {
       const int i = i0 + r, k = k0 + tx;
-      if (i < nx && k < nz) tile[r][tx] = aos[((static_cast<size_t>(i) * ny + j) * nz + k) * S + s];
+      if (i < nx && k < nz) {
+        const double v = aos[((static_cast<size_t>(i) * ny + j) * nz + k) * S + s];
+        tile[r][tx] = off ? v - o : v;
+      }
     }
     __syncthreads();
     for (int r = ty; r < 32; r += 8) {
@@ -36,14 +41,18 @@ __global__ void pack_kernel(const double* __restrict__ aos, T* __restrict__ f, i
 
 template <typename T>
 __global__ void unpack_kernel(const T* __restrict__ f, double* __restrict__ aos, int nx, int ny, int nz, int S,
-                              int nxp) {
+                              int nxp, const double* __restrict__ off) {
   __shared__ double tile[32][33];
   const int k0 = blockIdx.x * 32, i0 = blockIdx.y * 32, j = blockIdx.z;
   const int tx = threadIdx.x, ty = threadIdx.y;
   for (int s = 0; s < S; ++s) {
+    const double o = off ? off[s] : 0.0;
     for (int r = ty; r < 32; r += 8) {
       const int k = k0 + r, i = i0 + tx;
-      if (i < nx && k < nz) tile[r][tx] = static_cast<double>(f[((static_cast<size_t>(s) * nz + k) * ny + j) * nxp + i]);
+      if (i < nx && k < nz) {
+        const double v = static_cast<double>(f[((static_cast<size_t>(s) * nz + k) * ny + j) * nxp + i]);
+        tile[r][tx] = off ? v + o : v;
+      }
     }
     __syncthreads();
     for (int r = ty; r < 32; r += 8) {
@@ -57,22 +66,27 @@ __global__ void unpack_kernel(const T* __restrict__ f, double* __restrict__ aos,
 }  // namespace
 
 template <typename T>
-cudaError_t launch_pack(const double* aos, T* f, int nx, int ny, int nz, int S, int nxp, cudaStream_t st) {
+cudaError_t launch_pack(const double* aos, T* f, int nx, int ny, int nz, int S, int nxp, const double* off,
+                        cudaStream_t st) {
   dim3 grid((nz + 31) / 32, (nx + 31) / 32, ny), block(32, 8);
-  pack_kernel<T><<<grid, block, 0, st>>>(aos, f, nx, ny, nz, S, nxp);
+  pack_kernel<T><<<grid, block, 0, st>>>(aos, f, nx, ny, nz, S, nxp, off);
   return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t launch_unpack(const T* f, double* aos, int nx, int ny, int nz, int S, int nxp, cudaStream_t st) {
+cudaError_t launch_unpack(const T* f, double* aos, int nx, int ny, int nz, int S, int nxp, const double* off,
+                          cudaStream_t st) {
   dim3 grid((nz + 31) / 32, (nx + 31) / 32, ny), block(32, 8);
-  unpack_kernel<T><<<grid, block, 0, st>>>(f, aos, nx, ny, nz, S, nxp);
+  unpack_kernel<T><<<grid, block, 0, st>>>(f, aos, nx, ny, nz, S, nxp, off);
   return cudaGetLastError();
 }
 
-template cudaError_t launch_pack<double>(const double*, double*, int, int, int, int, int, cudaStream_t);
-template cudaError_t launch_pack<float>(const double*, float*, int, int, int, int, int, cudaStream_t);
-template cudaError_t launch_unpack<double>(const double*, double*, int, int, int, int, int, cudaStream_t);
-template cudaError_t launch_unpack<float>(const float*, double*, int, int, int, int, int, cudaStream_t);
+template cudaError_t launch_pack<double>(const double*, double*, int, int, int, int, int, const double*,
+                                         cudaStream_t);
+template cudaError_t launch_pack<float>(const double*, float*, int, int, int, int, int, const double*, cudaStream_t);
+template cudaError_t launch_unpack<double>(const double*, double*, int, int, int, int, int, const double*,
+                                           cudaStream_t);
+template cudaError_t launch_unpack<float>(const float*, double*, int, int, int, int, int, const double*,
+                                          cudaStream_t);
 
 }  // namespace bfvm

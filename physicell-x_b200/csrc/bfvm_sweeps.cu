@@ -17,9 +17,15 @@
 //            128-byte-wide boxes with the 128B swizzle, so thread t reading
 //            16-byte units of its own row (a transpose in shared memory) hits
 //            eight distinct bank groups per quarter-warp.  Agent sources and
-//            the first Dirichlet pin are applied as each element is read.
+//            the first Dirichlet pin are applied to the staged row before the
+//            recurrence reads it.
 //   y, z     consecutive threads own consecutive x; the tile is [line][x], so
 //            each step of the recurrence reads one contiguous shared-memory row.
+//
+// The recurrence is serial per line, so its speed is the latency of the
+// dependent FP64 chain.  Every load a step needs (its staged value and its
+// coefficients) is therefore issued for a whole batch of elements before the
+// chain over that batch starts; the chain itself only touches registers.
 //
 // Dirichlet pins are fused: a line lying in an activated face is written with
 // its face values; other lines get their two end voxels pinned after the
@@ -50,29 +56,42 @@ struct Arith;
 
 template <>
 struct Arith<double> {
-  static __device__ __forceinline__ double fwd0(double v, double d, double r) { return div_exact(v, d, r); }
-  static __device__ __forceinline__ double fwd(double c1, double yprev, double v, double d, double r) {
-    return div_exact(__fma_rn(c1, yprev, v), d, r);
+  // t_i = p_i + c1*y_{i-1}, contracted as the reference's g++ build does
+  static __device__ __forceinline__ double lin(double c1, double, double yprev, double v) {
+    return __fma_rn(c1, yprev, v);
   }
-  static __device__ __forceinline__ double back(double c, double xnext, double y) { return __fma_rn(-c, xnext, y); }
+  static __device__ __forceinline__ double div(double t, double d, double r, double) { return div_exact(t, d, r); }
+  static __device__ __forceinline__ double back(double c, double, double xnext, double y) {
+    return __fma_rn(-c, xnext, y);
+  }
 };
 
+// FP32: every fixed coefficient is a (hi, lo) float pair; the low part is
+// applied first so the pair acts as one coefficient of ~48 bits.
 template <>
 struct Arith<float> {
-  static __device__ __forceinline__ float fwd0(float v, double, float r) { return v * r; }
-  static __device__ __forceinline__ float fwd(float c1, float yprev, float v, double, float r) {
-    return __fmul_rn(__fmaf_rn(c1, yprev, v), r);
+  static __device__ __forceinline__ float lin(float c1h, float c1l, float yprev, float v) {
+    return __fmaf_rn(c1h, yprev, __fmaf_rn(c1l, yprev, v));
   }
-  static __device__ __forceinline__ float back(float c, float xnext, float y) { return __fmaf_rn(-c, xnext, y); }
+  static __device__ __forceinline__ float div(float t, double, float rh, float rl) {
+    return __fmaf_rn(t, rh, __fmul_rn(t, rl));
+  }
+  static __device__ __forceinline__ float back(float ch, float cl, float xnext, float y) {
+    return __fmaf_rn(-ch, xnext, __fmaf_rn(-cl, xnext, y));
+  }
 };
+
+template <typename T>
+constexpr bool kF32 = sizeof(T) == 4;
 
 // Apply every agent of voxel i (agents of this line are sorted by x index,
 // then by agent index) to the value v, in FP64, and return the result.
 template <typename T>
 __device__ __forceinline__ T apply_agents(T v, int i, int& a, int aend, int& next_i, const int* __restrict__ a_i,
                                           const double* __restrict__ c1, const double* __restrict__ c2,
-                                          const double* __restrict__ e2) {
+                                          const double* __restrict__ e2, double off) {
   double r = static_cast<double>(v);
+  if constexpr (kF32<T>) r += off;
   do {
     r += c1[a];
     r /= c2[a];
@@ -80,7 +99,16 @@ __device__ __forceinline__ T apply_agents(T v, int i, int& a, int aend, int& nex
     ++a;
     next_i = (a < aend) ? __ldg(a_i + a) : INT_MAX;
   } while (next_i == i);
+  if constexpr (kF32<T>) r -= off;
   return static_cast<T>(r);
+}
+
+// Address of element e (0..W-1) of a thread's 128-byte row in a chunk staged
+// with the 128B swizzle: 16-byte unit (e/U) is stored at unit (e/U) ^ (row%8).
+template <typename T>
+__device__ __forceinline__ T* swz_elem(unsigned char* row, int e, int sw) {
+  constexpr int U = 16 / sizeof(T);
+  return reinterpret_cast<T*>(row + (((e / U) ^ sw) << 4) + (e % U) * sizeof(T));
 }
 
 }  // namespace
@@ -132,10 +160,11 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
     else
       fv = p.yface + ((static_cast<size_t>(j == 0 ? 0 : 1) * S + s) * nz + k) * nx;
   }
-  double x0v = 0.0, x1v = 0.0;
+  const double off = kF32<T> ? p.off[s] : 0.0;
+  T x0v = T(0), x1v = T(0);
   if (act && valid) {
-    x0v = p.xface[(static_cast<size_t>(0 * S + s) * nz + k) * ny + j];
-    x1v = p.xface[(static_cast<size_t>(1 * S + s) * nz + k) * ny + j];
+    x0v = static_cast<T>(p.xface[(static_cast<size_t>(0 * S + s) * nz + k) * ny + j] - off);
+    x1v = static_cast<T>(p.xface[(static_cast<size_t>(1 * S + s) * nz + k) * ny + j] - off);
   }
   int a = 0, aend = 0, next_i = INT_MAX;
   const double *ac1 = nullptr, *ac2 = nullptr, *ae2 = nullptr;
@@ -151,37 +180,73 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
   const double* __restrict__ dn = p.ax.denom + static_cast<size_t>(s) * nx;
   const T* __restrict__ rc = p.ax.rcp + static_cast<size_t>(s) * nx;
   const T* __restrict__ cu = p.ax.cup + static_cast<size_t>(s) * nx;
+  const T* __restrict__ rcl = kF32<T> ? p.ax.rcp_lo + static_cast<size_t>(s) * nx : nullptr;
+  const T* __restrict__ cul = kF32<T> ? p.ax.cup_lo + static_cast<size_t>(s) * nx : nullptr;
   const T c1 = p.c1[s];
+  const T c1l = kF32<T> ? p.c1_lo[s] : T(0);
+  const T shift = kF32<T> ? p.shift[s] : T(0);
 
   unsigned char* row = tile + static_cast<size_t>(t) * 128;
   const int sw = t & 7;
   bool ok = true;
 
-  // Forward elimination, chunk by chunk as the TMA boxes land.
+  // Forward elimination, one chunk at a time as the TMA boxes land.
   T yprev = T(0);
   for (int c = 0; c < C; ++c) {
     if (ok) ok = mbar_wait(smem_u32(&bars[c]), 0);
     if (face) continue;
     unsigned char* crow = row + static_cast<size_t>(c) * chunk_bytes;
+    const int i0 = c * W;
+    const int iend = min(nx, i0 + W);
+    // Sources, then the pin before the sweep, on the staged row.
+    while (next_i < iend) {
+      T* e = swz_elem<T>(crow, next_i - i0, sw);
+      *e = apply_agents<T>(*e, next_i, a, aend, next_i, p.a_i, ac1, ac2, ae2, off);
+    }
+    if (act) {
+      if (i0 == 0) *swz_elem<T>(crow, 0, sw) = x0v;
+      if (nx - 1 < iend) *swz_elem<T>(crow, nx - 1 - i0, sw) = x1v;
+    }
+    T v[W];
+    double d[W];
+    T r[W], rl[W];
 #pragma unroll
     for (int u = 0; u < W / U; ++u) {
-      Unit* up = reinterpret_cast<Unit*>(crow + ((u ^ sw) << 4));
-      Unit uv = *up;
+      const Unit uv = *reinterpret_cast<const Unit*>(crow + ((u ^ sw) << 4));
+      const T* ev = reinterpret_cast<const T*>(&uv);
+#pragma unroll
+      for (int q = 0; q < U; ++q) v[u * U + q] = ev[q];
+    }
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+      const int i = min(i0 + q, nx - 1);
+      r[q] = __ldg(rc + i);
+      if constexpr (kF32<T>) {
+        rl[q] = __ldg(rcl + i);
+        d[q] = 0.0;
+      } else {
+        d[q] = __ldg(dn + i);
+        rl[q] = T(0);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+      const int i = i0 + q;
+      if (i < nx) {
+        const T vq = kF32<T> ? v[q] - shift : v[q];
+        const T tt = (i == 0) ? vq : Arith<T>::lin(c1, c1l, yprev, vq);
+        const T y = Arith<T>::div(tt, d[q], r[q], rl[q]);
+        v[q] = y;
+        yprev = y;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < W / U; ++u) {
+      Unit uv;
       T* ev = reinterpret_cast<T*>(&uv);
 #pragma unroll
-      for (int q = 0; q < U; ++q) {
-        const int i = c * W + u * U + q;
-        if (i < nx) {
-          T v = ev[q];
-          if (i == next_i) v = apply_agents<T>(v, i, a, aend, next_i, p.a_i, ac1, ac2, ae2);
-          if (act && (i == 0 || i == nx - 1)) v = static_cast<T>(i == 0 ? x0v : x1v);
-          const T y = (i == 0) ? Arith<T>::fwd0(v, __ldg(dn), __ldg(rc))
-                               : Arith<T>::fwd(c1, yprev, v, __ldg(dn + i), __ldg(rc + i));
-          ev[q] = y;
-          yprev = y;
-        }
-      }
-      *up = uv;
+      for (int q = 0; q < U; ++q) ev[q] = v[u * U + q];
+      *reinterpret_cast<Unit*>(crow + ((u ^ sw) << 4)) = uv;
     }
   }
   if (__syncthreads_or(!ok)) {
@@ -193,25 +258,47 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
   T xnext = T(0);
   for (int c = C - 1; c >= 0; --c) {
     unsigned char* crow = row + static_cast<size_t>(c) * chunk_bytes;
+    const int i0 = c * W;
+    if (face) {
+      for (int q = 0; q < W; ++q)
+        if (i0 + q < nx) *swz_elem<T>(crow, q, sw) = static_cast<T>(fv != nullptr ? fv[i0 + q] - off : 0.0);
+    } else {
+      T v[W];
+      T cw[W], cwl[W];
 #pragma unroll
-    for (int u = W / U - 1; u >= 0; --u) {
-      Unit* up = reinterpret_cast<Unit*>(crow + ((u ^ sw) << 4));
-      Unit uv = *up;
-      T* ev = reinterpret_cast<T*>(&uv);
+      for (int u = 0; u < W / U; ++u) {
+        const Unit uv = *reinterpret_cast<const Unit*>(crow + ((u ^ sw) << 4));
+        const T* ev = reinterpret_cast<const T*>(&uv);
 #pragma unroll
-      for (int q = U - 1; q >= 0; --q) {
-        const int i = c * W + u * U + q;
+        for (int q = 0; q < U; ++q) v[u * U + q] = ev[q];
+      }
+#pragma unroll
+      for (int q = 0; q < W; ++q) {
+        const int i = min(i0 + q, nx - 1);
+        cw[q] = __ldg(cu + i);
+        cwl[q] = kF32<T> ? __ldg(cul + i) : T(0);
+      }
+#pragma unroll
+      for (int q = W - 1; q >= 0; --q) {
+        const int i = i0 + q;
         if (i < nx) {
-          if (face) {
-            ev[q] = static_cast<T>(fv != nullptr ? fv[i] : 0.0);
-          } else {
-            const T x = (i == nx - 1) ? ev[q] : Arith<T>::back(__ldg(cu + i), xnext, ev[q]);
-            xnext = x;
-            ev[q] = (act && (i == 0 || i == nx - 1)) ? static_cast<T>(i == 0 ? x0v : x1v) : x;
-          }
+          const T x = (i == nx - 1) ? v[q] : Arith<T>::back(cw[q], cwl[q], xnext, v[q]);
+          xnext = x;
+          v[q] = x;
         }
       }
-      *up = uv;
+#pragma unroll
+      for (int u = 0; u < W / U; ++u) {
+        Unit uv;
+        T* ev = reinterpret_cast<T*>(&uv);
+#pragma unroll
+        for (int q = 0; q < U; ++q) ev[q] = v[u * U + q];
+        *reinterpret_cast<Unit*>(crow + ((u ^ sw) << 4)) = uv;
+      }
+      if (act) {
+        if (i0 == 0) *swz_elem<T>(crow, 0, sw) = x0v;
+        if (nx - 1 < i0 + W) *swz_elem<T>(crow, nx - 1 - i0, sw) = x1v;
+      }
     }
     fence_async_smem();
     __syncthreads();
@@ -229,6 +316,7 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
 template <typename T, int AXIS>
 __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<T> p,
                                                        int CH) {
+  constexpr int R = 16;  // rows staged in registers per batch of the recurrence
   extern __shared__ unsigned char smem_raw[];
   const int TI = blockDim.x;
   const int nx = p.nx, ny = p.ny, nz = p.nz, S = p.S;
@@ -266,7 +354,8 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
   bool face;
   const double* fv = nullptr;  // face-line values: fv[r * fstride]
   size_t fstride = 1;
-  double e0v = 0.0, e1v = 0.0;  // pinned values at the two ends of the line
+  const double off = kF32<T> ? p.off[s] : 0.0;
+  T e0v = T(0), e1v = T(0);  // pinned values at the two ends of the line
   if (AXIS == 1) {
     const int k = m;
     face = act && (i == 0 || i == nx - 1 || k == 0 || k == nz - 1);
@@ -280,8 +369,8 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
       }
     }
     if (act && valid) {
-      e0v = p.yface[(static_cast<size_t>(0 * S + s) * nz + k) * nx + i];
-      e1v = p.yface[(static_cast<size_t>(1 * S + s) * nz + k) * nx + i];
+      e0v = static_cast<T>(p.yface[(static_cast<size_t>(0 * S + s) * nz + k) * nx + i] - off);
+      e1v = static_cast<T>(p.yface[(static_cast<size_t>(1 * S + s) * nz + k) * nx + i] - off);
     }
   } else {
     const int j = m;
@@ -296,15 +385,20 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
       }
     }
     if (act && valid) {
-      e0v = p.zface[(static_cast<size_t>(0 * S + s) * ny + j) * nx + i];
-      e1v = p.zface[(static_cast<size_t>(1 * S + s) * ny + j) * nx + i];
+      e0v = static_cast<T>(p.zface[(static_cast<size_t>(0 * S + s) * ny + j) * nx + i] - off);
+      e1v = static_cast<T>(p.zface[(static_cast<size_t>(1 * S + s) * ny + j) * nx + i] - off);
     }
   }
   const AxisCoefs<T>& ac = (AXIS == 1) ? p.ay : p.az;
   const double* __restrict__ dn = ac.denom + static_cast<size_t>(s) * n;
   const T* __restrict__ rc = ac.rcp + static_cast<size_t>(s) * n;
   const T* __restrict__ cu = ac.cup + static_cast<size_t>(s) * n;
+  const T* __restrict__ rcl = kF32<T> ? ac.rcp_lo + static_cast<size_t>(s) * n : nullptr;
+  const T* __restrict__ cul = kF32<T> ? ac.cup_lo + static_cast<size_t>(s) * n : nullptr;
   const T c1 = p.c1[s];
+  const T c1l = kF32<T> ? p.c1_lo[s] : T(0);
+  const T shift = kF32<T> ? p.shift[s] : T(0);
+  T* col = tile + t;
   bool ok = true;
 
   T yprev = T(0);
@@ -312,12 +406,34 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
     if (ok) ok = mbar_wait(smem_u32(&bars[c]), 0);
     if (face) continue;
     const int r1 = min(n, (c + 1) * CH);
-    for (int r = c * CH; r < r1; ++r) {
-      const T v = tile[static_cast<size_t>(r) * TI + t];
-      const T y = (r == 0) ? Arith<T>::fwd0(v, __ldg(dn), __ldg(rc))
-                           : Arith<T>::fwd(c1, yprev, v, __ldg(dn + r), __ldg(rc + r));
-      tile[static_cast<size_t>(r) * TI + t] = y;
-      yprev = y;
+    for (int rb = c * CH; rb < r1; rb += R) {
+      T v[R];
+      double d[R];
+      T r[R], rl[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int rr = min(rb + q, r1 - 1);
+        v[q] = col[static_cast<size_t>(rr) * TI];
+        r[q] = __ldg(rc + rr);
+        if constexpr (kF32<T>) {
+          rl[q] = __ldg(rcl + rr);
+          d[q] = 0.0;
+        } else {
+          d[q] = __ldg(dn + rr);
+          rl[q] = T(0);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int rr = rb + q;
+        if (rr < r1) {
+          const T vq = kF32<T> ? v[q] - shift : v[q];
+          const T tt = (rr == 0) ? vq : Arith<T>::lin(c1, c1l, yprev, vq);
+          const T y = Arith<T>::div(tt, d[q], r[q], rl[q]);
+          col[static_cast<size_t>(rr) * TI] = y;
+          yprev = y;
+        }
+      }
     }
   }
   if (__syncthreads_or(!ok)) {
@@ -327,15 +443,31 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
 
   T xnext = T(0);
   for (int c = C - 1; c >= 0; --c) {
+    const int r0 = c * CH;
     const int r1 = min(n, (c + 1) * CH);
-    for (int r = r1 - 1; r >= c * CH; --r) {
-      T* e = tile + static_cast<size_t>(r) * TI + t;
-      if (face) {
-        *e = static_cast<T>(fv != nullptr ? fv[r * fstride] : 0.0);
-      } else {
-        const T x = (r == n - 1) ? *e : Arith<T>::back(__ldg(cu + r), xnext, *e);
-        xnext = x;
-        *e = (act && (r == 0 || r == n - 1)) ? static_cast<T>(r == 0 ? e0v : e1v) : x;
+    if (face) {
+      for (int rr = r0; rr < r1; ++rr)
+        col[static_cast<size_t>(rr) * TI] = static_cast<T>(fv != nullptr ? fv[rr * fstride] - off : 0.0);
+    } else {
+      for (int rb = r1 - 1; rb >= r0; rb -= R) {
+        T v[R];
+        T cw[R], cwl[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int rr = max(rb - q, r0);
+          v[q] = col[static_cast<size_t>(rr) * TI];
+          cw[q] = __ldg(cu + rr);
+          cwl[q] = kF32<T> ? __ldg(cul + rr) : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int rr = rb - q;
+          if (rr >= r0) {
+            const T x = (rr == n - 1) ? v[q] : Arith<T>::back(cw[q], cwl[q], xnext, v[q]);
+            xnext = x;
+            col[static_cast<size_t>(rr) * TI] = (act && (rr == 0 || rr == n - 1)) ? (rr == 0 ? e0v : e1v) : x;
+          }
+        }
       }
     }
     fence_async_smem();

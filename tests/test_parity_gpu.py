@@ -180,7 +180,9 @@ def test_upload_download_roundtrip_and_sums():
         if prec == "fp64":
             assert np.array_equal(back, wl.field0)
         else:
-            assert np.array_equal(back, wl.field0.astype(np.float32).astype(np.float64))
+            # stored as an FP32 deviation from a per-substrate FP64 offset
+            err = np.max(np.abs(back - wl.field0))
+            assert err <= 2.0 ** -23 * np.max(np.abs(wl.field0)) * 2, err
         sums = me.field_sums()
         np.testing.assert_allclose(sums, back.reshape(-1, wl.S).sum(axis=0), rtol=1e-12)
 

@@ -75,11 +75,11 @@ struct bfvm_ctx {
   cudaStream_t stream = nullptr;
   void* f = nullptr;           // field, device layout
   size_t field_bytes = 0;
-  // coefficients: per axis denom (f64) [S][n], rcp (T) [S][n], cup (T) [S][n]; c1 (T) [S]
-  double* d_denom = nullptr;   // x | y | z
-  void* d_rcp = nullptr;       // x | y | z
-  void* d_cup = nullptr;       // x | y | z
-  void* d_c1 = nullptr;         // c1 hi [S] (| lo [S] in FP32)
+  // coefficients: per axis a, DR rows [S][npad_a] at dr_off[a] and CU rows
+  // [S][npad_a] at cu_off[a] (bytes into d_coef); c1 as Coef<T>::C1 [S]
+  void* d_coef = nullptr;
+  size_t dr_off[3] = {0, 0, 0}, cu_off[3] = {0, 0, 0};
+  void* d_c1 = nullptr;
   double* d_off = nullptr;      // FP32: per-substrate field offsets [S]
   void* d_shift = nullptr;      // FP32: RN32(c2 * off) [S]
   int* d_active = nullptr;
@@ -166,23 +166,23 @@ SweepParams<T> make_params(bfvm_ctx* c, bool sources) {
   p.nxp = c->nxp;
   const size_t S = c->S;
   const bool f32 = sizeof(T) == 4;
-  p.c1 = static_cast<const T*>(c->d_c1);
-  p.c1_lo = f32 ? p.c1 + S : nullptr;
+  using DR = typename Coef<T>::DR;
+  using CU = typename Coef<T>::CU;
+  p.c1 = static_cast<const typename Coef<T>::C1*>(c->d_c1);
   p.off = f32 ? c->d_off : nullptr;
   p.shift = f32 ? static_cast<const T*>(c->d_shift) : nullptr;
   p.active = c->d_active;
   p.xface = c->d_faces;
   p.yface = p.xface + 2 * S * c->nz * c->ny;
   p.zface = p.yface + 2 * S * c->nz * c->nx;
-  const T* rcp = static_cast<const T*>(c->d_rcp);
-  const T* cup = static_cast<const T*>(c->d_cup);
-  const size_t ox = 0, oy = S * c->nx, oz = oy + S * c->ny;
-  const size_t tot = S * (c->nx + c->ny + c->nz);
-  const T* rlo = f32 ? rcp + tot : nullptr;
-  const T* clo = f32 ? cup + tot : nullptr;
-  p.ax = {c->d_denom + ox, rcp + ox, cup + ox, f32 ? rlo + ox : nullptr, f32 ? clo + ox : nullptr};
-  p.ay = {c->d_denom + oy, rcp + oy, cup + oy, f32 ? rlo + oy : nullptr, f32 ? clo + oy : nullptr};
-  p.az = {c->d_denom + oz, rcp + oz, cup + oz, f32 ? rlo + oz : nullptr, f32 ? clo + oz : nullptr};
+  const unsigned char* cb = static_cast<const unsigned char*>(c->d_coef);
+  const int n_axis[3] = {c->nx, c->ny, c->nz};
+  AxisCoefs<T>* axes[3] = {&p.ax, &p.ay, &p.az};
+  for (int a = 0; a < 3; ++a) {
+    axes[a]->dr = reinterpret_cast<const DR*>(cb + c->dr_off[a]);
+    axes[a]->cu = reinterpret_cast<const CU*>(cb + c->cu_off[a]);
+    axes[a]->npad = coef_pad(n_axis[a]);
+  }
   if (sources && c->n_agents > 0) {
     p.line_off = c->d_line_off;
     p.a_i = c->d_a_i;
@@ -229,21 +229,20 @@ bool config_fits(int eb, int nx, int ny, int nz, const SweepConfig& cfg) {
   return sweep_x_smem(eb, nx, cfg) <= lim && sweep_yz_smem(eb, ny, cfg) <= lim && sweep_yz_smem(eb, nz, cfg) <= lim;
 }
 
-// Default launch shape: 32 lines / 32 x-columns per CTA, shrunk (keeping the
-// TMA x-coordinate alignment) until the staged lines fit in shared memory.
+// Default launch shape: 32-line tiles, shrunk (keeping whole 128-byte rows)
+// until a CTA's staged tile fits in shared memory.
 bool pick_config(int eb, int nx, int ny, int nz, SweepConfig* cfg) {
   SweepConfig c;
-  c.x_lines = 32;
-  c.yz_tile = 32;
-  c.yz_chunk = 32;
-  const int min_tile = 128 / eb;  // keeps every TMA chunk 128-byte aligned in shared memory
+  const int min_tile = 128 / eb;
+  const size_t lim = 227 * 1024;
   while (!config_fits(eb, nx, ny, nz, c)) {
     bool changed = false;
-    if (sweep_x_smem(eb, nx, c) > 227 * 1024 && c.x_lines > 8) {
+    if (sweep_x_smem(eb, nx, c) > lim && c.x_lines > 8) {
       c.x_lines /= 2;
       changed = true;
     }
-    if ((sweep_yz_smem(eb, ny, c) > 227 * 1024 || sweep_yz_smem(eb, nz, c) > 227 * 1024) && c.yz_tile > min_tile) {
+    if ((sweep_yz_smem(eb, ny, c) > lim || sweep_yz_smem(eb, nz, c) > lim) &&
+        c.yz_tile > min_tile) {
       c.yz_tile /= 2;
       changed = true;
     }
@@ -253,46 +252,73 @@ bool pick_config(int eb, int nx, int ny, int nz, SweepConfig* cfg) {
   return true;
 }
 
+// Coefficient storage of one precision: sizes of the DR/CU rows and the
+// host-side packing (padding entries are neutral: a unit denominator and a
+// -0 upper diagonal).
+size_t coef_bytes(const bfvm_ctx* c, size_t* dr_off, size_t* cu_off) {
+  const size_t S = c->S;
+  const size_t dr_sz = c->prec == BFVM_FP64 ? sizeof(double2) : sizeof(float2);
+  const size_t cu_sz = c->prec == BFVM_FP64 ? sizeof(double) : sizeof(float2);
+  const int n_axis[3] = {c->nx, c->ny, c->nz};
+  size_t o = 0;
+  for (int a = 0; a < 3; ++a) {
+    const size_t rows = S * coef_pad(n_axis[a]);
+    dr_off[a] = o;
+    o += rows * dr_sz;
+    o = (o + 255) & ~size_t(255);
+    cu_off[a] = o;
+    o += rows * cu_sz;
+    o = (o + 255) & ~size_t(255);
+  }
+  return o;
+}
+
 int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
   const int S = c->S;
   const int n_axis[3] = {c->nx, c->ny, c->nz};
-  const size_t tot = static_cast<size_t>(S) * (c->nx + c->ny + c->nz);
-  std::vector<double> denom(tot), rcp64(tot), cup64(tot), c1(S);
-  size_t off = 0;
+  size_t dr_off[3], cu_off[3];
+  const size_t bytes = coef_bytes(c, dr_off, cu_off);
+  std::vector<unsigned char> host(bytes, 0);
+  std::vector<double> c1(S);
+  auto split = [](double x, float* hi, float* lo) {
+    *hi = static_cast<float>(x);
+    *lo = static_cast<float>(x - static_cast<double>(*hi));
+  };
   for (int ax = 0; ax < 3; ++ax) {
     const int n = n_axis[ax];
+    const int np = coef_pad(n);
     std::vector<double> dn(static_cast<size_t>(n) * S), cu(static_cast<size_t>(n) * S);
     thomas_axis_host(n, S, D, decay, c->dt, c->dx, dn.data(), cu.data(), c1.data());
     for (int s = 0; s < S; ++s)
-      for (int i = 0; i < n; ++i) {
-        const double d = dn[static_cast<size_t>(i) * S + s];
-        denom[off + static_cast<size_t>(s) * n + i] = d;
-        rcp64[off + static_cast<size_t>(s) * n + i] = 1.0 / d;
-        cup64[off + static_cast<size_t>(s) * n + i] = cu[static_cast<size_t>(i) * S + s];
+      for (int i = 0; i < np; ++i) {
+        const size_t q = static_cast<size_t>(s) * np + i;
+        const bool in = i < n;
+        const double d = in ? dn[static_cast<size_t>(i) * S + s] : 1.0;
+        const double r = 1.0 / d;  // RN(1/d), IEEE double division
+        const double u = in ? cu[static_cast<size_t>(i) * S + s] : -0.0;
+        if (c->prec == BFVM_FP64) {
+          reinterpret_cast<double2*>(host.data() + dr_off[ax])[q] = make_double2(d, r);
+          reinterpret_cast<double*>(host.data() + cu_off[ax])[q] = u;
+        } else {
+          float2 rr, uu;
+          split(r, &rr.x, &rr.y);
+          split(u, &uu.x, &uu.y);
+          reinterpret_cast<float2*>(host.data() + dr_off[ax])[q] = rr;
+          reinterpret_cast<float2*>(host.data() + cu_off[ax])[q] = uu;
+        }
       }
-    off += static_cast<size_t>(S) * n;
   }
-  BFVM_CUDA(cudaMemcpy(c->d_denom, denom.data(), tot * 8, cudaMemcpyHostToDevice));
+  BFVM_CUDA(cudaMemcpy(c->d_coef, host.data(), bytes, cudaMemcpyHostToDevice));
+  for (int a = 0; a < 3; ++a) {
+    c->dr_off[a] = dr_off[a];
+    c->cu_off[a] = cu_off[a];
+  }
   if (c->prec == BFVM_FP64) {
-    BFVM_CUDA(cudaMemcpy(c->d_rcp, rcp64.data(), tot * 8, cudaMemcpyHostToDevice));
-    BFVM_CUDA(cudaMemcpy(c->d_cup, cup64.data(), tot * 8, cudaMemcpyHostToDevice));
-    BFVM_CUDA(cudaMemcpy(c->d_c1, c1.data(), S * 8, cudaMemcpyHostToDevice));
+    BFVM_CUDA(cudaMemcpy(c->d_c1, c1.data(), S * sizeof(double), cudaMemcpyHostToDevice));
   } else {
-    // FP32 form: each FP64 coefficient rounded once into a float pair
-    // hi = RN32(x), lo = RN32(x - hi); arrays are [hi | lo].
-    std::vector<float> r32(2 * tot), c32(2 * tot), k32(2 * S);
-    auto split = [](double x, float* hi, float* lo) {
-      *hi = static_cast<float>(x);
-      *lo = static_cast<float>(x - static_cast<double>(*hi));
-    };
-    for (size_t q = 0; q < tot; ++q) {
-      split(rcp64[q], &r32[q], &r32[tot + q]);
-      split(cup64[q], &c32[q], &c32[tot + q]);
-    }
-    for (int s = 0; s < S; ++s) split(c1[s], &k32[s], &k32[S + s]);
-    BFVM_CUDA(cudaMemcpy(c->d_rcp, r32.data(), 2 * tot * 4, cudaMemcpyHostToDevice));
-    BFVM_CUDA(cudaMemcpy(c->d_cup, c32.data(), 2 * tot * 4, cudaMemcpyHostToDevice));
-    BFVM_CUDA(cudaMemcpy(c->d_c1, k32.data(), 2 * S * 4, cudaMemcpyHostToDevice));
+    std::vector<float2> k(S);
+    for (int s = 0; s < S; ++s) split(c1[s], &k[s].x, &k[s].y);
+    BFVM_CUDA(cudaMemcpy(c->d_c1, k.data(), S * sizeof(float2), cudaMemcpyHostToDevice));
   }
   // thomas_constant2 = decay; *= dt; /= 3 (BioFVM_solvers.cpp:208-209)
   c->c2.assign(S, 0.0);
@@ -449,14 +475,11 @@ int bfvm_create(const bfvm_config* cfg, bfvm_ctx** out) {
   c->stream = c->own_stream;
   const size_t S = c->S;
   c->field_bytes = static_cast<size_t>(c->nxp) * c->ny * c->nz * S * c->eb;
-  const size_t tot = S * (c->nx + c->ny + c->nz);
   int rc = BFVM_OK;
   if (rc == BFVM_OK) rc = dalloc(c, &c->f, c->field_bytes);
-  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_denom), tot * 8);
-  const size_t parts = c->prec == BFVM_FP32 ? 2 : 1;  // FP32 keeps hi and lo parts
-  if (rc == BFVM_OK) rc = dalloc(c, &c->d_rcp, parts * tot * c->eb);
-  if (rc == BFVM_OK) rc = dalloc(c, &c->d_cup, parts * tot * c->eb);
-  if (rc == BFVM_OK) rc = dalloc(c, &c->d_c1, parts * S * c->eb);
+  size_t dr_tmp[3], cu_tmp[3];
+  if (rc == BFVM_OK) rc = dalloc(c, &c->d_coef, coef_bytes(c, dr_tmp, cu_tmp));
+  if (rc == BFVM_OK) rc = dalloc(c, &c->d_c1, S * 16);
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_off), S * sizeof(double));
   if (rc == BFVM_OK) rc = dalloc(c, &c->d_shift, S * sizeof(float));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_active), S * sizeof(int));
@@ -493,9 +516,7 @@ int bfvm_destroy(bfvm_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_agents(c);
   dfree(c->f);
-  dfree(c->d_denom);
-  dfree(c->d_rcp);
-  dfree(c->d_cup);
+  dfree(c->d_coef);
   dfree(c->d_c1);
   dfree(c->d_off);
   dfree(c->d_shift);

@@ -23,26 +23,46 @@ namespace bfvm {
 
 constexpr int kMaxSubstrates = 64;
 
-// Thomas coefficients of one axis for all substrates, index [s][i].
-// The FP32 form keeps each FP64 coefficient as a float pair hi + lo
-// (hi = RN32(x), lo = RN32(x - hi)), so the fixed coefficients carry no
-// FP32 rounding bias from step to step; the FP64 form leaves the lo arrays
-// null.
+// Coefficient element types per precision.
+//   FP64: DR = {denom_i, RN(1/denom_i)} (one 16-byte load per element),
+//         CU = modified upper diagonal c_i, C1 = dt*D/dx^2.
+//   FP32: every FP64 coefficient x is kept as a float pair {hi, lo},
+//         hi = RN32(x), lo = RN32(x - hi), so fixed coefficients carry no
+//         FP32 rounding bias from step to step: DR = 1/denom_i, CU = c_i,
+//         C1 = c1, each as {hi, lo}.
+template <typename T>
+struct Coef;
+template <>
+struct Coef<double> {
+  using DR = double2;
+  using CU = double;
+  using C1 = double;
+};
+template <>
+struct Coef<float> {
+  using DR = float2;
+  using CU = float2;
+  using C1 = float2;
+};
+
+// Thomas coefficients of one axis for all substrates: rows [S][npad], npad =
+// the line length rounded up to 32, padded with neutral entries so batches
+// may read past the end of a line without bounds checks.
 template <typename T>
 struct AxisCoefs {
-  const double* denom;  // modified diagonal (FP64 always)
-  const T* rcp;         // RN(1/denom) in T (hi part in FP32)
-  const T* cup;         // modified upper diagonal in T (hi part in FP32)
-  const T* rcp_lo;      // FP32 only: low parts
-  const T* cup_lo;
+  const typename Coef<T>::DR* dr;
+  const typename Coef<T>::CU* cu;
+  int npad;
 };
+
+// Rows of coefficient storage per line of n voxels.
+inline int coef_pad(int n) { return (n + 31) / 32 * 32; }
 
 template <typename T>
 struct SweepParams {
   T* f;                  // field base
   int nx, ny, nz, S, nxp;
-  const T* c1;           // [S] dt*D/dx^2 (hi part in FP32)
-  const T* c1_lo;        // [S] FP32 only: low part of c1
+  const typename Coef<T>::C1* c1;  // [S] dt*D/dx^2
   // FP32 only: the field holds rho - off[s]; each sweep's right-hand side is
   // shifted by shift[s] = RN32(dt*decay/3 * off[s]) to match (the constant
   // off[s] solves the zero-flux system with factor 1 + dt*decay/3).
@@ -66,18 +86,19 @@ struct SweepParams {
   int* status;           // device status word
 };
 
-// Kernel launch configuration chosen by the host (autotuned per shape).
+// Launch configuration of the sweeps (chosen by the host, tunable).  One CTA
+// (one warp) owns one tile of lines and stages them whole in shared memory.
 struct SweepConfig {
   int x_lines = 32;   // lines per CTA in the x sweep (multiple of 8, <= 256)
-  int yz_tile = 32;   // consecutive x per CTA in the y/z sweeps (multiple of 16 fp64 / 32 fp32... see launcher)
-  int yz_chunk = 32;  // rows per TMA box along the line in the y/z sweeps (<= 256)
+  int yz_tile = 32;   // consecutive x per CTA in the y/z sweeps (whole 128-byte rows)
+  int yz_chunk = 32;  // target rows per TMA box along the line in the y/z sweeps (<= 256)
 };
 
 // The three tensor maps the sweeps use, built once per context.
 struct FieldMaps {
-  CUtensorMap x;   // box {16 or 32 (128 B), x_lines, 1, 1}, 128B swizzle
-  CUtensorMap y;   // box {yz_tile, yz_chunk, 1, 1}
-  CUtensorMap z;   // box {yz_tile, 1, yz_chunk, 1}
+  CUtensorMap x;   // box {128 bytes of x, x_lines, 1, 1}, 128B swizzle
+  CUtensorMap y;   // box {yz_tile, chunk rows, 1, 1}
+  CUtensorMap z;   // box {yz_tile, 1, chunk rows, 1}
 };
 
 // Host-side count of this library's kernel launches (bfvm_kernel_launches).
@@ -93,8 +114,7 @@ cudaError_t launch_sweep_y(const FieldMaps& maps, const SweepParams<T>& p, const
 template <typename T>
 cudaError_t launch_sweep_z(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st);
 
-// Shared-memory bytes one CTA of each sweep needs (0 if the shape is not
-// supported by that configuration).
+// Shared-memory bytes one CTA of each sweep needs.
 size_t sweep_x_smem(int elem_bytes, int nx, const SweepConfig& cfg);
 size_t sweep_yz_smem(int elem_bytes, int n_line, const SweepConfig& cfg);
 

@@ -84,6 +84,15 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, uint32_t sr
       : "memory");
 }
 
+// 1-D bulk copy global -> this CTA's shared memory (no multicast); both
+// addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
 __device__ __forceinline__ void tma_store_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 
 // Wait until every committed bulk store has finished READING shared memory.
@@ -105,19 +114,23 @@ __device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {
 // RN(q0 + e*r) is the correctly rounded quotient (P. Markstein, "Computation
 // of elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
 // Dev. 34(1), 1990; Theorem 4.x in Muller et al., Handbook of Floating-Point
-// Arithmetic).  The theorem needs the remainder not to underflow; for a
-// nonzero |t| < 2^-960 the plain IEEE division is used instead (never on
-// realistic densities, but it keeps the result exact for every input).  A
-// zero numerator returns q0 = t*r, which carries the sign of t as IEEE
-// division does.  The sweep denominators are all >= 1, so t*r cannot
-// overflow.
-__device__ __forceinline__ double div_exact(double t, double d, double r) {
+// Arithmetic).  The sweep denominators are all >= 1, so t*r cannot
+// overflow and the quotient has the sign of t; copysign restores the sign of
+// a zero numerator (the correction step would turn -0 into +0).  The theorem
+// needs the remainder not to underflow, which holds for |t| >= 2^-960 and
+// for t = 0: callers check div_needs_ieee(t) off the dependent chain and
+// redo the (never realistic) tiny cases with IEEE division.
+__device__ __forceinline__ double div_fast(double t, double d, double r) {
   const double q0 = t * r;
   const double e = __fma_rn(-q0, d, t);
-  double q = __fma_rn(e, r, q0);
-  q = (t == 0.0) ? q0 : q;
-  if (fabs(t) < 0x1p-960 && t != 0.0) q = t / d;
-  return q;
+  return copysign(__fma_rn(e, r, q0), t);
+}
+
+__device__ __forceinline__ bool div_needs_ieee(double t) { return fabs(t) < 0x1p-960 && t != 0.0; }
+
+// Exact t / d for every input (used outside the hot loops).
+__device__ __forceinline__ double div_exact(double t, double d, double r) {
+  return div_needs_ieee(t) ? t / d : div_fast(t, d, r);
 }
 
 }  // namespace bfvm

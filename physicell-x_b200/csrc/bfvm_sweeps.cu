@@ -23,9 +23,13 @@
 //            each step of the recurrence reads one contiguous shared-memory row.
 //
 // The recurrence is serial per line, so its speed is the latency of the
-// dependent FP64 chain.  Every load a step needs (its staged value and its
-// coefficients) is therefore issued for a whole batch of elements before the
-// chain over that batch starts; the chain itself only touches registers.
+// dependent chain: per element four FP64 operations forward (fma; Markstein
+// quotient) and one backward.  Every load a batch of elements needs is issued
+// before the chain over that batch starts, coefficient rows are padded so no
+// load needs a bounds check, and the chains start from -0.0, which makes the
+// first element need no special case (fma(c1, -0, v) == v and
+// fma(-c, -0, y) == y exactly, as c1 >= 0 and the modified upper diagonal
+// c <= 0).
 //
 // Dirichlet pins are fused: a line lying in an activated face is written with
 // its face values; other lines get their two end voxels pinned after the
@@ -37,10 +41,13 @@
 //   forward  y_0 = p_0 / d_0;  y_i = fma(c1, y_{i-1}, p_i) / d_i
 //   backward x_i = fma(-c_i, x_{i+1}, y_i)
 //   agent    rho = ((rho + c1_a) / c2_a) + e2_a
-// with the quotient by d_i computed exactly (div_exact, Markstein's
-// correction from a precomputed RN(1/d_i)), so results equal the reference's
-// bit for bit.  The FP32 form multiplies by RN32(1/d_i) and keeps the agent
-// update in FP64.
+// The quotient uses Markstein's correction from a precomputed RN(1/d_i)
+// (div_fast), which is the correctly rounded quotient except for a numerator
+// of -0 or a nonzero numerator below 2^-960; a batch that meets either is
+// redone with IEEE division, so results equal the reference's bit for bit.
+// The FP32 form stores rho - off[s], applies the matching right-hand-side
+// shift, and keeps every coefficient as a float (hi, lo) pair; agent updates
+// stay in FP64.
 #include <climits>
 #include <type_traits>
 
@@ -52,37 +59,56 @@ namespace bfvm {
 namespace {
 
 template <typename T>
-struct Arith;
-
-template <>
-struct Arith<double> {
-  // t_i = p_i + c1*y_{i-1}, contracted as the reference's g++ build does
-  static __device__ __forceinline__ double lin(double c1, double, double yprev, double v) {
-    return __fma_rn(c1, yprev, v);
-  }
-  static __device__ __forceinline__ double div(double t, double d, double r, double) { return div_exact(t, d, r); }
-  static __device__ __forceinline__ double back(double c, double, double xnext, double y) {
-    return __fma_rn(-c, xnext, y);
-  }
-};
-
-// FP32: every fixed coefficient is a (hi, lo) float pair; the low part is
-// applied first so the pair acts as one coefficient of ~48 bits.
-template <>
-struct Arith<float> {
-  static __device__ __forceinline__ float lin(float c1h, float c1l, float yprev, float v) {
-    return __fmaf_rn(c1h, yprev, __fmaf_rn(c1l, yprev, v));
-  }
-  static __device__ __forceinline__ float div(float t, double, float rh, float rl) {
-    return __fmaf_rn(t, rh, __fmul_rn(t, rl));
-  }
-  static __device__ __forceinline__ float back(float ch, float cl, float xnext, float y) {
-    return __fmaf_rn(-ch, xnext, __fmaf_rn(-cl, xnext, y));
-  }
-};
-
-template <typename T>
 constexpr bool kF32 = sizeof(T) == 4;
+
+// Forward recurrence over B staged values; out[q] receives y_q and the
+// running value is returned.
+__device__ __forceinline__ double markstein(double t, double d, double r) {
+  const double q0 = t * r;
+  const double e = __fma_rn(-q0, d, t);
+  return __fma_rn(e, r, q0);
+}
+
+template <int B>
+__device__ __forceinline__ double forward_batch(const double (&v)[B], const double2 (&cf)[B], double c1, double,
+                                                double y, double (&out)[B]) {
+  const double y0 = y;
+  bool slow = false;
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    const double t = __fma_rn(c1, y, v[q]);
+    // off the chain: the two cases Markstein's step does not cover
+    slow |= (fabs(t) < 0x1p-960) & (__double_as_longlong(t) != 0);
+    y = markstein(t, cf[q].x, cf[q].y);
+    out[q] = y;
+  }
+  if (slow) {
+    y = y0;
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      y = __fma_rn(c1, y, v[q]) / cf[q].x;
+      out[q] = y;
+    }
+  }
+  return y;
+}
+
+template <int B>
+__device__ __forceinline__ float forward_batch(const float (&v)[B], const float2 (&cf)[B], float2 c1, float shift,
+                                               float y, float (&out)[B]) {
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    const float t = __fmaf_rn(c1.x, y, __fmaf_rn(c1.y, y, v[q] - shift));
+    y = __fmaf_rn(t, cf[q].x, __fmul_rn(t, cf[q].y));
+    out[q] = y;
+  }
+  return y;
+}
+
+__device__ __forceinline__ double back_elem(double c, double xn, double y) { return __fma_rn(-c, xn, y); }
+__device__ __forceinline__ float back_elem(float2 c, float xn, float y) {
+  return __fmaf_rn(-c.x, xn, __fmaf_rn(-c.y, xn, y));
+}
 
 // Apply every agent of voxel i (agents of this line are sorted by x index,
 // then by agent index) to the value v, in FP64, and return the result.
@@ -103,12 +129,46 @@ __device__ __forceinline__ T apply_agents(T v, int i, int& a, int aend, int& nex
   return static_cast<T>(r);
 }
 
-// Address of element e (0..W-1) of a thread's 128-byte row in a chunk staged
-// with the 128B swizzle: 16-byte unit (e/U) is stored at unit (e/U) ^ (row%8).
+// Element e (0..W-1) of a thread's 128-byte row in a chunk staged with the
+// 128B swizzle: 16-byte unit (e/U) is stored at unit (e/U) ^ (row%8).
 template <typename T>
 __device__ __forceinline__ T* swz_elem(unsigned char* row, int e, int sw) {
   constexpr int U = 16 / sizeof(T);
   return reinterpret_cast<T*>(row + (((e / U) ^ sw) << 4) + (e % U) * sizeof(T));
+}
+
+template <typename T, int W>
+__device__ __forceinline__ void load_row(const unsigned char* crow, int sw, T (&v)[W]) {
+  constexpr int U = 16 / sizeof(T);
+  using Unit = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+#pragma unroll
+  for (int u = 0; u < W / U; ++u) {
+    const Unit uv = *reinterpret_cast<const Unit*>(crow + ((u ^ sw) << 4));
+    const T* ev = reinterpret_cast<const T*>(&uv);
+#pragma unroll
+    for (int q = 0; q < U; ++q) v[u * U + q] = ev[q];
+  }
+}
+
+template <typename T, int W>
+__device__ __forceinline__ void store_row(unsigned char* crow, int sw, const T (&v)[W]) {
+  constexpr int U = 16 / sizeof(T);
+  using Unit = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+#pragma unroll
+  for (int u = 0; u < W / U; ++u) {
+    Unit uv;
+    T* ev = reinterpret_cast<T*>(&uv);
+#pragma unroll
+    for (int q = 0; q < U; ++q) ev[q] = v[u * U + q];
+    *reinterpret_cast<Unit*>(crow + ((u ^ sw) << 4)) = uv;
+  }
+}
+
+// Offset that aligns the dynamic shared-memory window to `align` bytes
+// (pointers are formed as smem_raw + offset so they stay in the shared space).
+__device__ __forceinline__ uint32_t smem_align_pad(const void* smem_raw, uint32_t align) {
+  const uint32_t a = smem_u32(smem_raw);
+  return ((a + align - 1) & ~(align - 1)) - a;
 }
 
 }  // namespace
@@ -118,17 +178,17 @@ __device__ __forceinline__ T* swz_elem(unsigned char* row, int e, int sw) {
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<T> p) {
+  using DR = typename Coef<T>::DR;
+  using CU = typename Coef<T>::CU;
   constexpr int W = 128 / sizeof(T);  // elements per 128-byte row (one TMA box width)
-  constexpr int U = 16 / sizeof(T);   // elements per 16-byte unit
-  using Unit = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
   extern __shared__ unsigned char smem_raw[];
 
   const int TL = blockDim.x;
   const int nx = p.nx, ny = p.ny, nz = p.nz, S = p.S;
   const int C = (nx + W - 1) / W;
-  const uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
   uint64_t* bars = reinterpret_cast<uint64_t*>(base);
-  unsigned char* tile = reinterpret_cast<unsigned char*>(base + ((C * 8 + 1023) & ~1023));
+  unsigned char* tile = base + ((C * 8 + 1023) & ~1023);
   const uint32_t chunk_bytes = static_cast<uint32_t>(TL) * 128u;
 
   const int t = threadIdx.x;
@@ -144,7 +204,7 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
     for (int c = 0; c < C; ++c) {
       const uint32_t bar = smem_u32(&bars[c]);
       mbar_expect_tx(bar, chunk_bytes);
-      tma_load_4d(smem_u32(tile + static_cast<size_t>(c) * chunk_bytes), &map, bar, c * W, j0, k, s);
+      tma_load_4d(smem_u32(tile + c * chunk_bytes), &map, bar, c * W, j0, k, s);
     }
   }
 
@@ -177,25 +237,23 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
     ac2 = p.ac2 + static_cast<size_t>(s) * p.n_sorted;
     ae2 = p.ae2 + static_cast<size_t>(s) * p.n_sorted;
   }
-  const double* __restrict__ dn = p.ax.denom + static_cast<size_t>(s) * nx;
-  const T* __restrict__ rc = p.ax.rcp + static_cast<size_t>(s) * nx;
-  const T* __restrict__ cu = p.ax.cup + static_cast<size_t>(s) * nx;
-  const T* __restrict__ rcl = kF32<T> ? p.ax.rcp_lo + static_cast<size_t>(s) * nx : nullptr;
-  const T* __restrict__ cul = kF32<T> ? p.ax.cup_lo + static_cast<size_t>(s) * nx : nullptr;
-  const T c1 = p.c1[s];
-  const T c1l = kF32<T> ? p.c1_lo[s] : T(0);
+  const DR* __restrict__ drp = p.ax.dr + static_cast<size_t>(s) * p.ax.npad;
+  const CU* __restrict__ cup = p.ax.cu + static_cast<size_t>(s) * p.ax.npad;
+  const typename Coef<T>::C1 c1 = p.c1[s];
   const T shift = kF32<T> ? p.shift[s] : T(0);
 
-  unsigned char* row = tile + static_cast<size_t>(t) * 128;
+  unsigned char* row = tile + t * 128;
   const int sw = t & 7;
   bool ok = true;
 
-  // Forward elimination, one chunk at a time as the TMA boxes land.
-  T yprev = T(0);
+  // Forward elimination, one chunk at a time as the TMA boxes land.  Values
+  // past nx in the last chunk are TMA fill; the chain may run over them
+  // harmlessly (those results are never stored to the field).
+  T y = T(-0.0);
   for (int c = 0; c < C; ++c) {
     if (ok) ok = mbar_wait(smem_u32(&bars[c]), 0);
     if (face) continue;
-    unsigned char* crow = row + static_cast<size_t>(c) * chunk_bytes;
+    unsigned char* crow = row + c * chunk_bytes;
     const int i0 = c * W;
     const int iend = min(nx, i0 + W);
     // Sources, then the pin before the sweep, on the staged row.
@@ -207,47 +265,13 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
       if (i0 == 0) *swz_elem<T>(crow, 0, sw) = x0v;
       if (nx - 1 < iend) *swz_elem<T>(crow, nx - 1 - i0, sw) = x1v;
     }
-    T v[W];
-    double d[W];
-    T r[W], rl[W];
+    T v[W], out[W];
+    DR cf[W];
+    load_row<T, W>(crow, sw, v);
 #pragma unroll
-    for (int u = 0; u < W / U; ++u) {
-      const Unit uv = *reinterpret_cast<const Unit*>(crow + ((u ^ sw) << 4));
-      const T* ev = reinterpret_cast<const T*>(&uv);
-#pragma unroll
-      for (int q = 0; q < U; ++q) v[u * U + q] = ev[q];
-    }
-#pragma unroll
-    for (int q = 0; q < W; ++q) {
-      const int i = min(i0 + q, nx - 1);
-      r[q] = __ldg(rc + i);
-      if constexpr (kF32<T>) {
-        rl[q] = __ldg(rcl + i);
-        d[q] = 0.0;
-      } else {
-        d[q] = __ldg(dn + i);
-        rl[q] = T(0);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < W; ++q) {
-      const int i = i0 + q;
-      if (i < nx) {
-        const T vq = kF32<T> ? v[q] - shift : v[q];
-        const T tt = (i == 0) ? vq : Arith<T>::lin(c1, c1l, yprev, vq);
-        const T y = Arith<T>::div(tt, d[q], r[q], rl[q]);
-        v[q] = y;
-        yprev = y;
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < W / U; ++u) {
-      Unit uv;
-      T* ev = reinterpret_cast<T*>(&uv);
-#pragma unroll
-      for (int q = 0; q < U; ++q) ev[q] = v[u * U + q];
-      *reinterpret_cast<Unit*>(crow + ((u ^ sw) << 4)) = uv;
-    }
+    for (int q = 0; q < W; ++q) cf[q] = __ldg(drp + i0 + q);
+    y = forward_batch<W>(v, cf, c1, shift, y, out);
+    store_row<T, W>(crow, sw, out);
   }
   if (__syncthreads_or(!ok)) {
     if (t == 0) atomicExch(p.status, kDevTimeout);
@@ -255,46 +279,36 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
   }
 
   // Back substitution, last chunk first; each finished chunk is stored at once.
-  T xnext = T(0);
+  T xn = T(-0.0);
   for (int c = C - 1; c >= 0; --c) {
-    unsigned char* crow = row + static_cast<size_t>(c) * chunk_bytes;
+    unsigned char* crow = row + c * chunk_bytes;
     const int i0 = c * W;
     if (face) {
       for (int q = 0; q < W; ++q)
         if (i0 + q < nx) *swz_elem<T>(crow, q, sw) = static_cast<T>(fv != nullptr ? fv[i0 + q] - off : 0.0);
     } else {
       T v[W];
-      T cw[W], cwl[W];
+      CU cw[W];
+      load_row<T, W>(crow, sw, v);
 #pragma unroll
-      for (int u = 0; u < W / U; ++u) {
-        const Unit uv = *reinterpret_cast<const Unit*>(crow + ((u ^ sw) << 4));
-        const T* ev = reinterpret_cast<const T*>(&uv);
+      for (int q = 0; q < W; ++q) cw[q] = __ldg(cup + i0 + q);
+      if (i0 + W > nx) {
+        // the line ends inside this chunk: skip the fill past nx
 #pragma unroll
-        for (int q = 0; q < U; ++q) v[u * U + q] = ev[q];
-      }
+        for (int q = W - 1; q >= 0; --q) {
+          if (i0 + q < nx) {
+            xn = back_elem(cw[q], xn, v[q]);
+            v[q] = xn;
+          }
+        }
+      } else {
 #pragma unroll
-      for (int q = 0; q < W; ++q) {
-        const int i = min(i0 + q, nx - 1);
-        cw[q] = __ldg(cu + i);
-        cwl[q] = kF32<T> ? __ldg(cul + i) : T(0);
-      }
-#pragma unroll
-      for (int q = W - 1; q >= 0; --q) {
-        const int i = i0 + q;
-        if (i < nx) {
-          const T x = (i == nx - 1) ? v[q] : Arith<T>::back(cw[q], cwl[q], xnext, v[q]);
-          xnext = x;
-          v[q] = x;
+        for (int q = W - 1; q >= 0; --q) {
+          xn = back_elem(cw[q], xn, v[q]);
+          v[q] = xn;
         }
       }
-#pragma unroll
-      for (int u = 0; u < W / U; ++u) {
-        Unit uv;
-        T* ev = reinterpret_cast<T*>(&uv);
-#pragma unroll
-        for (int q = 0; q < U; ++q) ev[q] = v[u * U + q];
-        *reinterpret_cast<Unit*>(crow + ((u ^ sw) << 4)) = uv;
-      }
+      store_row<T, W>(crow, sw, v);
       if (act) {
         if (i0 == 0) *swz_elem<T>(crow, 0, sw) = x0v;
         if (nx - 1 < i0 + W) *swz_elem<T>(crow, nx - 1 - i0, sw) = x1v;
@@ -303,7 +317,7 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
     fence_async_smem();
     __syncthreads();
     if (t == 0) {
-      tma_store_4d(&map, smem_u32(tile + static_cast<size_t>(c) * chunk_bytes), c * W, j0, k, s);
+      tma_store_4d(&map, smem_u32(tile + c * chunk_bytes), c * W, j0, k, s);
       tma_store_commit();
     }
   }
@@ -313,16 +327,20 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
 // ---------------------------------------------------------------------------
 // y and z sweeps
 // ---------------------------------------------------------------------------
+constexpr int kRowBatch = 16;  // rows staged in registers per batch of the recurrence
+
 template <typename T, int AXIS>
 __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<T> p,
                                                        int CH) {
-  constexpr int R = 16;  // rows staged in registers per batch of the recurrence
+  using DR = typename Coef<T>::DR;
+  using CU = typename Coef<T>::CU;
+  constexpr int R = kRowBatch;
   extern __shared__ unsigned char smem_raw[];
   const int TI = blockDim.x;
   const int nx = p.nx, ny = p.ny, nz = p.nz, S = p.S;
   const int n = (AXIS == 1) ? ny : nz;
   const int C = (n + CH - 1) / CH;
-  const uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127);
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 128);
   uint64_t* bars = reinterpret_cast<uint64_t*>(base);
   T* tile = reinterpret_cast<T*>(base + ((C * 8 + 127) & ~127));
   const uint32_t chunk_bytes = static_cast<uint32_t>(CH) * TI * sizeof(T);
@@ -340,7 +358,7 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
     for (int c = 0; c < C; ++c) {
       const uint32_t bar = smem_u32(&bars[c]);
       mbar_expect_tx(bar, chunk_bytes);
-      T* dst = tile + static_cast<size_t>(c) * CH * TI;
+      T* dst = tile + c * CH * TI;
       if (AXIS == 1)
         tma_load_4d(smem_u32(dst), &map, bar, i0, c * CH, m, s);
       else
@@ -353,7 +371,7 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
   const bool act = p.active[s] != 0;
   bool face;
   const double* fv = nullptr;  // face-line values: fv[r * fstride]
-  size_t fstride = 1;
+  int fstride = 1;
   const double off = kF32<T> ? p.off[s] : 0.0;
   T e0v = T(0), e1v = T(0);  // pinned values at the two ends of the line
   if (AXIS == 1) {
@@ -390,95 +408,102 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
     }
   }
   const AxisCoefs<T>& ac = (AXIS == 1) ? p.ay : p.az;
-  const double* __restrict__ dn = ac.denom + static_cast<size_t>(s) * n;
-  const T* __restrict__ rc = ac.rcp + static_cast<size_t>(s) * n;
-  const T* __restrict__ cu = ac.cup + static_cast<size_t>(s) * n;
-  const T* __restrict__ rcl = kF32<T> ? ac.rcp_lo + static_cast<size_t>(s) * n : nullptr;
-  const T* __restrict__ cul = kF32<T> ? ac.cup_lo + static_cast<size_t>(s) * n : nullptr;
-  const T c1 = p.c1[s];
-  const T c1l = kF32<T> ? p.c1_lo[s] : T(0);
+  const DR* __restrict__ drp = ac.dr + static_cast<size_t>(s) * ac.npad;
+  const CU* __restrict__ cup = ac.cu + static_cast<size_t>(s) * ac.npad;
+  const typename Coef<T>::C1 c1 = p.c1[s];
   const T shift = kF32<T> ? p.shift[s] : T(0);
   T* col = tile + t;
   bool ok = true;
+  int waited = 0;  // chunks whose TMA load this thread has waited for
 
-  T yprev = T(0);
-  for (int c = 0; c < C; ++c) {
-    if (ok) ok = mbar_wait(smem_u32(&bars[c]), 0);
-    if (face) continue;
-    const int r1 = min(n, (c + 1) * CH);
-    for (int rb = c * CH; rb < r1; rb += R) {
-      T v[R];
-      double d[R];
-      T r[R], rl[R];
-#pragma unroll
-      for (int q = 0; q < R; ++q) {
-        const int rr = min(rb + q, r1 - 1);
-        v[q] = col[static_cast<size_t>(rr) * TI];
-        r[q] = __ldg(rc + rr);
-        if constexpr (kF32<T>) {
-          rl[q] = __ldg(rcl + rr);
-          d[q] = 0.0;
-        } else {
-          d[q] = __ldg(dn + rr);
-          rl[q] = T(0);
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < R; ++q) {
-        const int rr = rb + q;
-        if (rr < r1) {
-          const T vq = kF32<T> ? v[q] - shift : v[q];
-          const T tt = (rr == 0) ? vq : Arith<T>::lin(c1, c1l, yprev, vq);
-          const T y = Arith<T>::div(tt, d[q], r[q], rl[q]);
-          col[static_cast<size_t>(rr) * TI] = y;
-          yprev = y;
-        }
-      }
+  // Forward elimination in batches of R rows; a batch first waits for the
+  // chunks that cover it.  The tile holds a whole number of batches, so the
+  // last batch may read rows past n (TMA fill or unused rows): those results
+  // are never stored to the field.
+  T y = T(-0.0);
+  for (int rb = 0; rb < n; rb += R) {
+    const int need = min(C, (rb + R + CH - 1) / CH);
+    while (waited < need) {
+      if (ok) ok = mbar_wait(smem_u32(&bars[waited]), 0);
+      ++waited;
     }
+    if (face) continue;
+    T v[R], out[R];
+    DR cf[R];
+    T* cb = col + rb * TI;
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      v[q] = cb[q * TI];
+      cf[q] = __ldg(drp + rb + q);
+    }
+    y = forward_batch<R>(v, cf, c1, shift, y, out);
+#pragma unroll
+    for (int q = 0; q < R; ++q) cb[q * TI] = out[q];
+  }
+  while (waited < C) {
+    if (ok) ok = mbar_wait(smem_u32(&bars[waited]), 0);
+    ++waited;
   }
   if (__syncthreads_or(!ok)) {
     if (t == 0) atomicExch(p.status, kDevTimeout);
     return;
   }
 
-  T xnext = T(0);
-  for (int c = C - 1; c >= 0; --c) {
-    const int r0 = c * CH;
-    const int r1 = min(n, (c + 1) * CH);
+  // Back substitution in batches of R rows from the end; chunk c is stored
+  // once every row from its start on is final.
+  T xn = T(-0.0);
+  int next_store = C - 1;
+  const int last_b = ((n - 1) / R) * R;
+  for (int rb = last_b; rb >= 0; rb -= R) {
+    T* cb = col + rb * TI;
     if (face) {
-      for (int rr = r0; rr < r1; ++rr)
-        col[static_cast<size_t>(rr) * TI] = static_cast<T>(fv != nullptr ? fv[rr * fstride] - off : 0.0);
+      for (int rr = min(n - 1, rb + R - 1); rr >= rb; --rr)
+        col[rr * TI] = static_cast<T>(fv != nullptr ? fv[rr * fstride] - off : 0.0);
     } else {
-      for (int rb = r1 - 1; rb >= r0; rb -= R) {
-        T v[R];
-        T cw[R], cwl[R];
+      T v[R];
+      CU cw[R];
 #pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const int rr = max(rb - q, r0);
-          v[q] = col[static_cast<size_t>(rr) * TI];
-          cw[q] = __ldg(cu + rr);
-          cwl[q] = kF32<T> ? __ldg(cul + rr) : T(0);
-        }
+      for (int q = 0; q < R; ++q) {
+        v[q] = cb[q * TI];
+        cw[q] = __ldg(cup + rb + q);
+      }
+      if (rb == last_b) {
 #pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const int rr = rb - q;
-          if (rr >= r0) {
-            const T x = (rr == n - 1) ? v[q] : Arith<T>::back(cw[q], cwl[q], xnext, v[q]);
-            xnext = x;
-            col[static_cast<size_t>(rr) * TI] = (act && (rr == 0 || rr == n - 1)) ? (rr == 0 ? e0v : e1v) : x;
+        for (int q = R - 1; q >= 0; --q) {
+          if (rb + q < n) {
+            xn = back_elem(cw[q], xn, v[q]);
+            v[q] = xn;
           }
         }
+      } else {
+#pragma unroll
+        for (int q = R - 1; q >= 0; --q) {
+          xn = back_elem(cw[q], xn, v[q]);
+          v[q] = xn;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) cb[q * TI] = v[q];
+      if (act) {
+        if (rb == 0) col[0] = e0v;
+        if (rb == last_b) col[(n - 1) * TI] = e1v;
       }
     }
-    fence_async_smem();
-    __syncthreads();
-    if (t == 0) {
-      const uint32_t src = smem_u32(tile + static_cast<size_t>(c) * CH * TI);
-      if (AXIS == 1)
-        tma_store_4d(&map, src, i0, c * CH, m, s);
-      else
-        tma_store_4d(&map, src, i0, m, c * CH, s);
-      tma_store_commit();
+    // store every chunk whose rows are now all final (uniform across the CTA)
+    if (next_store >= 0 && next_store * CH >= rb) {
+      fence_async_smem();
+      __syncthreads();
+      if (t == 0) {
+        for (int c = next_store; c >= 0 && c * CH >= rb; --c) {
+          const uint32_t src = smem_u32(tile + c * CH * TI);
+          if (AXIS == 1)
+            tma_store_4d(&map, src, i0, c * CH, m, s);
+          else
+            tma_store_4d(&map, src, i0, m, c * CH, s);
+        }
+        tma_store_commit();
+      }
+      while (next_store >= 0 && next_store * CH >= rb) --next_store;
     }
   }
   if (t == 0) tma_store_wait_read();
@@ -498,11 +523,13 @@ static int yz_chunk_rows(int n, int target) {
   return (n + C - 1) / C;
 }
 
+// The y/z tile holds a whole number of register batches (kRowBatch rows) so
+// the last batch of a line never reads outside the tile.
 size_t sweep_yz_smem(int elem_bytes, int n_line, const SweepConfig& cfg) {
   const int CH = yz_chunk_rows(n_line, cfg.yz_chunk);
   const int C = (n_line + CH - 1) / CH;
-  return 128 + ((static_cast<size_t>(C) * 8 + 127) & ~size_t(127)) +
-         static_cast<size_t>(C) * CH * cfg.yz_tile * elem_bytes;
+  const size_t rows = (static_cast<size_t>(C) * CH + kRowBatch - 1) / kRowBatch * kRowBatch;
+  return 128 + ((static_cast<size_t>(C) * 8 + 127) & ~size_t(127)) + rows * cfg.yz_tile * elem_bytes;
 }
 
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {

@@ -161,7 +161,7 @@ def test_inactive_and_outside_agents_are_skipped():
 def test_runs_are_deterministic_and_launch_shape_independent():
     wl = W.small_random(35, nx=70, ny=45, nz=90, S=2, n_agents=3000, steps=3, agent_mode="gauss")
     outs = []
-    for launch in (None, (8, 16, 7), (64, 64, 64), (32, 32, 256)):
+    for launch in (None, (8, 16, 7), (64, 64, 64), (32, 32, 256), (16, 32, 40)):
         me = Microenvironment.from_workload(wl)
         if launch:
             me.set_launch(*launch)

@@ -198,6 +198,42 @@ int bfvm_timing_read(bfvm_ctx* ctx, double* ms_xyz, int* steps);
 
 const char* bfvm_status_string(int status);
 
+/* ---- batched engine --------------------------------------------------------
+ * Many resident solves of different grids and substrate counts advanced
+ * together: each LOD step is one fused launch holding the x, y and z sweeps
+ * of every member (per-member dependency counters order them) or, by
+ * schedule, one launch per sweep over every member; runs of steps replay a
+ * captured CUDA graph.  Members keep their own state and API
+ * (upload, agents, download); each gives the same result, bit for bit, as
+ * when stepped alone.  No reference counterpart: PhysiCell parameter sweeps
+ * run one process per parameter set (beta/params_run.py). */
+typedef struct bfvm_batch bfvm_batch;
+
+int bfvm_batch_create(int precision, int device, bfvm_batch** out);
+int bfvm_batch_destroy(bfvm_batch* batch);
+/* Add / remove a member (same precision and device as the batch).  A solve
+ * may belong to one batch; removal orders its later work after the batch's. */
+int bfvm_batch_add(bfvm_batch* batch, bfvm_ctx* ctx);
+int bfvm_batch_remove(bfvm_batch* batch, bfvm_ctx* ctx);
+int bfvm_batch_size(bfvm_batch* batch);
+/* nsteps LOD steps of every member (flags as for bfvm_step). */
+int bfvm_batch_step(bfvm_batch* batch, int nsteps, int flags);
+int bfvm_batch_synchronize(bfvm_batch* batch);
+void* bfvm_batch_stream(bfvm_batch* batch);
+/* Schedule of a step.  mode 0: one fused persistent launch per step (tiles
+ * of every member and sweep from one ordered work list, per-member
+ * dependency counters); mode 1: three launches per step (x, y, z), each over
+ * the tiles of every member.  yz_chunk: rows per TMA box in the y/z sweeps;
+ * order (mode 0): 0 members as added, 1 largest first; ctas_per_sm (mode 0):
+ * 0 = as many as fit; graph_steps: steps per captured CUDA graph. */
+int bfvm_batch_set_schedule(bfvm_batch* batch, int mode, int yz_chunk, int order, int ctas_per_sm, int graph_steps);
+int bfvm_batch_get_schedule(bfvm_batch* batch, int* mode, int* yz_chunk, int* order, int* ctas_per_sm,
+                            int* graph_steps);
+/* Time trial_steps fused steps under each candidate schedule, keep the
+ * fastest, and report its ms per step.  Member fields are restored after
+ * the trials. */
+int bfvm_batch_autotune(bfvm_batch* batch, int flags, int trial_steps, double* best_ms_per_step);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,17 @@ _SIGS = {
     "bfvm_timing_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_timing_read": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
     "bfvm_status_string": (C.c_char_p, [C.c_int]),
+    "bfvm_batch_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "bfvm_batch_destroy": (C.c_int, [C.c_void_p]),
+    "bfvm_batch_add": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bfvm_batch_remove": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bfvm_batch_size": (C.c_int, [C.c_void_p]),
+    "bfvm_batch_step": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "bfvm_batch_synchronize": (C.c_int, [C.c_void_p]),
+    "bfvm_batch_stream": (C.c_void_p, [C.c_void_p]),
+    "bfvm_batch_set_schedule": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "bfvm_batch_get_schedule": (C.c_int, [C.c_void_p] + [C.POINTER(C.c_int)] * 5),
+    "bfvm_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
 }
 
 

@@ -1,0 +1,460 @@
+// bfvm_batch.cu -- the batched engine: many resident solves of different
+// shapes advanced together, one fused launch (batch_step_kernel) per LOD
+// step, with the per-step sequence captured in a CUDA graph.
+//
+// The reference has no batched form: PhysiCell parameter sweeps run one
+// process per parameter set (beta/params_run.py).  Each member here is an
+// ordinary solve (bfvm_ctx) and gives the same result, bit for bit, as when
+// it is stepped alone -- the fused kernel runs the same per-tile code.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "bfvm_ctx.h"
+
+using namespace bfvm;
+
+struct bfvm_batch {
+  int prec = BFVM_FP64;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  std::vector<bfvm_ctx*> members;
+  // device tables (capacity `cap` members)
+  int cap = 0;
+  void* d_envs = nullptr;
+  int* d_pre = nullptr;
+  int* d_counters = nullptr;
+  BatchHeader* d_hdr = nullptr;
+  int* d_status = nullptr;
+  std::vector<unsigned char> h_envs;
+  // schedule
+  int mode = 0;         // 0: one fused persistent launch per step; 1: three launches (x, y, z) per step
+  int yz_chunk = 32;
+  int order = 0;        // 0: members in insertion order; 1: largest first
+  int ctas_per_sm = 0;  // 0: as many as fit
+  int graph_steps = 16;
+  // launch shape of the current tables
+  size_t smem = 0;
+  int grid = 0;
+  int items[3] = {0, 0, 0};
+  size_t axis_smem[3] = {0, 0, 0};
+  bool built_sources = false;
+  // captured graph of graph_steps steps
+  cudaGraphExec_t gexec = nullptr;
+  size_t g_smem = 0;
+  int g_grid = 0, g_cap = 0, g_steps = 0, g_mode = -1;
+  int g_items[3] = {0, 0, 0};
+  long long launches = 0;
+};
+
+namespace {
+
+int sm_count_dev(int dev) {
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  return n;
+}
+
+void drop_graph(bfvm_batch* b) {
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  b->gexec = nullptr;
+  b->g_steps = 0;
+}
+
+int ensure_capacity(bfvm_batch* b, int n) {
+  if (n <= b->cap && b->d_envs) return BFVM_OK;
+  const int cap = std::max(n, std::max(16, 2 * b->cap));
+  const size_t env_sz = b->prec == BFVM_FP64 ? sizeof(BatchEnv<double>) : sizeof(BatchEnv<float>);
+  void *envs = nullptr, *pre = nullptr, *cnt = nullptr;
+  if (cudaMalloc(&envs, env_sz * cap) != cudaSuccess || cudaMalloc(&pre, sizeof(int) * 3 * (cap + 1)) != cudaSuccess ||
+      cudaMalloc(&cnt, sizeof(int) * (1 + 3 * cap)) != cudaSuccess) {
+    cudaGetLastError();
+    if (envs) cudaFree(envs);
+    if (pre) cudaFree(pre);
+    if (cnt) cudaFree(cnt);
+    return BFVM_ERR_OOM;
+  }
+  if (b->d_envs) cudaFree(b->d_envs);
+  if (b->d_pre) cudaFree(b->d_pre);
+  if (b->d_counters) cudaFree(b->d_counters);
+  b->d_envs = envs;
+  b->d_pre = static_cast<int*>(pre);
+  b->d_counters = static_cast<int*>(cnt);
+  b->cap = cap;
+  drop_graph(b);
+  return BFVM_OK;
+}
+
+template <typename T>
+int build_tables(bfvm_batch* b, bool sources) {
+  const int n = static_cast<int>(b->members.size());
+  int rc = ensure_capacity(b, std::max(n, 1));
+  if (rc != BFVM_OK) return rc;
+  std::vector<int> idx(n);
+  std::iota(idx.begin(), idx.end(), 0);
+  if (b->order == 1) {
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) {
+      const bfvm_ctx* x = b->members[a];
+      const bfvm_ctx* y = b->members[c];
+      return 1LL * x->nx * x->ny * x->nz * x->S > 1LL * y->nx * y->ny * y->nz * y->S;
+    });
+  }
+  std::vector<BatchEnv<T>> envs(n);
+  std::vector<int> pre(3 * (b->cap + 1), 0);
+  size_t smem = 1024 + 1024;
+  size_t axis_smem[3] = {2048, 2048, 2048};
+  int items[3] = {0, 0, 0};
+  SweepConfig cfg;
+  cfg.x_lines = kBatchTile;
+  cfg.yz_tile = kBatchTile;
+  cfg.yz_chunk = b->yz_chunk;
+  for (int q = 0; q < n; ++q) {
+    bfvm_ctx* c = b->members[idx[q]];
+    BatchEnv<T>& E = envs[q];
+    std::memset(static_cast<void*>(&E), 0, sizeof(E));
+    FieldMaps maps;
+    if (encode_field_maps(&maps, c->f, c->eb, c->nx, c->ny, c->nz, c->S, c->nxp, cfg) != 0) return BFVM_ERR_CUDA;
+    E.mx = maps.x;
+    E.my = maps.y;
+    E.mz = maps.z;
+    E.p = make_params<T>(c, sources);
+    const int chy_target = b->yz_chunk;
+    auto rows = [chy_target](int n_line) {
+      const int C = (n_line + chy_target - 1) / chy_target;
+      return (n_line + C - 1) / C;
+    };
+    E.chy = rows(c->ny);
+    E.chz = rows(c->nz);
+    E.nty = (c->ny + kBatchTile - 1) / kBatchTile;
+    E.ntx = (c->nx + kBatchTile - 1) / kBatchTile;
+    const int tiles[3] = {E.nty * c->nz * c->S, E.ntx * c->nz * c->S, E.ntx * c->ny * c->S};
+    for (int a = 0; a < 3; ++a) {
+      pre[a * (b->cap + 1) + q] = items[a];
+      items[a] += tiles[a];
+    }
+    const size_t need = batch_member_smem(c->eb, c->nx, c->ny, c->nz, b->yz_chunk);
+    if (need > 227 * 1024) return BFVM_ERR_SHAPE;
+    smem = std::max(smem, need);
+    const int n_line[3] = {c->nx, c->ny, c->nz};
+    for (int a = 0; a < 3; ++a)
+      axis_smem[a] = std::max(axis_smem[a], batch_axis_smem(c->eb, a, n_line[a], b->yz_chunk));
+  }
+  for (int a = 0; a < 3; ++a) pre[a * (b->cap + 1) + n] = items[a];
+  BatchHeader hdr;
+  hdr.n_env = n;
+  for (int a = 0; a < 3; ++a) hdr.n_items[a] = items[a];
+  if (n > 0) BFVM_CUDA(cudaMemcpyAsync(b->d_envs, envs.data(), sizeof(BatchEnv<T>) * n, cudaMemcpyHostToDevice, b->stream));
+  BFVM_CUDA(cudaMemcpyAsync(b->d_pre, pre.data(), sizeof(int) * pre.size(), cudaMemcpyHostToDevice, b->stream));
+  BFVM_CUDA(cudaMemcpyAsync(b->d_hdr, &hdr, sizeof(hdr), cudaMemcpyHostToDevice, b->stream));
+  // the host copies above must stay alive until the copies ran
+  BFVM_CUDA(cudaStreamSynchronize(b->stream));
+  int occ = 0;
+  BFVM_CUDA(batch_occupancy<T>(smem, &occ));
+  if (occ <= 0) return BFVM_ERR_SHAPE;
+  if (b->ctas_per_sm > 0 && b->ctas_per_sm < occ) occ = b->ctas_per_sm;
+  const int total = items[0] + items[1] + items[2];
+  const int grid = std::max(1, std::min(total, occ * sm_count_dev(b->device)));
+  if (smem != b->smem || grid != b->grid) drop_graph(b);
+  for (int a = 0; a < 3; ++a) {
+    if (items[a] != b->items[a] || axis_smem[a] != b->axis_smem[a]) drop_graph(b);
+    b->items[a] = items[a];
+    b->axis_smem[a] = axis_smem[a];
+  }
+  b->smem = smem;
+  b->grid = grid;
+  b->built_sources = sources;
+  return BFVM_OK;
+}
+
+// Launches of one step on the batch stream (also used while capturing).
+template <typename T>
+cudaError_t enqueue_step(bfvm_batch* b) {
+  if (b->mode == 1)
+    return launch_batch_sweeps<T>(b->d_hdr, static_cast<const BatchEnv<T>*>(b->d_envs), b->d_pre, b->cap, b->items,
+                                  b->axis_smem, b->stream);
+  cudaError_t e = cudaMemsetAsync(b->d_counters, 0, sizeof(int) * (1 + 3 * b->cap), b->stream);
+  if (e != cudaSuccess) return e;
+  return launch_batch_step<T>(b->d_hdr, static_cast<const BatchEnv<T>*>(b->d_envs), b->d_pre, b->cap, b->d_counters,
+                              b->d_status, b->grid, b->smem, b->stream);
+}
+
+int kernels_per_step(const bfvm_batch* b) {
+  if (b->mode == 0) return 1;
+  return (b->items[0] > 0) + (b->items[1] > 0) + (b->items[2] > 0);
+}
+
+template <typename T>
+int launch_one(bfvm_batch* b) {
+  BFVM_CUDA(enqueue_step<T>(b));
+  note_launches(kernels_per_step(b));
+  b->launches += kernels_per_step(b);
+  return BFVM_OK;
+}
+
+template <typename T>
+int capture_graph(bfvm_batch* b) {
+  drop_graph(b);
+  cudaGraph_t g = nullptr;
+  BFVM_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  for (int s = 0; s < b->graph_steps; ++s) {
+    const cudaError_t e2 = enqueue_step<T>(b);
+    if (e2 != cudaSuccess) {
+      cudaStreamEndCapture(b->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return BFVM_ERR_CUDA;
+    }
+  }
+  BFVM_CUDA(cudaStreamEndCapture(b->stream, &g));
+  cudaError_t e = cudaGraphInstantiate(&b->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    b->gexec = nullptr;
+    return BFVM_ERR_CUDA;
+  }
+  b->g_steps = b->graph_steps;
+  b->g_smem = b->smem;
+  b->g_grid = b->grid;
+  b->g_cap = b->cap;
+  b->g_mode = b->mode;
+  for (int a = 0; a < 3; ++a) b->g_items[a] = b->items[a];
+  return BFVM_OK;
+}
+
+// Order the batch stream after every member's pending work, and every
+// member's later work after the batch.
+int join_members(bfvm_batch* b) {
+  for (bfvm_ctx* c : b->members) {
+    if (c->stream == b->stream) continue;
+    BFVM_CUDA(cudaEventRecord(b->ev, c->stream));
+    BFVM_CUDA(cudaStreamWaitEvent(b->stream, b->ev, 0));
+  }
+  return BFVM_OK;
+}
+
+int release_members(bfvm_batch* b) {
+  BFVM_CUDA(cudaEventRecord(b->ev, b->stream));
+  for (bfvm_ctx* c : b->members)
+    if (c->stream != b->stream) BFVM_CUDA(cudaStreamWaitEvent(c->stream, b->ev, 0));
+  return BFVM_OK;
+}
+
+template <typename T>
+int step_impl(bfvm_batch* b, int nsteps, bool sources) {
+  if (b->members.empty() || nsteps == 0) return BFVM_OK;
+  int rc = join_members(b);
+  if (rc != BFVM_OK) return rc;
+  if ((rc = build_tables<T>(b, sources)) != BFVM_OK) return rc;
+  int left = nsteps;
+  if (b->graph_steps > 1 && nsteps >= b->graph_steps) {
+    if (!b->gexec || b->g_steps != b->graph_steps || b->g_smem != b->smem || b->g_grid != b->grid ||
+        b->g_cap != b->cap || b->g_mode != b->mode || b->g_items[0] != b->items[0] ||
+        b->g_items[1] != b->items[1] || b->g_items[2] != b->items[2]) {
+      if ((rc = capture_graph<T>(b)) != BFVM_OK) return rc;
+    }
+    while (left >= b->g_steps) {
+      BFVM_CUDA(cudaGraphLaunch(b->gexec, b->stream));
+      note_launches(b->g_steps * kernels_per_step(b));
+      b->launches += b->g_steps * kernels_per_step(b);
+      left -= b->g_steps;
+    }
+  }
+  for (; left > 0; --left)
+    if ((rc = launch_one<T>(b)) != BFVM_OK) return rc;
+  return release_members(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+int bfvm_batch_create(int precision, int device, bfvm_batch** out) {
+  if (!out || (precision != BFVM_FP64 && precision != BFVM_FP32)) return BFVM_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return BFVM_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= ndev) return BFVM_ERR_NODEVICE;
+  DeviceGuard g(device);
+  bfvm_batch* b = new (std::nothrow) bfvm_batch();
+  if (!b) return BFVM_ERR_OOM;
+  b->prec = precision;
+  b->device = device;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMalloc(reinterpret_cast<void**>(&b->d_hdr), sizeof(BatchHeader)) != cudaSuccess ||
+      cudaMalloc(reinterpret_cast<void**>(&b->d_status), sizeof(int)) != cudaSuccess ||
+      cudaMemset(b->d_status, 0, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    bfvm_batch_destroy(b);
+    return BFVM_ERR_CUDA;
+  }
+  *out = b;
+  return BFVM_OK;
+}
+
+int bfvm_batch_destroy(bfvm_batch* b) {
+  if (!b) return BFVM_ERR_ARG;
+  DeviceGuard g(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  drop_graph(b);
+  if (b->d_envs) cudaFree(b->d_envs);
+  if (b->d_pre) cudaFree(b->d_pre);
+  if (b->d_counters) cudaFree(b->d_counters);
+  if (b->d_hdr) cudaFree(b->d_hdr);
+  if (b->d_status) cudaFree(b->d_status);
+  if (b->ev) cudaEventDestroy(b->ev);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return BFVM_OK;
+}
+
+int bfvm_batch_add(bfvm_batch* b, bfvm_ctx* c) {
+  if (!b || !c) return BFVM_ERR_ARG;
+  if (c->prec != b->prec || c->device != b->device) return BFVM_ERR_ARG;
+  if (std::find(b->members.begin(), b->members.end(), c) != b->members.end()) return BFVM_ERR_STATE;
+  if (batch_member_smem(c->eb, c->nx, c->ny, c->nz, b->yz_chunk) > 227 * 1024) return BFVM_ERR_SHAPE;
+  b->members.push_back(c);
+  return BFVM_OK;
+}
+
+int bfvm_batch_remove(bfvm_batch* b, bfvm_ctx* c) {
+  if (!b || !c) return BFVM_ERR_ARG;
+  auto it = std::find(b->members.begin(), b->members.end(), c);
+  if (it == b->members.end()) return BFVM_ERR_STATE;
+  DeviceGuard g(b->device);
+  // the member's next work must follow whatever the batch already queued
+  BFVM_CUDA(cudaEventRecord(b->ev, b->stream));
+  BFVM_CUDA(cudaStreamWaitEvent(c->stream, b->ev, 0));
+  b->members.erase(it);
+  return BFVM_OK;
+}
+
+int bfvm_batch_size(bfvm_batch* b) { return b ? static_cast<int>(b->members.size()) : 0; }
+
+int bfvm_batch_step(bfvm_batch* b, int nsteps, int flags) {
+  if (!b || nsteps < 0) return BFVM_ERR_ARG;
+  DeviceGuard g(b->device);
+  const bool sources = (flags & BFVM_STEP_SOURCES) != 0;
+  return b->prec == BFVM_FP64 ? step_impl<double>(b, nsteps, sources) : step_impl<float>(b, nsteps, sources);
+}
+
+int bfvm_batch_synchronize(bfvm_batch* b) {
+  if (!b) return BFVM_ERR_ARG;
+  DeviceGuard g(b->device);
+  BFVM_CUDA(cudaStreamSynchronize(b->stream));
+  int st = 0;
+  BFVM_CUDA(cudaMemcpy(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  int member_rc = BFVM_OK;
+  for (bfvm_ctx* c : b->members) {
+    const int rc = bfvm_synchronize(c);
+    if (rc != BFVM_OK) member_rc = rc;
+  }
+  if (st != 0) {
+    cudaMemset(b->d_status, 0, sizeof(int));
+    return BFVM_ERR_TIMEOUT;
+  }
+  return member_rc;
+}
+
+void* bfvm_batch_stream(bfvm_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
+
+int bfvm_batch_set_schedule(bfvm_batch* b, int mode, int yz_chunk, int order, int ctas_per_sm, int graph_steps) {
+  if (!b || mode < 0 || mode > 1 || yz_chunk < 1 || yz_chunk > 256 || order < 0 || order > 1 || ctas_per_sm < 0 ||
+      graph_steps < 1 || graph_steps > 1024)
+    return BFVM_ERR_ARG;
+  for (bfvm_ctx* c : b->members)
+    if (batch_member_smem(c->eb, c->nx, c->ny, c->nz, yz_chunk) > 227 * 1024) return BFVM_ERR_SHAPE;
+  b->mode = mode;
+  b->yz_chunk = yz_chunk;
+  b->order = order;
+  b->ctas_per_sm = ctas_per_sm;
+  b->graph_steps = graph_steps;
+  drop_graph(b);
+  return BFVM_OK;
+}
+
+int bfvm_batch_get_schedule(bfvm_batch* b, int* mode, int* yz_chunk, int* order, int* ctas_per_sm,
+                            int* graph_steps) {
+  if (!b) return BFVM_ERR_ARG;
+  if (mode) *mode = b->mode;
+  if (yz_chunk) *yz_chunk = b->yz_chunk;
+  if (order) *order = b->order;
+  if (ctas_per_sm) *ctas_per_sm = b->ctas_per_sm;
+  if (graph_steps) *graph_steps = b->graph_steps;
+  return BFVM_OK;
+}
+
+// Time `trial_steps` fused steps under each candidate schedule and keep the
+// fastest.  The fields are saved before and restored after every trial, so
+// tuning leaves the solves exactly as it found them (and every schedule
+// computes the same bits anyway).
+int bfvm_batch_autotune(bfvm_batch* b, int flags, int trial_steps, double* best_ms_per_step) {
+  if (!b || trial_steps < 1) return BFVM_ERR_ARG;
+  if (b->members.empty()) return BFVM_OK;
+  DeviceGuard g(b->device);
+  int rc = bfvm_batch_synchronize(b);
+  if (rc != BFVM_OK) return rc;
+  std::vector<void*> saved(b->members.size(), nullptr);
+  for (size_t q = 0; q < b->members.size(); ++q) {
+    bfvm_ctx* c = b->members[q];
+    if (cudaMalloc(&saved[q], c->field_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      for (void* p : saved)
+        if (p) cudaFree(p);
+      return BFVM_ERR_OOM;
+    }
+    BFVM_CUDA(cudaMemcpyAsync(saved[q], c->f, c->field_bytes, cudaMemcpyDeviceToDevice, b->stream));
+  }
+  struct Cand {
+    int mode, yz_chunk, order, ctas;
+  };
+  std::vector<Cand> cands;
+  for (int ch : {16, 32, 64}) {
+    cands.push_back({1, ch, 0, 0});
+    for (int ord : {0, 1})
+      for (int ctas : {0, 8, 4}) cands.push_back({0, ch, ord, ctas});
+  }
+  const int keep_graph = b->graph_steps;
+  double best = 1e30;
+  Cand best_c{b->mode, b->yz_chunk, b->order, b->ctas_per_sm};
+  cudaEvent_t e0, e1;
+  BFVM_CUDA(cudaEventCreate(&e0));
+  BFVM_CUDA(cudaEventCreate(&e1));
+  for (const Cand& cd : cands) {
+    if (bfvm_batch_set_schedule(b, cd.mode, cd.yz_chunk, cd.order, cd.ctas, 1) != BFVM_OK) continue;
+    if ((rc = bfvm_batch_step(b, 1, flags)) != BFVM_OK) break;  // warm-up (also builds the tables)
+    cudaEventRecord(e0, b->stream);
+    if ((rc = bfvm_batch_step(b, trial_steps, flags)) != BFVM_OK) break;
+    cudaEventRecord(e1, b->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const double per = ms / trial_steps;
+    if (per < best) {
+      best = per;
+      best_c = cd;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (size_t q = 0; q < b->members.size(); ++q) {
+    bfvm_ctx* c = b->members[q];
+    cudaMemcpyAsync(c->f, saved[q], c->field_bytes, cudaMemcpyDeviceToDevice, b->stream);
+  }
+  cudaStreamSynchronize(b->stream);
+  for (void* p : saved) cudaFree(p);
+  release_members(b);
+  if (rc != BFVM_OK) return rc;
+  bfvm_batch_set_schedule(b, best_c.mode, best_c.yz_chunk, best_c.order, best_c.ctas, keep_graph);
+  if (best_ms_per_step) *best_ms_per_step = best;
+  return BFVM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,141 @@
+// bfvm_ctx.h -- the state of one resident solve (the opaque bfvm_ctx of the
+// C ABI) and the host helpers shared by the translation units that launch
+// its kernels (single-solve steps and the batched engine).
+#pragma once
+
+#include <cstdio>
+#include <vector>
+
+#include "../../include/biofvm_b200.h"
+#include "bfvm_internal.h"
+
+struct bfvm_ctx {
+  int device = 0;
+  int nx = 0, ny = 0, nz = 0, S = 0, nxp = 0, prec = BFVM_FP64, eb = 8;
+  double dx = 0, dt = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  void* f = nullptr;           // field, device layout
+  size_t field_bytes = 0;
+  // coefficients: per axis a, DR rows [S][npad_a] at dr_off[a] and CU rows
+  // [S][npad_a] at cu_off[a] (bytes into d_coef); c1 as Coef<T>::C1 [S]
+  void* d_coef = nullptr;
+  size_t dr_off[3] = {0, 0, 0}, cu_off[3] = {0, 0, 0};
+  void* d_c1 = nullptr;
+  double* d_off = nullptr;      // FP32: per-substrate field offsets [S]
+  void* d_shift = nullptr;      // FP32: RN32(c2 * off) [S]
+  int* d_active = nullptr;
+  double* d_faces = nullptr;   // xface | yface | zface
+  int* d_status = nullptr;
+  double* d_sums = nullptr;    // partial sums + result
+  bfvm::FieldMaps maps{};
+  bfvm::SweepConfig cfg{};
+  // agents
+  int n_agents = 0, cap_agents = 0;
+  int* d_voxel = nullptr;
+  unsigned char* d_agent_active = nullptr;
+  double* d_c = nullptr;       // c1 | c2 | e2, [n][S] each
+  double* d_rates = nullptr;   // volume [n] | sec | upt | sat | exp [n][S]
+  unsigned* d_dev_voxel = nullptr;
+  unsigned* d_sorted_keys = nullptr;
+  int* d_sorted_vals = nullptr;
+  int* d_line_off = nullptr;
+  int* d_a_i = nullptr;
+  double* d_ac = nullptr;      // ac1 | ac2 | ae2, [S][n] each
+  int* d_nvalid = nullptr;
+  void* d_agent_scratch = nullptr;
+  double* d_sample = nullptr;
+  // host-side mirrors
+  std::vector<unsigned char> active;
+  std::vector<double> faces;    // same layout as d_faces
+  std::vector<double> c2;       // dt*decay/3 per substrate (thomas_constant2)
+  std::vector<double> off;      // FP32 offsets currently applied to the field
+  size_t device_bytes = 0;
+  double* d_staging = nullptr; // reference-layout field, for host uploads/downloads
+  // per-kernel timing: 4 events per recorded step
+  bool timing = false;
+  int timed_steps = 0;
+  std::vector<cudaEvent_t> events;
+};
+
+
+namespace bfvm {
+
+#define BFVM_CUDA(call)                                                                                      \
+  do {                                                                                                       \
+    cudaError_t e__ = (call);                                                                                \
+    if (e__ != cudaSuccess) {                                                                                \
+      std::fprintf(stderr, "biofvm_b200: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e__), __FILE__, \
+                   __LINE__);                                                                                \
+      return e__ == cudaErrorMemoryAllocation ? BFVM_ERR_OOM : BFVM_ERR_CUDA;                                \
+    }                                                                                                        \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+inline int dalloc(bfvm_ctx* c, void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return e == cudaErrorMemoryAllocation ? BFVM_ERR_OOM : BFVM_ERR_CUDA;
+  }
+  c->device_bytes += bytes;
+  return BFVM_OK;
+}
+
+inline void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+template <typename T>
+inline SweepParams<T> make_params(bfvm_ctx* c, bool sources) {
+  SweepParams<T> p{};
+  p.f = static_cast<T*>(c->f);
+  p.nx = c->nx;
+  p.ny = c->ny;
+  p.nz = c->nz;
+  p.S = c->S;
+  p.nxp = c->nxp;
+  const size_t S = c->S;
+  const bool f32 = sizeof(T) == 4;
+  using DR = typename Coef<T>::DR;
+  using CU = typename Coef<T>::CU;
+  p.c1 = static_cast<const typename Coef<T>::C1*>(c->d_c1);
+  p.off = f32 ? c->d_off : nullptr;
+  p.shift = f32 ? static_cast<const T*>(c->d_shift) : nullptr;
+  p.active = c->d_active;
+  p.xface = c->d_faces;
+  p.yface = p.xface + 2 * S * c->nz * c->ny;
+  p.zface = p.yface + 2 * S * c->nz * c->nx;
+  const unsigned char* cb = static_cast<const unsigned char*>(c->d_coef);
+  const int n_axis[3] = {c->nx, c->ny, c->nz};
+  AxisCoefs<T>* axes[3] = {&p.ax, &p.ay, &p.az};
+  for (int a = 0; a < 3; ++a) {
+    axes[a]->dr = reinterpret_cast<const DR*>(cb + c->dr_off[a]);
+    axes[a]->cu = reinterpret_cast<const CU*>(cb + c->cu_off[a]);
+    axes[a]->npad = coef_pad(n_axis[a]);
+  }
+  if (sources && c->n_agents > 0) {
+    p.line_off = c->d_line_off;
+    p.a_i = c->d_a_i;
+    p.ac1 = c->d_ac;
+    p.ac2 = c->d_ac + S * c->n_agents;
+    p.ae2 = c->d_ac + 2 * S * c->n_agents;
+    p.n_sorted = c->n_agents;
+  }
+  p.status = c->d_status;
+  return p;
+}
+
+}  // namespace bfvm

@@ -118,6 +118,46 @@ cudaError_t launch_sweep_z(const FieldMaps& maps, const SweepParams<T>& p, const
 size_t sweep_x_smem(int elem_bytes, int nx, const SweepConfig& cfg);
 size_t sweep_yz_smem(int elem_bytes, int n_line, const SweepConfig& cfg);
 
+// ---- batched engine: one fused launch per LOD step over many solves ------
+// Tiles are 32 lines (one warp) in every sweep of a batch.
+constexpr int kBatchTile = 32;
+
+template <typename T>
+struct alignas(64) BatchEnv {
+  CUtensorMap mx, my, mz;  // tensor maps of this solve's field (boxes as FieldMaps, 32-line tiles)
+  SweepParams<T> p;
+  int chy, chz;            // rows per TMA box of the y and z maps
+  int nty, ntx;            // tiles along y (x sweep) and along x (y and z sweeps)
+};
+
+// Device-resident description of the current membership; rewritten between
+// steps, so a captured step stays valid while the membership changes.
+struct BatchHeader {
+  int n_env;
+  int n_items[3];  // tiles of all members per sweep (x, y, z)
+};
+
+// pre[a*(cap+1) + e]: index of member e's first tile among the tiles of sweep a.
+// counters: [0] work dispenser, [1 + a*cap + e] tiles of sweep a of member e done.
+template <typename T>
+cudaError_t launch_batch_step(const BatchHeader* hdr, const BatchEnv<T>* envs, const int* pre, int cap, int* counters,
+                              int* status, int grid, size_t smem, cudaStream_t st);
+
+// Split schedule: three launches per step (x, y, z), each over the tiles of
+// every member; items[a] tiles and smem[a] bytes per CTA for sweep a.
+template <typename T>
+cudaError_t launch_batch_sweeps(const BatchHeader* hdr, const BatchEnv<T>* envs, const int* pre, int cap,
+                                const int items[3], const size_t smem[3], cudaStream_t st);
+
+// Shared memory one CTA of the fused step needs to hold any tile of a member.
+size_t batch_member_smem(int elem_bytes, int nx, int ny, int nz, int yz_chunk);
+// The same for one sweep (axis 0, 1, 2) of the split schedule.
+size_t batch_axis_smem(int elem_bytes, int axis, int n_line, int yz_chunk);
+
+// Resident CTAs per SM of the fused step at the given shared memory.
+template <typename T>
+cudaError_t batch_occupancy(size_t smem, int* ctas_per_sm);
+
 // Layout conversion between the reference AoS [x][y][z][S] (double) and the
 // device SoA [S][z][y][nxp] (T).
 // off: [S] offsets subtracted on pack / added on unpack (FP32), or null.

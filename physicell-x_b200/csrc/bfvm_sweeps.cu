@@ -61,6 +61,14 @@ namespace {
 template <typename T>
 constexpr bool kF32 = sizeof(T) == 4;
 
+// Chunks per line are bounded so one 64-bit word holds every barrier's phase.
+constexpr int kMaxChunks = 64;
+constexpr int kBarrierBytes = 1024;  // kMaxChunks barriers, padded to keep the tile 1024-byte aligned
+template <typename T>
+constexpr int kChunkX = 128 / static_cast<int>(sizeof(T));  // x-sweep chunk width (one 128-byte row)
+
+__device__ __forceinline__ uint64_t chunk_mask(int C) { return C >= 64 ? ~0ull : ((1ull << C) - 1ull); }
+
 // Forward recurrence over B staged values; out[q] receives y_q and the
 // running value is returned.
 __device__ __forceinline__ double markstein(double t, double d, double r) {
@@ -176,37 +184,35 @@ __device__ __forceinline__ uint32_t smem_align_pad(const void* smem_raw, uint32_
 // ---------------------------------------------------------------------------
 // x sweep
 // ---------------------------------------------------------------------------
+// One x-sweep tile: the lines (j0 .. j0+TL-1, k, s), TL = blockDim.x.  `base`
+// is 1024-byte-aligned shared memory holding kMaxChunks mbarriers (already
+// initialized) followed by the staged tile; `phase` holds the parity each
+// barrier completes next and is advanced here.  The chunks are stored back
+// with bulk stores that the caller must let finish reading shared memory
+// (tma_store_wait_read) before reusing it.  Returns false if a wait gave up.
 template <typename T>
-__global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<T> p) {
+__device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, int k, int s, unsigned char* base,
+                       uint64_t& phase) {
   using DR = typename Coef<T>::DR;
   using CU = typename Coef<T>::CU;
   constexpr int W = 128 / sizeof(T);  // elements per 128-byte row (one TMA box width)
-  extern __shared__ unsigned char smem_raw[];
 
   const int TL = blockDim.x;
   const int nx = p.nx, ny = p.ny, nz = p.nz, S = p.S;
   const int C = (nx + W - 1) / W;
-  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
   uint64_t* bars = reinterpret_cast<uint64_t*>(base);
-  unsigned char* tile = base + ((C * 8 + 1023) & ~1023);
+  unsigned char* tile = base + kBarrierBytes;
   const uint32_t chunk_bytes = static_cast<uint32_t>(TL) * 128u;
 
   const int t = threadIdx.x;
-  const int j0 = blockIdx.x * TL, k = blockIdx.y, s = blockIdx.z;
-
-  if (t == 0) {
-    prefetch_tmap(&map);
-    for (int c = 0; c < C; ++c) mbar_init(smem_u32(&bars[c]), 1);
-    fence_barrier_init();
-  }
-  __syncthreads();
   if (t == 0) {
     for (int c = 0; c < C; ++c) {
       const uint32_t bar = smem_u32(&bars[c]);
       mbar_expect_tx(bar, chunk_bytes);
-      tma_load_4d(smem_u32(tile + c * chunk_bytes), &map, bar, c * W, j0, k, s);
+      tma_load_4d(smem_u32(tile + c * chunk_bytes), map, bar, c * W, j0, k, s);
     }
   }
+  __syncthreads();  // reconverge before any lane blocks on a barrier
 
   const int j = j0 + t;
   const bool valid = j < ny;
@@ -251,7 +257,7 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
   // harmlessly (those results are never stored to the field).
   T y = T(-0.0);
   for (int c = 0; c < C; ++c) {
-    if (ok) ok = mbar_wait(smem_u32(&bars[c]), 0);
+    if (ok) ok = mbar_wait(smem_u32(&bars[c]), static_cast<uint32_t>(phase >> c) & 1u);
     if (face) continue;
     unsigned char* crow = row + c * chunk_bytes;
     const int i0 = c * W;
@@ -273,9 +279,10 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
     y = forward_batch<W>(v, cf, c1, shift, y, out);
     store_row<T, W>(crow, sw, out);
   }
+  phase ^= chunk_mask(C);
   if (__syncthreads_or(!ok)) {
     if (t == 0) atomicExch(p.status, kDevTimeout);
-    return;
+    return false;
   }
 
   // Back substitution, last chunk first; each finished chunk is stored at once.
@@ -317,11 +324,27 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
     fence_async_smem();
     __syncthreads();
     if (t == 0) {
-      tma_store_4d(&map, smem_u32(tile + c * chunk_bytes), c * W, j0, k, s);
+      tma_store_4d(map, smem_u32(tile + c * chunk_bytes), c * W, j0, k, s);
       tma_store_commit();
     }
   }
-  if (t == 0) tma_store_wait_read();
+  return true;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<T> p) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
+  const int C = (p.nx + kChunkX<T> - 1) / kChunkX<T>;
+  if (threadIdx.x == 0) {
+    prefetch_tmap(&map);
+    for (int c = 0; c < C; ++c) mbar_init(smem_u32(reinterpret_cast<uint64_t*>(base) + c), 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  uint64_t phase = 0;
+  x_tile<T>(&map, p, blockIdx.x * blockDim.x, blockIdx.y, blockIdx.z, base, phase);
+  if (threadIdx.x == 0) tma_store_wait_read();
 }
 
 // ---------------------------------------------------------------------------
@@ -329,42 +352,36 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
 // ---------------------------------------------------------------------------
 constexpr int kRowBatch = 16;  // rows staged in registers per batch of the recurrence
 
+// One y- or z-sweep tile: the lines (i0 .. i0+TI-1, m, s), TI = blockDim.x,
+// m = k for the y sweep and j for the z sweep, staged in TMA boxes of CH rows.
+// Shared-memory layout and contract as for x_tile (base 128-byte aligned).
 template <typename T, int AXIS>
-__global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<T> p,
-                                                       int CH) {
+__device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0, int m, int s, int CH,
+                        unsigned char* base, uint64_t& phase) {
   using DR = typename Coef<T>::DR;
   using CU = typename Coef<T>::CU;
   constexpr int R = kRowBatch;
-  extern __shared__ unsigned char smem_raw[];
   const int TI = blockDim.x;
   const int nx = p.nx, ny = p.ny, nz = p.nz, S = p.S;
   const int n = (AXIS == 1) ? ny : nz;
   const int C = (n + CH - 1) / CH;
-  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 128);
   uint64_t* bars = reinterpret_cast<uint64_t*>(base);
-  T* tile = reinterpret_cast<T*>(base + ((C * 8 + 127) & ~127));
+  T* tile = reinterpret_cast<T*>(base + kBarrierBytes);
   const uint32_t chunk_bytes = static_cast<uint32_t>(CH) * TI * sizeof(T);
 
   const int t = threadIdx.x;
-  const int i0 = blockIdx.x * TI, m = blockIdx.y, s = blockIdx.z;  // m = k (y sweep) or j (z sweep)
-
-  if (t == 0) {
-    prefetch_tmap(&map);
-    for (int c = 0; c < C; ++c) mbar_init(smem_u32(&bars[c]), 1);
-    fence_barrier_init();
-  }
-  __syncthreads();
   if (t == 0) {
     for (int c = 0; c < C; ++c) {
       const uint32_t bar = smem_u32(&bars[c]);
       mbar_expect_tx(bar, chunk_bytes);
       T* dst = tile + c * CH * TI;
       if (AXIS == 1)
-        tma_load_4d(smem_u32(dst), &map, bar, i0, c * CH, m, s);
+        tma_load_4d(smem_u32(dst), map, bar, i0, c * CH, m, s);
       else
-        tma_load_4d(smem_u32(dst), &map, bar, i0, m, c * CH, s);
+        tma_load_4d(smem_u32(dst), map, bar, i0, m, c * CH, s);
     }
   }
+  __syncthreads();  // reconverge before any lane blocks on a barrier
 
   const int i = i0 + t;
   const bool valid = i < nx;
@@ -424,7 +441,7 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
   for (int rb = 0; rb < n; rb += R) {
     const int need = min(C, (rb + R + CH - 1) / CH);
     while (waited < need) {
-      if (ok) ok = mbar_wait(smem_u32(&bars[waited]), 0);
+      if (ok) ok = mbar_wait(smem_u32(&bars[waited]), static_cast<uint32_t>(phase >> waited) & 1u);
       ++waited;
     }
     if (face) continue;
@@ -441,12 +458,13 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
     for (int q = 0; q < R; ++q) cb[q * TI] = out[q];
   }
   while (waited < C) {
-    if (ok) ok = mbar_wait(smem_u32(&bars[waited]), 0);
+    if (ok) ok = mbar_wait(smem_u32(&bars[waited]), static_cast<uint32_t>(phase >> waited) & 1u);
     ++waited;
   }
+  phase ^= chunk_mask(C);
   if (__syncthreads_or(!ok)) {
     if (t == 0) atomicExch(p.status, kDevTimeout);
-    return;
+    return false;
   }
 
   // Back substitution in batches of R rows from the end; chunk c is stored
@@ -497,16 +515,191 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
         for (int c = next_store; c >= 0 && c * CH >= rb; --c) {
           const uint32_t src = smem_u32(tile + c * CH * TI);
           if (AXIS == 1)
-            tma_store_4d(&map, src, i0, c * CH, m, s);
+            tma_store_4d(map, src, i0, c * CH, m, s);
           else
-            tma_store_4d(&map, src, i0, m, c * CH, s);
+            tma_store_4d(map, src, i0, m, c * CH, s);
         }
         tma_store_commit();
       }
       while (next_store >= 0 && next_store * CH >= rb) --next_store;
     }
   }
-  if (t == 0) tma_store_wait_read();
+  return true;
+}
+
+template <typename T, int AXIS>
+__global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<T> p,
+                                                       int CH) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 128);
+  const int n = (AXIS == 1) ? p.ny : p.nz;
+  const int C = (n + CH - 1) / CH;
+  if (threadIdx.x == 0) {
+    prefetch_tmap(&map);
+    for (int c = 0; c < C; ++c) mbar_init(smem_u32(reinterpret_cast<uint64_t*>(base) + c), 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  uint64_t phase = 0;
+  yz_tile<T, AXIS>(&map, p, blockIdx.x * blockDim.x, blockIdx.y, blockIdx.z, CH, base, phase);
+  if (threadIdx.x == 0) tma_store_wait_read();
+}
+
+// ---------------------------------------------------------------------------
+// batched step: x, y and z sweeps of many solves in one launch
+// ---------------------------------------------------------------------------
+// Persistent CTAs (one warp each) take tiles from one ordered list -- every
+// x tile of every member, then every y tile, then every z tile -- through an
+// atomic dispenser.  A y (z) tile of member e starts once all x (y) tiles of
+// e are done: each finished tile bumps a per-member counter with release
+// semantics after its bulk stores have completed.  Tiles are handed out in
+// list order, so every tile a waiting CTA depends on is already held by a
+// running CTA that does not itself wait on anything later: the waits always
+// end (and are bounded anyway).
+template <typename T>
+__global__ void __launch_bounds__(kBatchTile) batch_step_kernel(const BatchHeader* __restrict__ hdr,
+                                                                const BatchEnv<T>* __restrict__ envs,
+                                                                const int* __restrict__ pre, int cap,
+                                                                int* __restrict__ counters, int* __restrict__ status) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ int s_item;
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
+  const int t = threadIdx.x;
+  if (t == 0) {
+    for (int c = 0; c < kMaxChunks; ++c) mbar_init(smem_u32(reinterpret_cast<uint64_t*>(base) + c), 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const int n_env = hdr->n_env;
+  const int n0 = hdr->n_items[0], n1 = hdr->n_items[1], n2 = hdr->n_items[2];
+  const int total = n0 + n1 + n2;
+  int* dispenser = counters;
+  int* done = counters + 1;
+  uint64_t phase = 0;
+  for (;;) {
+    if (t == 0) s_item = atomicAdd(dispenser, 1);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= total) break;
+    int axis, local;
+    if (item < n0) {
+      axis = 0;
+      local = item;
+    } else if (item < n0 + n1) {
+      axis = 1;
+      local = item - n0;
+    } else {
+      axis = 2;
+      local = item - n0 - n1;
+    }
+    const int* pa = pre + axis * (cap + 1);
+    int lo = 0, hi = n_env - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(pa + mid) <= local)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const int e = lo;
+    const int tile = local - __ldg(pa + e);
+    const BatchEnv<T>& E = envs[e];
+    if (axis > 0) {
+      const int* pb = pre + (axis - 1) * (cap + 1);
+      const int need = __ldg(pb + e + 1) - __ldg(pb + e);
+      if (t == 0) {
+        const int* cnt = done + (axis - 1) * cap + e;
+        if (ld_acquire_gpu(cnt) < need) {
+          const unsigned long long t0 = global_ns();
+          while (ld_acquire_gpu(cnt) < need) {
+            __nanosleep(128);
+            if (global_ns() - t0 > kWaitLimitNs) {
+              atomicExch(status, kDevTimeout);
+              break;
+            }
+          }
+        }
+        fence_async_global();
+      }
+      __syncthreads();
+    }
+    const SweepParams<T>& p = E.p;
+    if (axis == 0) {
+      const int per = E.nty * p.nz;
+      const int s = tile / per, r = tile - s * per;
+      const int k = r / E.nty;
+      x_tile<T>(&E.mx, p, (r - k * E.nty) * kBatchTile, k, s, base, phase);
+    } else if (axis == 1) {
+      const int per = E.ntx * p.nz;
+      const int s = tile / per, r = tile - s * per;
+      const int k = r / E.ntx;
+      yz_tile<T, 1>(&E.my, p, (r - k * E.ntx) * kBatchTile, k, s, E.chy, base, phase);
+    } else {
+      const int per = E.ntx * p.ny;
+      const int s = tile / per, r = tile - s * per;
+      const int j = r / E.ntx;
+      yz_tile<T, 2>(&E.mz, p, (r - j * E.ntx) * kBatchTile, j, s, E.chz, base, phase);
+    }
+    if (t == 0) {
+      tma_store_wait_all();
+      fence_async_global();
+      red_release_gpu_add(done + axis * cap + e, 1);
+    }
+  }
+}
+
+// Split schedule: one launch per sweep over the tiles of every member (the
+// kernel boundary orders the sweeps; blocks map to tiles through the same
+// prefix table).
+template <typename T, int AXIS>
+__global__ void __launch_bounds__(kBatchTile) batch_sweep_kernel(const BatchHeader* __restrict__ hdr,
+                                                                 const BatchEnv<T>* __restrict__ envs,
+                                                                 const int* __restrict__ pre, int cap) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
+  const int local = blockIdx.x;
+  if (local >= hdr->n_items[AXIS]) return;
+  const int* pa = pre + AXIS * (cap + 1);
+  int lo = 0, hi = hdr->n_env - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(pa + mid) <= local)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const BatchEnv<T>& E = envs[lo];
+  const SweepParams<T>& p = E.p;
+  const int tile = local - __ldg(pa + lo);
+  int C;
+  if (AXIS == 0)
+    C = (p.nx + kChunkX<T> - 1) / kChunkX<T>;
+  else
+    C = ((AXIS == 1 ? p.ny : p.nz) + (AXIS == 1 ? E.chy : E.chz) - 1) / (AXIS == 1 ? E.chy : E.chz);
+  if (threadIdx.x == 0) {
+    for (int c = 0; c < C; ++c) mbar_init(smem_u32(reinterpret_cast<uint64_t*>(base) + c), 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  uint64_t phase = 0;
+  if (AXIS == 0) {
+    const int per = E.nty * p.nz;
+    const int s = tile / per, r = tile - s * per;
+    const int k = r / E.nty;
+    x_tile<T>(&E.mx, p, (r - k * E.nty) * kBatchTile, k, s, base, phase);
+  } else if (AXIS == 1) {
+    const int per = E.ntx * p.nz;
+    const int s = tile / per, r = tile - s * per;
+    const int k = r / E.ntx;
+    yz_tile<T, 1>(&E.my, p, (r - k * E.ntx) * kBatchTile, k, s, E.chy, base, phase);
+  } else {
+    const int per = E.ntx * p.ny;
+    const int s = tile / per, r = tile - s * per;
+    const int j = r / E.ntx;
+    yz_tile<T, 2>(&E.mz, p, (r - j * E.ntx) * kBatchTile, j, s, E.chz, base, phase);
+  }
+  if (threadIdx.x == 0) tma_store_wait_read();
 }
 
 // ---------------------------------------------------------------------------
@@ -515,7 +708,8 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
 size_t sweep_x_smem(int elem_bytes, int nx, const SweepConfig& cfg) {
   const int W = 128 / elem_bytes;
   const int C = (nx + W - 1) / W;
-  return 1024 + ((static_cast<size_t>(C) * 8 + 1023) & ~size_t(1023)) + static_cast<size_t>(C) * cfg.x_lines * 128;
+  if (C > kMaxChunks) return ~size_t(0);
+  return 1024 + kBarrierBytes + static_cast<size_t>(C) * cfg.x_lines * 128;
 }
 
 static int yz_chunk_rows(int n, int target) {
@@ -528,8 +722,9 @@ static int yz_chunk_rows(int n, int target) {
 size_t sweep_yz_smem(int elem_bytes, int n_line, const SweepConfig& cfg) {
   const int CH = yz_chunk_rows(n_line, cfg.yz_chunk);
   const int C = (n_line + CH - 1) / CH;
+  if (C > kMaxChunks) return ~size_t(0);
   const size_t rows = (static_cast<size_t>(C) * CH + kRowBatch - 1) / kRowBatch * kRowBatch;
-  return 128 + ((static_cast<size_t>(C) * 8 + 127) & ~size_t(127)) + rows * cfg.yz_tile * elem_bytes;
+  return 128 + kBarrierBytes + rows * cfg.yz_tile * elem_bytes;
 }
 
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
@@ -610,5 +805,82 @@ template cudaError_t launch_sweep_z<double>(const FieldMaps&, const SweepParams<
                                             cudaStream_t);
 template cudaError_t launch_sweep_z<float>(const FieldMaps&, const SweepParams<float>&, const SweepConfig&,
                                            cudaStream_t);
+
+
+size_t batch_member_smem(int eb, int nx, int ny, int nz, int yz_chunk) {
+  SweepConfig cfg;
+  cfg.x_lines = kBatchTile;
+  cfg.yz_tile = kBatchTile;
+  cfg.yz_chunk = yz_chunk;
+  const size_t a = sweep_x_smem(eb, nx, cfg), b = sweep_yz_smem(eb, ny, cfg), c = sweep_yz_smem(eb, nz, cfg);
+  size_t m = a > b ? a : b;
+  m = m > c ? m : c;
+  // the x layout aligns to 1024 bytes; the fused kernel uses it for every sweep
+  return m + 1024;
+}
+
+size_t batch_axis_smem(int eb, int axis, int n_line, int yz_chunk) {
+  SweepConfig cfg;
+  cfg.x_lines = kBatchTile;
+  cfg.yz_tile = kBatchTile;
+  cfg.yz_chunk = yz_chunk;
+  return (axis == 0 ? sweep_x_smem(eb, n_line, cfg) : sweep_yz_smem(eb, n_line, cfg)) + 1024;
+}
+
+template <typename T>
+cudaError_t batch_occupancy(size_t smem, int* ctas_per_sm) {
+  cudaError_t e = cudaFuncSetAttribute(batch_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, batch_step_kernel<T>, kBatchTile, smem);
+}
+
+template <typename T>
+cudaError_t launch_batch_step(const BatchHeader* hdr, const BatchEnv<T>* envs, const int* pre, int cap, int* counters,
+                              int* status, int grid, size_t smem, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(batch_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  batch_step_kernel<T><<<grid, kBatchTile, smem, st>>>(hdr, envs, pre, cap, counters, status);
+  return cudaGetLastError();
+}
+
+template cudaError_t batch_occupancy<double>(size_t, int*);
+template cudaError_t batch_occupancy<float>(size_t, int*);
+template cudaError_t launch_batch_step<double>(const BatchHeader*, const BatchEnv<double>*, const int*, int, int*, int*,
+                                               int, size_t, cudaStream_t);
+template cudaError_t launch_batch_step<float>(const BatchHeader*, const BatchEnv<float>*, const int*, int, int*, int*,
+                                              int, size_t, cudaStream_t);
+
+
+template <typename T>
+cudaError_t launch_batch_sweeps(const BatchHeader* hdr, const BatchEnv<T>* envs, const int* pre, int cap,
+                                const int items[3], const size_t smem[3], cudaStream_t st) {
+  cudaError_t e;
+  if (items[0] > 0) {
+    e = cudaFuncSetAttribute(batch_sweep_kernel<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem[0]));
+    if (e != cudaSuccess) return e;
+    batch_sweep_kernel<T, 0><<<items[0], kBatchTile, smem[0], st>>>(hdr, envs, pre, cap);
+  }
+  if (items[1] > 0) {
+    e = cudaFuncSetAttribute(batch_sweep_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem[1]));
+    if (e != cudaSuccess) return e;
+    batch_sweep_kernel<T, 1><<<items[1], kBatchTile, smem[1], st>>>(hdr, envs, pre, cap);
+  }
+  if (items[2] > 0) {
+    e = cudaFuncSetAttribute(batch_sweep_kernel<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem[2]));
+    if (e != cudaSuccess) return e;
+    batch_sweep_kernel<T, 2><<<items[2], kBatchTile, smem[2], st>>>(hdr, envs, pre, cap);
+  }
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_batch_sweeps<double>(const BatchHeader*, const BatchEnv<double>*, const int*, int,
+                                                 const int[3], const size_t[3], cudaStream_t);
+template cudaError_t launch_batch_sweeps<float>(const BatchHeader*, const BatchEnv<float>*, const int*, int,
+                                                const int[3], const size_t[3], cudaStream_t);
 
 }  // namespace bfvm

@@ -146,6 +146,22 @@ int bfvm_step(bfvm_ctx* ctx, int nsteps, int flags);
  * Microenvironment::simulate_cell_sources_and_sinks(dt), :1381-1384). */
 int bfvm_apply_sources(bfvm_ctx* ctx);
 
+/* No counterpart in the reference.  One source/sink stage (the operations of
+ * bfvm_apply_sources, same results) for n agents whose arrays are already in
+ * device memory on the solve's device: voxel [n] (reference voxel index, <0 =
+ * none), active [n] or NULL (all active), c1/c2/e2 [n][S] agent-list order.
+ * The arrays are read on the solve's stream; the solve's own agent list is
+ * left unchanged.  It calls no device allocator: the voxel sort runs in one
+ * fixed scratch array per device inside the library, for callers that must
+ * not allocate at that point (a loop whose device memory was reserved up
+ * front, or code where cudaMalloc is not allowed).  Limits: n <= 262144
+ * (larger: BFVM_ERR_ARG, no work queued); calls on the same device must not
+ * overlap in time (they share the scratch and would race); the first call on
+ * a device looks up the scratch address and should come before any stream
+ * capture begins. */
+int bfvm_apply_sources_noalloc(bfvm_ctx* ctx, int n, const int* voxel, const unsigned char* active,
+                               const double* c1, const double* c2, const double* e2);
+
 /* Densities at each agent's voxel, [n][S] host doubles, in agent-list order
  * (what Basic_Agent::nearest_density_vector returns to each agent,
  * BioFVM/BioFVM_basic_agent.cpp:389-392). */

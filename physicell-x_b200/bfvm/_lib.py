@@ -61,6 +61,7 @@ _SIGS = {
     "bfvm_step": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "bfvm_agent_constants_device": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double] + [C.c_void_p] * 9),
     "bfvm_apply_sources": (C.c_int, [C.c_void_p]),
+    "bfvm_apply_sources_noalloc": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 5),
     "bfvm_sample_agents": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_field_sums": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_synchronize": (C.c_int, [C.c_void_p]),

@@ -217,6 +217,37 @@ __global__ void agent_sources_kernel(int n, const unsigned* __restrict__ sk, uns
   (void)ny;
 }
 
+// The same stage with the constants read through the sorted order from the
+// agent-list layout c1/c2/e2[a*S + s], so no gathered copy is needed; the
+// operations and their order per voxel are those of agent_sources_kernel.
+template <typename T>
+__global__ void agent_sources_by_order_kernel(int n, const unsigned* __restrict__ sk, const int* __restrict__ order,
+                                              unsigned sentinel, int S, int nx, int nz_ny, int nxp,
+                                              const double* __restrict__ c1, const double* __restrict__ c2,
+                                              const double* __restrict__ e2, const double* __restrict__ off,
+                                              T* __restrict__ f) {
+  const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= static_cast<long long>(n) * S) return;
+  const int s = static_cast<int>(idx / n);
+  const int p = static_cast<int>(idx % n);
+  const unsigned key = sk[p];
+  if (key >= sentinel) return;
+  if (p > 0 && sk[p - 1] == key) return;
+  const int i = key % nx;
+  const int jk = key / nx;
+  T* rho = f + (static_cast<size_t>(s) * nz_ny + jk) * nxp + i;
+  double r = static_cast<double>(*rho);
+  if (off) r += off[s];
+  for (int q = p; q < n && sk[q] == key; ++q) {
+    const size_t a = static_cast<size_t>(order[q]) * S + s;
+    r += c1[a];
+    r /= c2[a];
+    r += e2[a];
+  }
+  if (off) r -= off[s];
+  *rho = static_cast<T>(r);
+}
+
 // Densities at each agent's voxel, in agent-list order, [n][S] FP64
 // (what Basic_Agent::nearest_density_vector exposes to the agent).
 template <typename T>
@@ -295,6 +326,62 @@ cudaError_t agents_build(const AgentBuild& b, cudaStream_t st, int* launches) {
   *launches = 2 + 3 * passes;
   return cudaGetLastError();
 }
+
+cudaError_t agents_sort(int n, const int* voxel, const unsigned char* active, int nx, int ny, int nz, void* scratch,
+                        cudaStream_t st, const unsigned** sorted_keys, const int** sorted_order, int* launches) {
+  *launches = 0;
+  if (n == 0) return cudaSuccess;
+  const unsigned sentinel = static_cast<unsigned>(nx) * ny * nz;
+  // scratch: keys0 | vals0 | keys1 | vals1 | hist; the passes ping-pong
+  // between the two key/value pairs.
+  unsigned* k0 = reinterpret_cast<unsigned*>(scratch);
+  int* v0 = reinterpret_cast<int*>(k0 + n);
+  unsigned* k1 = reinterpret_cast<unsigned*>(v0 + n);
+  int* v1 = reinterpret_cast<int*>(k1 + n);
+  unsigned* hist = reinterpret_cast<unsigned*>(v1 + n);
+  // The per-agent device voxel ids go to keys1, which the first pass then
+  // overwrites: this variant keeps no list-order copy.
+  agent_keys_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, voxel, active, nx, ny, nz, sentinel, k0, v0, k1);
+  int bits = 1;
+  while (bits < 32 && (static_cast<unsigned long long>(1) << bits) <= sentinel) ++bits;
+  const int passes = (bits + kRadixBits - 1) / kRadixBits;
+  const int nblocks = (n + kSortTile - 1) / kSortTile;
+  unsigned* kin = k0;
+  int* vin = v0;
+  for (int pass = 0; pass < passes; ++pass) {
+    unsigned* kout = (kin == k0) ? k1 : k0;
+    int* vout = (vin == v0) ? v1 : v0;
+    const int shift = pass * kRadixBits;
+    radix_hist_kernel<<<nblocks, kSortThreads, 0, st>>>(n, kin, shift, nblocks, hist);
+    scan_kernel<<<1, 1024, 0, st>>>(hist, kRadix * nblocks);
+    radix_scatter_kernel<<<nblocks, kSortThreads, 0, st>>>(n, kin, vin, shift, nblocks, hist, kout, vout);
+    kin = kout;
+    vin = vout;
+  }
+  *sorted_keys = kin;
+  *sorted_order = vin;
+  *launches = 1 + 3 * passes;
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t agents_apply_sources_by_order(int n, const unsigned* sorted_keys, const int* sorted_order, int S, int nx,
+                                          int ny, int nz, int nxp, const double* c1, const double* c2,
+                                          const double* e2, const double* off, T* f, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const unsigned sentinel = static_cast<unsigned>(nx) * ny * nz;
+  const long long total = static_cast<long long>(n) * S;
+  agent_sources_by_order_kernel<T><<<static_cast<unsigned>((total + 255) / 256), 256, 0, st>>>(
+      n, sorted_keys, sorted_order, sentinel, S, nx, ny * nz, nxp, c1, c2, e2, off, f);
+  return cudaGetLastError();
+}
+
+template cudaError_t agents_apply_sources_by_order<double>(int, const unsigned*, const int*, int, int, int, int, int,
+                                                           const double*, const double*, const double*,
+                                                           const double*, double*, cudaStream_t);
+template cudaError_t agents_apply_sources_by_order<float>(int, const unsigned*, const int*, int, int, int, int, int,
+                                                          const double*, const double*, const double*, const double*,
+                                                          float*, cudaStream_t);
 
 template <typename T>
 cudaError_t agents_apply_sources(int n, const unsigned* sorted_keys, int S, int nx, int ny, int nz, int nxp,

@@ -38,6 +38,20 @@ cudaError_t agents_compute_constants(int n, int S, double dt, double voxel_volum
 // Sorts and bins the list; *launches receives the number of kernels launched.
 cudaError_t agents_build(const AgentBuild& b, cudaStream_t st, int* launches);
 
+// Stable sort of the list by device voxel id inside caller-provided scratch of
+// agent_scratch_bytes(n) bytes (nothing else is written).  On return
+// *sorted_keys / *sorted_order point into the scratch: the sorted voxel ids
+// (nx*ny*nz = no voxel) and the agent index at each sorted position.
+cudaError_t agents_sort(int n, const int* voxel, const unsigned char* active, int nx, int ny, int nz, void* scratch,
+                        cudaStream_t st, const unsigned** sorted_keys, const int** sorted_order, int* launches);
+
+// Source/sink stage from a sort made by agents_sort, constants c1/c2/e2 in
+// agent-list layout [n][S]; off as below.
+template <typename T>
+cudaError_t agents_apply_sources_by_order(int n, const unsigned* sorted_keys, const int* sorted_order, int S, int nx,
+                                          int ny, int nz, int nxp, const double* c1, const double* c2,
+                                          const double* e2, const double* off, T* f, cudaStream_t st);
+
 // off: [S] field offsets of an FP32 solve (the field holds rho - off), or null.
 template <typename T>
 cudaError_t agents_apply_sources(int n, const unsigned* sorted_keys, int S, int nx, int ny, int nz, int nxp,

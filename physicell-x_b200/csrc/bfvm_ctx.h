@@ -128,7 +128,7 @@ inline SweepParams<T> make_params(bfvm_ctx* c, bool sources) {
   }
   if (sources && c->n_agents > 0) {
     p.line_off = c->d_line_off;
-    p.a_i = c->d_a_i;
+    p.a_key = c->d_sorted_keys;
     p.ac1 = c->d_ac;
     p.ac2 = c->d_ac + S * c->n_agents;
     p.ae2 = c->d_ac + 2 * S * c->n_agents;

@@ -45,9 +45,9 @@ struct Coef<float> {
   using C1 = float2;
 };
 
-// Thomas coefficients of one axis for all substrates: rows [S][npad], npad =
-// the line length rounded up to 32, padded with neutral entries so batches
-// may read past the end of a line without bounds checks.
+// Thomas coefficients of one axis for all substrates: rows [S][npad], padded
+// with neutral entries so the sweeps may read (and prefetch one batch ahead)
+// past the end of a line without bounds checks.
 template <typename T>
 struct AxisCoefs {
   const typename Coef<T>::DR* dr;
@@ -55,8 +55,11 @@ struct AxisCoefs {
   int npad;
 };
 
-// Rows of coefficient storage per line of n voxels.
-inline int coef_pad(int n) { return (n + 31) / 32 * 32; }
+// Rows of coefficient storage per line of n voxels: a y/z tile holds fewer
+// than n + 80 rows (at most 64 chunks, rounded up to 16-row batches) and the
+// sweeps prefetch the coefficients of the next 16-row batch, so every read
+// stays below n + 96.
+inline int coef_pad(int n) { return (n + 96 + 31) / 32 * 32; }
 
 template <typename T>
 struct SweepParams {
@@ -76,9 +79,10 @@ struct SweepParams {
   const double* zface;
   AxisCoefs<T> ax, ay, az;
   // Agents (optional): sorted by device voxel id, CSR over x-lines
-  // (line = k*ny + j).  a_i: x index; ac1/ac2/ae2: [S][n_sorted] FP64.
+  // (line = k*ny + j).  a_key: sorted device voxel ids ((k*ny + j)*nx + i);
+  // ac1/ac2/ae2: [S][n_sorted] FP64 in sorted order.
   const int* line_off;   // [ny*nz + 1] or nullptr when no sources this step
-  const int* a_i;
+  const unsigned* a_key;
   const double* ac1;
   const double* ac2;
   const double* ae2;

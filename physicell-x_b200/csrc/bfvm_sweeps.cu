@@ -118,23 +118,27 @@ __device__ __forceinline__ float back_elem(float2 c, float xn, float y) {
   return __fmaf_rn(-c.x, xn, __fmaf_rn(-c.y, xn, y));
 }
 
-// Apply every agent of voxel i (agents of this line are sorted by x index,
-// then by agent index) to the value v, in FP64, and return the result.
+// Apply the run of agents that starts at sorted position q (key `key`,
+// constants c1/c2/e2 of that first agent already loaded) to the staged value
+// at *e, in sorted order -- which is agent-list order within a voxel --
+// with the reference's three operations per agent, in FP64.
 template <typename T>
-__device__ __forceinline__ T apply_agents(T v, int i, int& a, int aend, int& next_i, const int* __restrict__ a_i,
-                                          const double* __restrict__ c1, const double* __restrict__ c2,
-                                          const double* __restrict__ e2, double off) {
-  double r = static_cast<double>(v);
+__device__ __forceinline__ void apply_run(T* e, int q, unsigned key, double c1, double c2, double e2, int qend,
+                                          const unsigned* __restrict__ a_key, const double* __restrict__ ac1,
+                                          const double* __restrict__ ac2, const double* __restrict__ ae2,
+                                          double off) {
+  double r = static_cast<double>(*e);
   if constexpr (kF32<T>) r += off;
-  do {
-    r += c1[a];
-    r /= c2[a];
-    r += e2[a];
-    ++a;
-    next_i = (a < aend) ? __ldg(a_i + a) : INT_MAX;
-  } while (next_i == i);
+  r += c1;
+  r /= c2;
+  r += e2;
+  for (int q2 = q + 1; q2 < qend && __ldg(a_key + q2) == key; ++q2) {
+    r += __ldg(ac1 + q2);
+    r /= __ldg(ac2 + q2);
+    r += __ldg(ae2 + q2);
+  }
   if constexpr (kF32<T>) r -= off;
-  return static_cast<T>(r);
+  *e = static_cast<T>(r);
 }
 
 // Element e (0..W-1) of a thread's 128-byte row in a chunk staged with the
@@ -196,6 +200,7 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   using DR = typename Coef<T>::DR;
   using CU = typename Coef<T>::CU;
   constexpr int W = 128 / sizeof(T);  // elements per 128-byte row (one TMA box width)
+  constexpr int kAgentRounds = 4;     // agent rounds whose data is loaded ahead
 
   const int TL = blockDim.x;
   const int nx = p.nx, ny = p.ny, nz = p.nz, S = p.S;
@@ -232,50 +237,97 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
     x0v = static_cast<T>(p.xface[(static_cast<size_t>(0 * S + s) * nz + k) * ny + j] - off);
     x1v = static_cast<T>(p.xface[(static_cast<size_t>(1 * S + s) * nz + k) * ny + j] - off);
   }
-  int a = 0, aend = 0, next_i = INT_MAX;
-  const double *ac1 = nullptr, *ac2 = nullptr, *ae2 = nullptr;
-  if (p.line_off != nullptr && valid && !face) {
-    const int line = k * ny + j;
-    a = __ldg(p.line_off + line);
-    aend = __ldg(p.line_off + line + 1);
-    next_i = (a < aend) ? __ldg(p.a_i + a) : INT_MAX;
-    ac1 = p.ac1 + static_cast<size_t>(s) * p.n_sorted;
-    ac2 = p.ac2 + static_cast<size_t>(s) * p.n_sorted;
-    ae2 = p.ae2 + static_cast<size_t>(s) * p.n_sorted;
-  }
   const DR* __restrict__ drp = p.ax.dr + static_cast<size_t>(s) * p.ax.npad;
   const CU* __restrict__ cup = p.ax.cu + static_cast<size_t>(s) * p.ax.npad;
   const typename Coef<T>::C1 c1 = p.c1[s];
   const T shift = kF32<T> ? p.shift[s] : T(0);
+  DR cfn[W];  // coefficients of the next chunk, loaded one chunk ahead
+#pragma unroll
+  for (int q = 0; q < W; ++q) cfn[q] = __ldg(drp + q);
 
   unsigned char* row = tile + t * 128;
   const int sw = t & 7;
   bool ok = true;
+  bool all_landed = false;
+
+  // Agent sources.  The agents of this tile's lines are one contiguous range
+  // of the sorted list; lanes take them in rounds of TL, each lane applying
+  // the run of agents that starts at its position to the staged voxel.  Runs
+  // never share a voxel, so the lanes are independent; faces are pinned over
+  // the result afterwards, as the reference pins after its source step.
+  if (p.line_off != nullptr) {
+    const int line0 = k * ny + j0;
+    const int A0 = __ldg(p.line_off + line0);
+    const int A1 = __ldg(p.line_off + line0 + min(TL, ny - j0));
+    if (A1 > A0) {  // uniform across the CTA
+      const double* ac1 = p.ac1 + static_cast<size_t>(s) * p.n_sorted;
+      const double* ac2 = p.ac2 + static_cast<size_t>(s) * p.n_sorted;
+      const double* ae2 = p.ae2 + static_cast<size_t>(s) * p.n_sorted;
+      unsigned akey[kAgentRounds], aprev[kAgentRounds];
+      double a1[kAgentRounds], a2[kAgentRounds], a3[kAgentRounds];
+#pragma unroll
+      for (int r = 0; r < kAgentRounds; ++r) {
+        const int q = A0 + t + r * TL;
+        const bool in = q < A1;
+        akey[r] = in ? __ldg(p.a_key + q) : 0u;
+        aprev[r] = (in && q > A0) ? __ldg(p.a_key + q - 1) : ~0u;
+        a1[r] = in ? __ldg(ac1 + q) : 0.0;
+        a2[r] = in ? __ldg(ac2 + q) : 1.0;
+        a3[r] = in ? __ldg(ae2 + q) : 0.0;
+      }
+      for (int c = 0; c < C; ++c)
+        if (ok) ok = mbar_wait(smem_u32(&bars[c]), static_cast<uint32_t>(phase >> c) & 1u);
+      all_landed = true;
+      auto elem = [&](unsigned key) {
+        const int line = static_cast<int>(key / static_cast<unsigned>(nx));
+        const int i = static_cast<int>(key - static_cast<unsigned>(line) * nx);
+        const int rl = line - line0;
+        return swz_elem<T>(tile + (i / W) * chunk_bytes + rl * 128, i % W, rl & 7);
+      };
+      if (ok) {
+#pragma unroll
+        for (int r = 0; r < kAgentRounds; ++r) {
+          const int q = A0 + t + r * TL;
+          if (q < A1 && akey[r] != aprev[r])
+            apply_run<T>(elem(akey[r]), q, akey[r], a1[r], a2[r], a3[r], A1, p.a_key, ac1, ac2, ae2, off);
+        }
+        for (int r = kAgentRounds; A0 + r * TL < A1; ++r) {
+          const int q = A0 + t + r * TL;
+          if (q < A1) {
+            const unsigned key = __ldg(p.a_key + q);
+            if (q == A0 || __ldg(p.a_key + q - 1) != key)
+              apply_run<T>(elem(key), q, key, __ldg(ac1 + q), __ldg(ac2 + q), __ldg(ae2 + q), A1, p.a_key, ac1, ac2,
+                           ae2, off);
+          }
+        }
+      }
+      __syncthreads();  // agents wrote rows of other lanes
+    }
+  }
 
   // Forward elimination, one chunk at a time as the TMA boxes land.  Values
   // past nx in the last chunk are TMA fill; the chain may run over them
   // harmlessly (those results are never stored to the field).
   T y = T(-0.0);
   for (int c = 0; c < C; ++c) {
-    if (ok) ok = mbar_wait(smem_u32(&bars[c]), static_cast<uint32_t>(phase >> c) & 1u);
+    if (!all_landed && ok) ok = mbar_wait(smem_u32(&bars[c]), static_cast<uint32_t>(phase >> c) & 1u);
+    DR cf[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) cf[q] = cfn[q];
+    if (c + 1 < C) {
+#pragma unroll
+      for (int q = 0; q < W; ++q) cfn[q] = __ldg(drp + (c + 1) * W + q);
+    }
     if (face) continue;
     unsigned char* crow = row + c * chunk_bytes;
     const int i0 = c * W;
-    const int iend = min(nx, i0 + W);
-    // Sources, then the pin before the sweep, on the staged row.
-    while (next_i < iend) {
-      T* e = swz_elem<T>(crow, next_i - i0, sw);
-      *e = apply_agents<T>(*e, next_i, a, aend, next_i, p.a_i, ac1, ac2, ae2, off);
-    }
+    // The pin before the sweep, on the staged row (after the sources).
     if (act) {
       if (i0 == 0) *swz_elem<T>(crow, 0, sw) = x0v;
-      if (nx - 1 < iend) *swz_elem<T>(crow, nx - 1 - i0, sw) = x1v;
+      if (nx - 1 < i0 + W) *swz_elem<T>(crow, nx - 1 - i0, sw) = x1v;
     }
     T v[W], out[W];
-    DR cf[W];
     load_row<T, W>(crow, sw, v);
-#pragma unroll
-    for (int q = 0; q < W; ++q) cf[q] = __ldg(drp + i0 + q);
     y = forward_batch<W>(v, cf, c1, shift, y, out);
     store_row<T, W>(crow, sw, out);
   }
@@ -286,19 +338,30 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   }
 
   // Back substitution, last chunk first; each finished chunk is stored at once.
+  CU cwn[W];
+#pragma unroll
+  for (int q = 0; q < W; ++q) cwn[q] = __ldg(cup + (C - 1) * W + q);
   T xn = T(-0.0);
   for (int c = C - 1; c >= 0; --c) {
     unsigned char* crow = row + c * chunk_bytes;
     const int i0 = c * W;
+    CU cw[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) cw[q] = cwn[q];
+    if (c > 0) {
+#pragma unroll
+      for (int q = 0; q < W; ++q) cwn[q] = __ldg(cup + (c - 1) * W + q);
+    }
     if (face) {
+      T fw[W];
+#pragma unroll
+      for (int q = 0; q < W; ++q) fw[q] = (fv != nullptr && i0 + q < nx) ? static_cast<T>(fv[i0 + q] - off) : T(0);
+#pragma unroll
       for (int q = 0; q < W; ++q)
-        if (i0 + q < nx) *swz_elem<T>(crow, q, sw) = static_cast<T>(fv != nullptr ? fv[i0 + q] - off : 0.0);
+        if (i0 + q < nx) *swz_elem<T>(crow, q, sw) = fw[q];
     } else {
       T v[W];
-      CU cw[W];
       load_row<T, W>(crow, sw, v);
-#pragma unroll
-      for (int q = 0; q < W; ++q) cw[q] = __ldg(cup + i0 + q);
       if (i0 + W > nx) {
         // the line ends inside this chunk: skip the fill past nx
 #pragma unroll
@@ -362,8 +425,14 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
   using CU = typename Coef<T>::CU;
   constexpr int R = kRowBatch;
   const int TI = blockDim.x;
-  const int nx = p.nx, ny = p.ny, nz = p.nz, S = p.S;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int n = (AXIS == 1) ? ny : nz;
+  const bool act = p.active[s] != 0;
+  // A tile whose lines all lie in an activated face is already final: its
+  // input holds the face values (every face voxel is pinned by the sweep
+  // before) and the pin after this sweep writes the same values again.
+  if (act && (m == 0 || m == ((AXIS == 1) ? nz : ny) - 1)) return true;
+
   const int C = (n + CH - 1) / CH;
   uint64_t* bars = reinterpret_cast<uint64_t*>(base);
   T* tile = reinterpret_cast<T*>(base + kBarrierBytes);
@@ -384,54 +453,22 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
   __syncthreads();  // reconverge before any lane blocks on a barrier
 
   const int i = i0 + t;
-  const bool valid = i < nx;
-  const bool act = p.active[s] != 0;
-  bool face;
-  const double* fv = nullptr;  // face-line values: fv[r * fstride]
-  int fstride = 1;
-  const double off = kF32<T> ? p.off[s] : 0.0;
-  T e0v = T(0), e1v = T(0);  // pinned values at the two ends of the line
-  if (AXIS == 1) {
-    const int k = m;
-    face = act && (i == 0 || i == nx - 1 || k == 0 || k == nz - 1);
-    if (face && valid) {
-      if (k == 0 || k == nz - 1) {
-        fv = p.zface + (static_cast<size_t>(k == 0 ? 0 : 1) * S + s) * ny * nx + i;
-        fstride = nx;
-      } else {
-        fv = p.xface + ((static_cast<size_t>(i == 0 ? 0 : 1) * S + s) * nz + k) * ny;
-        fstride = 1;
-      }
-    }
-    if (act && valid) {
-      e0v = static_cast<T>(p.yface[(static_cast<size_t>(0 * S + s) * nz + k) * nx + i] - off);
-      e1v = static_cast<T>(p.yface[(static_cast<size_t>(1 * S + s) * nz + k) * nx + i] - off);
-    }
-  } else {
-    const int j = m;
-    face = act && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1);
-    if (face && valid) {
-      if (j == 0 || j == ny - 1) {
-        fv = p.yface + (static_cast<size_t>(j == 0 ? 0 : 1) * S + s) * nz * nx + i;
-        fstride = nx;
-      } else {
-        fv = p.xface + (static_cast<size_t>(i == 0 ? 0 : 1) * S + s) * nz * ny + j;
-        fstride = ny;
-      }
-    }
-    if (act && valid) {
-      e0v = static_cast<T>(p.zface[(static_cast<size_t>(0 * S + s) * ny + j) * nx + i] - off);
-      e1v = static_cast<T>(p.zface[(static_cast<size_t>(1 * S + s) * ny + j) * nx + i] - off);
-    }
-  }
+  // Lines in an x face keep their (pinned) input, as above.
+  const bool face = act && (i == 0 || i == nx - 1);
   const AxisCoefs<T>& ac = (AXIS == 1) ? p.ay : p.az;
   const DR* __restrict__ drp = ac.dr + static_cast<size_t>(s) * ac.npad;
   const CU* __restrict__ cup = ac.cu + static_cast<size_t>(s) * ac.npad;
   const typename Coef<T>::C1 c1 = p.c1[s];
   const T shift = kF32<T> ? p.shift[s] : T(0);
+  DR cfn[R];  // coefficients of the next batch, loaded one batch ahead
+#pragma unroll
+  for (int q = 0; q < R; ++q) cfn[q] = __ldg(drp + q);
   T* col = tile + t;
   bool ok = true;
   int waited = 0;  // chunks whose TMA load this thread has waited for
+  // The two end voxels of the line lie in the y (z) faces: the pin after the
+  // sweep restores their input values.
+  T e0v = T(0), e1v = T(0);
 
   // Forward elimination in batches of R rows; a batch first waits for the
   // chunks that cover it.  The tile holds a whole number of batches, so the
@@ -444,14 +481,24 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
       if (ok) ok = mbar_wait(smem_u32(&bars[waited]), static_cast<uint32_t>(phase >> waited) & 1u);
       ++waited;
     }
-    if (face) continue;
-    T v[R], out[R];
     DR cf[R];
-    T* cb = col + rb * TI;
 #pragma unroll
     for (int q = 0; q < R; ++q) {
-      v[q] = cb[q * TI];
-      cf[q] = __ldg(drp + rb + q);
+      cf[q] = cfn[q];
+      cfn[q] = __ldg(drp + rb + R + q);
+    }
+    if (face) continue;
+    T v[R], out[R];
+    T* cb = col + rb * TI;
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
+    if (act) {
+      if (rb == 0) e0v = v[0];
+      if (rb + R > n - 1) {
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+          if (rb + q == n - 1) e1v = v[q];
+      }
     }
     y = forward_batch<R>(v, cf, c1, shift, y, out);
 #pragma unroll
@@ -472,19 +519,22 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
   T xn = T(-0.0);
   int next_store = C - 1;
   const int last_b = ((n - 1) / R) * R;
-  for (int rb = last_b; rb >= 0; rb -= R) {
-    T* cb = col + rb * TI;
-    if (face) {
-      for (int rr = min(n - 1, rb + R - 1); rr >= rb; --rr)
-        col[rr * TI] = static_cast<T>(fv != nullptr ? fv[rr * fstride] - off : 0.0);
-    } else {
-      T v[R];
-      CU cw[R];
+  CU cwn[R];
 #pragma unroll
-      for (int q = 0; q < R; ++q) {
-        v[q] = cb[q * TI];
-        cw[q] = __ldg(cup + rb + q);
-      }
+  for (int q = 0; q < R; ++q) cwn[q] = __ldg(cup + last_b + q);
+  for (int rb = last_b; rb >= 0; rb -= R) {
+    CU cw[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) cw[q] = cwn[q];
+    if (rb > 0) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) cwn[q] = __ldg(cup + rb - R + q);
+    }
+    if (!face) {
+      T* cb = col + rb * TI;
+      T v[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
       if (rb == last_b) {
 #pragma unroll
         for (int q = R - 1; q >= 0; --q) {

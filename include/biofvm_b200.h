@@ -193,9 +193,11 @@ int bfvm_field_offsets(bfvm_ctx* ctx, double* offsets);
 /* Bytes of device memory the solve holds (field, coefficients, agents). */
 size_t bfvm_device_bytes(bfvm_ctx* ctx);
 
-/* Launch shape of the sweeps: lines per CTA in the x sweep, x extent per CTA
- * and rows per TMA box in the y/z sweeps.  The defaults fit all extents up to
- * 256 in FP64; bfvm_set_launch re-encodes the TMA descriptors. */
+/* Launch shape of the sweeps: lines per CTA in the x sweep (a multiple of 8,
+ * at most 256), x extent per CTA in the y/z sweeps (16 -- FP64 only --, 32 or
+ * 64) and rows per TMA box in the y/z sweeps (1..256).  The defaults fit all
+ * extents up to 256 in FP64; bfvm_set_launch re-encodes the TMA descriptors
+ * and returns BFVM_ERR_ARG for other values. */
 int bfvm_get_launch(bfvm_ctx* ctx, int* x_lines, int* yz_tile, int* yz_chunk);
 int bfvm_set_launch(bfvm_ctx* ctx, int x_lines, int yz_tile, int yz_chunk);
 

@@ -151,6 +151,9 @@ size_t coef_bytes(const bfvm_ctx* c, size_t* dr_off, size_t* cu_off) {
 
 int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
   const int S = c->S;
+  c->screen = 1;
+  for (int s = 0; s < S; ++s)
+    if (!(D[s] >= 0.0) || !(decay[s] >= 0.0)) c->screen = 0;
   const int n_axis[3] = {c->nx, c->ny, c->nz};
   size_t dr_off[3], cu_off[3];
   const size_t bytes = coef_bytes(c, dr_off, cu_off);
@@ -819,11 +822,12 @@ extern "C" int bfvm_set_launch(bfvm_ctx* c, int x_lines, int yz_tile, int yz_chu
   cfg.x_lines = x_lines;
   cfg.yz_tile = yz_tile;
   cfg.yz_chunk = yz_chunk;
-  // x_lines: multiple of 8 (1024-byte swizzle atoms); yz_tile: whole 128-byte
+  // x_lines: multiple of 8 (1024-byte swizzle atoms), at most 256 (box
+  // limit); yz_tile: 16 (FP64 only), 32 or 64 consecutive x -- whole 128-byte
   // rows, so every TMA chunk starts 128-byte aligned in shared memory and
-  // every box's x coordinate is 16-byte aligned; both at most 256 (box limit).
+  // every box's x coordinate is 16-byte aligned.
   if (x_lines < 8 || x_lines > 256 || x_lines % 8 != 0) return BFVM_ERR_ARG;
-  if (yz_tile < 1 || yz_tile > 256 || (yz_tile * c->eb) % 128 != 0) return BFVM_ERR_ARG;
+  if ((yz_tile != 16 && yz_tile != 32 && yz_tile != 64) || (yz_tile * c->eb) % 128 != 0) return BFVM_ERR_ARG;
   if (yz_chunk < 1 || yz_chunk > 256) return BFVM_ERR_ARG;
   if (!config_fits(c->eb, c->nx, c->ny, c->nz, cfg)) return BFVM_ERR_SHAPE;
   DeviceGuard g(c->device);

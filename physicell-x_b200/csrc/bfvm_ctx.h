@@ -22,6 +22,7 @@ struct bfvm_ctx {
   void* d_coef = nullptr;
   size_t dr_off[3] = {0, 0, 0}, cu_off[3] = {0, 0, 0};
   void* d_c1 = nullptr;
+  int screen = 0;              // no negative diffusion or decay (SweepParams::screen)
   double* d_off = nullptr;      // FP32: per-substrate field offsets [S]
   void* d_shift = nullptr;      // FP32: RN32(c2 * off) [S]
   int* d_active = nullptr;
@@ -134,6 +135,7 @@ inline SweepParams<T> make_params(bfvm_ctx* c, bool sources) {
     p.ae2 = c->d_ac + 2 * S * c->n_agents;
     p.n_sorted = c->n_agents;
   }
+  p.screen = c->screen;
   p.status = c->d_status;
   return p;
 }

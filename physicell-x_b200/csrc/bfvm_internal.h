@@ -87,6 +87,9 @@ struct SweepParams {
   const double* ac2;
   const double* ae2;
   int n_sorted;
+  // Nonzero when no substrate has a negative diffusion coefficient or decay
+  // rate (c1 >= 0, every denominator >= 1): enables the FP64 input screen.
+  int screen;
   int* status;           // device status word
 };
 

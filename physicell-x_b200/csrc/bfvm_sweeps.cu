@@ -77,10 +77,34 @@ __device__ __forceinline__ double markstein(double t, double d, double r) {
   return __fma_rn(e, r, q0);
 }
 
+// FP64 forward batch.  With c1 >= 0 and every denominator >= 1 (screen set:
+// no negative diffusion or decay), a batch whose incoming value is not
+// negative and whose inputs are all >= 2^-960 has every numerator
+// t = fma(c1, y, v) >= 2^-960, where the Markstein quotient is exact: such
+// batches (checked on the inputs, off the chain) run the bare chain.  Other
+// batches check each numerator and redo the batch with IEEE division if one
+// is -0 or a nonzero value below 2^-960.
 template <int B>
 __device__ __forceinline__ double forward_batch(const double (&v)[B], const double2 (&cf)[B], double c1, double,
-                                                double y, double (&out)[B]) {
+                                                int screen, double y, double (&out)[B]) {
   const double y0 = y;
+  double mn[B];
+#pragma unroll
+  for (int q = 0; q < B; ++q) mn[q] = v[q];
+#pragma unroll
+  for (int w = B / 2; w >= 1; w /= 2) {
+#pragma unroll
+    for (int q = 0; q < w; ++q) mn[q] = fmin(mn[q], mn[q + w]);
+  }
+  const bool clean = screen != 0 && !(y0 < 0.0) && mn[0] >= 0x1p-960;
+  if (__all_sync(__activemask(), clean)) {
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      y = markstein(__fma_rn(c1, y, v[q]), cf[q].x, cf[q].y);
+      out[q] = y;
+    }
+    return y;
+  }
   bool slow = false;
 #pragma unroll
   for (int q = 0; q < B; ++q) {
@@ -103,7 +127,7 @@ __device__ __forceinline__ double forward_batch(const double (&v)[B], const doub
 
 template <int B>
 __device__ __forceinline__ float forward_batch(const float (&v)[B], const float2 (&cf)[B], float2 c1, float shift,
-                                               float y, float (&out)[B]) {
+                                               int, float y, float (&out)[B]) {
 #pragma unroll
   for (int q = 0; q < B; ++q) {
     const float t = __fmaf_rn(c1.x, y, __fmaf_rn(c1.y, y, v[q] - shift));
@@ -241,9 +265,18 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   const CU* __restrict__ cup = p.ax.cu + static_cast<size_t>(s) * p.ax.npad;
   const typename Coef<T>::C1 c1 = p.c1[s];
   const T shift = kF32<T> ? p.shift[s] : T(0);
-  DR cfn[W];  // coefficients of the next chunk, loaded one chunk ahead
+  // Coefficients of the forward pass: two register buffers used in turn, the
+  // idle one loaded with the chunk after next (rows are padded past C * W).
+  DR cfa[W], cfb[W];
 #pragma unroll
-  for (int q = 0; q < W; ++q) cfn[q] = __ldg(drp + q);
+  for (int q = 0; q < W; ++q) {
+    cfa[q] = __ldg(drp + q);
+    cfb[q] = __ldg(drp + W + q);
+  }
+  // The upper-diagonal row for the back substitution, staged after the tile
+  // (read back after the barrier that ends the forward pass).
+  CU* cus = reinterpret_cast<CU*>(tile + C * chunk_bytes);
+  for (int q = t; q < C * W; q += TL) cus[q] = __ldg(cup + q);
 
   unsigned char* row = tile + t * 128;
   const int sw = t & 7;
@@ -309,16 +342,10 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   // past nx in the last chunk are TMA fill; the chain may run over them
   // harmlessly (those results are never stored to the field).
   T y = T(-0.0);
-  for (int c = 0; c < C; ++c) {
+  const int screen = p.screen;
+  auto fwd = [&](int c, DR (&cf)[W]) {
     if (!all_landed && ok) ok = mbar_wait(smem_u32(&bars[c]), static_cast<uint32_t>(phase >> c) & 1u);
-    DR cf[W];
-#pragma unroll
-    for (int q = 0; q < W; ++q) cf[q] = cfn[q];
-    if (c + 1 < C) {
-#pragma unroll
-      for (int q = 0; q < W; ++q) cfn[q] = __ldg(drp + (c + 1) * W + q);
-    }
-    if (face) continue;
+    if (face) return;
     unsigned char* crow = row + c * chunk_bytes;
     const int i0 = c * W;
     // The pin before the sweep, on the staged row (after the sources).
@@ -328,8 +355,17 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
     }
     T v[W], out[W];
     load_row<T, W>(crow, sw, v);
-    y = forward_batch<W>(v, cf, c1, shift, y, out);
+    y = forward_batch<W>(v, cf, c1, shift, screen, y, out);
     store_row<T, W>(crow, sw, out);
+  };
+  for (int c = 0; c < C; c += 2) {
+    fwd(c, cfa);
+#pragma unroll
+    for (int q = 0; q < W; ++q) cfa[q] = __ldg(drp + (c + 2) * W + q);
+    if (c + 1 >= C) break;
+    fwd(c + 1, cfb);
+#pragma unroll
+    for (int q = 0; q < W; ++q) cfb[q] = __ldg(drp + (c + 3) * W + q);
   }
   phase ^= chunk_mask(C);
   if (__syncthreads_or(!ok)) {
@@ -338,20 +374,13 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   }
 
   // Back substitution, last chunk first; each finished chunk is stored at once.
-  CU cwn[W];
-#pragma unroll
-  for (int q = 0; q < W; ++q) cwn[q] = __ldg(cup + (C - 1) * W + q);
   T xn = T(-0.0);
   for (int c = C - 1; c >= 0; --c) {
     unsigned char* crow = row + c * chunk_bytes;
     const int i0 = c * W;
     CU cw[W];
 #pragma unroll
-    for (int q = 0; q < W; ++q) cw[q] = cwn[q];
-    if (c > 0) {
-#pragma unroll
-      for (int q = 0; q < W; ++q) cwn[q] = __ldg(cup + (c - 1) * W + q);
-    }
+    for (int q = 0; q < W; ++q) cw[q] = cus[i0 + q];
     if (face) {
       T fw[W];
 #pragma unroll
@@ -418,13 +447,12 @@ constexpr int kRowBatch = 16;  // rows staged in registers per batch of the recu
 // One y- or z-sweep tile: the lines (i0 .. i0+TI-1, m, s), TI = blockDim.x,
 // m = k for the y sweep and j for the z sweep, staged in TMA boxes of CH rows.
 // Shared-memory layout and contract as for x_tile (base 128-byte aligned).
-template <typename T, int AXIS>
+template <typename T, int AXIS, int TI>
 __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0, int m, int s, int CH,
                         unsigned char* base, uint64_t& phase) {
   using DR = typename Coef<T>::DR;
   using CU = typename Coef<T>::CU;
   constexpr int R = kRowBatch;
-  const int TI = blockDim.x;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int n = (AXIS == 1) ? ny : nz;
   const bool act = p.active[s] != 0;
@@ -460,34 +488,40 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
   const CU* __restrict__ cup = ac.cu + static_cast<size_t>(s) * ac.npad;
   const typename Coef<T>::C1 c1 = p.c1[s];
   const T shift = kF32<T> ? p.shift[s] : T(0);
-  DR cfn[R];  // coefficients of the next batch, loaded one batch ahead
+  const int screen = p.screen;
+  // Coefficients of the forward pass: two register buffers used in turn, the
+  // idle one loaded with the batch after next.
+  DR cfa[R], cfb[R];
 #pragma unroll
-  for (int q = 0; q < R; ++q) cfn[q] = __ldg(drp + q);
+  for (int q = 0; q < R; ++q) {
+    cfa[q] = __ldg(drp + q);
+    cfb[q] = __ldg(drp + R + q);
+  }
+  // The upper-diagonal row for the back substitution, staged after the tile
+  // (read back after the barrier that ends the forward pass).
+  const int rows = (C * CH + R - 1) / R * R;
+  CU* cus = reinterpret_cast<CU*>(tile + static_cast<size_t>(rows) * TI);
+  for (int q = t; q < rows; q += TI) cus[q] = __ldg(cup + q);
   T* col = tile + t;
   bool ok = true;
-  int waited = 0;  // chunks whose TMA load this thread has waited for
+  int waited = 0;     // chunks whose TMA load this thread has waited for
+  int wait_row = 0;   // first row of chunk `waited`
   // The two end voxels of the line lie in the y (z) faces: the pin after the
   // sweep restores their input values.
   T e0v = T(0), e1v = T(0);
-
-  // Forward elimination in batches of R rows; a batch first waits for the
-  // chunks that cover it.  The tile holds a whole number of batches, so the
-  // last batch may read rows past n (TMA fill or unused rows): those results
-  // are never stored to the field.
   T y = T(-0.0);
-  for (int rb = 0; rb < n; rb += R) {
-    const int need = min(C, (rb + R + CH - 1) / CH);
-    while (waited < need) {
+
+  // One forward batch of R rows from rb, after waiting for the chunks that
+  // cover it.  The tile holds a whole number of batches, so the last batch
+  // may read rows past n (TMA fill or unused rows): those results are never
+  // stored to the field.
+  auto fwd = [&](int rb, DR (&cf)[R]) {
+    while (waited < C && wait_row < rb + R) {
       if (ok) ok = mbar_wait(smem_u32(&bars[waited]), static_cast<uint32_t>(phase >> waited) & 1u);
       ++waited;
+      wait_row += CH;
     }
-    DR cf[R];
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      cf[q] = cfn[q];
-      cfn[q] = __ldg(drp + rb + R + q);
-    }
-    if (face) continue;
+    if (face) return;
     T v[R], out[R];
     T* cb = col + rb * TI;
 #pragma unroll
@@ -500,9 +534,18 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
           if (rb + q == n - 1) e1v = v[q];
       }
     }
-    y = forward_batch<R>(v, cf, c1, shift, y, out);
+    y = forward_batch<R>(v, cf, c1, shift, screen, y, out);
 #pragma unroll
     for (int q = 0; q < R; ++q) cb[q * TI] = out[q];
+  };
+  for (int rb = 0; rb < n; rb += 2 * R) {
+    fwd(rb, cfa);
+#pragma unroll
+    for (int q = 0; q < R; ++q) cfa[q] = __ldg(drp + rb + 2 * R + q);
+    if (rb + R >= n) break;
+    fwd(rb + R, cfb);
+#pragma unroll
+    for (int q = 0; q < R; ++q) cfb[q] = __ldg(drp + rb + 3 * R + q);
   }
   while (waited < C) {
     if (ok) ok = mbar_wait(smem_u32(&bars[waited]), static_cast<uint32_t>(phase >> waited) & 1u);
@@ -518,23 +561,19 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
   // once every row from its start on is final.
   T xn = T(-0.0);
   int next_store = C - 1;
+  int store_row = next_store * CH;  // first row of chunk next_store
   const int last_b = ((n - 1) / R) * R;
-  CU cwn[R];
-#pragma unroll
-  for (int q = 0; q < R; ++q) cwn[q] = __ldg(cup + last_b + q);
   for (int rb = last_b; rb >= 0; rb -= R) {
-    CU cw[R];
-#pragma unroll
-    for (int q = 0; q < R; ++q) cw[q] = cwn[q];
-    if (rb > 0) {
-#pragma unroll
-      for (int q = 0; q < R; ++q) cwn[q] = __ldg(cup + rb - R + q);
-    }
     if (!face) {
       T* cb = col + rb * TI;
+      const CU* cwp = cus + rb;
       T v[R];
+      CU cw[R];
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
+      for (int q = 0; q < R; ++q) {
+        v[q] = cb[q * TI];
+        cw[q] = cwp[q];
+      }
       if (rb == last_b) {
 #pragma unroll
         for (int q = R - 1; q >= 0; --q) {
@@ -558,7 +597,7 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
       }
     }
     // store every chunk whose rows are now all final (uniform across the CTA)
-    if (next_store >= 0 && next_store * CH >= rb) {
+    if (next_store >= 0 && store_row >= rb) {
       fence_async_smem();
       __syncthreads();
       if (t == 0) {
@@ -571,15 +610,18 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
         }
         tma_store_commit();
       }
-      while (next_store >= 0 && next_store * CH >= rb) --next_store;
+      while (next_store >= 0 && store_row >= rb) {
+        --next_store;
+        store_row -= CH;
+      }
     }
   }
   return true;
 }
 
-template <typename T, int AXIS>
-__global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<T> p,
-                                                       int CH) {
+template <typename T, int AXIS, int TI>
+__global__ void __launch_bounds__(TI) sweep_yz_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<T> p,
+                                                      int CH) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + smem_align_pad(smem_raw, 128);
   const int n = (AXIS == 1) ? p.ny : p.nz;
@@ -591,7 +633,7 @@ __global__ void __launch_bounds__(256) sweep_yz_kernel(const __grid_constant__ C
   }
   __syncthreads();
   uint64_t phase = 0;
-  yz_tile<T, AXIS>(&map, p, blockIdx.x * blockDim.x, blockIdx.y, blockIdx.z, CH, base, phase);
+  yz_tile<T, AXIS, TI>(&map, p, blockIdx.x * TI, blockIdx.y, blockIdx.z, CH, base, phase);
   if (threadIdx.x == 0) tma_store_wait_read();
 }
 
@@ -684,12 +726,12 @@ __global__ void __launch_bounds__(kBatchTile) batch_step_kernel(const BatchHeade
       const int per = E.ntx * p.nz;
       const int s = tile / per, r = tile - s * per;
       const int k = r / E.ntx;
-      yz_tile<T, 1>(&E.my, p, (r - k * E.ntx) * kBatchTile, k, s, E.chy, base, phase);
+      yz_tile<T, 1, kBatchTile>(&E.my, p, (r - k * E.ntx) * kBatchTile, k, s, E.chy, base, phase);
     } else {
       const int per = E.ntx * p.ny;
       const int s = tile / per, r = tile - s * per;
       const int j = r / E.ntx;
-      yz_tile<T, 2>(&E.mz, p, (r - j * E.ntx) * kBatchTile, j, s, E.chz, base, phase);
+      yz_tile<T, 2, kBatchTile>(&E.mz, p, (r - j * E.ntx) * kBatchTile, j, s, E.chz, base, phase);
     }
     if (t == 0) {
       tma_store_wait_all();
@@ -742,12 +784,12 @@ __global__ void __launch_bounds__(kBatchTile) batch_sweep_kernel(const BatchHead
     const int per = E.ntx * p.nz;
     const int s = tile / per, r = tile - s * per;
     const int k = r / E.ntx;
-    yz_tile<T, 1>(&E.my, p, (r - k * E.ntx) * kBatchTile, k, s, E.chy, base, phase);
+    yz_tile<T, 1, kBatchTile>(&E.my, p, (r - k * E.ntx) * kBatchTile, k, s, E.chy, base, phase);
   } else {
     const int per = E.ntx * p.ny;
     const int s = tile / per, r = tile - s * per;
     const int j = r / E.ntx;
-    yz_tile<T, 2>(&E.mz, p, (r - j * E.ntx) * kBatchTile, j, s, E.chz, base, phase);
+    yz_tile<T, 2, kBatchTile>(&E.mz, p, (r - j * E.ntx) * kBatchTile, j, s, E.chz, base, phase);
   }
   if (threadIdx.x == 0) tma_store_wait_read();
 }
@@ -759,7 +801,8 @@ size_t sweep_x_smem(int elem_bytes, int nx, const SweepConfig& cfg) {
   const int W = 128 / elem_bytes;
   const int C = (nx + W - 1) / W;
   if (C > kMaxChunks) return ~size_t(0);
-  return 1024 + kBarrierBytes + static_cast<size_t>(C) * cfg.x_lines * 128;
+  // alignment pad, barriers, the tile, the staged upper-diagonal row
+  return 1024 + kBarrierBytes + static_cast<size_t>(C) * cfg.x_lines * 128 + static_cast<size_t>(C) * W * 8;
 }
 
 static int yz_chunk_rows(int n, int target) {
@@ -774,7 +817,8 @@ size_t sweep_yz_smem(int elem_bytes, int n_line, const SweepConfig& cfg) {
   const int C = (n_line + CH - 1) / CH;
   if (C > kMaxChunks) return ~size_t(0);
   const size_t rows = (static_cast<size_t>(C) * CH + kRowBatch - 1) / kRowBatch * kRowBatch;
-  return 128 + kBarrierBytes + rows * cfg.yz_tile * elem_bytes;
+  // alignment pad, barriers, the tile, the staged upper-diagonal row
+  return 128 + kBarrierBytes + rows * cfg.yz_tile * elem_bytes + rows * 8;
 }
 
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
@@ -823,24 +867,40 @@ cudaError_t launch_sweep_x(const FieldMaps& maps, const SweepParams<T>& p, const
   return cudaGetLastError();
 }
 
+// One y or z sweep launch with the tile width as a compile-time constant.
+template <typename T, int AXIS, int TI>
+static cudaError_t launch_yz(const CUtensorMap& map, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
+  const int n = (AXIS == 1) ? p.ny : p.nz;
+  const size_t smem = sweep_yz_smem(sizeof(T), n, cfg);
+  cudaError_t e = cudaFuncSetAttribute(sweep_yz_kernel<T, AXIS, TI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((p.nx + TI - 1) / TI, (AXIS == 1) ? p.nz : p.ny, p.S);
+  sweep_yz_kernel<T, AXIS, TI><<<grid, TI, smem, st>>>(map, p, yz_chunk_rows(n, cfg.yz_chunk));
+  return cudaGetLastError();
+}
+
+template <typename T, int AXIS>
+static cudaError_t launch_yz_any(const CUtensorMap& map, const SweepParams<T>& p, const SweepConfig& cfg,
+                                 cudaStream_t st) {
+  switch (cfg.yz_tile) {
+    case 16:
+      if constexpr (sizeof(T) == 8) return launch_yz<T, AXIS, 16>(map, p, cfg, st);
+      return cudaErrorInvalidValue;
+    case 32: return launch_yz<T, AXIS, 32>(map, p, cfg, st);
+    case 64: return launch_yz<T, AXIS, 64>(map, p, cfg, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 template <typename T>
 cudaError_t launch_sweep_y(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
-  const size_t smem = sweep_yz_smem(sizeof(T), p.ny, cfg);
-  cudaError_t e = cudaFuncSetAttribute(sweep_yz_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  dim3 grid((p.nx + cfg.yz_tile - 1) / cfg.yz_tile, p.nz, p.S);
-  sweep_yz_kernel<T, 1><<<grid, cfg.yz_tile, smem, st>>>(maps.y, p, yz_chunk_rows(p.ny, cfg.yz_chunk));
-  return cudaGetLastError();
+  return launch_yz_any<T, 1>(maps.y, p, cfg, st);
 }
 
 template <typename T>
 cudaError_t launch_sweep_z(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
-  const size_t smem = sweep_yz_smem(sizeof(T), p.nz, cfg);
-  cudaError_t e = cudaFuncSetAttribute(sweep_yz_kernel<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  dim3 grid((p.nx + cfg.yz_tile - 1) / cfg.yz_tile, p.ny, p.S);
-  sweep_yz_kernel<T, 2><<<grid, cfg.yz_tile, smem, st>>>(maps.z, p, yz_chunk_rows(p.nz, cfg.yz_chunk));
-  return cudaGetLastError();
+  return launch_yz_any<T, 2>(maps.z, p, cfg, st);
 }
 
 template cudaError_t launch_sweep_x<double>(const FieldMaps&, const SweepParams<double>&, const SweepConfig&,

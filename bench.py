@@ -2,7 +2,7 @@
 """Benchmark of the BioFVM 3-D diffusion-decay LOD step with cell sources.
 
 Metric: voxel*substrate updates per second per LOD step (N*S*steps / time).
-Workload (one GPU): config2 -- 200^3 voxels, dx=10 um, 4 substrates with
+Workload (one GPU): cube200 -- 200^3 voxels, dx=10 um, 4 substrates with
 log-uniform D in [1e2,1e5] and decay in [1e-3,1] (substrate 0 Dirichlet 38
 on all faces), 100,000 agents with uptake in [0,10] and secretion in [0,1],
 FP64, dt=0.01 min.  One bench step = one LOD step: agent sources fused into
@@ -38,19 +38,24 @@ sys.path.insert(0, os.path.join(ROOT, "physicell-x_b200"))
 
 METRIC = "voxel·substrate updates/s per LOD step"
 UNIT = "voxel·substrate updates/s"
-WORKLOAD = ("config2: 200x200x200 voxels (dx=10 um), 4 substrates, 100000 agents, FP64, dt=0.01 min; "
+WORKLOAD = ("cube200: 200x200x200 voxels (dx=10 um), 4 substrates, 100000 agents, FP64, dt=0.01 min; "
             "one LOD step = fused agent sources + x/y/z Thomas sweeps with Dirichlet pins")
 
-# DRAM bytes per launch of each sweep kernel from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum) on this workload; see
-# profiles/sweeps_config2_fp64.md for the command and the raw figures.
-NCU_TRAFFIC = {}
+# DRAM bytes per launch of each sweep kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum) from one ncu capture of this workload at the current
+# kernels; profiles/sweeps_cube200_fp64.txt gives the command and the raw
+# figures.  Keys: (precision, sweep index 0=x 1=y 2=z).
+NCU_TRAFFIC = {
+    ("fp64", 0): 279770112 + 198588672,
+    ("fp64", 1): 265704704 + 195987968,
+    ("fp64", 2): 265680640 + 195192576,
+}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -64,6 +69,18 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+def max_over_ranks(x, dist=None, device="cpu"):
+    """Largest value of x over all ranks (the job's time is its slowest
+    rank's); x itself when there is one process."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def load_peaks():
@@ -87,16 +104,25 @@ class ClockSampler:
         self.proc = None
 
     def __enter__(self):
+        self.lines = []
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-lms", "100", "-i", str(self.dev)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
+            # nvidia-smi takes a moment to start: wait for its first sample so the
+            # samples cover the whole timed region (at most 10 s).
+            import select
+
+            ready, _, _ = select.select([self.proc.stdout], [], [], 10.0)
+            if ready:
+                first = self.proc.stdout.readline()
+                if first.strip():
+                    self.lines.append(first)
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -104,7 +130,7 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
                 out = ""
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+            self.lines += [ln for ln in out.splitlines() if ln.strip()]
 
     def summary(self):
         sm, mx, reasons = [], None, set()
@@ -126,17 +152,21 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline_sample(wl, steps=2):
+def cpu_baseline_sample(wl, budget_s=10.0):
     """Time the reference's own CPU path (oracle/_ref, all host threads) on a
-    bounded sample of the workload; the C restatement if the reference build
-    is absent."""
+    bounded sample of the workload -- as many LOD steps as fit in about
+    budget_s seconds after one timed probe step; the C restatement if the
+    reference build is absent."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
 
     threads = pyoracle.max_threads()
     if pyoracle.Reference.available():
         ref = pyoracle.Reference(wl, threads=threads)
-        ref.run(1, solver=0, threads=threads, sources_threads=threads, fetch=False)  # first call: factorization
+        t0 = time.perf_counter()
+        ref.run(1, solver=0, threads=threads, sources_threads=threads, fetch=False)  # also does the factorization
+        probe = time.perf_counter() - t0
+        steps = int(max(2, min(200, budget_s / max(probe, 1e-3))))
         t0 = time.perf_counter()
         ref.run(steps, solver=0, threads=threads, sources_threads=threads, fetch=False)
         dt = time.perf_counter() - t0
@@ -146,6 +176,7 @@ def cpu_baseline_sample(wl, steps=2):
         field = wl.field0.copy()
         c1, c2, e2 = pyoracle.Port.workload_constants(wl)
         dv = wl.dirichlet_values
+        steps = 2
         t0 = time.perf_counter()
         for _ in range(steps):
             pyoracle.Port.sources(field, wl.S, wl.agent_voxel, c1, c2, e2)
@@ -153,7 +184,7 @@ def cpu_baseline_sample(wl, steps=2):
         dt = time.perf_counter() - t0
         kind = "port"
     return {"value": wl.n_values * steps / dt, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{steps} LOD steps of config2 (sources + _BLOCKING sweeps, OpenMP {threads} threads), "
+            "sample": f"{steps} LOD steps of cube200 (sources + _BLOCKING sweeps, OpenMP {threads} threads), "
                       f"{dt:.2f} s"}
 
 
@@ -163,7 +194,7 @@ def run_reference_arm(args):
         return 0
     from bfvm import workloads as W
 
-    wl = W.config2()
+    wl = W.cube200()
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
 
@@ -193,7 +224,7 @@ def run_reference_arm(args):
             "config": {"workload": WORKLOAD, "solver": "diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING",
                        "sources": f"simulate_cell_sources_and_sinks, OpenMP {threads} threads"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"{args.steps} timed LOD steps of config2 after {max(1, args.warmup)} warm-up"},
+                             "sample": f"{args.steps} timed LOD steps of cube200 after {max(1, args.warmup)} warm-up"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -222,7 +253,7 @@ def main():
     from bfvm import Microenvironment, kernel_launches
     from bfvm import workloads as W
 
-    wl = W.config2()
+    wl = W.cube200()
     me = Microenvironment.from_workload(wl, precision=args.precision, device=local)
     stream = torch.cuda.ExternalStream(me.stream, device=torch.device("cuda", local))
     N, S, A = wl.n_voxels, wl.S, wl.n_agents
@@ -256,9 +287,7 @@ def main():
     ms_xyz, nrec = me.timing_read()
     ms_step = ms_total / args.steps
     if dist is not None:
-        t = torch.tensor([ms_step], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
+        ms_step = max_over_ranks(ms_step, dist, "cuda")
     value = world * N * S / (ms_step * 1e-3)
 
     # ---- roofline of the dominant kernel -------------------------------------
@@ -309,9 +338,7 @@ def main():
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s, dist, "cuda")
     h2d = A * 4 + 3 * A * S * 8
     d2h = A * S * 8
     e2e = {"value": world * N * S / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

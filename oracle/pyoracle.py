@@ -17,8 +17,10 @@ indexed ``((i*ny + j)*nz + k)*S + d`` (BioFVM/BioFVM_mesh.cpp:1149-1158).
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
+import sys
 import time
 
 import numpy as np
@@ -140,6 +142,24 @@ class Port:
                                    wl.saturation, wl.net_export)
 
 
+@contextlib.contextmanager
+def _stdout_to_stderr():
+    """The reference prints its banner and progress lines on stdout; send them
+    to stderr so a caller's stdout carries only its own output."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    try:
+        os.dup2(2, 1)
+        yield
+    finally:
+        try:
+            C.CDLL(None).fflush(None)
+        except Exception:
+            pass
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 class Reference:
     """The reference's own BioFVM solver and agents, built from its sources."""
 
@@ -148,6 +168,11 @@ class Reference:
     def __init__(self, wl, threads=0, dropin=False):
         self.L = self.lib(dropin)
         self.wl = wl
+        with _stdout_to_stderr():
+            self._setup(wl)
+        self.threads = threads
+
+    def _setup(self, wl):
         nx, ny, nz, S = wl.shape
         self.h = self.L.ref_env_create(nx, ny, nz, wl.dx, wl.origin[0], wl.origin[1], wl.origin[2], S,
                                        _f64(wl.D), _f64(wl.decay))
@@ -163,7 +188,6 @@ class Reference:
                                            _f64(wl.secretion[a]), _f64(wl.uptake[a]), _f64(wl.saturation[a]),
                                            _f64(wl.net_export[a]))
             self.agent_index.append(idx)
-        self.threads = threads
 
     @classmethod
     def available(cls, dropin=False):
@@ -237,10 +261,12 @@ class Reference:
         return c1, c2, e2
 
     def sources(self, threads=1):
-        self.L.ref_env_sources(self.h, self.wl.dt, threads)
+        with _stdout_to_stderr():
+            self.L.ref_env_sources(self.h, self.wl.dt, threads)
 
     def diffusion(self, solver=0, threads=None):
-        rc = self.L.ref_env_diffusion(self.h, self.wl.dt, solver, self.threads if threads is None else threads)
+        with _stdout_to_stderr():
+            rc = self.L.ref_env_diffusion(self.h, self.wl.dt, solver, self.threads if threads is None else threads)
         if rc != 0:
             raise RuntimeError(f"ref_env_diffusion solver={solver} rc={rc}")
 
@@ -249,8 +275,9 @@ class Reference:
 
     def run(self, nsteps=None, solver=0, threads=None, sources_threads=1, fetch=True):
         nsteps = self.wl.steps if nsteps is None else nsteps
-        rc = self.L.ref_env_run(self.h, self.wl.dt, nsteps, solver, self.threads if threads is None else threads,
-                                sources_threads)
+        with _stdout_to_stderr():
+            rc = self.L.ref_env_run(self.h, self.wl.dt, nsteps, solver, self.threads if threads is None else threads,
+                                    sources_threads)
         if rc != 0:
             raise RuntimeError(f"ref_env_run rc={rc}")
         return self.field() if fetch else None

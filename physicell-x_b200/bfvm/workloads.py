@@ -6,15 +6,15 @@ field and a list of point agents with secretion/uptake/export rates.  The
 shapes and value distributions follow the benchmark configurations of the
 diffusion-decay path:
 
-* ``config1`` -- 50^3 voxels, dx=20 um, 2 substrates (oxygen-like Dirichlet
+* ``cube50`` -- 50^3 voxels, dx=20 um, 2 substrates (oxygen-like Dirichlet
   38 on all faces; a zero-flux secreted substrate), 2,000 uniform agents,
   dt=0.01 min, 1000 steps.
-* ``config2`` -- 200^3, dx=10 um, 4 substrates with log-uniform D in
+* ``cube200`` -- 200^3, dx=10 um, 4 substrates with log-uniform D in
   [1e2,1e5] and decay in [1e-3,1]; substrate 0 Dirichlet 38; 100,000 uniform
   agents with per-agent uptake in [0,10] and secretion in [0,1]; 500 steps.
-* ``config3`` -- 640^3, dx=10 um, the two substrates of config1, 1,000,000
+* ``cube640`` -- 640^3, dx=10 um, the two substrates of cube50, 1,000,000
   agents in a Gaussian ball (sigma 1500 um) clamped into the box; 1000 steps.
-* ``config4_env`` / ``config5_request`` -- the uneven environments of the
+* ``uneven_env`` / ``serve_request`` -- the uneven environments of the
   batched and serving workloads (edges 24-128 / 32-256, 1-6 / 1-8 substrates,
   random Dirichlet activation and per-face values, 0-20k / 0-200k agents).
 
@@ -211,7 +211,7 @@ def make(name, nx, ny, nz, S, dx, dt, steps, D, decay, active, face_values, n_ag
 
 
 def _two_substrate(name, n, dx, steps, n_agents, seed, agent_mode="uniform", sigma=None):
-    """The two substrates of configs 1 and 3: oxygen-like (D=1e5, decay 0.1,
+    """The two substrates of cube50 and cube640: oxygen-like (D=1e5, decay 0.1,
     Dirichlet 38 on all faces, initial 38) and a zero-flux secreted substrate
     (D=1e3, decay 0.01, initial noise in [0, 0.1)).  Agents take up substrate
     0 at 10/min and secrete substrate 1 at 1/min towards saturation 1."""
@@ -232,15 +232,15 @@ def _two_substrate(name, n, dx, steps, n_agents, seed, agent_mode="uniform", sig
                 init_kind=[("const", 38.0), ("uniform", 0.0, 0.1)])
 
 
-def config1(seed=1, steps=1000, n=50, n_agents=2000):
-    return _two_substrate("config1", n, 20.0, steps, n_agents, seed)
+def cube50(seed=1, steps=1000, n=50, n_agents=2000):
+    return _two_substrate("cube50", n, 20.0, steps, n_agents, seed)
 
 
-def config3(seed=3, steps=1000, n=640, n_agents=1_000_000):
-    return _two_substrate("config3", n, 10.0, steps, n_agents, seed, agent_mode="gauss", sigma=1500.0 * n / 640)
+def cube640(seed=3, steps=1000, n=640, n_agents=1_000_000):
+    return _two_substrate("cube640", n, 10.0, steps, n_agents, seed, agent_mode="gauss", sigma=1500.0 * n / 640)
 
 
-def config2(seed=2, steps=500, n=200, n_agents=100_000, S=4):
+def cube200(seed=2, steps=500, n=200, n_agents=100_000, S=4):
     rng = np.random.Generator(np.random.PCG64(seed + 1000))
     D = _loguniform(rng, 1e2, 1e5, S)
     decay = _loguniform(rng, 1e-3, 1.0, S)
@@ -249,7 +249,7 @@ def config2(seed=2, steps=500, n=200, n_agents=100_000, S=4):
     fv = np.ones((6, S))
     fv[:, 0] = 38.0
     init = [("const", 38.0)] + [("uniform", 0.0, 1.0)] * (S - 1)
-    return make("config2", n, n, n, S, 10.0, 0.01, steps, D, decay, active, fv, n_agents, seed,
+    return make("cube200", n, n, n, S, 10.0, 0.01, steps, D, decay, active, fv, n_agents, seed,
                 uptake=lambda r, m: r.uniform(0.0, 10.0, (m, S)),
                 secretion=lambda r, m: r.uniform(0.0, 1.0, (m, S)), init_kind=init)
 
@@ -273,19 +273,19 @@ def _random_env(name, rng, seed, edge_lo, edge_hi, s_lo, s_hi, agents_hi, steps,
                 secretion=lambda r, m: r.uniform(0.0, 1.0, (m, S)), init_kind=init)
 
 
-def config4_env(index, seed=4, steps=200, agents_hi=20_000):
+def uneven_env(index, seed=4, steps=200, agents_hi=20_000):
     rng = np.random.Generator(np.random.PCG64([seed, index]))
-    return _random_env(f"config4[{index}]", rng, seed * 100003 + index, 24, 128, 1, 6, agents_hi, steps)
+    return _random_env(f"uneven[{index}]", rng, seed * 100003 + index, 24, 128, 1, 6, agents_hi, steps)
 
 
-def config4(n_envs=256, seed=4, steps=200, agents_hi=20_000):
-    return [config4_env(i, seed, steps, agents_hi) for i in range(n_envs)]
+def uneven_batch(n_envs=256, seed=4, steps=200, agents_hi=20_000):
+    return [uneven_env(i, seed, steps, agents_hi) for i in range(n_envs)]
 
 
-def config5_request(index, seed=5, steps_lo=100, steps_hi=10_000, agents_hi=200_000, edge_lo=32,
+def serve_request(index, seed=5, steps_lo=100, steps_hi=10_000, agents_hi=200_000, edge_lo=32,
                     edge_hi=256):
     rng = np.random.Generator(np.random.PCG64([seed, index]))
-    return _random_env(f"config5[{index}]", rng, seed * 100003 + index, edge_lo, edge_hi, 1, 8, agents_hi,
+    return _random_env(f"request[{index}]", rng, seed * 100003 + index, edge_lo, edge_hi, 1, 8, agents_hi,
                        steps_lo, dx=10.0, steps_hi=steps_hi)
 
 

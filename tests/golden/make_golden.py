@@ -54,12 +54,12 @@ def small_cases():
 def build(kind, kw):
     if kind == "small":
         return W.small_random(**kw)
-    if kind == "config1":
-        return W.config1(**kw)
-    if kind == "config2":
-        return W.config2(**kw)
-    if kind == "config4_env":
-        return W.config4_env(**kw)
+    if kind == "cube50":
+        return W.cube50(**kw)
+    if kind == "cube200":
+        return W.cube200(**kw)
+    if kind == "uneven_env":
+        return W.uneven_env(**kw)
     raise ValueError(kind)
 
 
@@ -88,7 +88,7 @@ def main():
         manifest.append(name)
         print(name, wl.shape, wl.n_agents, "agents")
 
-    big = [("config1", dict(steps=1000)), ("config2", dict(steps=10)), ("config4_env", dict(index=7, steps=50))]
+    big = [("cube50", dict(steps=1000)), ("cube200", dict(steps=10)), ("uneven_env", dict(index=7, steps=50))]
     rng = np.random.Generator(np.random.PCG64(2024))
     for kind, kw in big:
         wl = build(kind, kw)

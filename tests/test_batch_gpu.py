@@ -100,10 +100,10 @@ def test_batch_autotune_keeps_fields():
         assert np.array_equal(me.download_field(), Port.run(wl))
 
 
-def test_config4_sized_batch_runs():
-    """A slice of the config4 workload (uneven 24-128 edges, 1-6 substrates,
+def test_uneven_batch_slice_runs():
+    """A slice of the uneven_batch workload (uneven 24-128 edges, 1-6 substrates,
     random Dirichlet faces): a few fused steps, checked against solo runs."""
-    wls = W.config4(n_envs=6, steps=3, agents_hi=2000)
+    wls = W.uneven_batch(n_envs=6, steps=3, agents_hi=2000)
     batch = Batch("fp64")
     mes = []
     for wl in wls:

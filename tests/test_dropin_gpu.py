@@ -48,8 +48,8 @@ def test_dropin_fused_sources_bitwise():
     assert np.array_equal(a, gpu.field())
 
 
-def test_dropin_config1_hundred_steps():
-    wl = W.config1(steps=100)
+def test_dropin_cube50_hundred_steps():
+    wl = W.cube50(steps=100)
     cpu, gpu = _pair(wl)
     a = cpu.run(wl.steps, solver=0, sources_threads=1)
     b = gpu.run(wl.steps, solver=2, sources_threads=1)

@@ -62,11 +62,11 @@ def test_port_agent_constants_match_goldens(golden_dir):
         assert np.array_equal(c1, g["c1"]) and np.array_equal(c2, g["c2"]) and np.array_equal(e2, g["e2"]), name
 
 
-def test_port_matches_config1_golden_hash(golden_dir):
-    """config1 (50^3 x 2, 2000 agents) for all 1000 steps: bit-identical to the
+def test_port_matches_cube50_golden_hash(golden_dir):
+    """cube50 (50^3 x 2, 2000 agents) for all 1000 steps: bit-identical to the
     reference's own solver (SHA-256 of the final field)."""
-    g = _load(golden_dir, "config1_1000")
-    wl = W.config1(steps=1000)
+    g = _load(golden_dir, "cube50_1000")
+    wl = W.cube50(steps=1000)
     assert _sha(wl.field0) == str(g["field0_sha"])
     assert _sha(wl.agent_voxel) == str(g["voxel_sha"])
     field = wl.field0.copy()
@@ -81,9 +81,9 @@ def test_port_matches_config1_golden_hash(golden_dir):
     assert np.array_equal(field[g["sample_idx"]], g["sample_val"])
 
 
-def test_port_matches_config4_env_golden_hash(golden_dir):
-    g = _load(golden_dir, "config4_env_50")
-    wl = W.config4_env(index=7, steps=50)
+def test_port_matches_uneven_env_golden_hash(golden_dir):
+    g = _load(golden_dir, "uneven_env_50")
+    wl = W.uneven_env(index=7, steps=50)
     assert _sha(wl.field0) == str(g["field0_sha"])
     field = wl.field0.copy()
     c1, c2, e2 = Port.agent_constants(wl.dt, wl.agent_volume, wl.voxel_volume, wl.secretion, wl.uptake,

@@ -60,11 +60,11 @@ def test_small_goldens_bitwise(golden_dir):
         assert bad.size == 0, f"{name}: {bad.size} values differ, first {bad[:5]}"
 
 
-def test_config1_full_run_matches_reference_hash(golden_dir):
-    """config1 (50^3 x 2 substrates, 2000 agents), all 1000 LOD steps with fused
+def test_cube50_full_run_matches_reference_hash(golden_dir):
+    """cube50 (50^3 x 2 substrates, 2000 agents), all 1000 LOD steps with fused
     sources: the final field is bit-identical to the reference's."""
-    g = _load(golden_dir, "config1_1000")
-    wl = W.config1(steps=1000)
+    g = _load(golden_dir, "cube50_1000")
+    wl = W.cube50(steps=1000)
     assert _sha(wl.field0) == str(g["field0_sha"])
     me = Microenvironment.from_workload(wl)
     me.simulate_diffusion_decay(wl.steps, sources=True)
@@ -73,8 +73,8 @@ def test_config1_full_run_matches_reference_hash(golden_dir):
     assert _sha(out) == str(g["final_sha"])
 
 
-def test_config2_and_config4_env_match_reference_hash(golden_dir):
-    for name, wl in (("config2_10", W.config2(steps=10)), ("config4_env_50", W.config4_env(index=7, steps=50))):
+def test_cube200_and_uneven_env_match_reference_hash(golden_dir):
+    for name, wl in (("cube200_10", W.cube200(steps=10)), ("uneven_env_50", W.uneven_env(index=7, steps=50))):
         g = _load(golden_dir, name)
         assert _sha(wl.field0) == str(g["field0_sha"])
         me = Microenvironment.from_workload(wl)
@@ -203,10 +203,10 @@ def test_device_pointer_upload_matches_host_upload():
     assert np.array_equal(a.download_field(), out.cpu().numpy())
 
 
-def test_kat_uniform_field_at_config2_size():
-    """Size-independent property at the full config2 grid (200^3 x 4): a
+def test_kat_uniform_field_at_cube200_size():
+    """Size-independent property at the full cube200 grid (200^3 x 4): a
     uniform zero-flux field divides by (1 + dt*lambda/3)^3 per step."""
-    wl = W.config2(n_agents=0, steps=3)
+    wl = W.cube200(n_agents=0, steps=3)
     me = Microenvironment(wl.nx, wl.ny, wl.nz, wl.dx, wl.dt, wl.D, wl.decay)
     me.set_dirichlet_activation(np.zeros(wl.S, np.uint8))
     me.upload_field(np.full(wl.n_values, 5.0))
@@ -226,8 +226,8 @@ def test_fp32_within_tolerance_small(seed):
     assert np.all(err <= FP32_TOL), err
 
 
-def test_fp32_config1_full_run_within_tolerance():
-    wl = W.config1(steps=1000)
+def test_fp32_cube50_full_run_within_tolerance():
+    wl = W.cube50(steps=1000)
     ref = Port.run(wl)
     me = Microenvironment.from_workload(wl, precision="fp32")
     me.simulate_diffusion_decay(wl.steps, sources=True)

@@ -190,8 +190,20 @@ int bfvm_device_field(bfvm_ctx* ctx, void** ptr, int* pitch, int* elem_bytes);
  * the last field upload.  Uploads, downloads, sampling and sums apply them. */
 int bfvm_field_offsets(bfvm_ctx* ctx, double* offsets);
 
-/* Bytes of device memory the solve holds (field, coefficients, agents). */
+/* Bytes of device memory the solve holds now (field, coefficients, agents,
+ * host-transfer staging). */
 size_t bfvm_device_bytes(bfvm_ctx* ctx);
+
+/* Bytes that bfvm_create(cfg), one host field upload and bfvm_set_agents with
+ * n_agents agents would request -- for admission against a device-memory
+ * budget before anything is allocated (0 for an invalid configuration).  No
+ * counterpart in the reference, which has no device memory. */
+size_t bfvm_estimate_bytes(const bfvm_config* cfg, int n_agents);
+
+/* Free the buffer that host uploads and downloads stage the reference-layout
+ * field in (as large as an FP64 copy of the field); the next host transfer
+ * allocates it again.  No counterpart in the reference. */
+int bfvm_release_staging(bfvm_ctx* ctx);
 
 /* Launch shape of the sweeps: lines per CTA in the x sweep (a multiple of 8,
  * at most 256), x extent per CTA in the y/z sweeps (16 -- FP64 only --, 32 or

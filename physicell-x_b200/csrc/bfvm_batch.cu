@@ -43,6 +43,10 @@ struct bfvm_batch {
   int items[3] = {0, 0, 0};
   size_t axis_smem[3] = {0, 0, 0};
   bool built_sources = false;
+  // The device tables are rebuilt only when the membership, the schedule, the
+  // sources flag or a member's device pointers (bfvm_ctx::version) changed.
+  bool dirty = true;
+  std::vector<int> versions;
   // captured graph of graph_steps steps
   cudaGraphExec_t gexec = nullptr;
   size_t g_smem = 0;
@@ -248,7 +252,14 @@ int step_impl(bfvm_batch* b, int nsteps, bool sources) {
   if (b->members.empty() || nsteps == 0) return BFVM_OK;
   int rc = join_members(b);
   if (rc != BFVM_OK) return rc;
-  if ((rc = build_tables<T>(b, sources)) != BFVM_OK) return rc;
+  bool rebuild = b->dirty || sources != b->built_sources || b->versions.size() != b->members.size();
+  for (size_t q = 0; !rebuild && q < b->members.size(); ++q) rebuild = b->versions[q] != b->members[q]->version;
+  if (rebuild) {
+    if ((rc = build_tables<T>(b, sources)) != BFVM_OK) return rc;
+    b->versions.resize(b->members.size());
+    for (size_t q = 0; q < b->members.size(); ++q) b->versions[q] = b->members[q]->version;
+    b->dirty = false;
+  }
   int left = nsteps;
   if (b->graph_steps > 1 && nsteps >= b->graph_steps) {
     if (!b->gexec || b->g_steps != b->graph_steps || b->g_smem != b->smem || b->g_grid != b->grid ||
@@ -321,6 +332,7 @@ int bfvm_batch_add(bfvm_batch* b, bfvm_ctx* c) {
   if (std::find(b->members.begin(), b->members.end(), c) != b->members.end()) return BFVM_ERR_STATE;
   if (batch_member_smem(c->eb, c->nx, c->ny, c->nz, b->yz_chunk) > 227 * 1024) return BFVM_ERR_SHAPE;
   b->members.push_back(c);
+  b->dirty = true;
   return BFVM_OK;
 }
 
@@ -333,6 +345,7 @@ int bfvm_batch_remove(bfvm_batch* b, bfvm_ctx* c) {
   BFVM_CUDA(cudaEventRecord(b->ev, b->stream));
   BFVM_CUDA(cudaStreamWaitEvent(c->stream, b->ev, 0));
   b->members.erase(it);
+  b->dirty = true;
   return BFVM_OK;
 }
 
@@ -376,6 +389,7 @@ int bfvm_batch_set_schedule(bfvm_batch* b, int mode, int yz_chunk, int order, in
   b->order = order;
   b->ctas_per_sm = ctas_per_sm;
   b->graph_steps = graph_steps;
+  b->dirty = true;
   drop_graph(b);
   return BFVM_OK;
 }

@@ -216,17 +216,17 @@ size_t face_elems(const bfvm_ctx* c) {
 }
 
 int free_agents(bfvm_ctx* c) {
-  dfree(c->d_voxel);
-  dfree(c->d_agent_active);
-  dfree(c->d_c);
-  dfree(c->d_rates);
-  dfree(c->d_dev_voxel);
-  dfree(c->d_sorted_keys);
-  dfree(c->d_sorted_vals);
-  dfree(c->d_a_i);
-  dfree(c->d_ac);
-  dfree(c->d_agent_scratch);
-  dfree(c->d_sample);
+  dfree(c, c->d_voxel);
+  dfree(c, c->d_agent_active);
+  dfree(c, c->d_c);
+  dfree(c, c->d_rates);
+  dfree(c, c->d_dev_voxel);
+  dfree(c, c->d_sorted_keys);
+  dfree(c, c->d_sorted_vals);
+  dfree(c, c->d_a_i);
+  dfree(c, c->d_ac);
+  dfree(c, c->d_agent_scratch);
+  dfree(c, c->d_sample);
   c->d_voxel = nullptr;
   c->d_agent_active = nullptr;
   c->d_c = c->d_rates = c->d_ac = c->d_sample = nullptr;
@@ -234,6 +234,7 @@ int free_agents(bfvm_ctx* c) {
   c->d_sorted_vals = c->d_a_i = nullptr;
   c->d_agent_scratch = nullptr;
   c->cap_agents = 0;
+  ++c->version;
   return BFVM_OK;
 }
 
@@ -289,6 +290,7 @@ int build_agents(bfvm_ctx* c, int n) {
   BFVM_CUDA(agents_build(b, c->stream, &launches));
   note_launches(launches);
   c->n_agents = n;
+  ++c->version;
   return BFVM_OK;
 }
 
@@ -394,18 +396,18 @@ int bfvm_destroy(bfvm_ctx* c) {
   DeviceGuard g(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_agents(c);
-  dfree(c->f);
-  dfree(c->d_coef);
-  dfree(c->d_c1);
-  dfree(c->d_off);
-  dfree(c->d_shift);
-  dfree(c->d_active);
-  dfree(c->d_faces);
-  dfree(c->d_status);
-  dfree(c->d_nvalid);
-  dfree(c->d_line_off);
-  dfree(c->d_sums);
-  dfree(c->d_staging);
+  dfree(c, c->f);
+  dfree(c, c->d_coef);
+  dfree(c, c->d_c1);
+  dfree(c, c->d_off);
+  dfree(c, c->d_shift);
+  dfree(c, c->d_active);
+  dfree(c, c->d_faces);
+  dfree(c, c->d_status);
+  dfree(c, c->d_nvalid);
+  dfree(c, c->d_line_off);
+  dfree(c, c->d_sums);
+  dfree(c, c->d_staging);
   for (cudaEvent_t e : c->events) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -807,6 +809,49 @@ extern "C" int bfvm_device_field(bfvm_ctx* c, void** ptr, int* pitch, int* elem_
 }
 
 extern "C" size_t bfvm_device_bytes(bfvm_ctx* c) { return c ? c->device_bytes : 0; }
+
+// Bytes bfvm_create + one host field upload + bfvm_set_agents(n_agents) would
+// request, computed from the same sizes those calls allocate.
+extern "C" size_t bfvm_estimate_bytes(const bfvm_config* cfg, int n_agents) {
+  if (!cfg || cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1 || cfg->n_substrates < 1 || n_agents < 0 ||
+      (cfg->precision != BFVM_FP64 && cfg->precision != BFVM_FP32))
+    return 0;
+  bfvm_ctx c;
+  c.nx = cfg->nx;
+  c.ny = cfg->ny;
+  c.nz = cfg->nz;
+  c.S = cfg->n_substrates;
+  c.prec = cfg->precision;
+  c.eb = c.prec == BFVM_FP64 ? 8 : 4;
+  const int row_align = 128 / c.eb;
+  c.nxp = (c.nx + row_align - 1) / row_align * row_align;
+  const size_t S = c.S;
+  const size_t nvox = static_cast<size_t>(c.nx) * c.ny * c.nz;
+  size_t dr[3], cu[3];
+  size_t b = static_cast<size_t>(c.nxp) * c.ny * c.nz * S * c.eb;  // field
+  b += coef_bytes(&c, dr, cu);
+  b += S * 16 + S * sizeof(double) + S * sizeof(float) + S * sizeof(int);
+  b += face_elems(&c) * 8 + 2 * sizeof(int);
+  b += sizeof(int) * (static_cast<size_t>(c.ny) * c.nz + 1);
+  b += sizeof(double) * (S * 1024 + S);
+  b += sizeof(double) * nvox * S;  // host-transfer staging (bfvm_release_staging frees it)
+  if (n_agents > 0) {
+    const size_t cap = n_agents < 1024 ? 1024 : static_cast<size_t>(n_agents);
+    b += cap * (sizeof(int) + 1 + 4 * sizeof(unsigned));
+    b += sizeof(double) * cap * (3 * S + (1 + 4 * S) + 3 * S + S);
+    b += agent_scratch_bytes(static_cast<int>(cap));
+  }
+  return b;
+}
+
+extern "C" int bfvm_release_staging(bfvm_ctx* c) {
+  if (!c) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  dfree(c, c->d_staging);
+  c->d_staging = nullptr;
+  return BFVM_OK;
+}
 
 extern "C" int bfvm_get_launch(bfvm_ctx* c, int* x_lines, int* yz_tile, int* yz_chunk) {
   if (!c) return BFVM_ERR_ARG;

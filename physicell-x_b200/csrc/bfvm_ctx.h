@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cstdio>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/biofvm_b200.h"
@@ -51,7 +52,9 @@ struct bfvm_ctx {
   std::vector<double> faces;    // same layout as d_faces
   std::vector<double> c2;       // dt*decay/3 per substrate (thomas_constant2)
   std::vector<double> off;      // FP32 offsets currently applied to the field
-  size_t device_bytes = 0;
+  size_t device_bytes = 0;     // bytes currently allocated by dalloc
+  std::unordered_map<void*, size_t> alloc_bytes;
+  int version = 0;             // bumped whenever device pointers in SweepParams change
   double* d_staging = nullptr; // reference-layout field, for host uploads/downloads
   // per-kernel timing: 4 events per recorded step
   bool timing = false;
@@ -92,11 +95,19 @@ inline int dalloc(bfvm_ctx* c, void** p, size_t bytes) {
     return e == cudaErrorMemoryAllocation ? BFVM_ERR_OOM : BFVM_ERR_CUDA;
   }
   c->device_bytes += bytes;
+  c->alloc_bytes[*p] = bytes;
   return BFVM_OK;
 }
 
-inline void dfree(void* p) {
-  if (p) cudaFree(p);
+// Free a dalloc'ed buffer (null is a no-op) and take it off the account.
+inline void dfree(bfvm_ctx* c, void* p) {
+  if (!p) return;
+  auto it = c->alloc_bytes.find(p);
+  if (it != c->alloc_bytes.end()) {
+    c->device_bytes -= it->second;
+    c->alloc_bytes.erase(it);
+  }
+  cudaFree(p);
 }
 
 template <typename T>

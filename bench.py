@@ -61,6 +61,11 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--workload", choices=["cube200", "uneven_batch", "serve", "accuracy"], default="cube200",
+                    help="cube200 (default): the single-solve benchmark line; the others run the batched, "
+                         "serving and FP32-accuracy suites and print one JSON line each")
+    ap.add_argument("--requests", type=int, default=24, help="serve: requests in the stream")
+    ap.add_argument("--rate", type=float, default=1.0, help="serve: Poisson arrival rate (requests/s)")
     return ap.parse_args()
 
 
@@ -230,10 +235,52 @@ def run_reference_arm(args):
     return 0
 
 
+def run_suite(args):
+    """The batched, serving and accuracy suites (one GPU, rank 0 only)."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA GPU")
+    torch.cuda.set_device(local)
+    from bfvm import suites
+
+    if args.workload == "uneven_batch":
+        r = suites.uneven_batch(device=local)
+        line = {"metric": METRIC, "value": r["fp32_batch"]["updates_per_s"], "unit": UNIT, "n_gpus": 1,
+                "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "uneven_batch: 256 solves, edges 24-128, 1-6 substrates, 0-20k agents, "
+                                       "200 LOD steps with sources; FP32 batch vs plain FP64 one solve at a time"},
+                "suite": r}
+    elif args.workload == "serve":
+        r = suites.serve(n_requests=args.requests, rate=args.rate, device=local)
+        line = {"metric": "serve p50/p99 time-to-completion (s) and voxel·substrate updates/s",
+                "value": r["fp32_server"]["updates_per_s"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+                "dtype": "f32", "data": "synthetic",
+                "p50_s": r["fp32_server"]["p50_s"], "p99_s": r["fp32_server"]["p99_s"],
+                "config": {"workload": f"serve: {args.requests} requests, Poisson {args.rate}/s, edges 32-256, "
+                                       "1-8 substrates, 100-10000 steps, 0-200k agents; FP32 continuous batching "
+                                       "vs plain FP64 one request at a time"},
+                "suite": r}
+    else:
+        r = suites.accuracy(device=local)
+        line = {"metric": "FP32 relative error vs FP64 (per substrate, normwise L-infinity and L2)",
+                "value": max(max(x["linf_rel"]) for x in r), "unit": "relative", "n_gpus": 1,
+                "higher_is_better": False, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "cube50 1000 steps, cube200 500 steps, cube640 1000 steps, with sources"},
+                "suite": r}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload != "cube200":
+        return run_suite(args)
 
     rank, world, local = dist_env()
     import torch

@@ -1,0 +1,147 @@
+"""Measurement suites beyond the single-solve benchmark: the batched uneven
+workload, the serving stream, and the FP32-against-FP64 accuracy report.
+
+The FP64 reference results here come from the library's FP64 path, which the
+parity tests show to be bit-identical to the reference solver, so the FP32
+errors reported are errors against the reference's own FP64 results.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import workloads as W
+from .batch import Batch
+from .serve import Server, SolveRequest, poisson_arrivals, run_one_at_a_time
+from .solver import Microenvironment
+
+
+def _device_field(me, device):
+    """The solve's densities as a float64 CUDA tensor [voxels, S] (reference layout)."""
+    import torch
+
+    nx, ny, nz, S = me.shape
+    out = torch.empty((nx * ny * nz, S), dtype=torch.float64, device=torch.device("cuda", device))
+    me.download_field_device(out.data_ptr())
+    me.synchronize()
+    return out
+
+
+def field_errors(approx, ref):
+    """Per-substrate errors of `approx` against `ref` (tensors [voxels, S]):
+    normwise relative L-infinity max|a-r| / max|r| and relative L2."""
+    d = (approx - ref).abs()
+    r = ref.abs()
+    linf = (d.amax(dim=0) / r.amax(dim=0).clamp_min(1e-300)).tolist()
+    l2 = ((approx - ref).pow(2).sum(dim=0).sqrt() / ref.pow(2).sum(dim=0).sqrt().clamp_min(1e-300)).tolist()
+    return {"linf_rel": linf, "l2_rel": l2}
+
+
+def _timed_steps(me, steps, sources=True):
+    import torch
+
+    st = torch.cuda.ExternalStream(me.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    me.simulate_diffusion_decay(steps, sources=sources)
+    e1.record(st)
+    me.synchronize()
+    return e0.elapsed_time(e1) * 1e-3
+
+
+def uneven_batch(n_envs=256, steps=200, trial_steps=5, device=0):
+    """The uneven batch (n_envs solves, edges 24-128, 1-6 substrates, 0-20k
+    agents): plain FP64 one solve at a time, the FP64 batch and the FP32 batch
+    (autotuned), each for `steps` LOD steps with sources; FP32 errors against
+    FP64 per solve and substrate."""
+    import torch
+
+    wls = W.uneven_batch(n_envs, steps=steps)
+    tot = sum(wl.n_values for wl in wls)
+    out = {"envs": n_envs, "steps": steps, "values_per_step": tot}
+    # plain FP64, one solve at a time (each synchronised before the next starts)
+    ref = []
+    t_plain = 0.0
+    for wl in wls:
+        me = Microenvironment.from_workload(wl, "fp64", device)
+        t_plain += _timed_steps(me, steps)
+        ref.append(_device_field(me, device))
+        me.close()
+    out["fp64_plain"] = {"s": t_plain, "updates_per_s": tot * steps / t_plain}
+    for prec in ("fp64", "fp32"):
+        b = Batch(prec, device)
+        mes = [Microenvironment.from_workload(wl, prec, device) for wl in wls]
+        for me in mes:
+            b.add(me)
+        tuned_ms = b.autotune(sources=True, trial_steps=trial_steps)
+        bs = torch.cuda.ExternalStream(b.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(bs)
+        b.step(steps, sources=True)
+        e1.record(bs)
+        b.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3
+        res = {"s": t, "updates_per_s": tot * steps / t, "schedule": b.get_schedule(), "autotune_ms_per_step": tuned_ms}
+        if prec == "fp64":
+            res["bitwise_equal_to_plain"] = all(bool(torch.equal(_device_field(me, device), r))
+                                                for me, r in zip(mes, ref))
+        else:
+            worst_inf, worst_l2 = 0.0, 0.0
+            for me, r in zip(mes, ref):
+                e = field_errors(_device_field(me, device), r)
+                worst_inf = max(worst_inf, max(e["linf_rel"]))
+                worst_l2 = max(worst_l2, max(e["l2_rel"]))
+            res["max_linf_rel_vs_fp64"] = worst_inf
+            res["max_l2_rel_vs_fp64"] = worst_l2
+        b.close()
+        for me in mes:
+            me.close()
+        out[f"{prec}_batch"] = res
+    out["fp32_batch_over_fp64_plain"] = out["fp32_batch"]["updates_per_s"] / out["fp64_plain"]["updates_per_s"]
+    return out
+
+
+def single_accuracy(wl, device=0):
+    """One workload run to its full step count in FP64 and in FP32 (sources
+    fused); per-substrate FP32 errors and both times."""
+    out = {"workload": wl.name, "shape": list(wl.shape), "agents": wl.n_agents, "steps": wl.steps}
+    fields = {}
+    for prec in ("fp64", "fp32"):
+        me = Microenvironment.from_workload(wl, prec, device)
+        t = _timed_steps(me, wl.steps)
+        out[f"{prec}_s"] = t
+        out[f"{prec}_updates_per_s"] = wl.n_values * wl.steps / t
+        fields[prec] = _device_field(me, device)
+        me.close()
+    out.update(field_errors(fields["fp32"], fields["fp64"]))
+    return out
+
+
+def accuracy(names=("cube50", "cube200", "cube640"), device=0):
+    gens = {"cube50": W.cube50, "cube200": W.cube200, "cube640": W.cube640}
+    return [single_accuracy(gens[n](), device) for n in names]
+
+
+def serve(n_requests=24, rate=1.0, seed=5, quantum=64, device=0, **request_kw):
+    """A Poisson stream of requests (serving workload distribution unless
+    overridden) through the FP32 server, then the same stream through the
+    plain FP64 path one request at a time."""
+    arr = poisson_arrivals(n_requests, rate=rate, seed=seed)
+    reqs = [SolveRequest(i, W.serve_request(i, seed=seed, **request_kw), float(arr[i])) for i in range(n_requests)]
+    srv = Server("fp32", quantum=quantum, device=device)
+    st = srv.run(reqs)
+    srv.close()
+    base = run_one_at_a_time(reqs, "fp64", device)
+    s32, s64 = st.summary(), base.summary()
+    return {"requests": n_requests, "rate_per_s": rate, "seed": seed, "quantum": quantum,
+            "fp32_server": s32, "fp64_one_at_a_time": s64,
+            "throughput_ratio": (s32["updates_per_s"] / s64["updates_per_s"]) if s64["updates_per_s"] else None,
+            "request_sizes": [[r.workload.nx, r.workload.ny, r.workload.nz, r.workload.S, r.workload.steps,
+                               r.workload.n_agents] for r in reqs]}
+
+
+def timed(fn, *a, **k):
+    t0 = time.perf_counter()
+    r = fn(*a, **k)
+    return r, time.perf_counter() - t0

@@ -133,8 +133,8 @@ bool pick_config(int eb, int nx, int ny, int nz, SweepConfig* cfg) {
 // -0 upper diagonal).
 size_t coef_bytes(const bfvm_ctx* c, size_t* dr_off, size_t* cu_off) {
   const size_t S = c->S;
-  const size_t dr_sz = c->prec == BFVM_FP64 ? sizeof(double2) : sizeof(float2);
-  const size_t cu_sz = c->prec == BFVM_FP64 ? sizeof(double) : sizeof(float2);
+  const size_t dr_sz = c->prec == BFVM_FP64 ? sizeof(double2) : sizeof(double);
+  const size_t cu_sz = sizeof(double);
   const int n_axis[3] = {c->nx, c->ny, c->nz};
   size_t o = 0;
   for (int a = 0; a < 3; ++a) {
@@ -159,10 +159,6 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
   const size_t bytes = coef_bytes(c, dr_off, cu_off);
   std::vector<unsigned char> host(bytes, 0);
   std::vector<double> c1(S);
-  auto split = [](double x, float* hi, float* lo) {
-    *hi = static_cast<float>(x);
-    *lo = static_cast<float>(x - static_cast<double>(*hi));
-  };
   for (int ax = 0; ax < 3; ++ax) {
     const int n = n_axis[ax];
     const int np = coef_pad(n);
@@ -177,14 +173,10 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
         const double u = in ? cu[static_cast<size_t>(i) * S + s] : -0.0;
         if (c->prec == BFVM_FP64) {
           reinterpret_cast<double2*>(host.data() + dr_off[ax])[q] = make_double2(d, r);
-          reinterpret_cast<double*>(host.data() + cu_off[ax])[q] = u;
         } else {
-          float2 rr, uu;
-          split(r, &rr.x, &rr.y);
-          split(u, &uu.x, &uu.y);
-          reinterpret_cast<float2*>(host.data() + dr_off[ax])[q] = rr;
-          reinterpret_cast<float2*>(host.data() + cu_off[ax])[q] = uu;
+          reinterpret_cast<double*>(host.data() + dr_off[ax])[q] = r;
         }
+        reinterpret_cast<double*>(host.data() + cu_off[ax])[q] = u;
       }
   }
   BFVM_CUDA(cudaMemcpy(c->d_coef, host.data(), bytes, cudaMemcpyHostToDevice));
@@ -192,13 +184,7 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
     c->dr_off[a] = dr_off[a];
     c->cu_off[a] = cu_off[a];
   }
-  if (c->prec == BFVM_FP64) {
-    BFVM_CUDA(cudaMemcpy(c->d_c1, c1.data(), S * sizeof(double), cudaMemcpyHostToDevice));
-  } else {
-    std::vector<float2> k(S);
-    for (int s = 0; s < S; ++s) split(c1[s], &k[s].x, &k[s].y);
-    BFVM_CUDA(cudaMemcpy(c->d_c1, k.data(), S * sizeof(float2), cudaMemcpyHostToDevice));
-  }
+  BFVM_CUDA(cudaMemcpy(c->d_c1, c1.data(), S * sizeof(double), cudaMemcpyHostToDevice));
   // thomas_constant2 = decay; *= dt; /= 3 (BioFVM_solvers.cpp:208-209)
   c->c2.assign(S, 0.0);
   for (int s = 0; s < S; ++s) {
@@ -362,7 +348,7 @@ int bfvm_create(const bfvm_config* cfg, bfvm_ctx** out) {
   if (rc == BFVM_OK) rc = dalloc(c, &c->d_coef, coef_bytes(c, dr_tmp, cu_tmp));
   if (rc == BFVM_OK) rc = dalloc(c, &c->d_c1, S * 16);
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_off), S * sizeof(double));
-  if (rc == BFVM_OK) rc = dalloc(c, &c->d_shift, S * sizeof(float));
+  if (rc == BFVM_OK) rc = dalloc(c, &c->d_shift, S * sizeof(double));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_active), S * sizeof(int));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_faces), face_elems(c) * 8);
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_status), sizeof(int));
@@ -379,11 +365,10 @@ int bfvm_create(const bfvm_config* cfg, bfvm_ctx** out) {
   std::vector<int> act(S, 1);
   c->faces.assign(face_elems(c), 1.0);
   c->off.assign(S, 0.0);
-  std::vector<float> zero32(S, 0.f);
   if (cudaMemcpy(c->d_active, act.data(), S * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(c->d_faces, c->faces.data(), c->faces.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(c->d_off, c->off.data(), S * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(c->d_shift, zero32.data(), S * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+      cudaMemcpy(c->d_shift, c->off.data(), S * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(BFVM_ERR_CUDA);
   if (encode_field_maps(&c->maps, c->f, c->eb, c->nx, c->ny, c->nz, c->S, c->nxp, c->cfg) != 0)
     return fail(BFVM_ERR_CUDA);
@@ -498,7 +483,7 @@ static int choose_offsets(bfvm_ctx* c) {
   if (c->prec != BFVM_FP32) return BFVM_OK;
   const int S = c->S, nx = c->nx, ny = c->ny, nz = c->nz;
   std::vector<double> off(S, 0.0);
-  std::vector<float> shift(S, 0.f);
+  std::vector<double> shift(S, 0.0);
   const size_t px = static_cast<size_t>(nz) * ny, py = static_cast<size_t>(nz) * nx,
                pz = static_cast<size_t>(ny) * nx;
   for (int s = 0; s < S; ++s) {
@@ -515,11 +500,11 @@ static int choose_offsets(bfvm_ctx* c) {
       cnt += px + py + pz;
     }
     off[s] = acc / static_cast<double>(cnt);
-    shift[s] = static_cast<float>(c->c2[s] * off[s]);
+    shift[s] = c->c2[s] * off[s];
   }
   BFVM_CUDA(cudaStreamSynchronize(c->stream));
   BFVM_CUDA(cudaMemcpy(c->d_off, off.data(), S * sizeof(double), cudaMemcpyHostToDevice));
-  BFVM_CUDA(cudaMemcpy(c->d_shift, shift.data(), S * sizeof(float), cudaMemcpyHostToDevice));
+  BFVM_CUDA(cudaMemcpy(c->d_shift, shift.data(), S * sizeof(double), cudaMemcpyHostToDevice));
   c->off = off;
   return BFVM_OK;
 }

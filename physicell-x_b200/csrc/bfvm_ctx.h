@@ -125,7 +125,7 @@ inline SweepParams<T> make_params(bfvm_ctx* c, bool sources) {
   using CU = typename Coef<T>::CU;
   p.c1 = static_cast<const typename Coef<T>::C1*>(c->d_c1);
   p.off = f32 ? c->d_off : nullptr;
-  p.shift = f32 ? static_cast<const T*>(c->d_shift) : nullptr;
+  p.shift = f32 ? static_cast<const double*>(c->d_shift) : nullptr;
   p.active = c->d_active;
   p.xface = c->d_faces;
   p.yface = p.xface + 2 * S * c->nz * c->ny;

@@ -45,9 +45,9 @@
 // (div_fast), which is the correctly rounded quotient except for a numerator
 // of -0 or a nonzero numerator below 2^-960; a batch that meets either is
 // redone with IEEE division, so results equal the reference's bit for bit.
-// The FP32 form stores rho - off[s], applies the matching right-hand-side
-// shift, and keeps every coefficient as a float (hi, lo) pair; agent updates
-// stay in FP64.
+// The FP32 form stores rho - off[s] in FP32 and applies the matching
+// right-hand-side shift; its recurrence, coefficients and agent updates are
+// FP64, so each value is rounded to FP32 once per sweep, when it is stored.
 #include <climits>
 #include <type_traits>
 
@@ -125,22 +125,22 @@ __device__ __forceinline__ double forward_batch(const double (&v)[B], const doub
   return y;
 }
 
+// FP32 form: stored values are FP32, the recurrence runs in FP64 (the
+// running value y stays FP64 across elements and batches), each result is
+// rounded to FP32 once, when stored.  The quotient is t * RN(1/d).
 template <int B>
-__device__ __forceinline__ float forward_batch(const float (&v)[B], const float2 (&cf)[B], float2 c1, float shift,
-                                               int, float y, float (&out)[B]) {
+__device__ __forceinline__ double forward_batch(const float (&v)[B], const double (&cf)[B], double c1, double shift,
+                                                int, double y, float (&out)[B]) {
 #pragma unroll
   for (int q = 0; q < B; ++q) {
-    const float t = __fmaf_rn(c1.x, y, __fmaf_rn(c1.y, y, v[q] - shift));
-    y = __fmaf_rn(t, cf[q].x, __fmul_rn(t, cf[q].y));
-    out[q] = y;
+    const double t = __fma_rn(c1, y, static_cast<double>(v[q]) - shift);
+    y = __dmul_rn(t, cf[q]);
+    out[q] = static_cast<float>(y);
   }
   return y;
 }
 
 __device__ __forceinline__ double back_elem(double c, double xn, double y) { return __fma_rn(-c, xn, y); }
-__device__ __forceinline__ float back_elem(float2 c, float xn, float y) {
-  return __fmaf_rn(-c.x, xn, __fmaf_rn(-c.y, xn, y));
-}
 
 // Apply the run of agents that starts at sorted position q (key `key`,
 // constants c1/c2/e2 of that first agent already loaded) to the staged value
@@ -264,7 +264,7 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   const DR* __restrict__ drp = p.ax.dr + static_cast<size_t>(s) * p.ax.npad;
   const CU* __restrict__ cup = p.ax.cu + static_cast<size_t>(s) * p.ax.npad;
   const typename Coef<T>::C1 c1 = p.c1[s];
-  const T shift = kF32<T> ? p.shift[s] : T(0);
+  const double shift = kF32<T> ? p.shift[s] : 0.0;
   // Coefficients of the forward pass: two register buffers used in turn, the
   // idle one loaded with the chunk after next (rows are padded past C * W).
   DR cfa[W], cfb[W];
@@ -341,7 +341,7 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   // Forward elimination, one chunk at a time as the TMA boxes land.  Values
   // past nx in the last chunk are TMA fill; the chain may run over them
   // harmlessly (those results are never stored to the field).
-  T y = T(-0.0);
+  double y = -0.0;  // running value of the forward recurrence (FP64 in both forms)
   const int screen = p.screen;
   auto fwd = [&](int c, DR (&cf)[W]) {
     if (!all_landed && ok) ok = mbar_wait(smem_u32(&bars[c]), static_cast<uint32_t>(phase >> c) & 1u);
@@ -374,7 +374,7 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   }
 
   // Back substitution, last chunk first; each finished chunk is stored at once.
-  T xn = T(-0.0);
+  double xn = -0.0;  // running value of the back substitution
   for (int c = C - 1; c >= 0; --c) {
     unsigned char* crow = row + c * chunk_bytes;
     const int i0 = c * W;
@@ -397,14 +397,14 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
         for (int q = W - 1; q >= 0; --q) {
           if (i0 + q < nx) {
             xn = back_elem(cw[q], xn, v[q]);
-            v[q] = xn;
+            v[q] = static_cast<T>(xn);
           }
         }
       } else {
 #pragma unroll
         for (int q = W - 1; q >= 0; --q) {
           xn = back_elem(cw[q], xn, v[q]);
-          v[q] = xn;
+          v[q] = static_cast<T>(xn);
         }
       }
       store_row<T, W>(crow, sw, v);
@@ -487,7 +487,7 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
   const DR* __restrict__ drp = ac.dr + static_cast<size_t>(s) * ac.npad;
   const CU* __restrict__ cup = ac.cu + static_cast<size_t>(s) * ac.npad;
   const typename Coef<T>::C1 c1 = p.c1[s];
-  const T shift = kF32<T> ? p.shift[s] : T(0);
+  const double shift = kF32<T> ? p.shift[s] : 0.0;
   const int screen = p.screen;
   // Coefficients of the forward pass: two register buffers used in turn, the
   // idle one loaded with the batch after next.
@@ -509,7 +509,7 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
   // The two end voxels of the line lie in the y (z) faces: the pin after the
   // sweep restores their input values.
   T e0v = T(0), e1v = T(0);
-  T y = T(-0.0);
+  double y = -0.0;  // running value of the forward recurrence (FP64 in both forms)
 
   // One forward batch of R rows from rb, after waiting for the chunks that
   // cover it.  The tile holds a whole number of batches, so the last batch
@@ -559,7 +559,7 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
 
   // Back substitution in batches of R rows from the end; chunk c is stored
   // once every row from its start on is final.
-  T xn = T(-0.0);
+  double xn = -0.0;  // running value of the back substitution
   int next_store = C - 1;
   int store_row = next_store * CH;  // first row of chunk next_store
   const int last_b = ((n - 1) / R) * R;
@@ -579,14 +579,14 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
         for (int q = R - 1; q >= 0; --q) {
           if (rb + q < n) {
             xn = back_elem(cw[q], xn, v[q]);
-            v[q] = xn;
+            v[q] = static_cast<T>(xn);
           }
         }
       } else {
 #pragma unroll
         for (int q = R - 1; q >= 0; --q) {
           xn = back_elem(cw[q], xn, v[q]);
-          v[q] = xn;
+          v[q] = static_cast<T>(xn);
         }
       }
 #pragma unroll

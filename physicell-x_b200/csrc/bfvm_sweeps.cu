@@ -77,49 +77,51 @@ __device__ __forceinline__ double markstein(double t, double d, double r) {
   return __fma_rn(e, r, q0);
 }
 
-// FP64 forward batch.  With c1 >= 0 and every denominator >= 1 (screen set:
-// no negative diffusion or decay), a batch whose incoming value is not
-// negative and whose inputs are all >= 2^-960 has every numerator
-// t = fma(c1, y, v) >= 2^-960, where the Markstein quotient is exact: such
-// batches (checked on the inputs, off the chain) run the bare chain.  Other
-// batches check each numerator and redo the batch with IEEE division if one
+// FP64 forward batch.  The bare chain runs first.  With c1 >= 0 and every
+// denominator >= 1 (screen set: no negative diffusion or decay), a batch
+// whose incoming value is not negative and whose inputs are all >= 2^-960
+// has every numerator t = fma(c1, y, v) >= 2^-960, where the Markstein
+// quotient is exact.  That screen reads only the inputs (a signed minimum of
+// their high words, which orders non-negative doubles and puts negative ones
+// first), so it runs off the chain; a batch that fails it anywhere in the
+// warp is redone with each numerator checked, and with IEEE division if one
 // is -0 or a nonzero value below 2^-960.
 template <int B>
 __device__ __forceinline__ double forward_batch(const double (&v)[B], const double2 (&cf)[B], double c1, double,
                                                 int screen, double y, double (&out)[B]) {
   const double y0 = y;
-  double mn[B];
 #pragma unroll
-  for (int q = 0; q < B; ++q) mn[q] = v[q];
+  for (int q = 0; q < B; ++q) {
+    y = markstein(__fma_rn(c1, y, v[q]), cf[q].x, cf[q].y);
+    out[q] = y;
+  }
+  int hw[B];
+#pragma unroll
+  for (int q = 0; q < B; ++q) hw[q] = __double2hiint(v[q]);
 #pragma unroll
   for (int w = B / 2; w >= 1; w /= 2) {
 #pragma unroll
-    for (int q = 0; q < w; ++q) mn[q] = fmin(mn[q], mn[q + w]);
+    for (int q = 0; q < w; ++q) hw[q] = min(hw[q], hw[q + w]);
   }
-  const bool clean = screen != 0 && !(y0 < 0.0) && mn[0] >= 0x1p-960;
-  if (__all_sync(__activemask(), clean)) {
-#pragma unroll
-    for (int q = 0; q < B; ++q) {
-      y = markstein(__fma_rn(c1, y, v[q]), cf[q].x, cf[q].y);
-      out[q] = y;
-    }
-    return y;
-  }
-  bool slow = false;
-#pragma unroll
-  for (int q = 0; q < B; ++q) {
-    const double t = __fma_rn(c1, y, v[q]);
-    // off the chain: the two cases Markstein's step does not cover
-    slow |= (fabs(t) < 0x1p-960) & (__double_as_longlong(t) != 0);
-    y = markstein(t, cf[q].x, cf[q].y);
-    out[q] = y;
-  }
-  if (slow) {
+  constexpr int kHiTiny = 0x03F00000;  // high word of 2^-960
+  const bool clean = screen != 0 && !(y0 < 0.0) && hw[0] >= kHiTiny;  // -0 (a line's start) passes
+  if (!__all_sync(__activemask(), clean)) {
+    bool slow = false;
     y = y0;
 #pragma unroll
     for (int q = 0; q < B; ++q) {
-      y = __fma_rn(c1, y, v[q]) / cf[q].x;
+      const double t = __fma_rn(c1, y, v[q]);
+      slow |= (fabs(t) < 0x1p-960) & (__double_as_longlong(t) != 0);
+      y = markstein(t, cf[q].x, cf[q].y);
       out[q] = y;
+    }
+    if (slow) {
+      y = y0;
+#pragma unroll
+      for (int q = 0; q < B; ++q) {
+        y = __fma_rn(c1, y, v[q]) / cf[q].x;
+        out[q] = y;
+      }
     }
   }
   return y;

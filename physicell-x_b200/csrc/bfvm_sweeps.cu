@@ -381,8 +381,13 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
     unsigned char* crow = row + c * chunk_bytes;
     const int i0 = c * W;
     CU cw[W];
+    const double2* cwp = reinterpret_cast<const double2*>(cus + i0);  // 16-byte pairs
 #pragma unroll
-    for (int q = 0; q < W; ++q) cw[q] = cus[i0 + q];
+    for (int q = 0; q < W / 2; ++q) {
+      const double2 pr = cwp[q];
+      cw[2 * q] = pr.x;
+      cw[2 * q + 1] = pr.y;
+    }
     if (face) {
       T fw[W];
 #pragma unroll
@@ -568,13 +573,17 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
   for (int rb = last_b; rb >= 0; rb -= R) {
     if (!face) {
       T* cb = col + rb * TI;
-      const CU* cwp = cus + rb;
+      // the upper diagonal in 16-byte pairs (rb is a multiple of 16 rows)
+      const double2* cwp = reinterpret_cast<const double2*>(cus + rb);
       T v[R];
       CU cw[R];
 #pragma unroll
-      for (int q = 0; q < R; ++q) {
-        v[q] = cb[q * TI];
-        cw[q] = cwp[q];
+      for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
+#pragma unroll
+      for (int q = 0; q < R / 2; ++q) {
+        const double2 pr = cwp[q];
+        cw[2 * q] = pr.x;
+        cw[2 * q + 1] = pr.y;
       }
       if (rb == last_b) {
 #pragma unroll

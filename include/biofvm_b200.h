@@ -43,8 +43,8 @@ extern "C" {
 
 /* ---- precision ---------------------------------------------------------- */
 #define BFVM_FP64 0 /* FP64 sweeps and storage: the reference's arithmetic    */
-#define BFVM_FP32 1 /* FP32 sweeps and storage; FP64-factored coefficients,   */
-                    /* FP64 agent updates                                      */
+#define BFVM_FP32 1 /* FP32 storage (half the bytes); FP64 recurrence,         */
+                    /* coefficients and agent updates                          */
 
 /* ---- bfvm_step flags ----------------------------------------------------- */
 #define BFVM_STEP_SOURCES 1 /* apply the agents' sources/sinks ahead of each  */
@@ -200,10 +200,24 @@ size_t bfvm_device_bytes(bfvm_ctx* ctx);
  * counterpart in the reference, which has no device memory. */
 size_t bfvm_estimate_bytes(const bfvm_config* cfg, int n_agents);
 
-/* Free the buffer that host uploads and downloads stage the reference-layout
- * field in (as large as an FP64 copy of the field); the next host transfer
- * allocates it again.  No counterpart in the reference. */
+/* Free the buffers that host transfers stage through (the reference-layout
+ * field, as large as an FP64 copy of the field, and the gradient buffer of
+ * bfvm_compute_gradients); the next host transfer allocates them again.  No
+ * counterpart in the reference. */
 int bfvm_release_staging(bfvm_ctx* ctx);
+
+/* Gradients of every substrate at every voxel of the current field,
+ * out[(v*S + d)*3 + axis] (v = reference voxel index, axis x/y/z) in host
+ * memory -- Microenvironment::compute_all_gradient_vectors followed by
+ * gradient_vector(v) for every voxel (BioFVM/BioFVM_microenvironment.cpp:
+ * 1454-1616, 1431-1441).  One-sided differences at the line ends, central
+ * inside; FP64 results equal the reference's bit for bit.  An axis of length
+ * 1 gets 0 (the reference reads outside its array there).  Synchronous. */
+int bfvm_compute_gradients(bfvm_ctx* ctx, double* out);
+
+/* The same into device memory on the solve's device (3*S doubles per voxel),
+ * asynchronous on the solve's stream. */
+int bfvm_compute_gradients_device(bfvm_ctx* ctx, double* d_out);
 
 /* Launch shape of the sweeps: lines per CTA in the x sweep (a multiple of 8,
  * at most 256), x extent per CTA in the y/z sweeps (16 -- FP64 only --, 32 or

@@ -199,3 +199,41 @@ int orc_nearest_voxel(double x, double y, double z, double x0, double y0, double
   if (k < 0) k = 0;
   return (int)((i * ny + j) * nz + k);
 }
+
+/* BioFVM/BioFVM_microenvironment.cpp:1454-1616.  The three passes of the
+ * reference write disjoint components, so they are restated as one loop per
+ * component with the same expressions: value = a; value -= b; value /= h. */
+void orc_gradients(const double* field, int nx, int ny, int nz, int S, double dx, double* out) {
+  const double two_dx = dx * 2.0;
+  const long jump[3] = {(long)ny * nz * S, (long)nz * S, (long)S};
+  const int len[3] = {nx, ny, nz};
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        const int pos[3] = {i, j, k};
+        const long n = ((long)i * ny + j) * nz + k;
+        for (int d = 0; d < S; ++d) {
+          const long idx = n * S + d;
+          for (int ax = 0; ax < 3; ++ax) {
+            double g = 0.0;
+            if (len[ax] > 1) {
+              if (pos[ax] == 0) {
+                g = field[idx + jump[ax]];
+                g -= field[idx];
+                g /= dx;
+              } else if (pos[ax] == len[ax] - 1) {
+                g = field[idx];
+                g -= field[idx - jump[ax]];
+                g /= dx;
+              } else {
+                g = field[idx + jump[ax]];
+                g -= field[idx - jump[ax]];
+                g /= two_dx;
+              }
+            }
+            out[idx * 3 + ax] = g;
+          }
+        }
+      }
+}

@@ -65,6 +65,15 @@ void orc_sources(double* field, int S, int n_agents, const int* voxel, const uns
 int orc_nearest_voxel(double x, double y, double z, double x0, double y0, double z0, double dx,
                       int nx, int ny, int nz);
 
+/* Gradients of every substrate at every voxel, out[(v*S + d)*3 + axis]:
+ * one-sided differences (a - b) / dx at the two ends of each line and
+ * central differences (a - b) / (2 dx) inside, each as one subtraction and
+ * one division.  Restates Microenvironment::compute_all_gradient_vectors,
+ * BioFVM/BioFVM_microenvironment.cpp:1454-1616.  An axis of length 1 gets 0
+ * (the reference reads outside the array there; with nz == 1 it skips the z
+ * component). */
+void orc_gradients(const double* field, int nx, int ny, int nz, int S, double dx, double* out);
+
 #ifdef __cplusplus
 }
 #endif

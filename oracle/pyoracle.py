@@ -59,6 +59,8 @@ class Port:
             L.orc_sources.argtypes = [_dp, C.c_int, C.c_int, _ip, C.c_void_p, _dp, _dp, _dp]
             L.orc_nearest_voxel.argtypes = [C.c_double] * 7 + [C.c_int] * 3
             L.orc_nearest_voxel.restype = C.c_int
+            L.orc_gradients.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _dp]
+            L.orc_gradients.restype = None
             cls._lib = L
         return cls._lib
 
@@ -109,6 +111,15 @@ class Port:
             act = act_arr.ctypes.data
         cls.lib().orc_sources(field, S, len(voxel), voxel, act, _f64(c1).ravel(), _f64(c2).ravel(),
                               _f64(e2).ravel())
+
+    @classmethod
+    def gradients(cls, field, shape, dx):
+        """compute_all_gradient_vectors: array [voxels, S, 3]."""
+        nx, ny, nz, S = shape
+        f = _f64(field).ravel()
+        out = np.empty(nx * ny * nz * S * 3, np.float64)
+        cls.lib().orc_gradients(f, nx, ny, nz, S, float(dx), out)
+        return out.reshape(nx * ny * nz, S, 3)
 
     @classmethod
     def nearest_voxel(cls, pos, origin, dx, dims):
@@ -221,6 +232,8 @@ class Reference:
             L.ref_env_run.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]
             L.ref_env_run.restype = C.c_int
             L.ref_max_threads.restype = C.c_int
+            L.ref_env_gradients.argtypes = [vp, _dp]
+            L.ref_env_gradients.restype = None
             if dropin:
                 L.ref_env_dropin_fuse_sources.argtypes = [vp, C.c_int, C.c_double]
                 L.ref_env_dropin_fuse_sources.restype = C.c_int
@@ -272,6 +285,15 @@ class Reference:
 
     def apply_dirichlet(self):
         self.L.ref_env_apply_dirichlet(self.h)
+
+    def gradients(self):
+        """The reference's compute_all_gradient_vectors on the current field,
+        as [voxels, S, 3]."""
+        nx, ny, nz, S = self.wl.shape
+        out = np.empty(nx * ny * nz * S * 3, np.float64)
+        with _stdout_to_stderr():
+            self.L.ref_env_gradients(self.h, out)
+        return out.reshape(nx * ny * nz, S, 3)
 
     def run(self, nsteps=None, solver=0, threads=None, sources_threads=1, fetch=True):
         nsteps = self.wl.steps if nsteps is None else nsteps

@@ -267,4 +267,21 @@ int ref_env_dropin_fuse_sources(void* h, int enable, double dt) {
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
 
+/* Microenvironment::compute_all_gradient_vectors
+ * (BioFVM/BioFVM_microenvironment.cpp:1454-1616), read back through the
+ * public gradient_vector(n) accessor (:1431-1441) as out[(n*S + d)*3 + axis].
+ * The reference caches 2*dx in function statics on its first call, so every
+ * environment of one process must share dx for its results to be valid. */
+void ref_env_gradients(void* h, double* out) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  Microenvironment& M = *e->M;
+  M.compute_all_gradient_vectors();
+  const long nv = (long)e->nx * e->ny * e->nz;
+  for (long n = 0; n < nv; ++n) {
+    std::vector<gradient>& g = M.gradient_vector((int)n);
+    for (int d = 0; d < e->S; ++d)
+      for (int a = 0; a < 3; ++a) out[(n * e->S + d) * 3 + a] = g[d][a];
+  }
+}
+
 }  // extern "C"

@@ -159,6 +159,17 @@ class Microenvironment:
     def simulate_cell_sources_and_sinks(self):
         check(self.L.bfvm_apply_sources(self.h), "bfvm_apply_sources")
 
+    def compute_all_gradient_vectors(self, out=None):
+        """Gradients of every substrate at every voxel, [voxels, S, 3] in the
+        reference's voxel order (Microenvironment::compute_all_gradient_vectors)."""
+        nx, ny, nz, S = self.shape
+        out = np.empty((nx * ny * nz, S, 3), np.float64) if out is None else out
+        check(self.L.bfvm_compute_gradients(self.h, _ptr(out)), "bfvm_compute_gradients")
+        return out
+
+    def compute_all_gradient_vectors_device(self, ptr):
+        check(self.L.bfvm_compute_gradients_device(self.h, C.c_void_p(int(ptr))), "bfvm_compute_gradients_device")
+
     def synchronize(self):
         check(self.L.bfvm_synchronize(self.h), "bfvm_synchronize")
 

@@ -393,6 +393,7 @@ int bfvm_destroy(bfvm_ctx* c) {
   dfree(c, c->d_line_off);
   dfree(c, c->d_sums);
   dfree(c, c->d_staging);
+  dfree(c, c->d_grad);
   for (cudaEvent_t e : c->events) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -835,6 +836,8 @@ extern "C" int bfvm_release_staging(bfvm_ctx* c) {
   BFVM_CUDA(cudaStreamSynchronize(c->stream));
   dfree(c, c->d_staging);
   c->d_staging = nullptr;
+  dfree(c, c->d_grad);
+  c->d_grad = nullptr;
   return BFVM_OK;
 }
 

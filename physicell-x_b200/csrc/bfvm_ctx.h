@@ -56,6 +56,7 @@ struct bfvm_ctx {
   std::unordered_map<void*, size_t> alloc_bytes;
   int version = 0;             // bumped whenever device pointers in SweepParams change
   double* d_staging = nullptr; // reference-layout field, for host uploads/downloads
+  double* d_grad = nullptr;    // gradients for host reads (bfvm_compute_gradients)
   // per-kernel timing: 4 events per recorded step
   bool timing = false;
   int timed_steps = 0;

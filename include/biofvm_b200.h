@@ -206,6 +206,20 @@ size_t bfvm_estimate_bytes(const bfvm_config* cfg, int n_agents);
  * counterpart in the reference. */
 int bfvm_release_staging(bfvm_ctx* ctx);
 
+/* Bulk (per-voxel) sources and sinks.  Replaces the three callbacks
+ * Microenvironment::bulk_supply_rate_function, bulk_supply_target_densities_
+ * function and bulk_uptake_rate_function (BioFVM_microenvironment.h:210-212)
+ * with their values for every voxel: supply S, target T and uptake U, each a
+ * host array in the field's reference layout.  Kept on the device until
+ * replaced; three NULLs free them. */
+int bfvm_set_bulk_rates(bfvm_ctx* ctx, const double* supply, const double* target, const double* uptake);
+
+/* One Microenvironment::simulate_bulk_sources_and_sinks(dt)
+ * (BioFVM_microenvironment.cpp:1327-1368) with the rates above:
+ * rho = fma(dt, T*S, rho); rho /= ((U + S)*dt) + 1, bit for bit in FP64.
+ * BFVM_ERR_STATE if no rates were set.  Asynchronous on the solve's stream. */
+int bfvm_apply_bulk_sources(bfvm_ctx* ctx);
+
 /* Gradients of every substrate at every voxel of the current field,
  * out[(v*S + d)*3 + axis] (v = reference voxel index, axis x/y/z) in host
  * memory -- Microenvironment::compute_all_gradient_vectors followed by

@@ -237,3 +237,25 @@ void orc_gradients(const double* field, int nx, int ny, int nz, int S, double dx
         }
       }
 }
+
+/* BioFVM/BioFVM_microenvironment.cpp:1327-1368, one value at a time in the
+ * order of the reference's loops:
+ *   temp2 = T; temp2 *= S;                (:1346-1347)
+ *   rho += dt * temp2;     contracted to one fma by the reference build (:1349-1351)
+ *   temp3 = U; temp3 += S; temp3 *= dt; temp3 += 1;   (:1353-1360)
+ *   rho /= temp3;                                       (:1362-1363) */
+void orc_bulk_sources(double* field, long n_values, double dt, const double* supply, const double* target,
+                      const double* uptake) {
+#pragma omp parallel for schedule(static)
+  for (long q = 0; q < n_values; ++q) {
+    double t2 = target[q];
+    t2 *= supply[q];
+    double r = fma(dt, t2, field[q]);
+    double t3 = uptake[q];
+    t3 += supply[q];
+    t3 *= dt;
+    t3 += 1.0;
+    r /= t3;
+    field[q] = r;
+  }
+}

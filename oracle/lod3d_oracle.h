@@ -74,6 +74,15 @@ int orc_nearest_voxel(double x, double y, double z, double x0, double y0, double
  * component). */
 void orc_gradients(const double* field, int nx, int ny, int nz, int S, double dx, double* out);
 
+/* Bulk sources and sinks with per-voxel supply rate S, target density T and
+ * uptake rate U (arrays like the field): rho = fma(dt, S*T, rho) -- the
+ * reference's g++ build contracts `rho += dt * temp2` -- then
+ * rho /= ((U + S) * dt) + 1.  Restates
+ * Microenvironment::simulate_bulk_sources_and_sinks,
+ * BioFVM/BioFVM_microenvironment.cpp:1327-1368. */
+void orc_bulk_sources(double* field, long n_values, double dt, const double* supply, const double* target,
+                      const double* uptake);
+
 #ifdef __cplusplus
 }
 #endif

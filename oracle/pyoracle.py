@@ -61,6 +61,8 @@ class Port:
             L.orc_nearest_voxel.restype = C.c_int
             L.orc_gradients.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _dp]
             L.orc_gradients.restype = None
+            L.orc_bulk_sources.argtypes = [_dp, C.c_long, C.c_double, _dp, _dp, _dp]
+            L.orc_bulk_sources.restype = None
             cls._lib = L
         return cls._lib
 
@@ -111,6 +113,16 @@ class Port:
             act = act_arr.ctypes.data
         cls.lib().orc_sources(field, S, len(voxel), voxel, act, _f64(c1).ravel(), _f64(c2).ravel(),
                               _f64(e2).ravel())
+
+    @classmethod
+    def bulk_sources(cls, field, dt, supply, target, uptake):
+        """simulate_bulk_sources_and_sinks on `field` in place."""
+        f = field if field.dtype == np.float64 and field.flags.c_contiguous else None
+        if f is None:
+            raise ValueError("field must be a contiguous float64 array")
+        cls.lib().orc_bulk_sources(f.reshape(-1), f.size, float(dt), _f64(supply).ravel(), _f64(target).ravel(),
+                                   _f64(uptake).ravel())
+        return f
 
     @classmethod
     def gradients(cls, field, shape, dx):
@@ -234,6 +246,8 @@ class Reference:
             L.ref_max_threads.restype = C.c_int
             L.ref_env_gradients.argtypes = [vp, _dp]
             L.ref_env_gradients.restype = None
+            L.ref_env_bulk.argtypes = [vp, C.c_double, _dp, _dp, _dp, C.c_int]
+            L.ref_env_bulk.restype = None
             if dropin:
                 L.ref_env_dropin_fuse_sources.argtypes = [vp, C.c_int, C.c_double]
                 L.ref_env_dropin_fuse_sources.restype = C.c_int
@@ -285,6 +299,13 @@ class Reference:
 
     def apply_dirichlet(self):
         self.L.ref_env_apply_dirichlet(self.h)
+
+    def bulk_sources(self, supply, target, uptake, threads=1):
+        """The reference's simulate_bulk_sources_and_sinks(dt) with these
+        per-voxel rates (arrays like the field)."""
+        self._bulk = tuple(_f64(a).ravel().copy() for a in (supply, target, uptake))  # kept alive
+        with _stdout_to_stderr():
+            self.L.ref_env_bulk(self.h, self.wl.dt, *self._bulk, threads)
 
     def gradients(self):
         """The reference's compute_all_gradient_vectors on the current field,

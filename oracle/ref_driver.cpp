@@ -29,6 +29,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "BioFVM.h"
@@ -266,6 +267,45 @@ int ref_env_dropin_fuse_sources(void* h, int enable, double dt) {
 #endif
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
+
+/* Bulk sources and sinks: per-voxel supply rate S, target density T and
+ * uptake rate U [voxel][S] served to Microenvironment's three callback
+ * pointers (BioFVM_microenvironment.h:210-212) from arrays the caller owns,
+ * then one Microenvironment::simulate_bulk_sources_and_sinks(dt)
+ * (BioFVM_microenvironment.cpp:1327-1368). */
+namespace {
+struct BulkRates {
+  const double *S = nullptr, *T = nullptr, *U = nullptr;
+  int n = 0;
+};
+std::map<const Microenvironment*, BulkRates>& bulk_table() {
+  static std::map<const Microenvironment*, BulkRates> t;
+  return t;
+}
+void bulk_copy(const double* src, Microenvironment* M, int voxel, double* dst) {
+  const int n = bulk_table()[M].n;
+  std::memcpy(dst, src + (size_t)voxel * n, sizeof(double) * n);
+}
+void bulk_supply(Microenvironment* M, int v, double* w) { bulk_copy(bulk_table()[M].S, M, v, w); }
+void bulk_target(Microenvironment* M, int v, double* w) { bulk_copy(bulk_table()[M].T, M, v, w); }
+void bulk_uptake(Microenvironment* M, int v, double* w) { bulk_copy(bulk_table()[M].U, M, v, w); }
+}  // namespace
+
+void ref_env_bulk(void* h, double dt, const double* supply, const double* target, const double* uptake,
+                  int threads) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  Microenvironment& M = *e->M;
+  BulkRates& r = bulk_table()[&M];
+  r.S = supply;
+  r.T = target;
+  r.U = uptake;
+  r.n = e->S;
+  M.bulk_supply_rate_function = bulk_supply;
+  M.bulk_supply_target_densities_function = bulk_target;
+  M.bulk_uptake_rate_function = bulk_uptake;
+  omp_set_num_threads(threads > 0 ? threads : 1);
+  M.simulate_bulk_sources_and_sinks(dt);
+}
 
 /* Microenvironment::compute_all_gradient_vectors
  * (BioFVM/BioFVM_microenvironment.cpp:1454-1616), read back through the

@@ -72,6 +72,8 @@ _SIGS = {
     "bfvm_estimate_bytes": (C.c_size_t, [C.POINTER(bfvm_config), C.c_int]),
     "bfvm_release_staging": (C.c_int, [C.c_void_p]),
     "bfvm_compute_gradients": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bfvm_set_bulk_rates": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bfvm_apply_bulk_sources": (C.c_int, [C.c_void_p]),
     "bfvm_compute_gradients_device": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_field_offsets": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_get_launch": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),

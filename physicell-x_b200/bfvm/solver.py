@@ -159,6 +159,21 @@ class Microenvironment:
     def simulate_cell_sources_and_sinks(self):
         check(self.L.bfvm_apply_sources(self.h), "bfvm_apply_sources")
 
+    def set_bulk_rates(self, supply, target, uptake):
+        """Per-voxel supply rate, target density and uptake rate (arrays like
+        the field, reference layout); None for all three clears them."""
+        if supply is None and target is None and uptake is None:
+            check(self.L.bfvm_set_bulk_rates(self.h, None, None, None), "bfvm_set_bulk_rates")
+            return
+        arrs = [_f64(a).ravel() for a in (supply, target, uptake)]
+        for a in arrs:
+            if a.size != self.n_values:
+                raise ValueError(f"rate array has {a.size} values, expected {self.n_values}")
+        check(self.L.bfvm_set_bulk_rates(self.h, *[_ptr(a) for a in arrs]), "bfvm_set_bulk_rates")
+
+    def simulate_bulk_sources_and_sinks(self):
+        check(self.L.bfvm_apply_bulk_sources(self.h), "bfvm_apply_bulk_sources")
+
     def compute_all_gradient_vectors(self, out=None):
         """Gradients of every substrate at every voxel, [voxels, S, 3] in the
         reference's voxel order (Microenvironment::compute_all_gradient_vectors)."""

@@ -394,6 +394,7 @@ int bfvm_destroy(bfvm_ctx* c) {
   dfree(c, c->d_sums);
   dfree(c, c->d_staging);
   dfree(c, c->d_grad);
+  dfree(c, c->d_bulk);
   for (cudaEvent_t e : c->events) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -828,6 +829,50 @@ extern "C" size_t bfvm_estimate_bytes(const bfvm_config* cfg, int n_agents) {
     b += agent_scratch_bytes(static_cast<int>(cap));
   }
   return b;
+}
+
+extern "C" int bfvm_set_bulk_rates(bfvm_ctx* c, const double* supply, const double* target, const double* uptake) {
+  if (!c) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  if (!supply && !target && !uptake) {
+    BFVM_CUDA(cudaStreamSynchronize(c->stream));
+    dfree(c, c->d_bulk);
+    c->d_bulk = nullptr;
+    return BFVM_OK;
+  }
+  if (!supply || !target || !uptake) return BFVM_ERR_ARG;
+  const size_t plane = static_cast<size_t>(c->nxp) * c->ny * c->nz * c->S;
+  if (!c->d_bulk) {
+    const int rc = dalloc(c, reinterpret_cast<void**>(&c->d_bulk), 3 * plane * sizeof(double));
+    if (rc != BFVM_OK) return rc;
+  }
+  int rc = ensure_staging(c);
+  if (rc != BFVM_OK) return rc;
+  const size_t bytes = sizeof(double) * static_cast<size_t>(c->nx) * c->ny * c->nz * c->S;
+  const double* src[3] = {supply, target, uptake};
+  for (int a = 0; a < 3; ++a) {
+    BFVM_CUDA(cudaMemcpyAsync(c->d_staging, src[a], bytes, cudaMemcpyHostToDevice, c->stream));
+    BFVM_CUDA(launch_pack<double>(c->d_staging, c->d_bulk + a * plane, c->nx, c->ny, c->nz, c->S, c->nxp, nullptr,
+                                  c->stream));
+    note_launches(1);
+  }
+  return bfvm_synchronize(c);
+}
+
+extern "C" int bfvm_apply_bulk_sources(bfvm_ctx* c) {
+  if (!c) return BFVM_ERR_ARG;
+  if (!c->d_bulk) return BFVM_ERR_STATE;
+  DeviceGuard g(c->device);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (c->prec == BFVM_FP64)
+    BFVM_CUDA(launch_bulk<double>(static_cast<double*>(c->f), c->d_bulk, c->nx, c->ny, c->nz, c->S, c->nxp, c->dt,
+                                  nullptr, sms, c->stream));
+  else
+    BFVM_CUDA(launch_bulk<float>(static_cast<float*>(c->f), c->d_bulk, c->nx, c->ny, c->nz, c->S, c->nxp, c->dt,
+                                 c->d_off, sms, c->stream));
+  note_launches(1);
+  return BFVM_OK;
 }
 
 extern "C" int bfvm_release_staging(bfvm_ctx* c) {

@@ -57,6 +57,7 @@ struct bfvm_ctx {
   int version = 0;             // bumped whenever device pointers in SweepParams change
   double* d_staging = nullptr; // reference-layout field, for host uploads/downloads
   double* d_grad = nullptr;    // gradients for host reads (bfvm_compute_gradients)
+  double* d_bulk = nullptr;    // bulk supply | target | uptake rates, device layout (bfvm_set_bulk_rates)
   // per-kernel timing: 4 events per recorded step
   bool timing = false;
   int timed_steps = 0;

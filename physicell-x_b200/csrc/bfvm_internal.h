@@ -168,6 +168,12 @@ size_t batch_axis_smem(int elem_bytes, int axis, int n_line, int yz_chunk);
 template <typename T>
 cudaError_t batch_occupancy(size_t smem, int* ctas_per_sm);
 
+// Bulk sources and sinks (bfvm_bulk.cu): rates = [supply | target | uptake],
+// each S*nz*ny*nxp doubles in the field's device layout.
+template <typename T>
+cudaError_t launch_bulk(T* f, const double* rates, int nx, int ny, int nz, int S, int nxp, double dt,
+                        const double* off, int sm_count, cudaStream_t st);
+
 // Layout conversion between the reference AoS [x][y][z][S] (double) and the
 // device SoA [S][z][y][nxp] (T).
 // off: [S] offsets subtracted on pack / added on unpack (FP32), or null.

@@ -220,6 +220,15 @@ int bfvm_set_bulk_rates(bfvm_ctx* ctx, const double* supply, const double* targe
  * BFVM_ERR_STATE if no rates were set.  Asynchronous on the solve's stream. */
 int bfvm_apply_bulk_sources(bfvm_ctx* ctx);
 
+/* Microenvironment::write_to_matlab(filename)
+ * (BioFVM/BioFVM_microenvironment.cpp:1222-1249, BioFVM_matlab.cpp:536-578):
+ * the MATLAB v4 file with one column [cx, cy, cz, volume, densities...] per
+ * voxel in reference order, for a domain whose lower corner is
+ * (x_start, y_start, z_start) -- the bounding box the reference's
+ * resize_space was given.  Byte-identical to the reference's file for an FP64
+ * solve.  BFVM_ERR_ARG if the file cannot be written.  Synchronous. */
+int bfvm_write_matlab(bfvm_ctx* ctx, const char* path, double x_start, double y_start, double z_start);
+
 /* Gradients of every substrate at every voxel of the current field,
  * out[(v*S + d)*3 + axis] (v = reference voxel index, axis x/y/z) in host
  * memory -- Microenvironment::compute_all_gradient_vectors followed by

@@ -15,6 +15,8 @@
 #include "lod3d_oracle.h"
 
 #include <math.h>
+#include <stdio.h>
+#include <string.h>
 #include <stddef.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -258,4 +260,29 @@ void orc_bulk_sources(double* field, long n_values, double dt, const double* sup
     r /= t3;
     field[q] = r;
   }
+}
+
+/* BioFVM/BioFVM_microenvironment.cpp:1222-1249, BioFVM/BioFVM_matlab.cpp:536-578,
+ * centres from BioFVM/BioFVM_mesh.cpp:1436-1560 (one rank: the local start is
+ * start + 0.0). */
+int orc_write_matlab(const char* path, const double* field, int nx, int ny, int nz, int S, double x0, double y0,
+                     double z0, double dx) {
+  FILE* fp = fopen(path, "wb");
+  if (!fp) return -1;
+  static const char name[] = "multiscale_microenvironment";
+  const unsigned int hdr[5] = {0u, (unsigned int)(4 + S), (unsigned int)((long)nx * ny * nz), 0u,
+                               (unsigned int)(sizeof(name) - 1)};
+  fwrite(hdr, sizeof(unsigned int), 5, fp);
+  fwrite(name, 1, sizeof(name) - 1, fp);
+  double dv = dx * dx;
+  dv *= dx;
+  const double xs = x0 + 0.0, ys = y0 + 0.0, zs = z0 + 0.0;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        const double col[4] = {fma(i + 0.5, dx, xs), fma(j + 0.5, dx, ys), fma(k + 0.5, dx, zs), dv};
+        fwrite(col, sizeof(double), 4, fp);
+        fwrite(field + (((long)i * ny + j) * nz + k) * S, sizeof(double), (size_t)S, fp);
+      }
+  return fclose(fp) == 0 ? 0 : -1;
 }

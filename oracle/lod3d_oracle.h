@@ -83,6 +83,18 @@ void orc_gradients(const double* field, int nx, int ny, int nz, int S, double dx
 void orc_bulk_sources(double* field, long n_values, double dt, const double* supply, const double* target,
                       const double* uptake);
 
+/* Microenvironment::write_to_matlab(filename), one rank
+ * (BioFVM/BioFVM_microenvironment.cpp:1222-1249 with write_matlab4_header,
+ * BioFVM/BioFVM_matlab.cpp:536-578): a 20-byte MATLAB v4 header (type 0,
+ * rows 4+S, cols = voxels, imag 0, name length), the name
+ * "multiscale_microenvironment" without terminator, then per voxel in
+ * reference order the column [cx, cy, cz, dx*dy*dz, densities...].  Voxel
+ * centres are fma(i + 0.5, dx, start) as the reference's build computes
+ * x_start + (i+0.5)*dx (BioFVM/BioFVM_mesh.cpp:1436-1560).  Returns 0, or -1
+ * if the file cannot be written. */
+int orc_write_matlab(const char* path, const double* field, int nx, int ny, int nz, int S, double x0, double y0,
+                     double z0, double dx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,6 +63,8 @@ class Port:
             L.orc_gradients.restype = None
             L.orc_bulk_sources.argtypes = [_dp, C.c_long, C.c_double, _dp, _dp, _dp]
             L.orc_bulk_sources.restype = None
+            L.orc_write_matlab.argtypes = [C.c_char_p, _dp] + [C.c_int] * 4 + [C.c_double] * 4
+            L.orc_write_matlab.restype = C.c_int
             cls._lib = L
         return cls._lib
 
@@ -123,6 +125,14 @@ class Port:
         cls.lib().orc_bulk_sources(f.reshape(-1), f.size, float(dt), _f64(supply).ravel(), _f64(target).ravel(),
                                    _f64(uptake).ravel())
         return f
+
+    @classmethod
+    def write_matlab(cls, path, field, shape, origin, dx):
+        nx, ny, nz, S = shape
+        rc = cls.lib().orc_write_matlab(os.fsencode(path), _f64(field).ravel(), nx, ny, nz, S,
+                                        float(origin[0]), float(origin[1]), float(origin[2]), float(dx))
+        if rc != 0:
+            raise OSError(f"could not write {path}")
 
     @classmethod
     def gradients(cls, field, shape, dx):
@@ -248,6 +258,8 @@ class Reference:
             L.ref_env_gradients.restype = None
             L.ref_env_bulk.argtypes = [vp, C.c_double, _dp, _dp, _dp, C.c_int]
             L.ref_env_bulk.restype = None
+            L.ref_env_write_matlab.argtypes = [vp, C.c_char_p]
+            L.ref_env_write_matlab.restype = None
             if dropin:
                 L.ref_env_dropin_fuse_sources.argtypes = [vp, C.c_int, C.c_double]
                 L.ref_env_dropin_fuse_sources.restype = C.c_int
@@ -306,6 +318,11 @@ class Reference:
         self._bulk = tuple(_f64(a).ravel().copy() for a in (supply, target, uptake))  # kept alive
         with _stdout_to_stderr():
             self.L.ref_env_bulk(self.h, self.wl.dt, *self._bulk, threads)
+
+    def write_matlab(self, path):
+        """The reference's Microenvironment::write_to_matlab(path)."""
+        with _stdout_to_stderr():
+            self.L.ref_env_write_matlab(self.h, os.fsencode(path))
 
     def gradients(self):
         """The reference's compute_all_gradient_vectors on the current field,

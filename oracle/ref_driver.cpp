@@ -307,6 +307,14 @@ void ref_env_bulk(void* h, double dt, const double* supply, const double* target
   M.simulate_bulk_sources_and_sinks(dt);
 }
 
+/* Microenvironment::write_to_matlab(filename) (BioFVM_microenvironment.cpp:
+ * 1222-1249): MATLAB v4 header, then one column [cx, cy, cz, volume,
+ * densities...] per voxel. */
+void ref_env_write_matlab(void* h, const char* path) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  e->M->write_to_matlab(std::string(path));
+}
+
 /* Microenvironment::compute_all_gradient_vectors
  * (BioFVM/BioFVM_microenvironment.cpp:1454-1616), read back through the
  * public gradient_vector(n) accessor (:1431-1441) as out[(n*S + d)*3 + axis].

@@ -74,6 +74,7 @@ _SIGS = {
     "bfvm_compute_gradients": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_set_bulk_rates": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "bfvm_apply_bulk_sources": (C.c_int, [C.c_void_p]),
+    "bfvm_write_matlab": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double]),
     "bfvm_compute_gradients_device": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_field_offsets": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_get_launch": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),

@@ -174,6 +174,14 @@ class Microenvironment:
     def simulate_bulk_sources_and_sinks(self):
         check(self.L.bfvm_apply_bulk_sources(self.h), "bfvm_apply_bulk_sources")
 
+    def write_to_matlab(self, path, origin):
+        """Microenvironment::write_to_matlab: the MATLAB v4 density file;
+        origin is the domain's lower corner (x, y, z)."""
+        import os
+
+        check(self.L.bfvm_write_matlab(self.h, os.fsencode(str(path)), float(origin[0]), float(origin[1]),
+                                       float(origin[2])), "bfvm_write_matlab")
+
     def compute_all_gradient_vectors(self, out=None):
         """Gradients of every substrate at every voxel, [voxels, S, 3] in the
         reference's voxel order (Microenvironment::compute_all_gradient_vectors)."""

@@ -469,7 +469,9 @@ int bfvm_set_dirichlet_uniform(bfvm_ctx* c, const double* values) {
   return BFVM_OK;
 }
 
-static int ensure_staging(bfvm_ctx* c) {
+}  // extern "C"
+
+int bfvm::ensure_staging(bfvm_ctx* c) {
   if (c->d_staging) return BFVM_OK;
   return dalloc(c, reinterpret_cast<void**>(&c->d_staging),
                 sizeof(double) * static_cast<size_t>(c->nx) * c->ny * c->nz * c->S);
@@ -525,7 +527,7 @@ static int pack_from_device_aos(bfvm_ctx* c, const double* d_aos) {
   return BFVM_OK;
 }
 
-static int unpack_to_device_aos(bfvm_ctx* c, double* d_aos) {
+int bfvm::unpack_to_device_aos(bfvm_ctx* c, double* d_aos) {
   if (c->prec == BFVM_FP64)
     BFVM_CUDA(launch_unpack<double>(static_cast<const double*>(c->f), d_aos, c->nx, c->ny, c->nz, c->S, c->nxp,
                                     nullptr, c->stream));
@@ -535,6 +537,8 @@ static int unpack_to_device_aos(bfvm_ctx* c, double* d_aos) {
   note_launches(1);
   return BFVM_OK;
 }
+
+extern "C" {
 
 int bfvm_upload_field(bfvm_ctx* c, const double* field) {
   if (!c || !field) return BFVM_ERR_ARG;

@@ -88,6 +88,11 @@ struct DeviceGuard {
   }
 };
 
+// Host-transfer helpers of bfvm_capi.cu: the reference-layout staging buffer
+// (allocated on first use) and the device-layout -> reference-layout copy.
+int ensure_staging(bfvm_ctx* c);
+int unpack_to_device_aos(bfvm_ctx* c, double* d_aos);
+
 inline int dalloc(bfvm_ctx* c, void** p, size_t bytes) {
   if (bytes == 0) bytes = 16;
   cudaError_t e = cudaMalloc(p, bytes);

@@ -162,6 +162,35 @@ int bfvm_apply_sources(bfvm_ctx* ctx);
 int bfvm_apply_sources_noalloc(bfvm_ctx* ctx, int n, const int* voxel, const unsigned char* active,
                                const double* c1, const double* c2, const double* e2);
 
+/* Tracking of the substrates each agent internalizes: the reference's
+ * Microenvironment_Options::track_internalized_substrates_in_each_agent
+ * (BioFVM/BioFVM_microenvironment.h:477), per solve instead of per process.
+ * While on, every source/sink stage (bfvm_step with BFVM_STEP_SOURCES,
+ * bfvm_apply_sources, bfvm_batch_step) also keeps each agent's internalized
+ * amounts [n][S] (agent-list order), as Basic_Agent::simulate_secretion_and_uptake
+ * does (BioFVM/BioFVM_basic_agent.cpp:520-532, 553-556):
+ *   internal -= (((1 - c2) * rho + c1) / c2) * dx^3   before the agent's update,
+ *   internal -= e1                                    after it,
+ * e1 = net_export_rate * dt (:261-262).  Amounts start at zero; a new agent
+ * list keeps the amounts of the list positions it shares with the previous
+ * list and starts the others at zero.  bfvm_apply_sources_noalloc does not
+ * track.  Turning tracking off keeps nothing. */
+int bfvm_set_agent_tracking(bfvm_ctx* ctx, int on);
+/* e1 [n][S] (host, agent-list order) for a list set with bfvm_set_agents,
+ * whose exports otherwise count as zero; bfvm_set_agents_from_rates derives
+ * them from its net export rates.  Set again after every bfvm_set_agents.
+ * BFVM_ERR_STATE while tracking is off. */
+int bfvm_set_agent_exports(bfvm_ctx* ctx, const double* export1);
+/* Read / write the internalized amounts [n][S] (host, agent-list order);
+ * in == NULL writes zeros.  BFVM_ERR_STATE while tracking is off. */
+int bfvm_get_internalized(bfvm_ctx* ctx, double* out);
+int bfvm_set_internalized(bfvm_ctx* ctx, const double* in);
+/* Basic_Agent::release_internalized_substrates (BioFVM_basic_agent.cpp:
+ * 310-333) for count agents (list indices), in the order given: the voxel's
+ * densities gain internal / dx^3 * fraction[q][s] and the agent's amounts
+ * become zero.  fraction [count][S] host (fraction_released_at_death). */
+int bfvm_release_internalized(bfvm_ctx* ctx, int count, const int* agents, const double* fraction);
+
 /* Densities at each agent's voxel, [n][S] host doubles, in agent-list order
  * (what Basic_Agent::nearest_density_vector returns to each agent,
  * BioFVM/BioFVM_basic_agent.cpp:389-392). */

@@ -286,3 +286,45 @@ int orc_write_matlab(const char* path, const double* field, int nx, int ny, int 
       }
   return fclose(fp) == 0 ? 0 : -1;
 }
+
+/* BioFVM/BioFVM_basic_agent.cpp:509-559 with tracking on, in its operation
+ * order (no contractions: the steps run in separate loops and vector
+ * operators). */
+void orc_sources_tracked(double* field, int S, int n, const int* voxel, const unsigned char* active, const double* c1,
+                         const double* c2, const double* e2, const double* e1, double vvox, double* internal) {
+  for (int a = 0; a < n; ++a) {
+    if ((active && !active[a]) || voxel[a] < 0) continue;
+    double* rho = field + (size_t)voxel[a] * S;
+    for (int d = 0; d < S; ++d) {
+      const size_t q = (size_t)a * S + d;
+      double tec = 1.0;
+      tec -= c2[q];
+      tec *= rho[d];
+      tec += c1[q];
+      tec /= c2[q];
+      tec *= vvox;
+      internal[q] -= tec;
+    }
+    for (int d = 0; d < S; ++d) rho[d] += c1[(size_t)a * S + d];
+    for (int d = 0; d < S; ++d) rho[d] /= c2[(size_t)a * S + d];
+    for (int d = 0; d < S; ++d) rho[d] += e2[(size_t)a * S + d];
+    for (int d = 0; d < S; ++d) internal[(size_t)a * S + d] -= e1[(size_t)a * S + d];
+  }
+}
+
+/* BioFVM/BioFVM_basic_agent.cpp:310-333 for agents[0..count) in that order:
+ * internal /= vvox; internal *= fraction; rho += internal; internal = 0.
+ * Agents without a voxel (voxel < 0) are skipped. */
+void orc_release_internalized(double* field, int S, int count, const int* agents, const int* voxel,
+                              const double* fraction, double vvox, double* internal) {
+  for (int q = 0; q < count; ++q) {
+    const int a = agents[q];
+    if (voxel[a] < 0) continue;
+    double* rho = field + (size_t)voxel[a] * S;
+    double* in = internal + (size_t)a * S;
+    for (int d = 0; d < S; ++d) in[d] /= vvox;
+    for (int d = 0; d < S; ++d) in[d] *= fraction[(size_t)q * S + d];
+    for (int d = 0; d < S; ++d) rho[d] += in[d];
+    for (int d = 0; d < S; ++d) in[d] = 0.0;
+  }
+}

@@ -95,6 +95,21 @@ void orc_bulk_sources(double* field, long n_values, double dt, const double* sup
 int orc_write_matlab(const char* path, const double* field, int nx, int ny, int nz, int S, double x0, double y0,
                      double z0, double dx);
 
+/* orc_sources with the reference's tracking of internalized substrates
+ * (Microenvironment_Options::track_internalized_substrates_in_each_agent;
+ * BioFVM/BioFVM_basic_agent.cpp:520-532, 553-556): before agent a updates its
+ * voxel, internal[a][d] -= (((1 - c2) * rho + c1) / c2) * vvox, and after it,
+ * internal[a][d] -= e1[a][d] (its export in one step, net export rate * dt).
+ * internal accumulates: callers start it where they want. */
+void orc_sources_tracked(double* field, int S, int n, const int* voxel, const unsigned char* active, const double* c1,
+                         const double* c2, const double* e2, const double* e1, double vvox, double* internal);
+
+/* Basic_Agent::release_internalized_substrates (BioFVM/BioFVM_basic_agent.cpp:
+ * 310-333) for the listed agents in order; fraction [count][S] is each
+ * one's fraction_released_at_death. */
+void orc_release_internalized(double* field, int S, int count, const int* agents, const int* voxel,
+                              const double* fraction, double vvox, double* internal);
+
 #ifdef __cplusplus
 }
 #endif

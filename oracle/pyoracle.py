@@ -65,6 +65,11 @@ class Port:
             L.orc_bulk_sources.restype = None
             L.orc_write_matlab.argtypes = [C.c_char_p, _dp] + [C.c_int] * 4 + [C.c_double] * 4
             L.orc_write_matlab.restype = C.c_int
+            L.orc_sources_tracked.argtypes = [_dp, C.c_int, C.c_int, _ip, C.c_void_p, _dp, _dp, _dp, _dp, C.c_double,
+                                              _dp]
+            L.orc_sources_tracked.restype = None
+            L.orc_release_internalized.argtypes = [_dp, C.c_int, C.c_int, _ip, _ip, _dp, C.c_double, _dp]
+            L.orc_release_internalized.restype = None
             cls._lib = L
         return cls._lib
 
@@ -125,6 +130,28 @@ class Port:
         cls.lib().orc_bulk_sources(f.reshape(-1), f.size, float(dt), _f64(supply).ravel(), _f64(target).ravel(),
                                    _f64(uptake).ravel())
         return f
+
+    @classmethod
+    def sources_tracked(cls, field, S, voxel, c1, c2, e2, e1, vvox, internal, active=None):
+        """sources() with internalized-substrate tracking; internal [n, S]
+        accumulates in place."""
+        voxel = np.ascontiguousarray(voxel, np.int32)
+        act = None if active is None else np.ascontiguousarray(active, np.uint8)
+        cls.lib().orc_sources_tracked(field.reshape(-1), S, len(voxel), voxel,
+                                      None if act is None else act.ctypes.data_as(C.c_void_p),
+                                      _f64(c1).ravel(), _f64(c2).ravel(), _f64(e2).ravel(), _f64(e1).ravel(),
+                                      float(vvox), internal.reshape(-1))
+        return field
+
+    @classmethod
+    def release_internalized(cls, field, S, agents, voxel, fraction, vvox, internal):
+        """Release the listed agents' internalized amounts into their voxels
+        (in order); internal [n, S] and field change in place."""
+        agents = np.ascontiguousarray(agents, np.int32)
+        cls.lib().orc_release_internalized(field.reshape(-1), S, len(agents), agents,
+                                           np.ascontiguousarray(voxel, np.int32), _f64(fraction).ravel(),
+                                           float(vvox), internal.reshape(-1))
+        return field
 
     @classmethod
     def write_matlab(cls, path, field, shape, origin, dx):
@@ -260,6 +287,14 @@ class Reference:
             L.ref_env_bulk.restype = None
             L.ref_env_write_matlab.argtypes = [vp, C.c_char_p]
             L.ref_env_write_matlab.restype = None
+            L.ref_set_tracking.argtypes = [C.c_int]
+            L.ref_set_tracking.restype = None
+            L.ref_env_agent_internalized.argtypes = [vp, C.c_int, _dp]
+            L.ref_env_agent_internalized.restype = None
+            L.ref_env_agent_set_internalized.argtypes = [vp, C.c_int, _dp]
+            L.ref_env_agent_set_internalized.restype = None
+            L.ref_env_agent_release.argtypes = [vp, C.c_int, _dp]
+            L.ref_env_agent_release.restype = None
             if dropin:
                 L.ref_env_dropin_fuse_sources.argtypes = [vp, C.c_int, C.c_double]
                 L.ref_env_dropin_fuse_sources.restype = C.c_int
@@ -318,6 +353,29 @@ class Reference:
         self._bulk = tuple(_f64(a).ravel().copy() for a in (supply, target, uptake))  # kept alive
         with _stdout_to_stderr():
             self.L.ref_env_bulk(self.h, self.wl.dt, *self._bulk, threads)
+
+    def set_tracking(self, on):
+        """The process-wide track_internalized_substrates_in_each_agent option."""
+        self.L.ref_set_tracking(1 if on else 0)
+
+    def internalized(self):
+        """Every agent's internalized_substrates, [n, S]."""
+        n, S = self.wl.n_agents, self.wl.S
+        out = np.zeros((n, S))
+        o = np.zeros(S)
+        for a in range(n):
+            self.L.ref_env_agent_internalized(self.h, a, o)
+            out[a] = o
+        return out
+
+    def set_internalized(self, amounts):
+        for a in range(self.wl.n_agents):
+            self.L.ref_env_agent_set_internalized(self.h, a, _f64(amounts[a]))
+
+    def release(self, agents, fraction):
+        """release_internalized_substrates for the listed agents, in order."""
+        for q, a in enumerate(agents):
+            self.L.ref_env_agent_release(self.h, int(a), _f64(fraction[q]))
 
     def write_matlab(self, path):
         """The reference's Microenvironment::write_to_matlab(path)."""

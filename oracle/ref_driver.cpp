@@ -307,6 +307,34 @@ void ref_env_bulk(void* h, double dt, const double* supply, const double* target
   M.simulate_bulk_sources_and_sinks(dt);
 }
 
+/* Microenvironment_Options::track_internalized_substrates_in_each_agent
+ * (BioFVM_microenvironment.h:477), read by every agent's
+ * simulate_secretion_and_uptake (BioFVM_basic_agent.cpp:520-532, 553-556). */
+void ref_set_tracking(int on) { default_microenvironment_options.track_internalized_substrates_in_each_agent = on != 0; }
+
+/* Agent a's internalized_substrates [S] (BioFVM_basic_agent.h:134). */
+void ref_env_agent_internalized(void* h, int a, double* out) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  const std::vector<double>& v = *e->agents[a]->internalized_substrates;
+  for (int d = 0; d < e->S; ++d) out[d] = d < (int)v.size() ? v[d] : 0.0;
+}
+
+/* Overwrite agent a's internalized_substrates [S]. */
+void ref_env_agent_set_internalized(void* h, int a, const double* in) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  e->agents[a]->internalized_substrates->assign(in, in + e->S);
+}
+
+/* Basic_Agent::release_internalized_substrates (BioFVM_basic_agent.cpp:
+ * 310-333) for agent a with fraction_released_at_death = fraction [S]; the
+ * reference reads the default microenvironment, which is set to this one. */
+void ref_env_agent_release(void* h, int a, const double* fraction) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  set_default_microenvironment(e->M);
+  e->agents[a]->fraction_released_at_death->assign(fraction, fraction + e->S);
+  e->agents[a]->release_internalized_substrates();
+}
+
 /* Microenvironment::write_to_matlab(filename) (BioFVM_microenvironment.cpp:
  * 1222-1249): MATLAB v4 header, then one column [cx, cy, cz, volume,
  * densities...] per voxel. */

@@ -63,6 +63,11 @@ _SIGS = {
     "bfvm_apply_sources": (C.c_int, [C.c_void_p]),
     "bfvm_apply_sources_noalloc": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 5),
     "bfvm_sample_agents": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bfvm_set_agent_tracking": (C.c_int, [C.c_void_p, C.c_int]),
+    "bfvm_set_agent_exports": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bfvm_get_internalized": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bfvm_set_internalized": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bfvm_release_internalized": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "bfvm_field_sums": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_synchronize": (C.c_int, [C.c_void_p]),
     "bfvm_stream": (C.c_void_p, [C.c_void_p]),

@@ -150,6 +150,39 @@ class Microenvironment:
         check(self.L.bfvm_sample_agents(self.h, _ptr(out)), "bfvm_sample_agents")
         return out
 
+    # -- internalized substrates ---------------------------------------------
+    def set_track_internalized_substrates(self, on=True):
+        """Microenvironment_Options::track_internalized_substrates_in_each_agent
+        for this solve: every source/sink stage also keeps each agent's
+        internalized amounts (Basic_Agent::internalized_substrates)."""
+        check(self.L.bfvm_set_agent_tracking(self.h, 1 if on else 0), "bfvm_set_agent_tracking")
+
+    def set_agent_exports(self, export1):
+        """Per-agent export per step (net_export_rate * dt), [n, S], for a list
+        given as constants by set_agents."""
+        e1 = _f64(export1).reshape(self.n_agents, self.S)
+        check(self.L.bfvm_set_agent_exports(self.h, _ptr(e1)), "bfvm_set_agent_exports")
+
+    def internalized_substrates(self):
+        """Every agent's internalized amounts, [n, S] in agent-list order."""
+        out = np.empty((self.n_agents, self.S), np.float64)
+        check(self.L.bfvm_get_internalized(self.h, _ptr(out)), "bfvm_get_internalized")
+        return out
+
+    def set_internalized_substrates(self, amounts=None):
+        """Overwrite the internalized amounts ([n, S]; None: zeros)."""
+        a = None if amounts is None else _f64(amounts).reshape(self.n_agents, self.S)
+        check(self.L.bfvm_set_internalized(self.h, _ptr(a)), "bfvm_set_internalized")
+
+    def release_internalized_substrates(self, agents, fraction):
+        """Basic_Agent::release_internalized_substrates for the listed agents
+        (in order); fraction [len(agents), S] is each one's
+        fraction_released_at_death."""
+        idx = np.ascontiguousarray(agents, np.int32).ravel()
+        fr = _f64(np.broadcast_to(np.asarray(fraction, np.float64), (idx.size, self.S)))
+        check(self.L.bfvm_release_internalized(self.h, int(idx.size), _ptr(idx), _ptr(fr)),
+              "bfvm_release_internalized")
+
     # -- stepping -----------------------------------------------------------
     def simulate_diffusion_decay(self, nsteps=1, sources=False):
         """nsteps LOD steps; with sources=True each step first applies the agents

@@ -50,11 +50,14 @@ __global__ void agent_keys_kernel(int n, const int* __restrict__ voxel, const un
 
 // Basic_Agent::set_internal_uptake_constants (BioFVM_basic_agent.cpp:224-274),
 // operation by operation; the two axpy calls are fused multiply-adds as in the
-// reference's g++ build.
+// reference's g++ build.  e1 (optional) receives net_export_rate * dt, the
+// export an agent with internalized-substrate tracking subtracts from its own
+// amounts each step (cell_source_sink_solver_temp_export1).
 __global__ void agent_constants_kernel(int n, int S, double dt, double voxel_volume, const double* __restrict__ volume,
                                        const double* __restrict__ sec, const double* __restrict__ upt,
                                        const double* __restrict__ sat, const double* __restrict__ exp_,
-                                       double* __restrict__ c1, double* __restrict__ c2, double* __restrict__ e2) {
+                                       double* __restrict__ c1, double* __restrict__ c2, double* __restrict__ e2,
+                                       double* __restrict__ e1) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n * S) return;
   const int a = idx / S;
@@ -71,6 +74,7 @@ __global__ void agent_constants_kernel(int n, int S, double dt, double voxel_vol
   c1[idx] = t1;
   c2[idx] = t2;
   e2[idx] = x1 / voxel_volume;
+  if (e1) e1[idx] = x1;
 }
 
 __global__ void radix_hist_kernel(int n, const unsigned* __restrict__ keys, int shift, int nblocks,
@@ -194,7 +198,7 @@ template <typename T>
 __global__ void agent_sources_kernel(int n, const unsigned* __restrict__ sk, unsigned sentinel, int S, int nx, int ny,
                                      int nz, int nxp, const double* __restrict__ ac1, const double* __restrict__ ac2,
                                      const double* __restrict__ ae2, const double* __restrict__ off,
-                                     T* __restrict__ f) {
+                                     T* __restrict__ f, const AgentTrack tr) {
   const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (idx >= static_cast<long long>(n) * S) return;
   const int s = static_cast<int>(idx / n);
@@ -208,9 +212,8 @@ __global__ void agent_sources_kernel(int n, const unsigned* __restrict__ sk, uns
   double r = static_cast<double>(*rho);
   if (off) r += off[s];
   for (int q = p; q < n && sk[q] == key; ++q) {
-    r += ac1[static_cast<size_t>(s) * n + q];
-    r /= ac2[static_cast<size_t>(s) * n + q];
-    r += ae2[static_cast<size_t>(s) * n + q];
+    const size_t c = static_cast<size_t>(s) * n + q;
+    r = agent_update(r, ac1[c], ac2[c], ae2[c], q, s, tr);
   }
   if (off) r -= off[s];
   *rho = static_cast<T>(r);
@@ -278,11 +281,11 @@ size_t agent_scratch_bytes(int n) {
 
 cudaError_t agents_compute_constants(int n, int S, double dt, double voxel_volume, const double* volume,
                                      const double* sec, const double* upt, const double* sat, const double* exp_,
-                                     double* c1, double* c2, double* e2, cudaStream_t st) {
+                                     double* c1, double* c2, double* e2, cudaStream_t st, double* e1) {
   if (n == 0) return cudaSuccess;
   const int total = n * S;
   agent_constants_kernel<<<(total + 255) / 256, 256, 0, st>>>(n, S, dt, voxel_volume, volume, sec, upt, sat, exp_, c1,
-                                                              c2, e2);
+                                                              c2, e2, e1);
   return cudaGetLastError();
 }
 
@@ -386,12 +389,32 @@ template cudaError_t agents_apply_sources_by_order<float>(int, const unsigned*, 
 template <typename T>
 cudaError_t agents_apply_sources(int n, const unsigned* sorted_keys, int S, int nx, int ny, int nz, int nxp,
                                  const double* ac1, const double* ac2, const double* ae2, const double* off, T* f,
-                                 cudaStream_t st) {
+                                 const AgentTrack& track, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   const unsigned sentinel = static_cast<unsigned>(nx) * ny * nz;
   const long long total = static_cast<long long>(n) * S;
   agent_sources_kernel<T><<<static_cast<unsigned>((total + 255) / 256), 256, 0, st>>>(
-      n, sorted_keys, sentinel, S, nx, ny, nz, nxp, ac1, ac2, ae2, off, f);
+      n, sorted_keys, sentinel, S, nx, ny, nz, nxp, ac1, ac2, ae2, off, f, track);
+  return cudaGetLastError();
+}
+
+namespace {
+// dst[s*n + p] = src[order[p]*S + s]: a per-agent [n][S] array gathered into
+// sorted order, substrate-major.
+__global__ void gather_sorted_kernel(int n, int S, const int* __restrict__ order, const double* __restrict__ src,
+                                     double* __restrict__ dst) {
+  const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= static_cast<long long>(n) * S) return;
+  const int s = static_cast<int>(idx / n);
+  const int p = static_cast<int>(idx % n);
+  dst[idx] = src[static_cast<size_t>(order[p]) * S + s];
+}
+}  // namespace
+
+cudaError_t agents_gather_sorted(int n, int S, const int* order, const double* src, double* dst, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const long long total = static_cast<long long>(n) * S;
+  gather_sorted_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, st>>>(n, S, order, src, dst);
   return cudaGetLastError();
 }
 
@@ -407,9 +430,11 @@ cudaError_t agents_sample(int n, const unsigned* dev_voxel, int S, int nx, int n
 }
 
 template cudaError_t agents_apply_sources<double>(int, const unsigned*, int, int, int, int, int, const double*,
-                                                  const double*, const double*, const double*, double*, cudaStream_t);
+                                                  const double*, const double*, const double*, double*,
+                                                  const AgentTrack&, cudaStream_t);
 template cudaError_t agents_apply_sources<float>(int, const unsigned*, int, int, int, int, int, const double*,
-                                                 const double*, const double*, const double*, float*, cudaStream_t);
+                                                 const double*, const double*, const double*, float*,
+                                                 const AgentTrack&, cudaStream_t);
 template cudaError_t agents_sample<double>(int, const unsigned*, int, int, int, int, int, const double*,
                                            const double*, double*, cudaStream_t);
 template cudaError_t agents_sample<float>(int, const unsigned*, int, int, int, int, int, const float*, const double*,

@@ -6,6 +6,8 @@
 
 #include <cstddef>
 
+#include "bfvm_internal.h"
+
 namespace bfvm {
 
 struct AgentBuild {
@@ -33,7 +35,7 @@ size_t agent_scratch_bytes(int n);
 
 cudaError_t agents_compute_constants(int n, int S, double dt, double voxel_volume, const double* volume,
                                      const double* sec, const double* upt, const double* sat, const double* exp_,
-                                     double* c1, double* c2, double* e2, cudaStream_t st);
+                                     double* c1, double* c2, double* e2, cudaStream_t st, double* e1 = nullptr);
 
 // Sorts and bins the list; *launches receives the number of kernels launched.
 cudaError_t agents_build(const AgentBuild& b, cudaStream_t st, int* launches);
@@ -53,10 +55,15 @@ cudaError_t agents_apply_sources_by_order(int n, const unsigned* sorted_keys, co
                                           const double* e2, const double* off, T* f, cudaStream_t st);
 
 // off: [S] field offsets of an FP32 solve (the field holds rho - off), or null.
+// track: internalized-substrate tracking (track.internal null: off).
 template <typename T>
 cudaError_t agents_apply_sources(int n, const unsigned* sorted_keys, int S, int nx, int ny, int nz, int nxp,
                                  const double* ac1, const double* ac2, const double* ae2, const double* off, T* f,
-                                 cudaStream_t st);
+                                 const AgentTrack& track, cudaStream_t st);
+
+// dst[s*n + p] = src[order[p]*S + s]: a per-agent [n][S] array in list order
+// gathered into the sorted, substrate-major layout of ac1/ac2/ae2.
+cudaError_t agents_gather_sorted(int n, int S, const int* order, const double* src, double* dst, cudaStream_t st);
 
 template <typename T>
 cudaError_t agents_sample(int n, const unsigned* dev_voxel, int S, int nx, int ny, int nz, int nxp, const T* f,

@@ -406,9 +406,10 @@ int bfvm_batch_get_schedule(bfvm_batch* b, int* mode, int* yz_chunk, int* order,
 }
 
 // Time `trial_steps` fused steps under each candidate schedule and keep the
-// fastest.  The fields are saved before and restored after every trial, so
-// tuning leaves the solves exactly as it found them (and every schedule
-// computes the same bits anyway).
+// fastest.  The fields (and the agents' internalized amounts of tracking
+// solves) are saved before and restored after the trials, so tuning leaves
+// the solves exactly as it found them (and every schedule computes the same
+// bits anyway).
 int bfvm_batch_autotune(bfvm_batch* b, int flags, int trial_steps, double* best_ms_per_step) {
   if (!b || trial_steps < 1) return BFVM_ERR_ARG;
   if (b->members.empty()) return BFVM_OK;
@@ -416,15 +417,21 @@ int bfvm_batch_autotune(bfvm_batch* b, int flags, int trial_steps, double* best_
   int rc = bfvm_batch_synchronize(b);
   if (rc != BFVM_OK) return rc;
   std::vector<void*> saved(b->members.size(), nullptr);
+  auto internal_bytes = [](const bfvm_ctx* c) {
+    return c->track && c->d_internal ? sizeof(double) * c->S * static_cast<size_t>(c->n_internal) : size_t{0};
+  };
   for (size_t q = 0; q < b->members.size(); ++q) {
     bfvm_ctx* c = b->members[q];
-    if (cudaMalloc(&saved[q], c->field_bytes) != cudaSuccess) {
+    if (cudaMalloc(&saved[q], c->field_bytes + internal_bytes(c)) != cudaSuccess) {
       cudaGetLastError();
       for (void* p : saved)
         if (p) cudaFree(p);
       return BFVM_ERR_OOM;
     }
     BFVM_CUDA(cudaMemcpyAsync(saved[q], c->f, c->field_bytes, cudaMemcpyDeviceToDevice, b->stream));
+    if (internal_bytes(c))
+      BFVM_CUDA(cudaMemcpyAsync(static_cast<char*>(saved[q]) + c->field_bytes, c->d_internal, internal_bytes(c),
+                                cudaMemcpyDeviceToDevice, b->stream));
   }
   struct Cand {
     int mode, yz_chunk, order, ctas;
@@ -461,6 +468,9 @@ int bfvm_batch_autotune(bfvm_batch* b, int flags, int trial_steps, double* best_
   for (size_t q = 0; q < b->members.size(); ++q) {
     bfvm_ctx* c = b->members[q];
     cudaMemcpyAsync(c->f, saved[q], c->field_bytes, cudaMemcpyDeviceToDevice, b->stream);
+    if (internal_bytes(c))
+      cudaMemcpyAsync(c->d_internal, static_cast<char*>(saved[q]) + c->field_bytes, internal_bytes(c),
+                      cudaMemcpyDeviceToDevice, b->stream);
   }
   cudaStreamSynchronize(b->stream);
   for (void* p : saved) cudaFree(p);

@@ -213,6 +213,8 @@ int free_agents(bfvm_ctx* c) {
   dfree(c, c->d_ac);
   dfree(c, c->d_agent_scratch);
   dfree(c, c->d_sample);
+  dfree(c, c->d_ae1);
+  c->d_ae1 = nullptr;
   c->d_voxel = nullptr;
   c->d_agent_active = nullptr;
   c->d_c = c->d_rates = c->d_ac = c->d_sample = nullptr;
@@ -395,6 +397,7 @@ int bfvm_destroy(bfvm_ctx* c) {
   dfree(c, c->d_staging);
   dfree(c, c->d_grad);
   dfree(c, c->d_bulk);
+  dfree(c, c->d_internal);
   for (cudaEvent_t e : c->events) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -599,7 +602,9 @@ int bfvm_set_agents(bfvm_ctx* c, int n, const int* voxel, const unsigned char* a
     BFVM_CUDA(cudaMemcpyAsync(c->d_c + static_cast<size_t>(c->S) * n, c2, row, cudaMemcpyHostToDevice, c->stream));
     BFVM_CUDA(cudaMemcpyAsync(c->d_c + 2ull * c->S * n, e2, row, cudaMemcpyHostToDevice, c->stream));
   }
-  return build_agents(c, n);
+  c->agents_from_rates = 0;
+  rc = build_agents(c, n);
+  return rc == BFVM_OK ? tracking_after_agents(c) : rc;
 }
 
 int bfvm_set_agents_from_rates(bfvm_ctx* c, int n, const int* voxel, const unsigned char* active, const double* volume,
@@ -623,7 +628,9 @@ int bfvm_set_agents_from_rates(bfvm_ctx* c, int n, const int* voxel, const unsig
                                        c->d_c + SN, c->d_c + 2 * SN, c->stream));
     note_launches(1);
   }
-  return build_agents(c, n);
+  c->agents_from_rates = 1;
+  rc = build_agents(c, n);
+  return rc == BFVM_OK ? tracking_after_agents(c) : rc;
 }
 
 int bfvm_agent_constants_device(int n, int S, double dt, double voxel_volume, const double* volume,
@@ -652,11 +659,11 @@ int bfvm_apply_sources(bfvm_ctx* c) {
   if (c->prec == BFVM_FP64)
     BFVM_CUDA(agents_apply_sources<double>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
                                            c->d_ac + SN, c->d_ac + 2 * SN, nullptr, static_cast<double*>(c->f),
-                                           c->stream));
+                                           track_params(c), c->stream));
   else
     BFVM_CUDA(agents_apply_sources<float>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
                                           c->d_ac + SN, c->d_ac + 2 * SN, c->d_off, static_cast<float*>(c->f),
-                                          c->stream));
+                                          track_params(c), c->stream));
   note_launches(1);
   return BFVM_OK;
 }

@@ -47,6 +47,12 @@ struct bfvm_ctx {
   int* d_nvalid = nullptr;
   void* d_agent_scratch = nullptr;
   double* d_sample = nullptr;
+  // internalized-substrate tracking (bfvm_set_agent_tracking)
+  int track = 0;
+  double* d_ae1 = nullptr;      // [S][cap_agents] export per step, sorted order
+  double* d_internal = nullptr; // [cap_internal][S] amounts per agent, list order
+  int n_internal = 0, cap_internal = 0;
+  int agents_from_rates = 0;    // the list came from bfvm_set_agents_from_rates (rates kept in d_rates)
   // host-side mirrors
   std::vector<unsigned char> active;
   std::vector<double> faces;    // same layout as d_faces
@@ -93,6 +99,11 @@ struct DeviceGuard {
 int ensure_staging(bfvm_ctx* c);
 int unpack_to_device_aos(bfvm_ctx* c, double* d_aos);
 
+// bfvm_tracking.cu: after a new agent list is built, bring the tracking
+// buffers to its size (amounts of surviving list positions kept, new ones
+// zeroed) and set the per-step exports (from the rates, else zero).
+int tracking_after_agents(bfvm_ctx* c);
+
 inline int dalloc(bfvm_ctx* c, void** p, size_t bytes) {
   if (bytes == 0) bytes = 16;
   cudaError_t e = cudaMalloc(p, bytes);
@@ -115,6 +126,18 @@ inline void dfree(bfvm_ctx* c, void* p) {
     c->alloc_bytes.erase(it);
   }
   cudaFree(p);
+}
+
+inline AgentTrack track_params(const bfvm_ctx* c) {
+  AgentTrack t{};
+  if (!c->track || c->n_agents == 0) return t;
+  t.internal = c->d_internal;
+  t.order = c->d_sorted_vals;
+  t.ae1 = c->d_ae1;
+  t.vvox = c->dx * c->dx * c->dx;
+  t.S = c->S;
+  t.n = c->n_agents;
+  return t;
 }
 
 template <typename T>
@@ -152,6 +175,7 @@ inline SweepParams<T> make_params(bfvm_ctx* c, bool sources) {
     p.ac2 = c->d_ac + S * c->n_agents;
     p.ae2 = c->d_ac + 2 * S * c->n_agents;
     p.n_sorted = c->n_agents;
+    if (c->track) p.track = track_params(c);
   }
   p.screen = c->screen;
   p.status = c->d_status;

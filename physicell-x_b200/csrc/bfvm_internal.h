@@ -64,6 +64,43 @@ struct AxisCoefs {
 // stays below n + 96.
 inline int coef_pad(int n) { return (n + 96 + 31) / 32 * 32; }
 
+// Tracking of the substrates each agent internalizes
+// (Microenvironment_Options::track_internalized_substrates_in_each_agent;
+// BioFVM/BioFVM_basic_agent.cpp:520-532, 553-556).  internal == nullptr
+// turns it off.
+struct AgentTrack {
+  double* internal;      // [n][S] per agent in list order: accumulated change
+  const int* order;      // [n] agent index at each sorted position
+  const double* ae1;     // [S][n] export per step (net export rate * dt), sorted
+  double vvox;           // voxel volume
+  int S, n;
+};
+
+// One agent's update of one density value r (FP64), agent at sorted position
+// q, substrate s: the reference's rho += c1; rho /= c2; rho += e2, with the
+// internalized-substrate bookkeeping around it when tracking is on.  The
+// build's -fmad=false keeps every operation separately rounded, as the
+// reference's separate loops and vector operators are.
+__device__ __forceinline__ double agent_update(double r, double c1, double c2, double e2, int q, int s,
+                                               const AgentTrack& tr) {
+  double* in = nullptr;
+  if (tr.internal) {
+    double tec = 1.0;
+    tec -= c2;
+    tec *= r;
+    tec += c1;
+    tec /= c2;
+    tec *= tr.vvox;
+    in = tr.internal + static_cast<size_t>(tr.order[q]) * tr.S + s;
+    *in -= tec;
+  }
+  r += c1;
+  r /= c2;
+  r += e2;
+  if (in) *in -= tr.ae1[static_cast<size_t>(s) * tr.n + q];
+  return r;
+}
+
 template <typename T>
 struct SweepParams {
   T* f;                  // field base
@@ -90,6 +127,7 @@ struct SweepParams {
   const double* ac2;
   const double* ae2;
   int n_sorted;
+  AgentTrack track;      // internalized-substrate tracking (track.internal null: off)
   // Nonzero when no substrate has a negative diffusion coefficient or decay
   // rate (c1 >= 0, every denominator >= 1): enables the FP64 input screen.
   int screen;

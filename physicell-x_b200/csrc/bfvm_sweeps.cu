@@ -146,23 +146,18 @@ __device__ __forceinline__ double back_elem(double c, double xn, double y) { ret
 
 // Apply the run of agents that starts at sorted position q (key `key`,
 // constants c1/c2/e2 of that first agent already loaded) to the staged value
-// at *e, in sorted order -- which is agent-list order within a voxel --
-// with the reference's three operations per agent, in FP64.
+// at *e of substrate s, in sorted order -- which is agent-list order within a
+// voxel -- with the reference's three operations per agent, in FP64.
 template <typename T>
 __device__ __forceinline__ void apply_run(T* e, int q, unsigned key, double c1, double c2, double e2, int qend,
                                           const unsigned* __restrict__ a_key, const double* __restrict__ ac1,
                                           const double* __restrict__ ac2, const double* __restrict__ ae2,
-                                          double off) {
+                                          double off, int s, const AgentTrack& tr) {
   double r = static_cast<double>(*e);
   if constexpr (kF32<T>) r += off;
-  r += c1;
-  r /= c2;
-  r += e2;
-  for (int q2 = q + 1; q2 < qend && __ldg(a_key + q2) == key; ++q2) {
-    r += __ldg(ac1 + q2);
-    r /= __ldg(ac2 + q2);
-    r += __ldg(ae2 + q2);
-  }
+  r = agent_update(r, c1, c2, e2, q, s, tr);
+  for (int q2 = q + 1; q2 < qend && __ldg(a_key + q2) == key; ++q2)
+    r = agent_update(r, __ldg(ac1 + q2), __ldg(ac2 + q2), __ldg(ae2 + q2), q2, s, tr);
   if constexpr (kF32<T>) r -= off;
   *e = static_cast<T>(r);
 }
@@ -324,7 +319,8 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
         for (int r = 0; r < kAgentRounds; ++r) {
           const int q = A0 + t + r * TL;
           if (q < A1 && akey[r] != aprev[r])
-            apply_run<T>(elem(akey[r]), q, akey[r], a1[r], a2[r], a3[r], A1, p.a_key, ac1, ac2, ae2, off);
+            apply_run<T>(elem(akey[r]), q, akey[r], a1[r], a2[r], a3[r], A1, p.a_key, ac1, ac2, ae2, off, s,
+                         p.track);
         }
         for (int r = kAgentRounds; A0 + r * TL < A1; ++r) {
           const int q = A0 + t + r * TL;
@@ -332,7 +328,7 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
             const unsigned key = __ldg(p.a_key + q);
             if (q == A0 || __ldg(p.a_key + q - 1) != key)
               apply_run<T>(elem(key), q, key, __ldg(ac1 + q), __ldg(ac2 + q), __ldg(ae2 + q), A1, p.a_key, ac1, ac2,
-                           ae2, off);
+                           ae2, off, s, p.track);
           }
         }
       }

@@ -41,6 +41,7 @@ struct DropinState {
   std::vector<int> voxel;
   std::vector<unsigned char> active;
   std::vector<double> c1, c2, e2, plane;
+  std::vector<double> e1, internal;  // internalized-substrate tracking
 };
 
 std::mutex g_mu;
@@ -151,6 +152,11 @@ void diffusion_decay_solver__constant_coefficients_LOD_3D(Microenvironment& M, d
   if (st.agents != nullptr) {
     // Gather the agents as Basic_Agent::simulate_secretion_and_uptake sees them
     // (BioFVM_basic_agent.cpp:509-518): constants refreshed when the volume changed.
+    // With Microenvironment_Options::track_internalized_substrates_in_each_agent
+    // on (BioFVM_microenvironment.h:477), each agent's internalized_substrates
+    // go to the GPU with it and come back after the step
+    // (BioFVM_basic_agent.cpp:520-532, 553-556).
+    const bool track = default_microenvironment_options.track_internalized_substrates_in_each_agent;
     const std::vector<Basic_Agent*>& list = *st.agents;
     const size_t n = list.size();
     st.voxel.resize(n);
@@ -158,6 +164,10 @@ void diffusion_decay_solver__constant_coefficients_LOD_3D(Microenvironment& M, d
     st.c1.resize(n * S);
     st.c2.resize(n * S);
     st.e2.resize(n * S);
+    if (track) {
+      st.e1.resize(n * S);
+      st.internal.resize(n * S);
+    }
     for (size_t a = 0; a < n; ++a) {
       Basic_Agent* ag = list[a];
       st.active[a] = ag->is_active ? 1 : 0;
@@ -171,14 +181,37 @@ void diffusion_decay_solver__constant_coefficients_LOD_3D(Microenvironment& M, d
         st.c2[a * S + d] = t2[d];
         st.e2[a * S + d] = x2[d];
       }
+      if (track) {
+        const std::vector<double>& x1 = ag->get_cell_source_sink_solver_temp_export1();
+        const std::vector<double>& in = *ag->internalized_substrates;
+        for (int d = 0; d < S; ++d) {
+          st.e1[a * S + d] = d < static_cast<int>(x1.size()) ? x1[d] : 0.0;
+          st.internal[a * S + d] = d < static_cast<int>(in.size()) ? in[d] : 0.0;
+        }
+      }
     }
+    if (failed("bfvm_set_agent_tracking", bfvm_set_agent_tracking(ctx, track ? 1 : 0))) return;
     if (failed("bfvm_set_agents", bfvm_set_agents(ctx, static_cast<int>(n), st.voxel.data(), st.active.data(),
                                                   st.c1.data(), st.c2.data(), st.e2.data())))
       return;
+    if (track && n > 0) {
+      if (failed("bfvm_set_agent_exports", bfvm_set_agent_exports(ctx, st.e1.data()))) return;
+      if (failed("bfvm_set_internalized", bfvm_set_internalized(ctx, st.internal.data()))) return;
+    }
     flags = BFVM_STEP_SOURCES;
   }
 
   if (failed("bfvm_step", bfvm_step(ctx, 1, flags))) return;
+  if ((flags & BFVM_STEP_SOURCES) && default_microenvironment_options.track_internalized_substrates_in_each_agent &&
+      !st.agents->empty()) {
+    const std::vector<Basic_Agent*>& list = *st.agents;
+    if (failed("bfvm_get_internalized", bfvm_get_internalized(ctx, st.internal.data()))) return;
+    for (size_t a = 0; a < list.size(); ++a) {
+      std::vector<double>& in = *list[a]->internalized_substrates;
+      if (static_cast<int>(in.size()) < S) in.resize(S, 0.0);
+      for (int d = 0; d < S; ++d) in[d] = st.internal[a * S + d];
+    }
+  }
   if (!st.resident) {
     if (failed("bfvm_download_field", bfvm_download_field(ctx, M.p_density_vectors->data()))) return;
   }

@@ -33,6 +33,9 @@ void bfvm_b200_lod3d_serial(Microenvironment& M, double dt);
 // Apply the given agents' sources/sinks on the GPU, fused ahead of every
 // following LOD step of M (agents == nullptr turns it off).  The caller then
 // must not also call M.simulate_cell_sources_and_sinks for those steps.
+// With default_microenvironment_options.track_internalized_substrates_in_each_agent
+// on, each step also updates every agent's internalized_substrates, as the
+// reference's agent loop would.
 int bfvm_b200_set_fused_sources(Microenvironment& M, std::vector<Basic_Agent*>* agents, double dt);
 
 // Resident mode: the field stays on the GPU between steps and the host copy

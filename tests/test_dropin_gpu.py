@@ -48,6 +48,28 @@ def test_dropin_fused_sources_bitwise():
     assert np.array_equal(a, gpu.field())
 
 
+def test_dropin_fused_sources_track_internalized():
+    """track_internalized_substrates_in_each_agent on: the drop-in carries each
+    Basic_Agent's internalized_substrates through the fused GPU stage and
+    writes them back; field and amounts equal the reference's host loop."""
+    wl = W.small_random(406, nx=19, ny=15, nz=13, S=3, n_agents=300, steps=4, stack=True)
+    assert np.any(wl.net_export != 0)
+    cpu, gpu = _pair(wl)
+    cpu.set_tracking(True)
+    try:
+        a = cpu.run(wl.steps, solver=0, sources_threads=1)
+        a_in = cpu.internalized()
+        assert gpu.L.ref_env_dropin_fuse_sources(gpu.h, 1, wl.dt) == 0
+        for _ in range(wl.steps):
+            gpu.diffusion(solver=2)
+        b_in = gpu.internalized()
+    finally:
+        cpu.set_tracking(False)
+    assert np.any(a_in != 0)
+    assert np.array_equal(a, gpu.field())
+    assert np.array_equal(a_in, b_in)
+
+
 def test_dropin_cube50_hundred_steps():
     wl = W.cube50(steps=100)
     cpu, gpu = _pair(wl)

@@ -279,6 +279,17 @@ int bfvm_compute_gradients_device(bfvm_ctx* ctx, double* d_out);
 int bfvm_get_launch(bfvm_ctx* ctx, int* x_lines, int* yz_tile, int* yz_chunk);
 int bfvm_set_launch(bfvm_ctx* ctx, int x_lines, int yz_tile, int yz_chunk);
 
+/* Schedule of the single-solve sweeps.  Persistent sweeps run a compute warp
+ * and a copy warp per CTA, as many CTAs as fit, each walking a sequence of
+ * 32-line tiles and loading the next tile while it finishes the current one
+ * (with x_lines == yz_tile == 32 and lines of at most 64 chunks; other
+ * shapes run per tile).  persistent = 1 (default): y and z sweeps
+ * persistent where every resident CTA gets at least 8 tiles, x sweep one CTA
+ * per tile; 2: all three persistent; 0: one CTA per tile everywhere.  Every
+ * schedule computes the same bits. */
+int bfvm_set_sweep_schedule(bfvm_ctx* ctx, int persistent);
+int bfvm_get_sweep_schedule(bfvm_ctx* ctx, int* persistent);
+
 /* Number of this library's kernels launched by the calls so far (counted on
  * the host at each launch). */
 long long bfvm_kernel_launches(void);

@@ -260,6 +260,17 @@ class Microenvironment:
         check(self.L.bfvm_timing_read(self.h, _ptr(ms), C.byref(n)), "bfvm_timing_read")
         return ms, int(n.value)
 
+    def set_sweep_schedule(self, persistent=1):
+        """0: one CTA per tile; 1 (default): persistent y/z sweeps (a CTA walks
+        many tiles, the next loading while the current one finishes), x per
+        tile; 2: all three sweeps persistent.  True/False map to 1/0."""
+        check(self.L.bfvm_set_sweep_schedule(self.h, int(persistent)), "bfvm_set_sweep_schedule")
+
+    def get_sweep_schedule(self):
+        v = C.c_int()
+        check(self.L.bfvm_get_sweep_schedule(self.h, C.byref(v)), "bfvm_get_sweep_schedule")
+        return int(v.value)
+
     def get_launch(self):
         a, b, c = C.c_int(), C.c_int(), C.c_int()
         check(self.L.bfvm_get_launch(self.h, C.byref(a), C.byref(b), C.byref(c)), "bfvm_get_launch")

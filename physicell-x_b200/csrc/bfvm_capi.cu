@@ -897,6 +897,20 @@ extern "C" int bfvm_release_staging(bfvm_ctx* c) {
   return BFVM_OK;
 }
 
+extern "C" int bfvm_set_sweep_schedule(bfvm_ctx* c, int persistent) {
+  if (!c || persistent < 0 || persistent > 2) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  c->cfg.persistent = persistent;
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_get_sweep_schedule(bfvm_ctx* c, int* persistent) {
+  if (!c || !persistent) return BFVM_ERR_ARG;
+  *persistent = c->cfg.persistent;
+  return BFVM_OK;
+}
+
 extern "C" int bfvm_get_launch(bfvm_ctx* c, int* x_lines, int* yz_tile, int* yz_chunk) {
   if (!c) return BFVM_ERR_ARG;
   if (x_lines) *x_lines = c->cfg.x_lines;
@@ -911,6 +925,7 @@ extern "C" int bfvm_set_launch(bfvm_ctx* c, int x_lines, int yz_tile, int yz_chu
   cfg.x_lines = x_lines;
   cfg.yz_tile = yz_tile;
   cfg.yz_chunk = yz_chunk;
+  cfg.persistent = c->cfg.persistent;
   // x_lines: multiple of 8 (1024-byte swizzle atoms), at most 256 (box
   // limit); yz_tile: 16 (FP64 only), 32 or 64 consecutive x -- whole 128-byte
   // rows, so every TMA chunk starts 128-byte aligned in shared memory and

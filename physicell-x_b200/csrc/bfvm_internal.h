@@ -134,19 +134,35 @@ struct SweepParams {
   int* status;           // device status word
 };
 
-// Launch configuration of the sweeps (chosen by the host, tunable).  One CTA
-// (one warp) owns one tile of lines and stages them whole in shared memory.
+// Launch configuration of the sweeps (chosen by the host, tunable).  A tile
+// of lines is staged whole in one CTA's shared memory.  Two schedules:
+//   persistent  a compute warp and a copy warp per CTA, as many CTAs as
+//               fit, each walking a sequence of 32-line tiles through a ring
+//               of chunk slots (the next tile loads while this one finishes);
+//   per-tile    one CTA per tile of x_lines / yz_tile lines.
+// persistent = 1 (default) runs the y and z sweeps persistent when every
+// resident CTA gets at least 8 tiles (fewer measured slower) and the x sweep
+// per tile (the per-lane agent walk of the persistent x sweep measured slower
+// than the per-tile sweep's lane-per-run agents); 2 runs all three
+// persistent whatever the tile count; 0 all per tile.  Persistent needs x_lines == yz_tile == 32 and
+// lines of at most 64 chunks; other shapes run per tile.
 struct SweepConfig {
   int x_lines = 32;   // lines per CTA in the x sweep (multiple of 8, <= 256)
   int yz_tile = 32;   // consecutive x per CTA in the y/z sweeps (whole 128-byte rows)
-  int yz_chunk = 32;  // target rows per TMA box along the line in the y/z sweeps (<= 256)
+  int yz_chunk = 32;  // target rows per TMA box along the line in the y/z sweeps (<= 256; per-tile only)
+  int persistent = 1; // 0 per tile, 1 persistent y/z, 2 persistent x/y/z
 };
+
+// Rows per y/z chunk of the persistent schedule (one register batch).
+constexpr int kRingRows = 16;
 
 // The three tensor maps the sweeps use, built once per context.
 struct FieldMaps {
   CUtensorMap x;   // box {128 bytes of x, x_lines, 1, 1}, 128B swizzle
   CUtensorMap y;   // box {yz_tile, chunk rows, 1, 1}
   CUtensorMap z;   // box {yz_tile, 1, chunk rows, 1}
+  CUtensorMap ry;  // persistent schedule: box {32, kRingRows, 1, 1}
+  CUtensorMap rz;  // persistent schedule: box {32, 1, kRingRows, 1}
 };
 
 // Host-side count of this library's kernel launches (bfvm_kernel_launches).
@@ -162,9 +178,12 @@ cudaError_t launch_sweep_y(const FieldMaps& maps, const SweepParams<T>& p, const
 template <typename T>
 cudaError_t launch_sweep_z(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st);
 
-// Shared-memory bytes one CTA of each sweep needs.
+// Shared-memory bytes one CTA of each sweep needs (per-tile schedule), and
+// of the persistent schedule (0 where it does not apply).
 size_t sweep_x_smem(int elem_bytes, int nx, const SweepConfig& cfg);
 size_t sweep_yz_smem(int elem_bytes, int n_line, const SweepConfig& cfg);
+size_t ring_x_smem(int elem_bytes, int nx);
+size_t ring_yz_smem(int elem_bytes, int n_line);
 
 // ---- batched engine: one fused launch per LOD step over many solves ------
 // Tiles are 32 lines (one warp) in every sweep of a batch.

@@ -53,6 +53,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return done != 0;
 }
 
+// One arrival on the barrier (release semantics at CTA scope).
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
 // Wait for phase `parity` of the barrier; false if the wait limit ran out.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
@@ -98,6 +103,12 @@ __device__ __forceinline__ void tma_store_commit() { asm volatile("cp.async.bulk
 // Wait until every committed bulk store has finished READING shared memory.
 __device__ __forceinline__ void tma_store_wait_read() {
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// Wait until every committed bulk store but the most recent one has finished
+// READING shared memory.
+__device__ __forceinline__ void tma_store_wait_read_1() {
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
 }
 
 // Wait until every committed bulk store has completed its global writes.

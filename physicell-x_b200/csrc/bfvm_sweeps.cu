@@ -77,23 +77,25 @@ __device__ __forceinline__ double markstein(double t, double d, double r) {
   return __fma_rn(e, r, q0);
 }
 
-// FP64 forward batch.  The bare chain runs first.  With c1 >= 0 and every
-// denominator >= 1 (screen set: no negative diffusion or decay), a batch
-// whose incoming value is not negative and whose inputs are all >= 2^-960
-// has every numerator t = fma(c1, y, v) >= 2^-960, where the Markstein
-// quotient is exact.  That screen reads only the inputs (a signed minimum of
-// their high words, which orders non-negative doubles and puts negative ones
-// first), so it runs off the chain; a batch that fails it anywhere in the
-// warp is redone with each numerator checked, and with IEEE division if one
-// is -0 or a nonzero value below 2^-960.
-template <int B>
-__device__ __forceinline__ double forward_batch(const double (&v)[B], const double2 (&cf)[B], double c1, double,
-                                                int screen, double y, double (&out)[B]) {
+// FP64 forward batch.  The bare chain runs first and hands each result to
+// put(q, y) as soon as it is computed, so the stores overlap the chain.  With
+// c1 >= 0 and every denominator >= 1 (screen set: no negative diffusion or
+// decay), a batch whose incoming value is not negative and whose inputs are
+// all >= 2^-960 has every numerator t = fma(c1, y, v) >= 2^-960, where the
+// Markstein quotient is exact.  That screen reads only the inputs (a signed
+// minimum of their high words, which orders non-negative doubles and puts
+// negative ones first), so it runs off the chain; a batch that fails it
+// anywhere in the warp is redone from its inputs (still in registers) with
+// each numerator checked, and with IEEE division if one is -0 or a nonzero
+// value below 2^-960, and its results are stored again over the bare ones.
+template <int B, typename Put>
+__device__ __forceinline__ double forward_store(const double (&v)[B], const double2 (&cf)[B], double c1, double,
+                                                int screen, double y, Put&& put) {
   const double y0 = y;
 #pragma unroll
   for (int q = 0; q < B; ++q) {
     y = markstein(__fma_rn(c1, y, v[q]), cf[q].x, cf[q].y);
-    out[q] = y;
+    put(q, y);
   }
   int hw[B];
 #pragma unroll
@@ -113,14 +115,14 @@ __device__ __forceinline__ double forward_batch(const double (&v)[B], const doub
       const double t = __fma_rn(c1, y, v[q]);
       slow |= (fabs(t) < 0x1p-960) & (__double_as_longlong(t) != 0);
       y = markstein(t, cf[q].x, cf[q].y);
-      out[q] = y;
+      put(q, y);
     }
     if (slow) {
       y = y0;
 #pragma unroll
       for (int q = 0; q < B; ++q) {
         y = __fma_rn(c1, y, v[q]) / cf[q].x;
-        out[q] = y;
+        put(q, y);
       }
     }
   }
@@ -130,17 +132,96 @@ __device__ __forceinline__ double forward_batch(const double (&v)[B], const doub
 // FP32 form: stored values are FP32, the recurrence runs in FP64 (the
 // running value y stays FP64 across elements and batches), each result is
 // rounded to FP32 once, when stored.  The quotient is t * RN(1/d).
-template <int B>
-__device__ __forceinline__ double forward_batch(const float (&v)[B], const double (&cf)[B], double c1, double shift,
-                                                int, double y, float (&out)[B]) {
+template <int B, typename Put>
+__device__ __forceinline__ double forward_store(const float (&v)[B], const double (&cf)[B], double c1, double shift,
+                                                int, double y, Put&& put) {
 #pragma unroll
   for (int q = 0; q < B; ++q) {
     const double t = __fma_rn(c1, y, static_cast<double>(v[q]) - shift);
     y = __dmul_rn(t, cf[q]);
-    out[q] = static_cast<float>(y);
+    put(q, static_cast<float>(y));
   }
   return y;
 }
+
+// Bare FP64 forward chain over one batch (no screen); results go to put as
+// they are computed.  The caller screens the inputs (batch_min_hi) and redoes
+// the batch, or the whole line, with forward_checked if the screen fails.
+template <int B, typename Put>
+__device__ __forceinline__ double forward_bare(const double (&v)[B], const double2 (&cf)[B], double c1, double y,
+                                               Put&& put) {
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    y = markstein(__fma_rn(c1, y, v[q]), cf[q].x, cf[q].y);
+    put(q, y);
+  }
+  return y;
+}
+
+// The batch's inputs' minimum high word (signed): >= the high word of 2^-960
+// exactly when every input is >= 2^-960 (negative inputs sort first).
+template <int B>
+__device__ __forceinline__ int batch_min_hi(const double (&v)[B]) {
+  int hw[B];
+#pragma unroll
+  for (int q = 0; q < B; ++q) hw[q] = __double2hiint(v[q]);
+#pragma unroll
+  for (int w = B / 2; w >= 1; w /= 2) {
+#pragma unroll
+    for (int q = 0; q < w; ++q) hw[q] = min(hw[q], hw[q + w]);
+  }
+  return hw[0];
+}
+constexpr int kHiTiny = 0x03F00000;  // high word of 2^-960
+
+// The forward chain with every numerator checked: the Markstein quotient
+// where it is exact, IEEE division for a numerator of -0 or a nonzero value
+// below 2^-960 (the whole batch, as the reference divides).
+template <int B, typename Put>
+__device__ __forceinline__ double forward_checked(const double (&v)[B], const double2 (&cf)[B], double c1, double y,
+                                                  Put&& put) {
+  const double y0 = y;
+  bool slow = false;
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    const double t = __fma_rn(c1, y, v[q]);
+    slow |= (fabs(t) < 0x1p-960) & (__double_as_longlong(t) != 0);
+    y = markstein(t, cf[q].x, cf[q].y);
+    put(q, y);
+  }
+  if (slow) {
+    y = y0;
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      y = __fma_rn(c1, y, v[q]) / cf[q].x;
+      put(q, y);
+    }
+  }
+  return y;
+}
+
+// Writer of one thread's 128-byte row of a swizzled chunk, element by
+// element in order: values are gathered into 16-byte units and each unit is
+// stored when complete.
+template <typename T>
+struct RowPut {
+  static constexpr int U = 16 / sizeof(T);
+  using Unit = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+  unsigned char* crow;
+  int sw;
+  T buf[U];
+  template <typename V>
+  __device__ __forceinline__ void operator()(int q, V val) {
+    buf[q % U] = static_cast<T>(val);
+    if (q % U == U - 1) {
+      Unit uv;
+      T* ev = reinterpret_cast<T*>(&uv);
+#pragma unroll
+      for (int e = 0; e < U; ++e) ev[e] = buf[e];
+      *reinterpret_cast<Unit*>(crow + (((q / U) ^ sw) << 4)) = uv;
+    }
+  }
+};
 
 __device__ __forceinline__ double back_elem(double c, double xn, double y) { return __fma_rn(-c, xn, y); }
 
@@ -194,6 +275,25 @@ __device__ __forceinline__ void store_row(unsigned char* crow, int sw, const T (
 #pragma unroll
     for (int q = 0; q < U; ++q) ev[q] = v[u * U + q];
     *reinterpret_cast<Unit*>(crow + ((u ^ sw) << 4)) = uv;
+  }
+}
+
+// Copy m coefficients to shared memory with the CTA's threads, every
+// thread's loads in flight together (eight per thread per round).
+__device__ __forceinline__ void stage_row_cta(double* __restrict__ dst, const double* __restrict__ src, int m) {
+  const int t = threadIdx.x, nt = blockDim.x;
+  for (int q0 = 0; q0 < m; q0 += 8 * nt) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int q = q0 + u * nt + t;
+      v[u] = q < m ? __ldg(src + q) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int q = q0 + u * nt + t;
+      if (q < m) dst[q] = v[u];
+    }
   }
 }
 
@@ -273,7 +373,7 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   // The upper-diagonal row for the back substitution, staged after the tile
   // (read back after the barrier that ends the forward pass).
   CU* cus = reinterpret_cast<CU*>(tile + C * chunk_bytes);
-  for (int q = t; q < C * W; q += TL) cus[q] = __ldg(cup + q);
+  stage_row_cta(cus, cup, C * W);
 
   unsigned char* row = tile + t * 128;
   const int sw = t & 7;
@@ -341,9 +441,11 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   // harmlessly (those results are never stored to the field).
   double y = -0.0;  // running value of the forward recurrence (FP64 in both forms)
   const int screen = p.screen;
-  auto fwd = [&](int c, DR (&cf)[W]) {
+  // Tiles with no face or out-of-range line run the batches without per-lane checks.
+  const bool edge_tile = __syncthreads_or(face || !valid) != 0;
+  auto fwd = [&](bool edge, int c, DR (&cf)[W]) {
     if (!all_landed && ok) ok = mbar_wait(smem_u32(&bars[c]), static_cast<uint32_t>(phase >> c) & 1u);
-    if (face) return;
+    if (edge && (face || !valid)) return;  // lines past ny hold TMA fill, never stored
     unsigned char* crow = row + c * chunk_bytes;
     const int i0 = c * W;
     // The pin before the sweep, on the staged row (after the sources).
@@ -351,20 +453,31 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
       if (i0 == 0) *swz_elem<T>(crow, 0, sw) = x0v;
       if (nx - 1 < i0 + W) *swz_elem<T>(crow, nx - 1 - i0, sw) = x1v;
     }
-    T v[W], out[W];
+    T v[W];
     load_row<T, W>(crow, sw, v);
-    y = forward_batch<W>(v, cf, c1, shift, screen, y, out);
-    store_row<T, W>(crow, sw, out);
+    if (i0 + W > nx) {  // TMA fill past the line's end: any clean value (results never stored)
+#pragma unroll
+      for (int q = 0; q < W; ++q)
+        if (i0 + q >= nx) v[q] = T(1);
+    }
+    RowPut<T> put{crow, sw};
+    y = forward_store<W>(v, cf, c1, shift, screen, y, put);
   };
-  for (int c = 0; c < C; c += 2) {
-    fwd(c, cfa);
+  auto forward_pass = [&](bool edge) {
+    for (int c = 0; c < C; c += 2) {
+      fwd(edge, c, cfa);
 #pragma unroll
-    for (int q = 0; q < W; ++q) cfa[q] = __ldg(drp + (c + 2) * W + q);
-    if (c + 1 >= C) break;
-    fwd(c + 1, cfb);
+      for (int q = 0; q < W; ++q) cfa[q] = __ldg(drp + (c + 2) * W + q);
+      if (c + 1 >= C) break;
+      fwd(edge, c + 1, cfb);
 #pragma unroll
-    for (int q = 0; q < W; ++q) cfb[q] = __ldg(drp + (c + 3) * W + q);
-  }
+      for (int q = 0; q < W; ++q) cfb[q] = __ldg(drp + (c + 3) * W + q);
+    }
+  };
+  if (edge_tile)
+    forward_pass(true);
+  else
+    forward_pass(false);
   phase ^= chunk_mask(C);
   if (__syncthreads_or(!ok)) {
     if (t == 0) atomicExch(p.status, kDevTimeout);
@@ -373,7 +486,8 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
 
   // Back substitution, last chunk first; each finished chunk is stored at once.
   double xn = -0.0;  // running value of the back substitution
-  for (int c = C - 1; c >= 0; --c) {
+  auto back_chunk = [&](bool edge, int c) {
+    const bool E = edge;
     unsigned char* crow = row + c * chunk_bytes;
     const int i0 = c * W;
     CU cw[W];
@@ -384,14 +498,14 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
       cw[2 * q] = pr.x;
       cw[2 * q + 1] = pr.y;
     }
-    if (face) {
+    if (E && face) {
       T fw[W];
 #pragma unroll
       for (int q = 0; q < W; ++q) fw[q] = (fv != nullptr && i0 + q < nx) ? static_cast<T>(fv[i0 + q] - off) : T(0);
 #pragma unroll
       for (int q = 0; q < W; ++q)
         if (i0 + q < nx) *swz_elem<T>(crow, q, sw) = fw[q];
-    } else {
+    } else if (!E || valid) {
       T v[W];
       load_row<T, W>(crow, sw, v);
       if (i0 + W > nx) {
@@ -416,6 +530,12 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
         if (nx - 1 < i0 + W) *swz_elem<T>(crow, nx - 1 - i0, sw) = x1v;
       }
     }
+  };
+  for (int c = C - 1; c >= 0; --c) {
+    if (edge_tile)
+      back_chunk(true, c);
+    else
+      back_chunk(false, c);
     fence_async_smem();
     __syncthreads();
     if (t == 0) {
@@ -504,7 +624,7 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
   // (read back after the barrier that ends the forward pass).
   const int rows = (C * CH + R - 1) / R * R;
   CU* cus = reinterpret_cast<CU*>(tile + static_cast<size_t>(rows) * TI);
-  for (int q = t; q < rows; q += TI) cus[q] = __ldg(cup + q);
+  stage_row_cta(cus, cup, rows);
   T* col = tile + t;
   bool ok = true;
   int waited = 0;     // chunks whose TMA load this thread has waited for
@@ -513,19 +633,22 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
   // sweep restores their input values.
   T e0v = T(0), e1v = T(0);
   double y = -0.0;  // running value of the forward recurrence (FP64 in both forms)
+  int hwmin = INT_MAX;  // FP64: minimum input high word of this lane's line (the screen)
 
   // One forward batch of R rows from rb, after waiting for the chunks that
   // cover it.  The tile holds a whole number of batches, so the last batch
   // may read rows past n (TMA fill or unused rows): those results are never
   // stored to the field.
-  auto fwd = [&](int rb, DR (&cf)[R]) {
+  // Tiles with no face or out-of-range line run the batches without per-lane checks.
+  const bool edge_tile = __syncthreads_or(face || i >= nx) != 0;
+  auto fwd = [&](bool edge, int rb, DR (&cf)[R]) {
     while (waited < C && wait_row < rb + R) {
       if (ok) ok = mbar_wait(smem_u32(&bars[waited]), static_cast<uint32_t>(phase >> waited) & 1u);
       ++waited;
       wait_row += CH;
     }
-    if (face) return;
-    T v[R], out[R];
+    if (edge && (face || i >= nx)) return;  // lines past nx hold TMA fill, never stored
+    T v[R];
     T* cb = col + rb * TI;
 #pragma unroll
     for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
@@ -537,19 +660,34 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
           if (rb + q == n - 1) e1v = v[q];
       }
     }
-    y = forward_batch<R>(v, cf, c1, shift, screen, y, out);
+    if (rb + R > n) {  // rows past the line's end (TMA fill or unused): any clean value, never stored
 #pragma unroll
-    for (int q = 0; q < R; ++q) cb[q * TI] = out[q];
+      for (int q = 0; q < R; ++q)
+        if (rb + q >= n) v[q] = T(1);
+    }
+    auto put = [&](int q, auto val) { cb[q * TI] = static_cast<T>(val); };
+    if constexpr (kF32<T>) {
+      y = forward_store<R>(v, cf, c1, shift, screen, y, put);
+    } else {
+      y = forward_bare<R>(v, cf, c1, y, put);
+      hwmin = min(hwmin, batch_min_hi<R>(v));
+    }
   };
-  for (int rb = 0; rb < n; rb += 2 * R) {
-    fwd(rb, cfa);
+  auto forward_pass = [&](bool edge) {
+    for (int rb = 0; rb < n; rb += 2 * R) {
+      fwd(edge, rb, cfa);
 #pragma unroll
-    for (int q = 0; q < R; ++q) cfa[q] = __ldg(drp + rb + 2 * R + q);
-    if (rb + R >= n) break;
-    fwd(rb + R, cfb);
+      for (int q = 0; q < R; ++q) cfa[q] = __ldg(drp + rb + 2 * R + q);
+      if (rb + R >= n) break;
+      fwd(edge, rb + R, cfb);
 #pragma unroll
-    for (int q = 0; q < R; ++q) cfb[q] = __ldg(drp + rb + 3 * R + q);
-  }
+      for (int q = 0; q < R; ++q) cfb[q] = __ldg(drp + rb + 3 * R + q);
+    }
+  };
+  if (edge_tile)
+    forward_pass(true);
+  else
+    forward_pass(false);
   while (waited < C) {
     if (ok) ok = mbar_wait(smem_u32(&bars[waited]), static_cast<uint32_t>(phase >> waited) & 1u);
     ++waited;
@@ -559,6 +697,31 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
     if (t == 0) atomicExch(p.status, kDevTimeout);
     return false;
   }
+  if constexpr (!kF32<T>) {
+    // The screen, once per tile: a line with an input below 2^-960 (or
+    // negative) anywhere is redone from its inputs, which are still in the
+    // field (this tile's results are stored only by the back substitution).
+    if (__syncthreads_or(!(screen != 0 && hwmin >= kHiTiny))) {
+      if (!face && i < nx) {
+        const size_t row_stride = (AXIS == 1) ? static_cast<size_t>(p.nxp) : static_cast<size_t>(p.nxp) * p.ny;
+        const T* src = (AXIS == 1) ? p.f + ((static_cast<size_t>(s) * p.nz + m) * p.ny) * p.nxp + i
+                                   : p.f + (static_cast<size_t>(s) * p.nz * p.ny + m) * p.nxp + i;
+        y = -0.0;
+        for (int rb = 0; rb < n; rb += R) {
+          T v[R];
+          DR cf[R];
+#pragma unroll
+          for (int q = 0; q < R; ++q) {
+            v[q] = rb + q < n ? src[(rb + q) * row_stride] : T(1);
+            cf[q] = __ldg(drp + rb + q);
+          }
+          T* cb = col + rb * TI;
+          y = forward_checked<R>(v, cf, c1, y, [&](int q, auto val) { cb[q * TI] = static_cast<T>(val); });
+        }
+      }
+      __syncthreads();
+    }
+  }
 
   // Back substitution in batches of R rows from the end; chunk c is stored
   // once every row from its start on is final.
@@ -566,8 +729,8 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
   int next_store = C - 1;
   int store_row = next_store * CH;  // first row of chunk next_store
   const int last_b = ((n - 1) / R) * R;
-  for (int rb = last_b; rb >= 0; rb -= R) {
-    if (!face) {
+  auto back_batch = [&](bool edge, int rb) {
+    if (!edge || (!face && i < nx)) {
       T* cb = col + rb * TI;
       // the upper diagonal in 16-byte pairs (rb is a multiple of 16 rows)
       const double2* cwp = reinterpret_cast<const double2*>(cus + rb);
@@ -603,6 +766,12 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
         if (rb == last_b) col[(n - 1) * TI] = e1v;
       }
     }
+  };
+  for (int rb = last_b; rb >= 0; rb -= R) {
+    if (edge_tile)
+      back_batch(true, rb);
+    else
+      back_batch(false, rb);
     // store every chunk whose rows are now all final (uniform across the CTA)
     if (next_store >= 0 && store_row >= rb) {
       fence_async_smem();
@@ -642,6 +811,574 @@ __global__ void __launch_bounds__(TI) sweep_yz_kernel(const __grid_constant__ CU
   uint64_t phase = 0;
   yz_tile<T, AXIS, TI>(&map, p, blockIdx.x * TI, blockIdx.y, blockIdx.z, CH, base, phase);
   if (threadIdx.x == 0) tma_store_wait_read();
+}
+
+// ---------------------------------------------------------------------------
+// persistent schedule: a compute warp and a copy warp per CTA
+// ---------------------------------------------------------------------------
+// CTA b takes tiles b, b + G, b + 2G, ... (G CTAs in the grid, as many as fit
+// on the GPU at once).  Warp 0 computes; one lane of warp 1 issues every TMA
+// copy, so the compute warp never blocks on a copy it does not need yet.  A
+// tile's C chunks live in C shared-memory slots, each with two barriers:
+// `full` (the chunk's load landed) and `empty` (the compute warp finished the
+// chunk).  The back substitution finishes the chunks from the line's end; the
+// copy lane stores each finished chunk and, once the store has read its slot,
+// loads the next tile's chunk into it.  The first slot freed must take the
+// next tile's chunk 0, so the slot order flips from tile to tile: the k-th
+// tile of a CTA keeps chunk c in slot c for even k and in slot C-1-c for odd
+// k, and chunk c of tile k is followed in its slot by chunk C-1-c of tile k+1.
+// The next tile's loads therefore run under this tile's back substitution and
+// its stores under the next tile's forward elimination.  Each barrier
+// completes once per tile, so tile k waits on parity k&1.
+__device__ __forceinline__ int ring_slot(bool flip, int C, int c) { return flip ? C - 1 - c : c; }
+
+// CTA b of G takes tiles b, b + G, b + 2G, ...: the tiles in flight at any
+// moment are neighbours in memory (contiguous ranges per CTA measured 1.5x
+// slower in the x sweep).
+
+// Copy m coefficients to shared memory with every lane's loads in flight
+// together (eight per lane per round).
+__device__ __forceinline__ void stage_row(double* __restrict__ dst, const double* __restrict__ src, int m) {
+  const int t = threadIdx.x & 31;
+  for (int q0 = 0; q0 < m; q0 += 8 * 32) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int q = q0 + u * 32 + t;
+      v[u] = q < m ? __ldg(src + q) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int q = q0 + u * 32 + t;
+      if (q < m) dst[q] = v[u];
+    }
+  }
+}
+
+// The copy lane's loop, shared by the three sweeps.  load(tile, c, slot)
+// issues chunk c of a tile into a slot (arming its full barrier);
+// store(tile, c, slot) writes a finished chunk back.  Returns false if a
+// wait gave up.
+template <typename NextF, typename LoadF, typename StoreF>
+__device__ __forceinline__ bool ring_copy_loop(long long tile, long long ntiles, int C, const uint64_t* empty_bars,
+                                               NextF next_of, LoadF load, StoreF store) {
+  if (tile >= ntiles) return true;
+  for (int c = 0; c < C; ++c) load(tile, c, c);
+  for (uint32_t k = 0;; ++k) {
+    const long long nxt = next_of(tile);
+    const bool flip = (k & 1u) != 0;
+    for (int q = 0; q < C; ++q) {
+      const int c = C - 1 - q;  // chunks in the order the back substitution finishes them
+      const int sl = ring_slot(flip, C, c);
+      if (!mbar_wait(smem_u32(&empty_bars[sl]), k & 1u)) return false;
+      store(tile, c, sl);
+      tma_store_commit();
+      if (nxt < ntiles) {
+        tma_store_wait_read();  // the store has read the slot
+        load(nxt, q, sl);       // chunk q of the next tile: slot_{k+1}(q) == slot_k(C-1-q)
+      }
+    }
+    if (nxt >= ntiles) break;
+    tile = nxt;
+  }
+  tma_store_wait_read();
+  return true;
+}
+
+template <typename T, int AXIS>
+__global__ void __launch_bounds__(64) sweep_yz_ring_kernel(const __grid_constant__ CUtensorMap map,
+                                                           const SweepParams<T> p) {
+  using DR = typename Coef<T>::DR;
+  using CU = typename Coef<T>::CU;
+  constexpr int R = kRowBatch;
+  constexpr int CH = kRingRows;
+  static_assert(CH == R, "a y/z ring chunk is one register batch");
+  constexpr int TI = 32;
+  constexpr int kSlotElems = CH * TI;
+  constexpr uint32_t kSlotBytes = kSlotElems * sizeof(T);
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 128);
+  const int nx = p.nx;
+  const int n = (AXIS == 1) ? p.ny : p.nz;
+  const int nm = (AXIS == 1) ? p.nz : p.ny;  // the line's other coordinate (k for y, j for z)
+  const int C = (n + CH - 1) / CH;
+  const int ntx = (nx + TI - 1) / TI;
+  const long long per_s = static_cast<long long>(ntx) * nm;
+  const long long ntiles = per_s * p.S;
+  uint64_t* full = reinterpret_cast<uint64_t*>(base);
+  uint64_t* empty = full + kMaxChunks;
+  T* slots = reinterpret_cast<T*>(base + kBarrierBytes);
+  CU* cus = reinterpret_cast<CU*>(slots + static_cast<size_t>(C) * kSlotElems);
+  const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
+
+  // tile -> (i0, m, s), x tiles fastest
+  auto decode = [&](long long tile, int& i0, int& m, int& s) {
+    s = static_cast<int>(tile / per_s);
+    const long long r = tile - s * per_s;
+    m = static_cast<int>(r / ntx);
+    i0 = static_cast<int>(r - static_cast<long long>(m) * ntx) * TI;
+  };
+  // A tile whose lines all lie in an activated face is already final (its
+  // input holds the face values, which the pin after the sweep writes again).
+  auto skip = [&](long long tile) {
+    int i0, m, s;
+    decode(tile, i0, m, s);
+    return p.active[s] != 0 && (m == 0 || m == nm - 1);
+  };
+  // the next tile to work on after `tile` (ntiles when there is none)
+  auto next_of = [&](long long tile) {
+    do {
+      tile += gridDim.x;
+    } while (tile < ntiles && skip(tile));
+    return tile < ntiles ? tile : ntiles;
+  };
+  const long long first = blockIdx.x;
+
+  if (threadIdx.x == 0) {
+    prefetch_tmap(&map);
+    for (int c = 0; c < C; ++c) {
+      mbar_init(smem_u32(&full[c]), 1);
+      mbar_init(smem_u32(&empty[c]), 1);
+    }
+    fence_barrier_init();
+  }
+  __syncthreads();
+  long long tile = (first < ntiles && !skip(first)) ? first : next_of(first);
+
+  if (warp == 1) {
+    if (t != 0) return;
+    auto load = [&](long long tl, int c, int sl) {
+      int i0, m, s;
+      decode(tl, i0, m, s);
+      const uint32_t bar = smem_u32(&full[sl]);
+      mbar_expect_tx(bar, kSlotBytes);
+      const uint32_t dst = smem_u32(slots + static_cast<size_t>(sl) * kSlotElems);
+      if (AXIS == 1)
+        tma_load_4d(dst, &map, bar, i0, c * CH, m, s);
+      else
+        tma_load_4d(dst, &map, bar, i0, m, c * CH, s);
+    };
+    auto store = [&](long long tl, int c, int sl) {
+      int i0, m, s;
+      decode(tl, i0, m, s);
+      const uint32_t src = smem_u32(slots + static_cast<size_t>(sl) * kSlotElems);
+      if (AXIS == 1)
+        tma_store_4d(&map, src, i0, c * CH, m, s);
+      else
+        tma_store_4d(&map, src, i0, m, c * CH, s);
+    };
+    if (!ring_copy_loop(tile, ntiles, C, empty, next_of, load, store)) atomicExch(p.status, kDevTimeout);
+    return;
+  }
+
+  const int screen = p.screen;
+  int staged_s = -1;
+  for (uint32_t k = 0; tile < ntiles; ++k) {
+    int i0, m, s;
+    decode(tile, i0, m, s);
+    const bool flip = (k & 1u) != 0;
+    const uint32_t par = k & 1u;
+    const bool act = p.active[s] != 0;
+    const int i = i0 + t;
+    const bool face = act && (i == 0 || i == nx - 1);  // lines in an x face keep their (pinned) input
+    const AxisCoefs<T>& ac = (AXIS == 1) ? p.ay : p.az;
+    const DR* __restrict__ drp = ac.dr + static_cast<size_t>(s) * ac.npad;
+    const CU* __restrict__ cup = ac.cu + static_cast<size_t>(s) * ac.npad;
+    const typename Coef<T>::C1 c1 = p.c1[s];
+    const double shift = kF32<T> ? p.shift[s] : 0.0;
+    // the upper diagonal for the back substitution, restaged when the
+    // substrate changes (every lane finished reading the previous copy
+    // before the last __syncwarp)
+    if (s != staged_s) {
+      stage_row(cus, cup, C * CH);
+      staged_s = s;
+    }
+    DR cfa[R], cfb[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      cfa[q] = __ldg(drp + q);
+      cfb[q] = __ldg(drp + R + q);
+    }
+    auto col_of = [&](int c) { return slots + static_cast<size_t>(ring_slot(flip, C, c)) * kSlotElems + t; };
+    bool ok = true;
+    T e0v = T(0), e1v = T(0);
+    double y = -0.0;
+    int hwmin = INT_MAX;  // FP64: minimum input high word of this lane's line (the screen)
+    // Forward elimination over chunk c (one register batch); rows past n in
+    // the last chunk are TMA fill, and their results are never stored.
+    // Tiles with no face or out-of-range line run the batches without per-lane checks.
+    const bool edge_tile = __any_sync(0xffffffffu, face || i >= nx);
+    auto fwd = [&](bool edge, int c, DR (&cf)[R]) {
+      if (ok) ok = mbar_wait(smem_u32(&full[ring_slot(flip, C, c)]), par);
+      if (edge && (face || i >= nx)) return;  // lines past nx hold TMA fill, never stored
+      T* cb = col_of(c);
+      const int rb = c * CH;
+      T v[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
+      if (act) {
+        if (rb == 0) e0v = v[0];
+        if (rb + R > n - 1) {
+#pragma unroll
+          for (int q = 0; q < R; ++q)
+            if (rb + q == n - 1) e1v = v[q];
+        }
+      }
+      if (rb + R > n) {  // rows past the line's end (TMA fill): any clean value, never stored
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+          if (rb + q >= n) v[q] = T(1);
+      }
+      auto put = [&](int q, auto val) { cb[q * TI] = static_cast<T>(val); };
+      if constexpr (kF32<T>) {
+        y = forward_store<R>(v, cf, c1, shift, screen, y, put);
+      } else {
+        y = forward_bare<R>(v, cf, c1, y, put);
+        hwmin = min(hwmin, batch_min_hi<R>(v));
+      }
+    };
+    auto forward_pass = [&](bool edge) {
+      for (int c = 0; c < C; c += 2) {
+        fwd(edge, c, cfa);
+#pragma unroll
+        for (int q = 0; q < R; ++q) cfa[q] = __ldg(drp + (c + 2) * R + q);
+        if (c + 1 >= C) break;
+        fwd(edge, c + 1, cfb);
+#pragma unroll
+        for (int q = 0; q < R; ++q) cfb[q] = __ldg(drp + (c + 3) * R + q);
+      }
+    };
+    if (edge_tile)
+      forward_pass(true);
+    else
+      forward_pass(false);
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (t == 0) atomicExch(p.status, kDevTimeout);
+      break;
+    }
+    if constexpr (!kF32<T>) {
+      // The screen, once per tile: a line with an input below 2^-960 (or
+      // negative) anywhere is redone from its inputs, which are still in the
+      // field (this tile's results are stored only by the back substitution).
+      if (__any_sync(0xffffffffu, !(screen != 0 && hwmin >= kHiTiny))) {
+        if (!face && i < nx) {
+          const size_t row_stride = (AXIS == 1) ? static_cast<size_t>(p.nxp)
+                                                : static_cast<size_t>(p.nxp) * p.ny;
+          const T* src = (AXIS == 1) ? p.f + ((static_cast<size_t>(s) * p.nz + m) * p.ny) * p.nxp + i
+                                     : p.f + (static_cast<size_t>(s) * p.nz * p.ny + m) * p.nxp + i;
+          y = -0.0;
+          for (int c = 0; c < C; ++c) {
+            const int rb = c * CH;
+            T v[R];
+            DR cf[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+              v[q] = rb + q < n ? src[(rb + q) * row_stride] : T(1);
+              cf[q] = __ldg(drp + rb + q);
+            }
+            T* cb = col_of(c);
+            y = forward_checked<R>(v, cf, c1, y, [&](int q, auto val) { cb[q * TI] = static_cast<T>(val); });
+          }
+        }
+        __syncwarp();
+      }
+    }
+
+    // Back substitution, last chunk first; each finished chunk is handed to
+    // the copy lane through its empty barrier.
+    double xn = -0.0;
+    auto back_chunk = [&](bool edge, int c) {
+      const int rb = c * CH;
+      if (!edge || (!face && i < nx)) {
+        T* cb = col_of(c);
+        const double2* cwp = reinterpret_cast<const double2*>(cus + rb);  // 16-byte pairs
+        T v[R];
+        CU cw[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
+#pragma unroll
+        for (int q = 0; q < R / 2; ++q) {
+          const double2 pr = cwp[q];
+          cw[2 * q] = pr.x;
+          cw[2 * q + 1] = pr.y;
+        }
+        if (c == C - 1) {
+#pragma unroll
+          for (int q = R - 1; q >= 0; --q) {
+            if (rb + q < n) {
+              xn = back_elem(cw[q], xn, v[q]);
+              v[q] = static_cast<T>(xn);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int q = R - 1; q >= 0; --q) {
+            xn = back_elem(cw[q], xn, v[q]);
+            v[q] = static_cast<T>(xn);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) cb[q * TI] = v[q];
+        if (act) {
+          if (c == 0) cb[0] = e0v;
+          if (c == C - 1) cb[(n - 1 - rb) * TI] = e1v;
+        }
+      }
+    };
+    for (int c = C - 1; c >= 0; --c) {
+      if (edge_tile)
+        back_chunk(true, c);
+      else
+        back_chunk(false, c);
+      fence_async_smem();
+      __syncwarp();
+      if (t == 0) mbar_arrive(smem_u32(&empty[ring_slot(flip, C, c)]));
+    }
+    __syncwarp();
+    tile = next_of(tile);
+  }
+}
+
+// x sweep, persistent.  Chunk c of a tile is the 128-byte column [cW, cW+W)
+// of its 32 lines (W = 128 / sizeof(T)), staged with the 128B swizzle.  Each
+// lane applies the agents of its own line chunk by chunk just before the
+// forward elimination reads the chunk: its line's agents are one contiguous,
+// x-ordered range of the sorted list, and every voxel's run is applied in
+// sorted (agent-list) order, so the result equals applying all agents first.
+template <typename T>
+__global__ void __launch_bounds__(64) sweep_x_ring_kernel(const __grid_constant__ CUtensorMap map,
+                                                          const SweepParams<T> p) {
+  using DR = typename Coef<T>::DR;
+  using CU = typename Coef<T>::CU;
+  constexpr int W = 128 / sizeof(T);
+  constexpr int TL = 32;
+  constexpr uint32_t kSlotBytes = TL * 128u;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
+  const int nx = p.nx, ny = p.ny, nz = p.nz, S = p.S;
+  const int C = (nx + W - 1) / W;
+  const int nty = (ny + TL - 1) / TL;
+  const long long per_s = static_cast<long long>(nty) * nz;
+  const long long ntiles = per_s * S;
+  uint64_t* full = reinterpret_cast<uint64_t*>(base);
+  uint64_t* empty = full + kMaxChunks;
+  unsigned char* slots = base + kBarrierBytes;
+  CU* cus = reinterpret_cast<CU*>(slots + static_cast<size_t>(C) * kSlotBytes);
+  const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
+  const int sw = t & 7;
+
+  auto decode = [&](long long tile, int& j0, int& k, int& s) {
+    s = static_cast<int>(tile / per_s);
+    const long long r = tile - s * per_s;
+    k = static_cast<int>(r / nty);
+    j0 = static_cast<int>(r - static_cast<long long>(k) * nty) * TL;
+  };
+  auto next_of = [&](long long tile) { return tile + gridDim.x < ntiles ? tile + gridDim.x : ntiles; };
+  const long long first = blockIdx.x;
+
+  if (threadIdx.x == 0) {
+    prefetch_tmap(&map);
+    for (int c = 0; c < C; ++c) {
+      mbar_init(smem_u32(&full[c]), 1);
+      mbar_init(smem_u32(&empty[c]), 1);
+    }
+    fence_barrier_init();
+  }
+  __syncthreads();
+  long long tile = first < ntiles ? first : ntiles;
+
+  if (warp == 1) {
+    if (t != 0) return;
+    auto load = [&](long long tl, int c, int sl) {
+      int j0, k, s;
+      decode(tl, j0, k, s);
+      const uint32_t bar = smem_u32(&full[sl]);
+      mbar_expect_tx(bar, kSlotBytes);
+      tma_load_4d(smem_u32(slots + static_cast<size_t>(sl) * kSlotBytes), &map, bar, c * W, j0, k, s);
+    };
+    auto store = [&](long long tl, int c, int sl) {
+      int j0, k, s;
+      decode(tl, j0, k, s);
+      tma_store_4d(&map, smem_u32(slots + static_cast<size_t>(sl) * kSlotBytes), c * W, j0, k, s);
+    };
+    if (!ring_copy_loop(tile, ntiles, C, empty, next_of, load, store)) atomicExch(p.status, kDevTimeout);
+    return;
+  }
+
+  const int screen = p.screen;
+  int staged_s = -1;
+  for (uint32_t kk = 0; tile < ntiles; ++kk) {
+    int j0, k, s;
+    decode(tile, j0, k, s);
+    const bool flip = (kk & 1u) != 0;
+    const uint32_t par = kk & 1u;
+    const int j = j0 + t;
+    const bool valid = j < ny;
+    const bool act = p.active[s] != 0;
+    const bool face = act && (j == 0 || j == ny - 1 || k == 0 || k == nz - 1);
+    // Face-line values: the z-face plane when k is on a z face, else the y-face plane.
+    const double* fv = nullptr;
+    if (face && valid) {
+      if (k == 0 || k == nz - 1)
+        fv = p.zface + ((static_cast<size_t>(k == 0 ? 0 : 1) * S + s) * ny + j) * nx;
+      else
+        fv = p.yface + ((static_cast<size_t>(j == 0 ? 0 : 1) * S + s) * nz + k) * nx;
+    }
+    const double off = kF32<T> ? p.off[s] : 0.0;
+    T x0v = T(0), x1v = T(0);
+    if (act && valid) {
+      x0v = static_cast<T>(p.xface[(static_cast<size_t>(0 * S + s) * nz + k) * ny + j] - off);
+      x1v = static_cast<T>(p.xface[(static_cast<size_t>(1 * S + s) * nz + k) * ny + j] - off);
+    }
+    const DR* __restrict__ drp = p.ax.dr + static_cast<size_t>(s) * p.ax.npad;
+    const CU* __restrict__ cup = p.ax.cu + static_cast<size_t>(s) * p.ax.npad;
+    const typename Coef<T>::C1 c1 = p.c1[s];
+    const double shift = kF32<T> ? p.shift[s] : 0.0;
+    if (s != staged_s) {  // the upper diagonal, restaged when the substrate changes
+      stage_row(cus, cup, C * W);
+      staged_s = s;
+    }
+    DR cfa[W], cfb[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+      cfa[q] = __ldg(drp + q);
+      cfb[q] = __ldg(drp + W + q);
+    }
+    auto row_of = [&](int c) {
+      return slots + static_cast<size_t>(ring_slot(flip, C, c)) * kSlotBytes + t * 128;
+    };
+    // This lane's agents: sorted positions [a, a_end) of line k*ny + j.
+    int a = 0, a_end = 0;
+    unsigned line_key0 = 0;
+    if (p.line_off != nullptr && valid) {
+      const int line = k * ny + j;
+      a = __ldg(p.line_off + line);
+      a_end = __ldg(p.line_off + line + 1);
+      line_key0 = static_cast<unsigned>(line) * static_cast<unsigned>(nx);
+    }
+    const double* ac1 = p.ac1 + static_cast<size_t>(s) * p.n_sorted;
+    const double* ac2 = p.ac2 + static_cast<size_t>(s) * p.n_sorted;
+    const double* ae2 = p.ae2 + static_cast<size_t>(s) * p.n_sorted;
+    unsigned akey = a < a_end ? __ldg(p.a_key + a) : 0u;
+
+    bool ok = true;
+    double y = -0.0;
+    // Tiles with no face or out-of-range line run the batches without per-lane checks.
+    const bool edge_tile = __any_sync(0xffffffffu, face || !valid);
+    auto fwd = [&](bool edge, int c, DR (&cf)[W]) {
+      if (ok) ok = mbar_wait(smem_u32(&full[ring_slot(flip, C, c)]), par);
+      unsigned char* crow = row_of(c);
+      const int i0 = c * W;
+      // agents of this lane's line inside chunk c, each voxel's run in order
+      const unsigned lim = line_key0 + static_cast<unsigned>(i0 + W);
+      while (a < a_end && akey < lim) {
+        T* e = swz_elem<T>(crow, static_cast<int>(akey - line_key0) - i0, sw);
+        double r = static_cast<double>(*e);
+        if constexpr (kF32<T>) r += off;
+        const unsigned key = akey;
+        do {
+          r = agent_update(r, __ldg(ac1 + a), __ldg(ac2 + a), __ldg(ae2 + a), a, s, p.track);
+          ++a;
+          akey = a < a_end ? __ldg(p.a_key + a) : 0u;
+        } while (a < a_end && akey == key);
+        if constexpr (kF32<T>) r -= off;
+        *e = static_cast<T>(r);
+      }
+      if (edge && (face || !valid)) return;  // lines past ny hold TMA fill, never stored
+      // the pin before the sweep, on the staged row (after the sources)
+      if (act) {
+        if (i0 == 0) *swz_elem<T>(crow, 0, sw) = x0v;
+        if (nx - 1 < i0 + W) *swz_elem<T>(crow, nx - 1 - i0, sw) = x1v;
+      }
+      T v[W];
+      load_row<T, W>(crow, sw, v);
+      if (i0 + W > nx) {  // TMA fill past the line's end: any clean value (results never stored)
+#pragma unroll
+        for (int q = 0; q < W; ++q)
+          if (i0 + q >= nx) v[q] = T(1);
+      }
+      RowPut<T> put{crow, sw};
+      y = forward_store<W>(v, cf, c1, shift, screen, y, put);
+    };
+    auto forward_pass = [&](bool edge) {
+      for (int c = 0; c < C; c += 2) {
+        fwd(edge, c, cfa);
+#pragma unroll
+        for (int q = 0; q < W; ++q) cfa[q] = __ldg(drp + (c + 2) * W + q);
+        if (c + 1 >= C) break;
+        fwd(edge, c + 1, cfb);
+#pragma unroll
+        for (int q = 0; q < W; ++q) cfb[q] = __ldg(drp + (c + 3) * W + q);
+      }
+    };
+    if (edge_tile)
+      forward_pass(true);
+    else
+      forward_pass(false);
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (t == 0) atomicExch(p.status, kDevTimeout);
+      break;
+    }
+
+    // Back substitution, last chunk first; each finished chunk is handed to
+    // the copy lane through its empty barrier.
+    double xn = -0.0;
+    auto back_chunk = [&](bool edge, int c) {
+      const bool E = edge;
+      unsigned char* crow = row_of(c);
+      const int i0 = c * W;
+      CU cw[W];
+      const double2* cwp = reinterpret_cast<const double2*>(cus + i0);  // 16-byte pairs
+#pragma unroll
+      for (int q = 0; q < W / 2; ++q) {
+        const double2 pr = cwp[q];
+        cw[2 * q] = pr.x;
+        cw[2 * q + 1] = pr.y;
+      }
+      if (E && face) {
+        T fw[W];
+#pragma unroll
+        for (int q = 0; q < W; ++q) fw[q] = (fv != nullptr && i0 + q < nx) ? static_cast<T>(fv[i0 + q] - off) : T(0);
+#pragma unroll
+        for (int q = 0; q < W; ++q)
+          if (i0 + q < nx) *swz_elem<T>(crow, q, sw) = fw[q];
+      } else if (!E || valid) {
+        T v[W];
+        load_row<T, W>(crow, sw, v);
+        if (i0 + W > nx) {
+#pragma unroll
+          for (int q = W - 1; q >= 0; --q) {
+            if (i0 + q < nx) {
+              xn = back_elem(cw[q], xn, v[q]);
+              v[q] = static_cast<T>(xn);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int q = W - 1; q >= 0; --q) {
+            xn = back_elem(cw[q], xn, v[q]);
+            v[q] = static_cast<T>(xn);
+          }
+        }
+        store_row<T, W>(crow, sw, v);
+        if (act) {
+          if (i0 == 0) *swz_elem<T>(crow, 0, sw) = x0v;
+          if (nx - 1 < i0 + W) *swz_elem<T>(crow, nx - 1 - i0, sw) = x1v;
+        }
+      }
+    };
+    for (int c = C - 1; c >= 0; --c) {
+      if (edge_tile)
+        back_chunk(true, c);
+      else
+        back_chunk(false, c);
+      fence_async_smem();
+      __syncwarp();
+      if (t == 0) mbar_arrive(smem_u32(&empty[ring_slot(flip, C, c)]));
+    }
+    __syncwarp();
+    tile = next_of(tile);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -828,6 +1565,21 @@ size_t sweep_yz_smem(int elem_bytes, int n_line, const SweepConfig& cfg) {
   return 128 + kBarrierBytes + rows * cfg.yz_tile * elem_bytes + rows * 8;
 }
 
+size_t ring_x_smem(int elem_bytes, int nx) {
+  const int W = 128 / elem_bytes;
+  const int C = (nx + W - 1) / W;
+  if (C > kMaxChunks) return 0;
+  // alignment pad, barriers, C slots of 32 rows of 128 bytes, the staged upper-diagonal row
+  return 1024 + kBarrierBytes + static_cast<size_t>(C) * 32 * 128 + static_cast<size_t>(C) * W * 8;
+}
+
+size_t ring_yz_smem(int elem_bytes, int n_line) {
+  const int C = (n_line + kRingRows - 1) / kRingRows;
+  if (C > kMaxChunks) return 0;
+  const size_t rows = static_cast<size_t>(C) * kRingRows;
+  return 128 + kBarrierBytes + rows * 32 * elem_bytes + rows * 8;
+}
+
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (fn == nullptr) {
@@ -858,14 +1610,80 @@ int encode_field_maps(FieldMaps* maps, void* f, int eb, int nx, int ny, int nz, 
   const cuuint32_t bx[4] = {(cuuint32_t)(128 / eb), (cuuint32_t)cfg.x_lines, 1, 1};
   const cuuint32_t by[4] = {(cuuint32_t)cfg.yz_tile, (cuuint32_t)yz_chunk_rows(ny, cfg.yz_chunk), 1, 1};
   const cuuint32_t bz[4] = {(cuuint32_t)cfg.yz_tile, 1, (cuuint32_t)yz_chunk_rows(nz, cfg.yz_chunk), 1};
+  const cuuint32_t bry[4] = {32, (cuuint32_t)kRingRows, 1, 1};
+  const cuuint32_t brz[4] = {32, 1, (cuuint32_t)kRingRows, 1};
   int rc = encode_one(&maps->x, f, eb, dims, strides, bx, CU_TENSOR_MAP_SWIZZLE_128B);
   if (rc == 0) rc = encode_one(&maps->y, f, eb, dims, strides, by, CU_TENSOR_MAP_SWIZZLE_NONE);
   if (rc == 0) rc = encode_one(&maps->z, f, eb, dims, strides, bz, CU_TENSOR_MAP_SWIZZLE_NONE);
+  if (rc == 0) rc = encode_one(&maps->ry, f, eb, dims, strides, bry, CU_TENSOR_MAP_SWIZZLE_NONE);
+  if (rc == 0) rc = encode_one(&maps->rz, f, eb, dims, strides, brz, CU_TENSOR_MAP_SWIZZLE_NONE);
   return rc;
+}
+
+// Grid of a persistent launch: every CTA that fits on the device at once
+// (at most one per tile).  The kernel's dynamic shared-memory limit is raised
+// to the maximum once per device, and its occupancy looked up once per
+// shared-memory size (a few entries per thread, replaced round robin).
+template <typename K>
+static cudaError_t persistent_grid(K kernel, size_t smem, long long tiles, int* grid) {
+  struct Entry {
+    const void* k;
+    size_t smem;
+    int dev, blocks;
+  };
+  constexpr int kEntries = 16;
+  static thread_local Entry cache[kEntries] = {};
+  static thread_local int victim = 0;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const void* kp = reinterpret_cast<const void*>(kernel);
+  int blocks = -1;
+  bool attr_set = false;
+  for (const Entry& en : cache) {
+    if (en.k == kp && en.dev == dev) {
+      attr_set = true;
+      if (en.smem == smem) blocks = en.blocks;
+    }
+  }
+  if (blocks < 0) {
+    if (!attr_set) {
+      e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+      if (e != cudaSuccess) return e;
+    }
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 64, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    blocks = per_sm * sms;
+    cache[victim] = Entry{kp, smem, dev, blocks};
+    victim = (victim + 1) % kEntries;
+  }
+  if (blocks < 1) return cudaErrorInvalidConfiguration;
+  *grid = static_cast<int>(tiles < blocks ? tiles : blocks);
+  return cudaSuccess;
+}
+
+static bool use_ring_x(int eb, int nx, const SweepConfig& cfg) {
+  return cfg.persistent >= 2 && cfg.x_lines == 32 && ring_x_smem(eb, nx) != 0 && ring_x_smem(eb, nx) <= 227 * 1024;
+}
+
+static bool use_ring_yz(int eb, int n, const SweepConfig& cfg) {
+  return cfg.persistent >= 1 && cfg.yz_tile == 32 && ring_yz_smem(eb, n) != 0 && ring_yz_smem(eb, n) <= 227 * 1024;
 }
 
 template <typename T>
 cudaError_t launch_sweep_x(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
+  if (use_ring_x(sizeof(T), p.nx, cfg)) {
+    const size_t smem = ring_x_smem(sizeof(T), p.nx);
+    const long long tiles = static_cast<long long>((p.ny + 31) / 32) * p.nz * p.S;
+    int grid = 0;
+    cudaError_t e = persistent_grid(sweep_x_ring_kernel<T>, smem, tiles, &grid);
+    if (e != cudaSuccess) return e;
+    sweep_x_ring_kernel<T><<<grid, 64, smem, st>>>(maps.x, p);
+    return cudaGetLastError();
+  }
   const size_t smem = sweep_x_smem(sizeof(T), p.nx, cfg);
   cudaError_t e = cudaFuncSetAttribute(sweep_x_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -887,9 +1705,26 @@ static cudaError_t launch_yz(const CUtensorMap& map, const SweepParams<T>& p, co
   return cudaGetLastError();
 }
 
+// Tiles per resident CTA below which the persistent y/z sweeps lose to one
+// CTA per tile (measured on B200: FP64 100^3 and FP32 200^3 ran slower
+// persistent, FP64 200^3 / 400^3 and FP32 640^3 faster).
+constexpr long long kRingMinTilesPerCta = 8;
+
 template <typename T, int AXIS>
-static cudaError_t launch_yz_any(const CUtensorMap& map, const SweepParams<T>& p, const SweepConfig& cfg,
-                                 cudaStream_t st) {
+static cudaError_t launch_yz_any(const CUtensorMap& map, const CUtensorMap& ring_map, const SweepParams<T>& p,
+                                 const SweepConfig& cfg, cudaStream_t st) {
+  const int n = (AXIS == 1) ? p.ny : p.nz;
+  if (use_ring_yz(sizeof(T), n, cfg)) {
+    const size_t smem = ring_yz_smem(sizeof(T), n);
+    const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * p.S;
+    int grid = 0;
+    cudaError_t e = persistent_grid(sweep_yz_ring_kernel<T, AXIS>, smem, tiles, &grid);
+    if (e != cudaSuccess) return e;
+    if (cfg.persistent >= 2 || tiles >= kRingMinTilesPerCta * grid) {
+      sweep_yz_ring_kernel<T, AXIS><<<grid, 64, smem, st>>>(ring_map, p);
+      return cudaGetLastError();
+    }
+  }
   switch (cfg.yz_tile) {
     case 16:
       if constexpr (sizeof(T) == 8) return launch_yz<T, AXIS, 16>(map, p, cfg, st);
@@ -902,12 +1737,12 @@ static cudaError_t launch_yz_any(const CUtensorMap& map, const SweepParams<T>& p
 
 template <typename T>
 cudaError_t launch_sweep_y(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
-  return launch_yz_any<T, 1>(maps.y, p, cfg, st);
+  return launch_yz_any<T, 1>(maps.y, maps.ry, p, cfg, st);
 }
 
 template <typename T>
 cudaError_t launch_sweep_z(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
-  return launch_yz_any<T, 2>(maps.z, p, cfg, st);
+  return launch_yz_any<T, 2>(maps.z, maps.rz, p, cfg, st);
 }
 
 template cudaError_t launch_sweep_x<double>(const FieldMaps&, const SweepParams<double>&, const SweepConfig&,

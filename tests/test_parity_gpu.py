@@ -105,6 +105,38 @@ def test_edge_shapes_bitwise(shape):
     assert np.array_equal(me.download_field(), expect)
 
 
+def _screen_field(kind, n, rng):
+    if kind == "signed":  # negative inputs: the screen fails, every line is checked
+        return rng.uniform(-40.0, 40.0, n)
+    # zeros, -0, subnormals and values just around 2^-960 (numerators the
+    # Markstein quotient cannot take), mixed with ordinary values
+    pool = np.array([0.0, -0.0, 5e-324, 1e-310, 2.0 ** -1000, 2.0 ** -960, 2.0 ** -959, 1e-300, 3.0, 1e-5])
+    f = pool[rng.integers(0, pool.size, n)]
+    return np.where(rng.random(n) < 0.5, f, rng.uniform(0.0, 40.0, n))
+
+
+@pytest.mark.parametrize("kind", ["signed", "tiny"])
+def test_exact_division_fallbacks_bitwise(kind):
+    """Inputs that fail the exactness screen (negative values, zeros, -0,
+    subnormals, values near 2^-960) take the checked path and, where a
+    numerator needs it, IEEE division: bit-identical to the oracle under
+    every sweep schedule, on a small case and on one with enough tiles that
+    every persistent CTA walks several."""
+    rng = np.random.default_rng(4242)
+    for shape, schedules in (((23, 19, 17, 2), (0, 1, 2)), ((40, 300, 300, 1), (1, 2))):
+        nx, ny, nz, S = shape
+        wl = W.small_random(78, nx=nx, ny=ny, nz=nz, S=S, n_agents=300, steps=2, stack=True)
+        wl._field0 = _screen_field(kind, wl.n_values, rng)
+        expect = Port.run(wl)
+        for sched in schedules:
+            me = Microenvironment.from_workload(wl)
+            me.set_sweep_schedule(sched)
+            me.simulate_diffusion_decay(wl.steps, sources=True)
+            got = me.download_field()
+            me.close()
+            assert np.array_equal(got.view(np.int64), expect.view(np.int64)), (kind, shape, sched)
+
+
 def test_constants_from_rates_equal_precomputed():
     wl = W.small_random(31, n_agents=300, steps=3, stack=True)
     c1, c2, e2 = Port.workload_constants(wl)
@@ -170,6 +202,39 @@ def test_runs_are_deterministic_and_launch_shape_independent():
         me.close()
     for o in outs[1:]:
         assert np.array_equal(o, outs[0])
+
+
+def test_persistent_schedule_many_tiles_bitwise():
+    """Enough tiles that every CTA of the persistent sweeps walks several of
+    them (both slot orders, refills under the back substitution), with
+    stacked agents and internalized-substrate tracking: FP64 equals the
+    oracle bit for bit, and both schedules give the same bits in FP64 and FP32."""
+    wl = W.small_random(36, nx=40, ny=300, nz=300, S=2, n_agents=20000, steps=2, agent_mode="gauss", stack=True)
+    c1, c2, e2 = Port.workload_constants(wl)
+    f = wl.field0.copy()
+    internal = np.zeros((wl.n_agents, wl.S))
+    V = wl.dx * wl.dx * wl.dx
+    for _ in range(wl.steps):
+        Port.sources_tracked(f, wl.S, wl.agent_voxel, c1, c2, e2, wl.net_export * wl.dt, V, internal)
+        Port.lod_step(f, wl.shape, wl.D, wl.decay, wl.dt, wl.dx, wl.dirichlet_active, wl.dirichlet_values)
+    for precision in ("fp64", "fp32"):
+        outs = []
+        for persistent in (2, 1, 0):
+            me = Microenvironment.from_workload(wl, precision)
+            me.set_sweep_schedule(persistent)
+            assert me.get_sweep_schedule() == persistent
+            me.set_track_internalized_substrates(True)
+            me.simulate_diffusion_decay(wl.steps, sources=True)
+            outs.append((me.download_field(), me.internalized_substrates()))
+            me.close()
+        for o in outs[1:]:
+            assert np.array_equal(outs[0][0], o[0]), precision
+            assert np.array_equal(outs[0][1], o[1]), precision
+        if precision == "fp64":
+            assert np.array_equal(outs[0][0], f)
+            assert np.array_equal(outs[0][1], internal)
+        else:
+            assert np.all(_normwise(outs[0][0], f, wl.S) <= FP32_TOL)
 
 
 def test_upload_download_roundtrip_and_sums():

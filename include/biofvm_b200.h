@@ -191,6 +191,27 @@ int bfvm_set_internalized(bfvm_ctx* ctx, const double* in);
  * become zero.  fraction [count][S] host (fraction_released_at_death). */
 int bfvm_release_internalized(bfvm_ctx* ctx, int count, const int* agents, const double* fraction);
 
+/* Dirichlet nodes: any voxels (interior or on a face) with their own values
+ * and per-substrate activation -- Microenvironment::add_dirichlet_node /
+ * update_dirichlet_node (BioFVM/BioFVM_microenvironment.cpp:218-243) and
+ * set_substrate_dirichlet_activation(substrate, voxel, on) (:288-292).
+ * voxel [count] reference voxel indices, values [count][S], activation
+ * [count][S] or NULL (each substrate's current activation, as set by
+ * bfvm_set_dirichlet_activation).  Replaces the solve's node list (count 0
+ * clears it); a voxel given twice keeps its last entry.  Host pointers. */
+int bfvm_set_dirichlet_nodes(bfvm_ctx* ctx, int count, const int* voxel, const double* values,
+                             const unsigned char* activation);
+/* Microenvironment::apply_dirichlet_conditions (:303-323) for the node list.
+ * The 3-D step pins the six faces only, as the reference's _BLOCKING solver
+ * does; nodes are applied here and by bfvm_step_2d. */
+int bfvm_apply_dirichlet_nodes(bfvm_ctx* ctx);
+/* nsteps steps of the 2-D LOD solver, diffusion_decay_solver__constant_coefficients_LOD_2D
+ * (BioFVM/BioFVM_solvers.cpp:1668-1832), on a solve with nz == 1 (else
+ * BFVM_ERR_SHAPE): [sources (flags & BFVM_STEP_SOURCES)]; nodes pinned; x
+ * sweep; nodes pinned; y sweep; nodes pinned; constant2 = decay*dt/2.  No
+ * face is pinned by the sweeps: boundary conditions are the node list. */
+int bfvm_step_2d(bfvm_ctx* ctx, int nsteps, int flags);
+
 /* Densities at each agent's voxel, [n][S] host doubles, in agent-list order
  * (what Basic_Agent::nearest_density_vector returns to each agent,
  * BioFVM/BioFVM_basic_agent.cpp:389-392). */

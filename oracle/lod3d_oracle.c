@@ -24,8 +24,20 @@
 #include <omp.h>
 #endif
 
+/* halfstep = 0: the 3-D factorization (constant2 = lambda*dt/3); 1: the 2-D
+ * one of diffusion_decay_solver__constant_coefficients_LOD_2D
+ * (BioFVM_solvers.cpp:1696-1707: constant2 = lambda; *= dt; *= 0.5).  Every
+ * other step is the same in both solvers. */
+static void thomas_axis_k(int n, int S, const double* D, const double* decay, double dt, double dx, double* denom,
+                          double* cupper, double* c1, int halfstep);
+
 void orc_thomas_axis(int n, int S, const double* D, const double* decay, double dt, double dx,
                      double* denom, double* cupper, double* c1) {
+  thomas_axis_k(n, S, D, decay, dt, dx, denom, cupper, c1, 0);
+}
+
+static void thomas_axis_k(int n, int S, const double* D, const double* decay, double dt, double dx, double* denom,
+                          double* cupper, double* c1, int halfstep) {
   for (int d = 0; d < S; ++d) {
     /* BioFVM_solvers.cpp:196-218: constant1 = D; *= dt; /= dx; /= dx.
        constant1a = constant1 * -1.0; constant2 = lambda*dt/3;
@@ -37,7 +49,10 @@ void orc_thomas_axis(int n, int S, const double* D, const double* decay, double 
     double k1a = k1 * -1.0;
     double k2 = decay[d];
     k2 *= dt;
-    k2 /= 3.0;
+    if (halfstep)
+      k2 *= 0.5;
+    else
+      k2 /= 3.0;
     double k3 = 1.0;
     k3 += k1;
     k3 += k1;
@@ -327,4 +342,56 @@ void orc_release_internalized(double* field, int S, int count, const int* agents
     for (int d = 0; d < S; ++d) rho[d] += in[d];
     for (int d = 0; d < S; ++d) in[d] = 0.0;
   }
+}
+
+/* Microenvironment::apply_dirichlet_conditions (BioFVM/BioFVM_microenvironment.cpp:
+ * 303-323) over a node list: for node q, every substrate d with act[q][d]
+ * set takes values[q][d].  act NULL: all set.  Nodes hold distinct voxels. */
+void orc_dirichlet_nodes(double* field, int S, int count, const int* voxel, const double* values,
+                         const unsigned char* act) {
+  for (int q = 0; q < count; ++q)
+    for (int d = 0; d < S; ++d)
+      if (!act || act[(size_t)q * S + d]) field[(size_t)voxel[q] * S + d] = values[(size_t)q * S + d];
+}
+
+/* One step of the 2-D LOD solver, diffusion_decay_solver__constant_coefficients_LOD_2D
+ * (BioFVM/BioFVM_solvers.cpp:1668-1832) as its commented-out vector forms
+ * state it: nodes pinned; x sweep; nodes pinned; y sweep; nodes pinned.
+ * Field in the reference layout with nz = 1: (i*ny + j)*S + d.  The x lines
+ * step by ny*S values and the y lines by S (the reference's loops in this
+ * tree step by S and by nx, which walk other lines or past the array for
+ * most shapes, and add the y upper-diagonal term where the commented naxpy
+ * subtracts it; they agree with this restatement when ny == 1). */
+void orc_lod2d_step(double* p, int nx, int ny, int S, const double* D, const double* decay, double dt, double dx,
+                    int count, const int* voxel, const double* values, const unsigned char* act) {
+  double* coef = (double*)malloc(sizeof(double) * (2 * ((size_t)nx + ny) * S + S));
+  double *dnx = coef, *cx = dnx + (size_t)nx * S, *dny = cx + (size_t)nx * S, *cy = dny + (size_t)ny * S;
+  double* c1 = cy + (size_t)ny * S;
+  thomas_axis_k(nx, S, D, decay, dt, dx, dnx, cx, c1, 1);
+  thomas_axis_k(ny, S, D, decay, dt, dx, dny, cy, c1, 1);
+  const size_t jx = (size_t)ny * S, jy = (size_t)S;
+  orc_dirichlet_nodes(p, S, count, voxel, values, act);
+  for (int j = 0; j < ny; ++j)
+    for (int d = 0; d < S; ++d) {
+      double* q = p + (size_t)j * S + d;
+      q[0] /= dnx[d];
+      for (int i = 1; i < nx; ++i) {
+        q[i * jx] = fma(c1[d], q[(i - 1) * jx], q[i * jx]);
+        q[i * jx] /= dnx[(size_t)i * S + d];
+      }
+      for (int i = nx - 2; i >= 0; --i) q[i * jx] = fma(-cx[(size_t)i * S + d], q[(i + 1) * jx], q[i * jx]);
+    }
+  orc_dirichlet_nodes(p, S, count, voxel, values, act);
+  for (int i = 0; i < nx; ++i)
+    for (int d = 0; d < S; ++d) {
+      double* q = p + (size_t)i * jx + d;
+      q[0] /= dny[d];
+      for (int j = 1; j < ny; ++j) {
+        q[j * jy] = fma(c1[d], q[(j - 1) * jy], q[j * jy]);
+        q[j * jy] /= dny[(size_t)j * S + d];
+      }
+      for (int j = ny - 2; j >= 0; --j) q[j * jy] = fma(-cy[(size_t)j * S + d], q[(j + 1) * jy], q[j * jy]);
+    }
+  orc_dirichlet_nodes(p, S, count, voxel, values, act);
+  free(coef);
 }

@@ -110,6 +110,18 @@ void orc_sources_tracked(double* field, int S, int n, const int* voxel, const un
 void orc_release_internalized(double* field, int S, int count, const int* agents, const int* voxel,
                               const double* fraction, double vvox, double* internal);
 
+/* Interior Dirichlet nodes: apply_dirichlet_conditions (BioFVM_microenvironment.cpp:
+ * 303-323) for a list of distinct voxels, values [count][S], act [count][S]
+ * or NULL (all substrates). */
+void orc_dirichlet_nodes(double* field, int S, int count, const int* voxel, const double* values,
+                         const unsigned char* act);
+
+/* One 2-D LOD step (diffusion_decay_solver__constant_coefficients_LOD_2D,
+ * BioFVM/BioFVM_solvers.cpp:1668-1832) on an nx x ny x 1 grid, with the node
+ * list pinned before, between and after the two sweeps. */
+void orc_lod2d_step(double* p, int nx, int ny, int S, const double* D, const double* decay, double dt, double dx,
+                    int count, const int* voxel, const double* values, const unsigned char* act);
+
 #ifdef __cplusplus
 }
 #endif

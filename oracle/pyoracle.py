@@ -70,6 +70,11 @@ class Port:
             L.orc_sources_tracked.restype = None
             L.orc_release_internalized.argtypes = [_dp, C.c_int, C.c_int, _ip, _ip, _dp, C.c_double, _dp]
             L.orc_release_internalized.restype = None
+            L.orc_dirichlet_nodes.argtypes = [_dp, C.c_int, C.c_int, _ip, _dp, C.c_void_p]
+            L.orc_dirichlet_nodes.restype = None
+            L.orc_lod2d_step.argtypes = [_dp, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_int,
+                                         _ip, _dp, C.c_void_p]
+            L.orc_lod2d_step.restype = None
             cls._lib = L
         return cls._lib
 
@@ -141,6 +146,30 @@ class Port:
                                       None if act is None else act.ctypes.data_as(C.c_void_p),
                                       _f64(c1).ravel(), _f64(c2).ravel(), _f64(e2).ravel(), _f64(e1).ravel(),
                                       float(vvox), internal.reshape(-1))
+        return field
+
+    @staticmethod
+    def _nodes(voxel, values, act, S):
+        voxel = np.ascontiguousarray(voxel, np.int32)
+        values = _f64(values).reshape(voxel.size, S)
+        act = None if act is None else np.ascontiguousarray(act, np.uint8).reshape(voxel.size, S)
+        return voxel, values, act
+
+    @classmethod
+    def dirichlet_nodes(cls, field, S, voxel, values, act=None):
+        """Pin a node list (distinct voxels) in place; act [n, S] or None (all)."""
+        voxel, values, act = cls._nodes(voxel, values, act, S)
+        cls.lib().orc_dirichlet_nodes(field.reshape(-1), S, voxel.size, voxel, values.ravel(),
+                                      None if act is None else act.ctypes.data_as(C.c_void_p))
+        return field
+
+    @classmethod
+    def lod2d_step(cls, field, nx, ny, S, D, decay, dt, dx, voxel, values, act=None):
+        """One 2-D LOD step (nz = 1) with the node list pinned around the sweeps."""
+        voxel, values, act = cls._nodes(voxel, values, act, S)
+        cls.lib().orc_lod2d_step(field.reshape(-1), nx, ny, S, _f64(D), _f64(decay), float(dt), float(dx),
+                                 voxel.size, voxel, values.ravel(),
+                                 None if act is None else act.ctypes.data_as(C.c_void_p))
         return field
 
     @classmethod
@@ -295,6 +324,14 @@ class Reference:
             L.ref_env_agent_set_internalized.restype = None
             L.ref_env_agent_release.argtypes = [vp, C.c_int, _dp]
             L.ref_env_agent_release.restype = None
+            L.ref_env_add_dirichlet_node.argtypes = [vp, C.c_int, _dp]
+            L.ref_env_add_dirichlet_node.restype = None
+            L.ref_env_set_node_activation.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+            L.ref_env_set_node_activation.restype = None
+            L.ref_env_apply_dirichlet_conditions.argtypes = [vp]
+            L.ref_env_apply_dirichlet_conditions.restype = None
+            L.ref_env_lod2d.argtypes = [vp, C.c_double]
+            L.ref_env_lod2d.restype = None
             if dropin:
                 L.ref_env_dropin_fuse_sources.argtypes = [vp, C.c_int, C.c_double]
                 L.ref_env_dropin_fuse_sources.restype = C.c_int
@@ -367,6 +404,21 @@ class Reference:
             self.L.ref_env_agent_internalized(self.h, a, o)
             out[a] = o
         return out
+
+    def add_dirichlet_node(self, voxel, values):
+        self.L.ref_env_add_dirichlet_node(self.h, int(voxel), _f64(values))
+
+    def set_node_activation(self, voxel, substrate, on):
+        self.L.ref_env_set_node_activation(self.h, int(voxel), int(substrate), 1 if on else 0)
+
+    def apply_dirichlet_conditions(self):
+        """Microenvironment::apply_dirichlet_conditions: every Dirichlet node."""
+        self.L.ref_env_apply_dirichlet_conditions(self.h)
+
+    def lod2d(self):
+        """The reference's 2-D LOD solver, one step (use with ny == 1 only)."""
+        with _stdout_to_stderr():
+            self.L.ref_env_lod2d(self.h, self.wl.dt)
 
     def set_internalized(self, amounts):
         for a in range(self.wl.n_agents):

@@ -163,6 +163,35 @@ void ref_env_apply_dirichlet(void* h) {
   e->M->apply_dirichlet_boundaries_conditions(0, 1);
 }
 
+/* Microenvironment::add_dirichlet_node(voxel, values [S])
+ * (BioFVM_microenvironment.cpp:218-225). */
+void ref_env_add_dirichlet_node(void* h, int voxel, const double* values) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  std::vector<double> v(values, values + e->S);
+  e->M->add_dirichlet_node(voxel, v);
+}
+
+/* Microenvironment::set_substrate_dirichlet_activation(substrate, voxel, on)
+ * (BioFVM_microenvironment.cpp:288-292): one voxel's activation. */
+void ref_env_set_node_activation(void* h, int voxel, int substrate, int on) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  e->M->set_substrate_dirichlet_activation(substrate, voxel, on != 0);
+}
+
+/* Microenvironment::apply_dirichlet_conditions (BioFVM_microenvironment.cpp:303-323). */
+void ref_env_apply_dirichlet_conditions(void* h) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  e->M->apply_dirichlet_conditions();
+}
+
+/* One call of diffusion_decay_solver__constant_coefficients_LOD_2D(M, dt)
+ * (BioFVM_solvers.cpp:1668-1832).  Callers keep to shapes where its loops
+ * stay inside the density array (ny == 1). */
+void ref_env_lod2d(void* h, double dt) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  diffusion_decay_solver__constant_coefficients_LOD_2D(*e->M, dt);
+}
+
 /* Add one agent through the reference API.  Rates are [S] arrays.  Returns
  * the agent's index in this environment's list, or -1 if the reference
  * rejects the position. */

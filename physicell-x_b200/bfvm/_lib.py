@@ -65,6 +65,9 @@ _SIGS = {
     "bfvm_sample_agents": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_set_sweep_schedule": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_get_sweep_schedule": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "bfvm_set_dirichlet_nodes": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bfvm_apply_dirichlet_nodes": (C.c_int, [C.c_void_p]),
+    "bfvm_step_2d": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "bfvm_set_agent_tracking": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_set_agent_exports": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_get_internalized": (C.c_int, [C.c_void_p, C.c_void_p]),

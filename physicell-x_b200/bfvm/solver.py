@@ -150,6 +150,26 @@ class Microenvironment:
         check(self.L.bfvm_sample_agents(self.h, _ptr(out)), "bfvm_sample_agents")
         return out
 
+    # -- Dirichlet nodes and the 2-D solver ---------------------------------
+    def set_dirichlet_nodes(self, voxel, values, activation=None):
+        """Dirichlet nodes (Microenvironment::add_dirichlet_node and the
+        per-voxel set_substrate_dirichlet_activation): voxel [n] reference
+        indices, values [n, S], activation [n, S] or None (each substrate's
+        current activation).  Replaces the node list; an empty list clears it."""
+        v = np.ascontiguousarray(voxel, np.int32).ravel()
+        vals = _f64(values).reshape(v.size, self.S)
+        act = None if activation is None else np.ascontiguousarray(activation, np.uint8).reshape(v.size, self.S)
+        check(self.L.bfvm_set_dirichlet_nodes(self.h, int(v.size), _ptr(v), _ptr(vals), _ptr(act)),
+              "bfvm_set_dirichlet_nodes")
+
+    def apply_dirichlet_conditions(self):
+        """Microenvironment::apply_dirichlet_conditions over the node list."""
+        check(self.L.bfvm_apply_dirichlet_nodes(self.h), "bfvm_apply_dirichlet_nodes")
+
+    def simulate_diffusion_decay_2d(self, nsteps=1, sources=False):
+        """nsteps steps of the 2-D LOD solver (nz must be 1)."""
+        check(self.L.bfvm_step_2d(self.h, int(nsteps), BFVM_STEP_SOURCES if sources else 0), "bfvm_step_2d")
+
     # -- internalized substrates ---------------------------------------------
     def set_track_internalized_substrates(self, on=True):
         """Microenvironment_Options::track_internalized_substrates_in_each_agent

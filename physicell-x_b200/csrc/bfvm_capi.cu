@@ -27,8 +27,10 @@ void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); 
 // reference's thomas_denom*/thomas_c* and c1[S] = thomas_constant1.
 // Contractions are written out with std::fma (this file is compiled with
 // -ffp-contract=off), matching the reference's g++ FMA contraction of axpy.
+// half: the 2-D solver's constants (diffusion_decay_solver__constant_coefficients_LOD_2D,
+// :1696-1707: constant2 = decay; *= dt; *= 0.5), otherwise the same steps.
 void thomas_axis_host(int n, int S, const double* D, const double* decay, double dt, double dx, double* denom,
-                      double* cup, double* c1) {
+                      double* cup, double* c1, bool half) {
   for (int d = 0; d < S; ++d) {
     double k1 = D[d];
     k1 *= dt;
@@ -37,7 +39,10 @@ void thomas_axis_host(int n, int S, const double* D, const double* decay, double
     const double k1a = k1 * -1.0;
     double k2 = decay[d];
     k2 *= dt;
-    k2 /= 3.0;
+    if (half)
+      k2 *= 0.5;
+    else
+      k2 /= 3.0;
     double k3 = 1.0;
     k3 += k1;
     k3 += k1;
@@ -151,6 +156,8 @@ size_t coef_bytes(const bfvm_ctx* c, size_t* dr_off, size_t* cu_off) {
 
 int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
   const int S = c->S;
+  c->D.assign(D, D + S);
+  c->decay.assign(decay, decay + S);
   c->screen = 1;
   for (int s = 0; s < S; ++s)
     if (!(D[s] >= 0.0) || !(decay[s] >= 0.0)) c->screen = 0;
@@ -163,7 +170,7 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
     const int n = n_axis[ax];
     const int np = coef_pad(n);
     std::vector<double> dn(static_cast<size_t>(n) * S), cu(static_cast<size_t>(n) * S);
-    thomas_axis_host(n, S, D, decay, c->dt, c->dx, dn.data(), cu.data(), c1.data());
+    thomas_axis_host(n, S, D, decay, c->dt, c->dx, dn.data(), cu.data(), c1.data(), false);
     for (int s = 0; s < S; ++s)
       for (int i = 0; i < np; ++i) {
         const size_t q = static_cast<size_t>(s) * np + i;
@@ -398,6 +405,10 @@ int bfvm_destroy(bfvm_ctx* c) {
   dfree(c, c->d_grad);
   dfree(c, c->d_bulk);
   dfree(c, c->d_internal);
+  dfree(c, c->d_coef2d);
+  dfree(c, c->d_shift2d);
+  dfree(c, c->d_zero_active);
+  dfree(c, c->d_nodes);
   for (cudaEvent_t e : c->events) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -513,7 +524,7 @@ static int choose_offsets(bfvm_ctx* c) {
   BFVM_CUDA(cudaMemcpy(c->d_off, off.data(), S * sizeof(double), cudaMemcpyHostToDevice));
   BFVM_CUDA(cudaMemcpy(c->d_shift, shift.data(), S * sizeof(double), cudaMemcpyHostToDevice));
   c->off = off;
-  return BFVM_OK;
+  return update_shift_2d(c);
 }
 
 static int pack_from_device_aos(bfvm_ctx* c, const double* d_aos) {

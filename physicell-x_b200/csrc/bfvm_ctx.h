@@ -53,6 +53,15 @@ struct bfvm_ctx {
   double* d_internal = nullptr; // [cap_internal][S] amounts per agent, list order
   int n_internal = 0, cap_internal = 0;
   int agents_from_rates = 0;    // the list came from bfvm_set_agents_from_rates (rates kept in d_rates)
+  // 2-D LOD (bfvm_step_2d) and Dirichlet nodes (bfvm_set_dirichlet_nodes)
+  std::vector<double> D, decay; // the solve's rates (host copies)
+  void* d_coef2d = nullptr;     // x and y coefficient rows of the 2-D solver, laid out as d_coef
+  size_t dr2_off[2] = {0, 0}, cu2_off[2] = {0, 0};
+  std::vector<double> c2_2d;    // dt*decay/2 per substrate
+  double* d_shift2d = nullptr;  // FP32: c2_2d * off [S]
+  int* d_zero_active = nullptr; // [S] zeros: the 2-D sweeps pin no faces
+  int n_nodes = 0;
+  void* d_nodes = nullptr;      // long long offset [n] | double value [n][S] | uchar activation [n][S]
   // host-side mirrors
   std::vector<unsigned char> active;
   std::vector<double> faces;    // same layout as d_faces
@@ -98,6 +107,14 @@ struct DeviceGuard {
 // (allocated on first use) and the device-layout -> reference-layout copy.
 int ensure_staging(bfvm_ctx* c);
 int unpack_to_device_aos(bfvm_ctx* c, double* d_aos);
+
+// bfvm_lod2d.cu: the FP32 right-hand-side shift of the 2-D solver, brought
+// in line with the field offsets (no-op until the 2-D solver is set up).
+int update_shift_2d(bfvm_ctx* c);
+
+// bfvm_capi.cu: Thomas factorization of one axis (half: 2-D constants).
+void thomas_axis_host(int n, int S, const double* D, const double* decay, double dt, double dx, double* denom,
+                      double* cup, double* c1, bool half);
 
 // bfvm_tracking.cu: after a new agent list is built, bring the tracking
 // buffers to its size (amounts of surviving list positions kept, new ones

@@ -39,7 +39,8 @@ sys.path.insert(0, os.path.join(ROOT, "physicell-x_b200"))
 METRIC = "voxel·substrate updates/s per LOD step"
 UNIT = "voxel·substrate updates/s"
 WORKLOAD = ("cube200: 200x200x200 voxels (dx=10 um), 4 substrates, 100000 agents, FP64, dt=0.01 min; "
-            "one LOD step = fused agent sources + x/y/z Thomas sweeps with Dirichlet pins")
+            "one LOD step = agent sources (standalone kernel, timed with the x sweep) + x/y/z Thomas "
+            "sweeps with Dirichlet pins")
 
 # DRAM bytes per launch of each sweep kernel (dram__bytes_read.sum +
 # dram__bytes_write.sum) from one ncu capture of this workload at the current

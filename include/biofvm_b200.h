@@ -309,6 +309,10 @@ int bfvm_set_launch(bfvm_ctx* ctx, int x_lines, int yz_tile, int yz_chunk);
  * per tile; 2: all three persistent; 0: one CTA per tile everywhere.  Every
  * schedule computes the same bits. */
 int bfvm_set_sweep_schedule(bfvm_ctx* ctx, int persistent);
+/* Where bfvm_step applies the agents: fused = 0 (default) the standalone
+ * source kernel ahead of the sweeps, 1 inside the x sweep, on the staged
+ * tile.  Both give the same bits. */
+int bfvm_set_fused_sources(bfvm_ctx* ctx, int fused);
 int bfvm_get_sweep_schedule(bfvm_ctx* ctx, int* persistent);
 
 /* Number of this library's kernels launched by the calls so far (counted on

@@ -286,6 +286,11 @@ class Microenvironment:
         tile; 2: all three sweeps persistent.  True/False map to 1/0."""
         check(self.L.bfvm_set_sweep_schedule(self.h, int(persistent)), "bfvm_set_sweep_schedule")
 
+    def set_fused_sources(self, fused=True):
+        """Apply the agents inside the x sweep (True) or with the standalone
+        source kernel ahead of the sweeps (False, the default)."""
+        check(self.L.bfvm_set_fused_sources(self.h, 1 if fused else 0), "bfvm_set_fused_sources")
+
     def get_sweep_schedule(self):
         v = C.c_int()
         check(self.L.bfvm_get_sweep_schedule(self.h, C.byref(v)), "bfvm_get_sweep_schedule")

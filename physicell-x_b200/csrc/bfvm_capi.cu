@@ -80,7 +80,8 @@ constexpr int kMaxTimedSteps = 4096;
 
 template <typename T>
 int run_steps(bfvm_ctx* c, int nsteps, bool sources) {
-  const SweepParams<T> p = make_params<T>(c, sources);
+  const bool standalone = sources && c->n_agents > 0 && !c->cfg.fuse_sources;
+  const SweepParams<T> p = make_params<T>(c, sources && !standalone);
   for (int s = 0; s < nsteps; ++s) {
     cudaEvent_t* ev = nullptr;
     if (c->timing && c->timed_steps < kMaxTimedSteps) {
@@ -94,6 +95,10 @@ int run_steps(bfvm_ctx* c, int nsteps, bool sources) {
       ++c->timed_steps;
     }
     if (ev) BFVM_CUDA(cudaEventRecord(ev[0], c->stream));
+    if (standalone) {
+      const int rc = bfvm_apply_sources(c);  // timed with the x sweep
+      if (rc != BFVM_OK) return rc;
+    }
     BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, c->stream));
     if (ev) BFVM_CUDA(cudaEventRecord(ev[1], c->stream));
     BFVM_CUDA(launch_sweep_y<T>(c->maps, p, c->cfg, c->stream));
@@ -916,6 +921,14 @@ extern "C" int bfvm_set_sweep_schedule(bfvm_ctx* c, int persistent) {
   return BFVM_OK;
 }
 
+extern "C" int bfvm_set_fused_sources(bfvm_ctx* c, int fused) {
+  if (!c || (fused != 0 && fused != 1)) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  c->cfg.fuse_sources = fused;
+  return BFVM_OK;
+}
+
 extern "C" int bfvm_get_sweep_schedule(bfvm_ctx* c, int* persistent) {
   if (!c || !persistent) return BFVM_ERR_ARG;
   *persistent = c->cfg.persistent;
@@ -937,6 +950,7 @@ extern "C" int bfvm_set_launch(bfvm_ctx* c, int x_lines, int yz_tile, int yz_chu
   cfg.yz_tile = yz_tile;
   cfg.yz_chunk = yz_chunk;
   cfg.persistent = c->cfg.persistent;
+  cfg.fuse_sources = c->cfg.fuse_sources;
   // x_lines: multiple of 8 (1024-byte swizzle atoms), at most 256 (box
   // limit); yz_tile: 16 (FP64 only), 32 or 64 consecutive x -- whole 128-byte
   // rows, so every TMA chunk starts 128-byte aligned in shared memory and

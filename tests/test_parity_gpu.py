@@ -61,7 +61,7 @@ def test_small_goldens_bitwise(golden_dir):
 
 
 def test_cube50_full_run_matches_reference_hash(golden_dir):
-    """cube50 (50^3 x 2 substrates, 2000 agents), all 1000 LOD steps with fused
+    """cube50 (50^3 x 2 substrates, 2000 agents), all 1000 LOD steps with
     sources: the final field is bit-identical to the reference's."""
     g = _load(golden_dir, "cube50_1000")
     wl = W.cube50(steps=1000)
@@ -156,6 +156,27 @@ def test_standalone_sources_then_diffusion_equals_fused():
         me.simulate_cell_sources_and_sinks()
         me.simulate_diffusion_decay(1, sources=False)
     assert np.array_equal(me.download_field(), expect)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_fused_and_standalone_sources_give_the_same_bits(precision):
+    """bfvm_step with sources: the agents inside the x sweep or with the
+    standalone kernel ahead of it (the default), under every sweep schedule,
+    with stacked Gaussian agents and a grid large enough for many tiles."""
+    wl = W.small_random(37, nx=90, ny=120, nz=100, S=2, n_agents=30000, steps=3, agent_mode="gauss", stack=True)
+    outs = []
+    for fused in (True, False):
+        for sched in (0, 1, 2):
+            me = Microenvironment.from_workload(wl, precision)
+            me.set_fused_sources(fused)
+            me.set_sweep_schedule(sched)
+            me.simulate_diffusion_decay(wl.steps, sources=True)
+            outs.append(me.download_field())
+            me.close()
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+    if precision == "fp64":
+        assert np.array_equal(outs[0], Port.run(wl))
 
 
 def test_sources_only_matches_port_and_sampling():

@@ -42,14 +42,15 @@ WORKLOAD = ("cube200: 200x200x200 voxels (dx=10 um), 4 substrates, 100000 agents
             "one LOD step = agent sources (standalone kernel, timed with the x sweep) + x/y/z Thomas "
             "sweeps with Dirichlet pins")
 
-# DRAM bytes per launch of each sweep kernel (dram__bytes_read.sum +
+# DRAM bytes per launch of each timed interval (dram__bytes_read.sum +
 # dram__bytes_write.sum) from one ncu capture of this workload at the current
 # kernels; profiles/sweeps_cube200_fp64.txt gives the command and the raw
-# figures.  Keys: (precision, sweep index 0=x 1=y 2=z).
+# figures.  Keys: (precision, sweep index 0=x 1=y 2=z); the x interval is the
+# standalone source kernel plus the x sweep.
 NCU_TRAFFIC = {
-    ("fp64", 0): 279770112 + 198588672,
-    ("fp64", 1): 265704704 + 195987968,
-    ("fp64", 2): 265680640 + 195192576,
+    ("fp64", 0): (56553984 + 1460224) + (268286976 + 195136256),
+    ("fp64", 1): 265752576 + 194710528,
+    ("fp64", 2): 265712896 + 195134976,
 }
 
 

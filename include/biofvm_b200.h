@@ -212,6 +212,29 @@ int bfvm_apply_dirichlet_nodes(bfvm_ctx* ctx);
  * face is pinned by the sweeps: boundary conditions are the node list. */
 int bfvm_step_2d(bfvm_ctx* ctx, int nsteps, int flags);
 
+/* General_Mesh::write_to_matlab (BioFVM/BioFVM_mesh.cpp:425-447): MATLAB v4
+ * matrix "mesh", one column per voxel in reference order (centre x, y, z,
+ * volume), assembled on the device; same start arguments as
+ * bfvm_write_matlab. */
+int bfvm_write_mesh_matlab(bfvm_ctx* ctx, const char* path, double x_start, double y_start, double z_start);
+
+/* The microenvironment's MultiCellDS output: what
+ * add_BioFVM_substrates_to_open_xml_pugi (BioFVM/BioFVM_MultiCellDS.cpp:518-823,
+ * first call, MATLAB data files) and save_BioFVM_to_MultiCellDS_xml_pugi
+ * (:1880-1890) produce for this solve -- <base>_mesh0.mat,
+ * <base>_microenvironment0.mat and <base>.xml, the document with the
+ * <microenvironment> element and empty <metadata> and <cellular_information>
+ * (the reference's metadata carries wall-clock timestamps and its agents
+ * come from the cell model), byte for byte as the reference writes them.
+ * Names and units are the Microenvironment's (name, mesh.units,
+ * spatial_units, time_units, density_names/units [S]); bounding_box [6] is
+ * mesh.bounding_box (x, y, z minima, then maxima).  xml (capacity bytes) or
+ * NULL receives the document text, xml_length (or NULL) its length. */
+int bfvm_write_multicellds(bfvm_ctx* ctx, const char* filename_base, const char* domain_name,
+                           const char* mesh_units, const char* spatial_units, const char* time_units,
+                           const char* const* density_names, const char* const* density_units,
+                           const double* bounding_box, char* xml, size_t xml_capacity, size_t* xml_length);
+
 /* Densities at each agent's voxel, [n][S] host doubles, in agent-list order
  * (what Basic_Agent::nearest_density_vector returns to each agent,
  * BioFVM/BioFVM_basic_agent.cpp:389-392). */

@@ -332,6 +332,14 @@ class Reference:
             L.ref_env_apply_dirichlet_conditions.restype = None
             L.ref_env_lod2d.argtypes = [vp, C.c_double]
             L.ref_env_lod2d.restype = None
+            L.ref_env_set_names.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p]
+            L.ref_env_set_names.restype = None
+            L.ref_env_set_density_name.argtypes = [vp, C.c_int, C.c_char_p, C.c_char_p]
+            L.ref_env_set_density_name.restype = None
+            L.ref_env_bounding_box.argtypes = [vp, _dp]
+            L.ref_env_bounding_box.restype = None
+            L.ref_env_multicellds_substrates.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_long]
+            L.ref_env_multicellds_substrates.restype = C.c_long
             if dropin:
                 L.ref_env_dropin_fuse_sources.argtypes = [vp, C.c_int, C.c_double]
                 L.ref_env_dropin_fuse_sources.restype = C.c_int
@@ -414,6 +422,27 @@ class Reference:
     def apply_dirichlet_conditions(self):
         """Microenvironment::apply_dirichlet_conditions: every Dirichlet node."""
         self.L.ref_env_apply_dirichlet_conditions(self.h)
+
+    def bounding_box(self):
+        out = np.zeros(6)
+        self.L.ref_env_bounding_box(self.h, out)
+        return out
+
+    def multicellds_substrates(self, base, domain, mesh_units, spatial_units, time_units, names, units):
+        """The reference's add_BioFVM_substrates_to_open_xml_pugi + document
+        text (and its two MATLAB files under base).  The reference builds the
+        element once per process (a static flag) into a global document, so
+        call this at most once per process."""
+        e = lambda x: str(x).encode()
+        self.L.ref_env_set_names(self.h, e(domain), e(mesh_units), e(spatial_units), e(time_units))
+        for d, (nm, un) in enumerate(zip(names, units)):
+            self.L.ref_env_set_density_name(self.h, d, e(nm), e(un))
+        buf = C.create_string_buffer(1 << 24)
+        with _stdout_to_stderr():
+            n = self.L.ref_env_multicellds_substrates(self.h, e(base), buf, 1 << 24)
+        if n < 0:
+            raise RuntimeError("MultiCellDS document too large")
+        return buf.raw[:n].decode()
 
     def lod2d(self):
         """The reference's 2-D LOD solver, one step (use with ny == 1 only)."""

@@ -30,10 +30,12 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <sstream>
 #include <vector>
 
 #include "BioFVM.h"
 #include "BioFVM_agent_container.h"
+#include "BioFVM_MultiCellDS.h"
 #include "BioFVM_solvers.h"
 #include "DistPhy/DistPhy_Cartesian.h"
 #include "DistPhy/DistPhy_Environment.h"
@@ -161,6 +163,46 @@ void ref_env_set_dirichlet_face_values(void* h, const double* aos) {
 void ref_env_apply_dirichlet(void* h) {
   RefEnv* e = static_cast<RefEnv*>(h);
   e->M->apply_dirichlet_boundaries_conditions(0, 1);
+}
+
+/* The Microenvironment's names and units: name, mesh.units, spatial_units,
+ * time_units, and substrate d's density_names[d] / density_units[d]. */
+void ref_env_set_names(void* h, const char* domain, const char* mesh_units, const char* spatial_units,
+                       const char* time_units) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  e->M->name = domain;
+  e->M->mesh.units = mesh_units;
+  e->M->spatial_units = spatial_units;
+  e->M->time_units = time_units;
+}
+
+void ref_env_set_density_name(void* h, int d, const char* name, const char* units) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  e->M->density_names[d] = name;
+  e->M->density_units[d] = units;
+}
+
+/* mesh.bounding_box [6]. */
+void ref_env_bounding_box(void* h, double* out) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  for (int q = 0; q < 6; ++q) out[q] = e->M->mesh.bounding_box[q];
+}
+
+/* add_BioFVM_substrates_to_open_xml_pugi(biofvm_doc, base, M)
+ * (BioFVM_MultiCellDS.cpp:518-823) -- its first call in a process builds the
+ * <microenvironment> element and writes base_mesh0.mat and
+ * base_microenvironment0.mat -- then the global document as pugixml saves
+ * it (save_BioFVM_to_MultiCellDS_xml_pugi, :1880-1890) copied into out.
+ * Returns the text's length, or -1 if it does not fit in cap bytes. */
+long ref_env_multicellds_substrates(void* h, const char* base, char* out, long cap) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  add_BioFVM_substrates_to_open_xml_pugi(biofvm_doc, base, *e->M);
+  std::ostringstream ss;
+  biofvm_doc.save(ss);
+  const std::string t = ss.str();
+  if (static_cast<long>(t.size()) + 1 > cap) return -1;
+  std::memcpy(out, t.c_str(), t.size() + 1);
+  return static_cast<long>(t.size());
 }
 
 /* Microenvironment::add_dirichlet_node(voxel, values [S])

@@ -67,6 +67,10 @@ _SIGS = {
     "bfvm_set_fused_sources": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_get_sweep_schedule": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "bfvm_set_dirichlet_nodes": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bfvm_write_mesh_matlab": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double]),
+    "bfvm_write_multicellds": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
+                                         C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), C.c_void_p, C.c_char_p,
+                                         C.c_size_t, C.POINTER(C.c_size_t)]),
     "bfvm_apply_dirichlet_nodes": (C.c_int, [C.c_void_p]),
     "bfvm_step_2d": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "bfvm_set_agent_tracking": (C.c_int, [C.c_void_p, C.c_int]),

@@ -235,6 +235,33 @@ class Microenvironment:
         check(self.L.bfvm_write_matlab(self.h, os.fsencode(str(path)), float(origin[0]), float(origin[1]),
                                        float(origin[2])), "bfvm_write_matlab")
 
+    def write_mesh_matlab(self, path, origin):
+        """General_Mesh::write_to_matlab: the MATLAB v4 mesh file (voxel
+        centres and volumes); origin is the domain's lower corner."""
+        import os
+
+        check(self.L.bfvm_write_mesh_matlab(self.h, os.fsencode(str(path)), float(origin[0]), float(origin[1]),
+                                            float(origin[2])), "bfvm_write_mesh_matlab")
+
+    def write_multicellds(self, filename_base, bounding_box, names, units, domain_name="microenvironment",
+                          mesh_units="micron", spatial_units="micron", time_units="min"):
+        """The microenvironment's MultiCellDS output (<base>.xml,
+        <base>_mesh0.mat, <base>_microenvironment0.mat), as
+        save_BioFVM_to_MultiCellDS_xml_pugi writes them for the substrates;
+        returns the XML text."""
+        import os
+
+        enc = lambda x: str(x).encode()
+        n = (C.c_char_p * self.S)(*[enc(x) for x in names])
+        u = (C.c_char_p * self.S)(*[enc(x) for x in units])
+        bb = _f64(np.asarray(bounding_box, np.float64).ravel())
+        length = C.c_size_t()
+        check(self.L.bfvm_write_multicellds(self.h, os.fsencode(str(filename_base)), enc(domain_name), enc(mesh_units),
+                                            enc(spatial_units), enc(time_units), n, u, _ptr(bb), None, 0,
+                                            C.byref(length)), "bfvm_write_multicellds")
+        with open(str(filename_base) + ".xml", "rb") as fh:
+            return fh.read().decode()
+
     def compute_all_gradient_vectors(self, out=None):
         """Gradients of every substrate at every voxel, [voxels, S, 3] in the
         reference's voxel order (Microenvironment::compute_all_gradient_vectors)."""

@@ -14,6 +14,7 @@
 // densities from the reference-layout copy of the field) and streamed to the
 // file through a pinned host buffer.
 #include <cstdio>
+#include <cstring>
 
 #include "bfvm_ctx.h"
 
@@ -46,14 +47,26 @@ __global__ void matlab_columns_kernel(const double* __restrict__ aos, long long 
 
 }  // namespace
 
-extern "C" int bfvm_write_matlab(bfvm_ctx* c, const char* path, double x_start, double y_start, double z_start) {
+namespace bfvm {
+
+// One MATLAB v4 matrix of 4 + S rows (S = c->S with densities, else 0) and
+// one column per voxel, assembled on the device in chunks: the
+// microenvironment file (name "multiscale_microenvironment", with the
+// densities) or General_Mesh::write_to_matlab's mesh file
+// (BioFVM/BioFVM_mesh.cpp:425-447: name "mesh", centre and volume only).
+int write_matlab_columns(bfvm_ctx* c, const char* path, const char* name, bool densities, double x_start,
+                         double y_start, double z_start) {
   if (!c || !path) return BFVM_ERR_ARG;
   bfvm::DeviceGuard g(c->device);
-  int rc = bfvm::ensure_staging(c);
-  if (rc != BFVM_OK) return rc;
-  if ((rc = bfvm::unpack_to_device_aos(c, c->d_staging)) != BFVM_OK) return rc;
+  int rc = BFVM_OK;
+  if (densities) {
+    rc = bfvm::ensure_staging(c);
+    if (rc != BFVM_OK) return rc;
+    if ((rc = bfvm::unpack_to_device_aos(c, c->d_staging)) != BFVM_OK) return rc;
+  }
+  const int S = densities ? c->S : 0;
   const long long nv = static_cast<long long>(c->nx) * c->ny * c->nz;
-  const int w = 4 + c->S;
+  const int w = 4 + S;
   const long long chunk = nv < (1LL << 20) ? nv : (1LL << 20);  // voxels per transfer
   const size_t chunk_bytes = sizeof(double) * static_cast<size_t>(chunk) * w;
   double* d_cols = nullptr;
@@ -76,10 +89,10 @@ extern "C" int bfvm_write_matlab(bfvm_ctx* c, const char* path, double x_start, 
     std::fprintf(stderr, "biofvm_b200: cannot open %s for writing\n", path);
     return finish(BFVM_ERR_ARG);
   }
-  static const char name[] = "multiscale_microenvironment";
+  const size_t name_len = std::strlen(name);
   const unsigned int hdr[5] = {0u, static_cast<unsigned int>(w), static_cast<unsigned int>(nv), 0u,
-                               static_cast<unsigned int>(sizeof(name) - 1)};
-  bool ok = std::fwrite(hdr, sizeof(unsigned int), 5, fp) == 5 && std::fwrite(name, 1, sizeof(name) - 1, fp) == sizeof(name) - 1;
+                               static_cast<unsigned int>(name_len)};
+  bool ok = std::fwrite(hdr, sizeof(unsigned int), 5, fp) == 5 && std::fwrite(name, 1, name_len, fp) == name_len;
   double dv = c->dx * c->dx;
   dv *= c->dx;
   const double xs = x_start + 0.0, ys = y_start + 0.0, zs = z_start + 0.0;
@@ -91,7 +104,7 @@ extern "C" int bfvm_write_matlab(bfvm_ctx* c, const char* path, double x_start, 
     long long blocks = (total + 255) / 256;
     if (blocks > 8LL * sms) blocks = 8LL * sms;
     matlab_columns_kernel<<<static_cast<unsigned>(blocks), 256, 0, c->stream>>>(
-        c->d_staging, v0, cnt, c->ny, c->nz, c->S, xs, ys, zs, c->dx, dv, d_cols);
+        c->d_staging, v0, cnt, c->ny, c->nz, S, xs, ys, zs, c->dx, dv, d_cols);
     if (cudaGetLastError() != cudaSuccess) return finish(BFVM_ERR_CUDA);
     bfvm::note_launches(1);
     const size_t bytes = sizeof(double) * static_cast<size_t>(total);
@@ -102,4 +115,15 @@ extern "C" int bfvm_write_matlab(bfvm_ctx* c, const char* path, double x_start, 
   }
   if (!ok) std::fprintf(stderr, "biofvm_b200: writing %s failed\n", path);
   return finish(ok ? BFVM_OK : BFVM_ERR_ARG);
+}
+
+}  // namespace bfvm
+
+extern "C" int bfvm_write_matlab(bfvm_ctx* c, const char* path, double x_start, double y_start, double z_start) {
+  return bfvm::write_matlab_columns(c, path, "multiscale_microenvironment", true, x_start, y_start, z_start);
+}
+
+extern "C" int bfvm_write_mesh_matlab(bfvm_ctx* c, const char* path, double x_start, double y_start,
+                                      double z_start) {
+  return bfvm::write_matlab_columns(c, path, "mesh", false, x_start, y_start, z_start);
 }

@@ -326,6 +326,8 @@ class Reference:
             L.ref_env_agent_release.restype = None
             L.ref_env_add_dirichlet_node.argtypes = [vp, C.c_int, _dp]
             L.ref_env_add_dirichlet_node.restype = None
+            L.ref_env_remove_dirichlet_node.argtypes = [vp, C.c_int]
+            L.ref_env_remove_dirichlet_node.restype = None
             L.ref_env_set_node_activation.argtypes = [vp, C.c_int, C.c_int, C.c_int]
             L.ref_env_set_node_activation.restype = None
             L.ref_env_apply_dirichlet_conditions.argtypes = [vp]
@@ -343,6 +345,8 @@ class Reference:
             if dropin:
                 L.ref_env_dropin_fuse_sources.argtypes = [vp, C.c_int, C.c_double]
                 L.ref_env_dropin_fuse_sources.restype = C.c_int
+                L.ref_env_dropin_lod2d.argtypes = [vp, C.c_double]
+                L.ref_env_dropin_lod2d.restype = None
             cls._libs[path] = L
         return cls._libs[path]
 
@@ -416,6 +420,9 @@ class Reference:
     def add_dirichlet_node(self, voxel, values):
         self.L.ref_env_add_dirichlet_node(self.h, int(voxel), _f64(values))
 
+    def remove_dirichlet_node(self, voxel):
+        self.L.ref_env_remove_dirichlet_node(self.h, int(voxel))
+
     def set_node_activation(self, voxel, substrate, on):
         self.L.ref_env_set_node_activation(self.h, int(voxel), int(substrate), 1 if on else 0)
 
@@ -448,6 +455,12 @@ class Reference:
         """The reference's 2-D LOD solver, one step (use with ny == 1 only)."""
         with _stdout_to_stderr():
             self.L.ref_env_lod2d(self.h, self.wl.dt)
+
+    def dropin_lod2d(self):
+        """One step of the GPU drop-in's 2-D solver through the serial slot
+        (a Reference opened with dropin=True)."""
+        with _stdout_to_stderr():
+            self.L.ref_env_dropin_lod2d(self.h, self.wl.dt)
 
     def set_internalized(self, amounts):
         for a in range(self.wl.n_agents):

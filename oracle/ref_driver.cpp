@@ -49,6 +49,7 @@ namespace BioFVM {
 /* Provided by physicell-x_b200/host/biofvm_b200_dropin.cpp. */
 void bfvm_b200_release(Microenvironment& M);
 int bfvm_b200_set_fused_sources(Microenvironment& M, std::vector<Basic_Agent*>* agents, double dt);
+void bfvm_b200_install_2d(Microenvironment& M);
 }
 #endif
 
@@ -213,6 +214,12 @@ void ref_env_add_dirichlet_node(void* h, int voxel, const double* values) {
   e->M->add_dirichlet_node(voxel, v);
 }
 
+/* Microenvironment::remove_dirichlet_node (BioFVM_microenvironment.cpp:247-252). */
+void ref_env_remove_dirichlet_node(void* h, int voxel) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  e->M->remove_dirichlet_node(voxel);
+}
+
 /* Microenvironment::set_substrate_dirichlet_activation(substrate, voxel, on)
  * (BioFVM_microenvironment.cpp:288-292): one voxel's activation. */
 void ref_env_set_node_activation(void* h, int voxel, int substrate, int on) {
@@ -334,6 +341,15 @@ int ref_has_dropin(void) {
 int ref_env_dropin_fuse_sources(void* h, int enable, double dt) {
   RefEnv* e = static_cast<RefEnv*>(h);
   return bfvm_b200_set_fused_sources(*e->M, enable ? &e->agents : nullptr, dt);
+}
+
+/* One step of the drop-in's 2-D solver, installed in the serial slot and run
+ * through Microenvironment::simulate_diffusion_decay(dt) as a caller of the
+ * reference's 2-D solver would. */
+void ref_env_dropin_lod2d(void* h, double dt) {
+  RefEnv* e = static_cast<RefEnv*>(h);
+  bfvm_b200_install_2d(*e->M);
+  e->M->simulate_diffusion_decay(dt);
 }
 #endif
 

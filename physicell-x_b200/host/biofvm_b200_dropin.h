@@ -30,6 +30,16 @@ void bfvm_b200_install(Microenvironment& M);
 // The 2-argument (serial) signature, for Microenvironment::diffusion_decay_solver.
 void bfvm_b200_lod3d_serial(Microenvironment& M, double dt);
 
+// The 2-D LOD solver, diffusion_decay_solver__constant_coefficients_LOD_2D
+// (BioFVM_solvers.cpp:1668-1832), on the GPU for meshes one voxel deep in z:
+// Dirichlet nodes (add_dirichlet_node, per-voxel activation) pinned before and
+// after each sweep.  bfvm_b200_install_2d points the serial slot
+// (Microenvironment::diffusion_decay_solver) at it, so
+// M.simulate_diffusion_decay(dt) runs it.  Agents, resident mode and release
+// are shared with the 3-D solver below.
+void bfvm_b200_lod2d_serial(Microenvironment& M, double dt);
+void bfvm_b200_install_2d(Microenvironment& M);
+
 // Apply the given agents' sources/sinks on the GPU, fused ahead of every
 // following LOD step of M (agents == nullptr turns it off).  The caller then
 // must not also call M.simulate_cell_sources_and_sinks for those steps.

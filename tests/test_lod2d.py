@@ -105,6 +105,40 @@ def test_oracle_lod2d_matches_reference_build(seed):
     assert np.array_equal(f, want)
 
 
+@pytest.mark.skipif(not pyoracle.Reference.available(), reason="reference build not present")
+def test_oracle_nodes_follow_remove_dirichlet_node():
+    """remove_dirichlet_node clears the voxel's flag: the reference stops
+    pinning it and the oracle, given the list without it, agrees."""
+    wl = W.small_random(925, n_agents=0, steps=1)
+    rng = np.random.default_rng(25)
+    ref = pyoracle.Reference(wl, threads=1)
+    try:
+        nodes = _interior_nodes(wl, rng, 10, _face_nodes(wl), ref)
+        for v in rng.choice(sorted(nodes), 15, replace=False):
+            ref.remove_dirichlet_node(int(v))
+            del nodes[int(v)]
+        ref.apply_dirichlet_conditions()
+        want = ref.field()
+    finally:
+        ref.close()
+    vox, vals, act = _node_arrays(nodes, wl.S)
+    assert np.array_equal(Port.dirichlet_nodes(wl.field0.copy(), wl.S, vox, vals, act), want)
+
+
+@pytest.mark.skipif(not pyoracle.Reference.available(dropin=True), reason="drop-in library not built")
+def test_dropin_lod2d_rejects_a_3d_mesh():
+    """The drop-in's 2-D solver on a mesh deeper than one voxel prints its
+    error and returns before any device work, densities unchanged."""
+    wl = W.small_random(926, n_agents=0, steps=1)
+    assert wl.nz > 1
+    ref = pyoracle.Reference(wl, threads=1, dropin=True)
+    try:
+        ref.dropin_lod2d()
+        assert np.array_equal(ref.field(), wl.field0)
+    finally:
+        ref.close()
+
+
 def test_oracle_lod2d_conserves_mass_and_commutes():
     """No nodes and no decay: zero-flux sweeps keep each substrate's sum (to
     rounding).  The x and y solves of constant-coefficient lines commute, so
@@ -194,3 +228,71 @@ def test_gpu_nodes_apply_and_fp32_2d():
     with pytest.raises(BfvmError):
         me.set_dirichlet_nodes([8 ** 3], np.zeros((1, 1)))
     me.close()
+
+
+# ------------------------------------------------ GPU, C++ drop-in (2-D) --
+
+_dropin = pytest.mark.skipif(not pyoracle.Reference.available(dropin=True), reason="drop-in library not built")
+
+
+@pytest.mark.gpu
+@_dropin
+@pytest.mark.parametrize("seed", [0, 1])
+def test_gpu_dropin_lod2d_matches_reference_solver(seed):
+    """bfvm_b200_lod2d_serial in the serial slot of the reference's own
+    Microenvironment against the reference's 2-D solver, bit for bit, on the
+    shapes where the reference solver is defined (one substrate, ny == 1)."""
+    wl = W.small_random(940 + seed, nx=40 + 9 * seed, ny=1, nz=1, S=1, n_agents=0, steps=5)
+    wl.dirichlet_active[:] = 1
+    rng = np.random.default_rng(40 + seed)
+    keep = set(rng.choice(wl.nx, 3, replace=False).tolist())
+    cpu = pyoracle.Reference(wl, threads=1, dropin=True)
+    gpu = pyoracle.Reference(wl, threads=1, dropin=True)
+    try:
+        for r in (cpu, gpu):
+            for v in range(wl.nx):
+                if v not in keep:
+                    r.set_node_activation(v, 0, False)
+        for _ in range(wl.steps):
+            cpu.lod2d()
+            gpu.dropin_lod2d()
+        a, b = cpu.field(), gpu.field()
+    finally:
+        cpu.close()
+        gpu.close()
+    assert not np.array_equal(a, wl.field0)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+@_dropin
+@pytest.mark.parametrize("shape", [(50, 40, 1, 3), (33, 70, 1, 2)])
+def test_gpu_dropin_lod2d_nodes_and_sources_bitwise(shape):
+    """General 2-D meshes through the drop-in: interior nodes added, switched
+    and removed through the reference's API between steps, the agents'
+    sources fused on the GPU; bit for bit against the oracle."""
+    nx, ny, nz, S = shape
+    wl = W.small_random(960 + nx, nx=nx, ny=ny, nz=nz, S=S, n_agents=300, steps=3, stack=True)
+    rng = np.random.default_rng(nx)
+    gpu = pyoracle.Reference(wl, threads=1, dropin=True)
+    c1, c2, e2 = Port.workload_constants(wl)
+    f = wl.field0.copy()
+    try:
+        assert gpu.L.ref_env_dropin_fuse_sources(gpu.h, 1, wl.dt) == 0
+        nodes = _interior_nodes(wl, rng, 25, _face_nodes(wl), gpu)
+        for phase in range(2):
+            if phase == 1:
+                nodes = _interior_nodes(wl, rng, 5, nodes, gpu)
+                for v in rng.choice(sorted(nodes), 20, replace=False):
+                    gpu.remove_dirichlet_node(int(v))
+                    del nodes[int(v)]
+            vox, vals, act = _node_arrays(nodes, S)
+            for _ in range(wl.steps):
+                gpu.dropin_lod2d()
+                Port.sources(f, S, wl.agent_voxel, c1, c2, e2)
+                Port.lod2d_step(f, nx, ny, S, wl.D, wl.decay, wl.dt, wl.dx, vox, vals, act)
+        got = gpu.field()
+    finally:
+        gpu.close()
+    assert not np.array_equal(got, wl.field0)
+    assert np.array_equal(got, f)

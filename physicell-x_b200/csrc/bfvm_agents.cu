@@ -323,6 +323,11 @@ cudaError_t agents_build(const AgentBuild& b, cudaStream_t st, int* launches) {
     kin = kout;
     vin = vout;
   }
+  // the sort needs only the voxel ids; the constants are first read here
+  if (b.constants_ready) {
+    const cudaError_t e = cudaStreamWaitEvent(st, b.constants_ready, 0);
+    if (e != cudaSuccess) return e;
+  }
   agent_csr_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, b.sorted_keys, b.sorted_vals, sentinel, b.nx, b.ny * b.nz, b.S,
                                                     b.c1, b.c2, b.e2, b.line_off, b.a_i, b.ac1, b.ac2, b.ae2,
                                                     b.n_valid);

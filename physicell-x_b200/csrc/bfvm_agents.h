@@ -29,6 +29,7 @@ struct AgentBuild {
   double* ac2;
   double* ae2;
   int* n_valid;                // device scalar: agents with a voxel
+  cudaEvent_t constants_ready; // or nullptr: c1/c2/e2 are written by work this event completes
 };
 
 size_t agent_scratch_bytes(int n);

@@ -263,8 +263,9 @@ int ensure_agent_capacity(bfvm_ctx* c, int n) {
   return BFVM_OK;
 }
 
-int build_agents(bfvm_ctx* c, int n) {
+int build_agents(bfvm_ctx* c, int n, cudaEvent_t constants_ready = nullptr) {
   AgentBuild b{};
+  b.constants_ready = constants_ready;
   b.n = n;
   b.S = c->S;
   b.nx = c->nx;
@@ -415,6 +416,12 @@ int bfvm_destroy(bfvm_ctx* c) {
   dfree(c, c->d_zero_active);
   dfree(c, c->d_nodes);
   for (cudaEvent_t e : c->events) cudaEventDestroy(e);
+  if (c->copy_stream) {
+    cudaStreamSynchronize(c->copy_stream);
+    cudaStreamDestroy(c->copy_stream);
+  }
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return BFVM_OK;
@@ -592,6 +599,21 @@ int bfvm_download_field_device(bfvm_ctx* c, double* d_field) {
   return unpack_to_device_aos(c, d_field);
 }
 
+// The side stream that carries an agent list's constants (or rates) to the
+// device while the voxel ids, copied first on the solve's stream, are sorted.
+// Returns with copy_stream ordered after everything enqueued on the stream
+// so far (the previous list's readers of the constants included).
+static int fork_copy_stream(bfvm_ctx* c) {
+  if (!c->copy_stream) {
+    BFVM_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    BFVM_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    BFVM_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+  }
+  BFVM_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+  BFVM_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_fork, 0));
+  return BFVM_OK;
+}
+
 static int set_agents_common(bfvm_ctx* c, int n, const int* voxel, const unsigned char* active) {
   int rc = ensure_agent_capacity(c, n);
   if (rc != BFVM_OK) return rc;
@@ -613,13 +635,18 @@ int bfvm_set_agents(bfvm_ctx* c, int n, const int* voxel, const unsigned char* a
   int rc = set_agents_common(c, n, voxel, active);
   if (rc != BFVM_OK) return rc;
   const size_t row = sizeof(double) * c->S * static_cast<size_t>(n);
+  cudaEvent_t ready = nullptr;
   if (n > 0) {
-    BFVM_CUDA(cudaMemcpyAsync(c->d_c, c1, row, cudaMemcpyHostToDevice, c->stream));
-    BFVM_CUDA(cudaMemcpyAsync(c->d_c + static_cast<size_t>(c->S) * n, c2, row, cudaMemcpyHostToDevice, c->stream));
-    BFVM_CUDA(cudaMemcpyAsync(c->d_c + 2ull * c->S * n, e2, row, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = fork_copy_stream(c)) != BFVM_OK) return rc;
+    BFVM_CUDA(cudaMemcpyAsync(c->d_c, c1, row, cudaMemcpyHostToDevice, c->copy_stream));
+    BFVM_CUDA(cudaMemcpyAsync(c->d_c + static_cast<size_t>(c->S) * n, c2, row, cudaMemcpyHostToDevice,
+                              c->copy_stream));
+    BFVM_CUDA(cudaMemcpyAsync(c->d_c + 2ull * c->S * n, e2, row, cudaMemcpyHostToDevice, c->copy_stream));
+    BFVM_CUDA(cudaEventRecord(c->ev_join, c->copy_stream));
+    ready = c->ev_join;
   }
   c->agents_from_rates = 0;
-  rc = build_agents(c, n);
+  rc = build_agents(c, n, ready);
   return rc == BFVM_OK ? tracking_after_agents(c) : rc;
 }
 
@@ -629,23 +656,28 @@ int bfvm_set_agents_from_rates(bfvm_ctx* c, int n, const int* voxel, const unsig
   DeviceGuard g(c->device);
   int rc = set_agents_common(c, n, voxel, active);
   if (rc != BFVM_OK) return rc;
+  cudaEvent_t ready = nullptr;
   if (n > 0) {
     const size_t row = sizeof(double) * c->S * static_cast<size_t>(n);
     double* vol = c->d_rates;
     double* r = c->d_rates + n;
     const size_t SN = static_cast<size_t>(c->S) * n;
-    BFVM_CUDA(cudaMemcpyAsync(vol, volume, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
-    BFVM_CUDA(cudaMemcpyAsync(r, sec, row, cudaMemcpyHostToDevice, c->stream));
-    BFVM_CUDA(cudaMemcpyAsync(r + SN, upt, row, cudaMemcpyHostToDevice, c->stream));
-    BFVM_CUDA(cudaMemcpyAsync(r + 2 * SN, sat, row, cudaMemcpyHostToDevice, c->stream));
-    BFVM_CUDA(cudaMemcpyAsync(r + 3 * SN, exp_, row, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = fork_copy_stream(c)) != BFVM_OK) return rc;
+    cudaStream_t cs = c->copy_stream;
+    BFVM_CUDA(cudaMemcpyAsync(vol, volume, sizeof(double) * n, cudaMemcpyHostToDevice, cs));
+    BFVM_CUDA(cudaMemcpyAsync(r, sec, row, cudaMemcpyHostToDevice, cs));
+    BFVM_CUDA(cudaMemcpyAsync(r + SN, upt, row, cudaMemcpyHostToDevice, cs));
+    BFVM_CUDA(cudaMemcpyAsync(r + 2 * SN, sat, row, cudaMemcpyHostToDevice, cs));
+    BFVM_CUDA(cudaMemcpyAsync(r + 3 * SN, exp_, row, cudaMemcpyHostToDevice, cs));
     const double vvox = c->dx * c->dx * c->dx;
     BFVM_CUDA(agents_compute_constants(n, c->S, c->dt, vvox, vol, r, r + SN, r + 2 * SN, r + 3 * SN, c->d_c,
-                                       c->d_c + SN, c->d_c + 2 * SN, c->stream));
+                                       c->d_c + SN, c->d_c + 2 * SN, cs));
     note_launches(1);
+    BFVM_CUDA(cudaEventRecord(c->ev_join, cs));
+    ready = c->ev_join;
   }
   c->agents_from_rates = 1;
-  rc = build_agents(c, n);
+  rc = build_agents(c, n, ready);
   return rc == BFVM_OK ? tracking_after_agents(c) : rc;
 }
 

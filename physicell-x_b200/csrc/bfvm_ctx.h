@@ -16,6 +16,10 @@ struct bfvm_ctx {
   double dx = 0, dt = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  // agent lists: the constants cross to the device on copy_stream while the
+  // voxel ids are sorted on stream (fork: stream -> copy_stream, join back)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   void* f = nullptr;           // field, device layout
   size_t field_bytes = 0;
   // coefficients: per axis a, DR rows [S][npad_a] at dr_off[a] and CU rows

@@ -61,6 +61,11 @@ namespace {
 template <typename T>
 constexpr bool kF32 = sizeof(T) == 4;
 
+// Most rings (compute warp + copy warp pairs) in one persistent y/z CTA: the
+// register file holds 4 FP64 or 8 FP32 pairs.
+template <typename T>
+constexpr int kMaxRings = kF32<T> ? 8 : 4;
+
 // Chunks per line are bounded so one 64-bit word holds every barrier's phase.
 constexpr int kMaxChunks = 64;
 constexpr int kBarrierBytes = 1024;  // kMaxChunks barriers, padded to keep the tile 1024-byte aligned
@@ -891,8 +896,9 @@ __device__ __forceinline__ bool ring_copy_loop(long long tile, long long ntiles,
 }
 
 template <typename T, int AXIS>
-__global__ void __launch_bounds__(64) sweep_yz_ring_kernel(const __grid_constant__ CUtensorMap map,
-                                                           const SweepParams<T> p) {
+__global__ void __launch_bounds__(64 * kMaxRings<T>, 1) sweep_yz_ring_kernel(const __grid_constant__ CUtensorMap map,
+                                                                            const SweepParams<T> p,
+                                                                            uint32_t ring_bytes) {
   using DR = typename Coef<T>::DR;
   using CU = typename Coef<T>::CU;
   constexpr int R = kRowBatch;
@@ -910,11 +916,18 @@ __global__ void __launch_bounds__(64) sweep_yz_ring_kernel(const __grid_constant
   const int ntx = (nx + TI - 1) / TI;
   const long long per_s = static_cast<long long>(ntx) * nm;
   const long long ntiles = per_s * p.S;
-  uint64_t* full = reinterpret_cast<uint64_t*>(base);
-  uint64_t* empty = full + kMaxChunks;
-  T* slots = reinterpret_cast<T*>(base + kBarrierBytes);
-  CU* cus = reinterpret_cast<CU*>(slots + static_cast<size_t>(C) * kSlotElems);
+  // Rings per CTA: warps 0..rings-1 compute, warp rings + r is ring r's copy
+  // warp, so consecutive warps -- which the SM spreads over its four
+  // sub-partitions -- put the compute warps on different sub-partitions.
+  const int rings = static_cast<int>(blockDim.x) / 64;
   const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
+  const int ring = warp < rings ? warp : warp - rings;
+  unsigned char* rbase = base + static_cast<size_t>(ring) * ring_bytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(rbase);
+  uint64_t* empty = full + kMaxChunks;
+  T* slots = reinterpret_cast<T*>(rbase + kBarrierBytes);
+  CU* cus = reinterpret_cast<CU*>(slots + static_cast<size_t>(C) * kSlotElems);
+  const long long stride = static_cast<long long>(gridDim.x) * rings;
 
   // tile -> (i0, m, s), x tiles fastest
   auto decode = [&](long long tile, int& i0, int& m, int& s) {
@@ -933,24 +946,27 @@ __global__ void __launch_bounds__(64) sweep_yz_ring_kernel(const __grid_constant
   // the next tile to work on after `tile` (ntiles when there is none)
   auto next_of = [&](long long tile) {
     do {
-      tile += gridDim.x;
+      tile += stride;
     } while (tile < ntiles && skip(tile));
     return tile < ntiles ? tile : ntiles;
   };
-  const long long first = blockIdx.x;
+  const long long first = static_cast<long long>(blockIdx.x) * rings + ring;
 
   if (threadIdx.x == 0) {
     prefetch_tmap(&map);
-    for (int c = 0; c < C; ++c) {
-      mbar_init(smem_u32(&full[c]), 1);
-      mbar_init(smem_u32(&empty[c]), 1);
+    for (int r = 0; r < rings; ++r) {
+      uint64_t* rb = reinterpret_cast<uint64_t*>(base + static_cast<size_t>(r) * ring_bytes);
+      for (int c = 0; c < C; ++c) {
+        mbar_init(smem_u32(&rb[c]), 1);
+        mbar_init(smem_u32(&rb[kMaxChunks + c]), 1);
+      }
     }
     fence_barrier_init();
   }
   __syncthreads();
   long long tile = (first < ntiles && !skip(first)) ? first : next_of(first);
 
-  if (warp == 1) {
+  if (warp >= rings) {
     if (t != 0) return;
     auto load = [&](long long tl, int c, int sl) {
       int i0, m, s;
@@ -1578,11 +1594,27 @@ size_t ring_x_smem(int elem_bytes, int nx) {
   return 1024 + kBarrierBytes + static_cast<size_t>(C) * 32 * 128 + static_cast<size_t>(C) * W * 8;
 }
 
-size_t ring_yz_smem(int elem_bytes, int n_line) {
+// One y/z ring: barriers, C slots of kRingRows rows of 32 values, the staged
+// upper-diagonal row (a multiple of 128 bytes, so rings stack aligned).
+size_t ring_yz_bytes(int elem_bytes, int n_line) {
   const int C = (n_line + kRingRows - 1) / kRingRows;
   if (C > kMaxChunks) return 0;
   const size_t rows = static_cast<size_t>(C) * kRingRows;
-  return 128 + kBarrierBytes + rows * 32 * elem_bytes + rows * 8;
+  return kBarrierBytes + rows * 32 * elem_bytes + rows * 8;
+}
+
+// Rings per persistent y/z CTA: as many as fit (up to kMaxRings), 0 if none.
+static int ring_yz_count(int elem_bytes, int n_line) {
+  const size_t rb = ring_yz_bytes(elem_bytes, n_line);
+  if (rb == 0) return 0;
+  const int fit = static_cast<int>((227 * 1024 - 128) / rb);
+  const int cap = elem_bytes == 4 ? kMaxRings<float> : kMaxRings<double>;
+  return fit < cap ? fit : cap;
+}
+
+size_t ring_yz_smem(int elem_bytes, int n_line) {
+  const int rings = ring_yz_count(elem_bytes, n_line);
+  return rings == 0 ? 0 : 128 + rings * ring_yz_bytes(elem_bytes, n_line);
 }
 
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
@@ -1630,7 +1662,7 @@ int encode_field_maps(FieldMaps* maps, void* f, int eb, int nx, int ny, int nz, 
 // to the maximum once per device, and its occupancy looked up once per
 // shared-memory size (a few entries per thread, replaced round robin).
 template <typename K>
-static cudaError_t persistent_grid(K kernel, size_t smem, long long tiles, int* grid) {
+static cudaError_t persistent_grid(K kernel, size_t smem, long long tiles, int* grid, int threads = 64) {
   struct Entry {
     const void* k;
     size_t smem;
@@ -1657,7 +1689,7 @@ static cudaError_t persistent_grid(K kernel, size_t smem, long long tiles, int* 
       if (e != cudaSuccess) return e;
     }
     int per_sm = 0, sms = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 64, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
@@ -1720,13 +1752,16 @@ static cudaError_t launch_yz_any(const CUtensorMap& map, const CUtensorMap& ring
                                  const SweepConfig& cfg, cudaStream_t st) {
   const int n = (AXIS == 1) ? p.ny : p.nz;
   if (use_ring_yz(sizeof(T), n, cfg)) {
+    const int rings = ring_yz_count(sizeof(T), n);
     const size_t smem = ring_yz_smem(sizeof(T), n);
     const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * p.S;
     int grid = 0;
-    cudaError_t e = persistent_grid(sweep_yz_ring_kernel<T, AXIS>, smem, tiles, &grid);
+    cudaError_t e = persistent_grid(sweep_yz_ring_kernel<T, AXIS>, smem, (tiles + rings - 1) / rings, &grid,
+                                    64 * rings);
     if (e != cudaSuccess) return e;
-    if (cfg.persistent >= 2 || tiles >= kRingMinTilesPerCta * grid) {
-      sweep_yz_ring_kernel<T, AXIS><<<grid, 64, smem, st>>>(ring_map, p);
+    if (cfg.persistent >= 2 || tiles >= kRingMinTilesPerCta * grid * rings) {
+      sweep_yz_ring_kernel<T, AXIS>
+          <<<grid, 64 * rings, smem, st>>>(ring_map, p, static_cast<uint32_t>(ring_yz_bytes(sizeof(T), n)));
       return cudaGetLastError();
     }
   }

@@ -446,6 +446,11 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   // harmlessly (those results are never stored to the field).
   double y = -0.0;  // running value of the forward recurrence (FP64 in both forms)
   const int screen = p.screen;
+  // FP64 without fused agents: the input screen is one vote per tile (the
+  // staged inputs are then the field's, which a failing tile re-reads); with
+  // fused agents each batch is screened and redone from its registers.
+  const bool tile_screen = !kF32<T> && p.line_off == nullptr;
+  int hwmin = INT_MAX;  // minimum input high word of this lane's line
   // Every batch keeps its per-lane face and range checks: a per-tile vote
   // choosing a version without them measured slower here (x sweep, cube200:
   // FP64 0.166 against 0.163 ms, FP32 0.114 against 0.105).
@@ -468,6 +473,13 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
         if (i0 + q >= nx) v[q] = T(1);
     }
     RowPut<T> put{crow, sw};
+    if constexpr (!kF32<T>) {
+      if (tile_screen) {
+        y = forward_bare<W>(v, cf, c1, y, put);
+        hwmin = min(hwmin, batch_min_hi<W>(v));
+        return;
+      }
+    }
     y = forward_store<W>(v, cf, c1, shift, screen, y, put);
   };
   auto forward_pass = [&](bool edge) {
@@ -489,6 +501,38 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
   if (__syncthreads_or(!ok)) {
     if (t == 0) atomicExch(p.status, kDevTimeout);
     return false;
+  }
+  if constexpr (!kF32<T>) {
+    // The tile's screen: a line with an input below 2^-960 (or negative)
+    // anywhere is redone from its inputs -- the field still holds them (this
+    // tile's results are stored only by the back substitution) -- pinned as
+    // the staged row was, with every numerator checked.
+    if (tile_screen && __syncthreads_or(!(screen != 0 && hwmin >= kHiTiny))) {
+      if (!face && valid) {
+        const T* src = p.f + ((static_cast<size_t>(s) * nz + k) * ny + j) * p.nxp;
+        y = -0.0;
+        for (int c = 0; c < C; ++c) {
+          const int i0 = c * W;
+          T v[W];
+          DR cf[W];
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            v[q] = i0 + q < nx ? src[i0 + q] : T(1);
+            cf[q] = __ldg(drp + i0 + q);
+          }
+          if (act) {
+#pragma unroll
+            for (int q = 0; q < W; ++q) {
+              if (i0 + q == 0) v[q] = x0v;
+              if (i0 + q == nx - 1) v[q] = x1v;
+            }
+          }
+          RowPut<T> put{row + c * chunk_bytes, sw};
+          y = forward_checked<W>(v, cf, c1, y, put);
+        }
+      }
+      __syncthreads();
+    }
   }
 
   // Back substitution, last chunk first; each finished chunk is stored at once.

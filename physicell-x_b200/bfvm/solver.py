@@ -318,6 +318,11 @@ class Microenvironment:
         source kernel ahead of the sweeps (False, the default)."""
         check(self.L.bfvm_set_fused_sources(self.h, 1 if fused else 0), "bfvm_set_fused_sources")
 
+    def set_sweep_tmem(self, on=True):
+        """FP64 persistent y/z sweeps with tensor-memory rings (True, the
+        default) or shared-memory rings alone (False); same bits."""
+        check(self.L.bfvm_set_sweep_tmem(self.h, 1 if on else 0), "bfvm_set_sweep_tmem")
+
     def get_sweep_schedule(self):
         v = C.c_int()
         check(self.L.bfvm_get_sweep_schedule(self.h, C.byref(v)), "bfvm_get_sweep_schedule")

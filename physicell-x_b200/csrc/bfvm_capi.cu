@@ -367,12 +367,14 @@ int bfvm_create(const bfvm_config* cfg, bfvm_ctx** out) {
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_active), S * sizeof(int));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_faces), face_elems(c) * 8);
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_status), sizeof(int));
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_tile_counter), 2 * sizeof(unsigned long long));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_nvalid), sizeof(int));
   if (rc == BFVM_OK)
     rc = dalloc(c, reinterpret_cast<void**>(&c->d_line_off), sizeof(int) * (static_cast<size_t>(c->ny) * c->nz + 1));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_sums), sizeof(double) * (S * 1024 + S));
   if (rc != BFVM_OK) return fail(rc);
-  if (cudaMemset(c->f, 0, c->field_bytes) != cudaSuccess || cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess)
+  if (cudaMemset(c->f, 0, c->field_bytes) != cudaSuccess || cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess ||
+      cudaMemset(c->d_tile_counter, 0, 2 * sizeof(unsigned long long)) != cudaSuccess)
     return fail(BFVM_ERR_CUDA);
   if ((rc = upload_coefficients(c, cfg->diffusion_coefficients, cfg->decay_rates)) != BFVM_OK) return fail(rc);
   // Reference defaults: activation on, value 1.0 on every face voxel.
@@ -404,6 +406,7 @@ int bfvm_destroy(bfvm_ctx* c) {
   dfree(c, c->d_active);
   dfree(c, c->d_faces);
   dfree(c, c->d_status);
+  dfree(c, c->d_tile_counter);
   dfree(c, c->d_nvalid);
   dfree(c, c->d_line_off);
   dfree(c, c->d_sums);
@@ -958,6 +961,14 @@ extern "C" int bfvm_set_fused_sources(bfvm_ctx* c, int fused) {
   DeviceGuard g(c->device);
   BFVM_CUDA(cudaStreamSynchronize(c->stream));
   c->cfg.fuse_sources = fused;
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_set_sweep_tmem(bfvm_ctx* c, int on) {
+  if (!c || (on != 0 && on != 1)) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  c->cfg.tmem = on;
   return BFVM_OK;
 }
 

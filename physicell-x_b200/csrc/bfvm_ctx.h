@@ -33,6 +33,7 @@ struct bfvm_ctx {
   int* d_active = nullptr;
   double* d_faces = nullptr;   // xface | yface | zface
   int* d_status = nullptr;
+  unsigned long long* d_tile_counter = nullptr;  // [2] persistent TMEM y/z sweep work counter
   double* d_sums = nullptr;    // partial sums + result
   bfvm::FieldMaps maps{};
   bfvm::SweepConfig cfg{};
@@ -200,6 +201,7 @@ inline SweepParams<T> make_params(bfvm_ctx* c, bool sources) {
   }
   p.screen = c->screen;
   p.status = c->d_status;
+  p.tile_counter = c->d_tile_counter;
   return p;
 }
 

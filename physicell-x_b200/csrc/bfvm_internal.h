@@ -132,6 +132,9 @@ struct SweepParams {
   // rate (c1 >= 0, every denominator >= 1): enables the FP64 input screen.
   int screen;
   int* status;           // device status word
+  // [2] tiles handed out, CTAs finished: the persistent TMEM y/z sweep's
+  // work counter, zero between launches (its last CTA zeroes it)
+  unsigned long long* tile_counter;
 };
 
 // Launch configuration of the sweeps (chosen by the host, tunable).  A tile
@@ -157,6 +160,11 @@ struct SweepConfig {
   // ms per step), as it touches only the agents' voxels while the fused
   // path holds every x tile until all of its chunks have landed.
   int fuse_sources = 0;
+  // FP64 persistent y/z sweeps on lines of 48 to 256: 1 (default) adds four
+  // rings that keep their forward results in tensor memory next to the
+  // shared-memory rings (224 lines in flight per SM instead of 128); 0 uses
+  // shared memory alone.  Same bits either way.
+  int tmem = 1;
 };
 
 // Rows per y/z chunk of the persistent schedule (one register batch).

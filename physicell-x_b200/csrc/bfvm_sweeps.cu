@@ -1204,6 +1204,355 @@ __global__ void __launch_bounds__(64 * kMaxRings<T>, 1) sweep_yz_ring_kernel(con
   }
 }
 
+// y/z sweep, persistent, with tensor memory.  One CTA per SM of up to seven
+// rings, each one warp with no copy warp: warps 0..ns-1 (ns <= 3, as many as
+// shared memory holds) keep their tile's 16-row chunks in shared-memory slots
+// (forward results in place, as the ring above); the next four warps -- one
+// per TMEM lane quarter -- stream each chunk's input through three
+// shared-memory slots and keep the forward results in their 32 TMEM lanes
+// (32 columns per chunk, lines of at most 256).  Lane 0 of each warp issues
+// its ring's TMA loads; the back substitution writes the results straight to
+// the field (each row a coalesced 256-byte store), so a slot is free as soon
+// as the warp has read it and the next tile's chunks load into it at once.
+// Tiles are handed out by a per-solve counter (zeroed again by the launch's
+// last CTA), so rings of either kind take work as they free up.
+constexpr int kTmemRingSmem = 3;     // most shared-memory rings (warps 0..ns-1)
+constexpr int kTmemRingTmem = 4;     // TMEM rings (warps ns..ns+3), one per lane quarter
+constexpr int kTmemFlowSlots = 3;    // input slots of a TMEM ring
+constexpr int kTmemBarrierBytes = 128;
+constexpr int kTmemMaxChunks = 16;   // 16 chunks x 32 columns = the 512 TMEM columns
+
+// The shape of one y/z persistent sweep, shared by its rings.
+struct YzShape {
+  int nx, n, nm, C, ntx;
+  long long per_s, ntiles;
+  size_t row_stride;
+};
+
+// One ring of the TMEM sweep: TM = keeps its forward results in TMEM (input
+// through kTmemFlowSlots slots), else in its C shared-memory slots.  pend /
+// ppar return the loads still in flight (bit per slot, and the parity each
+// completes) when a wait gave up.
+template <int AXIS, bool TM>
+__device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const SweepParams<double>& p, const YzShape& g,
+                                             uint64_t* full, double* slots, double* cus, uint32_t tbase,
+                                             uint32_t& pend, uint32_t& ppar) {
+  using DR = double2;
+  constexpr int R = kRowBatch;
+  constexpr int CH = kRingRows;
+  constexpr int TI = 32;
+  constexpr int kSlotElems = CH * TI;
+  constexpr uint32_t kSlotBytes = kSlotElems * sizeof(double);
+  constexpr int KF = kTmemFlowSlots;
+  constexpr unsigned kAll = 0xffffffffu;
+  const int t = threadIdx.x & 31;
+  const int nx = g.nx, n = g.n, nm = g.nm, C = g.C, ntx = g.ntx;
+  const long long ntiles = g.ntiles;
+  unsigned long long* counter = p.tile_counter;
+
+  auto decode = [&](long long tile, int& i0, int& m, int& s) {
+    s = static_cast<int>(tile / g.per_s);
+    const long long r = tile - s * g.per_s;
+    m = static_cast<int>(r / ntx);
+    i0 = static_cast<int>(r - static_cast<long long>(m) * ntx) * TI;
+  };
+  // A tile whose lines all lie in an activated face is already final.
+  auto skip = [&](long long tile) {
+    int i0, m, s;
+    decode(tile, i0, m, s);
+    return p.active[s] != 0 && (m == 0 || m == nm - 1);
+  };
+  // The next tile for this ring (whole warp; ntiles when none is left).
+  auto grab = [&]() -> long long {
+    long long v = 0;
+    if (t == 0) {
+      do {
+        v = static_cast<long long>(atomicAdd(counter, 1ull));
+      } while (v < ntiles && skip(v));
+      if (v > ntiles) v = ntiles;
+    }
+    return __shfl_sync(kAll, v, 0);
+  };
+  // Chunk c of tile tl into slot sl, completing phase `par` of its barrier.
+  auto issue = [&](long long tl, int c, int sl, uint32_t par) {
+    if (t == 0) {
+      int i0, m, s;
+      decode(tl, i0, m, s);
+      const uint32_t bar = smem_u32(&full[sl]);
+      mbar_expect_tx(bar, kSlotBytes);
+      const uint32_t dst = smem_u32(slots + static_cast<size_t>(sl) * kSlotElems);
+      if (AXIS == 1)
+        tma_load_4d(dst, map, bar, i0, c * CH, m, s);
+      else
+        tma_load_4d(dst, map, bar, i0, m, c * CH, s);
+    }
+    pend |= 1u << sl;
+    ppar = (ppar & ~(1u << sl)) | (par << sl);
+  };
+
+  bool ok = true;
+  long long tile = grab();
+  if (tile < ntiles) {
+    const int first = TM ? KF : C;
+    for (int c = 0; c < first; ++c) issue(tile, c, c, 0u);
+  }
+  const int screen = p.screen;
+  int staged_s = -1;
+  int fsl = 0;        // TMEM ring: slot of the next input to consume
+  uint32_t fpar = 0;  // and the phase it completes
+  for (uint32_t k = 0; tile < ntiles; ++k) {
+    int i0, m, s;
+    decode(tile, i0, m, s);
+    const bool flip = (k & 1u) != 0;
+    const bool act = p.active[s] != 0;
+    const int i = i0 + t;
+    const bool face = act && (i == 0 || i == nx - 1);  // lines in an x face keep their (pinned) input
+    const bool lane_on = !face && i < nx;
+    const AxisCoefs<double>& ac = (AXIS == 1) ? p.ay : p.az;
+    const DR* __restrict__ drp = ac.dr + static_cast<size_t>(s) * ac.npad;
+    const double c1 = p.c1[s];
+    if (s != staged_s) {
+      stage_row(cus, ac.cu + static_cast<size_t>(s) * ac.npad, C * CH);
+      staged_s = s;
+      __syncwarp();
+    }
+    double* out = p.f + ((AXIS == 1) ? ((static_cast<size_t>(s) * p.nz + m) * p.ny) * p.nxp
+                                     : (static_cast<size_t>(s) * p.nz * p.ny + m) * p.nxp) + i;
+    DR cf[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) cf[q] = __ldg(drp + q);
+    double y = -0.0;
+    int hwmin = INT_MAX;
+    const bool edge_tile = __any_sync(kAll, !lane_on);
+    long long nxt = ntiles;
+
+    // ---- forward elimination ----
+    auto fwd_chunk = [&](bool edge, int c) {
+      const int rb = c * CH;
+      const int sl = TM ? fsl : ring_slot(flip, C, c);
+      const uint32_t par = TM ? fpar : (k & 1u);
+      if (ok) ok = mbar_wait(smem_u32(&full[sl]), par);
+      pend &= ~(1u << sl);
+      double* cb = slots + static_cast<size_t>(sl) * kSlotElems + t;
+      double yv[R];
+      if constexpr (TM) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) yv[q] = 0.0;
+      }
+      if (!edge || lane_on) {
+        double v[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
+        if (rb + R > n) {  // rows past the line's end (TMA fill): any clean value, never stored
+#pragma unroll
+          for (int q = 0; q < R; ++q)
+            if (rb + q >= n) v[q] = 1.0;
+        }
+        if constexpr (TM)
+          y = forward_bare<R>(v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
+        else
+          y = forward_bare<R>(v, cf, c1, y, [&](int q, double val) { cb[q * TI] = val; });
+        hwmin = min(hwmin, batch_min_hi<R>(v));
+      }
+      if constexpr (TM) {
+        __syncwarp();
+        tmem_st16d(tbase + 32u * c, yv);
+        __syncwarp();  // every lane has read the slot
+        // refill it with the input KF chunks on: of this tile, or the next
+        if (c == C - KF) nxt = grab();
+        const int cn = c + KF;
+        if (cn < C)
+          issue(tile, cn, sl, fpar ^ 1u);
+        else if (nxt < ntiles)
+          issue(nxt, cn - C, sl, fpar ^ 1u);
+        if (++fsl == KF) {
+          fsl = 0;
+          fpar ^= 1u;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) cf[q] = __ldg(drp + (c + 1) * R + q);
+    };
+    if (edge_tile) {
+      for (int c = 0; c < C; ++c) fwd_chunk(true, c);
+    } else {
+      for (int c = 0; c < C; ++c) fwd_chunk(false, c);
+    }
+    __syncwarp();
+    if constexpr (TM) tmem_wait_st();
+    if (!__all_sync(kAll, ok)) {
+      if (t == 0) atomicExch(p.status, kDevTimeout);
+      return;
+    }
+    // The screen, once per tile: a line with an input below 2^-960 (or
+    // negative) anywhere is redone from its inputs, which are still in the
+    // field (this tile's results are stored only by the back substitution).
+    if (__any_sync(kAll, !(screen != 0 && hwmin >= kHiTiny))) {
+      y = -0.0;
+      for (int c = 0; c < C; ++c) {
+        const int rb = c * CH;
+        double v[R];
+        DR cfr[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          v[q] = (lane_on && rb + q < n) ? out[static_cast<size_t>(rb + q) * g.row_stride] : 1.0;
+          cfr[q] = __ldg(drp + rb + q);
+        }
+        if constexpr (TM) {
+          double yv[R];
+#pragma unroll
+          for (int q = 0; q < R; ++q) yv[q] = 0.0;
+          if (lane_on) y = forward_checked<R>(v, cfr, c1, y, [&](int q, double val) { yv[q] = val; });
+          __syncwarp();
+          tmem_st16d(tbase + 32u * c, yv);
+        } else if (lane_on) {
+          double* cb = slots + static_cast<size_t>(ring_slot(flip, C, c)) * kSlotElems + t;
+          y = forward_checked<R>(v, cfr, c1, y, [&](int q, double val) { cb[q * TI] = val; });
+        }
+      }
+      __syncwarp();
+      if constexpr (TM) tmem_wait_st();
+      __syncwarp();
+    }
+    if constexpr (!TM) nxt = grab();
+
+    // ---- back substitution, last chunk first; results to the field ----
+    double xn = -0.0;
+    auto back_chunk = [&](bool edge, int c) {
+      const int rb = c * CH;
+      double v[R];
+      if constexpr (TM) {
+        __syncwarp();
+        tmem_ld16d(tbase + 32u * c, v);
+      } else {
+        const double* cb = slots + static_cast<size_t>(ring_slot(flip, C, c)) * kSlotElems + t;
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
+      }
+      if (!edge || lane_on) {
+        const double2* cwp = reinterpret_cast<const double2*>(cus + rb);  // 16-byte pairs
+        double cw[R];
+#pragma unroll
+        for (int q = 0; q < R / 2; ++q) {
+          const double2 pr = cwp[q];
+          cw[2 * q] = pr.x;
+          cw[2 * q + 1] = pr.y;
+        }
+        double* o = out + static_cast<size_t>(rb) * g.row_stride;
+        if (c == C - 1 || (act && c == 0)) {
+          // the line's end: rows past n are fill; an activated substrate's
+          // first and last rows keep their pinned input
+          const int r_lo = (act && c == 0) ? 1 : 0;
+          const int r_hi = min(R, n - rb - ((act && c == C - 1) ? 1 : 0));
+#pragma unroll
+          for (int q = R - 1; q >= 0; --q) {
+            if (rb + q < n) {
+              xn = back_elem(cw[q], xn, v[q]);
+              if (q >= r_lo && q < r_hi) o[q * g.row_stride] = xn;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int q = R - 1; q >= 0; --q) {
+            xn = back_elem(cw[q], xn, v[q]);
+            o[q * g.row_stride] = xn;
+          }
+        }
+      }
+      if constexpr (!TM) {
+        fence_async_smem();  // this lane's forward results in the slot precede the refill
+        __syncwarp();        // every lane has read the slot
+        // chunk C-1-c of the next tile takes this slot (slot order flips)
+        if (nxt < ntiles) issue(nxt, C - 1 - c, ring_slot(flip, C, c), (k + 1) & 1u);
+      }
+    };
+    if (edge_tile) {
+      for (int c = C - 1; c >= 0; --c) back_chunk(true, c);
+    } else {
+      for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
+    }
+    tile = nxt;
+  }
+}
+
+template <int AXIS>
+__global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
+    sweep_yz_tmem_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<double> p,
+                         uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes) {
+  constexpr int CH = kRingRows;
+  constexpr int TI = 32;
+  constexpr int kSlotElems = CH * TI;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 128);
+  YzShape g;
+  g.nx = p.nx;
+  g.n = (AXIS == 1) ? p.ny : p.nz;
+  g.nm = (AXIS == 1) ? p.nz : p.ny;  // the line's other coordinate (k for y, j for z)
+  g.C = (g.n + CH - 1) / CH;
+  g.ntx = (g.nx + TI - 1) / TI;
+  g.per_s = static_cast<long long>(g.ntx) * g.nm;
+  g.ntiles = g.per_s * p.S;
+  g.row_stride = (AXIS == 1) ? static_cast<size_t>(p.nxp) : static_cast<size_t>(p.nxp) * p.ny;
+  const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
+  const int ns = static_cast<int>(blockDim.x >> 5) - kTmemRingTmem;  // shared-memory rings
+  const bool tm = warp >= ns;
+  unsigned char* rbase = tm ? base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                  static_cast<size_t>(warp - ns) * tmem_ring_bytes
+                            : base + static_cast<size_t>(warp) * smem_ring_bytes;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                                    static_cast<size_t>(kTmemRingTmem) * tmem_ring_bytes);
+  const int nslots = tm ? kTmemFlowSlots : g.C;
+  uint64_t* full = reinterpret_cast<uint64_t*>(rbase);
+  double* slots = reinterpret_cast<double*>(rbase + (tm ? kTmemBarrierBytes : kBarrierBytes));
+  double* cus = slots + static_cast<size_t>(nslots) * kSlotElems;
+
+  if (t == 0) {
+    if (warp == 0) prefetch_tmap(&map);
+    for (int c = 0; c < nslots; ++c) mbar_init(smem_u32(&full[c]), 1);
+    fence_barrier_init();
+  }
+  __syncwarp();
+  if (warp == 0) {
+    tmem_alloc(smem_u32(tmem_slot), 512);
+    tmem_relinquish();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  uint32_t pend = 0, ppar = 0;
+  if (tm) {
+    tmem_fence_after();
+    const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
+    yz_tmem_ring<AXIS, true>(&map, p, g, full, slots, cus, tbase, pend, ppar);
+  } else {
+    yz_tmem_ring<AXIS, false>(&map, p, g, full, slots, cus, 0u, pend, ppar);
+  }
+
+  // Loads still in flight (only after a wait gave up) land before the CTA
+  // ends; then TMEM is released.
+  if (pend != 0) {
+    for (int sl = 0; sl < nslots; ++sl)
+      if ((pend >> sl) & 1u) mbar_wait(smem_u32(&full[sl]), (ppar >> sl) & 1u);
+  }
+  __syncwarp();
+  if (tm) {
+    tmem_wait_st();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tmem_fence_after();
+    tmem_dealloc(*tmem_slot, 512);
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned long long* counter = p.tile_counter;
+    if (atomicAdd(counter + 1, 1ull) == gridDim.x - 1) {
+      counter[0] = 0;
+      counter[1] = 0;
+    }
+  }
+}
+
 // x sweep, persistent.  Chunk c of a tile is the 128-byte column [cW, cW+W)
 // of its 32 lines (W = 128 / sizeof(T)), staged with the 128B swizzle.  Each
 // lane applies the agents of its own line chunk by chunk just before the
@@ -1790,11 +2139,58 @@ static cudaError_t launch_yz(const CUtensorMap& map, const SweepParams<T>& p, co
 // CTA per tile (measured on B200: FP64 100^3 and FP32 200^3 ran slower
 // persistent, FP64 200^3 / 400^3 and FP32 640^3 faster).
 constexpr long long kRingMinTilesPerCta = 8;
+// The TMEM sweep hands tiles out at run time, so fewer per ring still balance.
+constexpr long long kTmemMinTilesPerRing = 2;
+
+// One TMEM ring: barriers, the input slots, the staged upper-diagonal row.
+static size_t tmem_yz_ring_bytes(int n_line) {
+  const int C = (n_line + kRingRows - 1) / kRingRows;
+  return kTmemBarrierBytes + static_cast<size_t>(kTmemFlowSlots) * kRingRows * 32 * 8 +
+         static_cast<size_t>(C) * kRingRows * 8;
+}
+
+static size_t tmem_yz_smem(int n_line, int ns) {
+  // alignment pad, the rings, the TMEM address word (padded)
+  return 128 + ns * ring_yz_bytes(8, n_line) + kTmemRingTmem * tmem_yz_ring_bytes(n_line) + 128;
+}
+
+// The TMEM y/z sweep applies (FP64, lines of kTmemFlowSlots to
+// kTmemMaxChunks chunks); *ns = shared-memory rings beside the TMEM rings.
+static bool use_tmem_yz(int eb, int n_line, const SweepConfig& cfg, int* ns) {
+  const int C = (n_line + kRingRows - 1) / kRingRows;
+  if (eb != 8 || cfg.persistent < 1 || cfg.tmem == 0 || cfg.yz_tile != 32 || C < kTmemFlowSlots ||
+      C > kTmemMaxChunks)
+    return false;
+  for (int k = kTmemRingSmem; k >= 0; --k) {
+    if (tmem_yz_smem(n_line, k) <= 227 * 1024) {
+      *ns = k;
+      return true;
+    }
+  }
+  return false;
+}
 
 template <typename T, int AXIS>
 static cudaError_t launch_yz_any(const CUtensorMap& map, const CUtensorMap& ring_map, const SweepParams<T>& p,
                                  const SweepConfig& cfg, cudaStream_t st) {
   const int n = (AXIS == 1) ? p.ny : p.nz;
+  if constexpr (sizeof(T) == 8) {
+    int ns = 0;
+    if (use_tmem_yz(8, n, cfg, &ns)) {
+      const int rings = ns + kTmemRingTmem;
+      const size_t smem = tmem_yz_smem(n, ns);
+      const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * p.S;
+      int grid = 0;
+      cudaError_t e = persistent_grid(sweep_yz_tmem_kernel<AXIS>, smem, (tiles + rings - 1) / rings, &grid,
+                                      32 * rings);
+      if (e != cudaSuccess) return e;
+      if (cfg.persistent >= 2 || tiles >= kTmemMinTilesPerRing * grid * rings) {
+        sweep_yz_tmem_kernel<AXIS><<<grid, 32 * rings, smem, st>>>(
+            ring_map, p, static_cast<uint32_t>(ring_yz_bytes(8, n)), static_cast<uint32_t>(tmem_yz_ring_bytes(n)));
+        return cudaGetLastError();
+      }
+    }
+  }
   if (use_ring_yz(sizeof(T), n, cfg)) {
     const int rings = ring_yz_count(sizeof(T), n);
     const size_t smem = ring_yz_smem(sizeof(T), n);

@@ -123,7 +123,7 @@ def test_exact_division_fallbacks_bitwise(kind):
     every sweep schedule, on a small case and on one with enough tiles that
     every persistent CTA walks several."""
     rng = np.random.default_rng(4242)
-    for shape, schedules in (((23, 19, 17, 2), (0, 1, 2)), ((40, 300, 300, 1), (1, 2))):
+    for shape, schedules in (((23, 19, 17, 2), (0, 1, 2)), ((40, 300, 300, 1), (1, 2)), ((40, 200, 100, 1), (1, 2))):
         nx, ny, nz, S = shape
         wl = W.small_random(78, nx=nx, ny=ny, nz=nz, S=S, n_agents=300, steps=2, stack=True)
         wl._field0 = _screen_field(kind, wl.n_values, rng)
@@ -328,3 +328,24 @@ def test_kernel_launch_counter_moves():
     me.simulate_diffusion_decay(2, sources=True)
     me.synchronize()
     assert kernel_launches() - before >= 6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(64, 48, 40, 2), (33, 100, 57, 3), (200, 200, 120, 1), (70, 256, 130, 2),
+                                   (40, 257, 50, 1)])
+def test_tmem_sweeps_bitwise(shape):
+    """The persistent y/z sweeps with tensor-memory rings (lines of 3 to 16
+    chunks; 257 falls back to shared memory): with and without TMEM, under the
+    persistent schedules, bit for bit against the oracle, with sources,
+    faces, ragged line ends and partial x tiles."""
+    nx, ny, nz, S = shape
+    wl = W.small_random(990 + nx, nx=nx, ny=ny, nz=nz, S=S, n_agents=3000, steps=3, stack=True)
+    expect = Port.run(wl)
+    for sched, tmem in ((2, True), (1, True), (2, False)):
+        me = Microenvironment.from_workload(wl)
+        me.set_sweep_schedule(sched)
+        me.set_sweep_tmem(tmem)
+        me.simulate_diffusion_decay(wl.steps, sources=True)
+        got = me.download_field()
+        me.close()
+        assert np.array_equal(got, expect), (shape, sched, tmem)

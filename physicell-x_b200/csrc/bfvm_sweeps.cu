@@ -1273,11 +1273,10 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
     }
     return __shfl_sync(kAll, v, 0);
   };
-  // Chunk c of tile tl into slot sl, completing phase `par` of its barrier.
-  auto issue = [&](long long tl, int c, int sl, uint32_t par) {
+  // Chunk c of the tile at (i0, m, s) into slot sl, completing phase `par`
+  // of its barrier (tiles are decoded once, when taken).
+  auto issue = [&](int i0, int m, int s, int c, int sl, uint32_t par) {
     if (t == 0) {
-      int i0, m, s;
-      decode(tl, i0, m, s);
       const uint32_t bar = smem_u32(&full[sl]);
       mbar_expect_tx(bar, kSlotBytes);
       const uint32_t dst = smem_u32(slots + static_cast<size_t>(sl) * kSlotElems);
@@ -1292,17 +1291,18 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
 
   bool ok = true;
   long long tile = grab();
+  int ti0 = 0, tm_ = 0, ts = 0;  // the current tile, decoded
   if (tile < ntiles) {
+    decode(tile, ti0, tm_, ts);
     const int first = TM ? KF : C;
-    for (int c = 0; c < first; ++c) issue(tile, c, c, 0u);
+    for (int c = 0; c < first; ++c) issue(ti0, tm_, ts, c, c, 0u);
   }
   const int screen = p.screen;
   int staged_s = -1;
   int fsl = 0;        // TMEM ring: slot of the next input to consume
   uint32_t fpar = 0;  // and the phase it completes
   for (uint32_t k = 0; tile < ntiles; ++k) {
-    int i0, m, s;
-    decode(tile, i0, m, s);
+    const int i0 = ti0, m = tm_, s = ts;
     const bool flip = (k & 1u) != 0;
     const bool act = p.active[s] != 0;
     const int i = i0 + t;
@@ -1325,6 +1325,11 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
     int hwmin = INT_MAX;
     const bool edge_tile = __any_sync(kAll, !lane_on);
     long long nxt = ntiles;
+    int ni0 = 0, nm_ = 0, ns_ = 0;  // the next tile, decoded when taken
+    auto take_next = [&]() {
+      nxt = grab();
+      if (nxt < ntiles) decode(nxt, ni0, nm_, ns_);
+    };
 
     // ---- forward elimination ----
     auto fwd_chunk = [&](bool edge, int c) {
@@ -1335,10 +1340,6 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
       pend &= ~(1u << sl);
       double* cb = slots + static_cast<size_t>(sl) * kSlotElems + t;
       double yv[R];
-      if constexpr (TM) {
-#pragma unroll
-        for (int q = 0; q < R; ++q) yv[q] = 0.0;
-      }
       if (!edge || lane_on) {
         double v[R];
 #pragma unroll
@@ -1353,18 +1354,21 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
         else
           y = forward_bare<R>(v, cf, c1, y, [&](int q, double val) { cb[q * TI] = val; });
         hwmin = min(hwmin, batch_min_hi<R>(v));
+      } else if constexpr (TM) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) yv[q] = 0.0;  // lanes with no line: anything, never read
       }
       if constexpr (TM) {
         __syncwarp();
         tmem_st16d(tbase + 32u * c, yv);
         __syncwarp();  // every lane has read the slot
         // refill it with the input KF chunks on: of this tile, or the next
-        if (c == C - KF) nxt = grab();
+        if (c == C - KF) take_next();
         const int cn = c + KF;
         if (cn < C)
-          issue(tile, cn, sl, fpar ^ 1u);
+          issue(i0, m, s, cn, sl, fpar ^ 1u);
         else if (nxt < ntiles)
-          issue(nxt, cn - C, sl, fpar ^ 1u);
+          issue(ni0, nm_, ns_, cn - C, sl, fpar ^ 1u);
         if (++fsl == KF) {
           fsl = 0;
           fpar ^= 1u;
@@ -1414,16 +1418,24 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
       if constexpr (TM) tmem_wait_st();
       __syncwarp();
     }
-    if constexpr (!TM) nxt = grab();
+    if constexpr (!TM) take_next();
 
     // ---- back substitution, last chunk first; results to the field ----
     double xn = -0.0;
+    uint32_t tr[32];  // TMEM ring: the next chunk's forward results, loading
+    if constexpr (TM) {
+      __syncwarp();
+      tmem_ld32_issue(tbase + 32u * (C - 1), tr);
+    }
     auto back_chunk = [&](bool edge, int c) {
       const int rb = c * CH;
       double v[R];
       if constexpr (TM) {
         __syncwarp();
-        tmem_ld16d(tbase + 32u * c, v);
+        tmem_wait_ld32(tr);
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = __hiloint2double(static_cast<int>(tr[2 * q + 1]), static_cast<int>(tr[2 * q]));
+        if (c > 0) tmem_ld32_issue(tbase + 32u * (c - 1), tr);
       } else {
         const double* cb = slots + static_cast<size_t>(ring_slot(flip, C, c)) * kSlotElems + t;
 #pragma unroll
@@ -1463,7 +1475,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
         fence_async_smem();  // this lane's forward results in the slot precede the refill
         __syncwarp();        // every lane has read the slot
         // chunk C-1-c of the next tile takes this slot (slot order flips)
-        if (nxt < ntiles) issue(nxt, C - 1 - c, ring_slot(flip, C, c), (k + 1) & 1u);
+        if (nxt < ntiles) issue(ni0, nm_, ns_, C - 1 - c, ring_slot(flip, C, c), (k + 1) & 1u);
       }
     };
     if (edge_tile) {
@@ -1472,6 +1484,9 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
       for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
     }
     tile = nxt;
+    ti0 = ni0;
+    tm_ = nm_;
+    ts = ns_;
   }
 }
 

@@ -48,9 +48,9 @@ WORKLOAD = ("cube200: 200x200x200 voxels (dx=10 um), 4 substrates, 100000 agents
 # figures.  Keys: (precision, sweep index 0=x 1=y 2=z); the x interval is the
 # standalone source kernel plus the x sweep.
 NCU_TRAFFIC = {
-    ("fp64", 0): (56554496 + 1420800) + (268242432 + 195280384),
-    ("fp64", 1): 265725696 + 194925312,
-    ("fp64", 2): 265690112 + 195290624,
+    ("fp64", 0): (56556032 + 2542336) + (268330496 + 195878656),
+    ("fp64", 1): 266367232 + 194908928,
+    ("fp64", 2): 266125568 + 194762752,
 }
 
 

@@ -1235,7 +1235,7 @@ struct YzShape {
 // completes) when a wait gave up.
 template <int AXIS, bool TM>
 __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const SweepParams<double>& p, const YzShape& g,
-                                             uint64_t* full, double* slots, double* cus, uint32_t tbase,
+                                             int KF, uint64_t* full, double* slots, double* cus, uint32_t tbase,
                                              uint32_t& pend, uint32_t& ppar) {
   using DR = double2;
   constexpr int R = kRowBatch;
@@ -1243,7 +1243,6 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
   constexpr int TI = 32;
   constexpr int kSlotElems = CH * TI;
   constexpr uint32_t kSlotBytes = kSlotElems * sizeof(double);
-  constexpr int KF = kTmemFlowSlots;
   constexpr unsigned kAll = 0xffffffffu;
   const int t = threadIdx.x & 31;
   const int nx = g.nx, n = g.n, nm = g.nm, C = g.C, ntx = g.ntx;
@@ -1493,7 +1492,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
 template <int AXIS>
 __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
     sweep_yz_tmem_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<double> p,
-                         uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes) {
+                         uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf) {
   constexpr int CH = kRingRows;
   constexpr int TI = 32;
   constexpr int kSlotElems = CH * TI;
@@ -1516,7 +1515,7 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
                             : base + static_cast<size_t>(warp) * smem_ring_bytes;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(ns) * smem_ring_bytes +
                                                     static_cast<size_t>(kTmemRingTmem) * tmem_ring_bytes);
-  const int nslots = tm ? kTmemFlowSlots : g.C;
+  const int nslots = tm ? kf : g.C;
   uint64_t* full = reinterpret_cast<uint64_t*>(rbase);
   double* slots = reinterpret_cast<double*>(rbase + (tm ? kTmemBarrierBytes : kBarrierBytes));
   double* cus = slots + static_cast<size_t>(nslots) * kSlotElems;
@@ -1537,9 +1536,9 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   if (tm) {
     tmem_fence_after();
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
-    yz_tmem_ring<AXIS, true>(&map, p, g, full, slots, cus, tbase, pend, ppar);
+    yz_tmem_ring<AXIS, true>(&map, p, g, kf, full, slots, cus, tbase, pend, ppar);
   } else {
-    yz_tmem_ring<AXIS, false>(&map, p, g, full, slots, cus, 0u, pend, ppar);
+    yz_tmem_ring<AXIS, false>(&map, p, g, kf, full, slots, cus, 0u, pend, ppar);
   }
 
   // Loads still in flight (only after a wait gave up) land before the CTA
@@ -2157,28 +2156,32 @@ constexpr long long kRingMinTilesPerCta = 8;
 // The TMEM sweep hands tiles out at run time, so fewer per ring still balance.
 constexpr long long kTmemMinTilesPerRing = 2;
 
-// One TMEM ring: barriers, the input slots, the staged upper-diagonal row.
-static size_t tmem_yz_ring_bytes(int n_line) {
+// One TMEM ring of kf input slots: barriers, the slots, the staged
+// upper-diagonal row.
+static size_t tmem_yz_ring_bytes(int n_line, int kf) {
   const int C = (n_line + kRingRows - 1) / kRingRows;
-  return kTmemBarrierBytes + static_cast<size_t>(kTmemFlowSlots) * kRingRows * 32 * 8 +
-         static_cast<size_t>(C) * kRingRows * 8;
+  return kTmemBarrierBytes + static_cast<size_t>(kf) * kRingRows * 32 * 8 + static_cast<size_t>(C) * kRingRows * 8;
 }
 
-static size_t tmem_yz_smem(int n_line, int ns) {
+static size_t tmem_yz_smem(int n_line, int ns, int kf) {
   // alignment pad, the rings, the TMEM address word (padded)
-  return 128 + ns * ring_yz_bytes(8, n_line) + kTmemRingTmem * tmem_yz_ring_bytes(n_line) + 128;
+  return 128 + ns * ring_yz_bytes(8, n_line) + kTmemRingTmem * tmem_yz_ring_bytes(n_line, kf) + 128;
 }
 
 // The TMEM y/z sweep applies (FP64, lines of kTmemFlowSlots to
-// kTmemMaxChunks chunks); *ns = shared-memory rings beside the TMEM rings.
-static bool use_tmem_yz(int eb, int n_line, const SweepConfig& cfg, int* ns) {
+// kTmemMaxChunks chunks); *ns = shared-memory rings beside the TMEM rings (as
+// many as fit), *kf = input slots per TMEM ring.  More rings beat deeper TMEM
+// rings (cube200 y, B200: 3 + 4 rings of 3 slots 0.120 ms; 2 + 4 rings of 4,
+// 5, 6 slots 0.124, 0.127, 0.127 ms).
+static bool use_tmem_yz(int eb, int n_line, const SweepConfig& cfg, int* ns, int* kf) {
   const int C = (n_line + kRingRows - 1) / kRingRows;
   if (eb != 8 || cfg.persistent < 1 || cfg.tmem == 0 || cfg.yz_tile != 32 || C < kTmemFlowSlots ||
       C > kTmemMaxChunks)
     return false;
   for (int k = kTmemRingSmem; k >= 0; --k) {
-    if (tmem_yz_smem(n_line, k) <= 227 * 1024) {
+    if (tmem_yz_smem(n_line, k, kTmemFlowSlots) <= 227 * 1024) {
       *ns = k;
+      *kf = kTmemFlowSlots;
       return true;
     }
   }
@@ -2190,10 +2193,10 @@ static cudaError_t launch_yz_any(const CUtensorMap& map, const CUtensorMap& ring
                                  const SweepConfig& cfg, cudaStream_t st) {
   const int n = (AXIS == 1) ? p.ny : p.nz;
   if constexpr (sizeof(T) == 8) {
-    int ns = 0;
-    if (use_tmem_yz(8, n, cfg, &ns)) {
+    int ns = 0, kf = 0;
+    if (use_tmem_yz(8, n, cfg, &ns, &kf)) {
       const int rings = ns + kTmemRingTmem;
-      const size_t smem = tmem_yz_smem(n, ns);
+      const size_t smem = tmem_yz_smem(n, ns, kf);
       const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * p.S;
       int grid = 0;
       cudaError_t e = persistent_grid(sweep_yz_tmem_kernel<AXIS>, smem, (tiles + rings - 1) / rings, &grid,
@@ -2201,7 +2204,8 @@ static cudaError_t launch_yz_any(const CUtensorMap& map, const CUtensorMap& ring
       if (e != cudaSuccess) return e;
       if (cfg.persistent >= 2 || tiles >= kTmemMinTilesPerRing * grid * rings) {
         sweep_yz_tmem_kernel<AXIS><<<grid, 32 * rings, smem, st>>>(
-            ring_map, p, static_cast<uint32_t>(ring_yz_bytes(8, n)), static_cast<uint32_t>(tmem_yz_ring_bytes(n)));
+            ring_map, p, static_cast<uint32_t>(ring_yz_bytes(8, n)), static_cast<uint32_t>(tmem_yz_ring_bytes(n, kf)),
+            kf);
         return cudaGetLastError();
       }
     }

@@ -994,6 +994,7 @@ extern "C" int bfvm_set_launch(bfvm_ctx* c, int x_lines, int yz_tile, int yz_chu
   cfg.yz_chunk = yz_chunk;
   cfg.persistent = c->cfg.persistent;
   cfg.fuse_sources = c->cfg.fuse_sources;
+  cfg.tmem = c->cfg.tmem;
   // x_lines: multiple of 8 (1024-byte swizzle atoms), at most 256 (box
   // limit); yz_tile: 16 (FP64 only), 32 or 64 consecutive x -- whole 128-byte
   // rows, so every TMA chunk starts 128-byte aligned in shared memory and

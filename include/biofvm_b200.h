@@ -337,10 +337,12 @@ int bfvm_set_sweep_schedule(bfvm_ctx* ctx, int persistent);
  * tile.  Both give the same bits. */
 int bfvm_set_fused_sources(bfvm_ctx* ctx, int fused);
 int bfvm_get_sweep_schedule(bfvm_ctx* ctx, int* persistent);
-/* FP64 persistent y/z sweeps on lines of 48 to 256 voxels: on = 1 (default)
- * runs them with four extra rings that keep their forward results in the
- * SM's tensor memory (TMEM) beside the shared-memory rings; 0 uses shared
- * memory alone.  Both give the same bits. */
+/* Tensor-memory (TMEM) rings in the FP64 persistent sweeps: on = 1
+ * (default) in the y/z sweeps on lines of 48 to 256 voxels (four extra
+ * rings keep their forward results in the SM's TMEM beside the
+ * shared-memory rings); 2 also in the x sweep (lines of 32 to 256, agents
+ * not fused into it); 0 shared memory alone.  Every level gives the same
+ * bits. */
 int bfvm_set_sweep_tmem(bfvm_ctx* ctx, int on);
 
 /* Number of this library's kernels launched by the calls so far (counted on

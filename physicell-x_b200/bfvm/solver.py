@@ -318,10 +318,11 @@ class Microenvironment:
         source kernel ahead of the sweeps (False, the default)."""
         check(self.L.bfvm_set_fused_sources(self.h, 1 if fused else 0), "bfvm_set_fused_sources")
 
-    def set_sweep_tmem(self, on=True):
-        """FP64 persistent y/z sweeps with tensor-memory rings (True, the
-        default) or shared-memory rings alone (False); same bits."""
-        check(self.L.bfvm_set_sweep_tmem(self.h, 1 if on else 0), "bfvm_set_sweep_tmem")
+    def set_sweep_tmem(self, level=1):
+        """Tensor-memory rings in the FP64 persistent sweeps: 1 (the default)
+        in the y/z sweeps, 2 in the x sweep as well, 0 (or False) none; same
+        bits at every level."""
+        check(self.L.bfvm_set_sweep_tmem(self.h, int(level)), "bfvm_set_sweep_tmem")
 
     def get_sweep_schedule(self):
         v = C.c_int()

@@ -965,7 +965,7 @@ extern "C" int bfvm_set_fused_sources(bfvm_ctx* c, int fused) {
 }
 
 extern "C" int bfvm_set_sweep_tmem(bfvm_ctx* c, int on) {
-  if (!c || (on != 0 && on != 1)) return BFVM_ERR_ARG;
+  if (!c || on < 0 || on > 2) return BFVM_ERR_ARG;
   DeviceGuard g(c->device);
   BFVM_CUDA(cudaStreamSynchronize(c->stream));
   c->cfg.tmem = on;

@@ -160,10 +160,11 @@ struct SweepConfig {
   // ms per step), as it touches only the agents' voxels while the fused
   // path holds every x tile until all of its chunks have landed.
   int fuse_sources = 0;
-  // FP64 persistent y/z sweeps on lines of 48 to 256: 1 (default) adds four
-  // rings that keep their forward results in tensor memory next to the
-  // shared-memory rings (224 lines in flight per SM instead of 128); 0 uses
-  // shared memory alone.  Same bits either way.
+  // Tensor-memory rings in the FP64 persistent sweeps: 1 (default) in the
+  // y/z sweeps on lines of 48 to 256 (four rings keep their forward results
+  // in TMEM next to the shared-memory rings: 224 lines in flight per SM
+  // instead of 128); 2 also in the x sweep (lines of 32 to 256, agents not
+  // fused); 0 shared memory alone.  Same bits at every level.
   int tmem = 1;
 };
 

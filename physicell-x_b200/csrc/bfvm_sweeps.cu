@@ -1567,6 +1567,387 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   }
 }
 
+// x sweep, persistent, with tensor memory (FP64, agents in the standalone
+// source kernel, lines of 3 to 16 chunks).  The same plan as the y/z TMEM
+// sweep: one CTA per SM of ns shared-memory rings and four TMEM rings, each
+// one warp issuing its own TMA loads, tiles handed out by the per-solve
+// counter.  A tile is 32 x-lines of one (k, s); chunk c is the 128-byte
+// column [16c, 16c + 16) of the 32 lines, staged with the 128B swizzle, and
+// lane t owns line j0 + t.  A shared-memory ring stages the whole tile
+// (forward results in place); a TMEM ring streams the chunks through kf
+// input slots and keeps the forward results in its TMEM lanes.  The back
+// substitution leaves each chunk's results as 32 swizzled rows (in the slot,
+// or in the TMEM ring's staging chunk) and the warp writes them out
+// transposed: each store instruction covers two lines' 128-byte segments.
+constexpr int kXTmemBarrierBytes = 256;  // at the end of a ring
+
+// The shape of one x persistent sweep, shared by its rings.
+struct XShape {
+  int nx, ny, nz, C, ntj;
+  long long ntiles;
+};
+
+template <bool TM>
+__device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepParams<double>& p, const XShape& g,
+                                            int KF, unsigned char* slots, uint64_t* full, double* cus,
+                                            unsigned char* stage, uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
+  using DR = double2;
+  constexpr int W = 16;  // doubles per 128-byte chunk row
+  constexpr uint32_t kChunkBytes = 32u * 128u;
+  constexpr unsigned kAll = 0xffffffffu;
+  const int t = threadIdx.x & 31;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, C = g.C, ntj = g.ntj;
+  const int S = p.S;
+  const long long ntiles = g.ntiles;
+  unsigned long long* counter = p.tile_counter;
+  const int sw = t & 7;
+
+  auto decode = [&](long long tile, int& j0, int& k, int& s) {
+    const long long r = tile / ntj;
+    j0 = static_cast<int>(tile - r * ntj) * 32;
+    s = static_cast<int>(r / nz);
+    k = static_cast<int>(r - static_cast<long long>(s) * nz);
+  };
+  auto grab = [&]() -> long long {
+    long long v = 0;
+    if (t == 0) {
+      v = static_cast<long long>(atomicAdd(counter, 1ull));
+      if (v > ntiles) v = ntiles;
+    }
+    return __shfl_sync(kAll, v, 0);
+  };
+  auto issue = [&](int j0, int k, int s, int c, int sl, uint32_t par) {
+    if (t == 0) {
+      const uint32_t bar = smem_u32(&full[sl]);
+      mbar_expect_tx(bar, kChunkBytes);
+      tma_load_4d(smem_u32(slots + static_cast<size_t>(sl) * kChunkBytes), map, bar, c * W, j0, k, s);
+    }
+    pend |= 1u << sl;
+    ppar = (ppar & ~(1u << sl)) | (par << sl);
+  };
+
+  bool ok = true;
+  long long tile = grab();
+  int tj0 = 0, tk = 0, ts = 0;
+  if (tile < ntiles) {
+    decode(tile, tj0, tk, ts);
+    const int first = TM ? KF : C;
+    for (int c = 0; c < first; ++c) issue(tj0, tk, ts, c, c, 0u);
+  }
+  const int screen = p.screen;
+  int staged_s = -1;
+  int fsl = 0;
+  uint32_t fpar = 0;
+  for (uint32_t it = 0; tile < ntiles; ++it) {
+    const int j0 = tj0, k = tk, s = ts;
+    const bool flip = (it & 1u) != 0;
+    const int j = j0 + t;
+    const bool valid = j < ny;
+    const bool act = p.active[s] != 0;
+    const bool face = act && (j == 0 || j == ny - 1 || k == 0 || k == nz - 1);
+    const bool lane_on = valid && !face;
+    const DR* __restrict__ drp = p.ax.dr + static_cast<size_t>(s) * p.ax.npad;
+    const double c1 = p.c1[s];
+    if (s != staged_s) {
+      stage_row(cus, p.ax.cu + static_cast<size_t>(s) * p.ax.npad, C * W);
+      staged_s = s;
+      __syncwarp();
+    }
+    double x0v = 0.0, x1v = 0.0;
+    if (act && valid) {
+      x0v = p.xface[(static_cast<size_t>(0 * S + s) * nz + k) * ny + j];
+      x1v = p.xface[(static_cast<size_t>(1 * S + s) * nz + k) * ny + j];
+    }
+    const double* fv = nullptr;  // face lines: the face plane's row
+    if (face && valid) {
+      if (k == 0 || k == nz - 1)
+        fv = p.zface + ((static_cast<size_t>(k == 0 ? 0 : 1) * S + s) * ny + j) * nx;
+      else
+        fv = p.yface + ((static_cast<size_t>(j == 0 ? 0 : 1) * S + s) * nz + k) * nx;
+    }
+    double* plane = p.f + (static_cast<size_t>(s) * nz + k) * ny * static_cast<size_t>(p.nxp);
+    DR cf[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) cf[q] = __ldg(drp + q);
+    double y = -0.0;
+    int hwmin = INT_MAX;
+    const bool edge_tile = __any_sync(kAll, !lane_on);
+    long long nxt = ntiles;
+    int nj0 = 0, nk = 0, ns_ = 0;
+    auto take_next = [&]() {
+      nxt = grab();
+      if (nxt < ntiles) decode(nxt, nj0, nk, ns_);
+    };
+
+    // ---- forward elimination ----
+    auto fwd_chunk = [&](bool edge, int c) {
+      const int i0 = c * W;
+      const int sl = TM ? fsl : ring_slot(flip, C, c);
+      const uint32_t par = TM ? fpar : (it & 1u);
+      if (ok) ok = mbar_wait(smem_u32(&full[sl]), par);
+      pend &= ~(1u << sl);
+      unsigned char* crow = slots + static_cast<size_t>(sl) * kChunkBytes + t * 128;
+      double yv[W];
+      if (!edge || lane_on) {
+        double v[W];
+        load_row<double, W>(crow, sw, v);
+        if (act) {  // the pin before the sweep
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            if (i0 + q == 0) v[q] = x0v;
+            if (i0 + q == nx - 1) v[q] = x1v;
+          }
+        }
+        if (i0 + W > nx) {  // TMA fill past the line's end: any clean value, never stored
+#pragma unroll
+          for (int q = 0; q < W; ++q)
+            if (i0 + q >= nx) v[q] = 1.0;
+        }
+        if constexpr (TM) {
+          y = forward_bare<W>(v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
+        } else {
+          RowPut<double> put{crow, sw};
+          y = forward_bare<W>(v, cf, c1, y, put);
+        }
+        hwmin = min(hwmin, batch_min_hi<W>(v));
+      } else if constexpr (TM) {
+#pragma unroll
+        for (int q = 0; q < W; ++q) yv[q] = 0.0;  // lanes with no line: anything, never read
+      }
+      if constexpr (TM) {
+        __syncwarp();
+        tmem_st16d(tbase + 32u * c, yv);
+        __syncwarp();  // every lane has read the slot
+        if (c == C - KF) take_next();
+        const int cn = c + KF;
+        if (cn < C)
+          issue(j0, k, s, cn, sl, fpar ^ 1u);
+        else if (nxt < ntiles)
+          issue(nj0, nk, ns_, cn - C, sl, fpar ^ 1u);
+        if (++fsl == KF) {
+          fsl = 0;
+          fpar ^= 1u;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < W; ++q) cf[q] = __ldg(drp + (c + 1) * W + q);
+    };
+    if (edge_tile) {
+      for (int c = 0; c < C; ++c) fwd_chunk(true, c);
+    } else {
+      for (int c = 0; c < C; ++c) fwd_chunk(false, c);
+    }
+    __syncwarp();
+    if constexpr (TM) tmem_wait_st();
+    if (!__all_sync(kAll, ok)) {
+      if (t == 0) atomicExch(p.status, kDevTimeout);
+      return;
+    }
+    // The tile's screen: a line with an input below 2^-960 (or negative)
+    // anywhere is redone from its inputs -- the field still holds them (this
+    // tile's results are stored only by the back substitution) -- pinned as
+    // above, with every numerator checked.
+    if (__any_sync(kAll, !(screen != 0 && hwmin >= kHiTiny))) {
+      const double* src = plane + static_cast<size_t>(lane_on ? j : 0) * p.nxp;
+      y = -0.0;
+      for (int c = 0; c < C; ++c) {
+        const int i0 = c * W;
+        double v[W];
+        DR cfr[W];
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+          v[q] = (lane_on && i0 + q < nx) ? src[i0 + q] : 1.0;
+          cfr[q] = __ldg(drp + i0 + q);
+        }
+        if (act) {
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            if (i0 + q == 0) v[q] = x0v;
+            if (i0 + q == nx - 1) v[q] = x1v;
+          }
+        }
+        if constexpr (TM) {
+          double yv[W];
+#pragma unroll
+          for (int q = 0; q < W; ++q) yv[q] = 0.0;
+          if (lane_on) y = forward_checked<W>(v, cfr, c1, y, [&](int q, double val) { yv[q] = val; });
+          __syncwarp();
+          tmem_st16d(tbase + 32u * c, yv);
+        } else if (lane_on) {
+          RowPut<double> put{slots + static_cast<size_t>(ring_slot(flip, C, c)) * kChunkBytes + t * 128, sw};
+          y = forward_checked<W>(v, cfr, c1, y, put);
+        }
+      }
+      __syncwarp();
+      if constexpr (TM) tmem_wait_st();
+      __syncwarp();
+    }
+    if constexpr (!TM) take_next();
+
+    // ---- back substitution, last chunk first; results to the field ----
+    double xn = -0.0;
+    uint32_t tr[32];
+    if constexpr (TM) {
+      __syncwarp();
+      tmem_ld32_issue(tbase + 32u * (C - 1), tr);
+    }
+    auto back_chunk = [&](bool edge, int c) {
+      const int i0 = c * W;
+      unsigned char* cbase = TM ? stage : slots + static_cast<size_t>(ring_slot(flip, C, c)) * kChunkBytes;
+      unsigned char* crow = cbase + t * 128;
+      double v[W];
+      if constexpr (TM) {
+        __syncwarp();
+        tmem_wait_ld32(tr);
+#pragma unroll
+        for (int q = 0; q < W; ++q) v[q] = __hiloint2double(static_cast<int>(tr[2 * q + 1]), static_cast<int>(tr[2 * q]));
+        if (c > 0) tmem_ld32_issue(tbase + 32u * (c - 1), tr);
+      } else {
+        load_row<double, W>(crow, sw, v);
+      }
+      if (edge && face) {
+        if (fv != nullptr) {
+#pragma unroll
+          for (int q = 0; q < W; ++q) v[q] = (i0 + q < nx) ? fv[i0 + q] : 0.0;
+        }
+      } else if (!edge || valid) {
+        const double2* cwp = reinterpret_cast<const double2*>(cus + i0);  // 16-byte pairs
+        double cw[W];
+#pragma unroll
+        for (int q = 0; q < W / 2; ++q) {
+          const double2 pr = cwp[q];
+          cw[2 * q] = pr.x;
+          cw[2 * q + 1] = pr.y;
+        }
+        if (i0 + W > nx) {
+#pragma unroll
+          for (int q = W - 1; q >= 0; --q) {
+            if (i0 + q < nx) {
+              xn = back_elem(cw[q], xn, v[q]);
+              v[q] = xn;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int q = W - 1; q >= 0; --q) {
+            xn = back_elem(cw[q], xn, v[q]);
+            v[q] = xn;
+          }
+        }
+        if (act) {  // the pin after the sweep
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            if (i0 + q == 0) v[q] = x0v;
+            if (i0 + q == nx - 1) v[q] = x1v;
+          }
+        }
+      }
+      store_row<double, W>(crow, sw, v);
+      __syncwarp();
+      // out transposed: lanes 0-15 write line 2r's 16 values, 16-31 line 2r+1's
+      {
+        const int e = t & 15;
+        const int i = i0 + e;
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+          const int L = 2 * r + (t >> 4);
+          const double val = *swz_elem<double>(cbase + L * 128, e, L & 7);
+          if (j0 + L < ny && i < nx) plane[static_cast<size_t>(j0 + L) * p.nxp + i] = val;
+        }
+      }
+      if constexpr (!TM) {
+        fence_async_smem();  // this warp's writes to the slot precede the refill
+        __syncwarp();
+        if (nxt < ntiles) issue(nj0, nk, ns_, C - 1 - c, ring_slot(flip, C, c), (it + 1) & 1u);
+      } else {
+        __syncwarp();  // the staging chunk is read before the next chunk overwrites it
+      }
+    };
+    if (edge_tile) {
+      for (int c = C - 1; c >= 0; --c) back_chunk(true, c);
+    } else {
+      for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
+    }
+    tile = nxt;
+    tj0 = nj0;
+    tk = nk;
+    ts = ns_;
+  }
+}
+
+__global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
+    sweep_x_tmem_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<double> p,
+                        uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf) {
+  constexpr uint32_t kChunkBytes = 32u * 128u;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
+  XShape g;
+  g.nx = p.nx;
+  g.ny = p.ny;
+  g.nz = p.nz;
+  g.C = (g.nx + 15) / 16;
+  g.ntj = (g.ny + 31) / 32;
+  g.ntiles = static_cast<long long>(g.ntj) * g.nz * p.S;
+  const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
+  const int ns = static_cast<int>(blockDim.x >> 5) - kTmemRingTmem;
+  const bool tm = warp >= ns;
+  unsigned char* rbase = tm ? base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                  static_cast<size_t>(warp - ns) * tmem_ring_bytes
+                            : base + static_cast<size_t>(warp) * smem_ring_bytes;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                                    static_cast<size_t>(kTmemRingTmem) * tmem_ring_bytes);
+  // ring: [slots (+ staging chunk)] [upper diagonal] [barriers]
+  const int nslots = tm ? kf : g.C;
+  unsigned char* slots = rbase;
+  unsigned char* stage = tm ? rbase + static_cast<size_t>(kf) * kChunkBytes : nullptr;
+  double* cus = reinterpret_cast<double*>(rbase + static_cast<size_t>(nslots + (tm ? 1 : 0)) * kChunkBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(cus) +
+                                               static_cast<size_t>(g.C) * 16 * sizeof(double));
+
+  if (t == 0) {
+    if (warp == 0) prefetch_tmap(&map);
+    for (int c = 0; c < nslots; ++c) mbar_init(smem_u32(&full[c]), 1);
+    fence_barrier_init();
+  }
+  __syncwarp();
+  if (warp == 0) {
+    tmem_alloc(smem_u32(tmem_slot), 512);
+    tmem_relinquish();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  uint32_t pend = 0, ppar = 0;
+  if (tm) {
+    tmem_fence_after();
+    const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
+    x_tmem_ring<true>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+  } else {
+    x_tmem_ring<false>(&map, p, g, kf, slots, full, cus, nullptr, 0u, pend, ppar);
+  }
+  if (pend != 0) {
+    for (int sl = 0; sl < nslots; ++sl)
+      if ((pend >> sl) & 1u) mbar_wait(smem_u32(&full[sl]), (ppar >> sl) & 1u);
+  }
+  __syncwarp();
+  if (tm) {
+    tmem_wait_st();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tmem_fence_after();
+    tmem_dealloc(*tmem_slot, 512);
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned long long* counter = p.tile_counter;
+    if (atomicAdd(counter + 1, 1ull) == gridDim.x - 1) {
+      counter[0] = 0;
+      counter[1] = 0;
+    }
+  }
+}
+
 // x sweep, persistent.  Chunk c of a tile is the 128-byte column [cW, cW+W)
 // of its 32 lines (W = 128 / sizeof(T)), staged with the 128B swizzle.  Each
 // lane applies the agents of its own line chunk by chunk just before the
@@ -2117,8 +2498,66 @@ static bool use_ring_yz(int eb, int n, const SweepConfig& cfg) {
   return cfg.persistent >= 1 && cfg.yz_tile == 32 && ring_yz_smem(eb, n) != 0 && ring_yz_smem(eb, n) <= 227 * 1024;
 }
 
+// The TMEM sweeps hand tiles out at run time, so fewer per ring still balance.
+constexpr long long kTmemMinTilesPerRing = 2;
+
+// One ring of the TMEM x sweep (a multiple of 1024 bytes, so every chunk
+// stays on the 128B-swizzle atom): shared-memory ring = C chunks, TMEM ring
+// = kf input chunks and a staging chunk; then the upper diagonal, barriers.
+static size_t x_tmem_ring_bytes(int nx, bool tm, int kf) {
+  const int C = (nx + 15) / 16;
+  const size_t b = static_cast<size_t>(tm ? kf + 1 : C) * 32 * 128 + static_cast<size_t>(C) * 16 * 8 +
+                   kXTmemBarrierBytes;
+  return (b + 1023) / 1024 * 1024;
+}
+
+static size_t x_tmem_smem(int nx, int ns, int kf) {
+  // alignment pad, the rings, the TMEM address word
+  return 1024 + ns * x_tmem_ring_bytes(nx, false, kf) + kTmemRingTmem * x_tmem_ring_bytes(nx, true, kf) + 128;
+}
+
+// The TMEM x sweep applies (sweep TMEM level 2, FP64, agents not fused,
+// 32-line tiles, lines of 2 to kTmemMaxChunks chunks); *ns shared-memory
+// rings (as many as fit) and *kf input slots per TMEM ring.  Measured on B200
+// (x interval with the source kernel, against the per-tile x sweep): 256^3
+// 0.170 against 0.179 ms, 160^3 x 6 0.115 against 0.118, but 200^3 x 4 0.173
+// against 0.159 -- so it is not the default.
+static bool use_tmem_x(int eb, int nx, bool fused_agents, const SweepConfig& cfg, int* ns, int* kf) {
+  const int C = (nx + 15) / 16;
+  if (eb != 8 || fused_agents || cfg.persistent < 1 || cfg.tmem < 2 || cfg.x_lines != 32 || C < 2 ||
+      C > kTmemMaxChunks)
+    return false;
+  for (int k = kTmemRingSmem; k >= 0; --k) {
+    for (int f = min(C, kTmemFlowSlots); f >= 2; --f) {
+      if (x_tmem_smem(nx, k, f) <= 227 * 1024) {
+        *ns = k;
+        *kf = f;
+        return true;
+      }
+    }
+  }
+  return false;
+}
+
 template <typename T>
 cudaError_t launch_sweep_x(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
+  if constexpr (sizeof(T) == 8) {
+    int ns = 0, kf = 0;
+    if (use_tmem_x(8, p.nx, p.line_off != nullptr, cfg, &ns, &kf)) {
+      const int rings = ns + kTmemRingTmem;
+      const size_t smem = x_tmem_smem(p.nx, ns, kf);
+      const long long tiles = static_cast<long long>((p.ny + 31) / 32) * p.nz * p.S;
+      int grid = 0;
+      cudaError_t e = persistent_grid(sweep_x_tmem_kernel, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
+      if (e != cudaSuccess) return e;
+      if (cfg.persistent >= 2 || tiles >= kTmemMinTilesPerRing * grid * rings) {
+        sweep_x_tmem_kernel<<<grid, 32 * rings, smem, st>>>(
+            maps.x, p, static_cast<uint32_t>(x_tmem_ring_bytes(p.nx, false, kf)),
+            static_cast<uint32_t>(x_tmem_ring_bytes(p.nx, true, kf)), kf);
+        return cudaGetLastError();
+      }
+    }
+  }
   if (use_ring_x(sizeof(T), p.nx, cfg)) {
     const size_t smem = ring_x_smem(sizeof(T), p.nx);
     const long long tiles = static_cast<long long>((p.ny + 31) / 32) * p.nz * p.S;
@@ -2153,8 +2592,6 @@ static cudaError_t launch_yz(const CUtensorMap& map, const SweepParams<T>& p, co
 // CTA per tile (measured on B200: FP64 100^3 and FP32 200^3 ran slower
 // persistent, FP64 200^3 / 400^3 and FP32 640^3 faster).
 constexpr long long kRingMinTilesPerCta = 8;
-// The TMEM sweep hands tiles out at run time, so fewer per ring still balance.
-constexpr long long kTmemMinTilesPerRing = 2;
 
 // One TMEM ring of kf input slots: barriers, the slots, the staged
 // upper-diagonal row.

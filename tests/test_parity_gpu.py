@@ -332,16 +332,16 @@ def test_kernel_launch_counter_moves():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("shape", [(64, 48, 40, 2), (33, 100, 57, 3), (200, 200, 120, 1), (70, 256, 130, 2),
-                                   (40, 257, 50, 1)])
+                                   (40, 257, 50, 1), (256, 40, 36, 2), (20, 64, 48, 1), (257, 33, 34, 1)])
 def test_tmem_sweeps_bitwise(shape):
-    """The persistent y/z sweeps with tensor-memory rings (lines of 3 to 16
-    chunks; 257 falls back to shared memory): with and without TMEM, under the
-    persistent schedules, bit for bit against the oracle, with sources,
-    faces, ragged line ends and partial x tiles."""
+    """The persistent sweeps with tensor-memory rings (x lines of 2 to 16
+    chunks, y/z lines of 3 to 16; 257 falls back to shared memory): with and
+    without TMEM, under the persistent schedules, bit for bit against the
+    oracle, with sources, faces, ragged line ends and partial tiles."""
     nx, ny, nz, S = shape
     wl = W.small_random(990 + nx, nx=nx, ny=ny, nz=nz, S=S, n_agents=3000, steps=3, stack=True)
     expect = Port.run(wl)
-    for sched, tmem in ((2, True), (1, True), (2, False)):
+    for sched, tmem in ((2, 2), (1, 2), (1, 1), (2, 0)):
         me = Microenvironment.from_workload(wl)
         me.set_sweep_schedule(sched)
         me.set_sweep_tmem(tmem)

@@ -161,10 +161,11 @@ struct SweepConfig {
   // path holds every x tile until all of its chunks have landed.
   int fuse_sources = 0;
   // Tensor-memory rings in the FP64 persistent sweeps: 1 (default) in the
-  // y/z sweeps on lines of 48 to 256 (four rings keep their forward results
-  // in TMEM next to the shared-memory rings: 224 lines in flight per SM
-  // instead of 128); 2 also in the x sweep (lines of 32 to 256, agents not
-  // fused); 0 shared memory alone.  Same bits at every level.
+  // y/z sweeps on lines of 48 to 720 (up to four rings keep the forward
+  // results of a line's first 256 values in TMEM next to the shared-memory
+  // rings: 224 lines in flight per SM instead of 128 at lines of 200, 64
+  // instead of 32 at 640); 2 also in the x sweep (lines of 32 to 256, agents
+  // not fused); 0 shared memory alone.  Same bits at every level.
   int tmem = 1;
 };
 

@@ -1217,9 +1217,9 @@ __global__ void __launch_bounds__(64 * kMaxRings<T>, 1) sweep_yz_ring_kernel(con
 // Tiles are handed out by a per-solve counter (zeroed again by the launch's
 // last CTA), so rings of either kind take work as they free up.
 constexpr int kTmemRingSmem = 3;     // most shared-memory rings (warps 0..ns-1)
-constexpr int kTmemRingTmem = 4;     // TMEM rings (warps ns..ns+3), one per lane quarter
+constexpr int kTmemRingTmem = 4;     // most TMEM rings (warps ns..ns+nt-1), one per lane quarter
 constexpr int kTmemFlowSlots = 3;    // input slots of a TMEM ring
-constexpr int kTmemBarrierBytes = 128;
+constexpr int kTmemBarrierBytes = 256;  // up to 32 slot barriers
 constexpr int kTmemMaxChunks = 16;   // 16 chunks x 32 columns = the 512 TMEM columns
 
 // The shape of one y/z persistent sweep, shared by its rings.
@@ -1229,11 +1229,15 @@ struct YzShape {
   size_t row_stride;
 };
 
-// One ring of the TMEM sweep: TM = keeps its forward results in TMEM (input
-// through kTmemFlowSlots slots), else in its C shared-memory slots.  pend /
-// ppar return the loads still in flight (bit per slot, and the parity each
-// completes) when a wait gave up.
-template <int AXIS, bool TM>
+// One ring of the TMEM y/z sweep.  A line's first T chunks (T = min(C, 16)
+// for a TMEM ring, 0 for a shared-memory ring) stream through kf input
+// slots and keep their forward results in the ring's TMEM lanes; the other
+// C - T chunks stay resident in their own slots (forward results in place).
+// pend / ppar return the loads still in flight (bit per slot, and the parity
+// each completes) when a wait gave up.
+// MODE 0: shared-memory ring; 1: TMEM ring (C <= 16); 2: TMEM ring with
+// resident chunks (C > 16).
+template <int AXIS, int MODE>
 __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const SweepParams<double>& p, const YzShape& g,
                                              int KF, uint64_t* full, double* slots, double* cus, uint32_t tbase,
                                              uint32_t& pend, uint32_t& ppar) {
@@ -1246,6 +1250,10 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
   constexpr unsigned kAll = 0xffffffffu;
   const int t = threadIdx.x & 31;
   const int nx = g.nx, n = g.n, nm = g.nm, C = g.C, ntx = g.ntx;
+  constexpr bool TM = MODE != 0;
+  const int T = MODE == 0 ? 0 : (MODE == 1 ? C : kTmemMaxChunks);  // chunks kept in TMEM
+  const int NR = MODE == 1 ? 0 : C - T;                             // chunks resident in shared memory
+  const int RB = TM ? KF : 0;                      // first resident slot
   const long long ntiles = g.ntiles;
   unsigned long long* counter = p.tile_counter;
 
@@ -1287,18 +1295,20 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
     pend |= 1u << sl;
     ppar = (ppar & ~(1u << sl)) | (par << sl);
   };
+  // slot of resident chunk c (>= T) in tile parity `fl`
+  auto rslot = [&](bool fl, int c) { return RB + ring_slot(fl, NR, c - T); };
 
   bool ok = true;
   long long tile = grab();
   int ti0 = 0, tm_ = 0, ts = 0;  // the current tile, decoded
   if (tile < ntiles) {
     decode(tile, ti0, tm_, ts);
-    const int first = TM ? KF : C;
-    for (int c = 0; c < first; ++c) issue(ti0, tm_, ts, c, c, 0u);
+    for (int c = 0; c < (TM ? KF : 0); ++c) issue(ti0, tm_, ts, c, c, 0u);
+    for (int c = T; c < C; ++c) issue(ti0, tm_, ts, c, rslot(false, c), 0u);
   }
   const int screen = p.screen;
   int staged_s = -1;
-  int fsl = 0;        // TMEM ring: slot of the next input to consume
+  int fsl = 0;        // TMEM chunks: slot of the next input to consume
   uint32_t fpar = 0;  // and the phase it completes
   for (uint32_t k = 0; tile < ntiles; ++k) {
     const int i0 = ti0, m = tm_, s = ts;
@@ -1333,8 +1343,9 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
     // ---- forward elimination ----
     auto fwd_chunk = [&](bool edge, int c) {
       const int rb = c * CH;
-      const int sl = TM ? fsl : ring_slot(flip, C, c);
-      const uint32_t par = TM ? fpar : (k & 1u);
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
+      const int sl = flow ? fsl : rslot(flip, c);
+      const uint32_t par = flow ? fpar : (k & 1u);
       if (ok) ok = mbar_wait(smem_u32(&full[sl]), par);
       pend &= ~(1u << sl);
       double* cb = slots + static_cast<size_t>(sl) * kSlotElems + t;
@@ -1348,26 +1359,26 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
           for (int q = 0; q < R; ++q)
             if (rb + q >= n) v[q] = 1.0;
         }
-        if constexpr (TM)
+        if (flow)
           y = forward_bare<R>(v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
         else
           y = forward_bare<R>(v, cf, c1, y, [&](int q, double val) { cb[q * TI] = val; });
         hwmin = min(hwmin, batch_min_hi<R>(v));
-      } else if constexpr (TM) {
+      } else if (flow) {
 #pragma unroll
         for (int q = 0; q < R; ++q) yv[q] = 0.0;  // lanes with no line: anything, never read
       }
-      if constexpr (TM) {
+      if (flow) {
         __syncwarp();
         tmem_st16d(tbase + 32u * c, yv);
         __syncwarp();  // every lane has read the slot
         // refill it with the input KF chunks on: of this tile, or the next
-        if (c == C - KF) take_next();
+        if (c == T - KF && NR == 0) take_next();
         const int cn = c + KF;
-        if (cn < C)
+        if (cn < T)
           issue(i0, m, s, cn, sl, fpar ^ 1u);
-        else if (nxt < ntiles)
-          issue(ni0, nm_, ns_, cn - C, sl, fpar ^ 1u);
+        else if (NR == 0 && nxt < ntiles)
+          issue(ni0, nm_, ns_, cn - T, sl, fpar ^ 1u);
         if (++fsl == KF) {
           fsl = 0;
           fpar ^= 1u;
@@ -1401,7 +1412,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
           v[q] = (lane_on && rb + q < n) ? out[static_cast<size_t>(rb + q) * g.row_stride] : 1.0;
           cfr[q] = __ldg(drp + rb + q);
         }
-        if constexpr (TM) {
+        if (MODE == 1 || (MODE == 2 && c < T)) {
           double yv[R];
 #pragma unroll
           for (int q = 0; q < R; ++q) yv[q] = 0.0;
@@ -1409,7 +1420,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
           __syncwarp();
           tmem_st16d(tbase + 32u * c, yv);
         } else if (lane_on) {
-          double* cb = slots + static_cast<size_t>(ring_slot(flip, C, c)) * kSlotElems + t;
+          double* cb = slots + static_cast<size_t>(rslot(flip, c)) * kSlotElems + t;
           y = forward_checked<R>(v, cfr, c1, y, [&](int q, double val) { cb[q * TI] = val; });
         }
       }
@@ -1417,26 +1428,48 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
       if constexpr (TM) tmem_wait_st();
       __syncwarp();
     }
-    if constexpr (!TM) take_next();
+    if (NR > 0) {
+      take_next();
+      // the next tile's first inputs take the (now idle) input slots
+      if (TM && nxt < ntiles) {
+        for (int c = 0; c < KF; ++c) {
+          issue(ni0, nm_, ns_, c, fsl, fpar);
+          if (++fsl == KF) {
+            fsl = 0;
+            fpar ^= 1u;
+          }
+        }
+        // the consume cursor returns to where those loads start
+        for (int c = 0; c < KF; ++c) {
+          if (fsl == 0) {
+            fsl = KF - 1;
+            fpar ^= 1u;
+          } else {
+            --fsl;
+          }
+        }
+      }
+    }
 
     // ---- back substitution, last chunk first; results to the field ----
     double xn = -0.0;
-    uint32_t tr[32];  // TMEM ring: the next chunk's forward results, loading
+    uint32_t tr[32];  // TMEM chunks: the next chunk's forward results, loading
     if constexpr (TM) {
       __syncwarp();
-      tmem_ld32_issue(tbase + 32u * (C - 1), tr);
+      tmem_ld32_issue(tbase + 32u * (T - 1), tr);
     }
     auto back_chunk = [&](bool edge, int c) {
       const int rb = c * CH;
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
       double v[R];
-      if constexpr (TM) {
+      if (flow) {
         __syncwarp();
         tmem_wait_ld32(tr);
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = __hiloint2double(static_cast<int>(tr[2 * q + 1]), static_cast<int>(tr[2 * q]));
         if (c > 0) tmem_ld32_issue(tbase + 32u * (c - 1), tr);
       } else {
-        const double* cb = slots + static_cast<size_t>(ring_slot(flip, C, c)) * kSlotElems + t;
+        const double* cb = slots + static_cast<size_t>(rslot(flip, c)) * kSlotElems + t;
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
       }
@@ -1470,11 +1503,11 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
           }
         }
       }
-      if constexpr (!TM) {
+      if (!flow) {
         fence_async_smem();  // this lane's forward results in the slot precede the refill
         __syncwarp();        // every lane has read the slot
-        // chunk C-1-c of the next tile takes this slot (slot order flips)
-        if (nxt < ntiles) issue(ni0, nm_, ns_, C - 1 - c, ring_slot(flip, C, c), (k + 1) & 1u);
+        // the next tile's resident chunk for this slot (slot order flips)
+        if (nxt < ntiles) issue(ni0, nm_, ns_, T + (NR - 1 - (c - T)), rslot(flip, c), (k + 1) & 1u);
       }
     };
     if (edge_tile) {
@@ -1492,7 +1525,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
 template <int AXIS>
 __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
     sweep_yz_tmem_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<double> p,
-                         uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf) {
+                         uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns) {
   constexpr int CH = kRingRows;
   constexpr int TI = 32;
   constexpr int kSlotElems = CH * TI;
@@ -1508,14 +1541,14 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   g.ntiles = g.per_s * p.S;
   g.row_stride = (AXIS == 1) ? static_cast<size_t>(p.nxp) : static_cast<size_t>(p.nxp) * p.ny;
   const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
-  const int ns = static_cast<int>(blockDim.x >> 5) - kTmemRingTmem;  // shared-memory rings
+  const int nt = static_cast<int>(blockDim.x >> 5) - ns;  // TMEM rings (warps ns..ns+nt-1)
   const bool tm = warp >= ns;
   unsigned char* rbase = tm ? base + static_cast<size_t>(ns) * smem_ring_bytes +
                                   static_cast<size_t>(warp - ns) * tmem_ring_bytes
                             : base + static_cast<size_t>(warp) * smem_ring_bytes;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(ns) * smem_ring_bytes +
-                                                    static_cast<size_t>(kTmemRingTmem) * tmem_ring_bytes);
-  const int nslots = tm ? kf : g.C;
+                                                    static_cast<size_t>(nt) * tmem_ring_bytes);
+  const int nslots = tm ? kf + g.C - min(g.C, kTmemMaxChunks) : g.C;
   uint64_t* full = reinterpret_cast<uint64_t*>(rbase);
   double* slots = reinterpret_cast<double*>(rbase + (tm ? kTmemBarrierBytes : kBarrierBytes));
   double* cus = slots + static_cast<size_t>(nslots) * kSlotElems;
@@ -1536,9 +1569,12 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   if (tm) {
     tmem_fence_after();
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
-    yz_tmem_ring<AXIS, true>(&map, p, g, kf, full, slots, cus, tbase, pend, ppar);
+    if (g.C <= kTmemMaxChunks)
+      yz_tmem_ring<AXIS, 1>(&map, p, g, kf, full, slots, cus, tbase, pend, ppar);
+    else
+      yz_tmem_ring<AXIS, 2>(&map, p, g, kf, full, slots, cus, tbase, pend, ppar);
   } else {
-    yz_tmem_ring<AXIS, false>(&map, p, g, kf, full, slots, cus, 0u, pend, ppar);
+    yz_tmem_ring<AXIS, 0>(&map, p, g, kf, full, slots, cus, 0u, pend, ppar);
   }
 
   // Loads still in flight (only after a wait gave up) land before the CTA
@@ -2593,36 +2629,48 @@ static cudaError_t launch_yz(const CUtensorMap& map, const SweepParams<T>& p, co
 // persistent, FP64 200^3 / 400^3 and FP32 640^3 faster).
 constexpr long long kRingMinTilesPerCta = 8;
 
-// One TMEM ring of kf input slots: barriers, the slots, the staged
-// upper-diagonal row.
+// One TMEM ring: barriers, kf input slots plus a slot per chunk past the
+// 16 that TMEM holds, the staged upper-diagonal row.
 static size_t tmem_yz_ring_bytes(int n_line, int kf) {
   const int C = (n_line + kRingRows - 1) / kRingRows;
-  return kTmemBarrierBytes + static_cast<size_t>(kf) * kRingRows * 32 * 8 + static_cast<size_t>(C) * kRingRows * 8;
+  const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
+  return kTmemBarrierBytes + static_cast<size_t>(kf + resident) * kRingRows * 32 * 8 +
+         static_cast<size_t>(C) * kRingRows * 8;
 }
 
-static size_t tmem_yz_smem(int n_line, int ns, int kf) {
+static size_t tmem_yz_smem(int n_line, int ns, int nt, int kf) {
   // alignment pad, the rings, the TMEM address word (padded)
-  return 128 + ns * ring_yz_bytes(8, n_line) + kTmemRingTmem * tmem_yz_ring_bytes(n_line, kf) + 128;
+  return 128 + ns * ring_yz_bytes(8, n_line) + nt * tmem_yz_ring_bytes(n_line, kf) + 128;
 }
 
-// The TMEM y/z sweep applies (FP64, lines of kTmemFlowSlots to
-// kTmemMaxChunks chunks); *ns = shared-memory rings beside the TMEM rings (as
-// many as fit), *kf = input slots per TMEM ring.  More rings beat deeper TMEM
-// rings (cube200 y, B200: 3 + 4 rings of 3 slots 0.120 ms; 2 + 4 rings of 4,
-// 5, 6 slots 0.124, 0.127, 0.127 ms).
-static bool use_tmem_yz(int eb, int n_line, const SweepConfig& cfg, int* ns, int* kf) {
+// The TMEM y/z sweep applies (FP64, lines of at least kTmemFlowSlots chunks,
+// at most 32 slots per ring); *ns shared-memory rings and *nt TMEM rings (the
+// most rings that fit, TMEM rings first), *kf input slots per TMEM ring.
+// More rings beat deeper TMEM rings (cube200 y, B200: 3 + 4 rings of 3
+// slots 0.120 ms; 2 + 4 rings of 4, 5, 6 slots 0.124, 0.127, 0.127 ms).
+static bool use_tmem_yz(int eb, int n_line, const SweepConfig& cfg, int* ns, int* nt, int* kf) {
   const int C = (n_line + kRingRows - 1) / kRingRows;
-  if (eb != 8 || cfg.persistent < 1 || cfg.tmem == 0 || cfg.yz_tile != 32 || C < kTmemFlowSlots ||
-      C > kTmemMaxChunks)
-    return false;
-  for (int k = kTmemRingSmem; k >= 0; --k) {
-    if (tmem_yz_smem(n_line, k, kTmemFlowSlots) <= 227 * 1024) {
-      *ns = k;
-      *kf = kTmemFlowSlots;
-      return true;
+  if (eb != 8 || cfg.persistent < 1 || cfg.tmem == 0 || cfg.yz_tile != 32 || C < kTmemFlowSlots) return false;
+  const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
+  int best = 0;
+  for (int t = kTmemRingTmem; t >= 1; --t) {
+    for (int f = kTmemFlowSlots; f >= 2; --f) {
+      if (f + resident > 32) continue;
+      for (int k = kTmemRingSmem; k >= 0; --k) {
+        if (k > 0 && C > 32) continue;  // a shared-memory ring's barriers: one bit per slot
+        if (tmem_yz_smem(n_line, k, t, f) <= 227 * 1024) {
+          if (k + t > best) {
+            best = k + t;
+            *ns = k;
+            *nt = t;
+            *kf = f;
+          }
+          break;
+        }
+      }
     }
   }
-  return false;
+  return best > 0;
 }
 
 template <typename T, int AXIS>
@@ -2630,10 +2678,10 @@ static cudaError_t launch_yz_any(const CUtensorMap& map, const CUtensorMap& ring
                                  const SweepConfig& cfg, cudaStream_t st) {
   const int n = (AXIS == 1) ? p.ny : p.nz;
   if constexpr (sizeof(T) == 8) {
-    int ns = 0, kf = 0;
-    if (use_tmem_yz(8, n, cfg, &ns, &kf)) {
-      const int rings = ns + kTmemRingTmem;
-      const size_t smem = tmem_yz_smem(n, ns, kf);
+    int ns = 0, nt = 0, kf = 0;
+    if (use_tmem_yz(8, n, cfg, &ns, &nt, &kf)) {
+      const int rings = ns + nt;
+      const size_t smem = tmem_yz_smem(n, ns, nt, kf);
       const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * p.S;
       int grid = 0;
       cudaError_t e = persistent_grid(sweep_yz_tmem_kernel<AXIS>, smem, (tiles + rings - 1) / rings, &grid,
@@ -2642,7 +2690,7 @@ static cudaError_t launch_yz_any(const CUtensorMap& map, const CUtensorMap& ring
       if (cfg.persistent >= 2 || tiles >= kTmemMinTilesPerRing * grid * rings) {
         sweep_yz_tmem_kernel<AXIS><<<grid, 32 * rings, smem, st>>>(
             ring_map, p, static_cast<uint32_t>(ring_yz_bytes(8, n)), static_cast<uint32_t>(tmem_yz_ring_bytes(n, kf)),
-            kf);
+            kf, ns);
         return cudaGetLastError();
       }
     }

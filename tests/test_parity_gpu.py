@@ -332,12 +332,15 @@ def test_kernel_launch_counter_moves():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("shape", [(64, 48, 40, 2), (33, 100, 57, 3), (200, 200, 120, 1), (70, 256, 130, 2),
-                                   (40, 257, 50, 1), (256, 40, 36, 2), (20, 64, 48, 1), (257, 33, 34, 1)])
+                                   (40, 257, 50, 1), (256, 40, 36, 2), (20, 64, 48, 1), (257, 33, 34, 1),
+                                   (36, 400, 70, 2), (34, 40, 640, 1)])
 def test_tmem_sweeps_bitwise(shape):
     """The persistent sweeps with tensor-memory rings (x lines of 2 to 16
-    chunks, y/z lines of 3 to 16; 257 falls back to shared memory): with and
-    without TMEM, under the persistent schedules, bit for bit against the
-    oracle, with sources, faces, ragged line ends and partial tiles."""
+    chunks, falling back past 256; y/z lines of 3 to 16 chunks in TMEM and,
+    past 256, 16 in TMEM plus the rest resident in shared memory, up to 640):
+    with and without TMEM, under the persistent schedules, bit for bit
+    against the oracle, with sources, faces, ragged line ends and partial
+    tiles."""
     nx, ny, nz, S = shape
     wl = W.small_random(990 + nx, nx=nx, ny=ny, nz=nz, S=S, n_agents=3000, steps=3, stack=True)
     expect = Port.run(wl)

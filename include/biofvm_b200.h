@@ -338,11 +338,11 @@ int bfvm_set_sweep_schedule(bfvm_ctx* ctx, int persistent);
 int bfvm_set_fused_sources(bfvm_ctx* ctx, int fused);
 int bfvm_get_sweep_schedule(bfvm_ctx* ctx, int* persistent);
 /* Tensor-memory (TMEM) rings in the FP64 persistent sweeps: on = 1
- * (default) in the y/z sweeps on lines of 48 to 720 voxels (up to four extra
- * rings keep the forward results of a line's first 256 values in the SM's
- * TMEM beside the shared-memory rings); 2 also in the x sweep (lines of 32
- * to 256, agents not fused into it); 0 shared memory alone.  Every level
- * gives the same bits. */
+ * (default) in the y/z sweeps on lines of 48 to 720 voxels and in the x
+ * sweep on lines of 257 to 736 (agents not fused into it): up to four rings
+ * keep the forward results of a line's first 256 values in the SM's TMEM
+ * beside the shared-memory rings; 2 also in the x sweep on lines of 32 to
+ * 256; 0 shared memory alone.  Every level gives the same bits. */
 int bfvm_set_sweep_tmem(bfvm_ctx* ctx, int on);
 
 /* Number of this library's kernels launched by the calls so far (counted on

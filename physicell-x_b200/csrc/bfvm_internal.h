@@ -164,8 +164,9 @@ struct SweepConfig {
   // y/z sweeps on lines of 48 to 720 (up to four rings keep the forward
   // results of a line's first 256 values in TMEM next to the shared-memory
   // rings: 224 lines in flight per SM instead of 128 at lines of 200, 64
-  // instead of 32 at 640); 2 also in the x sweep (lines of 32 to 256, agents
-  // not fused); 0 shared memory alone.  Same bits at every level.
+  // instead of 32 at 640), and in the x sweep on lines of 257 to 736 (agents
+  // not fused); 2 also in the x sweep on lines of 32 to 256; 0 shared memory
+  // alone.  Same bits at every level.
   int tmem = 1;
 };
 

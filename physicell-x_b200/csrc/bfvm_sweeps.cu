@@ -1623,7 +1623,11 @@ struct XShape {
   long long ntiles;
 };
 
-template <bool TM>
+// MODE 0: shared-memory ring; 1: TMEM ring (C <= 16, its own staging
+// chunk); 2: TMEM ring with the chunks past 16 resident in shared memory (the
+// first input slot stages the TMEM chunks' results; the next tile's first
+// inputs load after the back substitution).
+template <int MODE>
 __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepParams<double>& p, const XShape& g,
                                             int KF, unsigned char* slots, uint64_t* full, double* cus,
                                             unsigned char* stage, uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
@@ -1637,6 +1641,11 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
   const long long ntiles = g.ntiles;
   unsigned long long* counter = p.tile_counter;
   const int sw = t & 7;
+  constexpr bool TM = MODE != 0;
+  const int T = MODE == 0 ? 0 : (MODE == 1 ? C : kTmemMaxChunks);  // chunks kept in TMEM
+  const int NR = MODE == 1 ? 0 : C - T;                             // chunks resident in shared memory
+  const int RB = TM ? KF : 0;                                       // first resident slot
+  auto rslot = [&](bool fl, int c) { return RB + ring_slot(fl, NR, c - T); };
 
   auto decode = [&](long long tile, int& j0, int& k, int& s) {
     const long long r = tile / ntj;
@@ -1667,8 +1676,8 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
   int tj0 = 0, tk = 0, ts = 0;
   if (tile < ntiles) {
     decode(tile, tj0, tk, ts);
-    const int first = TM ? KF : C;
-    for (int c = 0; c < first; ++c) issue(tj0, tk, ts, c, c, 0u);
+    for (int c = 0; c < (TM ? KF : 0); ++c) issue(tj0, tk, ts, c, c, 0u);
+    for (int c = T; c < C; ++c) issue(tj0, tk, ts, c, rslot(false, c), 0u);
   }
   const int screen = p.screen;
   int staged_s = -1;
@@ -1718,8 +1727,9 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
     // ---- forward elimination ----
     auto fwd_chunk = [&](bool edge, int c) {
       const int i0 = c * W;
-      const int sl = TM ? fsl : ring_slot(flip, C, c);
-      const uint32_t par = TM ? fpar : (it & 1u);
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
+      const int sl = flow ? fsl : rslot(flip, c);
+      const uint32_t par = flow ? fpar : (it & 1u);
       if (ok) ok = mbar_wait(smem_u32(&full[sl]), par);
       pend &= ~(1u << sl);
       unsigned char* crow = slots + static_cast<size_t>(sl) * kChunkBytes + t * 128;
@@ -1739,27 +1749,27 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
           for (int q = 0; q < W; ++q)
             if (i0 + q >= nx) v[q] = 1.0;
         }
-        if constexpr (TM) {
+        if (flow) {
           y = forward_bare<W>(v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
         } else {
           RowPut<double> put{crow, sw};
           y = forward_bare<W>(v, cf, c1, y, put);
         }
         hwmin = min(hwmin, batch_min_hi<W>(v));
-      } else if constexpr (TM) {
+      } else if (flow) {
 #pragma unroll
         for (int q = 0; q < W; ++q) yv[q] = 0.0;  // lanes with no line: anything, never read
       }
-      if constexpr (TM) {
+      if (flow) {
         __syncwarp();
         tmem_st16d(tbase + 32u * c, yv);
         __syncwarp();  // every lane has read the slot
-        if (c == C - KF) take_next();
+        if (MODE == 1 && c == T - KF) take_next();
         const int cn = c + KF;
-        if (cn < C)
+        if (cn < T)
           issue(j0, k, s, cn, sl, fpar ^ 1u);
-        else if (nxt < ntiles)
-          issue(nj0, nk, ns_, cn - C, sl, fpar ^ 1u);
+        else if (MODE == 1 && nxt < ntiles)
+          issue(nj0, nk, ns_, cn - T, sl, fpar ^ 1u);
         if (++fsl == KF) {
           fsl = 0;
           fpar ^= 1u;
@@ -1802,7 +1812,7 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
             if (i0 + q == nx - 1) v[q] = x1v;
           }
         }
-        if constexpr (TM) {
+        if (MODE == 1 || (MODE == 2 && c < T)) {
           double yv[W];
 #pragma unroll
           for (int q = 0; q < W; ++q) yv[q] = 0.0;
@@ -1810,7 +1820,7 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
           __syncwarp();
           tmem_st16d(tbase + 32u * c, yv);
         } else if (lane_on) {
-          RowPut<double> put{slots + static_cast<size_t>(ring_slot(flip, C, c)) * kChunkBytes + t * 128, sw};
+          RowPut<double> put{slots + static_cast<size_t>(rslot(flip, c)) * kChunkBytes + t * 128, sw};
           y = forward_checked<W>(v, cfr, c1, y, put);
         }
       }
@@ -1818,21 +1828,22 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
       if constexpr (TM) tmem_wait_st();
       __syncwarp();
     }
-    if constexpr (!TM) take_next();
+    if (MODE != 1) take_next();
 
     // ---- back substitution, last chunk first; results to the field ----
     double xn = -0.0;
     uint32_t tr[32];
     if constexpr (TM) {
       __syncwarp();
-      tmem_ld32_issue(tbase + 32u * (C - 1), tr);
+      tmem_ld32_issue(tbase + 32u * (T - 1), tr);
     }
     auto back_chunk = [&](bool edge, int c) {
       const int i0 = c * W;
-      unsigned char* cbase = TM ? stage : slots + static_cast<size_t>(ring_slot(flip, C, c)) * kChunkBytes;
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
+      unsigned char* cbase = flow ? stage : slots + static_cast<size_t>(rslot(flip, c)) * kChunkBytes;
       unsigned char* crow = cbase + t * 128;
       double v[W];
-      if constexpr (TM) {
+      if (flow) {
         __syncwarp();
         tmem_wait_ld32(tr);
 #pragma unroll
@@ -1891,10 +1902,10 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
           if (j0 + L < ny && i < nx) plane[static_cast<size_t>(j0 + L) * p.nxp + i] = val;
         }
       }
-      if constexpr (!TM) {
+      if (!flow) {
         fence_async_smem();  // this warp's writes to the slot precede the refill
         __syncwarp();
-        if (nxt < ntiles) issue(nj0, nk, ns_, C - 1 - c, ring_slot(flip, C, c), (it + 1) & 1u);
+        if (nxt < ntiles) issue(nj0, nk, ns_, T + (NR - 1 - (c - T)), rslot(flip, c), (it + 1) & 1u);
       } else {
         __syncwarp();  // the staging chunk is read before the next chunk overwrites it
       }
@@ -1903,6 +1914,27 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
       for (int c = C - 1; c >= 0; --c) back_chunk(true, c);
     } else {
       for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
+    }
+    if (MODE == 2 && nxt < ntiles) {
+      // the next tile's first inputs take the input slots (the first of
+      // which staged results just now)
+      fence_async_smem();
+      __syncwarp();
+      for (int c = 0; c < KF; ++c) {
+        issue(nj0, nk, ns_, c, fsl, fpar);
+        if (++fsl == KF) {
+          fsl = 0;
+          fpar ^= 1u;
+        }
+      }
+      for (int c = 0; c < KF; ++c) {  // the consume cursor returns to the first of them
+        if (fsl == 0) {
+          fsl = KF - 1;
+          fpar ^= 1u;
+        } else {
+          --fsl;
+        }
+      }
     }
     tile = nxt;
     tj0 = nj0;
@@ -1913,7 +1945,7 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
 
 __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
     sweep_x_tmem_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<double> p,
-                        uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf) {
+                        uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns) {
   constexpr uint32_t kChunkBytes = 32u * 128u;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
@@ -1925,18 +1957,20 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   g.ntj = (g.ny + 31) / 32;
   g.ntiles = static_cast<long long>(g.ntj) * g.nz * p.S;
   const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
-  const int ns = static_cast<int>(blockDim.x >> 5) - kTmemRingTmem;
+  const int nt = static_cast<int>(blockDim.x >> 5) - ns;  // TMEM rings (warps ns..ns+nt-1)
   const bool tm = warp >= ns;
   unsigned char* rbase = tm ? base + static_cast<size_t>(ns) * smem_ring_bytes +
                                   static_cast<size_t>(warp - ns) * tmem_ring_bytes
                             : base + static_cast<size_t>(warp) * smem_ring_bytes;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(ns) * smem_ring_bytes +
-                                                    static_cast<size_t>(kTmemRingTmem) * tmem_ring_bytes);
-  // ring: [slots (+ staging chunk)] [upper diagonal] [barriers]
-  const int nslots = tm ? kf : g.C;
+                                                    static_cast<size_t>(nt) * tmem_ring_bytes);
+  // ring: [slots (+ staging chunk)] [upper diagonal] [barriers]; a TMEM ring
+  // over more than 16 chunks stages in its first input slot
+  const bool own_stage = tm && g.C <= kTmemMaxChunks;
+  const int nslots = tm ? kf + g.C - min(g.C, kTmemMaxChunks) : g.C;
   unsigned char* slots = rbase;
-  unsigned char* stage = tm ? rbase + static_cast<size_t>(kf) * kChunkBytes : nullptr;
-  double* cus = reinterpret_cast<double*>(rbase + static_cast<size_t>(nslots + (tm ? 1 : 0)) * kChunkBytes);
+  unsigned char* stage = tm ? (own_stage ? rbase + static_cast<size_t>(nslots) * kChunkBytes : rbase) : nullptr;
+  double* cus = reinterpret_cast<double*>(rbase + static_cast<size_t>(nslots + (own_stage ? 1 : 0)) * kChunkBytes);
   uint64_t* full = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(cus) +
                                                static_cast<size_t>(g.C) * 16 * sizeof(double));
 
@@ -1956,9 +1990,12 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   if (tm) {
     tmem_fence_after();
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
-    x_tmem_ring<true>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+    if (own_stage)
+      x_tmem_ring<1>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+    else
+      x_tmem_ring<2>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
   } else {
-    x_tmem_ring<false>(&map, p, g, kf, slots, full, cus, nullptr, 0u, pend, ppar);
+    x_tmem_ring<0>(&map, p, g, kf, slots, full, cus, nullptr, 0u, pend, ppar);
   }
   if (pend != 0) {
     for (int sl = 0; sl < nslots; ++sl)
@@ -2538,50 +2575,63 @@ static bool use_ring_yz(int eb, int n, const SweepConfig& cfg) {
 constexpr long long kTmemMinTilesPerRing = 2;
 
 // One ring of the TMEM x sweep (a multiple of 1024 bytes, so every chunk
-// stays on the 128B-swizzle atom): shared-memory ring = C chunks, TMEM ring
-// = kf input chunks and a staging chunk; then the upper diagonal, barriers.
+// stays on the 128B-swizzle atom): shared-memory ring = C chunks; TMEM ring
+// = kf input chunks and a staging chunk, or, past 16 chunks, kf input chunks
+// and a resident chunk for each chunk past 16; then the upper diagonal and
+// the barriers.
 static size_t x_tmem_ring_bytes(int nx, bool tm, int kf) {
   const int C = (nx + 15) / 16;
-  const size_t b = static_cast<size_t>(tm ? kf + 1 : C) * 32 * 128 + static_cast<size_t>(C) * 16 * 8 +
-                   kXTmemBarrierBytes;
+  const int chunks = !tm ? C : (C <= kTmemMaxChunks ? kf + 1 : kf + C - kTmemMaxChunks);
+  const size_t b = static_cast<size_t>(chunks) * 32 * 128 + static_cast<size_t>(C) * 16 * 8 + kXTmemBarrierBytes;
   return (b + 1023) / 1024 * 1024;
 }
 
-static size_t x_tmem_smem(int nx, int ns, int kf) {
+static size_t x_tmem_smem(int nx, int ns, int nt, int kf) {
   // alignment pad, the rings, the TMEM address word
-  return 1024 + ns * x_tmem_ring_bytes(nx, false, kf) + kTmemRingTmem * x_tmem_ring_bytes(nx, true, kf) + 128;
+  return 1024 + ns * x_tmem_ring_bytes(nx, false, kf) + nt * x_tmem_ring_bytes(nx, true, kf) + 128;
 }
 
-// The TMEM x sweep applies (sweep TMEM level 2, FP64, agents not fused,
-// 32-line tiles, lines of 2 to kTmemMaxChunks chunks); *ns shared-memory
-// rings (as many as fit) and *kf input slots per TMEM ring.  Measured on B200
-// (x interval with the source kernel, against the per-tile x sweep): 256^3
-// 0.170 against 0.179 ms, 160^3 x 6 0.115 against 0.118, but 200^3 x 4 0.173
-// against 0.159 -- so it is not the default.
-static bool use_tmem_x(int eb, int nx, bool fused_agents, const SweepConfig& cfg, int* ns, int* kf) {
+// The TMEM x sweep applies (FP64, agents not fused, 32-line tiles, lines of
+// at least 2 chunks and at most 32 slots per ring): by default only on
+// lines past 16 chunks, where the per-tile x sweep holds 1-2 tiles per SM;
+// at sweep TMEM level 2 on every such line.  *ns shared-memory rings and *nt
+// TMEM rings (the most that fit), *kf input slots per TMEM ring.  Measured on
+// B200 against the per-tile x sweep (x interval with the source kernel):
+// 256^3 0.170 against 0.179 ms, 160^3 x 6 0.115 against 0.118, but 200^3 x 4
+// 0.173 against 0.159 -- so shorter lines keep the per-tile sweep by default.
+static bool use_tmem_x(int eb, int nx, bool fused_agents, const SweepConfig& cfg, int* ns, int* nt, int* kf) {
   const int C = (nx + 15) / 16;
-  if (eb != 8 || fused_agents || cfg.persistent < 1 || cfg.tmem < 2 || cfg.x_lines != 32 || C < 2 ||
-      C > kTmemMaxChunks)
-    return false;
-  for (int k = kTmemRingSmem; k >= 0; --k) {
+  if (eb != 8 || fused_agents || cfg.persistent < 1 || cfg.tmem == 0 || cfg.x_lines != 32 || C < 2) return false;
+  if (cfg.tmem < 2 && C <= kTmemMaxChunks) return false;
+  const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
+  int best = 0;
+  for (int t = kTmemRingTmem; t >= 1; --t) {
     for (int f = min(C, kTmemFlowSlots); f >= 2; --f) {
-      if (x_tmem_smem(nx, k, f) <= 227 * 1024) {
-        *ns = k;
-        *kf = f;
-        return true;
+      if (f + resident > 32) continue;
+      for (int k = kTmemRingSmem; k >= 0; --k) {
+        if (k > 0 && C > 32) continue;  // a shared-memory ring's barriers: one bit per slot
+        if (x_tmem_smem(nx, k, t, f) <= 227 * 1024) {
+          if (k + t > best) {
+            best = k + t;
+            *ns = k;
+            *nt = t;
+            *kf = f;
+          }
+          break;
+        }
       }
     }
   }
-  return false;
+  return best > 0;
 }
 
 template <typename T>
 cudaError_t launch_sweep_x(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
   if constexpr (sizeof(T) == 8) {
-    int ns = 0, kf = 0;
-    if (use_tmem_x(8, p.nx, p.line_off != nullptr, cfg, &ns, &kf)) {
-      const int rings = ns + kTmemRingTmem;
-      const size_t smem = x_tmem_smem(p.nx, ns, kf);
+    int ns = 0, nt = 0, kf = 0;
+    if (use_tmem_x(8, p.nx, p.line_off != nullptr, cfg, &ns, &nt, &kf)) {
+      const int rings = ns + nt;
+      const size_t smem = x_tmem_smem(p.nx, ns, nt, kf);
       const long long tiles = static_cast<long long>((p.ny + 31) / 32) * p.nz * p.S;
       int grid = 0;
       cudaError_t e = persistent_grid(sweep_x_tmem_kernel, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
@@ -2589,7 +2639,7 @@ cudaError_t launch_sweep_x(const FieldMaps& maps, const SweepParams<T>& p, const
       if (cfg.persistent >= 2 || tiles >= kTmemMinTilesPerRing * grid * rings) {
         sweep_x_tmem_kernel<<<grid, 32 * rings, smem, st>>>(
             maps.x, p, static_cast<uint32_t>(x_tmem_ring_bytes(p.nx, false, kf)),
-            static_cast<uint32_t>(x_tmem_ring_bytes(p.nx, true, kf)), kf);
+            static_cast<uint32_t>(x_tmem_ring_bytes(p.nx, true, kf)), kf, ns);
         return cudaGetLastError();
       }
     }

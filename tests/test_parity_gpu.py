@@ -120,21 +120,26 @@ def test_exact_division_fallbacks_bitwise(kind):
     """Inputs that fail the exactness screen (negative values, zeros, -0,
     subnormals, values near 2^-960) take the checked path and, where a
     numerator needs it, IEEE division: bit-identical to the oracle under
-    every sweep schedule, on a small case and on one with enough tiles that
-    every persistent CTA walks several."""
+    every sweep schedule and tensor-memory level, on a small case and on
+    ones with enough tiles that every persistent CTA walks several (lines in
+    TMEM, and past 256 partly resident in shared memory)."""
     rng = np.random.default_rng(4242)
-    for shape, schedules in (((23, 19, 17, 2), (0, 1, 2)), ((40, 300, 300, 1), (1, 2)), ((40, 200, 100, 1), (1, 2))):
+    cases = (((23, 19, 17, 2), (0, 1, 2), (1,)), ((40, 300, 300, 1), (1, 2), (1,)),
+             ((40, 200, 100, 1), (1, 2), (1, 2)), ((300, 40, 36, 1), (2,), (1,)))
+    for shape, schedules, levels in cases:
         nx, ny, nz, S = shape
         wl = W.small_random(78, nx=nx, ny=ny, nz=nz, S=S, n_agents=300, steps=2, stack=True)
         wl._field0 = _screen_field(kind, wl.n_values, rng)
         expect = Port.run(wl)
         for sched in schedules:
-            me = Microenvironment.from_workload(wl)
-            me.set_sweep_schedule(sched)
-            me.simulate_diffusion_decay(wl.steps, sources=True)
-            got = me.download_field()
-            me.close()
-            assert np.array_equal(got.view(np.int64), expect.view(np.int64)), (kind, shape, sched)
+            for level in levels:
+                me = Microenvironment.from_workload(wl)
+                me.set_sweep_schedule(sched)
+                me.set_sweep_tmem(level)
+                me.simulate_diffusion_decay(wl.steps, sources=True)
+                got = me.download_field()
+                me.close()
+                assert np.array_equal(got.view(np.int64), expect.view(np.int64)), (kind, shape, sched, level)
 
 
 def test_constants_from_rates_equal_precomputed():

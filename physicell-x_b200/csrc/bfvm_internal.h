@@ -201,6 +201,18 @@ size_t sweep_x_smem(int elem_bytes, int nx, const SweepConfig& cfg);
 size_t sweep_yz_smem(int elem_bytes, int n_line, const SweepConfig& cfg);
 size_t ring_x_smem(int elem_bytes, int nx);
 size_t ring_yz_smem(int elem_bytes, int n_line);
+// Bytes of one shared-memory ring of the persistent y/z sweeps.
+size_t ring_yz_bytes(int elem_bytes, int n_line);
+
+// The FP64 persistent sweeps with tensor-memory rings (bfvm_tmem_sweeps.cu):
+// each launches when it applies to the solve's shape and configuration and
+// sets *launched; otherwise it returns cudaSuccess with *launched false and
+// the caller runs another schedule.
+template <int AXIS>
+cudaError_t launch_tmem_yz(const CUtensorMap& ring_map, const SweepParams<double>& p, const SweepConfig& cfg,
+                           cudaStream_t st, bool* launched);
+cudaError_t launch_tmem_x(const CUtensorMap& map, const SweepParams<double>& p, const SweepConfig& cfg,
+                          cudaStream_t st, bool* launched);
 
 // ---- batched engine: one fused launch per LOD step over many solves ------
 // Tiles are 32 lines (one warp) in every sweep of a batch.

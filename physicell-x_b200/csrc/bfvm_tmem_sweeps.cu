@@ -1,0 +1,989 @@
+// bfvm_tmem_sweeps.cu -- the persistent FP64 sweeps with tensor-memory
+// (TMEM) rings, and their launches.
+//
+// Reference: the x, y and z sweeps of
+// diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING
+// (BioFVM/BioFVM_solvers.cpp:352-777, one rank) with the Dirichlet pins of
+// Microenvironment::apply_dirichlet_boundaries_conditions
+// (BioFVM/BioFVM_microenvironment.cpp:348-446), as in bfvm_sweeps.cu: same
+// operations in the same order, the same bits.
+//
+// A sweep's speed is set by how many Thomas systems (lines) an SM keeps in
+// flight, since each line's recurrence is a serial chain; a line's forward
+// results must be held until its back substitution.  Shared memory alone
+// holds 128 FP64 lines of 200 per SM.  These kernels add up to four rings
+// that keep their forward results in TMEM (one 32-lane quarter each, 512
+// 32-bit columns = 256 FP64 values per lane), so an SM holds 224 such lines.
+// TMEM is used as storage only (tcgen05.alloc / st / ld); no MMA runs.
+#include <climits>
+#include <type_traits>
+
+#include "bfvm_internal.h"
+#include "bfvm_ptx.cuh"
+#include "bfvm_sweep_common.cuh"
+
+namespace bfvm {
+
+// y/z sweep, persistent, with tensor memory.  One CTA per SM of up to seven
+// rings, each one warp with no copy warp: warps 0..ns-1 (ns <= 3, as many as
+// shared memory holds) keep their tile's 16-row chunks in shared-memory slots
+// (forward results in place, as the ring above); the next four warps -- one
+// per TMEM lane quarter -- stream each chunk's input through three
+// shared-memory slots and keep the forward results in their 32 TMEM lanes
+// (32 columns per chunk, lines of at most 256).  Lane 0 of each warp issues
+// its ring's TMA loads; the back substitution writes the results straight to
+// the field (each row a coalesced 256-byte store), so a slot is free as soon
+// as the warp has read it and the next tile's chunks load into it at once.
+// Tiles are handed out by a per-solve counter (zeroed again by the launch's
+// last CTA), so rings of either kind take work as they free up.
+constexpr int kTmemRingSmem = 3;     // most shared-memory rings (warps 0..ns-1)
+constexpr int kTmemRingTmem = 4;     // most TMEM rings (warps ns..ns+nt-1), one per lane quarter
+constexpr int kTmemFlowSlots = 3;    // input slots of a TMEM ring
+constexpr int kTmemBarrierBytes = 256;  // up to 32 slot barriers
+constexpr int kTmemMaxChunks = 16;   // 16 chunks x 32 columns = the 512 TMEM columns
+
+// The shape of one y/z persistent sweep, shared by its rings.
+struct YzShape {
+  int nx, n, nm, C, ntx;
+  long long per_s, ntiles;
+  size_t row_stride;
+};
+
+// One ring of the TMEM y/z sweep.  A line's first T chunks (T = min(C, 16)
+// for a TMEM ring, 0 for a shared-memory ring) stream through kf input
+// slots and keep their forward results in the ring's TMEM lanes; the other
+// C - T chunks stay resident in their own slots (forward results in place).
+// pend / ppar return the loads still in flight (bit per slot, and the parity
+// each completes) when a wait gave up.
+// MODE 0: shared-memory ring; 1: TMEM ring (C <= 16); 2: TMEM ring with
+// resident chunks (C > 16).
+template <int AXIS, int MODE>
+__device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const SweepParams<double>& p, const YzShape& g,
+                                             int KF, uint64_t* full, double* slots, double* cus, uint32_t tbase,
+                                             uint32_t& pend, uint32_t& ppar) {
+  using DR = double2;
+  constexpr int R = kRowBatch;
+  constexpr int CH = kRingRows;
+  constexpr int TI = 32;
+  constexpr int kSlotElems = CH * TI;
+  constexpr uint32_t kSlotBytes = kSlotElems * sizeof(double);
+  constexpr unsigned kAll = 0xffffffffu;
+  const int t = threadIdx.x & 31;
+  const int nx = g.nx, n = g.n, nm = g.nm, C = g.C, ntx = g.ntx;
+  constexpr bool TM = MODE != 0;
+  const int T = MODE == 0 ? 0 : (MODE == 1 ? C : kTmemMaxChunks);  // chunks kept in TMEM
+  const int NR = MODE == 1 ? 0 : C - T;                             // chunks resident in shared memory
+  const int RB = TM ? KF : 0;                      // first resident slot
+  const long long ntiles = g.ntiles;
+  unsigned long long* counter = p.tile_counter;
+
+  auto decode = [&](long long tile, int& i0, int& m, int& s) {
+    s = static_cast<int>(tile / g.per_s);
+    const long long r = tile - s * g.per_s;
+    m = static_cast<int>(r / ntx);
+    i0 = static_cast<int>(r - static_cast<long long>(m) * ntx) * TI;
+  };
+  // A tile whose lines all lie in an activated face is already final.
+  auto skip = [&](long long tile) {
+    int i0, m, s;
+    decode(tile, i0, m, s);
+    return p.active[s] != 0 && (m == 0 || m == nm - 1);
+  };
+  // The next tile for this ring (whole warp; ntiles when none is left).
+  auto grab = [&]() -> long long {
+    long long v = 0;
+    if (t == 0) {
+      do {
+        v = static_cast<long long>(atomicAdd(counter, 1ull));
+      } while (v < ntiles && skip(v));
+      if (v > ntiles) v = ntiles;
+    }
+    return __shfl_sync(kAll, v, 0);
+  };
+  // Chunk c of the tile at (i0, m, s) into slot sl, completing phase `par`
+  // of its barrier (tiles are decoded once, when taken).
+  auto issue = [&](int i0, int m, int s, int c, int sl, uint32_t par) {
+    if (t == 0) {
+      const uint32_t bar = smem_u32(&full[sl]);
+      mbar_expect_tx(bar, kSlotBytes);
+      const uint32_t dst = smem_u32(slots + static_cast<size_t>(sl) * kSlotElems);
+      if (AXIS == 1)
+        tma_load_4d(dst, map, bar, i0, c * CH, m, s);
+      else
+        tma_load_4d(dst, map, bar, i0, m, c * CH, s);
+    }
+    pend |= 1u << sl;
+    ppar = (ppar & ~(1u << sl)) | (par << sl);
+  };
+  // slot of resident chunk c (>= T) in tile parity `fl`
+  auto rslot = [&](bool fl, int c) { return RB + ring_slot(fl, NR, c - T); };
+
+  bool ok = true;
+  long long tile = grab();
+  int ti0 = 0, tm_ = 0, ts = 0;  // the current tile, decoded
+  if (tile < ntiles) {
+    decode(tile, ti0, tm_, ts);
+    for (int c = 0; c < (TM ? KF : 0); ++c) issue(ti0, tm_, ts, c, c, 0u);
+    for (int c = T; c < C; ++c) issue(ti0, tm_, ts, c, rslot(false, c), 0u);
+  }
+  const int screen = p.screen;
+  int staged_s = -1;
+  int fsl = 0;        // TMEM chunks: slot of the next input to consume
+  uint32_t fpar = 0;  // and the phase it completes
+  for (uint32_t k = 0; tile < ntiles; ++k) {
+    const int i0 = ti0, m = tm_, s = ts;
+    const bool flip = (k & 1u) != 0;
+    const bool act = p.active[s] != 0;
+    const int i = i0 + t;
+    const bool face = act && (i == 0 || i == nx - 1);  // lines in an x face keep their (pinned) input
+    const bool lane_on = !face && i < nx;
+    const AxisCoefs<double>& ac = (AXIS == 1) ? p.ay : p.az;
+    const DR* __restrict__ drp = ac.dr + static_cast<size_t>(s) * ac.npad;
+    const double c1 = p.c1[s];
+    if (s != staged_s) {
+      stage_row(cus, ac.cu + static_cast<size_t>(s) * ac.npad, C * CH);
+      staged_s = s;
+      __syncwarp();
+    }
+    double* out = p.f + ((AXIS == 1) ? ((static_cast<size_t>(s) * p.nz + m) * p.ny) * p.nxp
+                                     : (static_cast<size_t>(s) * p.nz * p.ny + m) * p.nxp) + i;
+    DR cf[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) cf[q] = __ldg(drp + q);
+    double y = -0.0;
+    int hwmin = INT_MAX;
+    const bool edge_tile = __any_sync(kAll, !lane_on);
+    long long nxt = ntiles;
+    int ni0 = 0, nm_ = 0, ns_ = 0;  // the next tile, decoded when taken
+    auto take_next = [&]() {
+      nxt = grab();
+      if (nxt < ntiles) decode(nxt, ni0, nm_, ns_);
+    };
+
+    // ---- forward elimination ----
+    auto fwd_chunk = [&](bool edge, int c) {
+      const int rb = c * CH;
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
+      const int sl = flow ? fsl : rslot(flip, c);
+      const uint32_t par = flow ? fpar : (k & 1u);
+      if (ok) ok = mbar_wait(smem_u32(&full[sl]), par);
+      pend &= ~(1u << sl);
+      double* cb = slots + static_cast<size_t>(sl) * kSlotElems + t;
+      double yv[R];
+      if (!edge || lane_on) {
+        double v[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
+        if (rb + R > n) {  // rows past the line's end (TMA fill): any clean value, never stored
+#pragma unroll
+          for (int q = 0; q < R; ++q)
+            if (rb + q >= n) v[q] = 1.0;
+        }
+        if (flow)
+          y = forward_bare<R>(v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
+        else
+          y = forward_bare<R>(v, cf, c1, y, [&](int q, double val) { cb[q * TI] = val; });
+        hwmin = min(hwmin, batch_min_hi<R>(v));
+      } else if (flow) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) yv[q] = 0.0;  // lanes with no line: anything, never read
+      }
+      if (flow) {
+        __syncwarp();
+        tmem_st16d(tbase + 32u * c, yv);
+        __syncwarp();  // every lane has read the slot
+        // refill it with the input KF chunks on: of this tile, or the next
+        if (c == T - KF && NR == 0) take_next();
+        const int cn = c + KF;
+        if (cn < T)
+          issue(i0, m, s, cn, sl, fpar ^ 1u);
+        else if (NR == 0 && nxt < ntiles)
+          issue(ni0, nm_, ns_, cn - T, sl, fpar ^ 1u);
+        if (++fsl == KF) {
+          fsl = 0;
+          fpar ^= 1u;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) cf[q] = __ldg(drp + (c + 1) * R + q);
+    };
+    if (edge_tile) {
+      for (int c = 0; c < C; ++c) fwd_chunk(true, c);
+    } else {
+      for (int c = 0; c < C; ++c) fwd_chunk(false, c);
+    }
+    __syncwarp();
+    if constexpr (TM) tmem_wait_st();
+    if (!__all_sync(kAll, ok)) {
+      if (t == 0) atomicExch(p.status, kDevTimeout);
+      return;
+    }
+    // The screen, once per tile: a line with an input below 2^-960 (or
+    // negative) anywhere is redone from its inputs, which are still in the
+    // field (this tile's results are stored only by the back substitution).
+    if (__any_sync(kAll, !(screen != 0 && hwmin >= kHiTiny))) {
+      y = -0.0;
+      for (int c = 0; c < C; ++c) {
+        const int rb = c * CH;
+        double v[R];
+        DR cfr[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          v[q] = (lane_on && rb + q < n) ? out[static_cast<size_t>(rb + q) * g.row_stride] : 1.0;
+          cfr[q] = __ldg(drp + rb + q);
+        }
+        if (MODE == 1 || (MODE == 2 && c < T)) {
+          double yv[R];
+#pragma unroll
+          for (int q = 0; q < R; ++q) yv[q] = 0.0;
+          if (lane_on) y = forward_checked<R>(v, cfr, c1, y, [&](int q, double val) { yv[q] = val; });
+          __syncwarp();
+          tmem_st16d(tbase + 32u * c, yv);
+        } else if (lane_on) {
+          double* cb = slots + static_cast<size_t>(rslot(flip, c)) * kSlotElems + t;
+          y = forward_checked<R>(v, cfr, c1, y, [&](int q, double val) { cb[q * TI] = val; });
+        }
+      }
+      __syncwarp();
+      if constexpr (TM) tmem_wait_st();
+      __syncwarp();
+    }
+    if (NR > 0) {
+      take_next();
+      // the next tile's first inputs take the (now idle) input slots
+      if (TM && nxt < ntiles) {
+        for (int c = 0; c < KF; ++c) {
+          issue(ni0, nm_, ns_, c, fsl, fpar);
+          if (++fsl == KF) {
+            fsl = 0;
+            fpar ^= 1u;
+          }
+        }
+        // the consume cursor returns to where those loads start
+        for (int c = 0; c < KF; ++c) {
+          if (fsl == 0) {
+            fsl = KF - 1;
+            fpar ^= 1u;
+          } else {
+            --fsl;
+          }
+        }
+      }
+    }
+
+    // ---- back substitution, last chunk first; results to the field ----
+    double xn = -0.0;
+    uint32_t tr[32];  // TMEM chunks: the next chunk's forward results, loading
+    if constexpr (TM) {
+      __syncwarp();
+      tmem_ld32_issue(tbase + 32u * (T - 1), tr);
+    }
+    auto back_chunk = [&](bool edge, int c) {
+      const int rb = c * CH;
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
+      double v[R];
+      if (flow) {
+        __syncwarp();
+        tmem_wait_ld32(tr);
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = __hiloint2double(static_cast<int>(tr[2 * q + 1]), static_cast<int>(tr[2 * q]));
+        if (c > 0) tmem_ld32_issue(tbase + 32u * (c - 1), tr);
+      } else {
+        const double* cb = slots + static_cast<size_t>(rslot(flip, c)) * kSlotElems + t;
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
+      }
+      if (!edge || lane_on) {
+        const double2* cwp = reinterpret_cast<const double2*>(cus + rb);  // 16-byte pairs
+        double cw[R];
+#pragma unroll
+        for (int q = 0; q < R / 2; ++q) {
+          const double2 pr = cwp[q];
+          cw[2 * q] = pr.x;
+          cw[2 * q + 1] = pr.y;
+        }
+        double* o = out + static_cast<size_t>(rb) * g.row_stride;
+        if (c == C - 1 || (act && c == 0)) {
+          // the line's end: rows past n are fill; an activated substrate's
+          // first and last rows keep their pinned input
+          const int r_lo = (act && c == 0) ? 1 : 0;
+          const int r_hi = min(R, n - rb - ((act && c == C - 1) ? 1 : 0));
+#pragma unroll
+          for (int q = R - 1; q >= 0; --q) {
+            if (rb + q < n) {
+              xn = back_elem(cw[q], xn, v[q]);
+              if (q >= r_lo && q < r_hi) o[q * g.row_stride] = xn;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int q = R - 1; q >= 0; --q) {
+            xn = back_elem(cw[q], xn, v[q]);
+            o[q * g.row_stride] = xn;
+          }
+        }
+      }
+      if (!flow) {
+        fence_async_smem();  // this lane's forward results in the slot precede the refill
+        __syncwarp();        // every lane has read the slot
+        // the next tile's resident chunk for this slot (slot order flips)
+        if (nxt < ntiles) issue(ni0, nm_, ns_, T + (NR - 1 - (c - T)), rslot(flip, c), (k + 1) & 1u);
+      }
+    };
+    if (edge_tile) {
+      for (int c = C - 1; c >= 0; --c) back_chunk(true, c);
+    } else {
+      for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
+    }
+    tile = nxt;
+    ti0 = ni0;
+    tm_ = nm_;
+    ts = ns_;
+  }
+}
+
+template <int AXIS>
+__global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
+    sweep_yz_tmem_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<double> p,
+                         uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns) {
+  constexpr int CH = kRingRows;
+  constexpr int TI = 32;
+  constexpr int kSlotElems = CH * TI;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 128);
+  YzShape g;
+  g.nx = p.nx;
+  g.n = (AXIS == 1) ? p.ny : p.nz;
+  g.nm = (AXIS == 1) ? p.nz : p.ny;  // the line's other coordinate (k for y, j for z)
+  g.C = (g.n + CH - 1) / CH;
+  g.ntx = (g.nx + TI - 1) / TI;
+  g.per_s = static_cast<long long>(g.ntx) * g.nm;
+  g.ntiles = g.per_s * p.S;
+  g.row_stride = (AXIS == 1) ? static_cast<size_t>(p.nxp) : static_cast<size_t>(p.nxp) * p.ny;
+  const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
+  const int nt = static_cast<int>(blockDim.x >> 5) - ns;  // TMEM rings (warps ns..ns+nt-1)
+  const bool tm = warp >= ns;
+  unsigned char* rbase = tm ? base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                  static_cast<size_t>(warp - ns) * tmem_ring_bytes
+                            : base + static_cast<size_t>(warp) * smem_ring_bytes;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                                    static_cast<size_t>(nt) * tmem_ring_bytes);
+  const int nslots = tm ? kf + g.C - min(g.C, kTmemMaxChunks) : g.C;
+  uint64_t* full = reinterpret_cast<uint64_t*>(rbase);
+  double* slots = reinterpret_cast<double*>(rbase + (tm ? kTmemBarrierBytes : kBarrierBytes));
+  double* cus = slots + static_cast<size_t>(nslots) * kSlotElems;
+
+  if (t == 0) {
+    if (warp == 0) prefetch_tmap(&map);
+    for (int c = 0; c < nslots; ++c) mbar_init(smem_u32(&full[c]), 1);
+    fence_barrier_init();
+  }
+  __syncwarp();
+  if (warp == 0) {
+    tmem_alloc(smem_u32(tmem_slot), 512);
+    tmem_relinquish();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  uint32_t pend = 0, ppar = 0;
+  if (tm) {
+    tmem_fence_after();
+    const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
+    if (g.C <= kTmemMaxChunks)
+      yz_tmem_ring<AXIS, 1>(&map, p, g, kf, full, slots, cus, tbase, pend, ppar);
+    else
+      yz_tmem_ring<AXIS, 2>(&map, p, g, kf, full, slots, cus, tbase, pend, ppar);
+  } else {
+    yz_tmem_ring<AXIS, 0>(&map, p, g, kf, full, slots, cus, 0u, pend, ppar);
+  }
+
+  // Loads still in flight (only after a wait gave up) land before the CTA
+  // ends; then TMEM is released.
+  if (pend != 0) {
+    for (int sl = 0; sl < nslots; ++sl)
+      if ((pend >> sl) & 1u) mbar_wait(smem_u32(&full[sl]), (ppar >> sl) & 1u);
+  }
+  __syncwarp();
+  if (tm) {
+    tmem_wait_st();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tmem_fence_after();
+    tmem_dealloc(*tmem_slot, 512);
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned long long* counter = p.tile_counter;
+    if (atomicAdd(counter + 1, 1ull) == gridDim.x - 1) {
+      counter[0] = 0;
+      counter[1] = 0;
+    }
+  }
+}
+
+// x sweep, persistent, with tensor memory (FP64, agents in the standalone
+// source kernel, lines of 3 to 16 chunks).  The same plan as the y/z TMEM
+// sweep: one CTA per SM of ns shared-memory rings and four TMEM rings, each
+// one warp issuing its own TMA loads, tiles handed out by the per-solve
+// counter.  A tile is 32 x-lines of one (k, s); chunk c is the 128-byte
+// column [16c, 16c + 16) of the 32 lines, staged with the 128B swizzle, and
+// lane t owns line j0 + t.  A shared-memory ring stages the whole tile
+// (forward results in place); a TMEM ring streams the chunks through kf
+// input slots and keeps the forward results in its TMEM lanes.  The back
+// substitution leaves each chunk's results as 32 swizzled rows (in the slot,
+// or in the TMEM ring's staging chunk) and the warp writes them out
+// transposed: each store instruction covers two lines' 128-byte segments.
+constexpr int kXTmemBarrierBytes = 256;  // at the end of a ring
+
+// The shape of one x persistent sweep, shared by its rings.
+struct XShape {
+  int nx, ny, nz, C, ntj;
+  long long ntiles;
+};
+
+// MODE 0: shared-memory ring; 1: TMEM ring (C <= 16, its own staging
+// chunk); 2: TMEM ring with the chunks past 16 resident in shared memory (the
+// first input slot stages the TMEM chunks' results; the next tile's first
+// inputs load after the back substitution).
+template <int MODE>
+__device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepParams<double>& p, const XShape& g,
+                                            int KF, unsigned char* slots, uint64_t* full, double* cus,
+                                            unsigned char* stage, uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
+  using DR = double2;
+  constexpr int W = 16;  // doubles per 128-byte chunk row
+  constexpr uint32_t kChunkBytes = 32u * 128u;
+  constexpr unsigned kAll = 0xffffffffu;
+  const int t = threadIdx.x & 31;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, C = g.C, ntj = g.ntj;
+  const int S = p.S;
+  const long long ntiles = g.ntiles;
+  unsigned long long* counter = p.tile_counter;
+  const int sw = t & 7;
+  constexpr bool TM = MODE != 0;
+  const int T = MODE == 0 ? 0 : (MODE == 1 ? C : kTmemMaxChunks);  // chunks kept in TMEM
+  const int NR = MODE == 1 ? 0 : C - T;                             // chunks resident in shared memory
+  const int RB = TM ? KF : 0;                                       // first resident slot
+  auto rslot = [&](bool fl, int c) { return RB + ring_slot(fl, NR, c - T); };
+
+  auto decode = [&](long long tile, int& j0, int& k, int& s) {
+    const long long r = tile / ntj;
+    j0 = static_cast<int>(tile - r * ntj) * 32;
+    s = static_cast<int>(r / nz);
+    k = static_cast<int>(r - static_cast<long long>(s) * nz);
+  };
+  auto grab = [&]() -> long long {
+    long long v = 0;
+    if (t == 0) {
+      v = static_cast<long long>(atomicAdd(counter, 1ull));
+      if (v > ntiles) v = ntiles;
+    }
+    return __shfl_sync(kAll, v, 0);
+  };
+  auto issue = [&](int j0, int k, int s, int c, int sl, uint32_t par) {
+    if (t == 0) {
+      const uint32_t bar = smem_u32(&full[sl]);
+      mbar_expect_tx(bar, kChunkBytes);
+      tma_load_4d(smem_u32(slots + static_cast<size_t>(sl) * kChunkBytes), map, bar, c * W, j0, k, s);
+    }
+    pend |= 1u << sl;
+    ppar = (ppar & ~(1u << sl)) | (par << sl);
+  };
+
+  bool ok = true;
+  long long tile = grab();
+  int tj0 = 0, tk = 0, ts = 0;
+  if (tile < ntiles) {
+    decode(tile, tj0, tk, ts);
+    for (int c = 0; c < (TM ? KF : 0); ++c) issue(tj0, tk, ts, c, c, 0u);
+    for (int c = T; c < C; ++c) issue(tj0, tk, ts, c, rslot(false, c), 0u);
+  }
+  const int screen = p.screen;
+  int staged_s = -1;
+  int fsl = 0;
+  uint32_t fpar = 0;
+  for (uint32_t it = 0; tile < ntiles; ++it) {
+    const int j0 = tj0, k = tk, s = ts;
+    const bool flip = (it & 1u) != 0;
+    const int j = j0 + t;
+    const bool valid = j < ny;
+    const bool act = p.active[s] != 0;
+    const bool face = act && (j == 0 || j == ny - 1 || k == 0 || k == nz - 1);
+    const bool lane_on = valid && !face;
+    const DR* __restrict__ drp = p.ax.dr + static_cast<size_t>(s) * p.ax.npad;
+    const double c1 = p.c1[s];
+    if (s != staged_s) {
+      stage_row(cus, p.ax.cu + static_cast<size_t>(s) * p.ax.npad, C * W);
+      staged_s = s;
+      __syncwarp();
+    }
+    double x0v = 0.0, x1v = 0.0;
+    if (act && valid) {
+      x0v = p.xface[(static_cast<size_t>(0 * S + s) * nz + k) * ny + j];
+      x1v = p.xface[(static_cast<size_t>(1 * S + s) * nz + k) * ny + j];
+    }
+    const double* fv = nullptr;  // face lines: the face plane's row
+    if (face && valid) {
+      if (k == 0 || k == nz - 1)
+        fv = p.zface + ((static_cast<size_t>(k == 0 ? 0 : 1) * S + s) * ny + j) * nx;
+      else
+        fv = p.yface + ((static_cast<size_t>(j == 0 ? 0 : 1) * S + s) * nz + k) * nx;
+    }
+    double* plane = p.f + (static_cast<size_t>(s) * nz + k) * ny * static_cast<size_t>(p.nxp);
+    DR cf[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) cf[q] = __ldg(drp + q);
+    double y = -0.0;
+    int hwmin = INT_MAX;
+    const bool edge_tile = __any_sync(kAll, !lane_on);
+    long long nxt = ntiles;
+    int nj0 = 0, nk = 0, ns_ = 0;
+    auto take_next = [&]() {
+      nxt = grab();
+      if (nxt < ntiles) decode(nxt, nj0, nk, ns_);
+    };
+
+    // ---- forward elimination ----
+    auto fwd_chunk = [&](bool edge, int c) {
+      const int i0 = c * W;
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
+      const int sl = flow ? fsl : rslot(flip, c);
+      const uint32_t par = flow ? fpar : (it & 1u);
+      if (ok) ok = mbar_wait(smem_u32(&full[sl]), par);
+      pend &= ~(1u << sl);
+      unsigned char* crow = slots + static_cast<size_t>(sl) * kChunkBytes + t * 128;
+      double yv[W];
+      if (!edge || lane_on) {
+        double v[W];
+        load_row<double, W>(crow, sw, v);
+        if (act) {  // the pin before the sweep
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            if (i0 + q == 0) v[q] = x0v;
+            if (i0 + q == nx - 1) v[q] = x1v;
+          }
+        }
+        if (i0 + W > nx) {  // TMA fill past the line's end: any clean value, never stored
+#pragma unroll
+          for (int q = 0; q < W; ++q)
+            if (i0 + q >= nx) v[q] = 1.0;
+        }
+        if (flow) {
+          y = forward_bare<W>(v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
+        } else {
+          RowPut<double> put{crow, sw};
+          y = forward_bare<W>(v, cf, c1, y, put);
+        }
+        hwmin = min(hwmin, batch_min_hi<W>(v));
+      } else if (flow) {
+#pragma unroll
+        for (int q = 0; q < W; ++q) yv[q] = 0.0;  // lanes with no line: anything, never read
+      }
+      if (flow) {
+        __syncwarp();
+        tmem_st16d(tbase + 32u * c, yv);
+        __syncwarp();  // every lane has read the slot
+        if (MODE == 1 && c == T - KF) take_next();
+        const int cn = c + KF;
+        if (cn < T)
+          issue(j0, k, s, cn, sl, fpar ^ 1u);
+        else if (MODE == 1 && nxt < ntiles)
+          issue(nj0, nk, ns_, cn - T, sl, fpar ^ 1u);
+        if (++fsl == KF) {
+          fsl = 0;
+          fpar ^= 1u;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < W; ++q) cf[q] = __ldg(drp + (c + 1) * W + q);
+    };
+    if (edge_tile) {
+      for (int c = 0; c < C; ++c) fwd_chunk(true, c);
+    } else {
+      for (int c = 0; c < C; ++c) fwd_chunk(false, c);
+    }
+    __syncwarp();
+    if constexpr (TM) tmem_wait_st();
+    if (!__all_sync(kAll, ok)) {
+      if (t == 0) atomicExch(p.status, kDevTimeout);
+      return;
+    }
+    // The tile's screen: a line with an input below 2^-960 (or negative)
+    // anywhere is redone from its inputs -- the field still holds them (this
+    // tile's results are stored only by the back substitution) -- pinned as
+    // above, with every numerator checked.
+    if (__any_sync(kAll, !(screen != 0 && hwmin >= kHiTiny))) {
+      const double* src = plane + static_cast<size_t>(lane_on ? j : 0) * p.nxp;
+      y = -0.0;
+      for (int c = 0; c < C; ++c) {
+        const int i0 = c * W;
+        double v[W];
+        DR cfr[W];
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+          v[q] = (lane_on && i0 + q < nx) ? src[i0 + q] : 1.0;
+          cfr[q] = __ldg(drp + i0 + q);
+        }
+        if (act) {
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            if (i0 + q == 0) v[q] = x0v;
+            if (i0 + q == nx - 1) v[q] = x1v;
+          }
+        }
+        if (MODE == 1 || (MODE == 2 && c < T)) {
+          double yv[W];
+#pragma unroll
+          for (int q = 0; q < W; ++q) yv[q] = 0.0;
+          if (lane_on) y = forward_checked<W>(v, cfr, c1, y, [&](int q, double val) { yv[q] = val; });
+          __syncwarp();
+          tmem_st16d(tbase + 32u * c, yv);
+        } else if (lane_on) {
+          RowPut<double> put{slots + static_cast<size_t>(rslot(flip, c)) * kChunkBytes + t * 128, sw};
+          y = forward_checked<W>(v, cfr, c1, y, put);
+        }
+      }
+      __syncwarp();
+      if constexpr (TM) tmem_wait_st();
+      __syncwarp();
+    }
+    if (MODE != 1) take_next();
+
+    // ---- back substitution, last chunk first; results to the field ----
+    double xn = -0.0;
+    uint32_t tr[32];
+    if constexpr (TM) {
+      __syncwarp();
+      tmem_ld32_issue(tbase + 32u * (T - 1), tr);
+    }
+    auto back_chunk = [&](bool edge, int c) {
+      const int i0 = c * W;
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
+      unsigned char* cbase = flow ? stage : slots + static_cast<size_t>(rslot(flip, c)) * kChunkBytes;
+      unsigned char* crow = cbase + t * 128;
+      double v[W];
+      if (flow) {
+        __syncwarp();
+        tmem_wait_ld32(tr);
+#pragma unroll
+        for (int q = 0; q < W; ++q) v[q] = __hiloint2double(static_cast<int>(tr[2 * q + 1]), static_cast<int>(tr[2 * q]));
+        if (c > 0) tmem_ld32_issue(tbase + 32u * (c - 1), tr);
+      } else {
+        load_row<double, W>(crow, sw, v);
+      }
+      if (edge && face) {
+        if (fv != nullptr) {
+#pragma unroll
+          for (int q = 0; q < W; ++q) v[q] = (i0 + q < nx) ? fv[i0 + q] : 0.0;
+        }
+      } else if (!edge || valid) {
+        const double2* cwp = reinterpret_cast<const double2*>(cus + i0);  // 16-byte pairs
+        double cw[W];
+#pragma unroll
+        for (int q = 0; q < W / 2; ++q) {
+          const double2 pr = cwp[q];
+          cw[2 * q] = pr.x;
+          cw[2 * q + 1] = pr.y;
+        }
+        if (i0 + W > nx) {
+#pragma unroll
+          for (int q = W - 1; q >= 0; --q) {
+            if (i0 + q < nx) {
+              xn = back_elem(cw[q], xn, v[q]);
+              v[q] = xn;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int q = W - 1; q >= 0; --q) {
+            xn = back_elem(cw[q], xn, v[q]);
+            v[q] = xn;
+          }
+        }
+        if (act) {  // the pin after the sweep
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            if (i0 + q == 0) v[q] = x0v;
+            if (i0 + q == nx - 1) v[q] = x1v;
+          }
+        }
+      }
+      store_row<double, W>(crow, sw, v);
+      __syncwarp();
+      // out transposed: lanes 0-15 write line 2r's 16 values, 16-31 line 2r+1's
+      {
+        const int e = t & 15;
+        const int i = i0 + e;
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+          const int L = 2 * r + (t >> 4);
+          const double val = *swz_elem<double>(cbase + L * 128, e, L & 7);
+          if (j0 + L < ny && i < nx) plane[static_cast<size_t>(j0 + L) * p.nxp + i] = val;
+        }
+      }
+      if (!flow) {
+        fence_async_smem();  // this warp's writes to the slot precede the refill
+        __syncwarp();
+        if (nxt < ntiles) issue(nj0, nk, ns_, T + (NR - 1 - (c - T)), rslot(flip, c), (it + 1) & 1u);
+      } else {
+        __syncwarp();  // the staging chunk is read before the next chunk overwrites it
+      }
+    };
+    if (edge_tile) {
+      for (int c = C - 1; c >= 0; --c) back_chunk(true, c);
+    } else {
+      for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
+    }
+    if (MODE == 2 && nxt < ntiles) {
+      // the next tile's first inputs take the input slots (the first of
+      // which staged results just now)
+      fence_async_smem();
+      __syncwarp();
+      for (int c = 0; c < KF; ++c) {
+        issue(nj0, nk, ns_, c, fsl, fpar);
+        if (++fsl == KF) {
+          fsl = 0;
+          fpar ^= 1u;
+        }
+      }
+      for (int c = 0; c < KF; ++c) {  // the consume cursor returns to the first of them
+        if (fsl == 0) {
+          fsl = KF - 1;
+          fpar ^= 1u;
+        } else {
+          --fsl;
+        }
+      }
+    }
+    tile = nxt;
+    tj0 = nj0;
+    tk = nk;
+    ts = ns_;
+  }
+}
+
+__global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
+    sweep_x_tmem_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<double> p,
+                        uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns) {
+  constexpr uint32_t kChunkBytes = 32u * 128u;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
+  XShape g;
+  g.nx = p.nx;
+  g.ny = p.ny;
+  g.nz = p.nz;
+  g.C = (g.nx + 15) / 16;
+  g.ntj = (g.ny + 31) / 32;
+  g.ntiles = static_cast<long long>(g.ntj) * g.nz * p.S;
+  const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
+  const int nt = static_cast<int>(blockDim.x >> 5) - ns;  // TMEM rings (warps ns..ns+nt-1)
+  const bool tm = warp >= ns;
+  unsigned char* rbase = tm ? base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                  static_cast<size_t>(warp - ns) * tmem_ring_bytes
+                            : base + static_cast<size_t>(warp) * smem_ring_bytes;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                                    static_cast<size_t>(nt) * tmem_ring_bytes);
+  // ring: [slots (+ staging chunk)] [upper diagonal] [barriers]; a TMEM ring
+  // over more than 16 chunks stages in its first input slot
+  const bool own_stage = tm && g.C <= kTmemMaxChunks;
+  const int nslots = tm ? kf + g.C - min(g.C, kTmemMaxChunks) : g.C;
+  unsigned char* slots = rbase;
+  unsigned char* stage = tm ? (own_stage ? rbase + static_cast<size_t>(nslots) * kChunkBytes : rbase) : nullptr;
+  double* cus = reinterpret_cast<double*>(rbase + static_cast<size_t>(nslots + (own_stage ? 1 : 0)) * kChunkBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(cus) +
+                                               static_cast<size_t>(g.C) * 16 * sizeof(double));
+
+  if (t == 0) {
+    if (warp == 0) prefetch_tmap(&map);
+    for (int c = 0; c < nslots; ++c) mbar_init(smem_u32(&full[c]), 1);
+    fence_barrier_init();
+  }
+  __syncwarp();
+  if (warp == 0) {
+    tmem_alloc(smem_u32(tmem_slot), 512);
+    tmem_relinquish();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  uint32_t pend = 0, ppar = 0;
+  if (tm) {
+    tmem_fence_after();
+    const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
+    if (own_stage)
+      x_tmem_ring<1>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+    else
+      x_tmem_ring<2>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+  } else {
+    x_tmem_ring<0>(&map, p, g, kf, slots, full, cus, nullptr, 0u, pend, ppar);
+  }
+  if (pend != 0) {
+    for (int sl = 0; sl < nslots; ++sl)
+      if ((pend >> sl) & 1u) mbar_wait(smem_u32(&full[sl]), (ppar >> sl) & 1u);
+  }
+  __syncwarp();
+  if (tm) {
+    tmem_wait_st();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tmem_fence_after();
+    tmem_dealloc(*tmem_slot, 512);
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned long long* counter = p.tile_counter;
+    if (atomicAdd(counter + 1, 1ull) == gridDim.x - 1) {
+      counter[0] = 0;
+      counter[1] = 0;
+    }
+  }
+}
+
+// ---- launch policy ----
+
+// The TMEM sweeps hand tiles out at run time, so fewer per ring still balance.
+constexpr long long kTmemMinTilesPerRing = 2;
+
+// One ring of the TMEM x sweep (a multiple of 1024 bytes, so every chunk
+// stays on the 128B-swizzle atom): shared-memory ring = C chunks; TMEM ring
+// = kf input chunks and a staging chunk, or, past 16 chunks, kf input chunks
+// and a resident chunk for each chunk past 16; then the upper diagonal and
+// the barriers.
+static size_t x_tmem_ring_bytes(int nx, bool tm, int kf) {
+  const int C = (nx + 15) / 16;
+  const int chunks = !tm ? C : (C <= kTmemMaxChunks ? kf + 1 : kf + C - kTmemMaxChunks);
+  const size_t b = static_cast<size_t>(chunks) * 32 * 128 + static_cast<size_t>(C) * 16 * 8 + kXTmemBarrierBytes;
+  return (b + 1023) / 1024 * 1024;
+}
+
+static size_t x_tmem_smem(int nx, int ns, int nt, int kf) {
+  // alignment pad, the rings, the TMEM address word
+  return 1024 + ns * x_tmem_ring_bytes(nx, false, kf) + nt * x_tmem_ring_bytes(nx, true, kf) + 128;
+}
+
+// The TMEM x sweep applies (FP64, agents not fused, 32-line tiles, lines of
+// at least 2 chunks and at most 32 slots per ring): by default only on
+// lines past 16 chunks, where the per-tile x sweep holds 1-2 tiles per SM;
+// at sweep TMEM level 2 on every such line.  *ns shared-memory rings and *nt
+// TMEM rings (the most that fit), *kf input slots per TMEM ring.  Measured on
+// B200 against the per-tile x sweep (x interval with the source kernel):
+// 256^3 0.170 against 0.179 ms, 160^3 x 6 0.115 against 0.118, but 200^3 x 4
+// 0.173 against 0.159 -- so shorter lines keep the per-tile sweep by default.
+static bool use_tmem_x(int eb, int nx, bool fused_agents, const SweepConfig& cfg, int* ns, int* nt, int* kf) {
+  const int C = (nx + 15) / 16;
+  if (eb != 8 || fused_agents || cfg.persistent < 1 || cfg.tmem == 0 || cfg.x_lines != 32 || C < 2) return false;
+  if (cfg.tmem < 2 && C <= kTmemMaxChunks) return false;
+  const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
+  int best = 0;
+  for (int t = kTmemRingTmem; t >= 1; --t) {
+    for (int f = min(C, kTmemFlowSlots); f >= 2; --f) {
+      if (f + resident > 32) continue;
+      for (int k = kTmemRingSmem; k >= 0; --k) {
+        if (k > 0 && C > 32) continue;  // a shared-memory ring's barriers: one bit per slot
+        if (x_tmem_smem(nx, k, t, f) <= 227 * 1024) {
+          if (k + t > best) {
+            best = k + t;
+            *ns = k;
+            *nt = t;
+            *kf = f;
+          }
+          break;
+        }
+      }
+    }
+  }
+  return best > 0;
+}
+
+// One TMEM ring: barriers, kf input slots plus a slot per chunk past the
+// 16 that TMEM holds, the staged upper-diagonal row.
+static size_t tmem_yz_ring_bytes(int n_line, int kf) {
+  const int C = (n_line + kRingRows - 1) / kRingRows;
+  const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
+  return kTmemBarrierBytes + static_cast<size_t>(kf + resident) * kRingRows * 32 * 8 +
+         static_cast<size_t>(C) * kRingRows * 8;
+}
+
+static size_t tmem_yz_smem(int n_line, int ns, int nt, int kf) {
+  // alignment pad, the rings, the TMEM address word (padded)
+  return 128 + ns * ring_yz_bytes(8, n_line) + nt * tmem_yz_ring_bytes(n_line, kf) + 128;
+}
+
+// The TMEM y/z sweep applies (FP64, lines of at least kTmemFlowSlots chunks,
+// at most 32 slots per ring); *ns shared-memory rings and *nt TMEM rings (the
+// most rings that fit, TMEM rings first), *kf input slots per TMEM ring.
+// More rings beat deeper TMEM rings (cube200 y, B200: 3 + 4 rings of 3
+// slots 0.120 ms; 2 + 4 rings of 4, 5, 6 slots 0.124, 0.127, 0.127 ms).
+static bool use_tmem_yz(int eb, int n_line, const SweepConfig& cfg, int* ns, int* nt, int* kf) {
+  const int C = (n_line + kRingRows - 1) / kRingRows;
+  if (eb != 8 || cfg.persistent < 1 || cfg.tmem == 0 || cfg.yz_tile != 32 || C < kTmemFlowSlots) return false;
+  const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
+  int best = 0;
+  for (int t = kTmemRingTmem; t >= 1; --t) {
+    for (int f = kTmemFlowSlots; f >= 2; --f) {
+      if (f + resident > 32) continue;
+      for (int k = kTmemRingSmem; k >= 0; --k) {
+        if (k > 0 && C > 32) continue;  // a shared-memory ring's barriers: one bit per slot
+        if (tmem_yz_smem(n_line, k, t, f) <= 227 * 1024) {
+          if (k + t > best) {
+            best = k + t;
+            *ns = k;
+            *nt = t;
+            *kf = f;
+          }
+          break;
+        }
+      }
+    }
+  }
+  return best > 0;
+}
+
+template <int AXIS>
+cudaError_t launch_tmem_yz(const CUtensorMap& ring_map, const SweepParams<double>& p, const SweepConfig& cfg,
+                           cudaStream_t st, bool* launched) {
+  *launched = false;
+  const int n = (AXIS == 1) ? p.ny : p.nz;
+  int ns = 0, nt = 0, kf = 0;
+  if (!use_tmem_yz(8, n, cfg, &ns, &nt, &kf)) return cudaSuccess;
+  const int rings = ns + nt;
+  const size_t smem = tmem_yz_smem(n, ns, nt, kf);
+  const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * p.S;
+  int grid = 0;
+  cudaError_t e = persistent_grid(sweep_yz_tmem_kernel<AXIS>, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
+  if (e != cudaSuccess) return e;
+  if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
+  sweep_yz_tmem_kernel<AXIS><<<grid, 32 * rings, smem, st>>>(
+      ring_map, p, static_cast<uint32_t>(ring_yz_bytes(8, n)), static_cast<uint32_t>(tmem_yz_ring_bytes(n, kf)), kf,
+      ns);
+  *launched = true;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tmem_x(const CUtensorMap& map, const SweepParams<double>& p, const SweepConfig& cfg,
+                          cudaStream_t st, bool* launched) {
+  *launched = false;
+  int ns = 0, nt = 0, kf = 0;
+  if (!use_tmem_x(8, p.nx, p.line_off != nullptr, cfg, &ns, &nt, &kf)) return cudaSuccess;
+  const int rings = ns + nt;
+  const size_t smem = x_tmem_smem(p.nx, ns, nt, kf);
+  const long long tiles = static_cast<long long>((p.ny + 31) / 32) * p.nz * p.S;
+  int grid = 0;
+  cudaError_t e = persistent_grid(sweep_x_tmem_kernel, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
+  if (e != cudaSuccess) return e;
+  if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
+  sweep_x_tmem_kernel<<<grid, 32 * rings, smem, st>>>(map, p, static_cast<uint32_t>(x_tmem_ring_bytes(p.nx, false, kf)),
+                                                      static_cast<uint32_t>(x_tmem_ring_bytes(p.nx, true, kf)), kf,
+                                                      ns);
+  *launched = true;
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_tmem_yz<1>(const CUtensorMap&, const SweepParams<double>&, const SweepConfig&,
+                                       cudaStream_t, bool*);
+template cudaError_t launch_tmem_yz<2>(const CUtensorMap&, const SweepParams<double>&, const SweepConfig&,
+                                       cudaStream_t, bool*);
+
+}  // namespace bfvm

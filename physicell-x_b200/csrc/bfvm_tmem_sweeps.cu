@@ -27,10 +27,11 @@ namespace bfvm {
 // y/z sweep, persistent, with tensor memory.  One CTA per SM of up to seven
 // rings, each one warp with no copy warp: warps 0..ns-1 (ns <= 3, as many as
 // shared memory holds) keep their tile's 16-row chunks in shared-memory slots
-// (forward results in place, as the ring above); the next four warps -- one
-// per TMEM lane quarter -- stream each chunk's input through three
-// shared-memory slots and keep the forward results in their 32 TMEM lanes
-// (32 columns per chunk, lines of at most 256).  Lane 0 of each warp issues
+// (forward results in place, as the ring sweep of bfvm_sweeps.cu does); the
+// next nt <= 4 warps -- one per TMEM lane quarter -- stream each of a line's
+// first 16 chunks through three shared-memory slots and keep its forward
+// results in their 32 TMEM lanes (32 columns per chunk), the chunks past 16
+// resident in shared-memory slots.  Lane 0 of each warp issues
 // its ring's TMA loads; the back substitution writes the results straight to
 // the field (each row a coalesced 256-byte store), so a slot is free as soon
 // as the warp has read it and the next tile's chunks load into it at once.

@@ -344,6 +344,14 @@ int bfvm_get_sweep_schedule(bfvm_ctx* ctx, int* persistent);
  * beside the shared-memory rings; 2 also in the x sweep on lines of 32 to
  * 256; 0 shared memory alone.  Every level gives the same bits. */
 int bfvm_set_sweep_tmem(bfvm_ctx* ctx, int on);
+/* The tensor-memory sweep a persistent FP64 sweep would run on lines of
+ * n_line voxels (host arithmetic, no device needed): axis 0 = the x sweep
+ * (agents not fused into it), 1 = the y or z sweep; tmem_level as
+ * bfvm_set_sweep_tmem.  Sets the shared-memory rings, TMEM rings and input
+ * slots per TMEM ring of one CTA per SM, or all three to 0 where that sweep
+ * does not apply (the shared-memory schedules run instead; a launch also
+ * falls back when the grid gives fewer than two tiles per ring). */
+int bfvm_tmem_sweep_plan(int axis, int n_line, int tmem_level, int* smem_rings, int* tmem_rings, int* input_slots);
 
 /* Number of this library's kernels launched by the calls so far (counted on
  * the host at each launch). */

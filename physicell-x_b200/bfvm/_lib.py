@@ -66,6 +66,8 @@ _SIGS = {
     "bfvm_set_sweep_schedule": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_set_fused_sources": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_set_sweep_tmem": (C.c_int, [C.c_void_p, C.c_int]),
+    "bfvm_tmem_sweep_plan": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int)]),
     "bfvm_get_sweep_schedule": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "bfvm_set_dirichlet_nodes": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "bfvm_write_mesh_matlab": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double]),

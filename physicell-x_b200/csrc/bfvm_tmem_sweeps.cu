@@ -18,6 +18,7 @@
 #include <climits>
 #include <type_traits>
 
+#include "biofvm_b200.h"
 #include "bfvm_internal.h"
 #include "bfvm_ptx.cuh"
 #include "bfvm_sweep_common.cuh"
@@ -988,3 +989,19 @@ template cudaError_t launch_tmem_yz<2>(const CUtensorMap&, const SweepParams<dou
                                        cudaStream_t, bool*);
 
 }  // namespace bfvm
+
+extern "C" int bfvm_tmem_sweep_plan(int axis, int n_line, int tmem_level, int* smem_rings, int* tmem_rings,
+                                    int* input_slots) {
+  if ((axis != 0 && axis != 1) || n_line < 1 || n_line > 65535 || tmem_level < 0 || tmem_level > 2 || !smem_rings ||
+      !tmem_rings || !input_slots)
+    return BFVM_ERR_ARG;
+  bfvm::SweepConfig cfg;
+  cfg.tmem = tmem_level;
+  int ns = 0, nt = 0, kf = 0;
+  const bool on = axis == 0 ? bfvm::use_tmem_x(8, n_line, false, cfg, &ns, &nt, &kf)
+                            : bfvm::use_tmem_yz(8, n_line, cfg, &ns, &nt, &kf);
+  *smem_rings = on ? ns : 0;
+  *tmem_rings = on ? nt : 0;
+  *input_slots = on ? kf : 0;
+  return BFVM_OK;
+}

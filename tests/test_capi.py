@@ -67,3 +67,35 @@ def test_create_rejects_bad_arguments():
         cfg = _lib.bfvm_config(kw["nx"], kw["ny"], kw["nz"], kw["S"], kw["dx"], kw["dt"], D, lam, kw["precision"], 0)
         assert L.bfvm_create(C.byref(cfg), C.byref(h)) == _lib.BFVM_ERR_ARG
     assert L.bfvm_create(None, C.byref(h)) == _lib.BFVM_ERR_ARG
+
+
+def _plan(axis, n, level=1):
+    L = _lib.lib()
+    a, b, c = C.c_int(-1), C.c_int(-1), C.c_int(-1)
+    assert L.bfvm_tmem_sweep_plan(axis, n, level, C.byref(a), C.byref(b), C.byref(c)) == _lib.BFVM_OK
+    return a.value, b.value, c.value
+
+
+def test_tmem_sweep_plan():
+    """The tensor-memory sweep configurations (shared-memory rings, TMEM
+    rings, input slots per TMEM ring) chosen per line length: those measured
+    on B200 (y/z: 3 + 4 rings at lines of 200, fewer shared-memory rings as
+    lines grow, TMEM rings partly resident past 256; x by default only past
+    256), and where the shared-memory schedules take over."""
+    yz = {40: (3, 4, 3), 200: (3, 4, 3), 256: (2, 4, 3), 300: (1, 4, 3), 400: (0, 4, 3), 500: (0, 2, 3),
+          640: (0, 2, 3), 700: (0, 1, 3), 720: (0, 1, 3), 32: (0, 0, 0), 800: (0, 0, 0)}
+    for n, want in yz.items():
+        assert _plan(1, n) == want, n
+        assert _plan(1, n, 0) == (0, 0, 0), n
+    x1 = {200: (0, 0, 0), 256: (0, 0, 0), 300: (1, 4, 3), 400: (0, 4, 3), 640: (0, 2, 2), 700: (0, 1, 3),
+          800: (0, 0, 0)}
+    for n, want in x1.items():
+        assert _plan(0, n) == want, n
+    x2 = {20: (3, 4, 2), 200: (3, 4, 2), 256: (2, 4, 3), 640: (0, 2, 2), 16: (0, 0, 0)}
+    for n, want in x2.items():
+        assert _plan(0, n, 2) == want, n
+    L = _lib.lib()
+    a = C.c_int()
+    for args in ((2, 100, 1), (1, 0, 1), (1, 100, 3), (0, 100, -1)):
+        assert L.bfvm_tmem_sweep_plan(*args, C.byref(a), C.byref(a), C.byref(a)) == _lib.BFVM_ERR_ARG
+    assert L.bfvm_tmem_sweep_plan(1, 100, 1, None, C.byref(a), C.byref(a)) == _lib.BFVM_ERR_ARG

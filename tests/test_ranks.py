@@ -1,4 +1,4 @@
-"""The multi-process side of bench.py on CPU: two gloo ranks on 127.0.0.1.
+"""The host side of bench.py on CPU: two gloo ranks on 127.0.0.1, the clock record.
 
 The solve does not shard (replicas only), so the only cross-rank steps are
 the barriers and the max of the per-rank step time; rank 0 alone prints.
@@ -78,3 +78,24 @@ def test_reference_arm_other_ranks_print_nothing(monkeypatch):
 
 if __name__ == "__main__":
     sys.exit(pytest.main([__file__, "-q"]))
+
+
+def test_clock_sampler_summary():
+    """The clock record bench.py attaches to its line: median SM clock under
+    load, the maximum clock, and which slowdown reasons were active in any
+    sample, from nvidia-smi's CSV rows (malformed and N/A rows skipped)."""
+    bench = _bench()
+    cs = bench.ClockSampler(0)
+    cs.lines = [
+        "0, 1965, 1965, 701.5, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
+        "0, 1950, 1965, 980.2, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+        "0, 1965, 1965, 990.0, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+        "garbage",
+        "0, [N/A], 1965, 10.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+    ]
+    s = cs.summary()
+    assert s == {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
+    cs.lines = ["0, 1200, 1965, 500.0, 0x0, Active, Not Active, Active, Not Active"]
+    assert cs.summary()["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"]
+    cs.lines = []
+    assert cs.summary() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}

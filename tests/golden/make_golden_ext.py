@@ -17,6 +17,7 @@ oracle/_ref/libbiofvm_ref.so (single MPI rank, one thread for agent loops):
              that solver stays on its lines
   gradients  compute_all_gradient_vectors (BioFVM_microenvironment.cpp:1454-1616)
   bulk       simulate_bulk_sources_and_sinks (:1327-1368)
+  matlab     write_to_matlab (:1222-1249): the file's size and SHA-256
 
 Each fixture stores every generated input (node lists, rates, amounts, the
 workload's parameters and a hash of its initial field) with the reference's
@@ -182,11 +183,37 @@ def bulk(seed):
     return save(f"ext_bulk_{seed}", kw, wl, supply=supply, target=target, uptake=uptake, final=final)
 
 
+def matlab(i):
+    """Microenvironment::write_to_matlab (BioFVM_microenvironment.cpp:1222-1249)
+    after one step: the field it wrote from, and the file's size and hash."""
+    import dataclasses
+    import tempfile
+
+    kw = dict(seed=3, nx=13, ny=7, nz=9, S=2, n_agents=5, steps=1)
+    wl = W.small_random(**kw)
+    repl = [{}, {"dx": 1.3, "origin": [-7.77, 2.9, -0.123]}][i]
+    if repl:
+        wl = dataclasses.replace(wl, dx=repl["dx"], origin=tuple(repl["origin"]))
+    ref = Reference(wl, threads=1)
+    try:
+        ref.run(1)
+        field = ref.field()
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "r.mat")
+            ref.write_matlab(path)
+            raw = open(path, "rb").read()
+    finally:
+        ref.close()
+    kw["replace"] = repl
+    return save(f"ext_matlab_{i}", kw, W.small_random(**{k: v for k, v in kw.items() if k != "replace"}),
+                field=field, file_sha=hashlib.sha256(raw).hexdigest(), file_size=len(raw))
+
+
 CASES = ([("tracking", (seed, stack)) for seed, stack in ((1, False), (2, True), (3, True))] + [("release", ())] +
          [("nodes", (seed,)) for seed in (0, 1, 2)] + [("lod2d", (seed,)) for seed in (0, 1, 2, 3)] +
          # every axis at least 2 long: the reference reads outside its array otherwise
          [("gradients", (i, shape)) for i, shape in enumerate([(9, 7, 5, 2), (2, 3, 4, 1), (33, 20, 12, 3)])] +
-         [("bulk", (seed,)) for seed in (1, 2, 3)])
+         [("bulk", (seed,)) for seed in (1, 2, 3)] + [("matlab", (i,)) for i in (0, 1)])
 
 
 def main():

@@ -1,9 +1,11 @@
 """The oracle against the golden fixtures of the calls around the step
 (tests/golden/make_golden_ext.py: outputs of the reference's own BioFVM code
 for internalized-substrate tracking and release, Dirichlet nodes, the 2-D LOD
-solver, gradients and bulk sources), bit for bit, without the reference tree.
+solver, gradients, bulk sources, and the MATLAB density file byte for byte),
+bit for bit, without the reference tree.
 Each fixture's workload is regenerated from its stored parameters and checked
 against the stored hash of its initial field first."""
+import dataclasses
 import hashlib
 import json
 import os
@@ -21,8 +23,11 @@ CASES = json.load(open(os.path.join(GOLD, "MANIFEST_EXT.json")))["cases"]
 def _load(name):
     z = np.load(os.path.join(GOLD, name + ".npz"))
     kw = json.loads(str(z["meta"]))["kw"]
+    repl = kw.pop("replace", None)
     wl = W.small_random(**kw)
     assert hashlib.sha256(np.ascontiguousarray(wl.field0).tobytes()).hexdigest() == str(z["field0_sha"]), name
+    if repl:
+        wl = dataclasses.replace(wl, dx=repl["dx"], origin=tuple(repl["origin"]))
     return z, wl
 
 
@@ -72,9 +77,20 @@ def _check_bulk(z, wl):
     assert np.array_equal(f, z["final"])
 
 
+def _check_matlab(z, wl, tmp):
+    path = os.path.join(tmp, "p.mat")
+    Port.write_matlab(path, z["field"], wl.shape, wl.origin, wl.dx)
+    raw = open(path, "rb").read()
+    assert len(raw) == int(z["file_size"])
+    assert hashlib.sha256(raw).hexdigest() == str(z["file_sha"])
+
+
 @pytest.mark.parametrize("name", CASES)
-def test_oracle_matches_golden_extension(name):
+def test_oracle_matches_golden_extension(name, tmp_path):
     z, wl = _load(name)
     kind = name.split("_")[1]
+    if kind == "matlab":
+        _check_matlab(z, wl, str(tmp_path))
+        return
     {"tracking": _check_tracking, "release": _check_release, "nodes": _check_nodes, "lod2d": _check_lod2d,
      "gradients": _check_gradients, "bulk": _check_bulk}[kind](z, wl)

@@ -426,17 +426,18 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
 }
 
 // x sweep, persistent, with tensor memory (FP64, agents in the standalone
-// source kernel, lines of 3 to 16 chunks).  The same plan as the y/z TMEM
-// sweep: one CTA per SM of ns shared-memory rings and four TMEM rings, each
-// one warp issuing its own TMA loads, tiles handed out by the per-solve
+// source kernel, lines of 2 to 46 chunks).  The same plan as the y/z TMEM
+// sweep: one CTA per SM of ns shared-memory rings and nt <= 4 TMEM rings,
+// each one warp issuing its own TMA loads, tiles handed out by the per-solve
 // counter.  A tile is 32 x-lines of one (k, s); chunk c is the 128-byte
 // column [16c, 16c + 16) of the 32 lines, staged with the 128B swizzle, and
 // lane t owns line j0 + t.  A shared-memory ring stages the whole tile
-// (forward results in place); a TMEM ring streams the chunks through kf
-// input slots and keeps the forward results in its TMEM lanes.  The back
-// substitution leaves each chunk's results as 32 swizzled rows (in the slot,
-// or in the TMEM ring's staging chunk) and the warp writes them out
-// transposed: each store instruction covers two lines' 128-byte segments.
+// (forward results in place); a TMEM ring streams a line's first 16 chunks
+// through kf input slots and keeps their forward results in its TMEM lanes,
+// the chunks past 16 resident in shared-memory slots.  The back substitution
+// leaves each chunk's results as 32 swizzled rows (in the slot, or in the
+// TMEM ring's staging chunk) and the warp writes them out transposed: each
+// store instruction covers two lines' 128-byte segments.
 constexpr int kXTmemBarrierBytes = 256;  // at the end of a ring
 
 // The shape of one x persistent sweep, shared by its rings.

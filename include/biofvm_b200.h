@@ -323,14 +323,18 @@ int bfvm_compute_gradients_device(bfvm_ctx* ctx, double* d_out);
 int bfvm_get_launch(bfvm_ctx* ctx, int* x_lines, int* yz_tile, int* yz_chunk);
 int bfvm_set_launch(bfvm_ctx* ctx, int x_lines, int yz_tile, int yz_chunk);
 
-/* Schedule of the single-solve sweeps.  Persistent sweeps run a compute warp
- * and a copy warp per CTA, as many CTAs as fit, each walking a sequence of
- * 32-line tiles and loading the next tile while it finishes the current one
- * (with x_lines == yz_tile == 32 and lines of at most 64 chunks; other
- * shapes run per tile).  persistent = 1 (default): y and z sweeps
- * persistent where every resident CTA gets at least 8 tiles, x sweep one CTA
- * per tile; 2: all three persistent; 0: one CTA per tile everywhere.  Every
- * schedule computes the same bits. */
+/* Schedule of the single-solve sweeps.  Persistent sweeps keep one CTA per SM
+ * (or as many as fit) walking a sequence of 32-line tiles, loading the next
+ * tile while they finish the current one (with x_lines == yz_tile == 32;
+ * other shapes run per tile): in FP64, where bfvm_set_sweep_tmem allows it,
+ * rings of one warp that keep forward results in shared memory or tensor
+ * memory and take tiles from a shared counter; otherwise a compute warp and
+ * a copy warp per ring (lines of at most 64 chunks).  persistent = 1
+ * (default): y and z sweeps persistent where every ring gets at least 2
+ * tiles (tensor-memory sweeps) or 8 (the others), x sweep one CTA per tile
+ * except on long lines with tensor memory; 2: all three persistent whatever
+ * the tile count; 0: one CTA per tile everywhere.  Every schedule computes
+ * the same bits. */
 int bfvm_set_sweep_schedule(bfvm_ctx* ctx, int persistent);
 /* Where bfvm_step applies the agents: fused = 0 (default) the standalone
  * source kernel ahead of the sweeps, 1 inside the x sweep, on the staged

@@ -248,7 +248,8 @@ int bfvm_field_sums(bfvm_ctx* ctx, double* out);
  * wait gave up since the last check, BFVM_ERR_CUDA on a CUDA error. */
 int bfvm_synchronize(bfvm_ctx* ctx);
 
-/* The cudaStream_t the solve runs on (as void*), for event timing. */
+/* The cudaStream_t the solve runs on (as void*), for event timing; NULL for a
+ * NULL ctx. */
 void* bfvm_stream(bfvm_ctx* ctx);
 /* Run the solve on a caller-owned stream (NULL: back to its own stream). */
 int bfvm_set_stream(bfvm_ctx* ctx, void* stream);
@@ -264,7 +265,7 @@ int bfvm_device_field(bfvm_ctx* ctx, void** ptr, int* pitch, int* elem_bytes);
 int bfvm_field_offsets(bfvm_ctx* ctx, double* offsets);
 
 /* Bytes of device memory the solve holds now (field, coefficients, agents,
- * host-transfer staging). */
+ * host-transfer staging); 0 for a NULL ctx. */
 size_t bfvm_device_bytes(bfvm_ctx* ctx);
 
 /* Bytes that bfvm_create(cfg), one host field upload and bfvm_set_agents with
@@ -389,10 +390,12 @@ int bfvm_batch_destroy(bfvm_batch* batch);
  * may belong to one batch; removal orders its later work after the batch's. */
 int bfvm_batch_add(bfvm_batch* batch, bfvm_ctx* ctx);
 int bfvm_batch_remove(bfvm_batch* batch, bfvm_ctx* ctx);
+/* Members of the batch (0 for a NULL batch). */
 int bfvm_batch_size(bfvm_batch* batch);
 /* nsteps LOD steps of every member (flags as for bfvm_step). */
 int bfvm_batch_step(bfvm_batch* batch, int nsteps, int flags);
 int bfvm_batch_synchronize(bfvm_batch* batch);
+/* The batch's stream (as void*); NULL for a NULL batch. */
 void* bfvm_batch_stream(bfvm_batch* batch);
 /* Schedule of a step.  mode 0: one fused persistent launch per step (tiles
  * of every member and sweep from one ordered work list, per-member

@@ -99,3 +99,23 @@ def test_tmem_sweep_plan():
     for args in ((2, 100, 1), (1, 0, 1), (1, 100, 3), (0, 100, -1)):
         assert L.bfvm_tmem_sweep_plan(*args, C.byref(a), C.byref(a), C.byref(a)) == _lib.BFVM_ERR_ARG
     assert L.bfvm_tmem_sweep_plan(1, 100, 1, None, C.byref(a), C.byref(a)) == _lib.BFVM_ERR_ARG
+
+
+# entry points that return a value rather than a status: what a NULL handle gives
+_NULL_VALUES = {"bfvm_stream": None, "bfvm_batch_stream": None, "bfvm_device_bytes": 0, "bfvm_batch_size": 0}
+
+
+def test_null_handles_are_rejected_before_any_device_work():
+    """Every entry point that takes a solve or batch handle first returns
+    BFVM_ERR_ARG for a NULL handle (zero and NULL for its other arguments),
+    without touching a device; the value-returning ones give NULL or 0."""
+    L = _lib.lib()
+    seen = 0
+    for name, (_, args) in _lib._SIGS.items():
+        if not args or args[0] is not C.c_void_p:
+            continue
+        vals = [0 if issubclass(a, C._SimpleCData) and a not in (C.c_void_p, C.c_char_p) else None for a in args]
+        got = getattr(L, name)(*vals)
+        assert got == _NULL_VALUES.get(name, _lib.BFVM_ERR_ARG), name
+        seen += 1
+    assert seen >= 50

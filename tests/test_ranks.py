@@ -1,4 +1,5 @@
-"""The host side of bench.py on CPU: two gloo ranks on 127.0.0.1, the clock record.
+"""The host side of bench.py on CPU: two gloo ranks on 127.0.0.1, the clock
+record, and the reference arm's line.
 
 The solve does not shard (replicas only), so the only cross-rank steps are
 the barriers and the max of the per-rank step time; rank 0 alone prints.
@@ -76,8 +77,31 @@ def test_reference_arm_other_ranks_print_nothing(monkeypatch):
     assert out.getvalue() == ""
 
 
-if __name__ == "__main__":
-    sys.exit(pytest.main([__file__, "-q"]))
+def test_reference_arm_line_on_rank_zero():
+    """`bench.py --impl reference` as launched for one GPU: the reference's
+    own CPU path on the full cube200 workload (one warm-up and one timed LOD
+    step here), one JSON line carrying the same metric, unit and workload as
+    the CUDA arm, the cpu_baseline it describes and an e2e with no copies."""
+    import json
+    import subprocess
+
+    bench = _bench()
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    proc = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                           "--warmup", "1"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert proc.returncode == 0, proc.stderr[-2000:]
+    lines = [ln for ln in proc.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, proc.stdout[-2000:]
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC and line["unit"] == bench.UNIT
+    assert line["config"]["workload"] == bench.WORKLOAD and line["dtype"] == "f64"
+    assert line["steps"] == 1 and line["warmup"] == 1 and line["n_gpus"] == 1 and line["higher_is_better"]
+    assert line["value"] > 0 and line["ms_per_step"] > 0
+    cb = line["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+
 
 
 def test_clock_sampler_summary():
@@ -99,3 +123,7 @@ def test_clock_sampler_summary():
     assert cs.summary()["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"]
     cs.lines = []
     assert cs.summary() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+
+
+if __name__ == "__main__":
+    sys.exit(pytest.main([__file__, "-q"]))

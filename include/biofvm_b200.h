@@ -343,10 +343,10 @@ int bfvm_set_sweep_schedule(bfvm_ctx* ctx, int persistent);
 int bfvm_set_fused_sources(bfvm_ctx* ctx, int fused);
 int bfvm_get_sweep_schedule(bfvm_ctx* ctx, int* persistent);
 /* Tensor-memory (TMEM) rings in the FP64 persistent sweeps: on = 1
- * (default) in the y/z sweeps on lines of 48 to 720 voxels and in the x
+ * (default) in the y/z sweeps on lines of 33 to 736 voxels and in the x
  * sweep on lines of 257 to 736 (agents not fused into it): up to four rings
  * keep the forward results of a line's first 256 values in the SM's TMEM
- * beside the shared-memory rings; 2 also in the x sweep on lines of 32 to
+ * beside the shared-memory rings; 2 also in the x sweep on lines of 17 to
  * 256; 0 shared memory alone.  Every level gives the same bits. */
 int bfvm_set_sweep_tmem(bfvm_ctx* ctx, int on);
 /* The tensor-memory sweep a persistent FP64 sweep would run on lines of

@@ -161,11 +161,11 @@ struct SweepConfig {
   // path holds every x tile until all of its chunks have landed.
   int fuse_sources = 0;
   // Tensor-memory rings in the FP64 persistent sweeps: 1 (default) in the
-  // y/z sweeps on lines of 48 to 720 (up to four rings keep the forward
+  // y/z sweeps on lines of 33 to 736 (up to four rings keep the forward
   // results of a line's first 256 values in TMEM next to the shared-memory
   // rings: 224 lines in flight per SM instead of 128 at lines of 200, 64
   // instead of 32 at 640), and in the x sweep on lines of 257 to 736 (agents
-  // not fused); 2 also in the x sweep on lines of 32 to 256; 0 shared memory
+  // not fused); 2 also in the x sweep on lines of 17 to 256; 0 shared memory
   // alone.  Same bits at every level.
   int tmem = 1;
 };

@@ -339,12 +339,14 @@ def test_kernel_launch_counter_moves():
 @pytest.mark.parametrize("shape", [(64, 48, 40, 2), (33, 100, 57, 3), (200, 200, 120, 1), (70, 256, 130, 2),
                                    (40, 257, 50, 1), (256, 40, 36, 2), (20, 64, 48, 1), (257, 33, 34, 1),
                                    (36, 400, 70, 2), (34, 40, 640, 1), (400, 36, 34, 2), (640, 33, 35, 1),
-                                   (36, 33, 700, 1), (700, 33, 34, 1)])
+                                   (36, 33, 700, 1), (700, 33, 34, 1), (36, 210, 736, 1), (736, 33, 34, 1),
+                                   (34, 650, 36, 1)])
 def test_tmem_sweeps_bitwise(shape):
     """The persistent sweeps with tensor-memory rings (lines of up to 16
     chunks in TMEM and, past 256, 16 in TMEM plus the rest resident in shared
-    memory, up to 720, one TMEM ring from 700; x lines of up to 256 only at
-    level 2):
+    memory, up to the longest planned line of 736, one TMEM ring from 657;
+    two input slots per TMEM ring at lines of 210, 650 and 736, three
+    elsewhere; x lines of up to 256 only at level 2):
     with and without TMEM, under the persistent schedules, bit for bit
     against the oracle, with sources, faces, ragged line ends and partial
     tiles."""

@@ -2,7 +2,7 @@
  * lod3d_oracle.h -- TEST INFRASTRUCTURE: the CPU oracle (plain C restatement)
  * of PhysiCell-X's BioFVM 3-D LOD diffusion-decay step and cell
  * sources/sinks.  Only tests, smoke() and bench.py's CPU-baseline leg may
- * call it; it is the checker, never the product.
+ * call it; it is the test oracle, never the product.
  *
  * Layout is the reference's: one flat array, index ((i*ny + j)*nz + k)*S + d
  * (Cartesian_Mesh::voxel_index, BioFVM/BioFVM_mesh.cpp:1149-1158, times the

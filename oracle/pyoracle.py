@@ -1,8 +1,8 @@
 """ctypes bindings for the CPU oracle -- TEST INFRASTRUCTURE.
 
 Only tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
-(and its ``--impl reference`` arm) import this module, always as the checker
-or the timed CPU reference, never as the product path.
+(and its ``--impl reference`` arm) import this module, always as the test
+oracle or the timed CPU reference, never as the product path.
 
 Two oracles share one numpy-facing interface:
 

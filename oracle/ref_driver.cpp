@@ -5,7 +5,7 @@
  * together with the unmodified reference sources (BioFVM/*.cpp, DistPhy/*.cpp)
  * and the single-rank MPI shim (oracle/mpi_shim/mpi.h) into
  * oracle/_ref/libbiofvm_ref.so by oracle/Makefile.  Only the tests, smoke()
- * and bench.py's CPU-baseline leg load that library, as the checker.
+ * and bench.py's CPU-baseline leg load that library, as the test oracle.
  *
  * What it drives (all reference code, nothing re-implemented here):
  *   - Microenvironment::resize_space(..., world, cart)   BioFVM_microenvironment.cpp:584-607

@@ -116,8 +116,8 @@ __global__ void scan_kernel(unsigned* __restrict__ x, int m) {
 }
 
 // Stable scatter of one radix pass.  Within a block the tile is walked in
-// rounds of 256 consecutive elements; an element's rank among equal digits is
-// (earlier rounds) + (earlier warps of this round) + (lower lanes of its warp),
+// steps of 256 consecutive elements; an element's rank among equal digits
+// is (earlier steps) + (earlier warps of this step) + (lower lanes of its warp),
 // so the output keeps the input order of equal digits.
 __global__ void radix_scatter_kernel(int n, const unsigned* __restrict__ kin, const int* __restrict__ vin, int shift,
                                      int nblocks, const unsigned* __restrict__ offsets, unsigned* __restrict__ kout,

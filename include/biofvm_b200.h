@@ -156,9 +156,13 @@ int bfvm_apply_sources(bfvm_ctx* ctx);
  * not allocate at that point (a loop whose device memory was reserved up
  * front, or code where cudaMalloc is not allowed).  Limits: n <= 262144
  * (larger: BFVM_ERR_ARG, no work queued); calls on the same device must not
- * overlap in time (they share the scratch and would race); the first call on
- * a device looks up the scratch address and should come before any stream
- * capture begins. */
+ * overlap in time (they share the scratch and would race).  The first call
+ * on a device (n = 0 is enough) is its set-up: it loads the scratch array and
+ * the kernels into device memory and looks up the array's address, so make
+ * it at set-up time, before the loop that must not allocate and before any
+ * stream capture begins; later calls allocate nothing.  The address is kept
+ * for the life of the process: after cudaDeviceReset on a device, do not call
+ * this entry point on that device again. */
 int bfvm_apply_sources_noalloc(bfvm_ctx* ctx, int n, const int* voxel, const unsigned char* active,
                                const double* c1, const double* c2, const double* e2);
 

@@ -240,6 +240,32 @@ def cube640(seed=3, steps=1000, n=640, n_agents=1_000_000):
     return _two_substrate("cube640", n, 10.0, steps, n_agents, seed, agent_mode="gauss", sigma=1500.0 * n / 640)
 
 
+def cube640_slab(axis, seed=3, steps=5, n=640, thickness=(12, 10), n_agents=20_000):
+    """cube640's substrates, dx, dt and Gaussian agent ball (sigma 1500 um
+    about the box centre, clamped into the box) on a slab that keeps the
+    full 640-voxel lines along one axis and is thin across the other two
+    (thickness voxels): every Thomas system of that axis has cube640's length
+    and coefficients, at a size the reference runs in seconds."""
+    dims = [thickness[0], thickness[1]]
+    dims.insert(axis, n)
+    nx, ny, nz = dims
+    fv = np.tile(np.array([38.0, 1.0]), (6, 1))
+
+    def upt(rng, m):
+        u = np.zeros((m, 2))
+        u[:, 0] = 10.0
+        return u
+
+    def sec(rng, m):
+        s = np.zeros((m, 2))
+        s[:, 1] = 1.0
+        return s
+
+    return make(f"cube640_slab{'xyz'[axis]}", nx, ny, nz, 2, 10.0, 0.01, steps, [1e5, 1e3], [0.1, 0.01], [1, 0],
+                fv, n_agents, seed + 10 * (axis + 1), agent_mode="gauss", sigma=1500.0, uptake=upt, secretion=sec,
+                init_kind=[("const", 38.0), ("uniform", 0.0, 0.1)])
+
+
 def cube200(seed=2, steps=500, n=200, n_agents=100_000, S=4):
     rng = np.random.Generator(np.random.PCG64(seed + 1000))
     D = _loguniform(rng, 1e2, 1e5, S)

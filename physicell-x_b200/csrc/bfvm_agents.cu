@@ -372,6 +372,24 @@ cudaError_t agents_sort(int n, const int* voxel, const unsigned char* active, in
   return cudaGetLastError();
 }
 
+// Loads (under CUDA's lazy module loading) every kernel agents_sort and
+// agents_apply_sources_by_order launch, so their first launch on the current
+// device allocates nothing for code.
+cudaError_t agents_preload_sort_kernels() {
+  const void* kernels[] = {reinterpret_cast<const void*>(agent_keys_kernel),
+                           reinterpret_cast<const void*>(radix_hist_kernel),
+                           reinterpret_cast<const void*>(scan_kernel),
+                           reinterpret_cast<const void*>(radix_scatter_kernel),
+                           reinterpret_cast<const void*>(agent_sources_by_order_kernel<double>),
+                           reinterpret_cast<const void*>(agent_sources_by_order_kernel<float>)};
+  for (const void* k : kernels) {
+    cudaFuncAttributes a;
+    const cudaError_t e = cudaFuncGetAttributes(&a, k);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 template <typename T>
 cudaError_t agents_apply_sources_by_order(int n, const unsigned* sorted_keys, const int* sorted_order, int S, int nx,
                                           int ny, int nz, int nxp, const double* c1, const double* c2,

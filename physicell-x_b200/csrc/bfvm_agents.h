@@ -48,6 +48,11 @@ cudaError_t agents_build(const AgentBuild& b, cudaStream_t st, int* launches);
 cudaError_t agents_sort(int n, const int* voxel, const unsigned char* active, int nx, int ny, int nz, void* scratch,
                         cudaStream_t st, const unsigned** sorted_keys, const int** sorted_order, int* launches);
 
+// Loads the kernels of agents_sort and agents_apply_sources_by_order on the
+// current device (lazy module loading would otherwise load them, and
+// allocate device memory for their code, at their first launch).
+cudaError_t agents_preload_sort_kernels();
+
 // Source/sink stage from a sort made by agents_sort, constants c1/c2/e2 in
 // agent-list layout [n][S]; off as below.
 template <typename T>

@@ -19,9 +19,14 @@
 //     not overlap in time: two host threads, or two streams whose work may run
 //     concurrently, would race on the scratch and corrupt each other's sort.
 //     Calls on different devices are independent.
-//   * The first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, which may load this module's device code); make
-//     that first call before any stream capture begins.
+//   * The first call on a device (n = 0 is enough) is its set-up: it looks up
+//     the array's device address (cudaGetSymbolAddress, which loads this
+//     module's device image and so places the array in device memory) and
+//     loads the kernels later calls launch.  Make it at set-up time, before
+//     the loop that must not allocate and before any stream capture begins.
+//   * The looked-up address is kept per device for the life of the process.
+//     After cudaDeviceReset on a device it is stale: do not call this entry
+//     point again on that device after a reset.
 //   * Nothing in the scratch has to start at zero: every word a call reads
 //     was written earlier in the same call (keys and histograms are rebuilt
 //     from the inputs), so the scratch is never cleared.
@@ -55,6 +60,13 @@ int scratch_address(int device, void** out) {
     if (e != cudaSuccess || p == nullptr) {
       std::fprintf(stderr, "biofvm_b200: cudaGetSymbolAddress of the sources scratch failed: %s\n",
                    cudaGetErrorString(e));
+      return BFVM_ERR_CUDA;
+    }
+    // Load the sort and source kernels now too, so that later calls on this
+    // device allocate nothing for code either.
+    const cudaError_t e2 = bfvm::agents_preload_sort_kernels();
+    if (e2 != cudaSuccess) {
+      std::fprintf(stderr, "biofvm_b200: loading the sources kernels failed: %s\n", cudaGetErrorString(e2));
       return BFVM_ERR_CUDA;
     }
     g_scratch_addr[device] = p;

@@ -75,16 +75,19 @@ bool failed(const char* what, int rc) {
   return true;
 }
 
-// M's state, its context (re)created when the mesh, substrate count, dx or dt
-// changed.  nullptr (after a message) when the context cannot be made.
+// M's state, its context (re)created when the mesh, substrate count or dx
+// changed.  A new dt alone keeps the context: the reference factors its
+// Thomas systems on the first call only (diffusion_solver_setup_done,
+// BioFVM/BioFVM_solvers.cpp:125,335) and steps every later call with the
+// first call's dt, diffusion coefficients and decay rates, and so does this
+// solver.  nullptr (after a message) when the context cannot be made.
 DropinState* state_for(Microenvironment& M, double dt) {
   DropinState& st = table()[&M];
   const int nx = static_cast<int>(M.mesh.x_coordinates.size());
   const int ny = static_cast<int>(M.mesh.y_coordinates.size());
   const int nz = static_cast<int>(M.mesh.z_coordinates.size());
   const int S = static_cast<int>(M.number_of_densities());
-  if (st.ctx == nullptr || st.nx != nx || st.ny != ny || st.nz != nz || st.S != S || st.dt != dt ||
-      st.dx != M.mesh.dx) {
+  if (st.ctx == nullptr || st.nx != nx || st.ny != ny || st.nz != nz || st.S != S || st.dx != M.mesh.dx) {
     if (st.ctx) bfvm_destroy(st.ctx);
     st.ctx = nullptr;
     st.uploaded = false;

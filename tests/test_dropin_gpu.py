@@ -90,3 +90,18 @@ def test_dropin_follows_dirichlet_changes_between_steps():
     a = cpu.run(3, solver=0)
     b = gpu.run(3, solver=2)
     assert np.array_equal(a, b)
+
+
+def test_dropin_keeps_first_dt_like_the_reference():
+    """The reference factors its Thomas systems on its first call only
+    (diffusion_solver_setup_done, BioFVM_solvers.cpp:125,335) and keeps that
+    call's dt afterwards; the drop-in keeps it too, so calls with another dt
+    still give the reference's bits."""
+    wl = W.small_random(407, steps=2)
+    cpu, gpu = _pair(wl)
+    for ref, solver in ((cpu, 0), (gpu, 2)):
+        ref.diffusion(solver=solver)
+        for dt in (wl.dt * 2.0, wl.dt * 0.5):
+            with __import__("pyoracle")._stdout_to_stderr():
+                assert ref.L.ref_env_diffusion(ref.h, dt, solver, 4) == 0
+    assert np.array_equal(cpu.field(), gpu.field())

@@ -95,6 +95,22 @@ def test_port_matches_uneven_env_golden_hash(golden_dir):
     assert _sha(field) == str(g["final_sha"])
 
 
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_port_matches_cube640_line_goldens(golden_dir, axis):
+    """cube640's substrates, coefficients and Gaussian agent ball on its
+    640-voxel lines along each axis: the C restatement gives the reference's
+    bits (the fixtures come from the reference build)."""
+    wl = W.cube640_slab(axis)
+    g = _load(golden_dir, f"{wl.name}_{wl.steps}")
+    assert _sha(wl.field0) == str(g["field0_sha"])
+    assert _sha(wl.agent_voxel) == str(g["voxel_sha"])
+    c1, c2, e2 = Port.workload_constants(wl)
+    assert _sha(c1) == str(g["c1_sha"]) and _sha(c2) == str(g["c2_sha"]) and _sha(e2) == str(g["e2_sha"])
+    field = Port.run(wl)
+    assert np.array_equal(field[g["sample_idx"]], g["sample_val"])
+    assert _sha(field) == str(g["final_sha"])
+
+
 # ---- analytic known answers (from the mathematics, not the reference) -------
 
 def _uniform_wl(n, S, D, decay, value, steps=5, active=0):

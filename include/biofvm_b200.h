@@ -118,6 +118,19 @@ int bfvm_download_field_device(bfvm_ctx* ctx, double* d_field);
 int bfvm_set_agents(bfvm_ctx* ctx, int n, const int* voxel, const unsigned char* active, const double* c1,
                     const double* c2, const double* e2);
 
+/* New constants for some agents of the current list, leaving the list, its
+ * voxels and its sort as they are: idx [n_changed] distinct list indices,
+ * c1, c2, e2 [n_changed][S] their new cell_source_sink_solver_temp1, _temp2
+ * and _temp_export2.  The reference recomputes an agent's constants only
+ * when its volume changed (Basic_Agent::simulate_secretion_and_uptake,
+ * BioFVM/BioFVM_basic_agent.cpp:509-518, calling set_internal_uptake_constants,
+ * :224-274), so a caller sends just those agents instead of the whole list.
+ * Later source stages use the new constants; a list set from rates keeps its
+ * rates (the exports tracked per agent do not change).  Host pointers;
+ * BFVM_ERR_ARG for an index outside the list or given twice. */
+int bfvm_update_agents(bfvm_ctx* ctx, int n_changed, const int* idx, const double* c1, const double* c2,
+                       const double* e2);
+
 /* Agent list from rates: volume [n] and secretion, uptake, saturation and
  * net-export rates [n][S]; the constants are computed on the device with the
  * arithmetic of Basic_Agent::set_internal_uptake_constants
@@ -139,7 +152,10 @@ int bfvm_agent_constants_device(int n, int S, double dt, double voxel_volume, co
  *  diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING]
  * (BioFVM_microenvironment.cpp:1370-1384; BioFVM_solvers.cpp:102-780):
  * Dirichlet pin, x sweep, pin, y sweep, pin, z sweep, pin.  Asynchronous on
- * the solve's stream. */
+ * the solve's stream.  Runs of more than 16 steps replay a captured CUDA
+ * graph of 16 steps (recaptured when the agents, tracking or launch settings
+ * change), unless per-step timing is on or the caller is capturing the
+ * solve's stream itself; the results are the same bits either way. */
 int bfvm_step(bfvm_ctx* ctx, int nsteps, int flags);
 
 /* The source/sink stage alone (one call of
@@ -248,9 +264,32 @@ int bfvm_sample_agents(bfvm_ctx* ctx, double* out);
  * (the mass-balance check; multiply by dx^3 for total substrate). */
 int bfvm_field_sums(bfvm_ctx* ctx, double* out);
 
+/* Periodic FP64 mass-balance record: after every `every`-th step of
+ * bfvm_step (counted from this call), the per-substrate sums of the
+ * densities over all voxels, accumulated in FP64 on the device in a fixed
+ * order (deterministic), are appended to a device ring of `capacity`
+ * records.  For an FP32 solve this is the FP64 check of the FP32 field: its
+ * records compare step for step with an FP64 solve's.  every = 0 turns it
+ * off and frees the ring.  No counterpart in the reference (one precision;
+ * its conservation printout is unit_test_conservation.cpp). */
+int bfvm_set_mass_log(bfvm_ctx* ctx, int every, int capacity);
+/* The records still in the ring, oldest first: out [min(kept, max_records)][S];
+ * *n_total = records made since bfvm_set_mass_log (records beyond the ring's
+ * capacity overwrite the oldest).  Synchronous; BFVM_ERR_STATE while off. */
+int bfvm_read_mass_log(bfvm_ctx* ctx, double* out, int max_records, int* n_total);
+
 /* Wait for the solve's stream; returns BFVM_ERR_TIMEOUT if a device-side
  * wait gave up since the last check, BFVM_ERR_CUDA on a CUDA error. */
 int bfvm_synchronize(bfvm_ctx* ctx);
+
+/* Upper bound, in nanoseconds, on every bounded device-side wait of this
+ * library's kernels on one device (a TMA copy's barrier, the batched
+ * engine's wait for a member's previous sweep): past it the kernel records a
+ * timeout, which the next bfvm_synchronize / bfvm_batch_synchronize returns
+ * as BFVM_ERR_TIMEOUT, and finishes without hanging the GPU.  Default 2 s;
+ * 1000 <= ns <= 60e9.  Applies to launches made after the call.  No
+ * counterpart in the reference, which has no device waits. */
+int bfvm_set_wait_limit_ns(int device, unsigned long long ns);
 
 /* The cudaStream_t the solve runs on (as void*), for event timing; NULL for a
  * NULL ctx. */
@@ -346,6 +385,20 @@ int bfvm_set_sweep_schedule(bfvm_ctx* ctx, int persistent);
  * tile.  Both give the same bits. */
 int bfvm_set_fused_sources(bfvm_ctx* ctx, int fused);
 int bfvm_get_sweep_schedule(bfvm_ctx* ctx, int* persistent);
+/* Arithmetic of the FP64 forward elimination.  chain = 0 (default): the
+ * reference's, operation by operation (fma, then a correctly rounded
+ * division), so results are the reference's bits.  chain = 1: the short
+ * chain y_i = fma(a_i, y_{i-1}, v_i * r_i) with r_i = RN(1/d_i) and
+ * a_i = RN(c1 * r_i) precomputed in FP64 at set-up -- one dependent FMA per
+ * element instead of an FMA and a division, and no exactness screen.  Its
+ * results differ from the reference's by a few units in the last place per
+ * sweep, within the 1e-12 relative per-voxel bound the FP64 path is held to
+ * (the tests measure it against the oracle).  The back substitution, the
+ * sources and the pins are the same in both.  The 2-D solver always uses
+ * chain 0.  FP64 solves only (BFVM_ERR_STATE otherwise). */
+int bfvm_set_fp64_chain(bfvm_ctx* ctx, int chain);
+int bfvm_get_fp64_chain(bfvm_ctx* ctx, int* chain);
+
 /* Tensor-memory (TMEM) rings in the FP64 persistent sweeps: on = 1
  * (default) in the y/z sweeps on lines of 33 to 736 voxels and in the x
  * sweep on lines of 257 to 736 (agents not fused into it): up to four rings
@@ -414,6 +467,16 @@ int bfvm_batch_get_schedule(bfvm_batch* batch, int* mode, int* yz_chunk, int* or
  * fastest, and report its ms per step.  Member fields are restored after
  * the trials. */
 int bfvm_batch_autotune(bfvm_batch* batch, int flags, int trial_steps, double* best_ms_per_step);
+
+/* Fault injection, for tests of the timeout path (fused schedule, mode 0,
+ * only: BFVM_ERR_STATE otherwise).  The first step of the next
+ * bfvm_batch_step call runs with this member's count of finished x tiles
+ * started far below zero, so the member's y tiles wait for x tiles that
+ * never count up: their bounded waits run out, bfvm_batch_synchronize
+ * returns BFVM_ERR_TIMEOUT (and clears the status), the member's field is
+ * left undefined and the other members' results are unaffected.  The fault
+ * is made on the host side of the dependency; nothing faults the GPU. */
+int bfvm_batch_inject_stall(bfvm_batch* batch, bfvm_ctx* member);
 
 #ifdef __cplusplus
 }

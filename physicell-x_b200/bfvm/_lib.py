@@ -58,6 +58,7 @@ _SIGS = {
     "bfvm_download_field_device": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_set_agents": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 5),
     "bfvm_set_agents_from_rates": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 7),
+    "bfvm_update_agents": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 4),
     "bfvm_step": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "bfvm_agent_constants_device": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double] + [C.c_void_p] * 9),
     "bfvm_apply_sources": (C.c_int, [C.c_void_p]),
@@ -66,6 +67,8 @@ _SIGS = {
     "bfvm_set_sweep_schedule": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_set_fused_sources": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_set_sweep_tmem": (C.c_int, [C.c_void_p, C.c_int]),
+    "bfvm_set_fp64_chain": (C.c_int, [C.c_void_p, C.c_int]),
+    "bfvm_get_fp64_chain": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "bfvm_tmem_sweep_plan": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                        C.POINTER(C.c_int)]),
     "bfvm_get_sweep_schedule": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
@@ -82,7 +85,10 @@ _SIGS = {
     "bfvm_set_internalized": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_release_internalized": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "bfvm_field_sums": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bfvm_set_mass_log": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "bfvm_read_mass_log": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "bfvm_synchronize": (C.c_int, [C.c_void_p]),
+    "bfvm_set_wait_limit_ns": (C.c_int, [C.c_int, C.c_ulonglong]),
     "bfvm_stream": (C.c_void_p, [C.c_void_p]),
     "bfvm_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_device_field": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
@@ -112,6 +118,7 @@ _SIGS = {
     "bfvm_batch_set_schedule": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "bfvm_batch_get_schedule": (C.c_int, [C.c_void_p] + [C.POINTER(C.c_int)] * 5),
     "bfvm_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "bfvm_batch_inject_stall": (C.c_int, [C.c_void_p, C.c_void_p]),
 }
 
 

@@ -15,7 +15,10 @@ is continuous batching:
   one launch per sweep over all members, replayed from a CUDA graph;
 * solves that finish in that quantum leave the batch at once and their
   densities are read back while the next quantum already runs, then their
-  memory is freed, which admits the next requests.
+  memory is freed, which admits the next requests;
+* a request can be cancelled (``Server.cancel``, from any thread) while it
+  waits or runs: between two quanta it is dropped from the queue, or leaves
+  the batch and is freed, and is reported as cancelled.
 
 A solve's result does not depend on what else is in the batch: members run the
 same per-tile code as a solve stepped alone (tests check this bit for bit).
@@ -24,6 +27,7 @@ from __future__ import annotations
 
 import collections
 import ctypes as C
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -121,6 +125,7 @@ class ServeStats:
     results: list = field(default_factory=list)
     wall: float = 0.0
     rejected: list = field(default_factory=list)
+    cancelled: list = field(default_factory=list)  # (rid, steps done) of cancelled requests
     peak_bytes: int = 0
     quanta: int = 0
 
@@ -130,7 +135,7 @@ class ServeStats:
     def summary(self):
         lat = self.latencies()
         upd = sum(r.updates for r in self.results)
-        return {"requests": len(self.results), "rejected": len(self.rejected),
+        return {"requests": len(self.results), "rejected": len(self.rejected), "cancelled": len(self.cancelled),
                 "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
                 "p99_s": float(np.percentile(lat, 99)) if lat.size else None,
                 "wall_s": self.wall, "updates": upd, "updates_per_s": upd / self.wall if self.wall > 0 else None,
@@ -154,13 +159,31 @@ class Server:
         self.budget = int(budget_bytes)
         self.batch = Batch(precision, device)
         self.batch.set_schedule(mode=mode, yz_chunk=yz_chunk, graph_steps=graph_steps)
+        self._cancel_lock = threading.Lock()
+        self._cancelled = set()
 
     def close(self):
         self.batch.close()
 
-    def run(self, requests, clock=time.perf_counter, poll=0.0005):
+    def cancel(self, rid):
+        """Cancel request `rid` (safe from any thread).  It takes effect
+        between two quanta: a waiting request is dropped, a running one leaves
+        the batch, its solve is freed and its steps so far are reported in
+        ``ServeStats.cancelled``.  The other solves' results do not change."""
+        with self._cancel_lock:
+            self._cancelled.add(rid)
+
+    def _take_cancellations(self):
+        with self._cancel_lock:
+            out = set(self._cancelled)
+            self._cancelled.clear()
+        return out
+
+    def run(self, requests, clock=time.perf_counter, poll=0.0005, on_quantum=None):
         """Serve the requests (arrival times relative to the start) and return
-        the statistics; blocks until every admissible request has finished."""
+        the statistics; blocks until every admissible request has finished or
+        was cancelled.  on_quantum(server, quanta) is called after each
+        quantum is enqueued (a client can cancel requests from it)."""
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         queue = collections.deque()
         active: list[_Active] = []
@@ -168,7 +191,26 @@ class Server:
         used = 0
         st = ServeStats()
         t0 = clock()
+        cancelled = set()
         while pending or queue or active or retiring:
+            cancelled |= self._take_cancellations()
+            if cancelled:
+                for dq in (pending, queue):
+                    for req in [r for r in dq if r.rid in cancelled]:
+                        dq.remove(req)
+                        st.cancelled.append((req.rid, 0))
+                        cancelled.discard(req.rid)
+                for a in [a for a in active if a.req.rid in cancelled]:
+                    # leaves between quanta: the batch orders the solve's
+                    # later work (its release) after the steps already queued
+                    self.batch.remove(a.me)
+                    a.me.close()
+                    used -= a.nbytes
+                    active.remove(a)
+                    st.cancelled.append((a.req.rid, int(a.req.workload.steps) - a.remaining))
+                    cancelled.discard(a.req.rid)
+                if not (pending or queue or active or retiring):
+                    break
             now = clock() - t0
             while pending and pending[0].arrival <= now:
                 queue.append(pending.popleft())
@@ -194,6 +236,8 @@ class Server:
                 k = min(self.quantum, min(a.remaining for a in active))
                 self.batch.step(k, sources=self.sources)
                 st.quanta += 1
+                if on_quantum is not None:
+                    on_quantum(self, st.quanta)
                 for a in active:
                     a.remaining -= k
                 finished = [a for a in active if a.remaining == 0]

@@ -135,6 +135,15 @@ class Microenvironment:
               "bfvm_set_agents")
         self.n_agents = n
 
+    def update_agents(self, idx, c1, c2, e2):
+        """New constants for the agents at list indices ``idx`` (the ones
+        whose volume changed, as Basic_Agent::simulate_secretion_and_uptake
+        recomputes only those); the list and its voxel sort are kept."""
+        i = np.ascontiguousarray(idx, np.int32).ravel()
+        m = i.size
+        c1, c2, e2 = (_f64(x).reshape(m, self.S) for x in (c1, c2, e2))
+        check(self.L.bfvm_update_agents(self.h, m, _ptr(i), _ptr(c1), _ptr(c2), _ptr(e2)), "bfvm_update_agents")
+
     def set_agents_from_rates(self, voxel, volume, secretion, uptake, saturation, net_export, active=None):
         v = np.ascontiguousarray(voxel, np.int32).ravel()
         n = v.size
@@ -281,6 +290,20 @@ class Microenvironment:
         check(self.L.bfvm_field_sums(self.h, _ptr(out)), "bfvm_field_sums")
         return out
 
+    def set_mass_log(self, every, capacity=4096):
+        """Record the FP64 per-substrate field sums after every `every`-th
+        step (0: off); see :meth:`mass_log`."""
+        check(self.L.bfvm_set_mass_log(self.h, int(every), int(capacity)), "bfvm_set_mass_log")
+        self._mass_capacity = int(capacity)
+
+    def mass_log(self):
+        """The mass-balance records still kept, oldest first, [records, S]."""
+        cap = getattr(self, "_mass_capacity", 0)
+        out = np.empty((cap, self.S), np.float64)
+        n = C.c_int()
+        check(self.L.bfvm_read_mass_log(self.h, _ptr(out), cap, C.byref(n)), "bfvm_read_mass_log")
+        return out[: min(n.value, cap)]
+
     # -- introspection --------------------------------------------------------
     @property
     def stream(self):
@@ -323,6 +346,12 @@ class Microenvironment:
         in the y/z sweeps, 2 in the x sweep as well, 0 (or False) none; same
         bits at every level."""
         check(self.L.bfvm_set_sweep_tmem(self.h, int(level)), "bfvm_set_sweep_tmem")
+
+    def set_fp64_chain(self, chain):
+        """FP64 forward elimination: 0 (default) the reference's arithmetic,
+        bit for bit; 1 the short chain (one FMA per element, within a few
+        ulp of the reference per sweep)."""
+        check(self.L.bfvm_set_fp64_chain(self.h, int(chain)), "bfvm_set_fp64_chain")
 
     def get_sweep_schedule(self):
         v = C.c_int()

@@ -102,11 +102,15 @@ def uneven_batch(n_envs=256, steps=200, trial_steps=5, device=0):
     return out
 
 
-def single_accuracy(wl, device=0):
+def single_accuracy(wl, device=0, mass_every=None):
     """One workload run to its full step count in FP64 and in FP32, with
-    agent sources; per-substrate FP32 errors and both times."""
+    agent sources; per-substrate FP32 errors and both times, and the
+    periodic FP64 mass-balance check: every `mass_every` steps (default a
+    tenth of the run) both forms record their per-substrate field sums in
+    FP64, and the FP32 records are compared with the FP64 ones."""
     out = {"workload": wl.name, "shape": list(wl.shape), "agents": wl.n_agents, "steps": wl.steps}
-    fields = {}
+    every = mass_every or max(1, wl.steps // 10)
+    fields, masses = {}, {}
     for prec in ("fp64", "fp32"):
         # one-time setup (module load, kernel attributes, occupancy queries)
         # on a throwaway solve of the same shape, so the timed run is warm
@@ -115,12 +119,17 @@ def single_accuracy(wl, device=0):
         _timed_steps(warm, 3)
         warm.close()
         me = Microenvironment.from_workload(wl, prec, device)
+        me.set_mass_log(every, capacity=wl.steps // every + 1)
         t = _timed_steps(me, wl.steps)
         out[f"{prec}_s"] = t
         out[f"{prec}_updates_per_s"] = wl.n_values * wl.steps / t
         fields[prec] = _device_field(me, device)
+        masses[prec] = me.mass_log()
         me.close()
     out.update(field_errors(fields["fp32"], fields["fp64"]))
+    m32, m64 = masses["fp32"], masses["fp64"]
+    out["mass_check"] = {"every_steps": every, "records": int(m64.shape[0]),
+                         "max_rel_vs_fp64": (np.abs(m32 - m64) / np.maximum(np.abs(m64), 1e-300)).max(axis=0).tolist()}
     return out
 
 

@@ -167,13 +167,14 @@ __global__ void agent_csr_kernel(int n, const unsigned* __restrict__ sk, const i
                                  int nx, int n_lines, int S, const double* __restrict__ c1, const double* __restrict__ c2,
                                  const double* __restrict__ e2, int* __restrict__ line_off, int* __restrict__ a_i,
                                  double* __restrict__ ac1, double* __restrict__ ac2, double* __restrict__ ae2,
-                                 int* __restrict__ n_valid_out) {
+                                 int* __restrict__ n_valid_out, int* __restrict__ agent_pos) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p == 0 && (n == 0 || sk[0] >= sentinel)) {
     *n_valid_out = 0;
     for (int l = 0; l <= n_lines; ++l) line_off[l] = 0;
   }
   if (p >= n) return;
+  if (agent_pos != nullptr) agent_pos[sv[p]] = p;
   const unsigned key = sk[p];
   if (key >= sentinel) return;
   const int line = static_cast<int>(key / nx);
@@ -294,7 +295,7 @@ cudaError_t agents_build(const AgentBuild& b, cudaStream_t st, int* launches) {
   const unsigned sentinel = static_cast<unsigned>(b.nx) * b.ny * b.nz;
   if (n == 0) {
     agent_csr_kernel<<<1, 1, 0, st>>>(0, b.sorted_keys, b.sorted_vals, sentinel, b.nx, b.ny * b.nz, b.S, b.c1, b.c2,
-                                      b.e2, b.line_off, b.a_i, b.ac1, b.ac2, b.ae2, b.n_valid);
+                                      b.e2, b.line_off, b.a_i, b.ac1, b.ac2, b.ae2, b.n_valid, nullptr);
     *launches = 1;
     return cudaGetLastError();
   }
@@ -330,7 +331,7 @@ cudaError_t agents_build(const AgentBuild& b, cudaStream_t st, int* launches) {
   }
   agent_csr_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, b.sorted_keys, b.sorted_vals, sentinel, b.nx, b.ny * b.nz, b.S,
                                                     b.c1, b.c2, b.e2, b.line_off, b.a_i, b.ac1, b.ac2, b.ae2,
-                                                    b.n_valid);
+                                                    b.n_valid, b.agent_pos);
   *launches = 2 + 3 * passes;
   return cudaGetLastError();
 }
@@ -369,6 +370,41 @@ cudaError_t agents_sort(int n, const int* voxel, const unsigned char* active, in
   *sorted_keys = kin;
   *sorted_order = vin;
   *launches = 1 + 3 * passes;
+  return cudaGetLastError();
+}
+
+// New constants for m listed agents (agent-list indices idx[m], rows v1/v2/v3
+// [m][S]) of a built list: written to the list-order arrays c1/c2/e2 [n][S]
+// and, through agent_pos (list index -> sorted position), to the sorted,
+// substrate-major arrays ac1/ac2/ae2 [S][n] the source stage reads.
+__global__ void agent_update_kernel(int m, int S, int n, const int* __restrict__ idx, const double* __restrict__ v1,
+                                    const double* __restrict__ v2, const double* __restrict__ v3,
+                                    const int* __restrict__ agent_pos, double* __restrict__ c1,
+                                    double* __restrict__ c2, double* __restrict__ e2, double* __restrict__ ac1,
+                                    double* __restrict__ ac2, double* __restrict__ ae2) {
+  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= static_cast<long long>(m) * S) return;
+  const int r = static_cast<int>(q / S), s = static_cast<int>(q % S);
+  const int a = idx[r];
+  const int p = agent_pos[a];
+  const size_t src = static_cast<size_t>(r) * S + s, lst = static_cast<size_t>(a) * S + s;
+  const size_t srt = static_cast<size_t>(s) * n + p;
+  const double x1 = v1[src], x2 = v2[src], x3 = v3[src];
+  c1[lst] = x1;
+  c2[lst] = x2;
+  e2[lst] = x3;
+  ac1[srt] = x1;
+  ac2[srt] = x2;
+  ae2[srt] = x3;
+}
+
+cudaError_t agents_update_constants(int m, int S, int n, const int* idx, const double* v1, const double* v2,
+                                    const double* v3, const int* agent_pos, double* c1, double* c2, double* e2,
+                                    double* ac1, double* ac2, double* ae2, cudaStream_t st) {
+  if (m == 0) return cudaSuccess;
+  const long long total = static_cast<long long>(m) * S;
+  agent_update_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, st>>>(m, S, n, idx, v1, v2, v3, agent_pos,
+                                                                                  c1, c2, e2, ac1, ac2, ae2);
   return cudaGetLastError();
 }
 

@@ -29,6 +29,7 @@ struct AgentBuild {
   double* ac2;
   double* ae2;
   int* n_valid;                // device scalar: agents with a voxel
+  int* agent_pos = nullptr;    // [n] or nullptr: sorted position of each list index
   cudaEvent_t constants_ready; // or nullptr: c1/c2/e2 are written by work this event completes
 };
 
@@ -47,6 +48,14 @@ cudaError_t agents_build(const AgentBuild& b, cudaStream_t st, int* launches);
 // (nx*ny*nz = no voxel) and the agent index at each sorted position.
 cudaError_t agents_sort(int n, const int* voxel, const unsigned char* active, int nx, int ny, int nz, void* scratch,
                         cudaStream_t st, const unsigned** sorted_keys, const int** sorted_order, int* launches);
+
+// New constants c1/c2/e2 (v1/v2/v3, rows [m][S]) for the m list indices idx
+// of a built list of n agents, written to the list-order arrays [n][S] and,
+// through agent_pos (from agents_build), to the sorted arrays [S][n].  The
+// indices must be distinct and in [0, n).
+cudaError_t agents_update_constants(int m, int S, int n, const int* idx, const double* v1, const double* v2,
+                                    const double* v3, const int* agent_pos, double* c1, double* c2, double* e2,
+                                    double* ac1, double* ac2, double* ae2, cudaStream_t st);
 
 // Loads the kernels of agents_sort and agents_apply_sources_by_order on the
 // current device (lazy module loading would otherwise load them, and

@@ -53,6 +53,8 @@ struct bfvm_batch {
   int g_grid = 0, g_cap = 0, g_steps = 0, g_mode = -1;
   int g_items[3] = {0, 0, 0};
   long long launches = 0;
+  std::vector<int> env_of;  // member index -> position in the device tables
+  bfvm_ctx* stall = nullptr;  // bfvm_batch_inject_stall: member whose next step's x tiles never count
 };
 
 namespace {
@@ -148,6 +150,8 @@ int build_tables(bfvm_batch* b, bool sources) {
       axis_smem[a] = std::max(axis_smem[a], batch_axis_smem(c->eb, a, n_line[a], b->yz_chunk));
   }
   for (int a = 0; a < 3; ++a) pre[a * (b->cap + 1) + n] = items[a];
+  b->env_of.assign(n, 0);
+  for (int q = 0; q < n; ++q) b->env_of[idx[q]] = q;
   BatchHeader hdr;
   hdr.n_env = n;
   for (int a = 0; a < 3; ++a) hdr.n_items[a] = items[a];
@@ -175,13 +179,20 @@ int build_tables(bfvm_batch* b, bool sources) {
 }
 
 // Launches of one step on the batch stream (also used while capturing).
+// stall_env >= 0 (fault injection, fused schedule only): that table entry's
+// finished-x-tile counter starts far below zero, so its y tiles wait on x
+// tiles that never count up and their bounded waits run out.
 template <typename T>
-cudaError_t enqueue_step(bfvm_batch* b) {
+cudaError_t enqueue_step(bfvm_batch* b, int stall_env = -1) {
   if (b->mode == 1)
     return launch_batch_sweeps<T>(b->d_hdr, static_cast<const BatchEnv<T>*>(b->d_envs), b->d_pre, b->cap, b->items,
                                   b->axis_smem, b->stream);
   cudaError_t e = cudaMemsetAsync(b->d_counters, 0, sizeof(int) * (1 + 3 * b->cap), b->stream);
   if (e != cudaSuccess) return e;
+  if (stall_env >= 0) {
+    e = cudaMemsetAsync(b->d_counters + 1 + stall_env, 0xC0, sizeof(int), b->stream);  // 0xC0C0C0C0 < 0
+    if (e != cudaSuccess) return e;
+  }
   return launch_batch_step<T>(b->d_hdr, static_cast<const BatchEnv<T>*>(b->d_envs), b->d_pre, b->cap, b->d_counters,
                               b->d_status, b->grid, b->smem, b->stream);
 }
@@ -192,8 +203,8 @@ int kernels_per_step(const bfvm_batch* b) {
 }
 
 template <typename T>
-int launch_one(bfvm_batch* b) {
-  BFVM_CUDA(enqueue_step<T>(b));
+int launch_one(bfvm_batch* b, int stall_env = -1) {
+  BFVM_CUDA(enqueue_step<T>(b, stall_env));
   note_launches(kernels_per_step(b));
   b->launches += kernels_per_step(b);
   return BFVM_OK;
@@ -261,7 +272,16 @@ int step_impl(bfvm_batch* b, int nsteps, bool sources) {
     b->dirty = false;
   }
   int left = nsteps;
-  if (b->graph_steps > 1 && nsteps >= b->graph_steps) {
+  if (b->stall != nullptr) {
+    // an injected stall applies to the first step of this call, launched alone
+    const auto it = std::find(b->members.begin(), b->members.end(), b->stall);
+    b->stall = nullptr;
+    if (it != b->members.end() && b->mode == 0) {
+      if ((rc = launch_one<T>(b, b->env_of[it - b->members.begin()])) != BFVM_OK) return rc;
+      --left;
+    }
+  }
+  if (b->graph_steps > 1 && left >= b->graph_steps) {
     if (!b->gexec || b->g_steps != b->graph_steps || b->g_smem != b->smem || b->g_grid != b->grid ||
         b->g_cap != b->cap || b->g_mode != b->mode || b->g_items[0] != b->items[0] ||
         b->g_items[1] != b->items[1] || b->g_items[2] != b->items[2]) {
@@ -377,6 +397,14 @@ int bfvm_batch_synchronize(bfvm_batch* b) {
 }
 
 void* bfvm_batch_stream(bfvm_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
+
+int bfvm_batch_inject_stall(bfvm_batch* b, bfvm_ctx* c) {
+  if (!b || !c) return BFVM_ERR_ARG;
+  if (std::find(b->members.begin(), b->members.end(), c) == b->members.end()) return BFVM_ERR_STATE;
+  if (b->mode != 0) return BFVM_ERR_STATE;
+  b->stall = c;
+  return BFVM_OK;
+}
 
 int bfvm_batch_set_schedule(bfvm_batch* b, int mode, int yz_chunk, int order, int ctas_per_sm, int graph_steps) {
   if (!b || mode < 0 || mode > 1 || yz_chunk < 1 || yz_chunk > 256 || order < 0 || order > 1 || ctas_per_sm < 0 ||

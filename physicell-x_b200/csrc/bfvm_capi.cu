@@ -19,7 +19,12 @@ using namespace bfvm;
 namespace bfvm {
 
 static std::atomic<long long> g_launches{0};
-void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+// Set while this thread captures a CUDA graph: captured launches are counted
+// when the graph is launched, not when they are recorded.
+static thread_local bool t_capturing = false;
+void note_launches(int n) {
+  if (!t_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
+}
 
 // Thomas factorization of one axis, FP64, operation by operation as in
 // diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING
@@ -77,11 +82,106 @@ void thomas_axis_host(int n, int S, const double* D, const double* decay, double
 namespace {
 
 constexpr int kMaxTimedSteps = 4096;
+// LOD steps per captured CUDA graph of bfvm_step (four launches each).
+constexpr int kGraphSteps = 16;
+
+// Everything a captured step holds by value: the kernels' parameters are
+// built from these (device pointers change only with c->version), the
+// launch shapes from the sweep configuration.
+std::vector<long long> step_key(const bfvm_ctx* c, bool sources) {
+  const SweepConfig& g = c->cfg;
+  return {c->version, sources ? 1 : 0, c->n_agents, c->track, g.x_lines, g.yz_tile, g.yz_chunk, g.persistent,
+          g.fuse_sources, g.tmem, static_cast<long long>(reinterpret_cast<uintptr_t>(c->d_internal)),
+          static_cast<long long>(reinterpret_cast<uintptr_t>(c->d_ae1))};
+}
+
+void drop_step_graph(bfvm_ctx* c) {
+  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  c->step_graph = nullptr;
+  c->graph_key.clear();
+}
+
+// The launches of one LOD step on c->stream (also while capturing): the
+// standalone source kernel (unless fused or without agents), then the x, y
+// and z sweeps; per-step timing events when ev is given.
+template <typename T>
+int enqueue_step(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, cudaEvent_t* ev) {
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[0], c->stream));
+  if (standalone) {
+    const int rc = bfvm_apply_sources(c);  // timed with the x sweep
+    if (rc != BFVM_OK) return rc;
+  }
+  BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, c->stream));
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[1], c->stream));
+  BFVM_CUDA(launch_sweep_y<T>(c->maps, p, c->cfg, c->stream));
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[2], c->stream));
+  BFVM_CUDA(launch_sweep_z<T>(c->maps, p, c->cfg, c->stream));
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[3], c->stream));
+  note_launches(3);
+  return BFVM_OK;
+}
+
+// Capture kGraphSteps steps into c->step_graph.  The caller has run at least
+// one step uncaptured since the key last changed, so every host-side set-up
+// of the launches (kernel attributes, occupancy lookups) is cached already.
+template <typename T>
+int capture_step_graph(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, const std::vector<long long>& key) {
+  drop_step_graph(c);
+  cudaGraph_t g = nullptr;
+  BFVM_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  t_capturing = true;
+  for (int s = 0; s < kGraphSteps; ++s) {
+    const int rc = enqueue_step<T>(c, p, standalone, nullptr);
+    if (rc != BFVM_OK) {
+      t_capturing = false;
+      cudaStreamEndCapture(c->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return rc;
+    }
+  }
+  t_capturing = false;
+  BFVM_CUDA(cudaStreamEndCapture(c->stream, &g));
+  const cudaError_t e = cudaGraphInstantiate(&c->step_graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    c->step_graph = nullptr;
+    return BFVM_ERR_CUDA;
+  }
+  c->graph_key = key;
+  return BFVM_OK;
+}
 
 template <typename T>
-int run_steps(bfvm_ctx* c, int nsteps, bool sources) {
+int run_steps_plain(bfvm_ctx* c, int nsteps, bool sources) {
   const bool standalone = sources && c->n_agents > 0 && !c->cfg.fuse_sources;
   const SweepParams<T> p = make_params<T>(c, sources && !standalone);
+  // Runs of steps replay a captured graph of kGraphSteps steps (the same
+  // launches, so the same bits), which removes most of the per-launch host
+  // cost on small grids.  Not while timing per step, nor on a stream the
+  // caller is capturing already (the steps then go into the caller's graph).
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  BFVM_CUDA(cudaStreamIsCapturing(c->stream, &cap));
+  if (!c->timing && cap == cudaStreamCaptureStatusNone && nsteps > kGraphSteps) {
+    const std::vector<long long> key = step_key(c, sources);
+    int left = nsteps;
+    if (c->step_graph == nullptr || c->graph_key != key) {
+      int rc = enqueue_step<T>(c, p, standalone, nullptr);  // the uncaptured warm step
+      if (rc != BFVM_OK) return rc;
+      --left;
+      if ((rc = capture_step_graph<T>(c, p, standalone, key)) != BFVM_OK) return rc;
+    }
+    const int per_step = 3 + (standalone ? 1 : 0);
+    for (; left >= kGraphSteps; left -= kGraphSteps) {
+      BFVM_CUDA(cudaGraphLaunch(c->step_graph, c->stream));
+      note_launches(kGraphSteps * per_step);
+    }
+    for (; left > 0; --left) {
+      const int rc = enqueue_step<T>(c, p, standalone, nullptr);
+      if (rc != BFVM_OK) return rc;
+    }
+    return BFVM_OK;
+  }
   for (int s = 0; s < nsteps; ++s) {
     cudaEvent_t* ev = nullptr;
     if (c->timing && c->timed_steps < kMaxTimedSteps) {
@@ -94,18 +194,26 @@ int run_steps(bfvm_ctx* c, int nsteps, bool sources) {
       ev = &c->events[4 * static_cast<size_t>(c->timed_steps)];
       ++c->timed_steps;
     }
-    if (ev) BFVM_CUDA(cudaEventRecord(ev[0], c->stream));
-    if (standalone) {
-      const int rc = bfvm_apply_sources(c);  // timed with the x sweep
-      if (rc != BFVM_OK) return rc;
-    }
-    BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, c->stream));
-    if (ev) BFVM_CUDA(cudaEventRecord(ev[1], c->stream));
-    BFVM_CUDA(launch_sweep_y<T>(c->maps, p, c->cfg, c->stream));
-    if (ev) BFVM_CUDA(cudaEventRecord(ev[2], c->stream));
-    BFVM_CUDA(launch_sweep_z<T>(c->maps, p, c->cfg, c->stream));
-    if (ev) BFVM_CUDA(cudaEventRecord(ev[3], c->stream));
-    note_launches(3);
+    const int rc = enqueue_step<T>(c, p, standalone, ev);
+    if (rc != BFVM_OK) return rc;
+  }
+  return BFVM_OK;
+}
+
+// nsteps LOD steps; with the mass-balance log on, a record after every
+// mass_every-th step since the log was enabled.
+template <typename T>
+int run_steps(bfvm_ctx* c, int nsteps, bool sources) {
+  if (c->mass_every <= 0) return run_steps_plain<T>(c, nsteps, sources);
+  int left = nsteps;
+  while (left > 0) {
+    const int to_record = static_cast<int>(c->mass_every - c->mass_steps % c->mass_every);
+    const int seg = left < to_record ? left : to_record;
+    int rc = run_steps_plain<T>(c, seg, sources);
+    if (rc != BFVM_OK) return rc;
+    c->mass_steps += seg;
+    left -= seg;
+    if (c->mass_steps % c->mass_every == 0 && (rc = enqueue_mass_record(c)) != BFVM_OK) return rc;
   }
   return BFVM_OK;
 }
@@ -163,9 +271,11 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
   const int S = c->S;
   c->D.assign(D, D + S);
   c->decay.assign(decay, decay + S);
-  c->screen = 1;
+  c->screen_exact = 1;
   for (int s = 0; s < S; ++s)
-    if (!(D[s] >= 0.0) || !(decay[s] >= 0.0)) c->screen = 0;
+    if (!(D[s] >= 0.0) || !(decay[s] >= 0.0)) c->screen_exact = 0;
+  const bool fast = c->prec == BFVM_FP64 && c->fp64_chain == 1;
+  c->screen = fast ? 2 : c->screen_exact;  // 2: the short chain (kScreenFast)
   const int n_axis[3] = {c->nx, c->ny, c->nz};
   size_t dr_off[3], cu_off[3];
   const size_t bytes = coef_bytes(c, dr_off, cu_off);
@@ -184,7 +294,9 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
         const double r = 1.0 / d;  // RN(1/d), IEEE double division
         const double u = in ? cu[static_cast<size_t>(i) * S + s] : -0.0;
         if (c->prec == BFVM_FP64) {
-          reinterpret_cast<double2*>(host.data() + dr_off[ax])[q] = make_double2(d, r);
+          // reference-exact chain: {d, RN(1/d)}; short chain: {RN(c1 * RN(1/d)), RN(1/d)}
+          const double first = fast ? c1[s] * r : d;
+          reinterpret_cast<double2*>(host.data() + dr_off[ax])[q] = make_double2(first, r);
         } else {
           reinterpret_cast<double*>(host.data() + dr_off[ax])[q] = r;
         }
@@ -225,6 +337,8 @@ int free_agents(bfvm_ctx* c) {
   dfree(c, c->d_ac);
   dfree(c, c->d_agent_scratch);
   dfree(c, c->d_sample);
+  dfree(c, c->d_agent_pos);
+  c->d_agent_pos = nullptr;
   dfree(c, c->d_ae1);
   c->d_ae1 = nullptr;
   c->d_voxel = nullptr;
@@ -255,6 +369,7 @@ int ensure_agent_capacity(bfvm_ctx* c, int n) {
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_ac), sizeof(double) * 3 * S * cap);
   if (rc == BFVM_OK) rc = dalloc(c, &c->d_agent_scratch, agent_scratch_bytes(cap));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_sample), sizeof(double) * S * cap);
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_agent_pos), sizeof(int) * cap);
   if (rc != BFVM_OK) {
     free_agents(c);
     return rc;
@@ -287,6 +402,7 @@ int build_agents(bfvm_ctx* c, int n, cudaEvent_t constants_ready = nullptr) {
   b.ac2 = c->d_ac + S * n;
   b.ae2 = c->d_ac + 2 * S * n;
   b.n_valid = c->d_nvalid;
+  b.agent_pos = c->d_agent_pos;
   int launches = 0;
   BFVM_CUDA(agents_build(b, c->stream, &launches));
   note_launches(launches);
@@ -418,7 +534,10 @@ int bfvm_destroy(bfvm_ctx* c) {
   dfree(c, c->d_shift2d);
   dfree(c, c->d_zero_active);
   dfree(c, c->d_nodes);
+  dfree(c, c->d_delta);
+  dfree(c, c->d_mass);
   for (cudaEvent_t e : c->events) cudaEventDestroy(e);
+  drop_step_graph(c);
   if (c->copy_stream) {
     cudaStreamSynchronize(c->copy_stream);
     cudaStreamDestroy(c->copy_stream);
@@ -684,6 +803,47 @@ int bfvm_set_agents_from_rates(bfvm_ctx* c, int n, const int* voxel, const unsig
   return rc == BFVM_OK ? tracking_after_agents(c) : rc;
 }
 
+int bfvm_update_agents(bfvm_ctx* c, int n_changed, const int* idx, const double* c1, const double* c2,
+                       const double* e2) {
+  if (!c || n_changed < 0 || (n_changed > 0 && (!idx || !c1 || !c2 || !e2))) return BFVM_ERR_ARG;
+  if (n_changed == 0) return BFVM_OK;
+  if (n_changed > c->n_agents) return BFVM_ERR_ARG;
+  // Distinct indices of the current list: the update kernel writes each
+  // listed agent's constants from one thread per substrate, in parallel.
+  std::vector<unsigned char> seen(static_cast<size_t>(c->n_agents), 0);
+  for (int q = 0; q < n_changed; ++q) {
+    const int a = idx[q];
+    if (a < 0 || a >= c->n_agents || seen[a]) return BFVM_ERR_ARG;
+    seen[a] = 1;
+  }
+  DeviceGuard g(c->device);
+  const size_t S = c->S, m = static_cast<size_t>(n_changed);
+  const size_t idx_bytes = (sizeof(int) * m + 255) & ~size_t(255);
+  const size_t row = sizeof(double) * S * m;
+  const size_t need = idx_bytes + 3 * row;
+  if (need > c->cap_delta) {
+    dfree(c, c->d_delta);
+    c->d_delta = nullptr;
+    c->cap_delta = 0;
+    const int rc = dalloc(c, &c->d_delta, need);
+    if (rc != BFVM_OK) return rc;
+    c->cap_delta = need;
+  }
+  unsigned char* base = static_cast<unsigned char*>(c->d_delta);
+  int* d_idx = reinterpret_cast<int*>(base);
+  double* v = reinterpret_cast<double*>(base + idx_bytes);
+  BFVM_CUDA(cudaMemcpyAsync(d_idx, idx, sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
+  BFVM_CUDA(cudaMemcpyAsync(v, c1, row, cudaMemcpyHostToDevice, c->stream));
+  BFVM_CUDA(cudaMemcpyAsync(v + S * m, c2, row, cudaMemcpyHostToDevice, c->stream));
+  BFVM_CUDA(cudaMemcpyAsync(v + 2 * S * m, e2, row, cudaMemcpyHostToDevice, c->stream));
+  const size_t SN = S * c->n_agents;
+  BFVM_CUDA(agents_update_constants(n_changed, c->S, c->n_agents, d_idx, v, v + S * m, v + 2 * S * m, c->d_agent_pos,
+                                    c->d_c, c->d_c + SN, c->d_c + 2 * SN, c->d_ac, c->d_ac + SN, c->d_ac + 2 * SN,
+                                    c->stream));
+  note_launches(1);
+  return BFVM_OK;
+}
+
 int bfvm_agent_constants_device(int n, int S, double dt, double voxel_volume, const double* volume,
                                 const double* sec, const double* upt, const double* sat, const double* exp_,
                                 double* c1, double* c2, double* e2, void* stream) {
@@ -813,6 +973,20 @@ extern "C" int bfvm_synchronize(bfvm_ctx* c) {
     cudaMemset(c->d_status, 0, sizeof(int));
     return BFVM_ERR_TIMEOUT;
   }
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_set_wait_limit_ns(int device, unsigned long long ns) {
+  if (ns < 1000ull || ns > 60000000000ull) return BFVM_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return BFVM_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= ndev) return BFVM_ERR_NODEVICE;
+  DeviceGuard g(device);
+  BFVM_CUDA(sweeps_set_wait_limit(ns));
+  BFVM_CUDA(tmem_sweeps_set_wait_limit(ns));
   return BFVM_OK;
 }
 
@@ -961,6 +1135,31 @@ extern "C" int bfvm_set_fused_sources(bfvm_ctx* c, int fused) {
   DeviceGuard g(c->device);
   BFVM_CUDA(cudaStreamSynchronize(c->stream));
   c->cfg.fuse_sources = fused;
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_set_fp64_chain(bfvm_ctx* c, int chain) {
+  if (!c || (chain != 0 && chain != 1)) return BFVM_ERR_ARG;
+  if (c->prec != BFVM_FP64) return BFVM_ERR_STATE;
+  if (chain == c->fp64_chain) return BFVM_OK;
+  DeviceGuard g(c->device);
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  const int prev = c->fp64_chain;
+  c->fp64_chain = chain;
+  const std::vector<double> D = c->D, decay = c->decay;
+  const int rc = upload_coefficients(c, D.data(), decay.data());
+  if (rc != BFVM_OK) {
+    c->fp64_chain = prev;
+    upload_coefficients(c, D.data(), decay.data());
+    return rc;
+  }
+  ++c->version;  // the sweeps' parameters (screen) changed: graphs and batch tables are rebuilt
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_get_fp64_chain(bfvm_ctx* c, int* chain) {
+  if (!c || !chain) return BFVM_ERR_ARG;
+  *chain = c->fp64_chain;
   return BFVM_OK;
 }
 

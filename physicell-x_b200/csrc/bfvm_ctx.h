@@ -27,7 +27,9 @@ struct bfvm_ctx {
   void* d_coef = nullptr;
   size_t dr_off[3] = {0, 0, 0}, cu_off[3] = {0, 0, 0};
   void* d_c1 = nullptr;
-  int screen = 0;              // no negative diffusion or decay (SweepParams::screen)
+  int screen = 0;              // SweepParams::screen of the 3-D sweeps (kScreenFast: short FP64 chain)
+  int screen_exact = 0;        // 1 when no diffusion or decay rate is negative (the exactness screen applies)
+  int fp64_chain = 0;          // bfvm_set_fp64_chain: 0 reference-exact, 1 short chain
   double* d_off = nullptr;      // FP32: per-substrate field offsets [S]
   void* d_shift = nullptr;      // FP32: RN32(c2 * off) [S]
   int* d_active = nullptr;
@@ -50,6 +52,9 @@ struct bfvm_ctx {
   int* d_a_i = nullptr;
   double* d_ac = nullptr;      // ac1 | ac2 | ae2, [S][n] each
   int* d_nvalid = nullptr;
+  int* d_agent_pos = nullptr;  // [n] sorted position of each list index
+  void* d_delta = nullptr;     // bfvm_update_agents staging: idx [m] | c1, c2, e2 [m][S]
+  size_t cap_delta = 0;        // bytes of d_delta
   void* d_agent_scratch = nullptr;
   double* d_sample = nullptr;
   // internalized-substrate tracking (bfvm_set_agent_tracking)
@@ -78,6 +83,15 @@ struct bfvm_ctx {
   double* d_staging = nullptr; // reference-layout field, for host uploads/downloads
   double* d_grad = nullptr;    // gradients for host reads (bfvm_compute_gradients)
   double* d_bulk = nullptr;    // bulk supply | target | uptake rates, device layout (bfvm_set_bulk_rates)
+  // periodic FP64 mass-balance record (bfvm_set_mass_log): partials
+  // [S][512] | ring [capacity][S] | record count (u64)
+  double* d_mass = nullptr;
+  int mass_every = 0, mass_capacity = 0;
+  long long mass_steps = 0;    // steps since the log was enabled
+  // bfvm_step's CUDA graph: kGraphSteps LOD steps captured once and replayed
+  // while nothing it captured by value changes (graph_key)
+  cudaGraphExec_t step_graph = nullptr;
+  std::vector<long long> graph_key;
   // per-kernel timing: 4 events per recorded step
   bool timing = false;
   int timed_steps = 0;
@@ -116,6 +130,10 @@ int unpack_to_device_aos(bfvm_ctx* c, double* d_aos);
 // bfvm_lod2d.cu: the FP32 right-hand-side shift of the 2-D solver, brought
 // in line with the field offsets (no-op until the 2-D solver is set up).
 int update_shift_2d(bfvm_ctx* c);
+
+// bfvm_mass.cu: one mass-balance record of the current field, enqueued on
+// the solve's stream.
+int enqueue_mass_record(bfvm_ctx* c);
 
 // bfvm_capi.cu: Thomas factorization of one axis (half: 2-D constants).
 void thomas_axis_host(int n, int S, const double* D, const double* decay, double dt, double dx, double* denom,

@@ -190,6 +190,10 @@ int encode_field_maps(FieldMaps* maps, void* f, int elem_bytes, int nx, int ny, 
 
 template <typename T>
 cudaError_t launch_sweep_x(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st);
+// The bounded-wait limit (ns) of the kernels in bfvm_sweeps.cu (sweeps and
+// the batched engine) and in bfvm_tmem_sweeps.cu, on the current device.
+cudaError_t sweeps_set_wait_limit(unsigned long long ns);
+cudaError_t tmem_sweeps_set_wait_limit(unsigned long long ns);
 template <typename T>
 cudaError_t launch_sweep_y(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st);
 template <typename T>

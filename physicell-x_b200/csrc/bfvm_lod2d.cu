@@ -161,6 +161,7 @@ SweepParams<T> make_params_2d(bfvm_ctx* c) {
   }
   p.active = c->d_zero_active;
   p.shift = sizeof(T) == 4 ? c->d_shift2d : nullptr;
+  p.screen = c->screen_exact;  // the 2-D rows are {d, 1/d}: the reference-exact chain
   return p;
 }
 

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <cuda.h>
+#include <cuda_runtime.h>
 
 namespace bfvm {
 
@@ -14,10 +15,19 @@ enum : int {
   kDevTimeout = 1,  // an mbarrier wait gave up (TMA copy never completed)
 };
 
-// Upper bound on any single wait in these kernels, in globaltimer ns.  A
-// healthy TMA copy completes in microseconds; the bound exists so that a
-// broken copy can never hang the GPU.
-constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+// Upper bound on any single wait in these kernels, in globaltimer ns
+// (default 2 s).  A healthy TMA copy completes in microseconds; the bound
+// exists so that a broken copy or a dependency that is never met can never
+// hang the GPU: the waiting kernel records kDevTimeout and moves on.  Each
+// translation unit that includes this header has its own copy of the
+// variable, set through set_module_wait_limit (bfvm_set_wait_limit_ns).
+constexpr unsigned long long kDefaultWaitLimitNs = 2000000000ull;
+static __device__ unsigned long long g_wait_limit_ns = kDefaultWaitLimitNs;
+
+// This translation unit's copy of the wait limit on the current device.
+static inline cudaError_t set_module_wait_limit(unsigned long long ns) {
+  return cudaMemcpyToSymbol(g_wait_limit_ns, &ns, sizeof(ns));
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -62,8 +72,9 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
+  const unsigned long long limit = g_wait_limit_ns;
   while (!mbar_try_wait(bar, parity)) {
-    if (global_ns() - t0 > kWaitLimitNs) return false;
+    if (global_ns() - t0 > limit) return false;
   }
   return true;
 }

@@ -33,6 +33,25 @@ constexpr int kChunkX = 128 / static_cast<int>(sizeof(T));  // x-sweep chunk wid
 
 __device__ __forceinline__ uint64_t chunk_mask(int C) { return C >= 64 ? ~0ull : ((1ull << C) - 1ull); }
 
+// SweepParams::screen values: 0 no input screen (every numerator checked),
+// 1 the exactness screen of the reference-exact chain, kScreenFast the
+// short FP64 chain (bfvm_set_fp64_chain), which needs no screen.
+constexpr int kScreenFast = 2;
+
+// The short FP64 forward chain: with cf = {a = RN(c1 * r), r = RN(1/d)},
+// y_i = fma(a_i, y_{i-1}, v_i * r_i) -- one dependent FMA per element
+// instead of the reference's fma and correctly rounded division.  Not the
+// reference's bits: within a few units in the last place per sweep.
+template <int B, typename Put>
+__device__ __forceinline__ double forward_fast(const double (&v)[B], const double2 (&cf)[B], double y, Put&& put) {
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    y = __fma_rn(cf[q].x, y, __dmul_rn(v[q], cf[q].y));
+    put(q, y);
+  }
+  return y;
+}
+
 // Forward recurrence over B staged values; out[q] receives y_q and the
 // running value is returned.
 __device__ __forceinline__ double markstein(double t, double d, double r) {
@@ -55,6 +74,7 @@ __device__ __forceinline__ double markstein(double t, double d, double r) {
 template <int B, typename Put>
 __device__ __forceinline__ double forward_store(const double (&v)[B], const double2 (&cf)[B], double c1, double,
                                                 int screen, double y, Put&& put) {
+  if (screen == kScreenFast) return forward_fast<B>(v, cf, y, put);
   const double y0 = y;
 #pragma unroll
   for (int q = 0; q < B; ++q) {
@@ -122,6 +142,19 @@ __device__ __forceinline__ double forward_bare(const double (&v)[B], const doubl
   return y;
 }
 
+// The bare chain of the screen's mode: the short chain when screen is
+// kScreenFast, else the reference-exact one (forward_bare).
+template <int B, typename Put>
+__device__ __forceinline__ double forward_any(int screen, const double (&v)[B], const double2 (&cf)[B], double c1,
+                                              double y, Put&& put) {
+  if (screen == kScreenFast) return forward_fast<B>(v, cf, y, put);
+  return forward_bare<B>(v, cf, c1, y, put);
+}
+
+// Whether a tile whose inputs' minimum high word is hwmin needs no redo:
+// always under the short chain, else when the screen passed.
+__device__ __forceinline__ bool screen_clean(int screen, int hwmin);
+
 // The batch's inputs' minimum high word (signed): >= the high word of 2^-960
 // exactly when every input is >= 2^-960 (negative inputs sort first).
 template <int B>
@@ -137,6 +170,10 @@ __device__ __forceinline__ int batch_min_hi(const double (&v)[B]) {
   return hw[0];
 }
 constexpr int kHiTiny = 0x03F00000;  // high word of 2^-960
+
+__device__ __forceinline__ bool screen_clean(int screen, int hwmin) {
+  return screen == kScreenFast || (screen != 0 && hwmin >= kHiTiny);
+}
 
 // The forward chain with every numerator checked: the Markstein quotient
 // where it is exact, IEEE division for a numerator of -0 or a nonzero value

@@ -226,7 +226,7 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
     RowPut<T> put{crow, sw};
     if constexpr (!kF32<T>) {
       if (tile_screen) {
-        y = forward_bare<W>(v, cf, c1, y, put);
+        y = forward_any<W>(screen, v, cf, c1, y, put);
         hwmin = min(hwmin, batch_min_hi<W>(v));
         return;
       }
@@ -258,7 +258,7 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
     // anywhere is redone from its inputs -- the field still holds them (this
     // tile's results are stored only by the back substitution) -- pinned as
     // the staged row was, with every numerator checked.
-    if (tile_screen && __syncthreads_or(!(screen != 0 && hwmin >= kHiTiny))) {
+    if (tile_screen && __syncthreads_or(!screen_clean(screen, hwmin))) {
       if (!face && valid) {
         const T* src = p.f + ((static_cast<size_t>(s) * nz + k) * ny + j) * p.nxp;
         y = -0.0;
@@ -473,7 +473,7 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
     if constexpr (kF32<T>) {
       y = forward_store<R>(v, cf, c1, shift, screen, y, put);
     } else {
-      y = forward_bare<R>(v, cf, c1, y, put);
+      y = forward_any<R>(screen, v, cf, c1, y, put);
       hwmin = min(hwmin, batch_min_hi<R>(v));
     }
   };
@@ -505,7 +505,7 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
     // The screen, once per tile: a line with an input below 2^-960 (or
     // negative) anywhere is redone from its inputs, which are still in the
     // field (this tile's results are stored only by the back substitution).
-    if (__syncthreads_or(!(screen != 0 && hwmin >= kHiTiny))) {
+    if (__syncthreads_or(!screen_clean(screen, hwmin))) {
       if (!face && i < nx) {
         const size_t row_stride = (AXIS == 1) ? static_cast<size_t>(p.nxp) : static_cast<size_t>(p.nxp) * p.ny;
         const T* src = (AXIS == 1) ? p.f + ((static_cast<size_t>(s) * p.nz + m) * p.ny) * p.nxp + i
@@ -828,7 +828,7 @@ __global__ void __launch_bounds__(64 * kMaxRings<T>, 1) sweep_yz_ring_kernel(con
       if constexpr (kF32<T>) {
         y = forward_store<R>(v, cf, c1, shift, screen, y, put);
       } else {
-        y = forward_bare<R>(v, cf, c1, y, put);
+        y = forward_any<R>(screen, v, cf, c1, y, put);
         hwmin = min(hwmin, batch_min_hi<R>(v));
       }
     };
@@ -855,7 +855,7 @@ __global__ void __launch_bounds__(64 * kMaxRings<T>, 1) sweep_yz_ring_kernel(con
       // The screen, once per tile: a line with an input below 2^-960 (or
       // negative) anywhere is redone from its inputs, which are still in the
       // field (this tile's results are stored only by the back substitution).
-      if (__any_sync(0xffffffffu, !(screen != 0 && hwmin >= kHiTiny))) {
+      if (__any_sync(0xffffffffu, !screen_clean(screen, hwmin))) {
         if (!face && i < nx) {
           const size_t row_stride = (AXIS == 1) ? static_cast<size_t>(p.nxp)
                                                 : static_cast<size_t>(p.nxp) * p.ny;
@@ -1243,9 +1243,10 @@ __global__ void __launch_bounds__(kBatchTile) batch_step_kernel(const BatchHeade
         const int* cnt = done + (axis - 1) * cap + e;
         if (ld_acquire_gpu(cnt) < need) {
           const unsigned long long t0 = global_ns();
+          const unsigned long long limit = g_wait_limit_ns;
           while (ld_acquire_gpu(cnt) < need) {
             __nanosleep(128);
-            if (global_ns() - t0 > kWaitLimitNs) {
+            if (global_ns() - t0 > limit) {
               atomicExch(status, kDevTimeout);
               break;
             }
@@ -1613,5 +1614,7 @@ template cudaError_t launch_batch_sweeps<double>(const BatchHeader*, const Batch
                                                  const int[3], const size_t[3], cudaStream_t);
 template cudaError_t launch_batch_sweeps<float>(const BatchHeader*, const BatchEnv<float>*, const int*, int,
                                                 const int[3], const size_t[3], cudaStream_t);
+
+cudaError_t sweeps_set_wait_limit(unsigned long long ns) { return set_module_wait_limit(ns); }
 
 }  // namespace bfvm

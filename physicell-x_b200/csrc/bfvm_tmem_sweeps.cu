@@ -182,9 +182,9 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
             if (rb + q >= n) v[q] = 1.0;
         }
         if (flow)
-          y = forward_bare<R>(v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
+          y = forward_any<R>(screen, v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
         else
-          y = forward_bare<R>(v, cf, c1, y, [&](int q, double val) { cb[q * TI] = val; });
+          y = forward_any<R>(screen, v, cf, c1, y, [&](int q, double val) { cb[q * TI] = val; });
         hwmin = min(hwmin, batch_min_hi<R>(v));
       } else if (flow) {
 #pragma unroll
@@ -223,7 +223,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
     // The screen, once per tile: a line with an input below 2^-960 (or
     // negative) anywhere is redone from its inputs, which are still in the
     // field (this tile's results are stored only by the back substitution).
-    if (__any_sync(kAll, !(screen != 0 && hwmin >= kHiTiny))) {
+    if (__any_sync(kAll, !screen_clean(screen, hwmin))) {
       y = -0.0;
       for (int c = 0; c < C; ++c) {
         const int rb = c * CH;
@@ -573,10 +573,10 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
             if (i0 + q >= nx) v[q] = 1.0;
         }
         if (flow) {
-          y = forward_bare<W>(v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
+          y = forward_any<W>(screen, v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
         } else {
           RowPut<double> put{crow, sw};
-          y = forward_bare<W>(v, cf, c1, y, put);
+          y = forward_any<W>(screen, v, cf, c1, y, put);
         }
         hwmin = min(hwmin, batch_min_hi<W>(v));
       } else if (flow) {
@@ -616,7 +616,7 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
     // anywhere is redone from its inputs -- the field still holds them (this
     // tile's results are stored only by the back substitution) -- pinned as
     // above, with every numerator checked.
-    if (__any_sync(kAll, !(screen != 0 && hwmin >= kHiTiny))) {
+    if (__any_sync(kAll, !screen_clean(screen, hwmin))) {
       const double* src = plane + static_cast<size_t>(lane_on ? j : 0) * p.nxp;
       y = -0.0;
       for (int c = 0; c < C; ++c) {
@@ -988,6 +988,8 @@ template cudaError_t launch_tmem_yz<1>(const CUtensorMap&, const SweepParams<dou
                                        cudaStream_t, bool*);
 template cudaError_t launch_tmem_yz<2>(const CUtensorMap&, const SweepParams<double>&, const SweepConfig&,
                                        cudaStream_t, bool*);
+
+cudaError_t tmem_sweeps_set_wait_limit(unsigned long long ns) { return set_module_wait_limit(ns); }
 
 }  // namespace bfvm
 

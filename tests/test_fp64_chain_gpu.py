@@ -1,0 +1,88 @@
+"""The short FP64 chain (bfvm_set_fp64_chain(ctx, 1)) against the oracle:
+within the 1e-12 relative per-voxel bound the FP64 path is held to, on the
+benchmark configurations' shapes and step counts, under every sweep kernel
+(per-tile, persistent, tensor memory, batched)."""
+import numpy as np
+import pytest
+
+from bfvm import Batch, Microenvironment
+from bfvm import workloads as W
+from pyoracle import Port
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12  # relative per voxel (floor 1e-30 on the magnitude)
+
+
+def _per_voxel(got, ref):
+    return float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-30)))
+
+
+def test_short_chain_cube50_all_steps_within_bound():
+    wl = W.cube50(steps=1000)
+    me = Microenvironment.from_workload(wl)
+    me.set_fp64_chain(1)
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    got = me.download_field()
+    err = _per_voxel(got, Port.run(wl))
+    assert 0.0 < err <= FP64_TOL, err
+
+
+@pytest.mark.parametrize("sched,tmem", [(0, 0), (1, 1), (2, 2), (2, 0)])
+def test_short_chain_every_kernel(sched, tmem):
+    wl = W.small_random(821, nx=70, ny=257, nz=40, S=3, n_agents=3000, steps=20, stack=True)
+    expect = Port.run(wl)
+    me = Microenvironment.from_workload(wl)
+    me.set_sweep_schedule(sched)
+    me.set_sweep_tmem(tmem)
+    me.set_fp64_chain(1)
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    assert _per_voxel(me.download_field(), expect) <= FP64_TOL
+    # back to the reference's arithmetic: the reference's bits again
+    me.upload_field(wl.field0)
+    me.set_fp64_chain(0)
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    np.testing.assert_array_equal(me.download_field(), expect)
+    me.close()
+
+
+def test_short_chain_in_the_batch():
+    wls = [W.uneven_env(i, steps=30) for i in range(4)]
+    b = Batch("fp64")
+    mes = []
+    for wl in wls:
+        me = Microenvironment.from_workload(wl)
+        me.set_fp64_chain(1)
+        b.add(me)
+        mes.append(me)
+    b.step(30, sources=True)
+    b.synchronize()
+    for wl, me in zip(wls, mes):
+        assert _per_voxel(me.download_field(), Port.run(wl)) <= FP64_TOL, wl.name
+    b.close()
+
+
+def test_short_chain_rejected_for_fp32():
+    wl = W.small_random(822, steps=1)
+    me = Microenvironment.from_workload(wl, precision="fp32")
+    with pytest.raises(Exception):
+        me.set_fp64_chain(1)
+    me.close()
+
+
+def test_short_chain_cube200_all_steps_against_reference_sample(golden_dir):
+    """cube200 for all 500 steps with the short chain: the 4096 sampled
+    voxels of the reference's own final field (its golden fixture) agree to
+    1e-12 relative, and the per-substrate sums to 1e-12."""
+    import os
+
+    g = np.load(os.path.join(golden_dir, "cube200_500.npz"))
+    wl = W.cube200(steps=500)
+    me = Microenvironment.from_workload(wl)
+    me.set_fp64_chain(1)
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    out = me.download_field()
+    me.close()
+    idx = g["sample_idx"]
+    assert _per_voxel(out[idx], g["sample_val"]) <= FP64_TOL
+    np.testing.assert_allclose(out.reshape(-1, wl.S).sum(axis=0), g["sums"], rtol=FP64_TOL)

@@ -83,3 +83,23 @@ def test_one_at_a_time_path_gives_the_same_fp64_results():
         assert np.array_equal(r.field, got[r.rid])
     summ = st.summary()
     assert summ["requests"] == 4 and summ["p99_s"] >= summ["p50_s"] > 0
+
+
+@pytest.mark.gpu
+def test_cancelled_request_leaves_the_others_unchanged():
+    """One request is cancelled while it runs in the batch; every other
+    result is bit-identical to the same request served alone."""
+    reqs = _requests(5, seed=51, steps_lo=60, steps_hi=90)
+    srv = Server("fp64", quantum=8)
+
+    def on_quantum(server, quanta):
+        if quanta == 3:
+            server.cancel(2)
+
+    st = srv.run(reqs, on_quantum=on_quantum)
+    srv.close()
+    assert [rid for rid, _ in st.cancelled] == [2]
+    assert 0 < st.cancelled[0][1] < reqs[2].workload.steps
+    assert sorted(r.rid for r in st.results) == [0, 1, 3, 4]
+    for res in st.results:
+        assert np.array_equal(res.field, _alone(reqs[res.rid], "fp64")), res.rid

@@ -128,3 +128,38 @@ def test_later_arrivals_wait_for_their_time(fakes):
     assert all(r.latency > 0 for r in st.results)
     s = st.summary()
     assert s["requests"] == 2 and s["updates"] == 2 * 5 * 1000 and s["wall_s"] > 0
+
+
+def test_cancellation_frees_the_solve_and_leaves_the_others_exact(fakes):
+    """Request 1 is cancelled after the second quantum (running) and request
+    3 before it is admitted (waiting); both are reported with the steps they
+    got, their solves are freed, and every other request runs exactly its
+    step count."""
+    reqs = [serve.SolveRequest(i, _workload(steps, nbytes), arrival=0.0)
+            for i, (steps, nbytes) in enumerate([(300, 30), (500, 30), (90, 30), (200, 60), (40, 10)])]
+    srv = serve.Server(budget_bytes=100, quantum=32)
+
+    def on_quantum(server, quanta):
+        if quanta == 2:
+            server.cancel(1)
+            server.cancel(3)
+
+    st = srv.run(reqs, clock=FakeClock(), on_quantum=on_quantum)
+    done = dict(st.cancelled)
+    assert set(done) == {1, 3}
+    assert done[1] == 64 and done[3] == 0  # two quanta of 32, and never admitted
+    assert sorted(r.rid for r in st.results) == [0, 2, 4]
+    by_steps = {me.wl.steps: me for me in fakes}
+    assert 200 not in by_steps  # request 3 was never created
+    assert by_steps[500].closed and by_steps[500].steps == 64
+    for steps in (300, 90, 40):
+        assert by_steps[steps].steps == steps and by_steps[steps].closed
+    assert st.summary()["cancelled"] == 2
+
+
+def test_cancelling_an_unknown_or_finished_request_changes_nothing(fakes):
+    reqs = [serve.SolveRequest(0, _workload(10, 10)), serve.SolveRequest(1, _workload(20, 10))]
+    srv = serve.Server(budget_bytes=100, quantum=8)
+    srv.cancel(99)
+    st = srv.run(reqs, clock=FakeClock())
+    assert sorted(r.rid for r in st.results) == [0, 1] and st.cancelled == []

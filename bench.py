@@ -5,16 +5,22 @@ Metric: voxel*substrate updates per second per LOD step (N*S*steps / time).
 Workload (one GPU): cube200 -- 200^3 voxels, dx=10 um, 4 substrates with
 log-uniform D in [1e2,1e5] and decay in [1e-3,1] (substrate 0 Dirichlet 38
 on all faces), 100,000 agents with uptake in [0,10] and secretion in [0,1],
-FP64, dt=0.01 min.  One bench step = one LOD step: agent sources fused into
-the x sweep, then the y and z sweeps (three kernels).
+FP64, dt=0.01 min.  One bench step = one LOD step: the standalone agent
+source kernel, then the x, y and z sweeps (four kernels), with the
+reference's arithmetic (bit-identical results).
 
   value  whole-job updates/s with the field resident in HBM (CUDA events on
          the solve's stream, max over ranks).  The field is 256 MB, larger
          than the 126 MB L2, so no flush is needed between steps.
-  e2e    the same metric through the C ABI with host buffers: every step
-         uploads the agent list (voxel + c1/c2/e2 from pinned host memory),
-         re-bins it on the device, runs the LOD step and reads the densities
-         at every agent's voxel back to the host.
+  e2e    the same metric through the C ABI with host buffers, as a
+         PhysiCell loop drives it: every step sends the constants of the 1%
+         of agents whose volume changed (bfvm_update_agents), every 10th
+         step the whole moved agent list (bfvm_set_agents: voxels and
+         constants, re-binned on the device), runs the LOD step and reads
+         the densities at every agent's voxel back to the host.
+  fp64_short_chain  the same resident step with the opt-in short FP64
+         forward chain (bfvm_set_fp64_chain), which is within 1e-12 of the
+         reference per voxel rather than bit-identical.
 
 Multi-GPU: one process per GPU, each advancing its own replica of the
 workload (the solve does not shard; replicas only), value summed.
@@ -40,7 +46,7 @@ METRIC = "voxel·substrate updates/s per LOD step"
 UNIT = "voxel·substrate updates/s"
 WORKLOAD = ("cube200: 200x200x200 voxels (dx=10 um), 4 substrates, 100000 agents, FP64, dt=0.01 min; "
             "one LOD step = agent sources (standalone kernel, timed with the x sweep) + x/y/z Thomas "
-            "sweeps with Dirichlet pins")
+            "sweeps with Dirichlet pins, the reference's arithmetic (bit-identical)")
 
 # DRAM bytes per launch of each timed interval (dram__bytes_read.sum +
 # dram__bytes_write.sum) from one ncu capture of this workload at the current
@@ -190,9 +196,11 @@ def cpu_baseline_sample(wl, budget_s=10.0):
             pyoracle.Port.lod_step(field, wl.shape, wl.D, wl.decay, wl.dt, wl.dx, wl.dirichlet_active, dv, threads)
         dt = time.perf_counter() - t0
         kind = "port"
-    return {"value": wl.n_values * steps / dt, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{steps} LOD steps of cube200 (sources + _BLOCKING sweeps, OpenMP {threads} threads), "
-                      f"{dt:.2f} s"}
+    out = {"value": wl.n_values * steps / dt, "unit": UNIT, "cores": threads, "kind": kind,
+           "sample": f"{steps} LOD steps of cube200 (sources + _BLOCKING sweeps, OpenMP {threads} threads), "
+                     f"{dt:.2f} s"}
+    out.update(host_cpu())
+    return out
 
 
 def run_reference_arm(args):
@@ -228,10 +236,14 @@ def run_reference_arm(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "solver": "diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING",
+            "config": {"workload": WORKLOAD, "parallelism": f"replicas x{args.gpus}",
+                       "l2": "inputs larger than L2 (256 MB field per GPU), no flush",
+                       "voxels": wl.n_voxels, "substrates": wl.S, "agents": wl.n_agents,
+                       "solver": "diffusion_decay_solver__constant_coefficients_LOD_3D_BLOCKING",
                        "sources": f"simulate_cell_sources_and_sinks, OpenMP {threads} threads"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"{args.steps} timed LOD steps of cube200 after {max(1, args.warmup)} warm-up"},
+            "cpu_baseline": dict({"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                                  "sample": f"{args.steps} timed LOD steps of cube200 after "
+                                            f"{max(1, args.warmup)} warm-up"}, **host_cpu()),
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -277,6 +289,55 @@ def run_suite(args):
     return 0
 
 
+def host_cpu():
+    """The host CPU: model name and physical cores (distinct core ids per
+    socket in /proc/cpuinfo), for the CPU baseline's record."""
+    model, cores = None, set()
+    try:
+        phys = core = None
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                k, _, v = ln.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "model name" and model is None:
+                    model = v
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    core = v
+                elif not k and phys is not None and core is not None:
+                    cores.add((phys, core))
+                    phys = core = None
+        if phys is not None and core is not None:
+            cores.add((phys, core))
+    except OSError:
+        pass
+    return {"cpu_model": model, "physical_cores": len(cores) or None, "logical_cpus": os.cpu_count()}
+
+
+def time_resident(me, steps, stream):
+    """Time `steps` resident LOD steps with sources on the solve's stream
+    (CUDA events), with the per-kernel split; returns (ms per step, per-kernel
+    ms [3], launches)."""
+    import torch
+
+    from bfvm import kernel_launches
+
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches0 = kernel_launches()
+    me.timing_enable(True)
+    ev0.record(stream)
+    for _ in range(steps):
+        me.simulate_diffusion_decay(1, sources=True)
+    ev1.record(stream)
+    me.synchronize()
+    torch.cuda.synchronize()
+    me.timing_enable(False)
+    ms_xyz, nrec = me.timing_read()
+    return ev0.elapsed_time(ev1) / steps, ms_xyz / max(1, nrec), kernel_launches() - launches0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -299,7 +360,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    from bfvm import Microenvironment, kernel_launches
+    from bfvm import Microenvironment
     from bfvm import workloads as W
 
     wl = W.cube200()
@@ -316,83 +377,128 @@ def main():
     me.synchronize()
 
     # ---- timed region (resident field) -------------------------------------
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    launches0 = kernel_launches()
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        me.timing_enable(True)
-        ev0.record(stream)
-        for _ in range(args.steps):
-            me.simulate_diffusion_decay(1, sources=True)
-        ev1.record(stream)
-        me.synchronize()
-        torch.cuda.synchronize()
-        me.timing_enable(False)
+        ms_step, per_kernel_ms, launches = time_resident(me, args.steps, stream)
     barrier()
-    launches = kernel_launches() - launches0
-    ms_total = ev0.elapsed_time(ev1)
-    ms_xyz, nrec = me.timing_read()
-    ms_step = ms_total / args.steps
     if dist is not None:
         ms_step = max_over_ranks(ms_step, dist, "cuda")
     value = world * N * S / (ms_step * 1e-3)
 
     # ---- roofline of the dominant kernel -------------------------------------
     eb = 8 if args.precision == "fp64" else 4
-    per_kernel_ms = ms_xyz / max(1, nrec)
     names = ["sweep_x (+sources, pins)", "sweep_y (+pins)", "sweep_z (+pins)"]
     field_bytes = 2 * N * S * eb
     coef_bytes = [3 * wl.nx * S * 8, 3 * wl.ny * S * 8, 3 * wl.nz * S * 8]
     agent_bytes = A * (4 + 3 * S * 8) + (wl.ny * wl.nz + 1) * 4
     alg = [field_bytes + coef_bytes[0] + agent_bytes, field_bytes + coef_bytes[1], field_bytes + coef_bytes[2]]
-    dom = int(np.argmax(per_kernel_ms))
     peak, peak_kind = load_peaks()
-    achieved = alg[dom] / (per_kernel_ms[dom] * 1e-3) / 1e9
-    traffic = NCU_TRAFFIC.get((args.precision, dom))
     step_bytes = sum(alg)
-    roofline = {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+
+    def roofline_of(kernel_ms, step_ms):
+        dom = int(np.argmax(kernel_ms))
+        achieved = alg[dom] / (kernel_ms[dom] * 1e-3) / 1e9
+        return {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": NCU_TRAFFIC.get((args.precision, dom)),
                 "algorithmic_bytes_per_launch": alg[dom],
-                "per_kernel": [{"kernel": names[k], "ms": per_kernel_ms[k],
-                                "GB/s": alg[k] / (per_kernel_ms[k] * 1e-3) / 1e9} for k in range(3)],
-                "step_frac": (step_bytes / (ms_step * 1e-3) / 1e9) / peak}
+                "per_kernel": [{"kernel": names[k], "ms": kernel_ms[k],
+                                "GB/s": alg[k] / (kernel_ms[k] * 1e-3) / 1e9} for k in range(3)],
+                "step_frac": (step_bytes / (step_ms * 1e-3) / 1e9) / peak}
+
+    roofline = roofline_of(per_kernel_ms, ms_step)
+
+    # ---- the opt-in short FP64 chain, same resident step ----------------------
+    short = None
+    if args.precision == "fp64":
+        me.set_fp64_chain(1)
+        me.simulate_diffusion_decay(3, sources=True)
+        me.synchronize()
+        torch.cuda.synchronize()
+        ms_short, kms_short, _ = time_resident(me, args.steps, stream)
+        if dist is not None:
+            ms_short = max_over_ranks(ms_short, dist, "cuda")
+        me.set_fp64_chain(0)
+        short = {"value": world * N * S / (ms_short * 1e-3), "unit": UNIT, "ms_per_step": ms_short,
+                 "roofline": roofline_of(kms_short, ms_short),
+                 "arithmetic": "forward y = fma(RN(c1/d), y, v*RN(1/d)); within 1e-12 relative per voxel of the "
+                               "reference (tests/test_fp64_chain_gpu.py), not bit-identical"}
+
+    # ---- gradients of the field (compute_all_gradient_vectors), resident -----
+    g_out = torch.empty(N * S * 3, dtype=torch.float64, device=torch.device("cuda", local))
+    for _ in range(2):
+        me.compute_all_gradient_vectors_device(g_out.data_ptr())
+    ge0, ge1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g_reps = 20
+    ge0.record(stream)
+    for _ in range(g_reps):
+        me.compute_all_gradient_vectors_device(g_out.data_ptr())
+    ge1.record(stream)
+    me.synchronize()
+    g_ms = ge0.elapsed_time(ge1) / g_reps
+    g_bytes = N * S * (eb + 3 * 8)
+    gradients = {"ms": g_ms, "algorithmic_bytes": g_bytes, "GB/s": g_bytes / (g_ms * 1e-3) / 1e9,
+                 "frac": g_bytes / (g_ms * 1e-3) / 1e9 / peak, "peak_source": peak_kind,
+                 "what": "bfvm_compute_gradients_device: the field read once, [voxel][S][3] FP64 written"}
+    del g_out
 
     # ---- e2e through the C ABI with host buffers -----------------------------
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     c1, c2, e2 = _agent_constants(wl)
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
-    h_vox, h_c1, h_c2, h_e2 = pin(wl.agent_voxel), pin(c1), pin(c2), pin(e2)
+    rng = np.random.Generator(np.random.PCG64(17))
+    # two agent layouts: the workload's, and every agent moved to a neighbouring voxel
+    moved = wl.agent_voxel.astype(np.int64) + rng.choice([-1, 1], A) * rng.choice([1, wl.nz, wl.ny * wl.nz], A)
+    moved = np.where((moved >= 0) & (moved < N), moved, wl.agent_voxel).astype(np.int32)
+    h_vox = [pin(wl.agent_voxel), pin(moved)]
+    h_c1, h_c2, h_e2 = pin(c1), pin(c2), pin(e2)
+    # eight rotating sets of the 1% of agents whose volume changed this step, with their new constants
+    n_delta = max(1, A // 100)
+    deltas = []
+    for _ in range(8):
+        idx = np.sort(rng.choice(A, n_delta, replace=False)).astype(np.int32)
+        g = 1.0 + 0.01 * rng.random((n_delta, 1))
+        deltas.append(tuple(pin(x) for x in (idx, c1[idx] * g, 1.0 + (c2[idx] - 1.0) * g, e2[idx])))
     h_out = pin(np.zeros((A, S)))
     from bfvm import _lib
     import ctypes as C
 
     L = me.L
     vp = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+    move_every = 10
 
-    def e2e_step():
-        _lib.check(L.bfvm_set_agents(me.h, A, vp(h_vox), None, vp(h_c1), vp(h_c2), vp(h_e2)), "bfvm_set_agents")
+    def e2e_step(k):
+        if k % move_every == 0:
+            _lib.check(L.bfvm_set_agents(me.h, A, vp(h_vox[(k // move_every) % 2]), None, vp(h_c1), vp(h_c2),
+                                         vp(h_e2)), "bfvm_set_agents")
+        else:
+            d = deltas[k % len(deltas)]
+            _lib.check(L.bfvm_update_agents(me.h, n_delta, *[vp(x) for x in d]), "bfvm_update_agents")
         _lib.check(L.bfvm_step(me.h, 1, _lib.BFVM_STEP_SOURCES), "bfvm_step")
         _lib.check(L.bfvm_sample_agents(me.h, vp(h_out)), "bfvm_sample_agents")
 
-    e2e_steps = args.e2e_steps or args.steps
-    for _ in range(3):
-        e2e_step()
+    e2e_steps = max(move_every, args.e2e_steps or args.steps)
+    e2e_steps -= e2e_steps % move_every
+    for k in range(move_every):
+        e2e_step(k)
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        e2e_step()
+    for k in range(e2e_steps):
+        e2e_step(k)
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     if dist is not None:
         e2e_s = max_over_ranks(e2e_s, dist, "cuda")
-    h2d = A * 4 + 3 * A * S * 8
+    full_h2d = A * 4 + 3 * A * S * 8
+    delta_h2d = n_delta * 4 + 3 * n_delta * S * 8
+    h2d = (full_h2d + (move_every - 1) * delta_h2d) / move_every
     d2h = A * S * 8
     e2e = {"value": world * N * S / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "ms_per_step": e2e_s * 1e3,
-           "path": "bfvm_set_agents (pinned host) + bfvm_step + bfvm_sample_agents (to pinned host)"}
+           "path": f"bfvm_update_agents ({n_delta} agents, pinned host) on 9 of 10 steps, bfvm_set_agents (all "
+                   f"{A} moved agents) on every 10th, + bfvm_step + bfvm_sample_agents (to pinned host), "
+                   "wall clock"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -411,8 +517,9 @@ def main():
                 "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}",
                            "l2": "inputs larger than L2 (256 MB field per GPU), no flush",
                            "voxels": N, "substrates": S, "agents": A},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clk.summary()}
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "fp64_short_chain": short,
+                "gradients": gradients,
+                "gpu_launches": launches, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     return 0
 

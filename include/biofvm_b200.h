@@ -395,7 +395,9 @@ int bfvm_get_sweep_schedule(bfvm_ctx* ctx, int* persistent);
  * sweep, within the 1e-12 relative per-voxel bound the FP64 path is held to
  * (the tests measure it against the oracle).  The back substitution, the
  * sources and the pins are the same in both.  The 2-D solver always uses
- * chain 0.  FP64 solves only (BFVM_ERR_STATE otherwise). */
+ * chain 0.  An FP32 solve's recurrence is FP64 too: chain 0 there is
+ * t = fma(c1, y, v - shift), y = t * RN(1/d); chain 1 is
+ * y = fma(c1 * RN(1/d), y, (v - shift) * RN(1/d)). */
 int bfvm_set_fp64_chain(bfvm_ctx* ctx, int chain);
 int bfvm_get_fp64_chain(bfvm_ctx* ctx, int* chain);
 

@@ -275,7 +275,7 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
   for (int s = 0; s < S; ++s)
     if (!(D[s] >= 0.0) || !(decay[s] >= 0.0)) c->screen_exact = 0;
   const bool fast = c->prec == BFVM_FP64 && c->fp64_chain == 1;
-  c->screen = fast ? 2 : c->screen_exact;  // 2: the short chain (kScreenFast)
+  c->screen = c->fp64_chain == 1 ? 2 : c->screen_exact;  // 2: the short chain (kScreenFast)
   const int n_axis[3] = {c->nx, c->ny, c->nz};
   size_t dr_off[3], cu_off[3];
   const size_t bytes = coef_bytes(c, dr_off, cu_off);
@@ -1140,7 +1140,6 @@ extern "C" int bfvm_set_fused_sources(bfvm_ctx* c, int fused) {
 
 extern "C" int bfvm_set_fp64_chain(bfvm_ctx* c, int chain) {
   if (!c || (chain != 0 && chain != 1)) return BFVM_ERR_ARG;
-  if (c->prec != BFVM_FP64) return BFVM_ERR_STATE;
   if (chain == c->fp64_chain) return BFVM_OK;
   DeviceGuard g(c->device);
   BFVM_CUDA(cudaStreamSynchronize(c->stream));

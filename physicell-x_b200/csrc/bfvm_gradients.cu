@@ -12,15 +12,222 @@
 //
 // Output layout is the reference's gradient_vectors: out[(v*S + d)*3 + axis]
 // with v = (i*ny + j)*nz + k, z fastest, while the device field is x
-// fastest.  A CTA owns 32 consecutive z by 8 consecutive x of one y-plane:
-// per substrate it stages that block with a one-voxel halo in x and z, and
-// the block's two y neighbours, in shared memory (rows of x read from the
-// field), computes the gradients of its 256 voxels into a shared-memory
-// output block, and then each warp writes one x row's 32 voxels -- a
-// contiguous run of the output -- for up to kGroup substrates at a time.
+// fastest, so the kernel transposes through shared memory.
+//
+// gradient_plane_kernel (used whenever its tensor map encodes): a CTA owns
+// 32 consecutive x by 8 consecutive z and walks a range of y planes.  Each
+// plane's block -- with a one-voxel halo in z and the x halo rounded out to
+// 16-byte boundaries, up to 4 substrates -- arrives by one TMA box load into
+// a ring of four plane slots, so planes j-1, j, j+1 are resident while j+2
+// loads and every field value is read from HBM about once (the halo and the
+// planes shared by neighbouring y ranges aside).  The 256 threads (lane = x,
+// warp = z) compute the plane's gradients into a shared-memory block ordered
+// like the output, which the CTA then writes as contiguous runs (one x row's
+// 8 voxels x 3 x substrates per run).  Algorithmic bytes per voxel and
+// substrate: 8 read + 24 written (FP64 field).
+//
+// gradient_kernel is the earlier form (32 z by 8 x of one plane per CTA,
+// rows read with plain loads), kept for grids whose map does not encode.
+#include <algorithm>
+
 #include "bfvm_ctx.h"
+#include "bfvm_ptx.cuh"
 
 namespace {
+
+constexpr int kGTX = 32;     // x per CTA (one warp's lanes)
+constexpr int kGTZ = 8;      // z per CTA (one per warp)
+constexpr int kGSlots = 4;   // plane slots: j-1, j, j+1 resident, j+2 loading
+constexpr int kGBoxZ = kGTZ + 2;
+template <typename T>
+constexpr int kGBoxX = sizeof(T) == 8 ? 36 : 40;  // x extent of a plane box (16-byte aligned origin)
+template <typename T>
+constexpr int kGX0 = sizeof(T) == 8 ? 2 : 4;      // box x origin below the CTA's first x
+
+template <typename T, int NS>
+__host__ __device__ constexpr size_t grad_slot_bytes() {
+  return (static_cast<size_t>(kGBoxX<T>) * kGBoxZ * NS * sizeof(T) + 127) / 128 * 128;
+}
+template <int NS>
+__host__ __device__ constexpr int grad_stage_stride() {  // doubles per x row of the output block (odd: no bank conflicts)
+  return kGTZ * 3 * NS + 1;
+}
+template <typename T, int NS>
+__host__ __device__ constexpr size_t grad_smem_bytes() {
+  return 128 + 128 + kGSlots * grad_slot_bytes<T, NS>() + sizeof(double) * kGTX * grad_stage_stride<NS>();
+}
+
+// Gradients of substrates s0 .. s0+ns-1 (ns <= NS) for the planes [jb, je)
+// of one (32 x, 8 z) column of the grid; planes come from `map` (the field,
+// box {kGBoxX, 1, 10, NS}: NS substrates from s0, those past S zero-filled).
+template <typename T, int NS>
+__global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_constant__ CUtensorMap map, int nx, int ny,
+                                                             int nz, int S, int s0, int jc,
+                                                             const double* __restrict__ off, double dx,
+                                                             double* __restrict__ out, int* status) {
+  const int ns = min(NS, S - s0);
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t a0 = bfvm::smem_u32(smem_raw);
+  unsigned char* base = smem_raw + (((a0 + 127u) & ~127u) - a0);  // 128-byte aligned (TMA destinations)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base);
+  unsigned char* slots = base + 128;
+  double* stg = reinterpret_cast<double*>(slots + kGSlots * grad_slot_bytes<T, NS>());
+  constexpr int BX = kGBoxX<T>;
+  constexpr int X0 = kGX0<T>;
+  constexpr int PS = BX * kGBoxZ;  // elements per substrate in a slot
+  constexpr uint32_t kBoxBytes = static_cast<uint32_t>(BX * kGBoxZ * NS * sizeof(T));
+  constexpr int SX = grad_stage_stride<NS>();
+  constexpr int RUN = kGTZ * 3 * NS;  // output doubles per x row of the block
+  const int i0 = blockIdx.x * kGTX, k0 = blockIdx.y * kGTZ;
+  const int jb = blockIdx.z * jc;
+  const int je = min(ny, jb + jc);
+  const int tid = threadIdx.x, lane = tid & 31, wz = tid >> 5;
+  const int jlast = min(je, ny - 1);  // last plane this CTA reads
+  const int jfirst = max(jb - 1, 0);  // first plane this CTA reads
+  // plane p lives in slot (p - jfirst) % 4 and is that slot's ((p - jfirst) / 4)-th load
+  auto slot_of = [&](int p) { return (p - jfirst) & (kGSlots - 1); };
+  auto parity_of = [&](int p) { return static_cast<uint32_t>(((p - jfirst) >> 2) & 1); };
+  auto issue = [&](int p) {
+    const int sl = slot_of(p);
+    const uint32_t bar = bfvm::smem_u32(&bars[sl]);
+    bfvm::mbar_expect_tx(bar, kBoxBytes);
+    bfvm::tma_load_4d(bfvm::smem_u32(slots + sl * grad_slot_bytes<T, NS>()), &map, bar, i0 - X0, p, k0 - 1, s0);
+  };
+  if (tid == 0) {
+    bfvm::prefetch_tmap(&map);
+    for (int q = 0; q < kGSlots; ++q) bfvm::mbar_init(bfvm::smem_u32(&bars[q]), 1);
+    bfvm::fence_barrier_init();
+  }
+  __syncthreads();
+  int issued = min(jfirst + kGSlots - 1, jlast);  // planes jfirst .. issued are (being) loaded
+  if (tid == 0)
+    for (int p = jfirst; p <= issued; ++p) issue(p);
+  bool ok = true;
+  int waited = jfirst - 1;  // planes jfirst .. waited have landed
+  auto wait_plane = [&](int p) {
+    if (ok) ok = bfvm::mbar_wait(bfvm::smem_u32(&bars[slot_of(p)]), parity_of(p));
+    if (ok) waited = p;
+  };
+  if (jb > 0) wait_plane(jb - 1);
+  const double two_dx = dx * 2.0;
+  // g = a; g -= b; g /= h  (BioFVM_microenvironment.cpp:1480-1482 and the
+  // matching lines of every end cap and interior loop)
+  auto grad = [](double a, double b, double h) {
+    double g = a;
+    g -= b;
+    return g / h;
+  };
+  const int i = i0 + lane, k = k0 + wz;
+  const int ix = lane + X0, iz = wz + 1;  // this thread's voxel in a slot
+  for (int j = jb; j < je; ++j) {
+    if (j == jb) wait_plane(j);
+    if (j + 1 < ny) wait_plane(j + 1);
+    if (!__syncthreads_and(ok)) break;  // a plane never landed: stop (status set below)
+    const T* P1 = reinterpret_cast<const T*>(slots + slot_of(j) * grad_slot_bytes<T, NS>());
+    const T* P0 = j > 0 ? reinterpret_cast<const T*>(slots + slot_of(j - 1) * grad_slot_bytes<T, NS>()) : P1;
+    const T* P2 = j + 1 < ny ? reinterpret_cast<const T*>(slots + slot_of(j + 1) * grad_slot_bytes<T, NS>()) : P1;
+    if (i < nx && k < nz) {
+#pragma unroll
+      for (int sl = 0; sl < NS; ++sl) {
+        if (sl >= ns) break;
+        const double o = off ? off[s0 + sl] : 0.0;
+        const int c = sl * PS + iz * BX + ix;
+        auto v = [&](const T* P, int e) { return static_cast<double>(P[e]) + o; };
+        const double ctr = v(P1, c);
+        double gx = 0.0, gy = 0.0, gz = 0.0;
+        if (nx > 1) {
+          if (i == 0)
+            gx = grad(v(P1, c + 1), ctr, dx);
+          else if (i == nx - 1)
+            gx = grad(ctr, v(P1, c - 1), dx);
+          else
+            gx = grad(v(P1, c + 1), v(P1, c - 1), two_dx);
+        }
+        if (ny > 1) {
+          if (j == 0)
+            gy = grad(v(P2, c), ctr, dx);
+          else if (j == ny - 1)
+            gy = grad(ctr, v(P0, c), dx);
+          else
+            gy = grad(v(P2, c), v(P0, c), two_dx);
+        }
+        if (nz > 1) {
+          if (k == 0)
+            gz = grad(v(P1, c + BX), ctr, dx);
+          else if (k == nz - 1)
+            gz = grad(ctr, v(P1, c - BX), dx);
+          else
+            gz = grad(v(P1, c + BX), v(P1, c - BX), two_dx);
+        }
+        double* o3 = stg + lane * SX + wz * 3 * NS + 3 * sl;
+        o3[0] = gx;
+        o3[1] = gy;
+        o3[2] = gz;
+      }
+    }
+    __syncthreads();  // the block is complete and every read of plane j-1 is done
+    if (j + 3 <= jlast) {
+      if (tid == 0) issue(j + 3);  // into plane j-1's slot
+      issued = j + 3;
+    }
+    // x row il of the block: 8 voxels x 3 x ns doubles, contiguous in the output when ns == S
+    const int nk = min(kGTZ, nz - k0);
+    for (int q = tid; q < kGTX * RUN; q += 256) {
+      const int il = q / RUN, r = q - il * RUN;
+      const int kl = r / (3 * NS), e = r - kl * (3 * NS);
+      if (i0 + il < nx && kl < nk && e < 3 * ns)
+        out[((static_cast<size_t>(i0 + il) * ny + j) * nz + k0 + kl) * (3 * static_cast<size_t>(S)) + 3 * s0 + e] =
+            stg[il * SX + r];
+    }
+    __syncthreads();  // the block is free for the next plane
+  }
+  if (!ok) {
+    // a wait gave up: let the loads still in flight land (each wait bounded)
+    // before the CTA's shared memory goes away, then report it
+    for (int p = waited + 1; p <= issued; ++p) bfvm::mbar_wait(bfvm::smem_u32(&bars[slot_of(p)]), parity_of(p));
+    if (tid == 0) atomicExch(status, bfvm::kDevTimeout);
+  }
+}
+
+template <typename T, int NS>
+cudaError_t launch_plane_kernel(bfvm_ctx* c, int s0, double* d_out) {
+  constexpr size_t smem = grad_smem_bytes<T, NS>();
+  cudaError_t e = cudaFuncSetAttribute(gradient_plane_kernel<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int xt = (c->nx + kGTX - 1) / kGTX, zt = (c->nz + kGTZ - 1) / kGTZ;
+  // enough y ranges for about 6 CTAs per SM, each range at least 8 planes
+  const long long want = 6LL * sms;
+  int chunks = static_cast<int>((want + static_cast<long long>(xt) * zt - 1) / (static_cast<long long>(xt) * zt));
+  chunks = std::max(1, std::min(chunks, (c->ny + 7) / 8));
+  const int jc = (c->ny + chunks - 1) / chunks;
+  const dim3 grid(xt, zt, (c->ny + jc - 1) / jc);
+  gradient_plane_kernel<T, NS><<<grid, 256, smem, c->stream>>>(
+      c->maps.g, c->nx, c->ny, c->nz, c->S, s0, jc, c->prec == BFVM_FP32 ? c->d_off : nullptr, c->dx, d_out,
+      c->d_status);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_plane_groups(bfvm_ctx* c, double* d_out, int* launches) {
+  *launches = 0;
+  const int G = std::min(4, c->S);  // substrates per box of c->maps.g
+  for (int s0 = 0; s0 < c->S; s0 += G) {
+    cudaError_t e = cudaSuccess;
+    switch (G) {
+      case 1: e = launch_plane_kernel<T, 1>(c, s0, d_out); break;
+      case 2: e = launch_plane_kernel<T, 2>(c, s0, d_out); break;
+      case 3: e = launch_plane_kernel<T, 3>(c, s0, d_out); break;
+      default: e = launch_plane_kernel<T, 4>(c, s0, d_out); break;
+    }
+    if (e != cudaSuccess) return e;
+    ++*launches;
+  }
+  return cudaSuccess;
+}
 
 constexpr int kGroup = 4;  // substrates staged per output block (keeps static shared memory under 48 KB)
 
@@ -114,6 +321,15 @@ __global__ void __launch_bounds__(256) gradient_kernel(const T* __restrict__ f, 
 }
 
 int launch_gradients(bfvm_ctx* c, double* d_out) {
+  if (c->maps.g_ok) {
+    int launches = 0;
+    if (c->prec == BFVM_FP64)
+      BFVM_CUDA(launch_plane_groups<double>(c, d_out, &launches));
+    else
+      BFVM_CUDA(launch_plane_groups<float>(c, d_out, &launches));
+    bfvm::note_launches(launches);
+    return BFVM_OK;
+  }
   const dim3 block(32, 8);
   const dim3 grid((c->nz + 31) / 32, (c->nx + 7) / 8, c->ny);
   if (c->prec == BFVM_FP64)

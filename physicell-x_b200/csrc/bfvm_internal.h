@@ -180,6 +180,8 @@ struct FieldMaps {
   CUtensorMap z;   // box {yz_tile, 1, chunk rows, 1}
   CUtensorMap ry;  // persistent schedule: box {32, kRingRows, 1, 1}
   CUtensorMap rz;  // persistent schedule: box {32, 1, kRingRows, 1}
+  CUtensorMap g;   // gradients: box {32 + 4 (FP64) or 32 + 8 (FP32) x, 1, 10 z, min(S, 4) substrates}
+  int g_ok;        // 1 when the gradient map could be encoded
 };
 
 // Host-side count of this library's kernel launches (bfvm_kernel_launches).

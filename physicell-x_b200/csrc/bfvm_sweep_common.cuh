@@ -115,10 +115,20 @@ __device__ __forceinline__ double forward_store(const double (&v)[B], const doub
 
 // FP32 form: stored values are FP32, the recurrence runs in FP64 (the
 // running value y stays FP64 across elements and batches), each result is
-// rounded to FP32 once, when stored.  The quotient is t * RN(1/d).
+// rounded to FP32 once, when stored.  The quotient is t * RN(1/d); under the
+// short chain (screen == kScreenFast) y = fma(c1 * r, y, (v - shift) * r),
+// one dependent FMA per element, the products formed off the chain.
 template <int B, typename Put>
 __device__ __forceinline__ double forward_store(const float (&v)[B], const double (&cf)[B], double c1, double shift,
-                                                int, double y, Put&& put) {
+                                                int screen, double y, Put&& put) {
+  if (screen == kScreenFast) {
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      y = __fma_rn(__dmul_rn(c1, cf[q]), y, __dmul_rn(static_cast<double>(v[q]) - shift, cf[q]));
+      put(q, static_cast<float>(y));
+    }
+    return y;
+  }
 #pragma unroll
   for (int q = 0; q < B; ++q) {
     const double t = __fma_rn(c1, y, static_cast<double>(v[q]) - shift);

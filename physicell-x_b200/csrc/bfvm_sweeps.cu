@@ -227,7 +227,7 @@ __device__ bool x_tile(const CUtensorMap* map, const SweepParams<T>& p, int j0, 
     if constexpr (!kF32<T>) {
       if (tile_screen) {
         y = forward_any<W>(screen, v, cf, c1, y, put);
-        hwmin = min(hwmin, batch_min_hi<W>(v));
+        if (screen != kScreenFast) hwmin = min(hwmin, batch_min_hi<W>(v));
         return;
       }
     }
@@ -474,7 +474,7 @@ __device__ bool yz_tile(const CUtensorMap* map, const SweepParams<T>& p, int i0,
       y = forward_store<R>(v, cf, c1, shift, screen, y, put);
     } else {
       y = forward_any<R>(screen, v, cf, c1, y, put);
-      hwmin = min(hwmin, batch_min_hi<R>(v));
+      if (screen != kScreenFast) hwmin = min(hwmin, batch_min_hi<R>(v));
     }
   };
   auto forward_pass = [&](bool edge) {
@@ -829,7 +829,7 @@ __global__ void __launch_bounds__(64 * kMaxRings<T>, 1) sweep_yz_ring_kernel(con
         y = forward_store<R>(v, cf, c1, shift, screen, y, put);
       } else {
         y = forward_any<R>(screen, v, cf, c1, y, put);
-        hwmin = min(hwmin, batch_min_hi<R>(v));
+        if (screen != kScreenFast) hwmin = min(hwmin, batch_min_hi<R>(v));
       }
     };
     auto forward_pass = [&](bool edge) {
@@ -1429,6 +1429,10 @@ int encode_field_maps(FieldMaps* maps, void* f, int eb, int nx, int ny, int nz, 
   if (rc == 0) rc = encode_one(&maps->z, f, eb, dims, strides, bz, CU_TENSOR_MAP_SWIZZLE_NONE);
   if (rc == 0) rc = encode_one(&maps->ry, f, eb, dims, strides, bry, CU_TENSOR_MAP_SWIZZLE_NONE);
   if (rc == 0) rc = encode_one(&maps->rz, f, eb, dims, strides, brz, CU_TENSOR_MAP_SWIZZLE_NONE);
+  // the gradient kernel's plane boxes: 32 x with a halo rounded out to 16-byte
+  // boundaries, one y plane, 8 z with a one-voxel halo, up to 4 substrates
+  const cuuint32_t bg[4] = {(cuuint32_t)(eb == 8 ? 36 : 40), 1, 10, (cuuint32_t)(S < 4 ? S : 4)};
+  maps->g_ok = rc == 0 && encode_one(&maps->g, f, eb, dims, strides, bg, CU_TENSOR_MAP_SWIZZLE_NONE) == 0;
   return rc;
 }
 

@@ -185,7 +185,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
           y = forward_any<R>(screen, v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
         else
           y = forward_any<R>(screen, v, cf, c1, y, [&](int q, double val) { cb[q * TI] = val; });
-        hwmin = min(hwmin, batch_min_hi<R>(v));
+        if (screen != kScreenFast) hwmin = min(hwmin, batch_min_hi<R>(v));
       } else if (flow) {
 #pragma unroll
         for (int q = 0; q < R; ++q) yv[q] = 0.0;  // lanes with no line: anything, never read
@@ -578,7 +578,7 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
           RowPut<double> put{crow, sw};
           y = forward_any<W>(screen, v, cf, c1, y, put);
         }
-        hwmin = min(hwmin, batch_min_hi<W>(v));
+        if (screen != kScreenFast) hwmin = min(hwmin, batch_min_hi<W>(v));
       } else if (flow) {
 #pragma unroll
         for (int q = 0; q < W; ++q) yv[q] = 0.0;  // lanes with no line: anything, never read

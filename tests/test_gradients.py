@@ -52,6 +52,25 @@ def test_gpu_gradients_bitwise_fp64(idx):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(70, 45, 37, 3), (65, 33, 40, 6), (200, 200, 30, 4), (31, 9, 17, 5),
+                                   (40, 300, 9, 1)])
+def test_gpu_gradients_plane_kernel_bitwise(shape):
+    """The plane-ring kernel on shapes with partial x/z tiles, several y
+    ranges, substrate groups of 4 with a partial last group."""
+    from bfvm import Microenvironment
+
+    nx, ny, nz, S = shape
+    wl = W.small_random(777 + nx, nx=nx, ny=ny, nz=nz, S=S, n_agents=500, steps=2)
+    me = Microenvironment.from_workload(wl)
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    field = me.download_field()
+    got = me.compute_all_gradient_vectors()
+    me.synchronize()
+    me.close()
+    assert np.array_equal(got, pyoracle.Port.gradients(field, wl.shape, wl.dx))
+
+
+@pytest.mark.gpu
 def test_gpu_gradients_fp32_and_device_output():
     import torch
 

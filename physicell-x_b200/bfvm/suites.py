@@ -50,29 +50,40 @@ def _timed_steps(me, steps, sources=True):
     return e0.elapsed_time(e1) * 1e-3
 
 
-def uneven_batch(n_envs=256, steps=200, trial_steps=5, device=0):
+def uneven_batch(n_envs=256, steps=200, trial_steps=5, device=0, chain=0):
     """The uneven batch (n_envs solves, edges 24-128, 1-6 substrates, 0-20k
-    agents): plain FP64 one solve at a time, the FP64 batch and the FP32 batch
-    (autotuned), each for `steps` LOD steps with sources; FP32 errors against
-    FP64 per solve and substrate."""
+    agents): plain FP64 and plain FP32 one solve at a time, the FP64 batch and
+    the FP32 batch (autotuned), each for `steps` LOD steps with sources; FP32
+    errors against FP64 per solve and substrate.  `chain` is the FP32 form's
+    recurrence (bfvm_set_fp64_chain); the FP64 runs keep the reference's
+    arithmetic.  The FP32-batch over FP64-plain ratio is split into its
+    precision factor (plain FP64 over plain FP32: half the bytes) and its
+    batching factor (plain FP32 over the FP32 batch: launches and idle gaps
+    of one-at-a-time solves removed)."""
     import torch
 
     wls = W.uneven_batch(n_envs, steps=steps)
     tot = sum(wl.n_values for wl in wls)
-    out = {"envs": n_envs, "steps": steps, "values_per_step": tot}
-    # plain FP64, one solve at a time (each synchronised before the next starts)
+    out = {"envs": n_envs, "steps": steps, "values_per_step": tot, "fp32_chain": chain}
+    # plain, one solve at a time (each synchronised before the next starts)
     ref = []
-    t_plain = 0.0
-    for wl in wls:
-        me = Microenvironment.from_workload(wl, "fp64", device)
-        t_plain += _timed_steps(me, steps)
-        ref.append(_device_field(me, device))
-        me.close()
-    out["fp64_plain"] = {"s": t_plain, "updates_per_s": tot * steps / t_plain}
+    for prec in ("fp64", "fp32"):
+        t_plain = 0.0
+        for wl in wls:
+            me = Microenvironment.from_workload(wl, prec, device)
+            if prec == "fp32":
+                me.set_fp64_chain(chain)
+            t_plain += _timed_steps(me, steps)
+            if prec == "fp64":
+                ref.append(_device_field(me, device))
+            me.close()
+        out[f"{prec}_plain"] = {"s": t_plain, "updates_per_s": tot * steps / t_plain}
     for prec in ("fp64", "fp32"):
         b = Batch(prec, device)
         mes = [Microenvironment.from_workload(wl, prec, device) for wl in wls]
         for me in mes:
+            if prec == "fp32":
+                me.set_fp64_chain(chain)
             b.add(me)
         tuned_ms = b.autotune(sources=True, trial_steps=trial_steps)
         bs = torch.cuda.ExternalStream(b.stream)
@@ -99,6 +110,12 @@ def uneven_batch(n_envs=256, steps=200, trial_steps=5, device=0):
             me.close()
         out[f"{prec}_batch"] = res
     out["fp32_batch_over_fp64_plain"] = out["fp32_batch"]["updates_per_s"] / out["fp64_plain"]["updates_per_s"]
+    out["decomposition"] = {
+        "precision_fp64_plain_over_fp32_plain": out["fp64_plain"]["s"] / out["fp32_plain"]["s"],
+        "batching_fp32_plain_over_fp32_batch": out["fp32_plain"]["s"] / out["fp32_batch"]["s"],
+        "batching_fp64_plain_over_fp64_batch": out["fp64_plain"]["s"] / out["fp64_batch"]["s"],
+        "bytes_ratio": 2.0,
+    }
     return out
 
 

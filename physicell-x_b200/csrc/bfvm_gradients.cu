@@ -166,8 +166,10 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
       }
     }
     __syncthreads();  // the block is complete and every read of plane j-1 is done
-    if (j + 3 <= jlast) {
-      if (tid == 0) issue(j + 3);  // into plane j-1's slot
+    // plane j+3 into plane j-1's slot, unless the prologue loaded it already
+    // (a CTA starting at plane 0 has no plane -1, so its prologue takes 0..3)
+    if (j + 3 <= jlast && j + 3 > issued) {
+      if (tid == 0) issue(j + 3);
       issued = j + 3;
     }
     // x row il of the block: 8 voxels x 3 x ns doubles, contiguous in the output when ns == S

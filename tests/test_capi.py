@@ -123,3 +123,13 @@ def test_null_handles_are_rejected_before_any_device_work():
         assert got == _NULL_VALUES.get(name, _lib.BFVM_ERR_ARG), name
         seen += 1
     assert seen >= 50
+
+
+def test_wait_limit_arguments_checked_first():
+    """The wait-limit setter rejects limits outside [1 us, 60 s] before it
+    looks for a device."""
+    L = _lib.lib()
+    assert L.bfvm_set_wait_limit_ns(0, 999) == _lib.BFVM_ERR_ARG
+    assert L.bfvm_set_wait_limit_ns(0, 60_000_000_001) == _lib.BFVM_ERR_ARG
+    if not _cuda_available():
+        assert L.bfvm_set_wait_limit_ns(0, 1_000_000) == _lib.BFVM_ERR_NODEVICE

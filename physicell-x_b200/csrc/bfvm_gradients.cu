@@ -110,11 +110,27 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
   };
   if (jb > 0) wait_plane(jb - 1);
   const double two_dx = dx * 2.0;
+  // The divisor's reciprocal, for the quotient by Markstein's correction of
+  // RN(g * RN(1/h)) -- three FP64 operations instead of the IEEE division
+  // sequence, and the same correctly rounded result wherever no intermediate
+  // leaves the normal range: the numerator and the first quotient between
+  // 2^-960 and 2^1000 in magnitude, h between 2^-100 and 2^100.  A numerator
+  // of +0 gives +0; anything else outside those bounds (-0, tiny, huge)
+  // takes the IEEE division.
+  const double rdx = 1.0 / dx, r2dx = 1.0 / two_dx;
+  const bool markstein_ok = dx >= 0x1p-100 && dx <= 0x1p99;
   // g = a; g -= b; g /= h  (BioFVM_microenvironment.cpp:1480-1482 and the
   // matching lines of every end cap and interior loop)
-  auto grad = [](double a, double b, double h) {
+  auto grad = [markstein_ok](double a, double b, double h, double rh) {
     double g = a;
     g -= b;
+    const double q0 = g * rh;
+    const double ag = fabs(g), aq = fabs(q0);
+    if (markstein_ok && ag >= 0x1p-960 && aq >= 0x1p-960 && ag < 0x1p1000 && aq < 0x1p1000) {
+      const double e = __fma_rn(-q0, h, g);
+      return __fma_rn(e, rh, q0);
+    }
+    if (g == 0.0 && !signbit(g)) return 0.0;
     return g / h;
   };
   const int i = i0 + lane, k = k0 + wz;
@@ -137,27 +153,27 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
         double gx = 0.0, gy = 0.0, gz = 0.0;
         if (nx > 1) {
           if (i == 0)
-            gx = grad(v(P1, c + 1), ctr, dx);
+            gx = grad(v(P1, c + 1), ctr, dx, rdx);
           else if (i == nx - 1)
-            gx = grad(ctr, v(P1, c - 1), dx);
+            gx = grad(ctr, v(P1, c - 1), dx, rdx);
           else
-            gx = grad(v(P1, c + 1), v(P1, c - 1), two_dx);
+            gx = grad(v(P1, c + 1), v(P1, c - 1), two_dx, r2dx);
         }
         if (ny > 1) {
           if (j == 0)
-            gy = grad(v(P2, c), ctr, dx);
+            gy = grad(v(P2, c), ctr, dx, rdx);
           else if (j == ny - 1)
-            gy = grad(ctr, v(P0, c), dx);
+            gy = grad(ctr, v(P0, c), dx, rdx);
           else
-            gy = grad(v(P2, c), v(P0, c), two_dx);
+            gy = grad(v(P2, c), v(P0, c), two_dx, r2dx);
         }
         if (nz > 1) {
           if (k == 0)
-            gz = grad(v(P1, c + BX), ctr, dx);
+            gz = grad(v(P1, c + BX), ctr, dx, rdx);
           else if (k == nz - 1)
-            gz = grad(ctr, v(P1, c - BX), dx);
+            gz = grad(ctr, v(P1, c - BX), dx, rdx);
           else
-            gz = grad(v(P1, c + BX), v(P1, c - BX), two_dx);
+            gz = grad(v(P1, c + BX), v(P1, c - BX), two_dx, r2dx);
         }
         double* o3 = stg + lane * SX + wz * 3 * NS + 3 * sl;
         o3[0] = gx;

@@ -712,25 +712,25 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
           }
         }
       }
+      if (flow) {
+        // the staging chunk's previous bulk store has read it
+        if (t == 0) tma_store_wait_read();
+        __syncwarp();
+      }
       store_row<double, W>(crow, sw, v);
+      // The chunk goes out as it is staged, in one bulk tensor store (rows
+      // past ny and columns past nx are clipped by the map).
+      fence_async_smem();
       __syncwarp();
-      // out transposed: lanes 0-15 write line 2r's 16 values, 16-31 line 2r+1's
-      {
-        const int e = t & 15;
-        const int i = i0 + e;
-#pragma unroll
-        for (int r = 0; r < 16; ++r) {
-          const int L = 2 * r + (t >> 4);
-          const double val = *swz_elem<double>(cbase + L * 128, e, L & 7);
-          if (j0 + L < ny && i < nx) plane[static_cast<size_t>(j0 + L) * p.nxp + i] = val;
-        }
+      if (t == 0) {
+        tma_store_4d(map, smem_u32(cbase), i0, j0, k, s);
+        tma_store_commit();
       }
       if (!flow) {
-        fence_async_smem();  // this warp's writes to the slot precede the refill
+        // the slot's refill waits for the store to have read it
+        if (t == 0) tma_store_wait_read();
         __syncwarp();
         if (nxt < ntiles) issue(nj0, nk, ns_, T + (NR - 1 - (c - T)), rslot(flip, c), (it + 1) & 1u);
-      } else {
-        __syncwarp();  // the staging chunk is read before the next chunk overwrites it
       }
     };
     if (edge_tile) {
@@ -740,7 +740,8 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
     }
     if (MODE == 2 && nxt < ntiles) {
       // the next tile's first inputs take the input slots (the first of
-      // which staged results just now)
+      // which staged results just now: its store must have read it)
+      if (t == 0) tma_store_wait_read();
       fence_async_smem();
       __syncwarp();
       for (int c = 0; c < KF; ++c) {
@@ -824,6 +825,7 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
     for (int sl = 0; sl < nslots; ++sl)
       if ((pend >> sl) & 1u) mbar_wait(smem_u32(&full[sl]), (ppar >> sl) & 1u);
   }
+  if (t == 0) tma_store_wait_read();  // this warp's bulk stores have read shared memory
   __syncwarp();
   if (tm) {
     tmem_wait_st();

@@ -402,11 +402,11 @@ int bfvm_set_fp64_chain(bfvm_ctx* ctx, int chain);
 int bfvm_get_fp64_chain(bfvm_ctx* ctx, int* chain);
 
 /* Tensor-memory (TMEM) rings in the FP64 persistent sweeps: on = 1
- * (default) in the y/z sweeps on lines of 33 to 736 voxels and in the x
- * sweep on lines of 257 to 736 (agents not fused into it): up to four rings
- * keep the forward results of a line's first 256 values in the SM's TMEM
- * beside the shared-memory rings; 2 also in the x sweep on lines of 17 to
- * 256; 0 shared memory alone.  Every level gives the same bits. */
+ * (default) in the y, z and x sweeps on lines of 33 to 736 voxels (the x
+ * sweep with agents not fused into it): up to four rings keep the forward
+ * results of a line's first 256 values in the SM's TMEM beside the
+ * shared-memory rings; 2 also in the x sweep on lines of 17 to 32; 0 shared
+ * memory alone.  Every level gives the same bits. */
 int bfvm_set_sweep_tmem(bfvm_ctx* ctx, int on);
 /* The tensor-memory sweep a persistent FP64 sweep would run on lines of
  * n_line voxels (host arithmetic, no device needed): axis 0 = the x sweep

@@ -111,11 +111,22 @@ int enqueue_step(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, cudaEven
     const int rc = bfvm_apply_sources(c);  // timed with the x sweep
     if (rc != BFVM_OK) return rc;
   }
-  BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, c->stream));
+  const bool part = c->fp64_chain == 2;
+  if (part && c->cfg.x_lines != 32) return BFVM_ERR_STATE;  // its x tiles are the 32-line boxes of maps.x
+  if (part)
+    BFVM_CUDA((launch_part<T, 0>(c->maps.x, p, c->part[0], c->stream)));
+  else
+    BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, c->stream));
   if (ev) BFVM_CUDA(cudaEventRecord(ev[1], c->stream));
-  BFVM_CUDA(launch_sweep_y<T>(c->maps, p, c->cfg, c->stream));
+  if (part)
+    BFVM_CUDA((launch_part<T, 1>(c->maps.ry, p, c->part[1], c->stream)));
+  else
+    BFVM_CUDA(launch_sweep_y<T>(c->maps, p, c->cfg, c->stream));
   if (ev) BFVM_CUDA(cudaEventRecord(ev[2], c->stream));
-  BFVM_CUDA(launch_sweep_z<T>(c->maps, p, c->cfg, c->stream));
+  if (part)
+    BFVM_CUDA((launch_part<T, 2>(c->maps.rz, p, c->part[2], c->stream)));
+  else
+    BFVM_CUDA(launch_sweep_z<T>(c->maps, p, c->cfg, c->stream));
   if (ev) BFVM_CUDA(cudaEventRecord(ev[3], c->stream));
   note_launches(3);
   return BFVM_OK;
@@ -154,7 +165,8 @@ int capture_step_graph(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, co
 
 template <typename T>
 int run_steps_plain(bfvm_ctx* c, int nsteps, bool sources) {
-  const bool standalone = sources && c->n_agents > 0 && !c->cfg.fuse_sources;
+  // the partitioned sweeps take no fused sources: the standalone kernel applies them
+  const bool standalone = sources && c->n_agents > 0 && (!c->cfg.fuse_sources || c->fp64_chain == 2);
   const SweepParams<T> p = make_params<T>(c, sources && !standalone);
   // Runs of steps replay a captured graph of kGraphSteps steps (the same
   // launches, so the same bits), which removes most of the per-launch host
@@ -274,8 +286,10 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
   c->screen_exact = 1;
   for (int s = 0; s < S; ++s)
     if (!(D[s] >= 0.0) || !(decay[s] >= 0.0)) c->screen_exact = 0;
-  const bool fast = c->prec == BFVM_FP64 && c->fp64_chain == 1;
-  c->screen = c->fp64_chain == 1 ? 2 : c->screen_exact;  // 2: the short chain (kScreenFast)
+  const bool fast = c->prec == BFVM_FP64 && c->fp64_chain >= 1;
+  // 2: the short chain (kScreenFast); under chain 2 the other kernels that
+  // step this solve (the batched engine) run the short chain too
+  c->screen = c->fp64_chain >= 1 ? 2 : c->screen_exact;
   const int n_axis[3] = {c->nx, c->ny, c->nz};
   size_t dr_off[3], cu_off[3];
   const size_t bytes = coef_bytes(c, dr_off, cu_off);
@@ -316,6 +330,77 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
     k2 *= c->dt;
     k2 /= 3.0;
     c->c2[s] = k2;
+  }
+  return BFVM_OK;
+}
+
+// The partitioned sweeps' coefficient rows of the three axes (see PartAxis):
+// products formed in long double from the FP64 factors and rounded once.
+int upload_part_coefficients(bfvm_ctx* c) {
+  const int S = c->S;
+  const int n_axis[3] = {c->nx, c->ny, c->nz};
+  size_t off[3][4];
+  size_t bytes = 0;
+  for (int a = 0; a < 3; ++a) {
+    const size_t rows = static_cast<size_t>(S) * coef_pad(n_axis[a]);
+    off[a][0] = bytes;
+    bytes += rows * 16;  // ra
+    off[a][1] = bytes;
+    bytes += rows * 16;  // pg
+    off[a][2] = bytes;
+    bytes += rows * 8;   // q
+    off[a][3] = bytes;
+    bytes += static_cast<size_t>(S) * kPartWarps * 16;  // ag
+    bytes = (bytes + 255) & ~size_t(255);
+  }
+  std::vector<unsigned char> host(bytes, 0);
+  std::vector<double> c1(S);
+  for (int a = 0; a < 3; ++a) {
+    const int n = n_axis[a];
+    const int np = coef_pad(n);
+    const int mseg = (n + kPartWarps - 1) / kPartWarps;
+    std::vector<double> dn(static_cast<size_t>(n) * S), cu(static_cast<size_t>(n) * S);
+    thomas_axis_host(n, S, c->D.data(), c->decay.data(), c->dt, c->dx, dn.data(), cu.data(), c1.data(), false);
+    double2* ra = reinterpret_cast<double2*>(host.data() + off[a][0]);
+    double2* pg = reinterpret_cast<double2*>(host.data() + off[a][1]);
+    double* q = reinterpret_cast<double*>(host.data() + off[a][2]);
+    double2* ag = reinterpret_cast<double2*>(host.data() + off[a][3]);
+    for (int s = 0; s < S; ++s) {
+      std::vector<double> av(n), gv(n);
+      for (int i = 0; i < n; ++i) {
+        const double r = 1.0 / dn[static_cast<size_t>(i) * S + s];
+        av[i] = i == 0 ? 0.0 : c1[s] * r;
+        gv[i] = i < n - 1 ? -cu[static_cast<size_t>(i) * S + s] : 0.0;
+        ra[static_cast<size_t>(s) * np + i] = make_double2(r, av[i]);
+      }
+      for (int w = 0; w < kPartWarps; ++w) {
+        const int lo = w * mseg, hi = std::min(n, lo + mseg);
+        long double pa = 1.0L, pq = 1.0L;
+        for (int i = lo; i < hi; ++i) {
+          pa *= static_cast<long double>(av[i]);
+          pg[static_cast<size_t>(s) * np + i] = make_double2(static_cast<double>(pa), gv[i]);
+        }
+        for (int i = hi - 1; i >= lo; --i) {
+          pq *= static_cast<long double>(gv[i]);
+          q[static_cast<size_t>(s) * np + i] = static_cast<double>(pq);
+        }
+        ag[static_cast<size_t>(s) * kPartWarps + w] = make_double2(static_cast<double>(pa), static_cast<double>(pq));
+      }
+    }
+  }
+  if (c->d_part) dfree(c, c->d_part);
+  c->d_part = nullptr;
+  int rc = dalloc(c, &c->d_part, bytes);
+  if (rc != BFVM_OK) return rc;
+  BFVM_CUDA(cudaMemcpy(c->d_part, host.data(), bytes, cudaMemcpyHostToDevice));
+  const unsigned char* b = static_cast<const unsigned char*>(c->d_part);
+  for (int a = 0; a < 3; ++a) {
+    c->part[a].ra = reinterpret_cast<const double2*>(b + off[a][0]);
+    c->part[a].pg = reinterpret_cast<const double2*>(b + off[a][1]);
+    c->part[a].q = reinterpret_cast<const double*>(b + off[a][2]);
+    c->part[a].ag = reinterpret_cast<const double2*>(b + off[a][3]);
+    c->part[a].mseg = (n_axis[a] + kPartWarps - 1) / kPartWarps;
+    c->part[a].npad = coef_pad(n_axis[a]);
   }
   return BFVM_OK;
 }
@@ -489,6 +574,11 @@ int bfvm_create(const bfvm_config* cfg, bfvm_ctx** out) {
     rc = dalloc(c, reinterpret_cast<void**>(&c->d_line_off), sizeof(int) * (static_cast<size_t>(c->ny) * c->nz + 1));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_sums), sizeof(double) * (S * 1024 + S));
   if (rc != BFVM_OK) return fail(rc);
+  if (cudaMallocHost(reinterpret_cast<void**>(&c->h_status), sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    c->h_status = nullptr;
+    return fail(BFVM_ERR_OOM);
+  }
   if (cudaMemset(c->f, 0, c->field_bytes) != cudaSuccess || cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess ||
       cudaMemset(c->d_tile_counter, 0, 2 * sizeof(unsigned long long)) != cudaSuccess)
     return fail(BFVM_ERR_CUDA);
@@ -522,6 +612,7 @@ int bfvm_destroy(bfvm_ctx* c) {
   dfree(c, c->d_active);
   dfree(c, c->d_faces);
   dfree(c, c->d_status);
+  if (c->h_status) cudaFreeHost(c->h_status);
   dfree(c, c->d_tile_counter);
   dfree(c, c->d_nvalid);
   dfree(c, c->d_line_off);
@@ -536,6 +627,7 @@ int bfvm_destroy(bfvm_ctx* c) {
   dfree(c, c->d_nodes);
   dfree(c, c->d_delta);
   dfree(c, c->d_mass);
+  dfree(c, c->d_part);
   for (cudaEvent_t e : c->events) cudaEventDestroy(e);
   drop_step_graph(c);
   if (c->copy_stream) {
@@ -966,10 +1058,10 @@ extern "C" int bfvm_field_offsets(bfvm_ctx* c, double* out) {
 extern "C" int bfvm_synchronize(bfvm_ctx* c) {
   if (!c) return BFVM_ERR_ARG;
   DeviceGuard g(c->device);
+  // the status word comes back behind the stream's work, in the same wait
+  BFVM_CUDA(cudaMemcpyAsync(c->h_status, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   BFVM_CUDA(cudaStreamSynchronize(c->stream));
-  int st = 0;
-  BFVM_CUDA(cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-  if (st != 0) {
+  if (*c->h_status != 0) {
     cudaMemset(c->d_status, 0, sizeof(int));
     return BFVM_ERR_TIMEOUT;
   }
@@ -1139,14 +1231,24 @@ extern "C" int bfvm_set_fused_sources(bfvm_ctx* c, int fused) {
 }
 
 extern "C" int bfvm_set_fp64_chain(bfvm_ctx* c, int chain) {
-  if (!c || (chain != 0 && chain != 1)) return BFVM_ERR_ARG;
+  if (!c || chain < 0 || chain > 2) return BFVM_ERR_ARG;
   if (chain == c->fp64_chain) return BFVM_OK;
+  if (chain == 2) {
+    // the partitioned sweeps stage whole 32-line tiles of up to kMaxChunks chunks
+    const int n_axis[3] = {c->nx, c->ny, c->nz};
+    for (int a = 0; a < 3; ++a)
+      if (part_smem_bytes(c->eb, n_axis[a], a) > 227 * 1024 ||
+          (n_axis[a] + (a == 0 ? 128 / c->eb : kRingRows) - 1) / (a == 0 ? 128 / c->eb : kRingRows) > kPartMaxChunks)
+        return BFVM_ERR_SHAPE;
+    if (c->cfg.x_lines != 32) return BFVM_ERR_STATE;
+  }
   DeviceGuard g(c->device);
   BFVM_CUDA(cudaStreamSynchronize(c->stream));
   const int prev = c->fp64_chain;
   c->fp64_chain = chain;
   const std::vector<double> D = c->D, decay = c->decay;
-  const int rc = upload_coefficients(c, D.data(), decay.data());
+  int rc = upload_coefficients(c, D.data(), decay.data());
+  if (rc == BFVM_OK && chain == 2) rc = upload_part_coefficients(c);
   if (rc != BFVM_OK) {
     c->fp64_chain = prev;
     upload_coefficients(c, D.data(), decay.data());

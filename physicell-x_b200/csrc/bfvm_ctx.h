@@ -29,12 +29,15 @@ struct bfvm_ctx {
   void* d_c1 = nullptr;
   int screen = 0;              // SweepParams::screen of the 3-D sweeps (kScreenFast: short FP64 chain)
   int screen_exact = 0;        // 1 when no diffusion or decay rate is negative (the exactness screen applies)
-  int fp64_chain = 0;          // bfvm_set_fp64_chain: 0 reference-exact, 1 short chain
+  int fp64_chain = 0;          // bfvm_set_fp64_chain: 0 reference-exact, 1 short chain, 2 partitioned
+  void* d_part = nullptr;      // partitioned-sweep coefficient rows of the three axes (chain 2)
+  bfvm::PartAxis part[3] = {};
   double* d_off = nullptr;      // FP32: per-substrate field offsets [S]
   void* d_shift = nullptr;      // FP32: RN32(c2 * off) [S]
   int* d_active = nullptr;
   double* d_faces = nullptr;   // xface | yface | zface
   int* d_status = nullptr;
+  int* h_status = nullptr;     // pinned host copy of d_status, read back in the same stream wait
   unsigned long long* d_tile_counter = nullptr;  // [2] persistent TMEM y/z sweep work counter
   double* d_sums = nullptr;    // partial sums + result
   bfvm::FieldMaps maps{};

@@ -49,8 +49,8 @@ __host__ __device__ constexpr size_t grad_slot_bytes() {
   return (static_cast<size_t>(kGBoxX<T>) * kGBoxZ * NS * sizeof(T) + 127) / 128 * 128;
 }
 template <int NS>
-__host__ __device__ constexpr int grad_stage_stride() {  // doubles per x row of the output block (odd: no bank conflicts)
-  return kGTZ * 3 * NS + 1;
+__host__ __device__ constexpr int grad_stage_stride() {  // doubles per x row of the output block (even: 16-byte rows)
+  return kGTZ * 3 * NS + 2;
 }
 template <typename T, int NS>
 __host__ __device__ constexpr size_t grad_smem_bytes() {
@@ -121,12 +121,14 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
   const bool markstein_ok = dx >= 0x1p-100 && dx <= 0x1p99;
   // g = a; g -= b; g /= h  (BioFVM_microenvironment.cpp:1480-1482 and the
   // matching lines of every end cap and interior loop)
+  // With h in [2^-100, 2^99], a numerator g in [2^-860, 2^900] in magnitude
+  // keeps both g and RN(g/h) inside those bounds: one test of g's exponent.
   auto grad = [markstein_ok](double a, double b, double h, double rh) {
     double g = a;
     g -= b;
+    const unsigned hw = static_cast<unsigned>(__double2hiint(g)) & 0x7FFFFFFFu;  // |g|'s high word
     const double q0 = g * rh;
-    const double ag = fabs(g), aq = fabs(q0);
-    if (markstein_ok && ag >= 0x1p-960 && aq >= 0x1p-960 && ag < 0x1p1000 && aq < 0x1p1000) {
+    if (markstein_ok && hw - 0x0A300000u < 0x78300000u - 0x0A300000u) {  // 2^-860 <= |g| < 2^900
       const double e = __fma_rn(-q0, h, g);
       return __fma_rn(e, rh, q0);
     }
@@ -188,14 +190,31 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
       if (tid == 0) issue(j + 3);
       issued = j + 3;
     }
-    // x row il of the block: 8 voxels x 3 x ns doubles, contiguous in the output when ns == S
+    // x row il of the block: 8 voxels x 3 x ns doubles, contiguous in the
+    // output when the group holds every substrate and the z tile is whole:
+    // then warp wz writes rows wz, wz + 8, ... as straight runs (16-byte
+    // stores when the run starts 16-byte aligned, i.e. S even)
     const int nk = min(kGTZ, nz - k0);
-    for (int q = tid; q < kGTX * RUN; q += 256) {
-      const int il = q / RUN, r = q - il * RUN;
-      const int kl = r / (3 * NS), e = r - kl * (3 * NS);
-      if (i0 + il < nx && kl < nk && e < 3 * ns)
-        out[((static_cast<size_t>(i0 + il) * ny + j) * nz + k0 + kl) * (3 * static_cast<size_t>(S)) + 3 * s0 + e] =
-            stg[il * SX + r];
+    if (ns == S && nk == kGTZ) {
+      for (int il = wz; il < kGTX; il += 8) {
+        if (i0 + il >= nx) break;
+        double* dst = out + ((static_cast<size_t>(i0 + il) * ny + j) * nz + k0) * (3 * static_cast<size_t>(S));
+        const double* src = stg + il * SX;
+        if ((S & 1) == 0) {
+          for (int u = lane; u < RUN / 2; u += 32)
+            reinterpret_cast<double2*>(dst)[u] = reinterpret_cast<const double2*>(src)[u];
+        } else {
+          for (int u = lane; u < RUN; u += 32) dst[u] = src[u];
+        }
+      }
+    } else {
+      for (int q = tid; q < kGTX * RUN; q += 256) {
+        const int il = q / RUN, r = q - il * RUN;
+        const int kl = r / (3 * NS), e = r - kl * (3 * NS);
+        if (i0 + il < nx && kl < nk && e < 3 * ns)
+          out[((static_cast<size_t>(i0 + il) * ny + j) * nz + k0 + kl) * (3 * static_cast<size_t>(S)) + 3 * s0 + e] =
+              stg[il * SX + r];
+      }
     }
     __syncthreads();  // the block is free for the next plane
   }

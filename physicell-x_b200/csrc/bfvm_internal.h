@@ -128,8 +128,10 @@ struct SweepParams {
   const double* ae2;
   int n_sorted;
   AgentTrack track;      // internalized-substrate tracking (track.internal null: off)
-  // Nonzero when no substrate has a negative diffusion coefficient or decay
-  // rate (c1 >= 0, every denominator >= 1): enables the FP64 input screen.
+  // 1 when no substrate has a negative diffusion coefficient or decay rate
+  // (c1 >= 0, every denominator >= 1): enables the FP64 input screen of the
+  // reference-exact chain; 0 checks every numerator; 2 (kScreenFast) runs
+  // the short chain (bfvm_set_fp64_chain), which needs no screen.
   int screen;
   int* status;           // device status word
   // [2] tiles handed out, CTAs finished: the persistent TMEM y/z sweep's
@@ -164,8 +166,8 @@ struct SweepConfig {
   // y/z sweeps on lines of 33 to 736 (up to four rings keep the forward
   // results of a line's first 256 values in TMEM next to the shared-memory
   // rings: 224 lines in flight per SM instead of 128 at lines of 200, 64
-  // instead of 32 at 640), and in the x sweep on lines of 257 to 736 (agents
-  // not fused); 2 also in the x sweep on lines of 17 to 256; 0 shared memory
+  // instead of 32 at 640), and in the x sweep on lines of 33 to 736 (agents
+  // not fused); 2 also in the x sweep on lines of 17 to 32; 0 shared memory
   // alone.  Same bits at every level.
   int tmem = 1;
 };
@@ -192,6 +194,27 @@ int encode_field_maps(FieldMaps* maps, void* f, int elem_bytes, int nx, int ny, 
 
 template <typename T>
 cudaError_t launch_sweep_x(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st);
+// Partitioned sweeps (bfvm_part_sweeps.cu, bfvm_set_fp64_chain(ctx, 2)):
+// kPartWarps warps per 32-line tile, warp w owning elements
+// [w*mseg, (w+1)*mseg) of every line.  Per axis and substrate, rows of npad:
+// ra = {RN(1/d_i), a_i = RN(c1 RN(1/d_i))} (a_0 = 0), pg = {P_i, g_i} with
+// g_i = -c_i (g_{n-1} = 0) and P_i the product of a from the segment start
+// to i, q = Q_i the product of g from i to the segment end; ag = {A_w, G_w}
+// [S][kPartWarps], each segment's products (1 for an empty segment).
+constexpr int kPartWarps = 8;
+constexpr int kPartMaxChunks = 64;  // chunks per staged line (their barriers fill the first 512 bytes)
+struct PartAxis {
+  const double2* ra;
+  const double2* pg;
+  const double* q;
+  const double2* ag;
+  int mseg;
+  int npad;
+};
+size_t part_smem_bytes(int elem_bytes, int n_line, int axis);
+template <typename T, int AXIS>
+cudaError_t launch_part(const CUtensorMap& map, const SweepParams<T>& p, const PartAxis& pa, cudaStream_t st);
+
 // The bounded-wait limit (ns) of the kernels in bfvm_sweeps.cu (sweeps and
 // the batched engine) and in bfvm_tmem_sweeps.cu, on the current device.
 cudaError_t sweeps_set_wait_limit(unsigned long long ns);

@@ -1,0 +1,266 @@
+// bfvm_part_sweeps.cu -- the partitioned sweeps (bfvm_set_fp64_chain(ctx, 2)).
+//
+// The reference solves each Thomas system with one serial recurrence per
+// line (BioFVM/BioFVM_solvers.cpp:352-777): forward y_i = (p_i + c1 y_{i-1})
+// / d_i, backward x_i = y_i - c_i x_{i+1}.  A thread per line runs that
+// chain element after element, so a sweep's speed is the latency of one
+// dependent step times the line length; the lines an SM can hold at once
+// (its shared memory) bound how many chains hide each other's latency.
+//
+// Here the recurrences are the same linear maps, evaluated by a partition
+// method.  A CTA stages one tile of 32 lines and runs 8 warps over it; warp w
+// owns the segment [w m, (w+1) m) of every line (m = ceil(n/8), rounded to
+// whole 16-byte units).  With a_i = c1 RN(1/d_i), b_i = p_i RN(1/d_i) and
+// g_i = -c_i (g_{n-1} = 0):
+//   1. each warp runs the forward recurrence over its segment from 0:
+//      y0_i = a_i y0_{i-1} + b_i, in place, and publishes its last value;
+//   2. each warp combines the segments before it into the value entering its
+//      own, y_in(w) = A_{w-1} y_in(w-1) + y0_end(w-1) (A_w = product of the
+//      segment's a), then, from its segment's end back to its start, forms
+//      y_i = P_i y_in + y0_i (P_i = product of a from the segment start to i)
+//      and runs the backward recurrence from 0: x0_i = g_i x0_{i+1} + y_i,
+//      publishing its first value;
+//   3. each warp combines the segments after it, x_in(w) = G_{w+1}
+//      x_in(w+1) + x0_start(w+1) (G_w = product of the segment's g), and
+//      forms x_i = Q_i x_in + x0_i (Q_i = product of g from i to the segment
+//      end).
+// The products P, Q, A, G depend only on the coefficients; the host forms
+// them in extended precision and rounds each once.  Every line's chain is
+// now a segment long (25 at n = 200 instead of 200), so a tile finishes in
+// a fraction of the time and the sweep is bound by HBM, not by the chain.
+//
+// The arithmetic is not the reference's operation order: results differ by
+// a few units in the last place per sweep (tests hold the FP64 results to
+// 1e-12 relative per voxel of the reference, as the FP64 short chain is).
+// The FP32 form uses the same kernels with its FP32 storage and FP64
+// arithmetic (each value is stored three times per sweep instead of once).
+//
+// Dirichlet semantics are those of the other sweeps (bfvm_sweeps.cu): the x
+// sweep writes a face line's face values and pins the line ends of an
+// activated substrate before and after; the y and z sweeps keep the input of
+// x-face lines and of whole tiles in an activated face, and restore the two
+// line ends (pinned by the sweep before) after the sweep.
+#include "bfvm_ctx.h"
+#include "bfvm_ptx.cuh"
+#include "bfvm_sweep_common.cuh"
+
+namespace bfvm {
+
+namespace {
+
+constexpr int kTL = 32;  // lines per tile (one per lane)
+
+// Shared memory of one CTA: barriers (kMaxChunks), the segment ends
+// [2][kPartWarps][32] FP64, then the tile (1024-byte aligned for the x
+// sweep's 128B swizzle).
+constexpr int kSegBytes = 2 * kPartWarps * kTL * 8;
+constexpr int kPartHead = 1024 + ((kSegBytes + 1023) / 1024) * 1024;
+
+template <typename T>
+__device__ __forceinline__ T* x_elem(unsigned char* tile, int e, int t) {
+  // element e of line t in the chunked, 128B-swizzled x tile
+  constexpr int EW = 128 / static_cast<int>(sizeof(T));  // elements per 128-byte row
+  constexpr int U = 16 / static_cast<int>(sizeof(T));    // elements per 16-byte unit
+  const int c = e / EW, r = e - c * EW;
+  return reinterpret_cast<T*>(tile + static_cast<size_t>(c) * (kTL * 128) + t * 128 + (((r / U) ^ (t & 7)) << 4) +
+                              (r % U) * static_cast<int>(sizeof(T)));
+}
+
+template <typename T, int AXIS>
+__global__ void __launch_bounds__(32 * kPartWarps) sweep_part_kernel(const __grid_constant__ CUtensorMap map,
+                                                                     const SweepParams<T> p, const PartAxis pa) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base);
+  double* yseg = reinterpret_cast<double*>(base + 1024);  // [kPartWarps][32]
+  double* xseg = yseg + kPartWarps * kTL;
+  unsigned char* tile = base + kPartHead;
+  constexpr int U = 16 / static_cast<int>(sizeof(T));
+  constexpr int CHE = AXIS == 0 ? 128 / static_cast<int>(sizeof(T)) : kRingRows;  // elements per chunk
+  constexpr uint32_t kChunkBytes = AXIS == 0 ? kTL * 128u : kRingRows * kTL * static_cast<uint32_t>(sizeof(T));
+  const int w = threadIdx.x >> 5, t = threadIdx.x & 31;
+  const int nx = p.nx, ny = p.ny, nz = p.nz, S = p.S;
+  const int n = AXIS == 0 ? nx : (AXIS == 1 ? ny : nz);
+  const int C = (n + CHE - 1) / CHE;
+  const int s = blockIdx.z;
+  const bool act = p.active[s] != 0;
+  // tile coordinates: x: lines (j0 + t, k); y: lines (i0 + t, k); z: lines (i0 + t, j)
+  const int l0 = blockIdx.x * kTL, m = blockIdx.y;
+  if (AXIS != 0 && act && (m == 0 || m == (AXIS == 1 ? nz : ny) - 1)) return;  // a face tile is final already
+
+  if (threadIdx.x == 0) {
+    prefetch_tmap(&map);
+    for (int c = 0; c < C; ++c) mbar_init(smem_u32(&bars[c]), 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int c = 0; c < C; ++c) {
+      const uint32_t bar = smem_u32(&bars[c]);
+      mbar_expect_tx(bar, kChunkBytes);
+      const uint32_t dst = smem_u32(tile + static_cast<size_t>(c) * kChunkBytes);
+      if (AXIS == 0)
+        tma_load_4d(dst, &map, bar, c * CHE, l0, m, s);
+      else if (AXIS == 1)
+        tma_load_4d(dst, &map, bar, l0, c * CHE, m, s);
+      else
+        tma_load_4d(dst, &map, bar, l0, m, c * CHE, s);
+    }
+  }
+  const int mseg = pa.mseg;
+  const int e_lo = w * mseg, e_hi = min(n, e_lo + mseg);
+  // wait for the chunks this warp's segment touches
+  bool ok = true;
+  for (int c = e_lo / CHE; c < C && c * CHE < e_hi; ++c)
+    if (ok) ok = mbar_wait(smem_u32(&bars[c]), 0u);
+
+  const int l = l0 + t;  // this lane's line (j for x, i for y and z)
+  const bool valid = l < (AXIS == 0 ? ny : nx);
+  bool face;
+  if (AXIS == 0)
+    face = act && (l == 0 || l == ny - 1 || m == 0 || m == nz - 1);
+  else
+    face = act && (l == 0 || l == nx - 1);
+  // y/z: lanes in an x face, and lanes past nx, keep their input
+  const bool keep = AXIS != 0 && (face || !valid);
+  const double off = kF32<T> ? p.off[s] : 0.0;
+  const double shift = kF32<T> ? p.shift[s] : 0.0;
+  auto elem = [&](int e) -> T* {
+    if constexpr (AXIS == 0)
+      return x_elem<T>(tile, e, t);
+    else
+      return reinterpret_cast<T*>(tile) + static_cast<size_t>(e) * kTL + t;
+  };
+  T e0v = T(0), e1v = T(0);  // x: the x-face values; y/z: the line ends' input
+  if (AXIS == 0) {
+    if (act && valid && !face) {
+      e0v = static_cast<T>(p.xface[(static_cast<size_t>(0 * S + s) * nz + m) * ny + l] - off);
+      e1v = static_cast<T>(p.xface[(static_cast<size_t>(1 * S + s) * nz + m) * ny + l] - off);
+      // the pin before the sweep, by the warps that own the two ends
+      if (e_lo == 0 && e_hi > 0) *elem(0) = e0v;
+      if (e_lo <= n - 1 && n - 1 < e_hi) *elem(n - 1) = e1v;
+    }
+  } else if (act) {
+    if (e_lo == 0 && e_hi > 0) e0v = *elem(0);
+    if (e_lo <= n - 1 && n - 1 < e_hi) e1v = *elem(n - 1);
+  }
+  const double2* __restrict__ ra = pa.ra + static_cast<size_t>(s) * pa.npad;  // {RN(1/d), a}
+  const double2* __restrict__ pg = pa.pg + static_cast<size_t>(s) * pa.npad;  // {P, g}
+  const double* __restrict__ qq = pa.q + static_cast<size_t>(s) * pa.npad;    // Q
+  const double2* __restrict__ ag = pa.ag + static_cast<size_t>(s) * kPartWarps;  // {A_w, G_w}
+
+  // 1. forward over the segment from 0, in place
+  double y = 0.0;
+  if (!keep) {
+    for (int e = e_lo; e < e_hi; ++e) {
+      const double2 c = __ldg(ra + e);
+      T* pe = elem(e);
+      const double v = kF32<T> ? static_cast<double>(*pe) - shift : static_cast<double>(*pe);
+      y = __fma_rn(c.y, y, __dmul_rn(v, c.x));
+      *pe = static_cast<T>(y);
+    }
+  }
+  yseg[w * kTL + t] = y;
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(p.status, kDevTimeout);
+    if (threadIdx.x == 0) {  // the other chunks' loads must land before the CTA exits
+      for (int c = 0; c < C; ++c) mbar_wait(smem_u32(&bars[c]), 0u);
+    }
+    __syncthreads();
+    return;
+  }
+  // 2. the value entering this segment, then y and the backward from 0
+  double yin = 0.0;
+  for (int v = 0; v < w; ++v) yin = __fma_rn(__ldg(&ag[v].x), yin, yseg[v * kTL + t]);
+  double x = 0.0;
+  if (!keep) {
+    for (int e = e_hi - 1; e >= e_lo; --e) {
+      const double2 c = __ldg(pg + e);
+      T* pe = elem(e);
+      const double ye = __fma_rn(c.x, yin, static_cast<double>(*pe));
+      x = __fma_rn(c.y, x, ye);
+      *pe = static_cast<T>(x);
+    }
+  }
+  xseg[w * kTL + t] = x;
+  __syncthreads();
+  // 3. the value entering this segment from the right, then x
+  double xin = 0.0;
+  for (int v = kPartWarps - 1; v > w; --v) xin = __fma_rn(__ldg(&ag[v].y), xin, xseg[v * kTL + t]);
+  if (!keep) {
+    if (AXIS == 0 && face && valid) {
+      // a face line takes the face plane's values
+      const double* fv = (m == 0 || m == nz - 1)
+                             ? p.zface + ((static_cast<size_t>(m == 0 ? 0 : 1) * S + s) * ny + l) * nx
+                             : p.yface + ((static_cast<size_t>(l == 0 ? 0 : 1) * S + s) * nz + m) * nx;
+      for (int e = e_lo; e < e_hi; ++e) *elem(e) = static_cast<T>(fv[e] - off);
+    } else {
+      for (int e = e_lo; e < e_hi; ++e) {
+        T* pe = elem(e);
+        *pe = static_cast<T>(__fma_rn(__ldg(qq + e), xin, static_cast<double>(*pe)));
+      }
+      // the pin after the sweep
+      if (act && (AXIS != 0 || valid)) {
+        if (e_lo == 0 && e_hi > 0) *elem(0) = e0v;
+        if (e_lo <= n - 1 && n - 1 < e_hi) *elem(n - 1) = e1v;
+      }
+    }
+  }
+  // 4. the tile back to the field (rows or lines past the grid are clipped)
+  fence_async_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int c = 0; c < C; ++c) {
+      const uint32_t src = smem_u32(tile + static_cast<size_t>(c) * kChunkBytes);
+      if (AXIS == 0)
+        tma_store_4d(&map, src, c * CHE, l0, m, s);
+      else if (AXIS == 1)
+        tma_store_4d(&map, src, l0, c * CHE, m, s);
+      else
+        tma_store_4d(&map, src, l0, m, c * CHE, s);
+    }
+    tma_store_commit();
+    tma_store_wait_read();
+  }
+  (void)U;
+}
+
+}  // namespace
+
+size_t part_smem_bytes(int eb, int n_line, int axis) {
+  const int che = axis == 0 ? 128 / eb : kRingRows;
+  const int C = (n_line + che - 1) / che;
+  const size_t chunk = axis == 0 ? static_cast<size_t>(kTL) * 128 : static_cast<size_t>(kRingRows) * kTL * eb;
+  return 1024 /* alignment pad */ + kPartHead + static_cast<size_t>(C) * chunk;
+}
+
+template <typename T, int AXIS>
+cudaError_t launch_part(const CUtensorMap& map, const SweepParams<T>& p, const PartAxis& pa, cudaStream_t st) {
+  const int n = AXIS == 0 ? p.nx : (AXIS == 1 ? p.ny : p.nz);
+  const size_t smem = part_smem_bytes(static_cast<int>(sizeof(T)), n, AXIS);
+  if (smem > 227 * 1024 || (n + (AXIS == 0 ? 128 / static_cast<int>(sizeof(T)) : kRingRows) - 1) /
+                                   (AXIS == 0 ? 128 / static_cast<int>(sizeof(T)) : kRingRows) > kPartMaxChunks)
+    return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(sweep_part_kernel<T, AXIS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  const int lines = AXIS == 0 ? p.ny : p.nx;
+  const dim3 grid((lines + kTL - 1) / kTL, AXIS == 2 ? p.ny : p.nz, p.S);
+  sweep_part_kernel<T, AXIS><<<grid, 32 * kPartWarps, smem, st>>>(map, p, pa);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_part<double, 0>(const CUtensorMap&, const SweepParams<double>&, const PartAxis&,
+                                            cudaStream_t);
+template cudaError_t launch_part<double, 1>(const CUtensorMap&, const SweepParams<double>&, const PartAxis&,
+                                            cudaStream_t);
+template cudaError_t launch_part<double, 2>(const CUtensorMap&, const SweepParams<double>&, const PartAxis&,
+                                            cudaStream_t);
+template cudaError_t launch_part<float, 0>(const CUtensorMap&, const SweepParams<float>&, const PartAxis&,
+                                           cudaStream_t);
+template cudaError_t launch_part<float, 1>(const CUtensorMap&, const SweepParams<float>&, const PartAxis&,
+                                           cudaStream_t);
+template cudaError_t launch_part<float, 2>(const CUtensorMap&, const SweepParams<float>&, const PartAxis&,
+                                           cudaStream_t);
+
+}  // namespace bfvm

@@ -869,17 +869,17 @@ static size_t x_tmem_smem(int nx, int ns, int nt, int kf) {
 }
 
 // The TMEM x sweep applies (FP64, agents not fused, 32-line tiles, lines of
-// at least 2 chunks and at most 32 slots per ring): by default only on
-// lines past 16 chunks, where the per-tile x sweep holds 1-2 tiles per SM;
-// at sweep TMEM level 2 on every such line.  *ns shared-memory rings and *nt
-// TMEM rings (the most that fit), *kf input slots per TMEM ring.  Measured on
-// B200 against the per-tile x sweep (x interval with the source kernel):
-// 256^3 0.170 against 0.179 ms, 160^3 x 6 0.115 against 0.118, but 200^3 x 4
-// 0.173 against 0.159 -- so shorter lines keep the per-tile sweep by default.
+// at least 2 chunks and at most 32 slots per ring): by default on lines of
+// at least 3 chunks (33 voxels), at sweep TMEM level 2 from 2 chunks.  *ns
+// shared-memory rings and *nt TMEM rings (the most that fit), *kf input
+// slots per TMEM ring.  Each finished chunk leaves by one bulk tensor store
+// from its staging chunk; measured on B200 at cube200 (200^3 x 4) against
+// the per-tile x sweep: 0.149 against 0.190 ms (the earlier transposed
+// write-out through global stores took 0.198).
 static bool use_tmem_x(int eb, int nx, bool fused_agents, const SweepConfig& cfg, int* ns, int* nt, int* kf) {
   const int C = (nx + 15) / 16;
   if (eb != 8 || fused_agents || cfg.persistent < 1 || cfg.tmem == 0 || cfg.x_lines != 32 || C < 2) return false;
-  if (cfg.tmem < 2 && C <= kTmemMaxChunks) return false;
+  if (cfg.tmem < 2 && C < 3) return false;
   const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
   int best = 0;
   for (int t = kTmemRingTmem; t >= 1; --t) {

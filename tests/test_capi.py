@@ -80,8 +80,8 @@ def test_tmem_sweep_plan():
     """The tensor-memory sweep configurations (shared-memory rings, TMEM
     rings, input slots per TMEM ring) chosen per line length: those measured
     on B200 (y/z: 3 + 4 rings at lines of 200, fewer shared-memory rings as
-    lines grow, TMEM rings partly resident past 256; x by default only past
-    256), two input slots where a third would cost a ring, and where the
+    lines grow, TMEM rings partly resident past 256; x by default from 33,
+    at level 2 from 17), two input slots where a third would cost a ring, and where the
     shared-memory schedules take over (y/z lines under 3 chunks of 16 rows,
     x lines under 2 at level 2, any line past 736 = 46 chunks, whose 30
     resident chunks and 2 input slots fill a ring's 32 slots)."""
@@ -91,8 +91,8 @@ def test_tmem_sweep_plan():
     for n, want in yz.items():
         assert _plan(1, n) == want, n
         assert _plan(1, n, 0) == (0, 0, 0), n
-    x1 = {200: (0, 0, 0), 256: (0, 0, 0), 257: (2, 4, 3), 300: (1, 4, 3), 400: (0, 4, 3), 640: (0, 2, 2),
-          700: (0, 1, 3), 736: (0, 1, 2), 737: (0, 0, 0), 800: (0, 0, 0)}
+    x1 = {32: (0, 0, 0), 33: (3, 4, 3), 200: (3, 4, 2), 256: (2, 4, 3), 257: (2, 4, 3), 300: (1, 4, 3),
+          400: (0, 4, 3), 640: (0, 2, 2), 700: (0, 1, 3), 736: (0, 1, 2), 737: (0, 0, 0), 800: (0, 0, 0)}
     for n, want in x1.items():
         assert _plan(0, n) == want, n
     x2 = {17: (3, 4, 2), 20: (3, 4, 2), 200: (3, 4, 2), 256: (2, 4, 3), 640: (0, 2, 2), 16: (0, 0, 0)}

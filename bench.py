@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--fp64-chain", type=int, choices=[0, 1, 2], default=0,
+                    help="arithmetic of the timed solve (bfvm_set_fp64_chain): 0 the reference's (default)")
     ap.add_argument("--workload", choices=["cube200", "uneven_batch", "serve", "accuracy"], default="cube200",
                     help="cube200 (default): the single-solve benchmark line; the others run the batched, "
                          "serving and FP32-accuracy suites and print one JSON line each")
@@ -365,6 +367,7 @@ def main():
 
     wl = W.cube200()
     me = Microenvironment.from_workload(wl, precision=args.precision, device=local)
+    me.set_fp64_chain(args.fp64_chain)
     stream = torch.cuda.ExternalStream(me.stream, device=torch.device("cuda", local))
     N, S, A = wl.n_voxels, wl.S, wl.n_agents
 
@@ -410,7 +413,7 @@ def main():
 
     # ---- the opt-in short FP64 chain, same resident step ----------------------
     short = None
-    if args.precision == "fp64":
+    if args.precision == "fp64" and args.fp64_chain == 0:
         me.set_fp64_chain(1)
         me.simulate_diffusion_decay(3, sources=True)
         me.synchronize()
@@ -418,7 +421,7 @@ def main():
         ms_short, kms_short, _ = time_resident(me, args.steps, stream)
         if dist is not None:
             ms_short = max_over_ranks(ms_short, dist, "cuda")
-        me.set_fp64_chain(0)
+        me.set_fp64_chain(args.fp64_chain)
         short = {"value": world * N * S / (ms_short * 1e-3), "unit": UNIT, "ms_per_step": ms_short,
                  "roofline": roofline_of(kms_short, ms_short),
                  "arithmetic": "forward y = fma(RN(c1/d), y, v*RN(1/d)); within 1e-12 relative per voxel of the "
@@ -514,7 +517,10 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}",
+                "config": {"workload": WORKLOAD if args.fp64_chain == 0 and args.precision == "fp64"
+                           else WORKLOAD.replace("FP64", args.precision.upper()).replace(
+                               "the reference's arithmetic (bit-identical)", f"arithmetic chain {args.fp64_chain}"),
+                           "parallelism": f"replicas x{world}",
                            "l2": "inputs larger than L2 (256 MB field per GPU), no flush",
                            "voxels": N, "substrates": S, "agents": A},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "fp64_short_chain": short,

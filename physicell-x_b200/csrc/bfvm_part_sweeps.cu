@@ -49,12 +49,14 @@ namespace bfvm {
 namespace {
 
 constexpr int kTL = 32;  // lines per tile (one per lane)
+constexpr int kPartMaxBuffers = 3;
 
-// Shared memory of one CTA: barriers (kMaxChunks), the segment ends
-// [2][kPartWarps][32] FP64, then the tile (1024-byte aligned for the x
-// sweep's 128B swizzle).
+// Shared memory of one CTA: barriers [kPartMaxBuffers][kPartMaxChunks], the
+// segment ends [2][kPartWarps][32] FP64, then the tile buffers, each
+// 1024-byte aligned (the x sweep's 128B swizzle).
+constexpr int kBarBytes = kPartMaxBuffers * kPartMaxChunks * 8;
 constexpr int kSegBytes = 2 * kPartWarps * kTL * 8;
-constexpr int kPartHead = 1024 + ((kSegBytes + 1023) / 1024) * 1024;
+constexpr int kPartHead = ((kBarBytes + 1023) / 1024) * 1024 + ((kSegBytes + 1023) / 1024) * 1024;
 
 template <typename T>
 __device__ __forceinline__ T* x_elem(unsigned char* tile, int e, int t) {
@@ -67,52 +69,77 @@ __device__ __forceinline__ T* x_elem(unsigned char* tile, int e, int t) {
 }
 
 template <typename T, int AXIS>
-__global__ void __launch_bounds__(32 * kPartWarps) sweep_part_kernel(const __grid_constant__ CUtensorMap map,
-                                                                     const SweepParams<T> p, const PartAxis pa) {
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base);
-  double* yseg = reinterpret_cast<double*>(base + 1024);  // [kPartWarps][32]
-  double* xseg = yseg + kPartWarps * kTL;
-  unsigned char* tile = base + kPartHead;
-  constexpr int U = 16 / static_cast<int>(sizeof(T));
-  constexpr int CHE = AXIS == 0 ? 128 / static_cast<int>(sizeof(T)) : kRingRows;  // elements per chunk
-  constexpr uint32_t kChunkBytes = AXIS == 0 ? kTL * 128u : kRingRows * kTL * static_cast<uint32_t>(sizeof(T));
+struct PartShape {
+  static constexpr int CHE = AXIS == 0 ? 128 / static_cast<int>(sizeof(T)) : kRingRows;  // elements per chunk
+  static constexpr uint32_t kChunkBytes =
+      AXIS == 0 ? kTL * 128u : kRingRows * kTL * static_cast<uint32_t>(sizeof(T));
+};
+
+// The tiles of one sweep: (line tile, m, s) with m = k for x and y, j for z.
+template <int AXIS>
+__device__ __forceinline__ void part_decode(long long tile, int nx, int ny, int nz, int& l0, int& m, int& s) {
+  const int ntl = ((AXIS == 0 ? ny : nx) + kTL - 1) / kTL;
+  const long long per_s = static_cast<long long>(ntl) * (AXIS == 2 ? ny : nz);
+  s = static_cast<int>(tile / per_s);
+  const long long r = tile - static_cast<long long>(s) * per_s;
+  m = static_cast<int>(r / ntl);
+  l0 = static_cast<int>(r - static_cast<long long>(m) * ntl) * kTL;
+}
+
+// Issue the TMA loads of a tile's C chunks into `buf`, completing on bars[c].
+template <typename T, int AXIS>
+__device__ __forceinline__ void part_issue(const CUtensorMap* map, unsigned char* buf, uint64_t* bars, int C, int l0,
+                                           int m, int s) {
+  using Sh = PartShape<T, AXIS>;
+  for (int c = 0; c < C; ++c) {
+    const uint32_t bar = smem_u32(&bars[c]);
+    mbar_expect_tx(bar, Sh::kChunkBytes);
+    const uint32_t dst = smem_u32(buf + static_cast<size_t>(c) * Sh::kChunkBytes);
+    if (AXIS == 0)
+      tma_load_4d(dst, map, bar, c * Sh::CHE, l0, m, s);
+    else if (AXIS == 1)
+      tma_load_4d(dst, map, bar, l0, c * Sh::CHE, m, s);
+    else
+      tma_load_4d(dst, map, bar, l0, m, c * Sh::CHE, s);
+  }
+}
+
+// Store a finished tile from `buf` (rows or lines past the grid are clipped).
+template <typename T, int AXIS>
+__device__ __forceinline__ void part_store(const CUtensorMap* map, unsigned char* buf, int C, int l0, int m, int s) {
+  using Sh = PartShape<T, AXIS>;
+  for (int c = 0; c < C; ++c) {
+    const uint32_t src = smem_u32(buf + static_cast<size_t>(c) * Sh::kChunkBytes);
+    if (AXIS == 0)
+      tma_store_4d(map, src, c * Sh::CHE, l0, m, s);
+    else if (AXIS == 1)
+      tma_store_4d(map, src, l0, c * Sh::CHE, m, s);
+    else
+      tma_store_4d(map, src, l0, m, c * Sh::CHE, s);
+  }
+  tma_store_commit();
+}
+
+// The partition method on one staged tile (see the file comment): waits for
+// the chunks of this warp's segment (barrier phase `par`), runs the three
+// passes in place, and calls after_pass1() between the first two (a point
+// every thread reaches after a CTA barrier).  Returns false (status set) if
+// a wait gave up.
+template <typename T, int AXIS, typename Hook>
+__device__ __forceinline__ bool part_tile(unsigned char* tile, uint64_t* bars, uint32_t par,
+                                          const SweepParams<T>& p, const PartAxis& pa, int l0, int m, int s,
+                                          double* yseg, double* xseg, Hook&& after_pass1) {
+  using Sh = PartShape<T, AXIS>;
   const int w = threadIdx.x >> 5, t = threadIdx.x & 31;
   const int nx = p.nx, ny = p.ny, nz = p.nz, S = p.S;
   const int n = AXIS == 0 ? nx : (AXIS == 1 ? ny : nz);
-  const int C = (n + CHE - 1) / CHE;
-  const int s = blockIdx.z;
   const bool act = p.active[s] != 0;
-  // tile coordinates: x: lines (j0 + t, k); y: lines (i0 + t, k); z: lines (i0 + t, j)
-  const int l0 = blockIdx.x * kTL, m = blockIdx.y;
-  if (AXIS != 0 && act && (m == 0 || m == (AXIS == 1 ? nz : ny) - 1)) return;  // a face tile is final already
-
-  if (threadIdx.x == 0) {
-    prefetch_tmap(&map);
-    for (int c = 0; c < C; ++c) mbar_init(smem_u32(&bars[c]), 1);
-    fence_barrier_init();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int c = 0; c < C; ++c) {
-      const uint32_t bar = smem_u32(&bars[c]);
-      mbar_expect_tx(bar, kChunkBytes);
-      const uint32_t dst = smem_u32(tile + static_cast<size_t>(c) * kChunkBytes);
-      if (AXIS == 0)
-        tma_load_4d(dst, &map, bar, c * CHE, l0, m, s);
-      else if (AXIS == 1)
-        tma_load_4d(dst, &map, bar, l0, c * CHE, m, s);
-      else
-        tma_load_4d(dst, &map, bar, l0, m, c * CHE, s);
-    }
-  }
   const int mseg = pa.mseg;
   const int e_lo = w * mseg, e_hi = min(n, e_lo + mseg);
-  // wait for the chunks this warp's segment touches
+  const int C = (n + Sh::CHE - 1) / Sh::CHE;
   bool ok = true;
-  for (int c = e_lo / CHE; c < C && c * CHE < e_hi; ++c)
-    if (ok) ok = mbar_wait(smem_u32(&bars[c]), 0u);
+  for (int c = e_lo / Sh::CHE; c < C && c * Sh::CHE < e_hi; ++c)
+    if (ok) ok = mbar_wait(smem_u32(&bars[c]), par);
 
   const int l = l0 + t;  // this lane's line (j for x, i for y and z)
   const bool valid = l < (AXIS == 0 ? ny : nx);
@@ -132,17 +159,19 @@ __global__ void __launch_bounds__(32 * kPartWarps) sweep_part_kernel(const __gri
       return reinterpret_cast<T*>(tile) + static_cast<size_t>(e) * kTL + t;
   };
   T e0v = T(0), e1v = T(0);  // x: the x-face values; y/z: the line ends' input
-  if (AXIS == 0) {
-    if (act && valid && !face) {
-      e0v = static_cast<T>(p.xface[(static_cast<size_t>(0 * S + s) * nz + m) * ny + l] - off);
-      e1v = static_cast<T>(p.xface[(static_cast<size_t>(1 * S + s) * nz + m) * ny + l] - off);
-      // the pin before the sweep, by the warps that own the two ends
-      if (e_lo == 0 && e_hi > 0) *elem(0) = e0v;
-      if (e_lo <= n - 1 && n - 1 < e_hi) *elem(n - 1) = e1v;
+  if (ok) {
+    if (AXIS == 0) {
+      if (act && valid && !face) {
+        e0v = static_cast<T>(p.xface[(static_cast<size_t>(0 * S + s) * nz + m) * ny + l] - off);
+        e1v = static_cast<T>(p.xface[(static_cast<size_t>(1 * S + s) * nz + m) * ny + l] - off);
+        // the pin before the sweep, by the warps that own the two ends
+        if (e_lo == 0 && e_hi > 0) *elem(0) = e0v;
+        if (e_lo <= n - 1 && n - 1 < e_hi) *elem(n - 1) = e1v;
+      }
+    } else if (act) {
+      if (e_lo == 0 && e_hi > 0) e0v = *elem(0);
+      if (e_lo <= n - 1 && n - 1 < e_hi) e1v = *elem(n - 1);
     }
-  } else if (act) {
-    if (e_lo == 0 && e_hi > 0) e0v = *elem(0);
-    if (e_lo <= n - 1 && n - 1 < e_hi) e1v = *elem(n - 1);
   }
   const double2* __restrict__ ra = pa.ra + static_cast<size_t>(s) * pa.npad;  // {RN(1/d), a}
   const double2* __restrict__ pg = pa.pg + static_cast<size_t>(s) * pa.npad;  // {P, g}
@@ -151,7 +180,7 @@ __global__ void __launch_bounds__(32 * kPartWarps) sweep_part_kernel(const __gri
 
   // 1. forward over the segment from 0, in place
   double y = 0.0;
-  if (!keep) {
+  if (!keep && ok) {
     for (int e = e_lo; e < e_hi; ++e) {
       const double2 c = __ldg(ra + e);
       T* pe = elem(e);
@@ -163,12 +192,9 @@ __global__ void __launch_bounds__(32 * kPartWarps) sweep_part_kernel(const __gri
   yseg[w * kTL + t] = y;
   if (__syncthreads_or(!ok)) {
     if (threadIdx.x == 0) atomicExch(p.status, kDevTimeout);
-    if (threadIdx.x == 0) {  // the other chunks' loads must land before the CTA exits
-      for (int c = 0; c < C; ++c) mbar_wait(smem_u32(&bars[c]), 0u);
-    }
-    __syncthreads();
-    return;
+    return false;
   }
+  after_pass1();
   // 2. the value entering this segment, then y and the backward from 0
   double yin = 0.0;
   for (int v = 0; v < w; ++v) yin = __fma_rn(__ldg(&ag[v].x), yin, yseg[v * kTL + t]);
@@ -206,46 +232,190 @@ __global__ void __launch_bounds__(32 * kPartWarps) sweep_part_kernel(const __gri
       }
     }
   }
-  // 4. the tile back to the field (rows or lines past the grid are clipped)
-  fence_async_smem();
+  fence_async_smem();  // the results are read by the bulk store next
   __syncthreads();
+  return true;
+}
+
+// One CTA per tile (tiles too large for two buffers).
+template <typename T, int AXIS>
+__global__ void __launch_bounds__(32 * kPartWarps) sweep_part_kernel(const __grid_constant__ CUtensorMap map,
+                                                                     const SweepParams<T> p, const PartAxis pa) {
+  using Sh = PartShape<T, AXIS>;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base);
+  double* yseg = reinterpret_cast<double*>(base + ((kBarBytes + 1023) / 1024) * 1024);
+  double* xseg = yseg + kPartWarps * kTL;
+  unsigned char* tile = base + kPartHead;
+  const int n = AXIS == 0 ? p.nx : (AXIS == 1 ? p.ny : p.nz);
+  const int C = (n + Sh::CHE - 1) / Sh::CHE;
+  const int s = blockIdx.z;
+  const int l0 = blockIdx.x * kTL, m = blockIdx.y;
+  if (AXIS != 0 && p.active[s] != 0 && (m == 0 || m == (AXIS == 1 ? p.nz : p.ny) - 1)) return;  // final already
   if (threadIdx.x == 0) {
-    for (int c = 0; c < C; ++c) {
-      const uint32_t src = smem_u32(tile + static_cast<size_t>(c) * kChunkBytes);
-      if (AXIS == 0)
-        tma_store_4d(&map, src, c * CHE, l0, m, s);
-      else if (AXIS == 1)
-        tma_store_4d(&map, src, l0, c * CHE, m, s);
-      else
-        tma_store_4d(&map, src, l0, m, c * CHE, s);
-    }
-    tma_store_commit();
+    prefetch_tmap(&map);
+    for (int c = 0; c < C; ++c) mbar_init(smem_u32(&bars[c]), 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) part_issue<T, AXIS>(&map, tile, bars, C, l0, m, s);
+  const bool ok = part_tile<T, AXIS>(tile, bars, 0u, p, pa, l0, m, s, yseg, xseg, [] {});
+  if (threadIdx.x == 0) {
+    if (ok) part_store<T, AXIS>(&map, tile, C, l0, m, s);
+    else
+      for (int c = 0; c < C; ++c) mbar_wait(smem_u32(&bars[c]), 0u);  // loads land before the CTA exits
     tma_store_wait_read();
   }
-  (void)U;
+}
+
+// Persistent: a CTA takes tiles blockIdx.x, + gridDim.x, ... (face tiles of
+// the y and z sweeps skipped) through NB tile buffers, tile k in buffer
+// k % NB.  Tile k + NB loads into the buffer of tile k once tile k's store
+// has read it -- issued during tile k + 1, after its first pass -- so each
+// load has the better part of NB - 1 tiles' work to land.
+template <typename T, int AXIS>
+__global__ void __launch_bounds__(32 * kPartWarps) sweep_part_pers_kernel(const __grid_constant__ CUtensorMap map,
+                                                                          const SweepParams<T> p, const PartAxis pa,
+                                                                          long long ntiles, int NB,
+                                                                          uint32_t buf_bytes) {
+  using Sh = PartShape<T, AXIS>;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base);  // [NB][kPartMaxChunks]
+  double* yseg = reinterpret_cast<double*>(base + ((kBarBytes + 1023) / 1024) * 1024);
+  double* xseg = yseg + kPartWarps * kTL;
+  unsigned char* bufs = base + kPartHead;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int n = AXIS == 0 ? nx : (AXIS == 1 ? ny : nz);
+  const int nm = AXIS == 2 ? ny : nz;
+  const int C = (n + Sh::CHE - 1) / Sh::CHE;
+  auto skip = [&](long long tile) {
+    if (AXIS == 0) return false;
+    int l0, m, s;
+    part_decode<AXIS>(tile, nx, ny, nz, l0, m, s);
+    return p.active[s] != 0 && (m == 0 || m == nm - 1);
+  };
+  auto next = [&](long long tile) {
+    do {
+      tile += gridDim.x;
+    } while (tile < ntiles && skip(tile));
+    return tile;
+  };
+  auto issue = [&](long long tile, int b) {
+    int l0, m, s;
+    part_decode<AXIS>(tile, nx, ny, nz, l0, m, s);
+    part_issue<T, AXIS>(&map, bufs + static_cast<size_t>(b) * buf_bytes, bars + b * kPartMaxChunks, C, l0, m, s);
+  };
+  if (threadIdx.x == 0) {
+    prefetch_tmap(&map);
+    for (int q = 0; q < NB * kPartMaxChunks; ++q) mbar_init(smem_u32(&bars[q]), 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  // the first NB tiles of this CTA
+  long long seq[kPartMaxBuffers];
+  seq[0] = next(static_cast<long long>(blockIdx.x) - gridDim.x);
+  for (int b = 1; b < NB; ++b) seq[b] = seq[b - 1] < ntiles ? next(seq[b - 1]) : ntiles;
+  int iss[kPartMaxBuffers] = {0, 0, 0};  // loads issued into each buffer (thread 0)
+  if (threadIdx.x == 0)
+    for (int b = 0; b < NB; ++b)
+      if (seq[b] < ntiles) {
+        issue(seq[b], b);
+        ++iss[b];
+      }
+  long long cur = seq[0];
+  long long last_issued = seq[NB - 1];  // the newest tile issued (or ntiles)
+  long long refill = -1;                // tile to load into the buffer of the previous tile
+  int prev_buf = -1;
+  bool ok = true;
+  for (long long k = 0; cur < ntiles && ok; ++k) {
+    const int b = static_cast<int>(k % NB);
+    const uint32_t par = static_cast<uint32_t>((k / NB) & 1);
+    int l0, m, s;
+    part_decode<AXIS>(cur, nx, ny, nz, l0, m, s);
+    unsigned char* tile = bufs + static_cast<size_t>(b) * buf_bytes;
+    const long long rf = refill;
+    const int pb = prev_buf;
+    ok = part_tile<T, AXIS>(tile, bars + b * kPartMaxChunks, par, p, pa, l0, m, s, yseg, xseg, [&] {
+      if (rf >= 0 && threadIdx.x == 0) {
+        tma_store_wait_read();  // the previous tile's store has read its buffer
+        issue(rf, pb);
+        ++iss[pb];
+      }
+    });
+    if (!ok) break;
+    if (threadIdx.x == 0) part_store<T, AXIS>(&map, tile, C, l0, m, s);
+    // the tile after the newest one issued goes into this buffer, next round
+    refill = last_issued < ntiles ? next(last_issued) : ntiles;
+    if (refill >= ntiles) refill = -1;
+    else last_issued = refill;
+    prev_buf = b;
+    cur = next(cur);
+  }
+  if (threadIdx.x == 0) {
+    tma_store_wait_read();
+    if (!ok) {
+      // a wait gave up: every buffer's newest loads land (each wait bounded) before the CTA exits
+      for (int b = 0; b < NB; ++b)
+        if (iss[b] > 0)
+          for (int c = 0; c < C; ++c)
+            mbar_wait(smem_u32(&bars[b * kPartMaxChunks + c]), static_cast<uint32_t>((iss[b] - 1) & 1));
+    }
+  }
 }
 
 }  // namespace
 
-size_t part_smem_bytes(int eb, int n_line, int axis) {
+static size_t part_buf_bytes(int eb, int n_line, int axis) {
   const int che = axis == 0 ? 128 / eb : kRingRows;
   const int C = (n_line + che - 1) / che;
   const size_t chunk = axis == 0 ? static_cast<size_t>(kTL) * 128 : static_cast<size_t>(kRingRows) * kTL * eb;
-  return 1024 /* alignment pad */ + kPartHead + static_cast<size_t>(C) * chunk;
+  return (static_cast<size_t>(C) * chunk + 1023) / 1024 * 1024;
+}
+
+size_t part_smem_bytes(int eb, int n_line, int axis) {
+  return 1024 /* alignment pad */ + kPartHead + part_buf_bytes(eb, n_line, axis);
 }
 
 template <typename T, int AXIS>
 cudaError_t launch_part(const CUtensorMap& map, const SweepParams<T>& p, const PartAxis& pa, cudaStream_t st) {
+  constexpr int eb = static_cast<int>(sizeof(T));
   const int n = AXIS == 0 ? p.nx : (AXIS == 1 ? p.ny : p.nz);
-  const size_t smem = part_smem_bytes(static_cast<int>(sizeof(T)), n, AXIS);
-  if (smem > 227 * 1024 || (n + (AXIS == 0 ? 128 / static_cast<int>(sizeof(T)) : kRingRows) - 1) /
-                                   (AXIS == 0 ? 128 / static_cast<int>(sizeof(T)) : kRingRows) > kPartMaxChunks)
-    return cudaErrorInvalidValue;
+  const int che = AXIS == 0 ? 128 / eb : kRingRows;
+  if ((n + che - 1) / che > kPartMaxChunks) return cudaErrorInvalidValue;
+  const size_t buf = part_buf_bytes(eb, n, AXIS);
+  const size_t lim = 227 * 1024;
+  // buffers per CTA: the most tile buffers per SM over the CTAs that fit
+  // (ties to more CTAs); one buffer means a CTA per tile
+  int NB = 0, best = 0;
+  for (int b = 2; b <= kPartMaxBuffers; ++b) {
+    const size_t smem_b = 1024 + kPartHead + b * buf;
+    if (smem_b > lim) break;
+    const int ctas = static_cast<int>((228 * 1024) / (smem_b + 1024));
+    if (ctas * b > best) {
+      best = ctas * b;
+      NB = b;
+    }
+  }
+  const int lines = AXIS == 0 ? p.ny : p.nx;
+  const int ntl = (lines + kTL - 1) / kTL;
+  if (NB >= 2) {
+    const size_t smem = 1024 + kPartHead + NB * buf;
+    const long long ntiles = static_cast<long long>(ntl) * (AXIS == 2 ? p.ny : p.nz) * p.S;
+    int grid = 0;
+    cudaError_t e = persistent_grid(sweep_part_pers_kernel<T, AXIS>, smem, ntiles, &grid, 32 * kPartWarps);
+    if (e != cudaSuccess) return e;
+    sweep_part_pers_kernel<T, AXIS><<<grid, 32 * kPartWarps, smem, st>>>(map, p, pa, ntiles, NB,
+                                                                         static_cast<uint32_t>(buf));
+    return cudaGetLastError();
+  }
+  const size_t smem = part_smem_bytes(eb, n, AXIS);
+  if (smem > lim) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(sweep_part_kernel<T, AXIS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  const int lines = AXIS == 0 ? p.ny : p.nx;
-  const dim3 grid((lines + kTL - 1) / kTL, AXIS == 2 ? p.ny : p.nz, p.S);
+  const dim3 grid(ntl, AXIS == 2 ? p.ny : p.nz, p.S);
   sweep_part_kernel<T, AXIS><<<grid, 32 * kPartWarps, smem, st>>>(map, p, pa);
   return cudaGetLastError();
 }

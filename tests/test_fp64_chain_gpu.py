@@ -100,7 +100,8 @@ def test_short_chain_cube200_all_steps_against_reference_sample(golden_dir, chai
 
 
 @pytest.mark.parametrize("shape", [(1, 1, 1, 1), (1, 7, 3, 2), (9, 2, 5, 3), (256, 3, 5, 1), (3, 256, 4, 2),
-                                   (5, 4, 256, 1), (129, 65, 33, 3), (33, 100, 57, 3), (200, 40, 37, 2)])
+                                   (5, 4, 256, 1), (129, 65, 33, 3), (33, 100, 57, 3), (200, 40, 37, 2),
+                                   (640, 33, 35, 1), (36, 640, 40, 1), (40, 34, 700, 2)])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_partitioned_sweeps_edge_shapes(shape, precision):
     """The partitioned sweeps on ragged and tiny shapes (segments shorter than
@@ -120,3 +121,21 @@ def test_partitioned_sweeps_edge_shapes(shape, precision):
     else:
         g, r = got.reshape(-1, S), expect.reshape(-1, S)
         assert np.all(np.max(np.abs(g - r), axis=0) <= 1e-5 * np.max(np.abs(r), axis=0))
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_partitioned_sweeps_cube640_lines_against_reference(golden_dir, axis):
+    """cube640's 640-voxel lines (one CTA per tile along that axis) with the
+    partitioned sweeps: every value of the reference's own 5-step fixture
+    sample within 1e-12 relative, and the sums."""
+    import os
+
+    wl = W.cube640_slab(axis)
+    g = np.load(os.path.join(golden_dir, f"{wl.name}_{wl.steps}.npz"))
+    me = Microenvironment.from_workload(wl)
+    me.set_fp64_chain(2)
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    out = me.download_field()
+    me.close()
+    assert _per_voxel(out[g["sample_idx"]], g["sample_val"]) <= FP64_TOL
+    np.testing.assert_allclose(out.reshape(-1, wl.S).sum(axis=0), g["sums"], rtol=FP64_TOL)

@@ -150,7 +150,14 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
         if (sl >= ns) break;
         const double o = off ? off[s0 + sl] : 0.0;
         const int c = sl * PS + iz * BX + ix;
-        auto v = [&](const T* P, int e) { return static_cast<double>(P[e]) + o; };
+        // FP32 fields hold rho - off; an FP64 field is read as it is (adding 0.0
+        // would also turn a -0 into +0, which the reference keeps)
+        auto v = [&](const T* P, int e) {
+          if constexpr (sizeof(T) == 4)
+            return static_cast<double>(P[e]) + o;
+          else
+            return static_cast<double>(P[e]);
+        };
         const double ctr = v(P1, c);
         double gx = 0.0, gy = 0.0, gz = 0.0;
         if (nx > 1) {

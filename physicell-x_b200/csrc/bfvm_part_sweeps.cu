@@ -178,15 +178,29 @@ __device__ __forceinline__ bool part_tile(unsigned char* tile, uint64_t* bars, u
   const double* __restrict__ qq = pa.q + static_cast<size_t>(s) * pa.npad;    // Q
   const double2* __restrict__ ag = pa.ag + static_cast<size_t>(s) * kPartWarps;  // {A_w, G_w}
 
+  // The passes go through a segment in groups of G elements, every load of a
+  // group issued before its arithmetic (the coefficient rows are padded past
+  // n, so their loads need no bound; the staged values do).
+  constexpr int G = 8;
   // 1. forward over the segment from 0, in place
   double y = 0.0;
   if (!keep && ok) {
-    for (int e = e_lo; e < e_hi; ++e) {
-      const double2 c = __ldg(ra + e);
-      T* pe = elem(e);
-      const double v = kF32<T> ? static_cast<double>(*pe) - shift : static_cast<double>(*pe);
-      y = __fma_rn(c.y, y, __dmul_rn(v, c.x));
-      *pe = static_cast<T>(y);
+    for (int e0 = e_lo; e0 < e_hi; e0 += G) {
+      const int ng = e_hi - e0;
+      double2 c[G];
+      double v[G];
+#pragma unroll
+      for (int q = 0; q < G; ++q) {
+        c[q] = __ldg(ra + e0 + q);
+        v[q] = q < ng ? static_cast<double>(*elem(e0 + q)) : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < G; ++q) {
+        if (q < ng) {
+          y = __fma_rn(c[q].y, y, __dmul_rn(kF32<T> ? v[q] - shift : v[q], c[q].x));
+          *elem(e0 + q) = static_cast<T>(y);
+        }
+      }
     }
   }
   yseg[w * kTL + t] = y;
@@ -200,12 +214,25 @@ __device__ __forceinline__ bool part_tile(unsigned char* tile, uint64_t* bars, u
   for (int v = 0; v < w; ++v) yin = __fma_rn(__ldg(&ag[v].x), yin, yseg[v * kTL + t]);
   double x = 0.0;
   if (!keep) {
-    for (int e = e_hi - 1; e >= e_lo; --e) {
-      const double2 c = __ldg(pg + e);
-      T* pe = elem(e);
-      const double ye = __fma_rn(c.x, yin, static_cast<double>(*pe));
-      x = __fma_rn(c.y, x, ye);
-      *pe = static_cast<T>(x);
+    for (int e1 = e_hi - 1; e1 >= e_lo; e1 -= G) {
+      const int ng = e1 - e_lo + 1;  // elements e1, e1 - 1, ... down to e_lo
+      double2 c[G];
+      double v[G];
+#pragma unroll
+      for (int q = 0; q < G; ++q) {
+        if (q < ng) {
+          c[q] = __ldg(pg + e1 - q);
+          v[q] = static_cast<double>(*elem(e1 - q));
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < G; ++q) {
+        if (q < ng) {
+          const double ye = __fma_rn(c[q].x, yin, v[q]);
+          x = __fma_rn(c[q].y, x, ye);
+          *elem(e1 - q) = static_cast<T>(x);
+        }
+      }
     }
   }
   xseg[w * kTL + t] = x;
@@ -221,9 +248,17 @@ __device__ __forceinline__ bool part_tile(unsigned char* tile, uint64_t* bars, u
                              : p.yface + ((static_cast<size_t>(l == 0 ? 0 : 1) * S + s) * nz + m) * nx;
       for (int e = e_lo; e < e_hi; ++e) *elem(e) = static_cast<T>(fv[e] - off);
     } else {
-      for (int e = e_lo; e < e_hi; ++e) {
-        T* pe = elem(e);
-        *pe = static_cast<T>(__fma_rn(__ldg(qq + e), xin, static_cast<double>(*pe)));
+      for (int e0 = e_lo; e0 < e_hi; e0 += G) {
+        const int ng = e_hi - e0;
+        double qv[G], v[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+          qv[q] = __ldg(qq + e0 + q);
+          v[q] = q < ng ? static_cast<double>(*elem(e0 + q)) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < G; ++q)
+          if (q < ng) *elem(e0 + q) = static_cast<T>(__fma_rn(qv[q], xin, v[q]));
       }
       // the pin after the sweep
       if (act && (AXIS != 0 || valid)) {
@@ -275,7 +310,7 @@ __global__ void __launch_bounds__(32 * kPartWarps) sweep_part_kernel(const __gri
 // has read it -- issued during tile k + 1, after its first pass -- so each
 // load has the better part of NB - 1 tiles' work to land.
 template <typename T, int AXIS>
-__global__ void __launch_bounds__(32 * kPartWarps) sweep_part_pers_kernel(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(32 * kPartWarps, 2) sweep_part_pers_kernel(const __grid_constant__ CUtensorMap map,
                                                                           const SweepParams<T> p, const PartAxis pa,
                                                                           long long ntiles, int NB,
                                                                           uint32_t buf_bytes) {

@@ -101,6 +101,14 @@ void drop_step_graph(bfvm_ctx* c) {
   c->graph_key.clear();
 }
 
+// Whether the y (axis 1) or z (axis 2) sweep runs partitioned: chain 2, a
+// line of at least kPartMinLine voxels, and a tile that fits one CTA.
+bool use_part(const bfvm_ctx* c, int axis) {
+  const int n = axis == 1 ? c->ny : c->nz;
+  return c->fp64_chain == 2 && n >= kPartMinLine && (n + kRingRows - 1) / kRingRows <= kPartMaxChunks &&
+         part_smem_bytes(c->eb, n) <= 227 * 1024;
+}
+
 // The launches of one LOD step on c->stream (also while capturing): the
 // standalone source kernel (unless fused or without agents), then the x, y
 // and z sweeps; per-step timing events when ev is given.
@@ -111,19 +119,14 @@ int enqueue_step(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, cudaEven
     const int rc = bfvm_apply_sources(c);  // timed with the x sweep
     if (rc != BFVM_OK) return rc;
   }
-  const bool part = c->fp64_chain == 2;
-  if (part && c->cfg.x_lines != 32) return BFVM_ERR_STATE;  // its x tiles are the 32-line boxes of maps.x
-  if (part)
-    BFVM_CUDA((launch_part<T, 0>(c->maps.x, p, c->part[0], c->stream)));
-  else
-    BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, c->stream));
+  BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, c->stream));
   if (ev) BFVM_CUDA(cudaEventRecord(ev[1], c->stream));
-  if (part)
+  if (use_part(c, 1))
     BFVM_CUDA((launch_part<T, 1>(c->maps.ry, p, c->part[1], c->stream)));
   else
     BFVM_CUDA(launch_sweep_y<T>(c->maps, p, c->cfg, c->stream));
   if (ev) BFVM_CUDA(cudaEventRecord(ev[2], c->stream));
-  if (part)
+  if (use_part(c, 2))
     BFVM_CUDA((launch_part<T, 2>(c->maps.rz, p, c->part[2], c->stream)));
   else
     BFVM_CUDA(launch_sweep_z<T>(c->maps, p, c->cfg, c->stream));
@@ -165,8 +168,7 @@ int capture_step_graph(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, co
 
 template <typename T>
 int run_steps_plain(bfvm_ctx* c, int nsteps, bool sources) {
-  // the partitioned sweeps take no fused sources: the standalone kernel applies them
-  const bool standalone = sources && c->n_agents > 0 && (!c->cfg.fuse_sources || c->fp64_chain == 2);
+  const bool standalone = sources && c->n_agents > 0 && !c->cfg.fuse_sources;
   const SweepParams<T> p = make_params<T>(c, sources && !standalone);
   // Runs of steps replay a captured graph of kGraphSteps steps (the same
   // launches, so the same bits), which removes most of the per-launch host
@@ -1233,15 +1235,6 @@ extern "C" int bfvm_set_fused_sources(bfvm_ctx* c, int fused) {
 extern "C" int bfvm_set_fp64_chain(bfvm_ctx* c, int chain) {
   if (!c || chain < 0 || chain > 2) return BFVM_ERR_ARG;
   if (chain == c->fp64_chain) return BFVM_OK;
-  if (chain == 2) {
-    // the partitioned sweeps stage whole 32-line tiles of up to kMaxChunks chunks
-    const int n_axis[3] = {c->nx, c->ny, c->nz};
-    for (int a = 0; a < 3; ++a)
-      if (part_smem_bytes(c->eb, n_axis[a], a) > 227 * 1024 ||
-          (n_axis[a] + (a == 0 ? 128 / c->eb : kRingRows) - 1) / (a == 0 ? 128 / c->eb : kRingRows) > kPartMaxChunks)
-        return BFVM_ERR_SHAPE;
-    if (c->cfg.x_lines != 32) return BFVM_ERR_STATE;
-  }
   DeviceGuard g(c->device);
   BFVM_CUDA(cudaStreamSynchronize(c->stream));
   const int prev = c->fp64_chain;

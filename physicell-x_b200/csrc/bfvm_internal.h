@@ -211,7 +211,12 @@ struct PartAxis {
   int mseg;
   int npad;
 };
-size_t part_smem_bytes(int elem_bytes, int n_line, int axis);
+size_t part_smem_bytes(int elem_bytes, int n_line);
+// Lines at least this long run the y and z sweeps partitioned under chain 2;
+// shorter lines, and the x sweep, run the short chain on the serial kernels
+// (measured on B200: the partitioned y/z sweep loses at lines of 200 --
+// 0.152 against 0.115 ms at cube200 -- and wins at 640: 2.40 against 3.60).
+constexpr int kPartMinLine = 320;
 template <typename T, int AXIS>
 cudaError_t launch_part(const CUtensorMap& map, const SweepParams<T>& p, const PartAxis& pa, cudaStream_t st);
 

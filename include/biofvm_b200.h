@@ -394,12 +394,26 @@ int bfvm_get_sweep_schedule(bfvm_ctx* ctx, int* persistent);
  * results differ from the reference's by a few units in the last place per
  * sweep, within the 1e-12 relative per-voxel bound the FP64 path is held to
  * (the tests measure it against the oracle).  The back substitution, the
- * sources and the pins are the same in both.  The 2-D solver always uses
- * chain 0.  An FP32 solve's recurrence is FP64 too: chain 0 there is
+ * sources and the pins are the same in both.  chain = 2: chain 1, except
+ * that long y and z lines are solved by a partition
+ * method (by default on lines of at least 512 voxels in FP64 and 288 in
+ * FP32, where it is the faster one): eight warps share each 32-line tile,
+ * each warp running both recurrences over one eighth of the line, joined
+ * through segment products that the host forms in extended precision at
+ * set-up.  Its results are
+ * held to the same 1e-12 bound.  The 2-D solver always uses chain 0.  An
+ * FP32 solve's recurrence is FP64 too: chain 0 there is
  * t = fma(c1, y, v - shift), y = t * RN(1/d); chain 1 is
- * y = fma(c1 * RN(1/d), y, (v - shift) * RN(1/d)). */
+ * y = fma(c1 * RN(1/d), y, (v - shift) * RN(1/d)); chain 2 stores the
+ * partitioned passes' intermediate values in FP32, so its bound is the FP32
+ * path's. */
 int bfvm_set_fp64_chain(bfvm_ctx* ctx, int chain);
 int bfvm_get_fp64_chain(bfvm_ctx* ctx, int* chain);
+/* The shortest y or z line that chain 2 solves partitioned: n_line >= 1,
+ * or -1 for the default of the solve's precision (512 FP64, 288 FP32).
+ * bfvm_get_partition_min_line returns the value in effect. */
+int bfvm_set_partition_min_line(bfvm_ctx* ctx, int n_line);
+int bfvm_get_partition_min_line(bfvm_ctx* ctx, int* n_line);
 
 /* Tensor-memory (TMEM) rings in the FP64 persistent sweeps: on = 1
  * (default) in the y, z and x sweeps on lines of 33 to 736 voxels (the x

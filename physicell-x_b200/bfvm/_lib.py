@@ -69,6 +69,8 @@ _SIGS = {
     "bfvm_set_sweep_tmem": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_set_fp64_chain": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_get_fp64_chain": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "bfvm_set_partition_min_line": (C.c_int, [C.c_void_p, C.c_int]),
+    "bfvm_get_partition_min_line": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "bfvm_tmem_sweep_plan": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                        C.POINTER(C.c_int)]),
     "bfvm_get_sweep_schedule": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),

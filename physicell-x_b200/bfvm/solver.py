@@ -350,8 +350,19 @@ class Microenvironment:
     def set_fp64_chain(self, chain):
         """FP64 forward elimination: 0 (default) the reference's arithmetic,
         bit for bit; 1 the short chain (one FMA per element, within a few
-        ulp of the reference per sweep)."""
+        ulp of the reference per sweep); 2 the short chain with long y and z
+        lines solved by the partition method."""
         check(self.L.bfvm_set_fp64_chain(self.h, int(chain)), "bfvm_set_fp64_chain")
+
+    def set_partition_min_line(self, n_line):
+        """The shortest y/z line chain 2 solves partitioned (-1: the
+        precision's default)."""
+        check(self.L.bfvm_set_partition_min_line(self.h, int(n_line)), "bfvm_set_partition_min_line")
+
+    def get_partition_min_line(self):
+        v = C.c_int()
+        check(self.L.bfvm_get_partition_min_line(self.h, C.byref(v)), "bfvm_get_partition_min_line")
+        return int(v.value)
 
     def get_sweep_schedule(self):
         v = C.c_int()

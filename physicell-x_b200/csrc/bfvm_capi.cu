@@ -85,13 +85,17 @@ constexpr int kMaxTimedSteps = 4096;
 // LOD steps per captured CUDA graph of bfvm_step (four launches each).
 constexpr int kGraphSteps = 16;
 
+int part_min_line(const bfvm_ctx* c) {
+  return c->part_min_line >= 0 ? c->part_min_line : (c->eb == 8 ? kPartMinLine64 : kPartMinLine32);
+}
+
 // Everything a captured step holds by value: the kernels' parameters are
 // built from these (device pointers change only with c->version), the
 // launch shapes from the sweep configuration.
 std::vector<long long> step_key(const bfvm_ctx* c, bool sources) {
   const SweepConfig& g = c->cfg;
   return {c->version, sources ? 1 : 0, c->n_agents, c->track, g.x_lines, g.yz_tile, g.yz_chunk, g.persistent,
-          g.fuse_sources, g.tmem, static_cast<long long>(reinterpret_cast<uintptr_t>(c->d_internal)),
+          g.fuse_sources, g.tmem, part_min_line(c), static_cast<long long>(reinterpret_cast<uintptr_t>(c->d_internal)),
           static_cast<long long>(reinterpret_cast<uintptr_t>(c->d_ae1))};
 }
 
@@ -102,10 +106,10 @@ void drop_step_graph(bfvm_ctx* c) {
 }
 
 // Whether the y (axis 1) or z (axis 2) sweep runs partitioned: chain 2, a
-// line of at least kPartMinLine voxels, and a tile that fits one CTA.
+// line of at least part_min_line voxels, and a tile that fits one CTA.
 bool use_part(const bfvm_ctx* c, int axis) {
   const int n = axis == 1 ? c->ny : c->nz;
-  return c->fp64_chain == 2 && n >= kPartMinLine && (n + kRingRows - 1) / kRingRows <= kPartMaxChunks &&
+  return c->fp64_chain == 2 && n >= part_min_line(c) && (n + kRingRows - 1) / kRingRows <= kPartMaxChunks &&
          part_smem_bytes(c->eb, n) <= 227 * 1024;
 }
 
@@ -1254,6 +1258,20 @@ extern "C" int bfvm_set_fp64_chain(bfvm_ctx* c, int chain) {
 extern "C" int bfvm_get_fp64_chain(bfvm_ctx* c, int* chain) {
   if (!c || !chain) return BFVM_ERR_ARG;
   *chain = c->fp64_chain;
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_set_partition_min_line(bfvm_ctx* c, int n_line) {
+  if (!c || n_line < -1 || n_line == 0) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  c->part_min_line = n_line;
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_get_partition_min_line(bfvm_ctx* c, int* n_line) {
+  if (!c || !n_line) return BFVM_ERR_ARG;
+  *n_line = part_min_line(c);
   return BFVM_OK;
 }
 

@@ -30,6 +30,7 @@ struct bfvm_ctx {
   int screen = 0;              // SweepParams::screen of the 3-D sweeps (kScreenFast: short FP64 chain)
   int screen_exact = 0;        // 1 when no diffusion or decay rate is negative (the exactness screen applies)
   int fp64_chain = 0;          // bfvm_set_fp64_chain: 0 reference-exact, 1 short chain, 2 partitioned
+  int part_min_line = -1;      // bfvm_set_partition_min_line (-1: the default of the precision)
   void* d_part = nullptr;      // partitioned-sweep coefficient rows of the three axes (chain 2)
   bfvm::PartAxis part[3] = {};
   double* d_off = nullptr;      // FP32: per-substrate field offsets [S]

@@ -212,11 +212,15 @@ struct PartAxis {
   int npad;
 };
 size_t part_smem_bytes(int elem_bytes, int n_line);
-// Lines at least this long run the y and z sweeps partitioned under chain 2;
-// shorter lines, and the x sweep, run the short chain on the serial kernels
-// (measured on B200: the partitioned y/z sweep loses at lines of 200 --
-// 0.152 against 0.115 ms at cube200 -- and wins at 640: 2.40 against 3.60).
-constexpr int kPartMinLine = 320;
+// By default, lines at least this long run the y and z sweeps partitioned
+// under chain 2 (bfvm_set_partition_min_line overrides it); shorter lines,
+// and the x sweep, run the short chain on the serial kernels.  Measured on
+// B200, mean y/z sweep time on n^3 cubes, partitioned over serial short
+// chain: FP64 1.23 at n = 200, 1.00 at 384, 1.09 at 448, 0.89 at 512, 0.64
+// at 640; FP32 1.25 at 200, 1.03 at 256, 0.97 at 288, 0.80 at 320, 0.49 at
+// 640 (FP32 tiles are half the bytes, so more CTAs share an SM).
+constexpr int kPartMinLine64 = 512;
+constexpr int kPartMinLine32 = 288;
 template <typename T, int AXIS>
 cudaError_t launch_part(const CUtensorMap& map, const SweepParams<T>& p, const PartAxis& pa, cudaStream_t st);
 

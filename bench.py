@@ -54,9 +54,9 @@ WORKLOAD = ("cube200: 200x200x200 voxels (dx=10 um), 4 substrates, 100000 agents
 # figures.  Keys: (precision, sweep index 0=x 1=y 2=z); the x interval is the
 # standalone source kernel plus the x sweep.
 NCU_TRAFFIC = {
-    ("fp64", 0): (56556032 + 2542336) + (268330496 + 195878656),
-    ("fp64", 1): 266367232 + 194908928,
-    ("fp64", 2): 266125568 + 194762752,
+    ("fp64", 0): (56552448 + 1760768) + (271819776 + 198265856),
+    ("fp64", 1): 266041600 + 197507840,
+    ("fp64", 2): 266002432 + 194630912,
 }
 
 

@@ -29,6 +29,7 @@
 // gradient_kernel is the earlier form (32 z by 8 x of one plane per CTA,
 // rows read with plain loads), kept for grids whose map does not encode.
 #include <algorithm>
+#include <cmath>
 
 #include "bfvm_ctx.h"
 #include "bfvm_ptx.cuh"
@@ -55,6 +56,14 @@ __host__ __device__ constexpr int grad_stage_stride() {  // doubles per x row of
 template <typename T, int NS>
 __host__ __device__ constexpr size_t grad_smem_bytes() {
   return 128 + 128 + kGSlots * grad_slot_bytes<T, NS>() + sizeof(double) * kGTX * grad_stage_stride<NS>();
+}
+
+// The quotient where Markstein's correction does not apply (kept out of
+// line, so the common path carries none of the division sequence): +0 for a
+// numerator of +0, else IEEE division.
+__device__ __noinline__ double grad_quotient_slow(double g, double h) {
+  if (g == 0.0 && !signbit(g)) return 0.0;
+  return g / h;
 }
 
 // Gradients of substrates s0 .. s0+ns-1 (ns <= NS) for the planes [jb, je)
@@ -128,15 +137,22 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
     g -= b;
     const unsigned hw = static_cast<unsigned>(__double2hiint(g)) & 0x7FFFFFFFu;  // |g|'s high word
     const double q0 = g * rh;
-    if (markstein_ok && hw - 0x0A300000u < 0x78300000u - 0x0A300000u) {  // 2^-860 <= |g| < 2^900
-      const double e = __fma_rn(-q0, h, g);
-      return __fma_rn(e, rh, q0);
-    }
-    if (g == 0.0 && !signbit(g)) return 0.0;
-    return g / h;
+    const double e = __fma_rn(-q0, h, g);
+    const double q = __fma_rn(e, rh, q0);
+    // 2^-860 <= |g| < 2^900, or g = +0 (which the correction maps to +0)
+    if (markstein_ok && (hw - 0x0A300000u < 0x78300000u - 0x0A300000u || __double_as_longlong(g) == 0)) return q;
+    return grad_quotient_slow(g, h);
   };
   const int i = i0 + lane, k = k0 + wz;
   const int ix = lane + X0, iz = wz + 1;  // this thread's voxel in a slot
+  // Per axis: a line's two ends take the one-sided difference over dx, the
+  // voxels between the central one over 2 dx.  The neighbours are read in
+  // every case (the halo and the ring hold them) and the end cases select
+  // the centre instead, so the components need no branches.
+  const bool x_lo = i == 0, x_hi = i == nx - 1;
+  const bool z_lo = k == 0, z_hi = k == nz - 1;
+  const double hx = (x_lo || x_hi) ? dx : two_dx, rhx = (x_lo || x_hi) ? rdx : r2dx;
+  const double hz = (z_lo || z_hi) ? dx : two_dx, rhz = (z_lo || z_hi) ? rdx : r2dx;
   for (int j = jb; j < je; ++j) {
     if (j == jb) wait_plane(j);
     if (j + 1 < ny) wait_plane(j + 1);
@@ -145,10 +161,14 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
     const T* P0 = j > 0 ? reinterpret_cast<const T*>(slots + slot_of(j - 1) * grad_slot_bytes<T, NS>()) : P1;
     const T* P2 = j + 1 < ny ? reinterpret_cast<const T*>(slots + slot_of(j + 1) * grad_slot_bytes<T, NS>()) : P1;
     if (i < nx && k < nz) {
+      const bool y_lo = j == 0, y_hi = j == ny - 1;
+      const double hy = (y_lo || y_hi) ? dx : two_dx, rhy = (y_lo || y_hi) ? rdx : r2dx;
+      double g3[3 * NS];
 #pragma unroll
       for (int sl = 0; sl < NS; ++sl) {
-        if (sl >= ns) break;
-        const double o = off ? off[s0 + sl] : 0.0;
+        // substrates past the group's last (sl >= ns) read the map's zero
+        // fill; their values are staged but never written out
+        const double o = (off && sl < ns) ? off[s0 + sl] : 0.0;
         const int c = sl * PS + iz * BX + ix;
         // FP32 fields hold rho - off; an FP64 field is read as it is (adding 0.0
         // would also turn a -0 into +0, which the reference keeps)
@@ -159,35 +179,22 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
             return static_cast<double>(P[e]);
         };
         const double ctr = v(P1, c);
-        double gx = 0.0, gy = 0.0, gz = 0.0;
-        if (nx > 1) {
-          if (i == 0)
-            gx = grad(v(P1, c + 1), ctr, dx, rdx);
-          else if (i == nx - 1)
-            gx = grad(ctr, v(P1, c - 1), dx, rdx);
-          else
-            gx = grad(v(P1, c + 1), v(P1, c - 1), two_dx, r2dx);
-        }
-        if (ny > 1) {
-          if (j == 0)
-            gy = grad(v(P2, c), ctr, dx, rdx);
-          else if (j == ny - 1)
-            gy = grad(ctr, v(P0, c), dx, rdx);
-          else
-            gy = grad(v(P2, c), v(P0, c), two_dx, r2dx);
-        }
-        if (nz > 1) {
-          if (k == 0)
-            gz = grad(v(P1, c + BX), ctr, dx, rdx);
-          else if (k == nz - 1)
-            gz = grad(ctr, v(P1, c - BX), dx, rdx);
-          else
-            gz = grad(v(P1, c + BX), v(P1, c - BX), two_dx, r2dx);
-        }
-        double* o3 = stg + lane * SX + wz * 3 * NS + 3 * sl;
-        o3[0] = gx;
-        o3[1] = gy;
-        o3[2] = gz;
+        const double xp = v(P1, c + 1), xm = v(P1, c - 1);
+        const double yp = v(P2, c), ym = v(P0, c);
+        const double zp = v(P1, c + BX), zm = v(P1, c - BX);
+        g3[3 * sl + 0] = nx > 1 ? grad(x_hi ? ctr : xp, x_lo ? ctr : xm, hx, rhx) : 0.0;
+        g3[3 * sl + 1] = ny > 1 ? grad(y_hi ? ctr : yp, y_lo ? ctr : ym, hy, rhy) : 0.0;
+        g3[3 * sl + 2] = nz > 1 ? grad(z_hi ? ctr : zp, z_lo ? ctr : zm, hz, rhz) : 0.0;
+      }
+      double* o3 = stg + lane * SX + wz * 3 * NS;
+      if constexpr ((NS & 1) == 0) {
+        // 16-byte stores: with NS even, a thread's 3 x NS values start on a
+        // 16-byte boundary (SX and 3 NS even, the block 128-byte aligned)
+#pragma unroll
+        for (int q = 0; q < 3 * NS; q += 2) reinterpret_cast<double2*>(o3)[q / 2] = make_double2(g3[q], g3[q + 1]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 3 * NS; ++q) o3[q] = g3[q];
       }
     }
     __syncthreads();  // the block is complete and every read of plane j-1 is done
@@ -200,14 +207,15 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
     // x row il of the block: 8 voxels x 3 x ns doubles, contiguous in the
     // output when the group holds every substrate and the z tile is whole:
     // then warp wz writes rows wz, wz + 8, ... as straight runs (16-byte
-    // stores when the run starts 16-byte aligned, i.e. S even)
+    // stores when the run starts 16-byte aligned: S even and out 16-byte
+    // aligned)
     const int nk = min(kGTZ, nz - k0);
     if (ns == S && nk == kGTZ) {
       for (int il = wz; il < kGTX; il += 8) {
         if (i0 + il >= nx) break;
         double* dst = out + ((static_cast<size_t>(i0 + il) * ny + j) * nz + k0) * (3 * static_cast<size_t>(S));
         const double* src = stg + il * SX;
-        if ((S & 1) == 0) {
+        if ((S & 1) == 0 && (reinterpret_cast<uintptr_t>(out) & 15u) == 0) {
           for (int u = lane; u < RUN / 2; u += 32)
             reinterpret_cast<double2*>(dst)[u] = reinterpret_cast<const double2*>(src)[u];
         } else {
@@ -243,10 +251,29 @@ cudaError_t launch_plane_kernel(bfvm_ctx* c, int s0, double* d_out) {
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int xt = (c->nx + kGTX - 1) / kGTX, zt = (c->nz + kGTZ - 1) / kGTZ;
-  // enough y ranges for about 6 CTAs per SM, each range at least 8 planes
-  const long long want = 6LL * sms;
-  int chunks = static_cast<int>((want + static_cast<long long>(xt) * zt - 1) / (static_cast<long long>(xt) * zt));
-  chunks = std::max(1, std::min(chunks, (c->ny + 7) / 8));
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gradient_plane_kernel<T, NS>, 256, smem);
+  if (e != cudaSuccess) return e;
+  const long long wave = static_cast<long long>(std::max(per_sm, 1)) * sms;
+  // y ranges of at least 8 planes: among the counts that fill at least one
+  // wave of CTAs (or the most ranges there are), the one whose last wave is
+  // fullest, the fewer ranges on a tie (each range re-reads a halo plane)
+  const long long cols = static_cast<long long>(xt) * zt;
+  const int most = std::max(1, (c->ny + 7) / 8);
+  int chunks = most;
+  double best = -1.0;
+  for (int q = 1; q <= most; ++q) {
+    const int jq = (c->ny + q - 1) / q;
+    const long long ctas = cols * ((c->ny + jq - 1) / jq);
+    if (ctas < wave && q < most) continue;
+    const double waves = static_cast<double>(ctas) / static_cast<double>(wave);
+    const double fill = waves / std::ceil(waves);
+    if (fill > best + 1e-9) {
+      best = fill;
+      chunks = q;
+    }
+    if (ctas >= 4 * wave) break;
+  }
   const int jc = (c->ny + chunks - 1) / chunks;
   const dim3 grid(xt, zt, (c->ny + jc - 1) / jc);
   gradient_plane_kernel<T, NS><<<grid, 256, smem, c->stream>>>(

@@ -87,6 +87,12 @@ def test_gpu_gradients_fp32_and_device_output():
     me64.compute_all_gradient_vectors_device(dev.data_ptr())
     me64.synchronize()
     assert np.array_equal(dev.cpu().numpy().reshape(g64.shape), g64)
+    # an output 8 bytes past a 16-byte boundary (S even: the kernel's 16-byte
+    # row stores give way to 8-byte ones)
+    dev8 = torch.zeros(g64.size + 1, dtype=torch.float64, device="cuda:0")
+    me64.compute_all_gradient_vectors_device(dev8.data_ptr() + 8)
+    me64.synchronize()
+    assert np.array_equal(dev8[1:].cpu().numpy().reshape(g64.shape), g64)
     for s in range(wl.S):
         scale = np.abs(g64[:, s, :]).max()
         assert np.abs(g32[:, s, :] - g64[:, s, :]).max() <= 1e-5 * scale

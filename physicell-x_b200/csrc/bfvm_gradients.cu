@@ -70,7 +70,7 @@ __device__ __noinline__ double grad_quotient_slow(double g, double h) {
 // of one (32 x, 8 z) column of the grid; planes come from `map` (the field,
 // box {kGBoxX, 1, 10, NS}: NS substrates from s0, those past S zero-filled).
 template <typename T, int NS>
-__global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_constant__ CUtensorMap map, int nx, int ny,
+__global__ void __launch_bounds__(256, 3) gradient_plane_kernel(const __grid_constant__ CUtensorMap map, int nx, int ny,
                                                              int nz, int S, int s0, int jc,
                                                              const double* __restrict__ off, double dx,
                                                              double* __restrict__ out, int* status) {
@@ -132,27 +132,42 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
   // matching lines of every end cap and interior loop)
   // With h in [2^-100, 2^99], a numerator g in [2^-860, 2^900] in magnitude
   // keeps both g and RN(g/h) inside those bounds: one test of g's exponent.
-  auto grad = [markstein_ok](double a, double b, double h, double rh) {
+  // grad() returns the corrected quotient and clears `fast` unless
+  // 2^-860 <= |g| < 2^900 or g = +0 (which the correction maps to +0); a
+  // voxel with any such component redoes them all with grad_exact().
+  auto grad = [](double a, double b, double h, double rh, bool& fast) {
     double g = a;
     g -= b;
     const unsigned hw = static_cast<unsigned>(__double2hiint(g)) & 0x7FFFFFFFu;  // |g|'s high word
     const double q0 = g * rh;
     const double e = __fma_rn(-q0, h, g);
-    const double q = __fma_rn(e, rh, q0);
-    // 2^-860 <= |g| < 2^900, or g = +0 (which the correction maps to +0)
-    if (markstein_ok && (hw - 0x0A300000u < 0x78300000u - 0x0A300000u || __double_as_longlong(g) == 0)) return q;
+    fast &= (hw - 0x0A300000u < 0x78300000u - 0x0A300000u) | (__double_as_longlong(g) == 0);
+    return __fma_rn(e, rh, q0);
+  };
+  auto grad_exact = [markstein_ok](double a, double b, double h, double rh) {
+    double g = a;
+    g -= b;
+    const unsigned hw = static_cast<unsigned>(__double2hiint(g)) & 0x7FFFFFFFu;
+    if (markstein_ok && (hw - 0x0A300000u < 0x78300000u - 0x0A300000u || __double_as_longlong(g) == 0)) {
+      const double q0 = g * rh;
+      return __fma_rn(__fma_rn(-q0, h, g), rh, q0);
+    }
     return grad_quotient_slow(g, h);
   };
   const int i = i0 + lane, k = k0 + wz;
   const int ix = lane + X0, iz = wz + 1;  // this thread's voxel in a slot
   // Per axis: a line's two ends take the one-sided difference over dx, the
-  // voxels between the central one over 2 dx.  The neighbours are read in
-  // every case (the halo and the ring hold them) and the end cases select
-  // the centre instead, so the components need no branches.
+  // voxels between the central one over 2 dx.  Each component is
+  // (value at +o) - (value at -o) with offsets that are 0 at the matching
+  // end (the centre stands in for the missing neighbour), so the component
+  // needs no branch or select; an axis of length 1 is zeroed at the end.
   const bool x_lo = i == 0, x_hi = i == nx - 1;
   const bool z_lo = k == 0, z_hi = k == nz - 1;
+  const int oxp = x_hi ? 0 : 1, oxm = x_lo ? 0 : 1;
+  const int ozp = z_hi ? 0 : BX, ozm = z_lo ? 0 : BX;
   const double hx = (x_lo || x_hi) ? dx : two_dx, rhx = (x_lo || x_hi) ? rdx : r2dx;
   const double hz = (z_lo || z_hi) ? dx : two_dx, rhz = (z_lo || z_hi) ? rdx : r2dx;
+  const bool zero_x = nx == 1, zero_y = ny == 1, zero_z = nz == 1;
   for (int j = jb; j < je; ++j) {
     if (j == jb) wait_plane(j);
     if (j + 1 < ny) wait_plane(j + 1);
@@ -163,28 +178,43 @@ __global__ void __launch_bounds__(256) gradient_plane_kernel(const __grid_consta
     if (i < nx && k < nz) {
       const bool y_lo = j == 0, y_hi = j == ny - 1;
       const double hy = (y_lo || y_hi) ? dx : two_dx, rhy = (y_lo || y_hi) ? rdx : r2dx;
+      const T* Pyp = y_hi ? P1 : P2;  // plane j+1, or j itself at the last plane
+      const T* Pym = y_lo ? P1 : P0;  // plane j-1, or j itself at the first plane
       double g3[3 * NS];
+      bool fast = markstein_ok;
+      // substrates past the group's last (sl >= ns) read the map's zero
+      // fill; their values are staged but never written out
+      // FP32 fields hold rho - off; an FP64 field is read as it is (adding 0.0
+      // would also turn a -0 into +0, which the reference keeps)
+      auto v = [&](const T* P, int e, double o) {
+        if constexpr (sizeof(T) == 4)
+          return static_cast<double>(P[e]) + o;
+        else
+          return static_cast<double>(P[e]);
+      };
 #pragma unroll
       for (int sl = 0; sl < NS; ++sl) {
-        // substrates past the group's last (sl >= ns) read the map's zero
-        // fill; their values are staged but never written out
-        const double o = (off && sl < ns) ? off[s0 + sl] : 0.0;
+        const double o = (sizeof(T) == 4 && sl < ns) ? off[s0 + sl] : 0.0;
         const int c = sl * PS + iz * BX + ix;
-        // FP32 fields hold rho - off; an FP64 field is read as it is (adding 0.0
-        // would also turn a -0 into +0, which the reference keeps)
-        auto v = [&](const T* P, int e) {
-          if constexpr (sizeof(T) == 4)
-            return static_cast<double>(P[e]) + o;
-          else
-            return static_cast<double>(P[e]);
-        };
-        const double ctr = v(P1, c);
-        const double xp = v(P1, c + 1), xm = v(P1, c - 1);
-        const double yp = v(P2, c), ym = v(P0, c);
-        const double zp = v(P1, c + BX), zm = v(P1, c - BX);
-        g3[3 * sl + 0] = nx > 1 ? grad(x_hi ? ctr : xp, x_lo ? ctr : xm, hx, rhx) : 0.0;
-        g3[3 * sl + 1] = ny > 1 ? grad(y_hi ? ctr : yp, y_lo ? ctr : ym, hy, rhy) : 0.0;
-        g3[3 * sl + 2] = nz > 1 ? grad(z_hi ? ctr : zp, z_lo ? ctr : zm, hz, rhz) : 0.0;
+        g3[3 * sl + 0] = grad(v(P1, c + oxp, o), v(P1, c - oxm, o), hx, rhx, fast);
+        g3[3 * sl + 1] = grad(v(Pyp, c, o), v(Pym, c, o), hy, rhy, fast);
+        g3[3 * sl + 2] = grad(v(P1, c + ozp, o), v(P1, c - ozm, o), hz, rhz, fast);
+      }
+      if (!fast) {  // rare: a component outside the correction's range
+#pragma unroll
+        for (int sl = 0; sl < NS; ++sl) {
+          const double o = (sizeof(T) == 4 && sl < ns) ? off[s0 + sl] : 0.0;
+          const int c = sl * PS + iz * BX + ix;
+          g3[3 * sl + 0] = grad_exact(v(P1, c + oxp, o), v(P1, c - oxm, o), hx, rhx);
+          g3[3 * sl + 1] = grad_exact(v(Pyp, c, o), v(Pym, c, o), hy, rhy);
+          g3[3 * sl + 2] = grad_exact(v(P1, c + ozp, o), v(P1, c - ozm, o), hz, rhz);
+        }
+      }
+#pragma unroll
+      for (int sl = 0; sl < NS; ++sl) {
+        if (zero_x) g3[3 * sl + 0] = 0.0;
+        if (zero_y) g3[3 * sl + 1] = 0.0;
+        if (zero_z) g3[3 * sl + 2] = 0.0;
       }
       double* o3 = stg + lane * SX + wz * 3 * NS;
       if constexpr ((NS & 1) == 0) {

@@ -1490,9 +1490,13 @@ template <typename T, int AXIS>
 static cudaError_t launch_yz_any(const CUtensorMap& map, const CUtensorMap& ring_map, const SweepParams<T>& p,
                                  const SweepConfig& cfg, cudaStream_t st) {
   const int n = (AXIS == 1) ? p.ny : p.nz;
-  if constexpr (sizeof(T) == 8) {
+  {
     bool launched = false;
-    const cudaError_t e = launch_tmem_yz<AXIS>(ring_map, p, cfg, st, &launched);
+    cudaError_t e;
+    if constexpr (sizeof(T) == 8)
+      e = launch_tmem_yz<AXIS>(ring_map, p, cfg, st, &launched);
+    else
+      e = launch_tmem_yz_f32<AXIS>(ring_map, p, cfg, st, &launched);
     if (e != cudaSuccess || launched) return e;
   }
   if (use_ring_yz(sizeof(T), n, cfg)) {

@@ -846,6 +846,342 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   }
 }
 
+// ---- FP32 y/z sweep with tensor memory ----
+//
+// The FP32 form's y and z sweeps on the plan of the FP64 one above: values
+// are stored in FP32 (rounded once, when stored) while the recurrence runs in
+// FP64, exactly as the shared-memory ring sweep of bfvm_sweeps.cu computes
+// them, so results are that sweep's bits.  An FP32 forward result takes one
+// TMEM column, so a ring keeps its 16 chunks in 256 columns and two rings
+// share each lane quarter (warps ns + r and ns + r + 4 take the quarter's two
+// column halves): up to eight TMEM rings beside up to five shared-memory
+// rings, 416 lines of 200 per SM where the shared-memory ring sweep holds 224.
+constexpr int kTmemRingSmemF32 = 5;  // most shared-memory rings (warps 0..ns-1)
+constexpr int kTmemRingTmemF32 = 8;  // most TMEM rings, two per lane quarter
+
+template <int AXIS, int MODE>
+__device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const SweepParams<float>& p,
+                                                 const YzShape& g, int KF, uint64_t* full, float* slots, double* cus,
+                                                 uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
+  constexpr int R = kRowBatch;
+  constexpr int CH = kRingRows;
+  constexpr int TI = 32;
+  constexpr int kSlotElems = CH * TI;
+  constexpr uint32_t kSlotBytes = kSlotElems * sizeof(float);
+  constexpr unsigned kAll = 0xffffffffu;
+  const int t = threadIdx.x & 31;
+  const int nx = g.nx, n = g.n, nm = g.nm, C = g.C, ntx = g.ntx;
+  constexpr bool TM = MODE != 0;
+  const int T = MODE == 0 ? 0 : (MODE == 1 ? C : kTmemMaxChunks);  // chunks kept in TMEM
+  const int NR = MODE == 1 ? 0 : C - T;                             // chunks resident in shared memory
+  const int RB = TM ? KF : 0;                                       // first resident slot
+  const long long ntiles = g.ntiles;
+  unsigned long long* counter = p.tile_counter;
+
+  auto decode = [&](long long tile, int& i0, int& m, int& s) {
+    s = static_cast<int>(tile / g.per_s);
+    const long long r = tile - s * g.per_s;
+    m = static_cast<int>(r / ntx);
+    i0 = static_cast<int>(r - static_cast<long long>(m) * ntx) * TI;
+  };
+  auto skip = [&](long long tile) {  // every line of the tile in an activated face: final already
+    int i0, m, s;
+    decode(tile, i0, m, s);
+    return p.active[s] != 0 && (m == 0 || m == nm - 1);
+  };
+  auto grab = [&]() -> long long {
+    long long v = 0;
+    if (t == 0) {
+      do {
+        v = static_cast<long long>(atomicAdd(counter, 1ull));
+      } while (v < ntiles && skip(v));
+      if (v > ntiles) v = ntiles;
+    }
+    return __shfl_sync(kAll, v, 0);
+  };
+  auto issue = [&](int i0, int m, int s, int c, int sl, uint32_t par) {
+    if (t == 0) {
+      const uint32_t bar = smem_u32(&full[sl]);
+      mbar_expect_tx(bar, kSlotBytes);
+      const uint32_t dst = smem_u32(slots + static_cast<size_t>(sl) * kSlotElems);
+      if (AXIS == 1)
+        tma_load_4d(dst, map, bar, i0, c * CH, m, s);
+      else
+        tma_load_4d(dst, map, bar, i0, m, c * CH, s);
+    }
+    pend |= 1u << sl;
+    ppar = (ppar & ~(1u << sl)) | (par << sl);
+  };
+  auto rslot = [&](bool fl, int c) { return RB + ring_slot(fl, NR, c - T); };
+
+  bool ok = true;
+  long long tile = grab();
+  int ti0 = 0, tm_ = 0, ts = 0;
+  if (tile < ntiles) {
+    decode(tile, ti0, tm_, ts);
+    for (int c = 0; c < (TM ? KF : 0); ++c) issue(ti0, tm_, ts, c, c, 0u);
+    for (int c = T; c < C; ++c) issue(ti0, tm_, ts, c, rslot(false, c), 0u);
+  }
+  const int screen = p.screen;
+  int staged_s = -1;
+  int fsl = 0;
+  uint32_t fpar = 0;
+  for (uint32_t k = 0; tile < ntiles; ++k) {
+    const int i0 = ti0, m = tm_, s = ts;
+    const bool flip = (k & 1u) != 0;
+    const bool act = p.active[s] != 0;
+    const int i = i0 + t;
+    const bool face = act && (i == 0 || i == nx - 1);  // lines in an x face keep their (pinned) input
+    const bool lane_on = !face && i < nx;
+    const AxisCoefs<float>& ac = (AXIS == 1) ? p.ay : p.az;
+    const double* __restrict__ drp = ac.dr + static_cast<size_t>(s) * ac.npad;  // RN(1/d)
+    const double c1 = p.c1[s];
+    const double shift = p.shift[s];
+    if (s != staged_s) {
+      stage_row(cus, ac.cu + static_cast<size_t>(s) * ac.npad, C * CH);
+      staged_s = s;
+      __syncwarp();
+    }
+    float* out = p.f + ((AXIS == 1) ? ((static_cast<size_t>(s) * p.nz + m) * p.ny) * p.nxp
+                                    : (static_cast<size_t>(s) * p.nz * p.ny + m) * p.nxp) + i;
+    double cf[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) cf[q] = __ldg(drp + q);
+    double y = -0.0;
+    const bool edge_tile = __any_sync(kAll, !lane_on);
+    long long nxt = ntiles;
+    int ni0 = 0, nm_ = 0, ns_ = 0;
+    auto take_next = [&]() {
+      nxt = grab();
+      if (nxt < ntiles) decode(nxt, ni0, nm_, ns_);
+    };
+
+    // ---- forward elimination (FP64 recurrence, results rounded to FP32) ----
+    auto fwd_chunk = [&](bool edge, int c) {
+      const int rb = c * CH;
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
+      const int sl = flow ? fsl : rslot(flip, c);
+      const uint32_t par = flow ? fpar : (k & 1u);
+      if (ok) ok = mbar_wait(smem_u32(&full[sl]), par);
+      pend &= ~(1u << sl);
+      float* cb = slots + static_cast<size_t>(sl) * kSlotElems + t;
+      float yv[R];
+      if (!edge || lane_on) {
+        float v[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
+        if (rb + R > n) {  // rows past the line's end (TMA fill): any clean value, never stored
+#pragma unroll
+          for (int q = 0; q < R; ++q)
+            if (rb + q >= n) v[q] = 1.0f;
+        }
+        if (flow)
+          y = forward_store<R>(v, cf, c1, shift, screen, y, [&](int q, float val) { yv[q] = val; });
+        else
+          y = forward_store<R>(v, cf, c1, shift, screen, y, [&](int q, float val) { cb[q * TI] = val; });
+      } else if (flow) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) yv[q] = 0.0f;  // lanes with no line: anything, never read
+      }
+      if (flow) {
+        __syncwarp();
+        tmem_st16f(tbase + 16u * c, yv);
+        __syncwarp();  // every lane has read the slot
+        if (c == T - KF && NR == 0) take_next();
+        const int cn = c + KF;
+        if (cn < T)
+          issue(i0, m, s, cn, sl, fpar ^ 1u);
+        else if (NR == 0 && nxt < ntiles)
+          issue(ni0, nm_, ns_, cn - T, sl, fpar ^ 1u);
+        if (++fsl == KF) {
+          fsl = 0;
+          fpar ^= 1u;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) cf[q] = __ldg(drp + (c + 1) * R + q);
+    };
+    if (edge_tile) {
+      for (int c = 0; c < C; ++c) fwd_chunk(true, c);
+    } else {
+      for (int c = 0; c < C; ++c) fwd_chunk(false, c);
+    }
+    __syncwarp();
+    if constexpr (TM) tmem_wait_st();
+    if (!__all_sync(kAll, ok)) {
+      if (t == 0) atomicExch(p.status, kDevTimeout);
+      return;
+    }
+    if (NR > 0) {
+      take_next();
+      if (TM && nxt < ntiles) {
+        for (int c = 0; c < KF; ++c) {
+          issue(ni0, nm_, ns_, c, fsl, fpar);
+          if (++fsl == KF) {
+            fsl = 0;
+            fpar ^= 1u;
+          }
+        }
+        for (int c = 0; c < KF; ++c) {  // the consume cursor returns to where those loads start
+          if (fsl == 0) {
+            fsl = KF - 1;
+            fpar ^= 1u;
+          } else {
+            --fsl;
+          }
+        }
+      }
+    }
+
+    // ---- back substitution, last chunk first; results to the field ----
+    double xn = -0.0;
+    uint32_t tr[16];
+    if constexpr (TM) {
+      __syncwarp();
+      tmem_ld16_issue(tbase + 16u * (T - 1), tr);
+    }
+    auto back_chunk = [&](bool edge, int c) {
+      const int rb = c * CH;
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
+      float v[R];
+      if (flow) {
+        __syncwarp();
+        tmem_wait_ld16(tr);
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = __uint_as_float(tr[q]);
+        if (c > 0) tmem_ld16_issue(tbase + 16u * (c - 1), tr);
+      } else {
+        const float* cb = slots + static_cast<size_t>(rslot(flip, c)) * kSlotElems + t;
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
+      }
+      if (!edge || lane_on) {
+        const double2* cwp = reinterpret_cast<const double2*>(cus + rb);  // 16-byte pairs
+        double cw[R];
+#pragma unroll
+        for (int q = 0; q < R / 2; ++q) {
+          const double2 pr = cwp[q];
+          cw[2 * q] = pr.x;
+          cw[2 * q + 1] = pr.y;
+        }
+        float* o = out + static_cast<size_t>(rb) * g.row_stride;
+        if (c == C - 1 || (act && c == 0)) {
+          // the line's end: rows past n are fill; an activated substrate's
+          // first and last rows keep their pinned input
+          const int r_lo = (act && c == 0) ? 1 : 0;
+          const int r_hi = min(R, n - rb - ((act && c == C - 1) ? 1 : 0));
+#pragma unroll
+          for (int q = R - 1; q >= 0; --q) {
+            if (rb + q < n) {
+              xn = back_elem(cw[q], xn, static_cast<double>(v[q]));
+              if (q >= r_lo && q < r_hi) o[q * g.row_stride] = static_cast<float>(xn);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int q = R - 1; q >= 0; --q) {
+            xn = back_elem(cw[q], xn, static_cast<double>(v[q]));
+            o[q * g.row_stride] = static_cast<float>(xn);
+          }
+        }
+      }
+      if (!flow) {
+        __syncwarp();  // every lane has read the slot
+        if (nxt < ntiles) issue(ni0, nm_, ns_, T + (NR - 1 - (c - T)), rslot(flip, c), (k + 1) & 1u);
+      }
+    };
+    if (edge_tile) {
+      for (int c = C - 1; c >= 0; --c) back_chunk(true, c);
+    } else {
+      for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
+    }
+    tile = nxt;
+    ti0 = ni0;
+    tm_ = nm_;
+    ts = ns_;
+  }
+}
+
+template <int AXIS>
+__global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
+    sweep_yz_tmem_f32_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<float> p,
+                             uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns) {
+  constexpr int CH = kRingRows;
+  constexpr int TI = 32;
+  constexpr int kSlotElems = CH * TI;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 128);
+  YzShape g;
+  g.nx = p.nx;
+  g.n = (AXIS == 1) ? p.ny : p.nz;
+  g.nm = (AXIS == 1) ? p.nz : p.ny;
+  g.C = (g.n + CH - 1) / CH;
+  g.ntx = (g.nx + TI - 1) / TI;
+  g.per_s = static_cast<long long>(g.ntx) * g.nm;
+  g.ntiles = g.per_s * p.S;
+  g.row_stride = (AXIS == 1) ? static_cast<size_t>(p.nxp) : static_cast<size_t>(p.nxp) * p.ny;
+  const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
+  const int nt = static_cast<int>(blockDim.x >> 5) - ns;  // TMEM rings (warps ns..ns+nt-1)
+  const bool tm = warp >= ns;
+  unsigned char* rbase = tm ? base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                  static_cast<size_t>(warp - ns) * tmem_ring_bytes
+                            : base + static_cast<size_t>(warp) * smem_ring_bytes;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                                    static_cast<size_t>(nt) * tmem_ring_bytes);
+  const int nslots = tm ? kf + g.C - min(g.C, kTmemMaxChunks) : g.C;
+  uint64_t* full = reinterpret_cast<uint64_t*>(rbase);
+  float* slots = reinterpret_cast<float*>(rbase + (tm ? kTmemBarrierBytes : kBarrierBytes));
+  double* cus = reinterpret_cast<double*>(slots + static_cast<size_t>(nslots) * kSlotElems);
+
+  if (t == 0) {
+    if (warp == 0) prefetch_tmap(&map);
+    for (int c = 0; c < nslots; ++c) mbar_init(smem_u32(&full[c]), 1);
+    fence_barrier_init();
+  }
+  __syncwarp();
+  if (warp == 0) {
+    tmem_alloc(smem_u32(tmem_slot), 512);
+    tmem_relinquish();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  uint32_t pend = 0, ppar = 0;
+  if (tm) {
+    tmem_fence_after();
+    // lane quarter warp % 4; the second ring on a quarter takes columns 256..511
+    const uint32_t half = static_cast<uint32_t>((warp - ns) >= 4 ? 256 : 0);
+    const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + half;
+    if (g.C <= kTmemMaxChunks)
+      yz_tmem_ring_f32<AXIS, 1>(&map, p, g, kf, full, slots, cus, tbase, pend, ppar);
+    else
+      yz_tmem_ring_f32<AXIS, 2>(&map, p, g, kf, full, slots, cus, tbase, pend, ppar);
+  } else {
+    yz_tmem_ring_f32<AXIS, 0>(&map, p, g, kf, full, slots, cus, 0u, pend, ppar);
+  }
+  if (pend != 0) {
+    for (int sl = 0; sl < nslots; ++sl)
+      if ((pend >> sl) & 1u) mbar_wait(smem_u32(&full[sl]), (ppar >> sl) & 1u);
+  }
+  __syncwarp();
+  if (tm) {
+    tmem_wait_st();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tmem_fence_after();
+    tmem_dealloc(*tmem_slot, 512);
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned long long* counter = p.tile_counter;
+    if (atomicAdd(counter + 1, 1ull) == gridDim.x - 1) {
+      counter[0] = 0;
+      counter[1] = 0;
+    }
+  }
+}
+
 // ---- launch policy ----
 
 // The TMEM sweeps hand tiles out at run time, so fewer per ring still balance.
@@ -991,20 +1327,89 @@ template cudaError_t launch_tmem_yz<1>(const CUtensorMap&, const SweepParams<dou
 template cudaError_t launch_tmem_yz<2>(const CUtensorMap&, const SweepParams<double>&, const SweepConfig&,
                                        cudaStream_t, bool*);
 
+// One FP32 TMEM ring: barriers, kf input slots plus a slot per chunk past the
+// 16 that its 256 TMEM columns hold, the staged upper-diagonal row (FP64).
+static size_t tmem_yz_f32_ring_bytes(int n_line, int kf) {
+  const int C = (n_line + kRingRows - 1) / kRingRows;
+  const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
+  return kTmemBarrierBytes + static_cast<size_t>(kf + resident) * kRingRows * 32 * 4 +
+         static_cast<size_t>(C) * kRingRows * 8;
+}
+
+static size_t tmem_yz_f32_smem(int n_line, int ns, int nt, int kf) {
+  return 128 + ns * ring_yz_bytes(4, n_line) + nt * tmem_yz_f32_ring_bytes(n_line, kf) + 128;
+}
+
+// The FP32 TMEM y/z sweep applies (FP32, lines of at least kTmemFlowSlots
+// chunks, at most 32 slots per ring); the most rings that fit, TMEM rings
+// first, then the most input slots.
+static bool use_tmem_yz_f32(int eb, int n_line, const SweepConfig& cfg, int* ns, int* nt, int* kf) {
+  const int C = (n_line + kRingRows - 1) / kRingRows;
+  if (eb != 4 || cfg.persistent < 1 || cfg.tmem == 0 || cfg.yz_tile != 32 || C < kTmemFlowSlots) return false;
+  const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
+  int best = 0;
+  for (int t = kTmemRingTmemF32; t >= 1; --t) {
+    for (int f = kTmemFlowSlots; f >= 2; --f) {
+      if (f + resident > 32) continue;
+      for (int k = kTmemRingSmemF32; k >= 0; --k) {
+        if (k > 0 && C > 32) continue;  // a shared-memory ring's barriers: one bit per slot
+        if (tmem_yz_f32_smem(n_line, k, t, f) <= 227 * 1024) {
+          if (k + t > best) {
+            best = k + t;
+            *ns = k;
+            *nt = t;
+            *kf = f;
+          }
+          break;
+        }
+      }
+    }
+  }
+  return best > 0;
+}
+
+template <int AXIS>
+cudaError_t launch_tmem_yz_f32(const CUtensorMap& ring_map, const SweepParams<float>& p, const SweepConfig& cfg,
+                               cudaStream_t st, bool* launched) {
+  *launched = false;
+  const int n = (AXIS == 1) ? p.ny : p.nz;
+  int ns = 0, nt = 0, kf = 0;
+  if (!use_tmem_yz_f32(4, n, cfg, &ns, &nt, &kf)) return cudaSuccess;
+  const int rings = ns + nt;
+  const size_t smem = tmem_yz_f32_smem(n, ns, nt, kf);
+  const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * p.S;
+  int grid = 0;
+  cudaError_t e =
+      persistent_grid(sweep_yz_tmem_f32_kernel<AXIS>, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
+  if (e != cudaSuccess) return e;
+  if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
+  sweep_yz_tmem_f32_kernel<AXIS><<<grid, 32 * rings, smem, st>>>(
+      ring_map, p, static_cast<uint32_t>(ring_yz_bytes(4, n)), static_cast<uint32_t>(tmem_yz_f32_ring_bytes(n, kf)),
+      kf, ns);
+  *launched = true;
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_tmem_yz_f32<1>(const CUtensorMap&, const SweepParams<float>&, const SweepConfig&,
+                                           cudaStream_t, bool*);
+template cudaError_t launch_tmem_yz_f32<2>(const CUtensorMap&, const SweepParams<float>&, const SweepConfig&,
+                                           cudaStream_t, bool*);
+
 cudaError_t tmem_sweeps_set_wait_limit(unsigned long long ns) { return set_module_wait_limit(ns); }
 
 }  // namespace bfvm
 
 extern "C" int bfvm_tmem_sweep_plan(int axis, int n_line, int tmem_level, int* smem_rings, int* tmem_rings,
                                     int* input_slots) {
-  if ((axis != 0 && axis != 1) || n_line < 1 || n_line > 65535 || tmem_level < 0 || tmem_level > 2 || !smem_rings ||
+  if (axis < 0 || axis > 2 || n_line < 1 || n_line > 65535 || tmem_level < 0 || tmem_level > 2 || !smem_rings ||
       !tmem_rings || !input_slots)
     return BFVM_ERR_ARG;
   bfvm::SweepConfig cfg;
   cfg.tmem = tmem_level;
   int ns = 0, nt = 0, kf = 0;
-  const bool on = axis == 0 ? bfvm::use_tmem_x(8, n_line, false, cfg, &ns, &nt, &kf)
-                            : bfvm::use_tmem_yz(8, n_line, cfg, &ns, &nt, &kf);
+  const bool on = axis == 0   ? bfvm::use_tmem_x(8, n_line, false, cfg, &ns, &nt, &kf)
+                  : axis == 1 ? bfvm::use_tmem_yz(8, n_line, cfg, &ns, &nt, &kf)
+                              : bfvm::use_tmem_yz_f32(4, n_line, cfg, &ns, &nt, &kf);
   *smem_rings = on ? ns : 0;
   *tmem_rings = on ? nt : 0;
   *input_slots = on ? kf : 0;

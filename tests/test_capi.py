@@ -84,7 +84,9 @@ def test_tmem_sweep_plan():
     at level 2 from 17), two input slots where a third would cost a ring, and where the
     shared-memory schedules take over (y/z lines under 3 chunks of 16 rows,
     x lines under 2 at level 2, any line past 736 = 46 chunks, whose 30
-    resident chunks and 2 input slots fill a ring's 32 slots)."""
+    resident chunks and 2 input slots fill a ring's 32 slots); and the FP32
+    y/z sweep's (axis 2: up to 5 shared-memory and 8 TMEM rings, two per
+    lane quarter)."""
     yz = {33: (3, 4, 3), 40: (3, 4, 3), 200: (3, 4, 3), 210: (3, 4, 2), 256: (2, 4, 3), 300: (1, 4, 3),
           400: (0, 4, 3), 500: (0, 2, 3), 640: (0, 2, 3), 650: (0, 2, 2), 657: (0, 1, 3), 700: (0, 1, 3),
           720: (0, 1, 3), 736: (0, 1, 2), 32: (0, 0, 0), 737: (0, 0, 0), 800: (0, 0, 0)}
@@ -100,7 +102,12 @@ def test_tmem_sweep_plan():
         assert _plan(0, n, 2) == want, n
     L = _lib.lib()
     a = C.c_int()
-    for args in ((2, 100, 1), (1, 0, 1), (1, 100, 3), (0, 100, -1)):
+    f32 = {32: (0, 0, 0), 33: (5, 8, 3), 200: (5, 8, 3), 256: (5, 8, 2), 257: (4, 8, 2), 300: (3, 8, 2),
+           400: (0, 8, 3), 512: (0, 5, 3), 640: (0, 3, 3), 736: (0, 3, 2), 737: (0, 0, 0)}
+    for n, want in f32.items():
+        assert _plan(2, n) == want, n
+        assert _plan(2, n, 0) == (0, 0, 0), n
+    for args in ((3, 100, 1), (-1, 100, 1), (1, 0, 1), (1, 100, 3), (0, 100, -1)):
         assert L.bfvm_tmem_sweep_plan(*args, C.byref(a), C.byref(a), C.byref(a)) == _lib.BFVM_ERR_ARG
     assert L.bfvm_tmem_sweep_plan(1, 100, 1, None, C.byref(a), C.byref(a)) == _lib.BFVM_ERR_ARG
 

@@ -251,11 +251,13 @@ cudaError_t launch_tmem_yz(const CUtensorMap& ring_map, const SweepParams<double
                            cudaStream_t st, bool* launched);
 cudaError_t launch_tmem_x(const CUtensorMap& map, const SweepParams<double>& p, const SweepConfig& cfg,
                           cudaStream_t st, bool* launched);
-// The FP32 y/z sweeps with tensor-memory rings (bfvm_tmem_sweeps.cu), same
+// The FP32 sweeps with tensor-memory rings (bfvm_tmem_sweeps.cu), same
 // contract.
 template <int AXIS>
 cudaError_t launch_tmem_yz_f32(const CUtensorMap& ring_map, const SweepParams<float>& p, const SweepConfig& cfg,
                                cudaStream_t st, bool* launched);
+cudaError_t launch_tmem_x_f32(const CUtensorMap& map, const SweepParams<float>& p, const SweepConfig& cfg,
+                              cudaStream_t st, bool* launched);
 
 // ---- batched engine: one fused launch per LOD step over many solves ------
 // Tiles are 32 lines (one warp) in every sweep of a batch.

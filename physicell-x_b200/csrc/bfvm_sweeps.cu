@@ -1446,9 +1446,13 @@ static bool use_ring_yz(int eb, int n, const SweepConfig& cfg) {
 
 template <typename T>
 cudaError_t launch_sweep_x(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
-  if constexpr (sizeof(T) == 8) {
+  {
     bool launched = false;
-    const cudaError_t e = launch_tmem_x(maps.x, p, cfg, st, &launched);
+    cudaError_t e;
+    if constexpr (sizeof(T) == 8)
+      e = launch_tmem_x(maps.x, p, cfg, st, &launched);
+    else
+      e = launch_tmem_x_f32(maps.x, p, cfg, st, &launched);
     if (e != cudaSuccess || launched) return e;
   }
   if (use_ring_x(sizeof(T), p.nx, cfg)) {

@@ -1182,6 +1182,408 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
   }
 }
 
+// ---- FP32 x sweep with tensor memory ----
+//
+// The FP64 x sweep's plan above for the FP32 form: values stored in FP32,
+// the recurrence in FP64, the pins and face values as the per-tile FP32 x
+// sweep of bfvm_sweeps.cu applies them, so results are its bits.  A chunk is
+// the 128-byte column [32c, 32c + 32) of the tile's 32 lines; its forward
+// results take 32 TMEM columns, so a ring keeps 8 chunks (lines of up to 256)
+// in 256 columns and two rings share each lane quarter.
+constexpr int kXTmemRingSmemF32 = 3;   // most shared-memory rings (warps 0..ns-1)
+constexpr int kXTmemRingTmemF32 = 8;   // most TMEM rings, two per lane quarter
+constexpr int kXTmemMaxChunksF32 = 8;  // chunks of a TMEM ring in its 256 columns
+
+template <int MODE>
+__device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const SweepParams<float>& p,
+                                                const XShape& g, int KF, unsigned char* slots, uint64_t* full,
+                                                double* cus, unsigned char* stage, uint32_t tbase, uint32_t& pend,
+                                                uint32_t& ppar) {
+  constexpr int W = 32;  // floats per 128-byte chunk row
+  constexpr uint32_t kChunkBytes = 32u * 128u;
+  constexpr unsigned kAll = 0xffffffffu;
+  const int t = threadIdx.x & 31;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, C = g.C, ntj = g.ntj;
+  const int S = p.S;
+  const long long ntiles = g.ntiles;
+  unsigned long long* counter = p.tile_counter;
+  const int sw = t & 7;
+  constexpr bool TM = MODE != 0;
+  const int T = MODE == 0 ? 0 : (MODE == 1 ? C : kXTmemMaxChunksF32);  // chunks kept in TMEM
+  const int NR = MODE == 1 ? 0 : C - T;                                 // chunks resident in shared memory
+  const int RB = TM ? KF : 0;                                           // first resident slot
+  auto rslot = [&](bool fl, int c) { return RB + ring_slot(fl, NR, c - T); };
+
+  auto decode = [&](long long tile, int& j0, int& k, int& s) {
+    const long long r = tile / ntj;
+    j0 = static_cast<int>(tile - r * ntj) * 32;
+    s = static_cast<int>(r / nz);
+    k = static_cast<int>(r - static_cast<long long>(s) * nz);
+  };
+  auto grab = [&]() -> long long {
+    long long v = 0;
+    if (t == 0) {
+      v = static_cast<long long>(atomicAdd(counter, 1ull));
+      if (v > ntiles) v = ntiles;
+    }
+    return __shfl_sync(kAll, v, 0);
+  };
+  auto issue = [&](int j0, int k, int s, int c, int sl, uint32_t par) {
+    if (t == 0) {
+      const uint32_t bar = smem_u32(&full[sl]);
+      mbar_expect_tx(bar, kChunkBytes);
+      tma_load_4d(smem_u32(slots + static_cast<size_t>(sl) * kChunkBytes), map, bar, c * W, j0, k, s);
+    }
+    pend |= 1u << sl;
+    ppar = (ppar & ~(1u << sl)) | (par << sl);
+  };
+
+  bool ok = true;
+  long long tile = grab();
+  int tj0 = 0, tk = 0, ts = 0;
+  if (tile < ntiles) {
+    decode(tile, tj0, tk, ts);
+    for (int c = 0; c < (TM ? KF : 0); ++c) issue(tj0, tk, ts, c, c, 0u);
+    for (int c = T; c < C; ++c) issue(tj0, tk, ts, c, rslot(false, c), 0u);
+  }
+  const int screen = p.screen;
+  int staged_s = -1;
+  int fsl = 0;
+  uint32_t fpar = 0;
+  for (uint32_t it = 0; tile < ntiles; ++it) {
+    const int j0 = tj0, k = tk, s = ts;
+    const bool flip = (it & 1u) != 0;
+    const int j = j0 + t;
+    const bool valid = j < ny;
+    const bool act = p.active[s] != 0;
+    const bool face = act && (j == 0 || j == ny - 1 || k == 0 || k == nz - 1);
+    const bool lane_on = valid && !face;
+    const double* __restrict__ drp = p.ax.dr + static_cast<size_t>(s) * p.ax.npad;  // RN(1/d)
+    const double c1 = p.c1[s];
+    const double shift = p.shift[s];
+    const double off = p.off[s];
+    if (s != staged_s) {
+      stage_row(cus, p.ax.cu + static_cast<size_t>(s) * p.ax.npad, C * W);
+      staged_s = s;
+      __syncwarp();
+    }
+    float x0v = 0.0f, x1v = 0.0f;
+    if (act && valid) {
+      x0v = static_cast<float>(p.xface[(static_cast<size_t>(0 * S + s) * nz + k) * ny + j] - off);
+      x1v = static_cast<float>(p.xface[(static_cast<size_t>(1 * S + s) * nz + k) * ny + j] - off);
+    }
+    const double* fv = nullptr;  // face lines: the face plane's row
+    if (face && valid) {
+      if (k == 0 || k == nz - 1)
+        fv = p.zface + ((static_cast<size_t>(k == 0 ? 0 : 1) * S + s) * ny + j) * nx;
+      else
+        fv = p.yface + ((static_cast<size_t>(j == 0 ? 0 : 1) * S + s) * nz + k) * nx;
+    }
+    double cf[16];  // the coefficients RN(1/d) of the next 16 values
+#pragma unroll
+    for (int q = 0; q < 16; ++q) cf[q] = __ldg(drp + q);
+    double y = -0.0;
+    const bool edge_tile = __any_sync(kAll, !lane_on);
+    long long nxt = ntiles;
+    int nj0 = 0, nk = 0, ns_ = 0;
+    auto take_next = [&]() {
+      nxt = grab();
+      if (nxt < ntiles) decode(nxt, nj0, nk, ns_);
+    };
+
+    // ---- forward elimination (FP64 recurrence, results rounded to FP32) ----
+    // A chunk row is handled as two halves of 16 values (units 4h .. 4h+3 of
+    // the swizzled row, TMEM columns 32c + 16h ..), which keeps the
+    // registers of one half live at a time.
+    auto fwd_chunk = [&](bool edge, int c) {
+      const int i0 = c * W;
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
+      const int sl = flow ? fsl : rslot(flip, c);
+      const uint32_t par = flow ? fpar : (it & 1u);
+      if (ok) ok = mbar_wait(smem_u32(&full[sl]), par);
+      pend &= ~(1u << sl);
+      unsigned char* crow = slots + static_cast<size_t>(sl) * kChunkBytes + t * 128;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int e0 = i0 + 16 * h;
+        float yh[16];
+        if (!edge || lane_on) {
+          float vh[16];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float4 f4 = *reinterpret_cast<const float4*>(crow + (((4 * h + u) ^ sw) << 4));
+            vh[4 * u] = f4.x;
+            vh[4 * u + 1] = f4.y;
+            vh[4 * u + 2] = f4.z;
+            vh[4 * u + 3] = f4.w;
+          }
+          if (act) {  // the pin before the sweep
+            if (e0 == 0) vh[0] = x0v;
+            if (e0 <= nx - 1 && nx - 1 < e0 + 16) {
+#pragma unroll
+              for (int q = 0; q < 16; ++q)
+                if (e0 + q == nx - 1) vh[q] = x1v;
+            }
+          }
+          if (flow) {
+            y = forward_store<16>(vh, cf, c1, shift, screen, y, [&](int q, float val) { yh[q] = val; });
+          } else {
+            RowPut<float> put{crow, sw};
+            y = forward_store<16>(vh, cf, c1, shift, screen, y, [&](int q, float val) { put(16 * h + q, val); });
+          }
+        } else if (flow) {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) yh[q] = 0.0f;  // lanes with no line: anything, never read
+        }
+        if (flow) {
+          __syncwarp();
+          tmem_st16f(tbase + 32u * c + 16u * h, yh);
+        }
+        // the next half's coefficients (rows are padded past the line)
+#pragma unroll
+        for (int q = 0; q < 16; ++q) cf[q] = __ldg(drp + e0 + 16 + q);
+      }
+      if (flow) {
+        __syncwarp();  // every lane has read the slot
+        if (MODE == 1 && c == T - KF) take_next();
+        const int cn = c + KF;
+        if (cn < T)
+          issue(j0, k, s, cn, sl, fpar ^ 1u);
+        else if (MODE == 1 && nxt < ntiles)
+          issue(nj0, nk, ns_, cn - T, sl, fpar ^ 1u);
+        if (++fsl == KF) {
+          fsl = 0;
+          fpar ^= 1u;
+        }
+      }
+    };
+    if (edge_tile) {
+      for (int c = 0; c < C; ++c) fwd_chunk(true, c);
+    } else {
+      for (int c = 0; c < C; ++c) fwd_chunk(false, c);
+    }
+    __syncwarp();
+    if constexpr (TM) tmem_wait_st();
+    if (!__all_sync(kAll, ok)) {
+      if (t == 0) atomicExch(p.status, kDevTimeout);
+      return;
+    }
+    if (MODE != 1) take_next();
+
+    // ---- back substitution, last chunk first, upper half first; results to the field ----
+    double xn = -0.0;
+    uint32_t tr[16];  // TMEM chunks: the next half's forward results, loading
+    if constexpr (TM) {
+      __syncwarp();
+      tmem_ld16_issue(tbase + 32u * (T - 1) + 16u, tr);
+    }
+    auto back_chunk = [&](bool edge, int c) {
+      const int i0 = c * W;
+      const bool flow = MODE == 1 || (MODE == 2 && c < T);
+      unsigned char* cbase = flow ? stage : slots + static_cast<size_t>(rslot(flip, c)) * kChunkBytes;
+      unsigned char* crow = cbase + t * 128;
+      if (flow) {
+        // the staging chunk's previous bulk store has read it
+        if (t == 0) tma_store_wait_read();
+        __syncwarp();
+      }
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        const int h = 1 - hh;
+        const int e0 = i0 + 16 * h;
+        float vh[16];
+        if (flow) {
+          __syncwarp();
+          tmem_wait_ld16(tr);
+#pragma unroll
+          for (int q = 0; q < 16; ++q) vh[q] = __uint_as_float(tr[q]);
+          if (h == 1)
+            tmem_ld16_issue(tbase + 32u * c, tr);
+          else if (c > 0)
+            tmem_ld16_issue(tbase + 32u * (c - 1) + 16u, tr);
+        } else {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float4 f4 = *reinterpret_cast<const float4*>(crow + (((4 * h + u) ^ sw) << 4));
+            vh[4 * u] = f4.x;
+            vh[4 * u + 1] = f4.y;
+            vh[4 * u + 2] = f4.z;
+            vh[4 * u + 3] = f4.w;
+          }
+        }
+        if (edge && face) {
+          if (fv != nullptr) {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) vh[q] = (e0 + q < nx) ? static_cast<float>(fv[e0 + q] - off) : 0.0f;
+          }
+        } else if (!edge || valid) {
+          const double2* cwp = reinterpret_cast<const double2*>(cus + e0);  // 16-byte pairs
+          if (e0 + 16 > nx) {
+#pragma unroll
+            for (int g2 = 7; g2 >= 0; --g2) {
+              const double2 pr = cwp[g2];
+              if (e0 + 2 * g2 + 1 < nx) {
+                xn = back_elem(pr.y, xn, static_cast<double>(vh[2 * g2 + 1]));
+                vh[2 * g2 + 1] = static_cast<float>(xn);
+              }
+              if (e0 + 2 * g2 < nx) {
+                xn = back_elem(pr.x, xn, static_cast<double>(vh[2 * g2]));
+                vh[2 * g2] = static_cast<float>(xn);
+              }
+            }
+          } else {
+#pragma unroll
+            for (int g2 = 7; g2 >= 0; --g2) {
+              const double2 pr = cwp[g2];
+              xn = back_elem(pr.y, xn, static_cast<double>(vh[2 * g2 + 1]));
+              vh[2 * g2 + 1] = static_cast<float>(xn);
+              xn = back_elem(pr.x, xn, static_cast<double>(vh[2 * g2]));
+              vh[2 * g2] = static_cast<float>(xn);
+            }
+          }
+          if (act) {  // the pin after the sweep
+            if (e0 == 0) vh[0] = x0v;
+            if (e0 <= nx - 1 && nx - 1 < e0 + 16) {
+#pragma unroll
+              for (int q = 0; q < 16; ++q)
+                if (e0 + q == nx - 1) vh[q] = x1v;
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          *reinterpret_cast<float4*>(crow + (((4 * h + u) ^ sw) << 4)) =
+              make_float4(vh[4 * u], vh[4 * u + 1], vh[4 * u + 2], vh[4 * u + 3]);
+      }
+      // the chunk goes out as it is staged (rows past ny, columns past nx clipped)
+      fence_async_smem();
+      __syncwarp();
+      if (t == 0) {
+        tma_store_4d(map, smem_u32(cbase), i0, j0, k, s);
+        tma_store_commit();
+      }
+      if (!flow) {
+        // the slot's refill waits for the store to have read it
+        if (t == 0) tma_store_wait_read();
+        __syncwarp();
+        if (nxt < ntiles) issue(nj0, nk, ns_, T + (NR - 1 - (c - T)), rslot(flip, c), (it + 1) & 1u);
+      }
+    };
+    if (edge_tile) {
+      for (int c = C - 1; c >= 0; --c) back_chunk(true, c);
+    } else {
+      for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
+    }
+    if (MODE == 2 && nxt < ntiles) {
+      // the next tile's first inputs take the input slots (the first of
+      // which staged results just now: its store must have read it)
+      if (t == 0) tma_store_wait_read();
+      fence_async_smem();
+      __syncwarp();
+      for (int c = 0; c < KF; ++c) {
+        issue(nj0, nk, ns_, c, fsl, fpar);
+        if (++fsl == KF) {
+          fsl = 0;
+          fpar ^= 1u;
+        }
+      }
+      for (int c = 0; c < KF; ++c) {  // the consume cursor returns to the first of them
+        if (fsl == 0) {
+          fsl = KF - 1;
+          fpar ^= 1u;
+        } else {
+          --fsl;
+        }
+      }
+    }
+    tile = nxt;
+    tj0 = nj0;
+    tk = nk;
+    ts = ns_;
+  }
+}
+
+__global__ void __launch_bounds__(32 * (kXTmemRingSmemF32 + kXTmemRingTmemF32), 1)
+    sweep_x_tmem_f32_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<float> p,
+                            uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns) {
+  constexpr uint32_t kChunkBytes = 32u * 128u;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
+  XShape g;
+  g.nx = p.nx;
+  g.ny = p.ny;
+  g.nz = p.nz;
+  g.C = (g.nx + 31) / 32;
+  g.ntj = (g.ny + 31) / 32;
+  g.ntiles = static_cast<long long>(g.ntj) * g.nz * p.S;
+  const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
+  const int nt = static_cast<int>(blockDim.x >> 5) - ns;  // TMEM rings (warps ns..ns+nt-1)
+  const bool tm = warp >= ns;
+  unsigned char* rbase = tm ? base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                  static_cast<size_t>(warp - ns) * tmem_ring_bytes
+                            : base + static_cast<size_t>(warp) * smem_ring_bytes;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(ns) * smem_ring_bytes +
+                                                    static_cast<size_t>(nt) * tmem_ring_bytes);
+  // ring: [slots (+ staging chunk)] [upper diagonal] [barriers]; a TMEM ring
+  // over more than 8 chunks stages in its first input slot
+  const bool own_stage = tm && g.C <= kXTmemMaxChunksF32;
+  const int nslots = tm ? kf + g.C - min(g.C, kXTmemMaxChunksF32) : g.C;
+  unsigned char* slots = rbase;
+  unsigned char* stage = tm ? (own_stage ? rbase + static_cast<size_t>(nslots) * kChunkBytes : rbase) : nullptr;
+  double* cus = reinterpret_cast<double*>(rbase + static_cast<size_t>(nslots + (own_stage ? 1 : 0)) * kChunkBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(cus) +
+                                               static_cast<size_t>(g.C) * 32 * sizeof(double));
+
+  if (t == 0) {
+    if (warp == 0) prefetch_tmap(&map);
+    for (int c = 0; c < nslots; ++c) mbar_init(smem_u32(&full[c]), 1);
+    fence_barrier_init();
+  }
+  __syncwarp();
+  if (warp == 0) {
+    tmem_alloc(smem_u32(tmem_slot), 512);
+    tmem_relinquish();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  uint32_t pend = 0, ppar = 0;
+  if (tm) {
+    tmem_fence_after();
+    // lane quarter warp % 4; the second ring on a quarter takes columns 256..511
+    const uint32_t half = static_cast<uint32_t>((warp - ns) >= 4 ? 256 : 0);
+    const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + half;
+    if (own_stage)
+      x_tmem_ring_f32<1>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+    else
+      x_tmem_ring_f32<2>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+  } else {
+    x_tmem_ring_f32<0>(&map, p, g, kf, slots, full, cus, nullptr, 0u, pend, ppar);
+  }
+  if (pend != 0) {
+    for (int sl = 0; sl < nslots; ++sl)
+      if ((pend >> sl) & 1u) mbar_wait(smem_u32(&full[sl]), (ppar >> sl) & 1u);
+  }
+  if (t == 0) tma_store_wait_read();  // this warp's bulk stores have read shared memory
+  __syncwarp();
+  if (tm) {
+    tmem_wait_st();
+    tmem_fence_before();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tmem_fence_after();
+    tmem_dealloc(*tmem_slot, 512);
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned long long* counter = p.tile_counter;
+    if (atomicAdd(counter + 1, 1ull) == gridDim.x - 1) {
+      counter[0] = 0;
+      counter[1] = 0;
+    }
+  }
+}
+
 // ---- launch policy ----
 
 // The TMEM sweeps hand tiles out at run time, so fewer per ring still balance.
@@ -1395,13 +1797,82 @@ template cudaError_t launch_tmem_yz_f32<1>(const CUtensorMap&, const SweepParams
 template cudaError_t launch_tmem_yz_f32<2>(const CUtensorMap&, const SweepParams<float>&, const SweepConfig&,
                                            cudaStream_t, bool*);
 
+// One ring of the FP32 TMEM x sweep (a multiple of 1024 bytes, so every chunk
+// stays on the 128B-swizzle atom): shared-memory ring = C chunks; TMEM ring
+// = kf input chunks and a staging chunk, or, past 8 chunks, kf input chunks
+// and a resident chunk for each chunk past 8; then the upper diagonal (FP64)
+// and the barriers.
+static size_t x_tmem_f32_ring_bytes(int nx, bool tm, int kf) {
+  const int C = (nx + 31) / 32;
+  const int chunks = !tm ? C : (C <= kXTmemMaxChunksF32 ? kf + 1 : kf + C - kXTmemMaxChunksF32);
+  const size_t b = static_cast<size_t>(chunks) * 32 * 128 + static_cast<size_t>(C) * 32 * 8 + kXTmemBarrierBytes;
+  return (b + 1023) / 1024 * 1024;
+}
+
+static size_t x_tmem_f32_smem(int nx, int ns, int nt, int kf) {
+  return 1024 + ns * x_tmem_f32_ring_bytes(nx, false, kf) + nt * x_tmem_f32_ring_bytes(nx, true, kf) + 128;
+}
+
+// The FP32 TMEM x sweep applies (FP32, agents not fused, 32-line tiles, at
+// most 32 slots per ring): by default on lines of more than 8 chunks (257
+// voxels), at sweep TMEM level 2 from 2 chunks (33); *ns shared-memory rings
+// and *nt TMEM rings (the most that fit), *kf input slots per TMEM ring.
+// Measured on B200 against the per-tile FP32 x sweep, n^3 cubes with 2
+// substrates: equal at n = 200 and 320 (cube200's 4 substrates: 0.127
+// against 0.120 ms), 0.405 against 0.552 ms at 400, 0.815 / 1.001 at 512,
+// 2.22 / 2.74 at 640 -- where the per-tile sweep fits few tiles per SM.
+static bool use_tmem_x_f32(int eb, int nx, bool fused_agents, const SweepConfig& cfg, int* ns, int* nt, int* kf) {
+  const int C = (nx + 31) / 32;
+  if (eb != 4 || fused_agents || cfg.persistent < 1 || cfg.tmem == 0 || cfg.x_lines != 32 || C < 2) return false;
+  if (cfg.tmem < 2 && C <= kXTmemMaxChunksF32) return false;
+  const int resident = C > kXTmemMaxChunksF32 ? C - kXTmemMaxChunksF32 : 0;
+  int best = 0;
+  for (int t = kXTmemRingTmemF32; t >= 1; --t) {
+    for (int f = min(C, kTmemFlowSlots); f >= 2; --f) {
+      if (f + resident > 32) continue;
+      for (int k = kXTmemRingSmemF32; k >= 0; --k) {
+        if (k > 0 && C > 32) continue;  // a shared-memory ring's barriers: one bit per slot
+        if (x_tmem_f32_smem(nx, k, t, f) <= 227 * 1024) {
+          if (k + t > best) {
+            best = k + t;
+            *ns = k;
+            *nt = t;
+            *kf = f;
+          }
+          break;
+        }
+      }
+    }
+  }
+  return best > 0;
+}
+
+cudaError_t launch_tmem_x_f32(const CUtensorMap& map, const SweepParams<float>& p, const SweepConfig& cfg,
+                              cudaStream_t st, bool* launched) {
+  *launched = false;
+  int ns = 0, nt = 0, kf = 0;
+  if (!use_tmem_x_f32(4, p.nx, p.line_off != nullptr, cfg, &ns, &nt, &kf)) return cudaSuccess;
+  const int rings = ns + nt;
+  const size_t smem = x_tmem_f32_smem(p.nx, ns, nt, kf);
+  const long long tiles = static_cast<long long>((p.ny + 31) / 32) * p.nz * p.S;
+  int grid = 0;
+  cudaError_t e = persistent_grid(sweep_x_tmem_f32_kernel, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
+  if (e != cudaSuccess) return e;
+  if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
+  sweep_x_tmem_f32_kernel<<<grid, 32 * rings, smem, st>>>(
+      map, p, static_cast<uint32_t>(x_tmem_f32_ring_bytes(p.nx, false, kf)),
+      static_cast<uint32_t>(x_tmem_f32_ring_bytes(p.nx, true, kf)), kf, ns);
+  *launched = true;
+  return cudaGetLastError();
+}
+
 cudaError_t tmem_sweeps_set_wait_limit(unsigned long long ns) { return set_module_wait_limit(ns); }
 
 }  // namespace bfvm
 
 extern "C" int bfvm_tmem_sweep_plan(int axis, int n_line, int tmem_level, int* smem_rings, int* tmem_rings,
                                     int* input_slots) {
-  if (axis < 0 || axis > 2 || n_line < 1 || n_line > 65535 || tmem_level < 0 || tmem_level > 2 || !smem_rings ||
+  if (axis < 0 || axis > 3 || n_line < 1 || n_line > 65535 || tmem_level < 0 || tmem_level > 2 || !smem_rings ||
       !tmem_rings || !input_slots)
     return BFVM_ERR_ARG;
   bfvm::SweepConfig cfg;
@@ -1409,7 +1880,8 @@ extern "C" int bfvm_tmem_sweep_plan(int axis, int n_line, int tmem_level, int* s
   int ns = 0, nt = 0, kf = 0;
   const bool on = axis == 0   ? bfvm::use_tmem_x(8, n_line, false, cfg, &ns, &nt, &kf)
                   : axis == 1 ? bfvm::use_tmem_yz(8, n_line, cfg, &ns, &nt, &kf)
-                              : bfvm::use_tmem_yz_f32(4, n_line, cfg, &ns, &nt, &kf);
+                  : axis == 2 ? bfvm::use_tmem_yz_f32(4, n_line, cfg, &ns, &nt, &kf)
+                              : bfvm::use_tmem_x_f32(4, n_line, false, cfg, &ns, &nt, &kf);
   *smem_rings = on ? ns : 0;
   *tmem_rings = on ? nt : 0;
   *input_slots = on ? kf : 0;

@@ -366,18 +366,20 @@ def test_tmem_sweeps_bitwise(shape):
 @pytest.mark.gpu
 @pytest.mark.parametrize("shape", [(64, 48, 40, 2), (33, 100, 57, 3), (70, 256, 130, 2), (40, 257, 50, 1),
                                    (20, 64, 48, 1), (36, 400, 70, 2), (34, 40, 640, 1), (36, 33, 700, 1),
-                                   (36, 210, 736, 1), (34, 650, 36, 1), (200, 200, 40, 4)])
+                                   (36, 210, 736, 1), (34, 650, 36, 1), (200, 200, 40, 4), (257, 33, 34, 1),
+                                   (640, 33, 35, 1), (300, 70, 36, 2), (1000, 33, 34, 1)])
 @pytest.mark.parametrize("chain", [0, 1])
 def test_tmem_sweeps_fp32_bitwise(shape, chain):
-    """The FP32 y/z sweeps with tensor-memory rings (two rings per TMEM lane
-    quarter, lines of up to 16 chunks in TMEM and the rest resident): bit for
-    bit the FP32 shared-memory sweeps (TMEM off), under both persistent
-    schedules and both forms of the recurrence, and within the FP32 form's
-    tolerance of the oracle."""
+    """The FP32 sweeps with tensor-memory rings (two rings per TMEM lane
+    quarter; y/z lines of up to 16 chunks of 16 rows in TMEM, x lines of up
+    to 8 chunks of 32 values, the rest resident in shared memory): bit for bit
+    the FP32 shared-memory sweeps (TMEM off), under both persistent schedules
+    and both forms of the recurrence, and within the FP32 form's tolerance of
+    the oracle."""
     nx, ny, nz, S = shape
     wl = W.small_random(1990 + nx + ny, nx=nx, ny=ny, nz=nz, S=S, n_agents=3000, steps=3, stack=True)
     runs = {}
-    for sched, tmem in ((1, 0), (1, 1), (2, 1)):
+    for sched, tmem in ((1, 0), (1, 1), (2, 1), (1, 2)):
         me = Microenvironment.from_workload(wl, precision="fp32")
         me.set_fp64_chain(chain)
         me.set_sweep_schedule(sched)

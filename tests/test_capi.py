@@ -80,16 +80,18 @@ def test_tmem_sweep_plan():
     """The tensor-memory sweep configurations (shared-memory rings, TMEM
     rings, input slots per TMEM ring) chosen per line length: those measured
     on B200 (y/z: 3 + 4 rings at lines of 200, fewer shared-memory rings as
-    lines grow, TMEM rings partly resident past 256; x by default from 33,
-    at level 2 from 17), two input slots where a third would cost a ring, and where the
+    lines grow, TMEM rings partly resident past 256, the forward coefficient
+    pairs staged in shared memory where that costs no ring; x by default from
+    33, at level 2 from 17), two input slots where a third would cost a ring
+    (or the staged pairs), and where the
     shared-memory schedules take over (y/z lines under 3 chunks of 16 rows,
     x lines under 2 at level 2, any line past 736 = 46 chunks, whose 30
     resident chunks and 2 input slots fill a ring's 32 slots); and the FP32
     sweeps' (axis 2 y/z: up to 5 shared-memory and 8 TMEM rings, two per
     lane quarter; axis 3 x: up to 3 + 8 rings, 32-value chunks, 8 of them
     in a ring's TMEM columns, by default past 256 and at level 2 from 33)."""
-    yz = {33: (3, 4, 3), 40: (3, 4, 3), 200: (3, 4, 3), 210: (3, 4, 2), 256: (2, 4, 3), 300: (1, 4, 3),
-          400: (0, 4, 3), 500: (0, 2, 3), 640: (0, 2, 3), 650: (0, 2, 2), 657: (0, 1, 3), 700: (0, 1, 3),
+    yz = {33: (3, 4, 3), 40: (3, 4, 3), 200: (3, 4, 2), 210: (3, 4, 2), 256: (2, 4, 3), 300: (1, 4, 3),
+          400: (0, 4, 2), 500: (0, 2, 3), 640: (0, 2, 3), 650: (0, 2, 2), 657: (0, 1, 3), 700: (0, 1, 3),
           720: (0, 1, 3), 736: (0, 1, 2), 32: (0, 0, 0), 737: (0, 0, 0), 800: (0, 0, 0)}
     for n, want in yz.items():
         assert _plan(1, n) == want, n

@@ -876,7 +876,7 @@ constexpr int kTmemRingTmemF32 = 8;  // most TMEM rings, two per lane quarter
 template <int AXIS, int MODE>
 __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const SweepParams<float>& p,
                                                  const YzShape& g, int KF, uint64_t* full, float* slots, double* cus,
-                                                 uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
+                                                 double* drs, uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
   constexpr int R = kRowBatch;
   constexpr int CH = kRingRows;
   constexpr int TI = 32;
@@ -953,14 +953,23 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
     const double shift = p.shift[s];
     if (s != staged_s) {
       stage_row(cus, ac.cu + static_cast<size_t>(s) * ac.npad, C * CH);
+      if (drs) stage_row(drs, drp, (C + 1) * CH);  // RN(1/d), one chunk past the line
       staged_s = s;
       __syncwarp();
     }
     float* out = p.f + ((AXIS == 1) ? ((static_cast<size_t>(s) * p.nz + m) * p.ny) * p.nxp
                                     : (static_cast<size_t>(s) * p.nz * p.ny + m) * p.nxp) + i;
-    double cf[R];
+    auto load_cf = [&](int c, double (&cf)[R]) {
+      if (drs) {
 #pragma unroll
-    for (int q = 0; q < R; ++q) cf[q] = __ldg(drp + q);
+        for (int q = 0; q < R; ++q) cf[q] = drs[c * R + q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < R; ++q) cf[q] = __ldg(drp + c * R + q);
+      }
+    };
+    double cf[R];
+    load_cf(0, cf);
     double y = -0.0;
     const bool edge_tile = __any_sync(kAll, !lane_on);
     long long nxt = ntiles;
@@ -1012,8 +1021,7 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
           fpar ^= 1u;
         }
       }
-#pragma unroll
-      for (int q = 0; q < R; ++q) cf[q] = __ldg(drp + (c + 1) * R + q);
+      load_cf(c + 1, cf);
     };
     if (edge_tile) {
       for (int c = 0; c < C; ++c) fwd_chunk(true, c);
@@ -1119,7 +1127,7 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
 template <int AXIS>
 __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
     sweep_yz_tmem_f32_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<float> p,
-                             uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns) {
+                             uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns, int stage_dr) {
   constexpr int CH = kRingRows;
   constexpr int TI = 32;
   constexpr int kSlotElems = CH * TI;
@@ -1143,9 +1151,11 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(ns) * smem_ring_bytes +
                                                     static_cast<size_t>(nt) * tmem_ring_bytes);
   const int nslots = tm ? kf + g.C - min(g.C, kTmemMaxChunks) : g.C;
+  // ring: [barriers] [slots] [upper diagonal] [RN(1/d), when staged]
   uint64_t* full = reinterpret_cast<uint64_t*>(rbase);
-  float* slots = reinterpret_cast<float*>(rbase + (tm ? kTmemBarrierBytes : kBarrierBytes));
+  float* slots = reinterpret_cast<float*>(rbase + kTmemBarrierBytes);
   double* cus = reinterpret_cast<double*>(slots + static_cast<size_t>(nslots) * kSlotElems);
+  double* drs = stage_dr ? cus + static_cast<size_t>(g.C) * CH : nullptr;
 
   if (t == 0) {
     if (warp == 0) prefetch_tmap(&map);
@@ -1166,11 +1176,11 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
     const uint32_t half = static_cast<uint32_t>((warp - ns) >= 4 ? 256 : 0);
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + half;
     if (g.C <= kTmemMaxChunks)
-      yz_tmem_ring_f32<AXIS, 1>(&map, p, g, kf, full, slots, cus, tbase, pend, ppar);
+      yz_tmem_ring_f32<AXIS, 1>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
     else
-      yz_tmem_ring_f32<AXIS, 2>(&map, p, g, kf, full, slots, cus, tbase, pend, ppar);
+      yz_tmem_ring_f32<AXIS, 2>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
   } else {
-    yz_tmem_ring_f32<AXIS, 0>(&map, p, g, kf, full, slots, cus, 0u, pend, ppar);
+    yz_tmem_ring_f32<AXIS, 0>(&map, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
   }
   if (pend != 0) {
     for (int sl = 0; sl < nslots; ++sl)
@@ -1764,40 +1774,56 @@ template cudaError_t launch_tmem_yz<1>(const CUtensorMap&, const SweepParams<dou
 template cudaError_t launch_tmem_yz<2>(const CUtensorMap&, const SweepParams<double>&, const SweepConfig&,
                                        cudaStream_t, bool*);
 
-// One FP32 TMEM ring: barriers, kf input slots plus a slot per chunk past the
-// 16 that its 256 TMEM columns hold, the staged upper-diagonal row (FP64).
-static size_t tmem_yz_f32_ring_bytes(int n_line, int kf) {
-  const int C = (n_line + kRingRows - 1) / kRingRows;
-  const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
-  return kTmemBarrierBytes + static_cast<size_t>(kf + resident) * kRingRows * 32 * 4 +
-         static_cast<size_t>(C) * kRingRows * 8;
+// The staged FP64 coefficient rows of one FP32 ring: the upper diagonal
+// and, with `dr`, RN(1/d) one chunk past the line (as for FP64 above).
+static size_t tmem_yz_f32_coef_bytes(int C, bool dr) {
+  return static_cast<size_t>(C) * kRingRows * 8 + (dr ? static_cast<size_t>(C + 1) * kRingRows * 8 : 0);
 }
 
-static size_t tmem_yz_f32_smem(int n_line, int ns, int nt, int kf) {
-  return 128 + ns * ring_yz_bytes(4, n_line) + nt * tmem_yz_f32_ring_bytes(n_line, kf) + 128;
+// One FP32 TMEM ring: barriers, kf input slots plus a slot per chunk past the
+// 16 that its 256 TMEM columns hold, the staged coefficient rows.
+static size_t tmem_yz_f32_ring_bytes(int n_line, int kf, bool dr) {
+  const int C = (n_line + kRingRows - 1) / kRingRows;
+  const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
+  return kTmemBarrierBytes + static_cast<size_t>(kf + resident) * kRingRows * 32 * 4 + tmem_yz_f32_coef_bytes(C, dr);
+}
+
+// One FP32 shared-memory ring: barriers (at most 32 chunks), the tile, the
+// staged coefficient rows.
+static size_t tmem_yz_f32_smem_ring_bytes(int n_line, bool dr) {
+  const int C = (n_line + kRingRows - 1) / kRingRows;
+  return kTmemBarrierBytes + static_cast<size_t>(C) * kRingRows * 32 * 4 + tmem_yz_f32_coef_bytes(C, dr);
+}
+
+static size_t tmem_yz_f32_smem(int n_line, int ns, int nt, int kf, bool dr) {
+  return 128 + ns * tmem_yz_f32_smem_ring_bytes(n_line, dr) + nt * tmem_yz_f32_ring_bytes(n_line, kf, dr) + 128;
 }
 
 // The FP32 TMEM y/z sweep applies (FP32, lines of at least kTmemFlowSlots
 // chunks, at most 32 slots per ring); the most rings that fit, TMEM rings
 // first, then the most input slots.
-static bool use_tmem_yz_f32(int eb, int n_line, const SweepConfig& cfg, int* ns, int* nt, int* kf) {
+static bool use_tmem_yz_f32(int eb, int n_line, const SweepConfig& cfg, int* ns, int* nt, int* kf, bool* dr) {
   const int C = (n_line + kRingRows - 1) / kRingRows;
   if (eb != 4 || cfg.persistent < 1 || cfg.tmem == 0 || cfg.yz_tile != 32 || C < kTmemFlowSlots) return false;
   const int resident = C > kTmemMaxChunks ? C - kTmemMaxChunks : 0;
+  // the most rings with RN(1/d) staged, unless staging it costs a ring
   int best = 0;
-  for (int t = kTmemRingTmemF32; t >= 1; --t) {
-    for (int f = kTmemFlowSlots; f >= 2; --f) {
-      if (f + resident > 32) continue;
-      for (int k = kTmemRingSmemF32; k >= 0; --k) {
-        if (k > 0 && C > 32) continue;  // a shared-memory ring's barriers: one bit per slot
-        if (tmem_yz_f32_smem(n_line, k, t, f) <= 227 * 1024) {
-          if (k + t > best) {
-            best = k + t;
-            *ns = k;
-            *nt = t;
-            *kf = f;
+  for (int staged = 1; staged >= 0; --staged) {
+    for (int t = kTmemRingTmemF32; t >= 1; --t) {
+      for (int f = kTmemFlowSlots; f >= 2; --f) {
+        if (f + resident > 32) continue;
+        for (int k = kTmemRingSmemF32; k >= 0; --k) {
+          if (k > 0 && C > 32) continue;  // a shared-memory ring's barriers: one bit per slot
+          if (tmem_yz_f32_smem(n_line, k, t, f, staged != 0) <= 227 * 1024) {
+            if (k + t > best) {
+              best = k + t;
+              *ns = k;
+              *nt = t;
+              *kf = f;
+              *dr = staged != 0;
+            }
+            break;
           }
-          break;
         }
       }
     }
@@ -1811,9 +1837,10 @@ cudaError_t launch_tmem_yz_f32(const CUtensorMap& ring_map, const SweepParams<fl
   *launched = false;
   const int n = (AXIS == 1) ? p.ny : p.nz;
   int ns = 0, nt = 0, kf = 0;
-  if (!use_tmem_yz_f32(4, n, cfg, &ns, &nt, &kf)) return cudaSuccess;
+  bool dr = false;
+  if (!use_tmem_yz_f32(4, n, cfg, &ns, &nt, &kf, &dr)) return cudaSuccess;
   const int rings = ns + nt;
-  const size_t smem = tmem_yz_f32_smem(n, ns, nt, kf);
+  const size_t smem = tmem_yz_f32_smem(n, ns, nt, kf, dr);
   const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * p.S;
   int grid = 0;
   cudaError_t e =
@@ -1821,8 +1848,8 @@ cudaError_t launch_tmem_yz_f32(const CUtensorMap& ring_map, const SweepParams<fl
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
   sweep_yz_tmem_f32_kernel<AXIS><<<grid, 32 * rings, smem, st>>>(
-      ring_map, p, static_cast<uint32_t>(ring_yz_bytes(4, n)), static_cast<uint32_t>(tmem_yz_f32_ring_bytes(n, kf)),
-      kf, ns);
+      ring_map, p, static_cast<uint32_t>(tmem_yz_f32_smem_ring_bytes(n, dr)),
+      static_cast<uint32_t>(tmem_yz_f32_ring_bytes(n, kf, dr)), kf, ns, dr ? 1 : 0);
   *launched = true;
   return cudaGetLastError();
 }
@@ -1916,7 +1943,7 @@ extern "C" int bfvm_tmem_sweep_plan(int axis, int n_line, int tmem_level, int* s
   bool dr = false;
   const bool on = axis == 0   ? bfvm::use_tmem_x(8, n_line, false, cfg, &ns, &nt, &kf)
                   : axis == 1 ? bfvm::use_tmem_yz(8, n_line, cfg, &ns, &nt, &kf, &dr)
-                  : axis == 2 ? bfvm::use_tmem_yz_f32(4, n_line, cfg, &ns, &nt, &kf)
+                  : axis == 2 ? bfvm::use_tmem_yz_f32(4, n_line, cfg, &ns, &nt, &kf, &dr)
                               : bfvm::use_tmem_x_f32(4, n_line, false, cfg, &ns, &nt, &kf);
   *smem_rings = on ? ns : 0;
   *tmem_rings = on ? nt : 0;

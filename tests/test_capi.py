@@ -106,7 +106,7 @@ def test_tmem_sweep_plan():
     L = _lib.lib()
     a = C.c_int()
     f32 = {32: (0, 0, 0), 33: (5, 8, 3), 200: (5, 8, 3), 256: (5, 8, 2), 257: (4, 8, 2), 300: (3, 8, 2),
-           400: (0, 8, 3), 512: (0, 5, 3), 640: (0, 3, 3), 736: (0, 3, 2), 737: (0, 0, 0)}
+           400: (0, 8, 3), 512: (0, 5, 2), 640: (0, 3, 3), 736: (0, 3, 2), 737: (0, 0, 0)}
     for n, want in f32.items():
         assert _plan(2, n) == want, n
         assert _plan(2, n, 0) == (0, 0, 0), n

@@ -55,8 +55,8 @@ WORKLOAD = ("cube200: 200x200x200 voxels (dx=10 um), 4 substrates, 100000 agents
 # standalone source kernel plus the x sweep.
 NCU_TRAFFIC = {
     ("fp64", 0): (56552448 + 1760768) + (271819776 + 198265856),
-    ("fp64", 1): 266041600 + 197507840,
-    ("fp64", 2): 266002432 + 194630912,
+    ("fp64", 1): 266214656 + 198479872,
+    ("fp64", 2): 266218240 + 195012864,
 }
 
 

@@ -416,13 +416,12 @@ int bfvm_set_partition_min_line(bfvm_ctx* ctx, int n_line);
 int bfvm_get_partition_min_line(bfvm_ctx* ctx, int* n_line);
 
 /* Tensor-memory (TMEM) rings in the persistent sweeps: on = 1 (default) in
- * the FP64 x, y and z sweeps and the FP32 y and z sweeps on lines of 33 to
- * 736 voxels, and the FP32 x sweep on lines of 257 to 1216 (the x sweeps
- * with agents not fused into them): up to four FP64 rings, or eight FP32
- * rings (two per TMEM lane quarter), keep the forward results of a line's
- * first 256 values in the SM's TMEM beside the shared-memory rings; 2 also
- * in the FP64 x sweep on lines of 17 to 32 and the FP32 x sweep from 33; 0
- * shared memory alone.  Every level gives the same bits. */
+ * the x, y and z sweeps of both precisions on lines of 33 to 736 voxels
+ * (FP32 x lines to 1216; the x sweeps with agents not fused into them): up
+ * to four FP64 rings, or eight FP32 rings (two per TMEM lane quarter), keep
+ * the forward results of a line's first 256 values in the SM's TMEM beside
+ * the shared-memory rings; 2 also in the FP64 x sweep on lines of 17 to 32;
+ * 0 shared memory alone.  Every level gives the same bits. */
 int bfvm_set_sweep_tmem(bfvm_ctx* ctx, int on);
 /* The tensor-memory sweep a persistent sweep would run on lines of n_line
  * voxels (host arithmetic, no device needed): axis 0 = the FP64 x sweep

@@ -674,6 +674,10 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
       __syncwarp();
       tmem_ld32_issue(tbase + 32u * (T - 1), tr);
     }
+    int pend_refill = -1;  // a resident chunk whose slot waits for its store to be read
+    auto refill = [&](int cc) {
+      if (nxt < ntiles) issue(nj0, nk, ns_, T + (NR - 1 - (cc - T)), rslot(flip, cc), (it + 1) & 1u);
+    };
     auto back_chunk = [&](bool edge, int c) {
       const int i0 = c * W;
       const bool flow = MODE == 1 || (MODE == 2 && c < T);
@@ -730,6 +734,10 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
         // the staging chunk's previous bulk store has read it
         if (t == 0) tma_store_wait_read();
         __syncwarp();
+        if (pend_refill >= 0) {  // every store has read its chunk: the waiting slot refills too
+          refill(pend_refill);
+          pend_refill = -1;
+        }
       }
       store_row<double, W>(crow, sw, v);
       // The chunk goes out as it is staged, in one bulk tensor store (rows
@@ -741,16 +749,26 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
         tma_store_commit();
       }
       if (!flow) {
-        // the slot's refill waits for the store to have read it
-        if (t == 0) tma_store_wait_read();
-        __syncwarp();
-        if (nxt < ntiles) issue(nj0, nk, ns_, T + (NR - 1 - (c - T)), rslot(flip, c), (it + 1) & 1u);
+        // A slot refills once its store has read it: the previous resident
+        // chunk's slot now (its store is done reading while this chunk's
+        // stays in flight), this chunk's at the next one or after the tile.
+        if (pend_refill >= 0) {
+          if (t == 0) tma_store_wait_read_1();
+          __syncwarp();
+          refill(pend_refill);
+        }
+        pend_refill = c;
       }
     };
     if (edge_tile) {
       for (int c = C - 1; c >= 0; --c) back_chunk(true, c);
     } else {
       for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
+    }
+    if (pend_refill >= 0) {
+      if (t == 0) tma_store_wait_read();
+      __syncwarp();
+      refill(pend_refill);
     }
     if (MODE == 2 && nxt < ntiles) {
       // the next tile's first inputs take the input slots (the first of
@@ -1214,7 +1232,7 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
 // the 128-byte column [32c, 32c + 32) of the tile's 32 lines; its forward
 // results take 32 TMEM columns, so a ring keeps 8 chunks (lines of up to 256)
 // in 256 columns and two rings share each lane quarter.
-constexpr int kXTmemRingSmemF32 = 3;   // most shared-memory rings (warps 0..ns-1)
+constexpr int kXTmemRingSmemF32 = 0;   // shared-memory rings (none: measured slower, see use_tmem_x_f32)
 constexpr int kXTmemRingTmemF32 = 8;   // most TMEM rings, two per lane quarter
 constexpr int kXTmemMaxChunksF32 = 8;  // chunks of a TMEM ring in its 256 columns
 
@@ -1401,6 +1419,10 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
       __syncwarp();
       tmem_ld16_issue(tbase + 32u * (T - 1) + 16u, tr);
     }
+    int pend_refill = -1;  // a resident chunk whose slot waits for its store to be read
+    auto refill = [&](int cc) {
+      if (nxt < ntiles) issue(nj0, nk, ns_, T + (NR - 1 - (cc - T)), rslot(flip, cc), (it + 1) & 1u);
+    };
     auto back_chunk = [&](bool edge, int c) {
       const int i0 = c * W;
       const bool flow = MODE == 1 || (MODE == 2 && c < T);
@@ -1410,6 +1432,10 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
         // the staging chunk's previous bulk store has read it
         if (t == 0) tma_store_wait_read();
         __syncwarp();
+        if (pend_refill >= 0) {  // every store has read its chunk: the waiting slot refills too
+          refill(pend_refill);
+          pend_refill = -1;
+        }
       }
 #pragma unroll
       for (int hh = 0; hh < 2; ++hh) {
@@ -1487,16 +1513,26 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
         tma_store_commit();
       }
       if (!flow) {
-        // the slot's refill waits for the store to have read it
-        if (t == 0) tma_store_wait_read();
-        __syncwarp();
-        if (nxt < ntiles) issue(nj0, nk, ns_, T + (NR - 1 - (c - T)), rslot(flip, c), (it + 1) & 1u);
+        // A slot refills once its store has read it: the previous resident
+        // chunk's slot now (its store is done reading while this chunk's
+        // stays in flight), this chunk's at the next one or after the tile.
+        if (pend_refill >= 0) {
+          if (t == 0) tma_store_wait_read_1();
+          __syncwarp();
+          refill(pend_refill);
+        }
+        pend_refill = c;
       }
     };
     if (edge_tile) {
       for (int c = C - 1; c >= 0; --c) back_chunk(true, c);
     } else {
       for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
+    }
+    if (pend_refill >= 0) {
+      if (t == 0) tma_store_wait_read();
+      __syncwarp();
+      refill(pend_refill);
     }
     if (MODE == 2 && nxt < ntiles) {
       // the next tile's first inputs take the input slots (the first of
@@ -1875,18 +1911,17 @@ static size_t x_tmem_f32_smem(int nx, int ns, int nt, int kf) {
   return 1024 + ns * x_tmem_f32_ring_bytes(nx, false, kf) + nt * x_tmem_f32_ring_bytes(nx, true, kf) + 128;
 }
 
-// The FP32 TMEM x sweep applies (FP32, agents not fused, 32-line tiles, at
-// most 32 slots per ring): by default on lines of more than 8 chunks (257
-// voxels), at sweep TMEM level 2 from 2 chunks (33); *ns shared-memory rings
-// and *nt TMEM rings (the most that fit), *kf input slots per TMEM ring.
-// Measured on B200 against the per-tile FP32 x sweep, n^3 cubes with 2
-// substrates: equal at n = 200 and 320 (cube200's 4 substrates: 0.127
-// against 0.120 ms), 0.405 against 0.552 ms at 400, 0.815 / 1.001 at 512,
-// 2.22 / 2.74 at 640 -- where the per-tile sweep fits few tiles per SM.
+// The FP32 TMEM x sweep applies (FP32, agents not fused, 32-line tiles,
+// lines of at least 2 chunks = 33 voxels, at most 32 slots per ring): *nt
+// TMEM rings (the most that fit) and *kf input slots per ring, no
+// shared-memory rings.  Measured on B200 against the per-tile FP32 x sweep:
+// cube200 (4 substrates) 0.110 against 0.120 ms, n^3 cubes with 2
+// substrates 0.98-1.00 from 256 to 640 voxels, 1.06 at 200 (2.4 tiles per
+// ring); with 3 shared-memory rings beside the 8 TMEM rings it had lost 6%
+// at cube200 (0.127 ms), 5 + 4 rings 24%.
 static bool use_tmem_x_f32(int eb, int nx, bool fused_agents, const SweepConfig& cfg, int* ns, int* nt, int* kf) {
   const int C = (nx + 31) / 32;
   if (eb != 4 || fused_agents || cfg.persistent < 1 || cfg.tmem == 0 || cfg.x_lines != 32 || C < 2) return false;
-  if (cfg.tmem < 2 && C <= kXTmemMaxChunksF32) return false;
   const int resident = C > kXTmemMaxChunksF32 ? C - kXTmemMaxChunksF32 : 0;
   int best = 0;
   for (int t = kXTmemRingTmemF32; t >= 1; --t) {

@@ -88,8 +88,8 @@ def test_tmem_sweep_plan():
     x lines under 2 at level 2, any line past 736 = 46 chunks, whose 30
     resident chunks and 2 input slots fill a ring's 32 slots); and the FP32
     sweeps' (axis 2 y/z: up to 5 shared-memory and 8 TMEM rings, two per
-    lane quarter; axis 3 x: up to 3 + 8 rings, 32-value chunks, 8 of them
-    in a ring's TMEM columns, by default past 256 and at level 2 from 33)."""
+    lane quarter; axis 3 x: TMEM rings only, up to 8, 32-value chunks, 8
+    of them in a ring's TMEM columns)."""
     yz = {33: (3, 4, 3), 40: (3, 4, 3), 200: (3, 4, 2), 210: (3, 4, 2), 256: (2, 4, 3), 300: (1, 4, 3),
           400: (0, 4, 2), 500: (0, 2, 3), 640: (0, 2, 3), 650: (0, 2, 2), 657: (0, 1, 3), 700: (0, 1, 3),
           720: (0, 1, 3), 736: (0, 1, 2), 32: (0, 0, 0), 737: (0, 0, 0), 800: (0, 0, 0)}
@@ -110,13 +110,12 @@ def test_tmem_sweep_plan():
     for n, want in f32.items():
         assert _plan(2, n) == want, n
         assert _plan(2, n, 0) == (0, 0, 0), n
-    fx32 = {32: (0, 0, 0), 33: (0, 0, 0), 200: (0, 0, 0), 256: (0, 0, 0), 257: (2, 8, 2), 300: (1, 8, 2),
-            400: (0, 7, 2), 640: (0, 3, 3), 1024: (0, 1, 3)}
+    fx32 = {32: (0, 0, 0), 33: (0, 8, 2), 200: (0, 8, 3), 256: (0, 8, 3), 257: (0, 8, 3), 300: (0, 8, 3),
+            400: (0, 7, 2), 640: (0, 3, 3), 1024: (0, 1, 3), 1216: (0, 1, 2), 1217: (0, 0, 0)}
     for n, want in fx32.items():
         assert _plan(3, n) == want, n
-        assert _plan(3, n, 0) == (0, 0, 0), n
-    for n, want in {32: (0, 0, 0), 33: (3, 8, 2), 200: (3, 8, 2), 256: (3, 8, 2), 640: (0, 3, 3)}.items():
         assert _plan(3, n, 2) == want, n
+        assert _plan(3, n, 0) == (0, 0, 0), n
     for args in ((4, 100, 1), (-1, 100, 1), (1, 0, 1), (1, 100, 3), (0, 100, -1)):
         assert L.bfvm_tmem_sweep_plan(*args, C.byref(a), C.byref(a), C.byref(a)) == _lib.BFVM_ERR_ARG
     assert L.bfvm_tmem_sweep_plan(1, 100, 1, None, C.byref(a), C.byref(a)) == _lib.BFVM_ERR_ARG

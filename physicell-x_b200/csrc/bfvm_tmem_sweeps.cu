@@ -888,7 +888,7 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
 // share each lane quarter (warps ns + r and ns + r + 4 take the quarter's two
 // column halves): up to eight TMEM rings beside up to five shared-memory
 // rings, 416 lines of 200 per SM where the shared-memory ring sweep holds 224.
-constexpr int kTmemRingSmemF32 = 5;  // most shared-memory rings (warps 0..ns-1)
+constexpr int kTmemRingSmemF32 = 3;  // most shared-memory rings (warps 0..ns-1; 3 measured best of 0-5)
 constexpr int kTmemRingTmemF32 = 8;  // most TMEM rings, two per lane quarter
 
 template <int AXIS, int MODE>

@@ -87,7 +87,7 @@ def test_tmem_sweep_plan():
     shared-memory schedules take over (y/z lines under 3 chunks of 16 rows,
     x lines under 2 at level 2, any line past 736 = 46 chunks, whose 30
     resident chunks and 2 input slots fill a ring's 32 slots); and the FP32
-    sweeps' (axis 2 y/z: up to 5 shared-memory and 8 TMEM rings, two per
+    sweeps' (axis 2 y/z: up to 3 shared-memory and 8 TMEM rings, two per
     lane quarter; axis 3 x: TMEM rings only, up to 8, 32-value chunks, 8
     of them in a ring's TMEM columns)."""
     yz = {33: (3, 4, 3), 40: (3, 4, 3), 200: (3, 4, 2), 210: (3, 4, 2), 256: (2, 4, 3), 300: (1, 4, 3),
@@ -105,7 +105,7 @@ def test_tmem_sweep_plan():
         assert _plan(0, n, 2) == want, n
     L = _lib.lib()
     a = C.c_int()
-    f32 = {32: (0, 0, 0), 33: (5, 8, 3), 200: (5, 8, 3), 256: (5, 8, 2), 257: (4, 8, 2), 300: (3, 8, 2),
+    f32 = {32: (0, 0, 0), 33: (3, 8, 3), 200: (3, 8, 3), 256: (3, 8, 3), 257: (3, 8, 3), 300: (3, 8, 2),
            400: (0, 8, 3), 512: (0, 5, 2), 640: (0, 3, 3), 736: (0, 3, 2), 737: (0, 0, 0)}
     for n, want in f32.items():
         assert _plan(2, n) == want, n

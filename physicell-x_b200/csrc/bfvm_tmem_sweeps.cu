@@ -1236,11 +1236,13 @@ constexpr int kXTmemRingSmemF32 = 0;   // shared-memory rings (none: measured sl
 constexpr int kXTmemRingTmemF32 = 8;   // most TMEM rings, two per lane quarter
 constexpr int kXTmemMaxChunksF32 = 8;  // chunks of a TMEM ring in its 256 columns
 
-template <int MODE>
+// STAGED: RN(1/d) read from the ring's copy `drs` in shared memory, else
+// from global memory.
+template <int MODE, bool STAGED>
 __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const SweepParams<float>& p,
                                                 const XShape& g, int KF, unsigned char* slots, uint64_t* full,
-                                                double* cus, unsigned char* stage, uint32_t tbase, uint32_t& pend,
-                                                uint32_t& ppar) {
+                                                double* cus, double* drs, unsigned char* stage, uint32_t tbase,
+                                                uint32_t& pend, uint32_t& ppar) {
   constexpr int W = 32;  // floats per 128-byte chunk row
   constexpr uint32_t kChunkBytes = 32u * 128u;
   constexpr unsigned kAll = 0xffffffffu;
@@ -1306,6 +1308,7 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
     const double off = p.off[s];
     if (s != staged_s) {
       stage_row(cus, p.ax.cu + static_cast<size_t>(s) * p.ax.npad, C * W);
+      if (STAGED) stage_row(drs, drp, (C + 1) * W);  // RN(1/d), one chunk past the line (the prefetch)
       staged_s = s;
       __syncwarp();
     }
@@ -1323,7 +1326,7 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
     }
     double cf[16];  // the coefficients RN(1/d) of the next 16 values
 #pragma unroll
-    for (int q = 0; q < 16; ++q) cf[q] = __ldg(drp + q);
+    for (int q = 0; q < 16; ++q) cf[q] = STAGED ? drs[q] : __ldg(drp + q);
     double y = -0.0;
     const bool edge_tile = __any_sync(kAll, !lane_on);
     long long nxt = ntiles;
@@ -1383,7 +1386,7 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
         }
         // the next half's coefficients (rows are padded past the line)
 #pragma unroll
-        for (int q = 0; q < 16; ++q) cf[q] = __ldg(drp + e0 + 16 + q);
+        for (int q = 0; q < 16; ++q) cf[q] = STAGED ? drs[e0 + 16 + q] : __ldg(drp + e0 + 16 + q);
       }
       if (flow) {
         __syncwarp();  // every lane has read the slot
@@ -1565,7 +1568,7 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
 
 __global__ void __launch_bounds__(32 * (kXTmemRingSmemF32 + kXTmemRingTmemF32), 1)
     sweep_x_tmem_f32_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<float> p,
-                            uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns) {
+                            uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns, int stage_dr) {
   constexpr uint32_t kChunkBytes = 32u * 128u;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + smem_align_pad(smem_raw, 1024);
@@ -1584,15 +1587,17 @@ __global__ void __launch_bounds__(32 * (kXTmemRingSmemF32 + kXTmemRingTmemF32), 
                             : base + static_cast<size_t>(warp) * smem_ring_bytes;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(ns) * smem_ring_bytes +
                                                     static_cast<size_t>(nt) * tmem_ring_bytes);
-  // ring: [slots (+ staging chunk)] [upper diagonal] [barriers]; a TMEM ring
-  // over more than 8 chunks stages in its first input slot
+  // ring: [slots (+ staging chunk)] [upper diagonal] [RN(1/d) when staged]
+  // [barriers]; a TMEM ring over more than 8 chunks stages in its first input slot
   const bool own_stage = tm && g.C <= kXTmemMaxChunksF32;
   const int nslots = tm ? kf + g.C - min(g.C, kXTmemMaxChunksF32) : g.C;
   unsigned char* slots = rbase;
   unsigned char* stage = tm ? (own_stage ? rbase + static_cast<size_t>(nslots) * kChunkBytes : rbase) : nullptr;
   double* cus = reinterpret_cast<double*>(rbase + static_cast<size_t>(nslots + (own_stage ? 1 : 0)) * kChunkBytes);
-  uint64_t* full = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(cus) +
-                                               static_cast<size_t>(g.C) * 32 * sizeof(double));
+  // RN(1/d) of (C + 1) chunks when staged, then the barriers
+  double* drs = stage_dr ? cus + static_cast<size_t>(g.C) * 32 : nullptr;
+  uint64_t* full =
+      reinterpret_cast<uint64_t*>(cus + static_cast<size_t>(g.C) * 32 + (stage_dr ? (g.C + 1) * 32 : 0));
 
   if (t == 0) {
     if (warp == 0) prefetch_tmap(&map);
@@ -1612,12 +1617,17 @@ __global__ void __launch_bounds__(32 * (kXTmemRingSmemF32 + kXTmemRingTmemF32), 
     // lane quarter warp % 4; the second ring on a quarter takes columns 256..511
     const uint32_t half = static_cast<uint32_t>((warp - ns) >= 4 ? 256 : 0);
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + half;
-    if (own_stage)
-      x_tmem_ring_f32<1>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+    if (own_stage && stage_dr)
+      x_tmem_ring_f32<1, true>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
+    else if (own_stage)
+      x_tmem_ring_f32<1, false>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
+    else if (stage_dr)
+      x_tmem_ring_f32<2, true>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
     else
-      x_tmem_ring_f32<2>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+      x_tmem_ring_f32<2, false>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
   } else {
-    x_tmem_ring_f32<0>(&map, p, g, kf, slots, full, cus, nullptr, 0u, pend, ppar);
+    // no shared-memory rings are planned (kXTmemRingSmemF32 = 0); kept for the plan's range
+    x_tmem_ring_f32<0, false>(&map, p, g, kf, slots, full, cus, drs, nullptr, 0u, pend, ppar);
   }
   if (pend != 0) {
     for (int sl = 0; sl < nslots; ++sl)
@@ -1900,15 +1910,17 @@ template cudaError_t launch_tmem_yz_f32<2>(const CUtensorMap&, const SweepParams
 // = kf input chunks and a staging chunk, or, past 8 chunks, kf input chunks
 // and a resident chunk for each chunk past 8; then the upper diagonal (FP64)
 // and the barriers.
-static size_t x_tmem_f32_ring_bytes(int nx, bool tm, int kf) {
+static size_t x_tmem_f32_ring_bytes(int nx, bool tm, int kf, bool dr) {
   const int C = (nx + 31) / 32;
   const int chunks = !tm ? C : (C <= kXTmemMaxChunksF32 ? kf + 1 : kf + C - kXTmemMaxChunksF32);
-  const size_t b = static_cast<size_t>(chunks) * 32 * 128 + static_cast<size_t>(C) * 32 * 8 + kXTmemBarrierBytes;
+  // chunks, the upper diagonal (C chunks), RN(1/d) (C + 1 chunks) when staged, barriers
+  const size_t b = static_cast<size_t>(chunks) * 32 * 128 + static_cast<size_t>(dr ? 2 * C + 1 : C) * 32 * 8 +
+                   kXTmemBarrierBytes;
   return (b + 1023) / 1024 * 1024;
 }
 
-static size_t x_tmem_f32_smem(int nx, int ns, int nt, int kf) {
-  return 1024 + ns * x_tmem_f32_ring_bytes(nx, false, kf) + nt * x_tmem_f32_ring_bytes(nx, true, kf) + 128;
+static size_t x_tmem_f32_smem(int nx, int ns, int nt, int kf, bool dr) {
+  return 1024 + ns * x_tmem_f32_ring_bytes(nx, false, kf, dr) + nt * x_tmem_f32_ring_bytes(nx, true, kf, dr) + 128;
 }
 
 // The FP32 TMEM x sweep applies (FP32, agents not fused, 32-line tiles,
@@ -1919,24 +1931,30 @@ static size_t x_tmem_f32_smem(int nx, int ns, int nt, int kf) {
 // substrates 0.98-1.00 from 256 to 640 voxels, 1.06 at 200 (2.4 tiles per
 // ring); with 3 shared-memory rings beside the 8 TMEM rings it had lost 6%
 // at cube200 (0.127 ms), 5 + 4 rings 24%.
-static bool use_tmem_x_f32(int eb, int nx, bool fused_agents, const SweepConfig& cfg, int* ns, int* nt, int* kf) {
+static bool use_tmem_x_f32(int eb, int nx, bool fused_agents, const SweepConfig& cfg, int* ns, int* nt, int* kf,
+                           bool* dr) {
   const int C = (nx + 31) / 32;
   if (eb != 4 || fused_agents || cfg.persistent < 1 || cfg.tmem == 0 || cfg.x_lines != 32 || C < 2) return false;
   const int resident = C > kXTmemMaxChunksF32 ? C - kXTmemMaxChunksF32 : 0;
+  // the most rings with RN(1/d) staged per ring (cube200: 0.106 against
+  // 0.110 ms), unless staging it costs a ring
   int best = 0;
-  for (int t = kXTmemRingTmemF32; t >= 1; --t) {
-    for (int f = min(C, kTmemFlowSlots); f >= 2; --f) {
-      if (f + resident > 32) continue;
-      for (int k = kXTmemRingSmemF32; k >= 0; --k) {
-        if (k > 0 && C > 32) continue;  // a shared-memory ring's barriers: one bit per slot
-        if (x_tmem_f32_smem(nx, k, t, f) <= 227 * 1024) {
-          if (k + t > best) {
-            best = k + t;
-            *ns = k;
-            *nt = t;
-            *kf = f;
+  for (int staged = 1; staged >= 0; --staged) {
+    for (int t = kXTmemRingTmemF32; t >= 1; --t) {
+      for (int f = min(C, kTmemFlowSlots); f >= 2; --f) {
+        if (f + resident > 32) continue;
+        for (int k = kXTmemRingSmemF32; k >= 0; --k) {
+          if (k > 0 && C > 32) continue;  // a shared-memory ring's barriers: one bit per slot
+          if (x_tmem_f32_smem(nx, k, t, f, staged != 0) <= 227 * 1024) {
+            if (k + t > best) {
+              best = k + t;
+              *ns = k;
+              *nt = t;
+              *kf = f;
+              *dr = staged != 0;
+            }
+            break;
           }
-          break;
         }
       }
     }
@@ -1948,17 +1966,18 @@ cudaError_t launch_tmem_x_f32(const CUtensorMap& map, const SweepParams<float>& 
                               cudaStream_t st, bool* launched) {
   *launched = false;
   int ns = 0, nt = 0, kf = 0;
-  if (!use_tmem_x_f32(4, p.nx, p.line_off != nullptr, cfg, &ns, &nt, &kf)) return cudaSuccess;
+  bool dr = false;
+  if (!use_tmem_x_f32(4, p.nx, p.line_off != nullptr, cfg, &ns, &nt, &kf, &dr)) return cudaSuccess;
   const int rings = ns + nt;
-  const size_t smem = x_tmem_f32_smem(p.nx, ns, nt, kf);
+  const size_t smem = x_tmem_f32_smem(p.nx, ns, nt, kf, dr);
   const long long tiles = static_cast<long long>((p.ny + 31) / 32) * p.nz * p.S;
   int grid = 0;
   cudaError_t e = persistent_grid(sweep_x_tmem_f32_kernel, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
   sweep_x_tmem_f32_kernel<<<grid, 32 * rings, smem, st>>>(
-      map, p, static_cast<uint32_t>(x_tmem_f32_ring_bytes(p.nx, false, kf)),
-      static_cast<uint32_t>(x_tmem_f32_ring_bytes(p.nx, true, kf)), kf, ns);
+      map, p, static_cast<uint32_t>(x_tmem_f32_ring_bytes(p.nx, false, kf, dr)),
+      static_cast<uint32_t>(x_tmem_f32_ring_bytes(p.nx, true, kf, dr)), kf, ns, dr ? 1 : 0);
   *launched = true;
   return cudaGetLastError();
 }
@@ -1979,7 +1998,7 @@ extern "C" int bfvm_tmem_sweep_plan(int axis, int n_line, int tmem_level, int* s
   const bool on = axis == 0   ? bfvm::use_tmem_x(8, n_line, false, cfg, &ns, &nt, &kf)
                   : axis == 1 ? bfvm::use_tmem_yz(8, n_line, cfg, &ns, &nt, &kf, &dr)
                   : axis == 2 ? bfvm::use_tmem_yz_f32(4, n_line, cfg, &ns, &nt, &kf, &dr)
-                              : bfvm::use_tmem_x_f32(4, n_line, false, cfg, &ns, &nt, &kf);
+                              : bfvm::use_tmem_x_f32(4, n_line, false, cfg, &ns, &nt, &kf, &dr);
   *smem_rings = on ? ns : 0;
   *tmem_rings = on ? nt : 0;
   *input_slots = on ? kf : 0;

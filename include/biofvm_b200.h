@@ -396,7 +396,7 @@ int bfvm_get_sweep_schedule(bfvm_ctx* ctx, int* persistent);
  * (the tests measure it against the oracle).  The back substitution, the
  * sources and the pins are the same in both.  chain = 2: chain 1, except
  * that long y and z lines are solved by a partition
- * method (by default on lines of at least 512 voxels in FP64 and 288 in
+ * method (by default on lines of at least 512 voxels in FP64 and 448 in
  * FP32, where it is the faster one): eight warps share each 32-line tile,
  * each warp running both recurrences over one eighth of the line, joined
  * through segment products that the host forms in extended precision at
@@ -410,7 +410,7 @@ int bfvm_get_sweep_schedule(bfvm_ctx* ctx, int* persistent);
 int bfvm_set_fp64_chain(bfvm_ctx* ctx, int chain);
 int bfvm_get_fp64_chain(bfvm_ctx* ctx, int* chain);
 /* The shortest y or z line that chain 2 solves partitioned: n_line >= 1,
- * or -1 for the default of the solve's precision (512 FP64, 288 FP32).
+ * or -1 for the default of the solve's precision (512 FP64, 448 FP32).
  * bfvm_get_partition_min_line returns the value in effect. */
 int bfvm_set_partition_min_line(bfvm_ctx* ctx, int n_line);
 int bfvm_get_partition_min_line(bfvm_ctx* ctx, int* n_line);

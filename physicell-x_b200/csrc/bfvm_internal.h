@@ -216,11 +216,11 @@ size_t part_smem_bytes(int elem_bytes, int n_line);
 // under chain 2 (bfvm_set_partition_min_line overrides it); shorter lines,
 // and the x sweep, run the short chain on the serial kernels.  Measured on
 // B200, mean y/z sweep time on n^3 cubes, partitioned over serial short
-// chain: FP64 1.23 at n = 200, 1.00 at 384, 1.09 at 448, 0.89 at 512, 0.64
-// at 640; FP32 1.25 at 200, 1.03 at 256, 0.97 at 288, 0.80 at 320, 0.49 at
-// 640 (FP32 tiles are half the bytes, so more CTAs share an SM).
+// chain: FP64 1.00 at n = 384 and 448, 0.94 at 512, 0.64 at 640; FP32 (the
+// serial sweeps with their tensor-memory rings) 1.21 at 288, 1.06 at 320,
+// 1.07 at 384, 0.93 at 448, 0.80 at 512, 0.65 at 640.
 constexpr int kPartMinLine64 = 512;
-constexpr int kPartMinLine32 = 288;
+constexpr int kPartMinLine32 = 448;
 template <typename T, int AXIS>
 cudaError_t launch_part(const CUtensorMap& map, const SweepParams<T>& p, const PartAxis& pa, cudaStream_t st);
 

@@ -59,7 +59,9 @@ struct YzShape {
 // each completes) when a wait gave up.
 // MODE 0: shared-memory ring; 1: TMEM ring (C <= 16); 2: TMEM ring with
 // resident chunks (C > 16).
-template <int AXIS, int MODE>
+// STAGED: the forward pairs read from the ring's copy `drs` in shared
+// memory, else from global memory.
+template <int AXIS, int MODE, bool STAGED>
 __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const SweepParams<double>& p, const YzShape& g,
                                              int KF, uint64_t* full, double* slots, double* cus, double2* drs,
                                              uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
@@ -147,7 +149,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
       // substitution, the forward pairs (one chunk past the line, for the
       // prefetch) -- read as shared-memory broadcasts
       stage_row(cus, ac.cu + static_cast<size_t>(s) * ac.npad, C * CH);
-      if (drs) stage_row(reinterpret_cast<double*>(drs), reinterpret_cast<const double*>(drp), 2 * (C + 1) * CH);
+      if (STAGED) stage_row(reinterpret_cast<double*>(drs), reinterpret_cast<const double*>(drp), 2 * (C + 1) * CH);
       staged_s = s;
       __syncwarp();
     }
@@ -155,13 +157,8 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
                                      : (static_cast<size_t>(s) * p.nz * p.ny + m) * p.nxp) + i;
     // forward pairs of chunk c (staged, or from global where the plan had no room)
     auto load_cf = [&](int c, DR (&cf)[R]) {
-      if (drs) {
 #pragma unroll
-        for (int q = 0; q < R; ++q) cf[q] = drs[c * R + q];
-      } else {
-#pragma unroll
-        for (int q = 0; q < R; ++q) cf[q] = __ldg(drp + c * R + q);
-      }
+      for (int q = 0; q < R; ++q) cf[q] = STAGED ? drs[c * R + q] : __ldg(drp + c * R + q);
     };
     DR cf[R];
     load_cf(0, cf);
@@ -405,12 +402,22 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   if (tm) {
     tmem_fence_after();
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
-    if (g.C <= kTmemMaxChunks)
-      yz_tmem_ring<AXIS, 1>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
-    else
-      yz_tmem_ring<AXIS, 2>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+    if (g.C <= kTmemMaxChunks) {
+      if (stage_dr)
+        yz_tmem_ring<AXIS, 1, true>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+      else
+        yz_tmem_ring<AXIS, 1, false>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+    } else {
+      if (stage_dr)
+        yz_tmem_ring<AXIS, 2, true>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+      else
+        yz_tmem_ring<AXIS, 2, false>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+    }
   } else {
-    yz_tmem_ring<AXIS, 0>(&map, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
+    if (stage_dr)
+      yz_tmem_ring<AXIS, 0, true>(&map, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
+    else
+      yz_tmem_ring<AXIS, 0, false>(&map, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
   }
 
   // Loads still in flight (only after a wait gave up) land before the CTA

@@ -113,7 +113,7 @@ def test_partitioned_sweeps_edge_shapes(shape, precision):
     expect = Port.run(wl)
     me = Microenvironment.from_workload(wl, precision=precision)
     me.set_fp64_chain(2)
-    assert me.get_partition_min_line() == (512 if precision == "fp64" else 288)
+    assert me.get_partition_min_line() == (512 if precision == "fp64" else 448)
     me.set_partition_min_line(1)  # every y and z line, however short, runs partitioned
     me.simulate_diffusion_decay(wl.steps, sources=True)
     got = me.download_field()

@@ -21,6 +21,13 @@ reference's arithmetic (bit-identical results).
   fp64_short_chain  the same resident step with the opt-in short FP64
          forward chain (bfvm_set_fp64_chain), which is within 1e-12 of the
          reference per voxel rather than bit-identical.
+  roofline  of the slowest kernel of the step (the x sweep), from CUDA
+         events around each kernel: its algorithmic bytes (the field read
+         and written once, its coefficients) over its time, against the
+         measured HBM copy bandwidth; per_kernel lists the source kernel and
+         the three sweeps, x_interval the source kernel and the x sweep
+         together, step_frac the whole step (six field passes, coefficients
+         and agents) over the step time.
 
 Multi-GPU: one process per GPU, each advancing its own replica of the
 workload (the solve does not shard; replicas only), value summed.
@@ -48,15 +55,15 @@ WORKLOAD = ("cube200: 200x200x200 voxels (dx=10 um), 4 substrates, 100000 agents
             "one LOD step = agent sources (standalone kernel, timed with the x sweep) + x/y/z Thomas "
             "sweeps with Dirichlet pins, the reference's arithmetic (bit-identical)")
 
-# DRAM bytes per launch of each timed interval (dram__bytes_read.sum +
-# dram__bytes_write.sum) from one ncu capture of this workload at the current
-# kernels; profiles/sweeps_cube200_fp64.txt gives the command and the raw
-# figures.  Keys: (precision, sweep index 0=x 1=y 2=z); the x interval is the
-# standalone source kernel plus the x sweep.
+# DRAM bytes per launch of each timed kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum) from one-kernel ncu captures of this workload at the
+# current kernels; profiles/sweeps_cube200_fp64.txt gives the commands and
+# the raw figures.  Keys: (precision, kernel index 0=sources 1=x 2=y 3=z).
 NCU_TRAFFIC = {
-    ("fp64", 0): (56552448 + 1760768) + (271819776 + 198265856),
-    ("fp64", 1): 266214656 + 198479872,
-    ("fp64", 2): 266218240 + 195012864,
+    ("fp64", 0): 56552448 + 1760768,
+    ("fp64", 1): 271819776 + 198265856,
+    ("fp64", 2): 266214656 + 198479872,
+    ("fp64", 3): 266218240 + 195012864,
 }
 
 
@@ -336,8 +343,8 @@ def time_resident(me, steps, stream):
     me.synchronize()
     torch.cuda.synchronize()
     me.timing_enable(False)
-    ms_xyz, nrec = me.timing_read()
-    return ev0.elapsed_time(ev1) / steps, ms_xyz / max(1, nrec), kernel_launches() - launches0
+    ms_sxyz, nrec = me.timing_read_kernels()
+    return ev0.elapsed_time(ev1) / steps, ms_sxyz / max(1, nrec), kernel_launches() - launches0
 
 
 def main():
@@ -390,23 +397,32 @@ def main():
     value = world * N * S / (ms_step * 1e-3)
 
     # ---- roofline of the dominant kernel -------------------------------------
+    # per kernel of the step: the standalone source kernel, then the sweeps;
+    # algorithmic bytes: a sweep reads and writes the field once and reads its
+    # axis' coefficients; the source kernel reads the agents (voxel id and
+    # three constants per substrate) and the x-line offsets, and reads and
+    # writes each agent's voxel values
     eb = 8 if args.precision == "fp64" else 4
-    names = ["sweep_x (+sources, pins)", "sweep_y (+pins)", "sweep_z (+pins)"]
+    names = ["agent_sources", "sweep_x (+pins)", "sweep_y (+pins)", "sweep_z (+pins)"]
     field_bytes = 2 * N * S * eb
     coef_bytes = [3 * wl.nx * S * 8, 3 * wl.ny * S * 8, 3 * wl.nz * S * 8]
     agent_bytes = A * (4 + 3 * S * 8) + (wl.ny * wl.nz + 1) * 4
-    alg = [field_bytes + coef_bytes[0] + agent_bytes, field_bytes + coef_bytes[1], field_bytes + coef_bytes[2]]
+    alg = [agent_bytes + A * S * 2 * eb] + [field_bytes + coef_bytes[a] for a in range(3)]
     peak, peak_kind = load_peaks()
-    step_bytes = sum(alg)
+    step_bytes = 3 * field_bytes + sum(coef_bytes) + agent_bytes  # six field passes + coefficients + agents
 
     def roofline_of(kernel_ms, step_ms):
-        dom = int(np.argmax(kernel_ms))
+        dom = 1 + int(np.argmax(kernel_ms[1:]))  # the slowest sweep (the source kernel is a few % of the step)
         achieved = alg[dom] / (kernel_ms[dom] * 1e-3) / 1e9
+        x_int = kernel_ms[0] + kernel_ms[1]
         return {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": NCU_TRAFFIC.get((args.precision, dom)),
                 "algorithmic_bytes_per_launch": alg[dom],
                 "per_kernel": [{"kernel": names[k], "ms": kernel_ms[k],
-                                "GB/s": alg[k] / (kernel_ms[k] * 1e-3) / 1e9} for k in range(3)],
+                                "GB/s": alg[k] / (kernel_ms[k] * 1e-3) / 1e9} for k in range(4)],
+                # the source kernel and the x sweep together, as one interval
+                "x_interval": {"ms": x_int, "GB/s": (alg[0] + alg[1]) / (x_int * 1e-3) / 1e9,
+                               "frac": (alg[0] + alg[1]) / (x_int * 1e-3) / 1e9 / peak},
                 "step_frac": (step_bytes / (step_ms * 1e-3) / 1e9) / peak}
 
     roofline = roofline_of(per_kernel_ms, ms_step)

@@ -439,12 +439,17 @@ long long bfvm_kernel_launches(void);
 
 /* Per-kernel timing, the device counterpart of the reference's per-step
  * timers (tests/mpi/diffusion/main.cpp:197-214): while enabled, every step
- * records CUDA events on the solve's stream around the x, y and z sweep
- * kernels.  bfvm_timing_read waits for the stream and returns the summed
- * durations [3] (ms: x, y, z) and the number of steps recorded, then clears
- * them.  At most 4096 steps are recorded between reads. */
+ * records CUDA events on the solve's stream around the source kernel and the
+ * x, y and z sweep kernels.  bfvm_timing_read waits for the stream and
+ * returns the summed durations [3] (ms: sources with x, y, z) and the number
+ * of steps recorded, then clears them.  At most 4096 steps are recorded
+ * between reads. */
 int bfvm_timing_enable(bfvm_ctx* ctx, int on);
 int bfvm_timing_read(bfvm_ctx* ctx, double* ms_xyz, int* steps);
+/* The same records split by kernel: ms_sxyz [4] = the standalone source
+ * kernel (0 without one), the x, y and z sweeps.  Reads and clears the
+ * records as bfvm_timing_read does. */
+int bfvm_timing_read_kernels(bfvm_ctx* ctx, double* ms_sxyz, int* steps);
 
 const char* bfvm_status_string(int status);
 

@@ -108,6 +108,7 @@ _SIGS = {
     "bfvm_kernel_launches": (C.c_longlong, []),
     "bfvm_timing_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_timing_read": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
+    "bfvm_timing_read_kernels": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
     "bfvm_status_string": (C.c_char_p, [C.c_int]),
     "bfvm_batch_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "bfvm_batch_destroy": (C.c_int, [C.c_void_p]),

@@ -324,10 +324,19 @@ class Microenvironment:
         check(self.L.bfvm_timing_enable(self.h, 1 if on else 0), "bfvm_timing_enable")
 
     def timing_read(self):
-        """(ms_x, ms_y, ms_z) summed over the recorded steps, and the step count."""
+        """(ms_x, ms_y, ms_z) summed over the recorded steps (the source kernel
+        counted with x), and the step count."""
         ms = np.zeros(3, np.float64)
         n = C.c_int()
         check(self.L.bfvm_timing_read(self.h, _ptr(ms), C.byref(n)), "bfvm_timing_read")
+        return ms, int(n.value)
+
+    def timing_read_kernels(self):
+        """(ms_sources, ms_x, ms_y, ms_z) summed over the recorded steps, and
+        the step count."""
+        ms = np.zeros(4, np.float64)
+        n = C.c_int()
+        check(self.L.bfvm_timing_read_kernels(self.h, _ptr(ms), C.byref(n)), "bfvm_timing_read_kernels")
         return ms, int(n.value)
 
     def set_sweep_schedule(self, persistent=1):

@@ -82,6 +82,7 @@ void thomas_axis_host(int n, int S, const double* D, const double* decay, double
 namespace {
 
 constexpr int kMaxTimedSteps = 4096;
+constexpr int kStepEvents = 5;  // timing events per recorded step (enqueue_step)
 // LOD steps per captured CUDA graph of bfvm_step (four launches each).
 constexpr int kGraphSteps = 16;
 
@@ -115,26 +116,28 @@ bool use_part(const bfvm_ctx* c, int axis) {
 
 // The launches of one LOD step on c->stream (also while capturing): the
 // standalone source kernel (unless fused or without agents), then the x, y
-// and z sweeps; per-step timing events when ev is given.
+// and z sweeps; per-step timing events when ev is given (kStepEvents: before
+// the sources, before the x sweep, after it, after y, after z).
 template <typename T>
 int enqueue_step(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, cudaEvent_t* ev) {
   if (ev) BFVM_CUDA(cudaEventRecord(ev[0], c->stream));
   if (standalone) {
-    const int rc = bfvm_apply_sources(c);  // timed with the x sweep
+    const int rc = bfvm_apply_sources(c);
     if (rc != BFVM_OK) return rc;
   }
-  BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, c->stream));
   if (ev) BFVM_CUDA(cudaEventRecord(ev[1], c->stream));
+  BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, c->stream));
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[2], c->stream));
   if (use_part(c, 1))
     BFVM_CUDA((launch_part<T, 1>(c->maps.ry, p, c->part[1], c->stream)));
   else
     BFVM_CUDA(launch_sweep_y<T>(c->maps, p, c->cfg, c->stream));
-  if (ev) BFVM_CUDA(cudaEventRecord(ev[2], c->stream));
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[3], c->stream));
   if (use_part(c, 2))
     BFVM_CUDA((launch_part<T, 2>(c->maps.rz, p, c->part[2], c->stream)));
   else
     BFVM_CUDA(launch_sweep_z<T>(c->maps, p, c->cfg, c->stream));
-  if (ev) BFVM_CUDA(cudaEventRecord(ev[3], c->stream));
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[4], c->stream));
   note_launches(3);
   return BFVM_OK;
 }
@@ -203,13 +206,13 @@ int run_steps_plain(bfvm_ctx* c, int nsteps, bool sources) {
   for (int s = 0; s < nsteps; ++s) {
     cudaEvent_t* ev = nullptr;
     if (c->timing && c->timed_steps < kMaxTimedSteps) {
-      const size_t need = 4 * static_cast<size_t>(c->timed_steps + 1);
+      const size_t need = kStepEvents * static_cast<size_t>(c->timed_steps + 1);
       while (c->events.size() < need) {
         cudaEvent_t e;
         BFVM_CUDA(cudaEventCreate(&e));
         c->events.push_back(e);
       }
-      ev = &c->events[4 * static_cast<size_t>(c->timed_steps)];
+      ev = &c->events[kStepEvents * static_cast<size_t>(c->timed_steps)];
       ++c->timed_steps;
     }
     const int rc = enqueue_step<T>(c, p, standalone, ev);
@@ -1094,22 +1097,33 @@ extern "C" int bfvm_timing_enable(bfvm_ctx* c, int on) {
   return BFVM_OK;
 }
 
-extern "C" int bfvm_timing_read(bfvm_ctx* c, double* ms_xyz, int* steps) {
-  if (!c || !ms_xyz) return BFVM_ERR_ARG;
+extern "C" int bfvm_timing_read_kernels(bfvm_ctx* c, double* ms_sxyz, int* steps) {
+  if (!c || !ms_sxyz) return BFVM_ERR_ARG;
   DeviceGuard g(c->device);
   BFVM_CUDA(cudaStreamSynchronize(c->stream));
-  double acc[3] = {0, 0, 0};
+  double acc[kStepEvents - 1] = {0, 0, 0, 0};
   for (int s = 0; s < c->timed_steps; ++s) {
-    const cudaEvent_t* ev = &c->events[4 * static_cast<size_t>(s)];
-    for (int k = 0; k < 3; ++k) {
+    const cudaEvent_t* ev = &c->events[kStepEvents * static_cast<size_t>(s)];
+    for (int k = 0; k + 1 < kStepEvents; ++k) {
       float ms = 0.f;
       BFVM_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
       acc[k] += ms;
     }
   }
-  for (int k = 0; k < 3; ++k) ms_xyz[k] = acc[k];
+  for (int k = 0; k + 1 < kStepEvents; ++k) ms_sxyz[k] = acc[k];
   if (steps) *steps = c->timed_steps;
   c->timed_steps = 0;
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_timing_read(bfvm_ctx* c, double* ms_xyz, int* steps) {
+  if (!c || !ms_xyz) return BFVM_ERR_ARG;
+  double ms[4];
+  const int rc = bfvm_timing_read_kernels(c, ms, steps);
+  if (rc != BFVM_OK) return rc;
+  ms_xyz[0] = ms[0] + ms[1];  // the sources with the x sweep
+  ms_xyz[1] = ms[2];
+  ms_xyz[2] = ms[3];
   return BFVM_OK;
 }
 

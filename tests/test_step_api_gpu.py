@@ -132,3 +132,24 @@ def test_mass_log_records_every_k_steps_and_checks_fp32():
         if step % 20 == 0:
             np.testing.assert_allclose(a[step // 20 - 1], f.reshape(-1, wl.S).sum(axis=0), rtol=1e-12)
     np.testing.assert_allclose(logs[("fp32", False)], a, rtol=1e-6)
+
+
+def test_per_kernel_timing_records():
+    """bfvm_timing_read_kernels splits each recorded step into the source
+    kernel and the three sweeps; bfvm_timing_read reports the source kernel
+    with the x sweep; both clear the records; the results are unchanged."""
+    wl = W.small_random(613, nx=40, ny=36, nz=30, S=2, n_agents=800, steps=4, stack=True)
+    me = Microenvironment.from_workload(wl)
+    me.timing_enable(True)
+    for _ in range(2):
+        me.simulate_diffusion_decay(1, sources=True)
+    ms, n = me.timing_read_kernels()
+    assert n == 2 and np.all(ms > 0.0)
+    for _ in range(2):
+        me.simulate_diffusion_decay(1, sources=True)
+    xyz, n = me.timing_read()
+    assert n == 2 and np.all(xyz > 0.0)
+    assert me.timing_read_kernels()[1] == 0 and me.timing_read()[1] == 0
+    me.timing_enable(False)
+    np.testing.assert_array_equal(me.download_field(), Port.run(wl))
+    me.close()

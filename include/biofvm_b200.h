@@ -480,12 +480,25 @@ void* bfvm_batch_stream(bfvm_batch* batch);
 /* Schedule of a step.  mode 0: one fused persistent launch per step (tiles
  * of every member and sweep from one ordered work list, per-member
  * dependency counters); mode 1: three launches per step (x, y, z), each over
- * the tiles of every member.  yz_chunk: rows per TMA box in the y/z sweeps;
- * order (mode 0): 0 members as added, 1 largest first; ctas_per_sm (mode 0):
- * 0 = as many as fit; graph_steps: steps per captured CUDA graph. */
+ * the tiles of every member; mode 2: mode 1 for the members under the direct
+ * threshold, the others stepped one after another with their own kernels
+ * (the tensor-memory sweeps of bfvm_step), all on the batch stream and in
+ * its graph.  yz_chunk: rows per TMA box in the y/z sweeps; order (mode 0):
+ * 0 members as added, 1 largest first; ctas_per_sm (mode 0): 0 = as many as
+ * fit; graph_steps: steps per captured CUDA graph.  Every mode gives each
+ * member the bits of bfvm_step. */
 int bfvm_batch_set_schedule(bfvm_batch* batch, int mode, int yz_chunk, int order, int ctas_per_sm, int graph_steps);
 int bfvm_batch_get_schedule(bfvm_batch* batch, int* mode, int* yz_chunk, int* order, int* ctas_per_sm,
                             int* graph_steps);
+/* Mode 2: members of at least `values` voxel-substrate values (nx*ny*nz*S,
+ * default 2097152 = 128^3 x 1) are stepped with their own kernels.
+ * Measured on B200: a mix of 256^3 and 200^3 solves (4 substrates) with 40
+ * small ones steps in 1.23 ms under mode 2 against 2.05 ms under mode 1
+ * (FP64); the serving workload's FP32 server runs at 7.6e10 against 6.8e10
+ * updates/s; 256 uneven solves of edges 24-128 stay faster under mode 1,
+ * where the batched sweeps keep the GPU full across members. */
+int bfvm_batch_set_direct_threshold(bfvm_batch* batch, long long values);
+int bfvm_batch_get_direct_threshold(bfvm_batch* batch, long long* values);
 /* Time trial_steps fused steps under each candidate schedule, keep the
  * fastest, and report its ms per step.  Member fields are restored after
  * the trials. */

@@ -120,6 +120,8 @@ _SIGS = {
     "bfvm_batch_stream": (C.c_void_p, [C.c_void_p]),
     "bfvm_batch_set_schedule": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "bfvm_batch_get_schedule": (C.c_int, [C.c_void_p] + [C.POINTER(C.c_int)] * 5),
+    "bfvm_batch_set_direct_threshold": (C.c_int, [C.c_void_p, C.c_longlong]),
+    "bfvm_batch_get_direct_threshold": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     "bfvm_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "bfvm_batch_inject_stall": (C.c_int, [C.c_void_p, C.c_void_p]),
 }

@@ -59,9 +59,21 @@ class Batch:
 
     def set_schedule(self, mode=0, yz_chunk=32, order=0, ctas_per_sm=0, graph_steps=16):
         """mode 0: one fused persistent launch per step; mode 1: one launch per
-        sweep over every member."""
+        sweep over every member; mode 2: mode 1 for the members under the
+        direct threshold, the others stepped with their own kernels."""
         check(self.L.bfvm_batch_set_schedule(self.h, int(mode), int(yz_chunk), int(order), int(ctas_per_sm),
                                              int(graph_steps)), "bfvm_batch_set_schedule")
+
+    def set_direct_threshold(self, values):
+        """Mode 2: members of at least `values` voxel-substrate values step
+        with their own kernels."""
+        check(self.L.bfvm_batch_set_direct_threshold(self.h, C.c_longlong(int(values))),
+              "bfvm_batch_set_direct_threshold")
+
+    def get_direct_threshold(self):
+        v = C.c_longlong()
+        check(self.L.bfvm_batch_get_direct_threshold(self.h, C.byref(v)), "bfvm_batch_get_direct_threshold")
+        return int(v.value)
 
     def get_schedule(self):
         v = [C.c_int() for _ in range(5)]

@@ -12,7 +12,9 @@ is continuous batching:
   uploaded and it joins the batch;
 * each iteration advances every resident solve by a quantum of LOD steps
   (never past the end of any of them) with one ``bfvm_batch_step`` call --
-  one launch per sweep over all members, replayed from a CUDA graph;
+  by default (batch mode 2) one launch per sweep over the members under
+  2,097,152 voxel-substrate values and the larger ones stepped with their own
+  tensor-memory kernels, all replayed from a CUDA graph;
 * solves that finish in that quantum leave the batch at once and their
   densities are read back while the next quantum already runs, then their
   memory is freed, which admits the next requests;
@@ -145,8 +147,8 @@ class ServeStats:
 class Server:
     """Continuous-batching loop over one GPU (see the module docstring)."""
 
-    def __init__(self, precision="fp32", budget_bytes=None, device=0, quantum=64, sources=True, mode=1,
-                 yz_chunk=32, graph_steps=16):
+    def __init__(self, precision="fp32", budget_bytes=None, device=0, quantum=64, sources=True, mode=2,
+                 yz_chunk=32, graph_steps=16, direct_min=None):
         import torch
 
         self.precision = precision
@@ -159,6 +161,8 @@ class Server:
         self.budget = int(budget_bytes)
         self.batch = Batch(precision, device)
         self.batch.set_schedule(mode=mode, yz_chunk=yz_chunk, graph_steps=graph_steps)
+        if direct_min is not None:
+            self.batch.set_direct_threshold(direct_min)
         self._cancel_lock = threading.Lock()
         self._cancelled = set()
 

@@ -155,13 +155,14 @@ def accuracy(names=("cube50", "cube200", "cube640"), device=0):
     return [single_accuracy(gens[n](), device) for n in names]
 
 
-def serve(n_requests=24, rate=1.0, seed=5, quantum=64, device=0, **request_kw):
+def serve(n_requests=24, rate=1.0, seed=5, quantum=64, device=0, mode=2, direct_min=None, **request_kw):
     """A Poisson stream of requests (serving workload distribution unless
-    overridden) through the FP32 server, then the same stream through the
-    plain FP64 path one request at a time."""
+    overridden) through the FP32 server (batch schedule `mode`, and for mode
+    2 the direct threshold), then the same stream through the plain FP64 path
+    one request at a time."""
     arr = poisson_arrivals(n_requests, rate=rate, seed=seed)
     reqs = [SolveRequest(i, W.serve_request(i, seed=seed, **request_kw), float(arr[i])) for i in range(n_requests)]
-    srv = Server("fp32", quantum=quantum, device=device)
+    srv = Server("fp32", quantum=quantum, device=device, mode=mode, direct_min=direct_min)
     st = srv.run(reqs)
     srv.close()
     base = run_one_at_a_time(reqs, "fp64", device)

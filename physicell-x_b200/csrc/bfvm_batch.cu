@@ -32,7 +32,12 @@ struct bfvm_batch {
   int* d_status = nullptr;
   std::vector<unsigned char> h_envs;
   // schedule
-  int mode = 0;         // 0: one fused persistent launch per step; 1: three launches (x, y, z) per step
+  int mode = 0;         // 0: one fused persistent launch per step; 1: three launches (x, y, z) per step;
+                        // 2: as 1 for the members under direct_min values, the others stepped with
+                        // their own kernels (enqueue_step_on) on the batch stream
+  long long direct_min = 2097152;  // mode 2: N*S (voxel-substrate values) from which a member steps directly
+  std::vector<bfvm_ctx*> direct;  // mode 2: the members stepped directly (set with the tables)
+  int direct_launches = 0;        // their kernels per step
   int yz_chunk = 32;
   int order = 0;        // 0: members in insertion order; 1: largest first
   int ctas_per_sm = 0;  // 0: as many as fit
@@ -100,8 +105,20 @@ int build_tables(bfvm_batch* b, bool sources) {
   const int n = static_cast<int>(b->members.size());
   int rc = ensure_capacity(b, std::max(n, 1));
   if (rc != BFVM_OK) return rc;
-  std::vector<int> idx(n);
-  std::iota(idx.begin(), idx.end(), 0);
+  // mode 2: the large members step with their own kernels, outside the tables
+  std::vector<int> idx;
+  b->direct.clear();
+  b->direct_launches = 0;
+  for (int q = 0; q < n; ++q) {
+    bfvm_ctx* c = b->members[q];
+    if (b->mode == 2 && 1LL * c->nx * c->ny * c->nz * c->S >= b->direct_min) {
+      b->direct.push_back(c);
+      b->direct_launches += 3 + ((sources && c->n_agents > 0 && !c->cfg.fuse_sources) ? 1 : 0);
+    } else {
+      idx.push_back(q);
+    }
+  }
+  const int nb = static_cast<int>(idx.size());
   if (b->order == 1) {
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) {
       const bfvm_ctx* x = b->members[a];
@@ -109,7 +126,7 @@ int build_tables(bfvm_batch* b, bool sources) {
       return 1LL * x->nx * x->ny * x->nz * x->S > 1LL * y->nx * y->ny * y->nz * y->S;
     });
   }
-  std::vector<BatchEnv<T>> envs(n);
+  std::vector<BatchEnv<T>> envs(nb);
   std::vector<int> pre(3 * (b->cap + 1), 0);
   size_t smem = 1024 + 1024;
   size_t axis_smem[3] = {2048, 2048, 2048};
@@ -118,7 +135,7 @@ int build_tables(bfvm_batch* b, bool sources) {
   cfg.x_lines = kBatchTile;
   cfg.yz_tile = kBatchTile;
   cfg.yz_chunk = b->yz_chunk;
-  for (int q = 0; q < n; ++q) {
+  for (int q = 0; q < nb; ++q) {
     bfvm_ctx* c = b->members[idx[q]];
     BatchEnv<T>& E = envs[q];
     std::memset(static_cast<void*>(&E), 0, sizeof(E));
@@ -149,13 +166,14 @@ int build_tables(bfvm_batch* b, bool sources) {
     for (int a = 0; a < 3; ++a)
       axis_smem[a] = std::max(axis_smem[a], batch_axis_smem(c->eb, a, n_line[a], b->yz_chunk));
   }
-  for (int a = 0; a < 3; ++a) pre[a * (b->cap + 1) + n] = items[a];
-  b->env_of.assign(n, 0);
-  for (int q = 0; q < n; ++q) b->env_of[idx[q]] = q;
+  for (int a = 0; a < 3; ++a) pre[a * (b->cap + 1) + nb] = items[a];
+  b->env_of.assign(n, -1);
+  for (int q = 0; q < nb; ++q) b->env_of[idx[q]] = q;
   BatchHeader hdr;
-  hdr.n_env = n;
+  hdr.n_env = nb;
   for (int a = 0; a < 3; ++a) hdr.n_items[a] = items[a];
-  if (n > 0) BFVM_CUDA(cudaMemcpyAsync(b->d_envs, envs.data(), sizeof(BatchEnv<T>) * n, cudaMemcpyHostToDevice, b->stream));
+  if (nb > 0)
+    BFVM_CUDA(cudaMemcpyAsync(b->d_envs, envs.data(), sizeof(BatchEnv<T>) * nb, cudaMemcpyHostToDevice, b->stream));
   BFVM_CUDA(cudaMemcpyAsync(b->d_pre, pre.data(), sizeof(int) * pre.size(), cudaMemcpyHostToDevice, b->stream));
   BFVM_CUDA(cudaMemcpyAsync(b->d_hdr, &hdr, sizeof(hdr), cudaMemcpyHostToDevice, b->stream));
   // the host copies above must stay alive until the copies ran
@@ -175,6 +193,7 @@ int build_tables(bfvm_batch* b, bool sources) {
   b->smem = smem;
   b->grid = grid;
   b->built_sources = sources;
+  drop_graph(b);  // the direct members' launches live in the graph too
   return BFVM_OK;
 }
 
@@ -184,9 +203,14 @@ int build_tables(bfvm_batch* b, bool sources) {
 // tiles that never count up and their bounded waits run out.
 template <typename T>
 cudaError_t enqueue_step(bfvm_batch* b, int stall_env = -1) {
-  if (b->mode == 1)
-    return launch_batch_sweeps<T>(b->d_hdr, static_cast<const BatchEnv<T>*>(b->d_envs), b->d_pre, b->cap, b->items,
-                                  b->axis_smem, b->stream);
+  if (b->mode >= 1) {
+    cudaError_t e = launch_batch_sweeps<T>(b->d_hdr, static_cast<const BatchEnv<T>*>(b->d_envs), b->d_pre, b->cap,
+                                           b->items, b->axis_smem, b->stream);
+    if (e != cudaSuccess) return e;
+    for (bfvm_ctx* c : b->direct)
+      if (enqueue_step_on(c, b->built_sources, b->stream) != BFVM_OK) return cudaErrorLaunchFailure;
+    return cudaSuccess;
+  }
   cudaError_t e = cudaMemsetAsync(b->d_counters, 0, sizeof(int) * (1 + 3 * b->cap), b->stream);
   if (e != cudaSuccess) return e;
   if (stall_env >= 0) {
@@ -197,6 +221,8 @@ cudaError_t enqueue_step(bfvm_batch* b, int stall_env = -1) {
                               b->d_status, b->grid, b->smem, b->stream);
 }
 
+// The batched kernels of one step (the directly stepped members count their
+// own launches as they enqueue them).
 int kernels_per_step(const bfvm_batch* b) {
   if (b->mode == 0) return 1;
   return (b->items[0] > 0) + (b->items[1] > 0) + (b->items[2] > 0);
@@ -206,7 +232,7 @@ template <typename T>
 int launch_one(bfvm_batch* b, int stall_env = -1) {
   BFVM_CUDA(enqueue_step<T>(b, stall_env));
   note_launches(kernels_per_step(b));
-  b->launches += kernels_per_step(b);
+  b->launches += kernels_per_step(b) + b->direct_launches;
   return BFVM_OK;
 }
 
@@ -215,15 +241,18 @@ int capture_graph(bfvm_batch* b) {
   drop_graph(b);
   cudaGraph_t g = nullptr;
   BFVM_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  set_launch_capture(true);  // the replays count the launches
   for (int s = 0; s < b->graph_steps; ++s) {
     const cudaError_t e2 = enqueue_step<T>(b);
     if (e2 != cudaSuccess) {
+      set_launch_capture(false);
       cudaStreamEndCapture(b->stream, &g);
       if (g) cudaGraphDestroy(g);
       cudaGetLastError();
       return BFVM_ERR_CUDA;
     }
   }
+  set_launch_capture(false);
   BFVM_CUDA(cudaStreamEndCapture(b->stream, &g));
   cudaError_t e = cudaGraphInstantiate(&b->gexec, g, 0);
   cudaGraphDestroy(g);
@@ -289,8 +318,8 @@ int step_impl(bfvm_batch* b, int nsteps, bool sources) {
     }
     while (left >= b->g_steps) {
       BFVM_CUDA(cudaGraphLaunch(b->gexec, b->stream));
-      note_launches(b->g_steps * kernels_per_step(b));
-      b->launches += b->g_steps * kernels_per_step(b);
+      note_launches(b->g_steps * (kernels_per_step(b) + b->direct_launches));
+      b->launches += b->g_steps * (kernels_per_step(b) + b->direct_launches);
       left -= b->g_steps;
     }
   }
@@ -407,7 +436,7 @@ int bfvm_batch_inject_stall(bfvm_batch* b, bfvm_ctx* c) {
 }
 
 int bfvm_batch_set_schedule(bfvm_batch* b, int mode, int yz_chunk, int order, int ctas_per_sm, int graph_steps) {
-  if (!b || mode < 0 || mode > 1 || yz_chunk < 1 || yz_chunk > 256 || order < 0 || order > 1 || ctas_per_sm < 0 ||
+  if (!b || mode < 0 || mode > 2 || yz_chunk < 1 || yz_chunk > 256 || order < 0 || order > 1 || ctas_per_sm < 0 ||
       graph_steps < 1 || graph_steps > 1024)
     return BFVM_ERR_ARG;
   for (bfvm_ctx* c : b->members)
@@ -419,6 +448,22 @@ int bfvm_batch_set_schedule(bfvm_batch* b, int mode, int yz_chunk, int order, in
   b->graph_steps = graph_steps;
   b->dirty = true;
   drop_graph(b);
+  return BFVM_OK;
+}
+
+int bfvm_batch_set_direct_threshold(bfvm_batch* b, long long values) {
+  if (!b || values < 1) return BFVM_ERR_ARG;
+  if (values != b->direct_min) {
+    b->direct_min = values;
+    b->dirty = true;
+    drop_graph(b);
+  }
+  return BFVM_OK;
+}
+
+int bfvm_batch_get_direct_threshold(bfvm_batch* b, long long* values) {
+  if (!b || !values) return BFVM_ERR_ARG;
+  *values = b->direct_min;
   return BFVM_OK;
 }
 
@@ -463,20 +508,26 @@ int bfvm_batch_autotune(bfvm_batch* b, int flags, int trial_steps, double* best_
   }
   struct Cand {
     int mode, yz_chunk, order, ctas;
+    long long direct_min;
   };
   std::vector<Cand> cands;
   for (int ch : {16, 32, 64}) {
-    cands.push_back({1, ch, 0, 0});
+    cands.push_back({1, ch, 0, 0, b->direct_min});
     for (int ord : {0, 1})
-      for (int ctas : {0, 8, 4}) cands.push_back({0, ch, ord, ctas});
+      for (int ctas : {0, 8, 4}) cands.push_back({0, ch, ord, ctas, b->direct_min});
   }
+  // mode 2: members from 32^3, 64^3 or 128^3 voxel-substrate values step directly
+  for (long long dm : {32768LL, 262144LL, 2097152LL})
+    for (int ch : {32, 64}) cands.push_back({2, ch, 0, 0, dm});
   const int keep_graph = b->graph_steps;
+  const long long keep_direct = b->direct_min;
   double best = 1e30;
-  Cand best_c{b->mode, b->yz_chunk, b->order, b->ctas_per_sm};
+  Cand best_c{b->mode, b->yz_chunk, b->order, b->ctas_per_sm, b->direct_min};
   cudaEvent_t e0, e1;
   BFVM_CUDA(cudaEventCreate(&e0));
   BFVM_CUDA(cudaEventCreate(&e1));
   for (const Cand& cd : cands) {
+    b->direct_min = cd.direct_min;
     if (bfvm_batch_set_schedule(b, cd.mode, cd.yz_chunk, cd.order, cd.ctas, 1) != BFVM_OK) continue;
     if ((rc = bfvm_batch_step(b, 1, flags)) != BFVM_OK) break;  // warm-up (also builds the tables)
     cudaEventRecord(e0, b->stream);
@@ -503,7 +554,11 @@ int bfvm_batch_autotune(bfvm_batch* b, int flags, int trial_steps, double* best_
   cudaStreamSynchronize(b->stream);
   for (void* p : saved) cudaFree(p);
   release_members(b);
-  if (rc != BFVM_OK) return rc;
+  if (rc != BFVM_OK) {
+    b->direct_min = keep_direct;
+    return rc;
+  }
+  b->direct_min = best_c.direct_min;
   bfvm_batch_set_schedule(b, best_c.mode, best_c.yz_chunk, best_c.order, best_c.ctas, keep_graph);
   if (best_ms_per_step) *best_ms_per_step = best;
   return BFVM_OK;

@@ -22,6 +22,7 @@ static std::atomic<long long> g_launches{0};
 // Set while this thread captures a CUDA graph: captured launches are counted
 // when the graph is launched, not when they are recorded.
 static thread_local bool t_capturing = false;
+void set_launch_capture(bool on) { t_capturing = on; }
 void note_launches(int n) {
   if (!t_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
 }
@@ -119,25 +120,27 @@ bool use_part(const bfvm_ctx* c, int axis) {
 // and z sweeps; per-step timing events when ev is given (kStepEvents: before
 // the sources, before the x sweep, after it, after y, after z).
 template <typename T>
-int enqueue_step(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, cudaEvent_t* ev) {
-  if (ev) BFVM_CUDA(cudaEventRecord(ev[0], c->stream));
+int enqueue_step(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, cudaEvent_t* ev,
+                 cudaStream_t st = nullptr) {
+  if (st == nullptr) st = c->stream;
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[0], st));
   if (standalone) {
-    const int rc = bfvm_apply_sources(c);
+    const int rc = apply_sources_on(c, st);
     if (rc != BFVM_OK) return rc;
   }
-  if (ev) BFVM_CUDA(cudaEventRecord(ev[1], c->stream));
-  BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, c->stream));
-  if (ev) BFVM_CUDA(cudaEventRecord(ev[2], c->stream));
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[1], st));
+  BFVM_CUDA(launch_sweep_x<T>(c->maps, p, c->cfg, st));
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[2], st));
   if (use_part(c, 1))
-    BFVM_CUDA((launch_part<T, 1>(c->maps.ry, p, c->part[1], c->stream)));
+    BFVM_CUDA((launch_part<T, 1>(c->maps.ry, p, c->part[1], st)));
   else
-    BFVM_CUDA(launch_sweep_y<T>(c->maps, p, c->cfg, c->stream));
-  if (ev) BFVM_CUDA(cudaEventRecord(ev[3], c->stream));
+    BFVM_CUDA(launch_sweep_y<T>(c->maps, p, c->cfg, st));
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[3], st));
   if (use_part(c, 2))
-    BFVM_CUDA((launch_part<T, 2>(c->maps.rz, p, c->part[2], c->stream)));
+    BFVM_CUDA((launch_part<T, 2>(c->maps.rz, p, c->part[2], st)));
   else
-    BFVM_CUDA(launch_sweep_z<T>(c->maps, p, c->cfg, c->stream));
-  if (ev) BFVM_CUDA(cudaEventRecord(ev[4], c->stream));
+    BFVM_CUDA(launch_sweep_z<T>(c->maps, p, c->cfg, st));
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[4], st));
   note_launches(3);
   return BFVM_OK;
 }
@@ -966,19 +969,9 @@ int bfvm_step(bfvm_ctx* c, int nsteps, int flags) {
 int bfvm_apply_sources(bfvm_ctx* c) {
   if (!c) return BFVM_ERR_ARG;
   DeviceGuard g(c->device);
-  if (c->n_agents == 0) return BFVM_OK;
-  const size_t SN = static_cast<size_t>(c->S) * c->n_agents;
-  if (c->prec == BFVM_FP64)
-    BFVM_CUDA(agents_apply_sources<double>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
-                                           c->d_ac + SN, c->d_ac + 2 * SN, nullptr, static_cast<double*>(c->f),
-                                           track_params(c), c->stream));
-  else
-    BFVM_CUDA(agents_apply_sources<float>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
-                                          c->d_ac + SN, c->d_ac + 2 * SN, c->d_off, static_cast<float*>(c->f),
-                                          track_params(c), c->stream));
-  note_launches(1);
-  return BFVM_OK;
+  return bfvm::apply_sources_on(c, c->stream);
 }
+
 
 int bfvm_sample_agents(bfvm_ctx* c, double* out) {
   if (!c || (!out && c->n_agents > 0)) return BFVM_ERR_ARG;
@@ -1336,3 +1329,29 @@ extern "C" int bfvm_set_launch(bfvm_ctx* c, int x_lines, int yz_tile, int yz_chu
   c->cfg = cfg;
   return BFVM_OK;
 }
+
+namespace bfvm {
+
+int apply_sources_on(bfvm_ctx* c, cudaStream_t st) {
+  if (c->n_agents == 0) return BFVM_OK;
+  const size_t SN = static_cast<size_t>(c->S) * c->n_agents;
+  if (c->prec == BFVM_FP64)
+    BFVM_CUDA(agents_apply_sources<double>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
+                                           c->d_ac + SN, c->d_ac + 2 * SN, nullptr, static_cast<double*>(c->f),
+                                           track_params(c), st));
+  else
+    BFVM_CUDA(agents_apply_sources<float>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
+                                          c->d_ac + SN, c->d_ac + 2 * SN, c->d_off, static_cast<float*>(c->f),
+                                          track_params(c), st));
+  note_launches(1);
+  return BFVM_OK;
+}
+
+int enqueue_step_on(bfvm_ctx* c, bool sources, cudaStream_t st) {
+  const bool standalone = sources && c->n_agents > 0 && !c->cfg.fuse_sources;
+  if (c->prec == BFVM_FP64)
+    return enqueue_step<double>(c, make_params<double>(c, sources && !standalone), standalone, nullptr, st);
+  return enqueue_step<float>(c, make_params<float>(c, sources && !standalone), standalone, nullptr, st);
+}
+
+}  // namespace bfvm

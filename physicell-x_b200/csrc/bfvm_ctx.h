@@ -138,6 +138,14 @@ int update_shift_2d(bfvm_ctx* c);
 // bfvm_mass.cu: one mass-balance record of the current field, enqueued on
 // the solve's stream.
 int enqueue_mass_record(bfvm_ctx* c);
+// The standalone source kernel of the solve's agents on stream st
+// (bfvm_apply_sources on the solve's own stream).
+int apply_sources_on(bfvm_ctx* c, cudaStream_t st);
+// One LOD step of the solve (sources when asked, then the x, y and z sweeps,
+// with the solve's own kernels and settings) enqueued on stream st, as
+// bfvm_step launches it; used by the batched engine for members it steps
+// with their own kernels.
+int enqueue_step_on(bfvm_ctx* c, bool sources, cudaStream_t st);
 
 // bfvm_capi.cu: Thomas factorization of one axis (half: 2-D constants).
 void thomas_axis_host(int n, int S, const double* D, const double* decay, double dt, double dx, double* denom,

@@ -188,6 +188,9 @@ struct FieldMaps {
 
 // Host-side count of this library's kernel launches (bfvm_kernel_launches).
 void note_launches(int n);
+// While on, note_launches counts nothing (launches being captured into a
+// graph are counted when the graph is replayed).
+void set_launch_capture(bool on);
 
 int encode_field_maps(FieldMaps* maps, void* f, int elem_bytes, int nx, int ny, int nz, int S, int nxp,
                       const SweepConfig& cfg);

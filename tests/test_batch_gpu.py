@@ -23,11 +23,17 @@ def _envs(n, seed, steps, agents_hi=300, edge_lo=3, edge_hi=40):
     return out
 
 
-@pytest.mark.parametrize("mode,graph_steps", [(0, 1), (0, 4), (1, 1), (1, 4)])
+# mode 2 with a threshold of 5000 voxel-substrate values: the larger members
+# step with their own kernels, the rest through the batched sweeps
+DIRECT_TEST = 5000
+
+
+@pytest.mark.parametrize("mode,graph_steps", [(0, 1), (0, 4), (1, 1), (1, 4), (2, 1), (2, 4)])
 def test_batch_fp64_members_match_oracle_bitwise(mode, graph_steps):
     wls = _envs(12, 7, steps=9)
     batch = Batch("fp64")
     batch.set_schedule(mode=mode, graph_steps=graph_steps)
+    batch.set_direct_threshold(DIRECT_TEST)
     mes = []
     for wl in wls:
         me = Microenvironment.from_workload(wl)
@@ -39,9 +45,12 @@ def test_batch_fp64_members_match_oracle_bitwise(mode, graph_steps):
         assert np.array_equal(me.download_field(), Port.run(wl)), wl.name
 
 
-def test_batch_fp32_equals_single_fp32_bitwise():
+@pytest.mark.parametrize("mode", [0, 2])
+def test_batch_fp32_equals_single_fp32_bitwise(mode):
     wls = _envs(8, 8, steps=6)
     batch = Batch("fp32")
+    batch.set_schedule(mode=mode, graph_steps=4)
+    batch.set_direct_threshold(DIRECT_TEST)
     singles, mes = [], []
     for wl in wls:
         me = Microenvironment.from_workload(wl, precision="fp32")
@@ -55,13 +64,14 @@ def test_batch_fp32_equals_single_fp32_bitwise():
         assert np.array_equal(me.download_field(), ref)
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2])
 def test_batch_membership_changes_between_steps(mode):
     """Members join and leave between steps (continuous batching); each still
     ends bit-identical to its solo run."""
     wls = _envs(6, 9, steps=8)
     batch = Batch("fp64")
     batch.set_schedule(mode=mode, graph_steps=2)
+    batch.set_direct_threshold(DIRECT_TEST)
     mes = [Microenvironment.from_workload(wl) for wl in wls]
     done = {}
     for me in mes[:3]:
@@ -115,3 +125,29 @@ def test_uneven_batch_slice_runs():
         solo = Microenvironment.from_workload(wl)
         solo.simulate_diffusion_decay(3, sources=True)
         assert np.array_equal(me.download_field(), solo.download_field())
+
+
+def test_batch_direct_members_count_their_launches():
+    """Mode 2: the launch counter counts the directly stepped members' kernels
+    once per step, whether launched one step at a time or replayed from the
+    batch's graph."""
+    from bfvm import kernel_launches
+
+    wls = [W.small_random(9100 + i, nx=24 + 8 * i, ny=20 + 8 * i, nz=18 + 8 * i, S=2, n_agents=300, steps=1)
+           for i in range(3)]
+    batch = Batch("fp64")
+    batch.set_schedule(mode=2, graph_steps=4)
+    batch.set_direct_threshold(20000)  # the two larger members step directly
+    mes = [Microenvironment.from_workload(wl) for wl in wls]
+    for me in mes:
+        batch.add(me)
+    assert batch.get_direct_threshold() == 20000
+    batch.step(1, sources=True)
+    batch.synchronize()
+    per_step = 3 + 2 * 4  # three batched sweeps, two members x (sources + 3 sweeps)
+    for n in (1, 8):
+        before = kernel_launches()
+        batch.step(n, sources=True)
+        batch.synchronize()
+        assert kernel_launches() - before == n * per_step
+    batch.close()

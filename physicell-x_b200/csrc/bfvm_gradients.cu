@@ -168,6 +168,7 @@ __global__ void __launch_bounds__(256, 3) gradient_plane_kernel(const __grid_con
   const double hx = (x_lo || x_hi) ? dx : two_dx, rhx = (x_lo || x_hi) ? rdx : r2dx;
   const double hz = (z_lo || z_hi) ? dx : two_dx, rhz = (z_lo || z_hi) ? rdx : r2dx;
   const bool zero_x = nx == 1, zero_y = ny == 1, zero_z = nz == 1;
+  const bool any_zero_axis = zero_x || zero_y || zero_z;
   for (int j = jb; j < je; ++j) {
     if (j == jb) wait_plane(j);
     if (j + 1 < ny) wait_plane(j + 1);
@@ -210,11 +211,13 @@ __global__ void __launch_bounds__(256, 3) gradient_plane_kernel(const __grid_con
           g3[3 * sl + 2] = grad_exact(v(P1, c + ozp, o), v(P1, c - ozm, o), hz, rhz);
         }
       }
+      if (any_zero_axis) {  // uniform: grids with an axis of length 1 only
 #pragma unroll
-      for (int sl = 0; sl < NS; ++sl) {
-        if (zero_x) g3[3 * sl + 0] = 0.0;
-        if (zero_y) g3[3 * sl + 1] = 0.0;
-        if (zero_z) g3[3 * sl + 2] = 0.0;
+        for (int sl = 0; sl < NS; ++sl) {
+          if (zero_x) g3[3 * sl + 0] = 0.0;
+          if (zero_y) g3[3 * sl + 1] = 0.0;
+          if (zero_z) g3[3 * sl + 2] = 0.0;
+        }
       }
       double* o3 = stg + lane * SX + wz * 3 * NS;
       if constexpr ((NS & 1) == 0) {

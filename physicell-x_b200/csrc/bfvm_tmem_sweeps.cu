@@ -581,11 +581,12 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
       if (!edge || lane_on) {
         double v[W];
         load_row<double, W>(crow, sw, v);
-        if (act) {  // the pin before the sweep
+        if (act) {  // the pin before the sweep (uniform tests: the line's first and last chunk)
+          if (i0 == 0) v[0] = x0v;
+          if (nx - 1 < i0 + W) {
 #pragma unroll
-          for (int q = 0; q < W; ++q) {
-            if (i0 + q == 0) v[q] = x0v;
-            if (i0 + q == nx - 1) v[q] = x1v;
+            for (int q = 0; q < W; ++q)
+              if (i0 + q == nx - 1) v[q] = x1v;
           }
         }
         if (i0 + W > nx) {  // TMA fill past the line's end: any clean value, never stored
@@ -730,10 +731,11 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
           }
         }
         if (act) {  // the pin after the sweep
+          if (i0 == 0) v[0] = x0v;
+          if (nx - 1 < i0 + W) {
 #pragma unroll
-          for (int q = 0; q < W; ++q) {
-            if (i0 + q == 0) v[q] = x0v;
-            if (i0 + q == nx - 1) v[q] = x1v;
+            for (int q = 0; q < W; ++q)
+              if (i0 + q == nx - 1) v[q] = x1v;
           }
         }
       }

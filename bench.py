@@ -79,6 +79,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--substrate-streams", type=int, choices=[1, 2], default=2,
+                    help="bfvm_set_substrate_streams of the timed solve: 2 (default) sweeps the two halves of the "
+                         "substrates on two streams, 1 in one sequence of launches")
     ap.add_argument("--fp64-chain", type=int, choices=[0, 1, 2], default=0,
                     help="arithmetic of the timed solve (bfvm_set_fp64_chain): 0 the reference's (default)")
     ap.add_argument("--workload", choices=["cube200", "uneven_batch", "serve", "accuracy"], default="cube200",
@@ -386,6 +389,7 @@ def main():
     wl = W.cube200()
     me = Microenvironment.from_workload(wl, precision=args.precision, device=local)
     me.set_fp64_chain(args.fp64_chain)
+    me.set_substrate_streams(args.substrate_streams)
     stream = torch.cuda.ExternalStream(me.stream, device=torch.device("cuda", local))
     N, S, A = wl.n_voxels, wl.S, wl.n_agents
 
@@ -550,7 +554,8 @@ def main():
                                "the reference's arithmetic (bit-identical)", f"arithmetic chain {args.fp64_chain}"),
                            "parallelism": f"replicas x{world}",
                            "l2": "inputs larger than L2 (256 MB field per GPU), no flush",
-                           "voxels": N, "substrates": S, "agents": A},
+                           "voxels": N, "substrates": S, "agents": A,
+                           "substrate_streams": args.substrate_streams},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "fp64_short_chain": short,
                 "gradients": gradients,
                 "gpu_launches": launches, "clocks": clk.summary()}

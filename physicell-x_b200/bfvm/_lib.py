@@ -66,6 +66,8 @@ _SIGS = {
     "bfvm_sample_agents": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bfvm_set_sweep_schedule": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_set_fused_sources": (C.c_int, [C.c_void_p, C.c_int]),
+    "bfvm_set_substrate_streams": (C.c_int, [C.c_void_p, C.c_int]),
+    "bfvm_get_substrate_streams": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "bfvm_set_sweep_tmem": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_set_fp64_chain": (C.c_int, [C.c_void_p, C.c_int]),
     "bfvm_get_fp64_chain": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),

@@ -350,6 +350,17 @@ class Microenvironment:
         source kernel ahead of the sweeps (False, the default)."""
         check(self.L.bfvm_set_fused_sources(self.h, 1 if fused else 0), "bfvm_set_fused_sources")
 
+    def set_substrate_streams(self, streams=2):
+        """Runs of steps sweep the two halves of the substrates on two streams
+        (2, the default) or every substrate in one sequence of launches (1);
+        the same bits either way."""
+        check(self.L.bfvm_set_substrate_streams(self.h, int(streams)), "bfvm_set_substrate_streams")
+
+    def substrate_streams(self):
+        v = C.c_int(0)
+        check(self.L.bfvm_get_substrate_streams(self.h, C.byref(v)), "bfvm_get_substrate_streams")
+        return v.value
+
     def set_sweep_tmem(self, level=1):
         """Tensor-memory rings in the FP64 persistent sweeps: 1 (the default)
         in the y/z sweeps, 2 in the x sweep as well, 0 (or False) none; same

@@ -199,10 +199,10 @@ template <typename T>
 __global__ void agent_sources_kernel(int n, const unsigned* __restrict__ sk, unsigned sentinel, int S, int nx, int ny,
                                      int nz, int nxp, const double* __restrict__ ac1, const double* __restrict__ ac2,
                                      const double* __restrict__ ae2, const double* __restrict__ off,
-                                     T* __restrict__ f, const AgentTrack tr) {
+                                     T* __restrict__ f, const AgentTrack tr, int s_lo, int s_hi) {
   const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (idx >= static_cast<long long>(n) * S) return;
-  const int s = static_cast<int>(idx / n);
+  if (idx >= static_cast<long long>(n) * (s_hi - s_lo)) return;
+  const int s = s_lo + static_cast<int>(idx / n);
   const int p = static_cast<int>(idx % n);
   const unsigned key = sk[p];
   if (key >= sentinel) return;
@@ -448,12 +448,14 @@ template cudaError_t agents_apply_sources_by_order<float>(int, const unsigned*, 
 template <typename T>
 cudaError_t agents_apply_sources(int n, const unsigned* sorted_keys, int S, int nx, int ny, int nz, int nxp,
                                  const double* ac1, const double* ac2, const double* ae2, const double* off, T* f,
-                                 const AgentTrack& track, cudaStream_t st) {
+                                 const AgentTrack& track, cudaStream_t st, int s_lo, int s_hi) {
   if (n == 0) return cudaSuccess;
+  if (s_hi < 0) s_hi = S;
+  if (s_lo < 0 || s_lo >= s_hi || s_hi > S) return cudaErrorInvalidValue;
   const unsigned sentinel = static_cast<unsigned>(nx) * ny * nz;
-  const long long total = static_cast<long long>(n) * S;
+  const long long total = static_cast<long long>(n) * (s_hi - s_lo);
   agent_sources_kernel<T><<<static_cast<unsigned>((total + 255) / 256), 256, 0, st>>>(
-      n, sorted_keys, sentinel, S, nx, ny, nz, nxp, ac1, ac2, ae2, off, f, track);
+      n, sorted_keys, sentinel, S, nx, ny, nz, nxp, ac1, ac2, ae2, off, f, track, s_lo, s_hi);
   return cudaGetLastError();
 }
 
@@ -490,10 +492,10 @@ cudaError_t agents_sample(int n, const unsigned* dev_voxel, int S, int nx, int n
 
 template cudaError_t agents_apply_sources<double>(int, const unsigned*, int, int, int, int, int, const double*,
                                                   const double*, const double*, const double*, double*,
-                                                  const AgentTrack&, cudaStream_t);
+                                                  const AgentTrack&, cudaStream_t, int, int);
 template cudaError_t agents_apply_sources<float>(int, const unsigned*, int, int, int, int, int, const double*,
                                                  const double*, const double*, const double*, float*,
-                                                 const AgentTrack&, cudaStream_t);
+                                                 const AgentTrack&, cudaStream_t, int, int);
 template cudaError_t agents_sample<double>(int, const unsigned*, int, int, int, int, int, const double*,
                                            const double*, double*, cudaStream_t);
 template cudaError_t agents_sample<float>(int, const unsigned*, int, int, int, int, int, const float*, const double*,

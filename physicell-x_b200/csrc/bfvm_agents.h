@@ -71,10 +71,11 @@ cudaError_t agents_apply_sources_by_order(int n, const unsigned* sorted_keys, co
 
 // off: [S] field offsets of an FP32 solve (the field holds rho - off), or null.
 // track: internalized-substrate tracking (track.internal null: off).
+// Substrates s_lo .. s_hi - 1 only (s_hi < 0: through S - 1).
 template <typename T>
 cudaError_t agents_apply_sources(int n, const unsigned* sorted_keys, int S, int nx, int ny, int nz, int nxp,
                                  const double* ac1, const double* ac2, const double* ae2, const double* off, T* f,
-                                 const AgentTrack& track, cudaStream_t st);
+                                 const AgentTrack& track, cudaStream_t st, int s_lo = 0, int s_hi = -1);
 
 // dst[s*n + p] = src[order[p]*S + s]: a per-agent [n][S] array in list order
 // gathered into the sorted, substrate-major layout of ac1/ac2/ae2.

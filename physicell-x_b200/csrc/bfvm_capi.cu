@@ -96,7 +96,7 @@ int part_min_line(const bfvm_ctx* c) {
 // launch shapes from the sweep configuration.
 std::vector<long long> step_key(const bfvm_ctx* c, bool sources) {
   const SweepConfig& g = c->cfg;
-  return {c->version, sources ? 1 : 0, c->n_agents, c->track, g.x_lines, g.yz_tile, g.yz_chunk, g.persistent,
+  return {c->version, sources ? 1 : 0, c->n_agents, c->track, c->sub_streams, g.x_lines, g.yz_tile, g.yz_chunk, g.persistent,
           g.fuse_sources, g.tmem, part_min_line(c), static_cast<long long>(reinterpret_cast<uintptr_t>(c->d_internal)),
           static_cast<long long>(reinterpret_cast<uintptr_t>(c->d_ae1))};
 }
@@ -117,15 +117,16 @@ bool use_part(const bfvm_ctx* c, int axis) {
 
 // The launches of one LOD step on c->stream (also while capturing): the
 // standalone source kernel (unless fused or without agents), then the x, y
-// and z sweeps; per-step timing events when ev is given (kStepEvents: before
-// the sources, before the x sweep, after it, after y, after z).
+// and z sweeps, over the substrates [p.s_lo, p.s_hi); per-step timing events
+// when ev is given (kStepEvents: before the sources, before the x sweep,
+// after it, after y, after z).
 template <typename T>
 int enqueue_step(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, cudaEvent_t* ev,
                  cudaStream_t st = nullptr) {
   if (st == nullptr) st = c->stream;
   if (ev) BFVM_CUDA(cudaEventRecord(ev[0], st));
   if (standalone) {
-    const int rc = apply_sources_on(c, st);
+    const int rc = apply_sources_on(c, st, p.s_lo, p.s_hi);
     if (rc != BFVM_OK) return rc;
   }
   if (ev) BFVM_CUDA(cudaEventRecord(ev[1], st));
@@ -145,6 +146,44 @@ int enqueue_step(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, cudaEven
   return BFVM_OK;
 }
 
+// Whether runs of steps split the substrates into two groups on two streams.
+// Every launch of a step touches only its own substrates (the sources, the
+// sweeps, their pins), so the two groups are independent problems; each
+// persistent sweep leaves SMs idle while its last tiles finish, and the
+// other group's kernels take them.  Not while timing single kernels.
+bool use_groups(const bfvm_ctx* c) { return c->sub_streams == 2 && c->S >= 2 && !c->timing; }
+
+// nsteps LOD steps on c->stream: one group, or the substrates [0, h) on
+// c->stream and [h, S) on c->group_stream (its own tile counter), forked and
+// joined around the whole run so that neither group waits on the other.
+template <typename T>
+int enqueue_steps(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, int nsteps) {
+  if (nsteps <= 0) return BFVM_OK;
+  if (!use_groups(c)) {
+    for (int s = 0; s < nsteps; ++s) {
+      const int rc = enqueue_step<T>(c, p, standalone, nullptr);
+      if (rc != BFVM_OK) return rc;
+    }
+    return BFVM_OK;
+  }
+  const int h = (c->S + 1) / 2;
+  SweepParams<T> pa = p, pb = p;
+  pa.s_lo = 0;
+  pa.s_hi = h;
+  pb.s_lo = h;
+  pb.s_hi = c->S;
+  pb.tile_counter = c->d_tile_counter + 2;
+  BFVM_CUDA(cudaEventRecord(c->ev_gfork, c->stream));
+  BFVM_CUDA(cudaStreamWaitEvent(c->group_stream, c->ev_gfork, 0));
+  int rc = BFVM_OK;
+  for (int s = 0; s < nsteps && rc == BFVM_OK; ++s) rc = enqueue_step<T>(c, pa, standalone, nullptr, c->stream);
+  for (int s = 0; s < nsteps && rc == BFVM_OK; ++s) rc = enqueue_step<T>(c, pb, standalone, nullptr, c->group_stream);
+  // joined even after a failed launch, so that a capture can end
+  BFVM_CUDA(cudaEventRecord(c->ev_gjoin, c->group_stream));
+  BFVM_CUDA(cudaStreamWaitEvent(c->stream, c->ev_gjoin, 0));
+  return rc;
+}
+
 // Capture kGraphSteps steps into c->step_graph.  The caller has run at least
 // one step uncaptured since the key last changed, so every host-side set-up
 // of the launches (kernel attributes, occupancy lookups) is cached already.
@@ -154,8 +193,8 @@ int capture_step_graph(bfvm_ctx* c, const SweepParams<T>& p, bool standalone, co
   cudaGraph_t g = nullptr;
   BFVM_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   t_capturing = true;
-  for (int s = 0; s < kGraphSteps; ++s) {
-    const int rc = enqueue_step<T>(c, p, standalone, nullptr);
+  {
+    const int rc = enqueue_steps<T>(c, p, standalone, kGraphSteps);
     if (rc != BFVM_OK) {
       t_capturing = false;
       cudaStreamEndCapture(c->stream, &g);
@@ -190,22 +229,19 @@ int run_steps_plain(bfvm_ctx* c, int nsteps, bool sources) {
     const std::vector<long long> key = step_key(c, sources);
     int left = nsteps;
     if (c->step_graph == nullptr || c->graph_key != key) {
-      int rc = enqueue_step<T>(c, p, standalone, nullptr);  // the uncaptured warm step
+      int rc = enqueue_steps<T>(c, p, standalone, 1);  // the uncaptured warm step
       if (rc != BFVM_OK) return rc;
       --left;
       if ((rc = capture_step_graph<T>(c, p, standalone, key)) != BFVM_OK) return rc;
     }
-    const int per_step = 3 + (standalone ? 1 : 0);
+    const int per_step = (3 + (standalone ? 1 : 0)) * (use_groups(c) ? 2 : 1);
     for (; left >= kGraphSteps; left -= kGraphSteps) {
       BFVM_CUDA(cudaGraphLaunch(c->step_graph, c->stream));
       note_launches(kGraphSteps * per_step);
     }
-    for (; left > 0; --left) {
-      const int rc = enqueue_step<T>(c, p, standalone, nullptr);
-      if (rc != BFVM_OK) return rc;
-    }
-    return BFVM_OK;
+    return enqueue_steps<T>(c, p, standalone, left);
   }
+  if (!c->timing) return enqueue_steps<T>(c, p, standalone, nsteps);
   for (int s = 0; s < nsteps; ++s) {
     cudaEvent_t* ev = nullptr;
     if (c->timing && c->timed_steps < kMaxTimedSteps) {
@@ -273,7 +309,7 @@ bool pick_config(int eb, int nx, int ny, int nz, SweepConfig* cfg) {
 // Coefficient storage of one precision: sizes of the DR/CU rows and the
 // host-side packing (padding entries are neutral: a unit denominator and a
 // -0 upper diagonal).
-size_t coef_bytes(const bfvm_ctx* c, size_t* dr_off, size_t* cu_off) {
+size_t coef_bytes(const bfvm_ctx* c, size_t* dr_off, size_t* cu_off, size_t* conv_off = nullptr) {
   const size_t S = c->S;
   const size_t dr_sz = c->prec == BFVM_FP64 ? sizeof(double2) : sizeof(double);
   const size_t cu_sz = sizeof(double);
@@ -288,7 +324,30 @@ size_t coef_bytes(const bfvm_ctx* c, size_t* dr_off, size_t* cu_off) {
     o += rows * cu_sz;
     o = (o + 255) & ~size_t(255);
   }
-  return o;
+  // each axis's first converged index per substrate (AxisCoefs::conv)
+  for (int a = 0; a < 3; ++a) {
+    if (conv_off) conv_off[a] = o;
+    o += S * sizeof(int);
+  }
+  return (o + 255) & ~size_t(255);
+}
+
+// The first index from which a factorized row is constant: the constant-
+// coefficient factorization d_i = fma(c1, c_{i-1}, k3), c_i = -c1 / d_i is a
+// contraction that reaches a fixed point in FP64 after a few to a few dozen
+// entries (4 for D dt/dx^2 = 0.01, 57 for 10), after which every entry up to
+// the line's second-to-last is bit-identical.  Returns the smallest i such
+// that entries i .. n-2 of both rows (as uploaded) equal entry n-2; n when
+// the line is shorter than 3.
+template <typename DR>
+static int converged_from(const DR* dr, const double* cu, int n) {
+  if (n < 3) return n;
+  const int e = n - 2;
+  int i = e;
+  while (i > 0 && std::memcmp(&dr[i - 1], &dr[e], sizeof(DR)) == 0 &&
+         std::memcmp(&cu[i - 1], &cu[e], sizeof(double)) == 0)
+    --i;
+  return i;
 }
 
 int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
@@ -303,8 +362,8 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
   // step this solve (the batched engine) run the short chain too
   c->screen = c->fp64_chain >= 1 ? 2 : c->screen_exact;
   const int n_axis[3] = {c->nx, c->ny, c->nz};
-  size_t dr_off[3], cu_off[3];
-  const size_t bytes = coef_bytes(c, dr_off, cu_off);
+  size_t dr_off[3], cu_off[3], conv_off[3];
+  const size_t bytes = coef_bytes(c, dr_off, cu_off, conv_off);
   std::vector<unsigned char> host(bytes, 0);
   std::vector<double> c1(S);
   for (int ax = 0; ax < 3; ++ax) {
@@ -328,11 +387,20 @@ int upload_coefficients(bfvm_ctx* c, const double* D, const double* decay) {
         }
         reinterpret_cast<double*>(host.data() + cu_off[ax])[q] = u;
       }
+    int* conv = reinterpret_cast<int*>(host.data() + conv_off[ax]);
+    for (int s = 0; s < S; ++s) {
+      const size_t r0 = static_cast<size_t>(s) * np;
+      const double* cur = reinterpret_cast<const double*>(host.data() + cu_off[ax]) + r0;
+      conv[s] = c->prec == BFVM_FP64
+                    ? converged_from(reinterpret_cast<const double2*>(host.data() + dr_off[ax]) + r0, cur, n)
+                    : converged_from(reinterpret_cast<const double*>(host.data() + dr_off[ax]) + r0, cur, n);
+    }
   }
   BFVM_CUDA(cudaMemcpy(c->d_coef, host.data(), bytes, cudaMemcpyHostToDevice));
   for (int a = 0; a < 3; ++a) {
     c->dr_off[a] = dr_off[a];
     c->cu_off[a] = cu_off[a];
+    c->conv_off[a] = conv_off[a];
   }
   BFVM_CUDA(cudaMemcpy(c->d_c1, c1.data(), S * sizeof(double), cudaMemcpyHostToDevice));
   // thomas_constant2 = decay; *= dt; /= 3 (BioFVM_solvers.cpp:208-209)
@@ -580,7 +648,7 @@ int bfvm_create(const bfvm_config* cfg, bfvm_ctx** out) {
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_active), S * sizeof(int));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_faces), face_elems(c) * 8);
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_status), sizeof(int));
-  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_tile_counter), 2 * sizeof(unsigned long long));
+  if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_tile_counter), 4 * sizeof(unsigned long long));
   if (rc == BFVM_OK) rc = dalloc(c, reinterpret_cast<void**>(&c->d_nvalid), sizeof(int));
   if (rc == BFVM_OK)
     rc = dalloc(c, reinterpret_cast<void**>(&c->d_line_off), sizeof(int) * (static_cast<size_t>(c->ny) * c->nz + 1));
@@ -592,7 +660,13 @@ int bfvm_create(const bfvm_config* cfg, bfvm_ctx** out) {
     return fail(BFVM_ERR_OOM);
   }
   if (cudaMemset(c->f, 0, c->field_bytes) != cudaSuccess || cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess ||
-      cudaMemset(c->d_tile_counter, 0, 2 * sizeof(unsigned long long)) != cudaSuccess)
+      cudaMemset(c->d_tile_counter, 0, 4 * sizeof(unsigned long long)) != cudaSuccess)
+    return fail(BFVM_ERR_CUDA);
+  // made here, not on first use, so that steps may run inside a caller's
+  // stream capture of any mode
+  if (cudaStreamCreateWithFlags(&c->group_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_gfork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_gjoin, cudaEventDisableTiming) != cudaSuccess)
     return fail(BFVM_ERR_CUDA);
   if ((rc = upload_coefficients(c, cfg->diffusion_coefficients, cfg->decay_rates)) != BFVM_OK) return fail(rc);
   // Reference defaults: activation on, value 1.0 on every face voxel.
@@ -648,6 +722,12 @@ int bfvm_destroy(bfvm_ctx* c) {
   }
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->group_stream) {
+    cudaStreamSynchronize(c->group_stream);
+    cudaStreamDestroy(c->group_stream);
+  }
+  if (c->ev_gfork) cudaEventDestroy(c->ev_gfork);
+  if (c->ev_gjoin) cudaEventDestroy(c->ev_gjoin);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return BFVM_OK;
@@ -1235,6 +1315,20 @@ extern "C" int bfvm_set_sweep_schedule(bfvm_ctx* c, int persistent) {
   return BFVM_OK;
 }
 
+extern "C" int bfvm_set_substrate_streams(bfvm_ctx* c, int streams) {
+  if (!c || (streams != 1 && streams != 2)) return BFVM_ERR_ARG;
+  DeviceGuard g(c->device);
+  BFVM_CUDA(cudaStreamSynchronize(c->stream));
+  c->sub_streams = streams;  // part of the step graph's key: recaptured on the next run
+  return BFVM_OK;
+}
+
+extern "C" int bfvm_get_substrate_streams(const bfvm_ctx* c, int* streams) {
+  if (!c || !streams) return BFVM_ERR_ARG;
+  *streams = c->sub_streams;
+  return BFVM_OK;
+}
+
 extern "C" int bfvm_set_fused_sources(bfvm_ctx* c, int fused) {
   if (!c || (fused != 0 && fused != 1)) return BFVM_ERR_ARG;
   DeviceGuard g(c->device);
@@ -1332,17 +1426,17 @@ extern "C" int bfvm_set_launch(bfvm_ctx* c, int x_lines, int yz_tile, int yz_chu
 
 namespace bfvm {
 
-int apply_sources_on(bfvm_ctx* c, cudaStream_t st) {
+int apply_sources_on(bfvm_ctx* c, cudaStream_t st, int s_lo, int s_hi) {
   if (c->n_agents == 0) return BFVM_OK;
   const size_t SN = static_cast<size_t>(c->S) * c->n_agents;
   if (c->prec == BFVM_FP64)
     BFVM_CUDA(agents_apply_sources<double>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
                                            c->d_ac + SN, c->d_ac + 2 * SN, nullptr, static_cast<double*>(c->f),
-                                           track_params(c), st));
+                                           track_params(c), st, s_lo, s_hi));
   else
     BFVM_CUDA(agents_apply_sources<float>(c->n_agents, c->d_sorted_keys, c->S, c->nx, c->ny, c->nz, c->nxp, c->d_ac,
                                           c->d_ac + SN, c->d_ac + 2 * SN, c->d_off, static_cast<float*>(c->f),
-                                          track_params(c), st));
+                                          track_params(c), st, s_lo, s_hi));
   note_launches(1);
   return BFVM_OK;
 }

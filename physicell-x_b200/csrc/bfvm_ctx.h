@@ -20,12 +20,19 @@ struct bfvm_ctx {
   // voxel ids are sorted on stream (fork: stream -> copy_stream, join back)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // substrate groups (bfvm_set_substrate_streams): runs of steps sweep the
+  // second half of the substrates on group_stream, forked from stream and
+  // joined back, so each group's kernels fill the other's idle SMs
+  int sub_streams = 2;
+  cudaStream_t group_stream = nullptr;
+  cudaEvent_t ev_gfork = nullptr, ev_gjoin = nullptr;
   void* f = nullptr;           // field, device layout
   size_t field_bytes = 0;
   // coefficients: per axis a, DR rows [S][npad_a] at dr_off[a] and CU rows
   // [S][npad_a] at cu_off[a] (bytes into d_coef); c1 as Coef<T>::C1 [S]
   void* d_coef = nullptr;
   size_t dr_off[3] = {0, 0, 0}, cu_off[3] = {0, 0, 0};
+  size_t conv_off[3] = {0, 0, 0};  // int [S] per axis: AxisCoefs::conv
   void* d_c1 = nullptr;
   int screen = 0;              // SweepParams::screen of the 3-D sweeps (kScreenFast: short FP64 chain)
   int screen_exact = 0;        // 1 when no diffusion or decay rate is negative (the exactness screen applies)
@@ -39,7 +46,7 @@ struct bfvm_ctx {
   double* d_faces = nullptr;   // xface | yface | zface
   int* d_status = nullptr;
   int* h_status = nullptr;     // pinned host copy of d_status, read back in the same stream wait
-  unsigned long long* d_tile_counter = nullptr;  // [2] persistent TMEM y/z sweep work counter
+  unsigned long long* d_tile_counter = nullptr;  // [2] per substrate group: persistent sweeps' work counter
   double* d_sums = nullptr;    // partial sums + result
   bfvm::FieldMaps maps{};
   bfvm::SweepConfig cfg{};
@@ -139,8 +146,9 @@ int update_shift_2d(bfvm_ctx* c);
 // the solve's stream.
 int enqueue_mass_record(bfvm_ctx* c);
 // The standalone source kernel of the solve's agents on stream st
-// (bfvm_apply_sources on the solve's own stream).
-int apply_sources_on(bfvm_ctx* c, cudaStream_t st);
+// (bfvm_apply_sources on the solve's own stream), substrates [s_lo, s_hi)
+// (s_hi < 0: all from s_lo).
+int apply_sources_on(bfvm_ctx* c, cudaStream_t st, int s_lo = 0, int s_hi = -1);
 // One LOD step of the solve (sources when asked, then the x, y and z sweeps,
 // with the solve's own kernels and settings) enqueued on stream st, as
 // bfvm_step launches it; used by the batched engine for members it steps
@@ -219,6 +227,7 @@ inline SweepParams<T> make_params(bfvm_ctx* c, bool sources) {
     axes[a]->dr = reinterpret_cast<const DR*>(cb + c->dr_off[a]);
     axes[a]->cu = reinterpret_cast<const CU*>(cb + c->cu_off[a]);
     axes[a]->npad = coef_pad(n_axis[a]);
+    axes[a]->conv = reinterpret_cast<const int*>(cb + c->conv_off[a]);
   }
   if (sources && c->n_agents > 0) {
     p.line_off = c->d_line_off;
@@ -232,6 +241,8 @@ inline SweepParams<T> make_params(bfvm_ctx* c, bool sources) {
   p.screen = c->screen;
   p.status = c->d_status;
   p.tile_counter = c->d_tile_counter;
+  p.s_lo = 0;
+  p.s_hi = c->S;
   return p;
 }
 

@@ -56,6 +56,10 @@ struct AxisCoefs {
   const typename Coef<T>::DR* dr;
   const typename Coef<T>::CU* cu;
   int npad;
+  // [S] or null: the first index from which a substrate's DR and CU entries
+  // equal those of entry n - 2 (the factorization's fixed point), so that
+  // the tensor-memory sweeps keep them in registers past it
+  const int* conv;
 };
 
 // Rows of coefficient storage per line of n voxels: a y/z tile holds fewer
@@ -137,6 +141,10 @@ struct SweepParams {
   // [2] tiles handed out, CTAs finished: the persistent TMEM y/z sweep's
   // work counter, zero between launches (its last CTA zeroes it)
   unsigned long long* tile_counter;
+  // The substrates a launch sweeps: [s_lo, s_hi) (make_params: all of them).
+  // Substrates are independent through the whole step, so the step may run
+  // as two substrate groups on two streams (bfvm_set_substrate_streams).
+  int s_lo, s_hi;
 };
 
 // Launch configuration of the sweeps (chosen by the host, tunable).  A tile
@@ -184,6 +192,17 @@ struct FieldMaps {
   CUtensorMap rz;  // persistent schedule: box {32, 1, kRingRows, 1}
   CUtensorMap g;   // gradients: box {32 + 4 (FP64) or 32 + 8 (FP32) x, 1, 10 z, min(S, 4) substrates}
   int g_ok;        // 1 when the gradient map could be encoded
+  // tensor-memory x sweeps: 3-D {nx, ny * nz rows (row k * ny + j), S}, box
+  // {128 bytes of x, 32 rows, 1}, 128B swizzle -- a tile is 32 consecutive
+  // rows of one substrate, across y-row ends
+  CUtensorMap xr;
+  int xr_ok;
+  // tensor-memory y/z sweeps, the partial x tiles of several planes packed
+  // into one tile: py has the dimensions {nx, nz, ny, S} (x, plane k, row j,
+  // substrate), pz {nx, ny, nz, S}; box {pyz_w, 32 / pyz_w, 16 rows, 1}.
+  // pyz_w = 0 when nx % 32 leaves nothing to pack (or is above 16).
+  CUtensorMap py, pz;
+  int pyz_w;
 };
 
 // Host-side count of this library's kernel launches (bfvm_kernel_launches).
@@ -249,16 +268,18 @@ size_t ring_yz_bytes(int elem_bytes, int n_line);
 // each launches when it applies to the solve's shape and configuration and
 // sets *launched; otherwise it returns cudaSuccess with *launched false and
 // the caller runs another schedule.
+// The y/z sweeps take the packed map of their axis and its group width pw
+// (FieldMaps::py / pz, pyz_w; 0 when no partial x tiles are packed).
 template <int AXIS>
-cudaError_t launch_tmem_yz(const CUtensorMap& ring_map, const SweepParams<double>& p, const SweepConfig& cfg,
-                           cudaStream_t st, bool* launched);
+cudaError_t launch_tmem_yz(const CUtensorMap& ring_map, const CUtensorMap& pmap, int pw,
+                           const SweepParams<double>& p, const SweepConfig& cfg, cudaStream_t st, bool* launched);
 cudaError_t launch_tmem_x(const CUtensorMap& map, const SweepParams<double>& p, const SweepConfig& cfg,
                           cudaStream_t st, bool* launched);
 // The FP32 sweeps with tensor-memory rings (bfvm_tmem_sweeps.cu), same
 // contract.
 template <int AXIS>
-cudaError_t launch_tmem_yz_f32(const CUtensorMap& ring_map, const SweepParams<float>& p, const SweepConfig& cfg,
-                               cudaStream_t st, bool* launched);
+cudaError_t launch_tmem_yz_f32(const CUtensorMap& ring_map, const CUtensorMap& pmap, int pw,
+                               const SweepParams<float>& p, const SweepConfig& cfg, cudaStream_t st, bool* launched);
 cudaError_t launch_tmem_x_f32(const CUtensorMap& map, const SweepParams<float>& p, const SweepConfig& cfg,
                               cudaStream_t st, bool* launched);
 

@@ -158,6 +158,7 @@ SweepParams<T> make_params_2d(bfvm_ctx* c) {
     axes[a]->dr = reinterpret_cast<const DR*>(cb + c->dr2_off[a]);
     axes[a]->cu = reinterpret_cast<const CU*>(cb + c->cu2_off[a]);
     axes[a]->npad = coef_pad(n_axis[a]);
+    axes[a]->conv = nullptr;  // every chunk reads its coefficients
   }
   p.active = c->d_zero_active;
   p.shift = sizeof(T) == 4 ? c->d_shift2d : nullptr;

@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(32 * kPartWarps) sweep_part_kernel(const __gri
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int n = AXIS == 1 ? ny : nz;
   const int C = (n + kRingRows - 1) / kRingRows;
-  const int i0 = blockIdx.x * kTL, m = blockIdx.y, s = blockIdx.z;
+  const int i0 = blockIdx.x * kTL, m = blockIdx.y, s = p.s_lo + static_cast<int>(blockIdx.z);
   const bool act = p.active[s] != 0;
   if (act && (m == 0 || m == (AXIS == 1 ? nz : ny) - 1)) return;  // a face tile is final already
 
@@ -235,7 +235,7 @@ cudaError_t launch_part(const CUtensorMap& map, const SweepParams<T>& p, const P
   cudaError_t e = cudaFuncSetAttribute(sweep_part_kernel<T, AXIS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  const dim3 grid((p.nx + kTL - 1) / kTL, AXIS == 1 ? p.nz : p.ny, p.S);
+  const dim3 grid((p.nx + kTL - 1) / kTL, AXIS == 1 ? p.nz : p.ny, p.s_hi - p.s_lo);
   sweep_part_kernel<T, AXIS><<<grid, 32 * kPartWarps, smem, st>>>(map, p, pa);
   return cudaGetLastError();
 }

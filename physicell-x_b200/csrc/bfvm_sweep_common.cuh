@@ -161,6 +161,28 @@ __device__ __forceinline__ double forward_any(int screen, const double (&v)[B], 
   return forward_bare<B>(v, cf, c1, y, put);
 }
 
+// The bare chain of the screen's mode over a batch whose coefficients are
+// all one pair cf (the converged part of a factorized row): the same
+// operations as forward_any with cf in every position.
+template <int B, typename Put>
+__device__ __forceinline__ double forward_any_const(int screen, const double (&v)[B], double2 cf, double c1,
+                                                    double y, Put&& put) {
+  if (screen == kScreenFast) {
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      y = __fma_rn(cf.x, y, __dmul_rn(v[q], cf.y));
+      put(q, y);
+    }
+    return y;
+  }
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    y = markstein(__fma_rn(c1, y, v[q]), cf.x, cf.y);
+    put(q, y);
+  }
+  return y;
+}
+
 // Whether a tile whose inputs' minimum high word is hwmin needs no redo:
 // always under the short chain, else when the screen passed.
 __device__ __forceinline__ bool screen_clean(int screen, int hwmin);

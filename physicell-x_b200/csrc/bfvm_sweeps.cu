@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(256) sweep_x_kernel(const __grid_constant__ CU
   }
   __syncthreads();
   uint64_t phase = 0;
-  x_tile<T>(&map, p, blockIdx.x * blockDim.x, blockIdx.y, blockIdx.z, base, phase);
+  x_tile<T>(&map, p, blockIdx.x * blockDim.x, blockIdx.y, p.s_lo + blockIdx.z, base, phase);
   if (threadIdx.x == 0) tma_store_wait_read();
 }
 
@@ -613,7 +613,7 @@ __global__ void __launch_bounds__(TI) sweep_yz_kernel(const __grid_constant__ CU
   }
   __syncthreads();
   uint64_t phase = 0;
-  yz_tile<T, AXIS, TI>(&map, p, blockIdx.x * TI, blockIdx.y, blockIdx.z, CH, base, phase);
+  yz_tile<T, AXIS, TI>(&map, p, blockIdx.x * TI, blockIdx.y, p.s_lo + blockIdx.z, CH, base, phase);
   if (threadIdx.x == 0) tma_store_wait_read();
 }
 
@@ -689,7 +689,7 @@ __global__ void __launch_bounds__(64 * kMaxRings<T>, 1) sweep_yz_ring_kernel(con
   const int C = (n + CH - 1) / CH;
   const int ntx = (nx + TI - 1) / TI;
   const long long per_s = static_cast<long long>(ntx) * nm;
-  const long long ntiles = per_s * p.S;
+  const long long ntiles = per_s * (p.s_hi - p.s_lo);
   // Rings per CTA: warps 0..rings-1 compute, warp rings + r is ring r's copy
   // warp, so consecutive warps -- which the SM spreads over its four
   // sub-partitions -- put the compute warps on different sub-partitions.
@@ -705,8 +705,9 @@ __global__ void __launch_bounds__(64 * kMaxRings<T>, 1) sweep_yz_ring_kernel(con
 
   // tile -> (i0, m, s), x tiles fastest
   auto decode = [&](long long tile, int& i0, int& m, int& s) {
-    s = static_cast<int>(tile / per_s);
-    const long long r = tile - s * per_s;
+    const int sg = static_cast<int>(tile / per_s);
+    const long long r = tile - sg * per_s;
+    s = p.s_lo + sg;
     m = static_cast<int>(r / ntx);
     i0 = static_cast<int>(r - static_cast<long long>(m) * ntx) * TI;
   };
@@ -954,7 +955,7 @@ __global__ void __launch_bounds__(64) sweep_x_ring_kernel(const __grid_constant_
   const int C = (nx + W - 1) / W;
   const int nty = (ny + TL - 1) / TL;
   const long long per_s = static_cast<long long>(nty) * nz;
-  const long long ntiles = per_s * S;
+  const long long ntiles = per_s * (p.s_hi - p.s_lo);
   uint64_t* full = reinterpret_cast<uint64_t*>(base);
   uint64_t* empty = full + kMaxChunks;
   unsigned char* slots = base + kBarrierBytes;
@@ -963,8 +964,9 @@ __global__ void __launch_bounds__(64) sweep_x_ring_kernel(const __grid_constant_
   const int sw = t & 7;
 
   auto decode = [&](long long tile, int& j0, int& k, int& s) {
-    s = static_cast<int>(tile / per_s);
-    const long long r = tile - s * per_s;
+    const int sg = static_cast<int>(tile / per_s);
+    const long long r = tile - sg * per_s;
+    s = p.s_lo + sg;
     k = static_cast<int>(r / nty);
     j0 = static_cast<int>(r - static_cast<long long>(k) * nty) * TL;
   };
@@ -1405,13 +1407,13 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 }
 
 static int encode_one(CUtensorMap* map, void* f, int elem_bytes, const cuuint64_t dims[4], const cuuint64_t strides[3],
-                      const cuuint32_t box[4], CUtensorMapSwizzle swz) {
+                      const cuuint32_t box[4], CUtensorMapSwizzle swz, int rank = 4) {
   auto enc = get_encode();
   if (enc == nullptr) return -1;
   const cuuint32_t estr[4] = {1, 1, 1, 1};
-  CUresult r = enc(map, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, f, dims,
-                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r = enc(map, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                   static_cast<cuuint32_t>(rank), f, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? 0 : -2;
 }
 
@@ -1433,6 +1435,28 @@ int encode_field_maps(FieldMaps* maps, void* f, int eb, int nx, int ny, int nz, 
   // boundaries, one y plane, 8 z with a one-voxel halo, up to 4 substrates
   const cuuint32_t bg[4] = {(cuuint32_t)(eb == 8 ? 36 : 40), 1, 10, (cuuint32_t)(S < 4 ? S : 4)};
   maps->g_ok = rc == 0 && encode_one(&maps->g, f, eb, dims, strides, bg, CU_TENSOR_MAP_SWIZZLE_NONE) == 0;
+  // the tensor-memory x sweeps' rows: planes are contiguous (stride ny rows),
+  // so row k * ny + j of a substrate is one dimension
+  const unsigned long long rows = static_cast<unsigned long long>(ny) * nz;
+  const cuuint64_t dr[4] = {(cuuint64_t)nx, (cuuint64_t)rows, (cuuint64_t)S, 1};
+  const cuuint64_t sr[3] = {(cuuint64_t)nxp * eb, (cuuint64_t)nxp * rows * eb, 0};
+  const cuuint32_t br[4] = {(cuuint32_t)(128 / eb), 32, 1, 1};
+  maps->xr_ok = rc == 0 && rows < (1ull << 31) - 64 &&
+                encode_one(&maps->xr, f, eb, dr, sr, br, CU_TENSOR_MAP_SWIZZLE_128B, 3) == 0;
+  // the y/z sweeps' packed partial x tiles: a box of pw x by 32 / pw planes
+  // by kRingRows rows along the line (the y map lists plane k before row j)
+  maps->pyz_w = 0;
+  const int rem = nx % 32;
+  if (rc == 0 && rem != 0 && rem <= 16) {
+    int w = 16 / eb;  // a box row of at least 16 bytes
+    while (w < rem) w *= 2;
+    const cuuint32_t bp[4] = {(cuuint32_t)w, (cuuint32_t)(32 / w), (cuuint32_t)kRingRows, 1};
+    const cuuint64_t dpy[4] = {(cuuint64_t)nx, (cuuint64_t)nz, (cuuint64_t)ny, (cuuint64_t)S};
+    const cuuint64_t spy[3] = {(cuuint64_t)nxp * ny * eb, (cuuint64_t)nxp * eb, (cuuint64_t)nxp * ny * nz * eb};
+    if (encode_one(&maps->py, f, eb, dpy, spy, bp, CU_TENSOR_MAP_SWIZZLE_NONE) == 0 &&
+        encode_one(&maps->pz, f, eb, dims, strides, bp, CU_TENSOR_MAP_SWIZZLE_NONE) == 0)
+      maps->pyz_w = w;
+  }
   return rc;
 }
 
@@ -1449,15 +1473,17 @@ cudaError_t launch_sweep_x(const FieldMaps& maps, const SweepParams<T>& p, const
   {
     bool launched = false;
     cudaError_t e;
-    if constexpr (sizeof(T) == 8)
-      e = launch_tmem_x(maps.x, p, cfg, st, &launched);
-    else
-      e = launch_tmem_x_f32(maps.x, p, cfg, st, &launched);
-    if (e != cudaSuccess || launched) return e;
+    if (maps.xr_ok) {
+      if constexpr (sizeof(T) == 8)
+        e = launch_tmem_x(maps.xr, p, cfg, st, &launched);
+      else
+        e = launch_tmem_x_f32(maps.xr, p, cfg, st, &launched);
+      if (e != cudaSuccess || launched) return e;
+    }
   }
   if (use_ring_x(sizeof(T), p.nx, cfg)) {
     const size_t smem = ring_x_smem(sizeof(T), p.nx);
-    const long long tiles = static_cast<long long>((p.ny + 31) / 32) * p.nz * p.S;
+    const long long tiles = static_cast<long long>((p.ny + 31) / 32) * p.nz * (p.s_hi - p.s_lo);
     int grid = 0;
     cudaError_t e = persistent_grid(sweep_x_ring_kernel<T>, smem, tiles, &grid);
     if (e != cudaSuccess) return e;
@@ -1467,7 +1493,7 @@ cudaError_t launch_sweep_x(const FieldMaps& maps, const SweepParams<T>& p, const
   const size_t smem = sweep_x_smem(sizeof(T), p.nx, cfg);
   cudaError_t e = cudaFuncSetAttribute(sweep_x_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((p.ny + cfg.x_lines - 1) / cfg.x_lines, p.nz, p.S);
+  dim3 grid((p.ny + cfg.x_lines - 1) / cfg.x_lines, p.nz, p.s_hi - p.s_lo);
   sweep_x_kernel<T><<<grid, cfg.x_lines, smem, st>>>(maps.x, p);
   return cudaGetLastError();
 }
@@ -1480,7 +1506,7 @@ static cudaError_t launch_yz(const CUtensorMap& map, const SweepParams<T>& p, co
   cudaError_t e = cudaFuncSetAttribute(sweep_yz_kernel<T, AXIS, TI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((p.nx + TI - 1) / TI, (AXIS == 1) ? p.nz : p.ny, p.S);
+  dim3 grid((p.nx + TI - 1) / TI, (AXIS == 1) ? p.nz : p.ny, p.s_hi - p.s_lo);
   sweep_yz_kernel<T, AXIS, TI><<<grid, TI, smem, st>>>(map, p, yz_chunk_rows(n, cfg.yz_chunk));
   return cudaGetLastError();
 }
@@ -1491,22 +1517,22 @@ static cudaError_t launch_yz(const CUtensorMap& map, const SweepParams<T>& p, co
 constexpr long long kRingMinTilesPerCta = 8;
 
 template <typename T, int AXIS>
-static cudaError_t launch_yz_any(const CUtensorMap& map, const CUtensorMap& ring_map, const SweepParams<T>& p,
-                                 const SweepConfig& cfg, cudaStream_t st) {
+static cudaError_t launch_yz_any(const CUtensorMap& map, const CUtensorMap& ring_map, const CUtensorMap& pmap, int pw,
+                                 const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
   const int n = (AXIS == 1) ? p.ny : p.nz;
   {
     bool launched = false;
     cudaError_t e;
     if constexpr (sizeof(T) == 8)
-      e = launch_tmem_yz<AXIS>(ring_map, p, cfg, st, &launched);
+      e = launch_tmem_yz<AXIS>(ring_map, pmap, pw, p, cfg, st, &launched);
     else
-      e = launch_tmem_yz_f32<AXIS>(ring_map, p, cfg, st, &launched);
+      e = launch_tmem_yz_f32<AXIS>(ring_map, pmap, pw, p, cfg, st, &launched);
     if (e != cudaSuccess || launched) return e;
   }
   if (use_ring_yz(sizeof(T), n, cfg)) {
     const int rings = ring_yz_count(sizeof(T), n);
     const size_t smem = ring_yz_smem(sizeof(T), n);
-    const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * p.S;
+    const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * (p.s_hi - p.s_lo);
     int grid = 0;
     cudaError_t e = persistent_grid(sweep_yz_ring_kernel<T, AXIS>, smem, (tiles + rings - 1) / rings, &grid,
                                     64 * rings);
@@ -1529,12 +1555,12 @@ static cudaError_t launch_yz_any(const CUtensorMap& map, const CUtensorMap& ring
 
 template <typename T>
 cudaError_t launch_sweep_y(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
-  return launch_yz_any<T, 1>(maps.y, maps.ry, p, cfg, st);
+  return launch_yz_any<T, 1>(maps.y, maps.ry, maps.py, maps.pyz_w, p, cfg, st);
 }
 
 template <typename T>
 cudaError_t launch_sweep_z(const FieldMaps& maps, const SweepParams<T>& p, const SweepConfig& cfg, cudaStream_t st) {
-  return launch_yz_any<T, 2>(maps.z, maps.rz, p, cfg, st);
+  return launch_yz_any<T, 2>(maps.z, maps.rz, maps.pz, maps.pyz_w, p, cfg, st);
 }
 
 template cudaError_t launch_sweep_x<double>(const FieldMaps&, const SweepParams<double>&, const SweepConfig&,

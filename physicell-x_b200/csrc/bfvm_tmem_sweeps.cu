@@ -49,7 +49,38 @@ struct YzShape {
   int nx, n, nm, C, ntx;
   long long per_s, ntiles;
   size_t row_stride;
+  // Packed tiles: when nx % 32 = rem is 1..16, a plane's last x tile would
+  // hold rem lines at the cost of a full one (the sweeps are latency bound).
+  // Instead the first ntr = nx / 32 tiles of each plane are regular and the
+  // rem-wide remainders of P = 32 / pw consecutive planes (pw = rem rounded
+  // up to a power of two, at least 16 bytes) share one tile, loaded by the
+  // packed map as a box {pw x, P planes, 16 rows}: lane t owns x = i0 + t %
+  // pw of plane m0 + t / pw, and the slot keeps the layout [row][32 lanes].
+  // pw = 0: no packing (ntr = ntx).
+  int ntr, pw, pw_log, P;
+  long long nreg;  // regular tiles per substrate, ntr * nm
 };
+
+// Fill the tile enumeration of a YzShape (nx, nm set) for group width pw.
+__device__ __forceinline__ void yz_shape_tiles(YzShape& g, int pw, int S) {
+  constexpr int TI = 32;
+  g.ntx = (g.nx + TI - 1) / TI;
+  g.pw = pw;
+  if (pw > 0) {
+    g.ntr = g.nx / TI;
+    g.P = TI / pw;
+    g.pw_log = 31 - __clz(pw);
+    g.nreg = static_cast<long long>(g.ntr) * g.nm;
+    g.per_s = g.nreg + (g.nm + g.P - 1) / g.P;
+  } else {
+    g.ntr = g.ntx;
+    g.P = 1;
+    g.pw_log = 0;
+    g.nreg = static_cast<long long>(g.ntx) * g.nm;
+    g.per_s = g.nreg;
+  }
+  g.ntiles = g.per_s * S;
+}
 
 // One ring of the TMEM y/z sweep.  A line's first T chunks (T = min(C, 16)
 // for a TMEM ring, 0 for a shared-memory ring) stream through kf input
@@ -62,7 +93,7 @@ struct YzShape {
 // STAGED: the forward pairs read from the ring's copy `drs` in shared
 // memory, else from global memory.
 template <int AXIS, int MODE, bool STAGED>
-__device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const SweepParams<double>& p, const YzShape& g,
+__device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUtensorMap* pmap, const SweepParams<double>& p, const YzShape& g,
                                              int KF, uint64_t* full, double* slots, double* cus, double2* drs,
                                              uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
   using DR = double2;
@@ -73,7 +104,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
   constexpr uint32_t kSlotBytes = kSlotElems * sizeof(double);
   constexpr unsigned kAll = 0xffffffffu;
   const int t = threadIdx.x & 31;
-  const int nx = g.nx, n = g.n, nm = g.nm, C = g.C, ntx = g.ntx;
+  const int nx = g.nx, n = g.n, nm = g.nm, C = g.C, ntr = g.ntr;
   constexpr bool TM = MODE != 0;
   const int T = MODE == 0 ? 0 : (MODE == 1 ? C : kTmemMaxChunks);  // chunks kept in TMEM
   const int NR = MODE == 1 ? 0 : C - T;                             // chunks resident in shared memory
@@ -81,17 +112,27 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
   const long long ntiles = g.ntiles;
   unsigned long long* counter = p.tile_counter;
 
-  auto decode = [&](long long tile, int& i0, int& m, int& s) {
-    s = static_cast<int>(tile / g.per_s);
-    const long long r = tile - s * g.per_s;
-    m = static_cast<int>(r / ntx);
-    i0 = static_cast<int>(r - static_cast<long long>(m) * ntx) * TI;
+  // tile -> (i0, m, s, packed): regular tiles first, then packed ones (m the
+  // first plane of the group)
+  auto decode = [&](long long tile, int& i0, int& m, int& s, bool& pk) {
+    const int sg = static_cast<int>(tile / g.per_s);
+    const long long r = tile - sg * g.per_s;
+    s = p.s_lo + sg;
+    pk = r >= g.nreg;
+    if (pk) {
+      m = static_cast<int>(r - g.nreg) * g.P;
+      i0 = g.ntr * TI;
+    } else {
+      m = static_cast<int>(r / ntr);
+      i0 = static_cast<int>(r - static_cast<long long>(m) * ntr) * TI;
+    }
   };
   // A tile whose lines all lie in an activated face is already final.
   auto skip = [&](long long tile) {
     int i0, m, s;
-    decode(tile, i0, m, s);
-    return p.active[s] != 0 && (m == 0 || m == nm - 1);
+    bool pk;
+    decode(tile, i0, m, s, pk);
+    return !pk && p.active[s] != 0 && (m == 0 || m == nm - 1);
   };
   // The next tile for this ring (whole warp; ntiles when none is left).
   auto grab = [&]() -> long long {
@@ -106,12 +147,14 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
   };
   // Chunk c of the tile at (i0, m, s) into slot sl, completing phase `par`
   // of its barrier (tiles are decoded once, when taken).
-  auto issue = [&](int i0, int m, int s, int c, int sl, uint32_t par) {
+  auto issue = [&](int i0, int m, int s, bool pk, int c, int sl, uint32_t par) {
     if (t == 0) {
       const uint32_t bar = smem_u32(&full[sl]);
       mbar_expect_tx(bar, kSlotBytes);
       const uint32_t dst = smem_u32(slots + static_cast<size_t>(sl) * kSlotElems);
-      if (AXIS == 1)
+      if (pk)  // the packed map's dimensions: x, planes, rows along the line, substrate
+        tma_load_4d(dst, pmap, bar, i0, m, c * CH, s);
+      else if (AXIS == 1)
         tma_load_4d(dst, map, bar, i0, c * CH, m, s);
       else
         tma_load_4d(dst, map, bar, i0, m, c * CH, s);
@@ -125,10 +168,11 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
   bool ok = true;
   long long tile = grab();
   int ti0 = 0, tm_ = 0, ts = 0;  // the current tile, decoded
+  bool tp = false;
   if (tile < ntiles) {
-    decode(tile, ti0, tm_, ts);
-    for (int c = 0; c < (TM ? KF : 0); ++c) issue(ti0, tm_, ts, c, c, 0u);
-    for (int c = T; c < C; ++c) issue(ti0, tm_, ts, c, rslot(false, c), 0u);
+    decode(tile, ti0, tm_, ts, tp);
+    for (int c = 0; c < (TM ? KF : 0); ++c) issue(ti0, tm_, ts, tp, c, c, 0u);
+    for (int c = T; c < C; ++c) issue(ti0, tm_, ts, tp, c, rslot(false, c), 0u);
   }
   const int screen = p.screen;
   int staged_s = -1;
@@ -136,11 +180,17 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
   uint32_t fpar = 0;  // and the phase it completes
   for (uint32_t k = 0; tile < ntiles; ++k) {
     const int i0 = ti0, m = tm_, s = ts;
+    const bool pk = tp;
     const bool flip = (k & 1u) != 0;
     const bool act = p.active[s] != 0;
-    const int i = i0 + t;
-    const bool face = act && (i == 0 || i == nx - 1);  // lines in an x face keep their (pinned) input
-    const bool lane_on = !face && i < nx;
+    // this lane's line (x = i, plane ml); lines in an activated face keep
+    // their (pinned) input
+    const int i = pk ? i0 + (t & (g.pw - 1)) : i0 + t;
+    const int ml = pk ? m + (t >> g.pw_log) : m;
+    const bool inr = i < nx && ml < nm;
+    const bool face = act && (i == 0 || i == nx - 1 || ml == 0 || ml == nm - 1);
+    const bool lane_on = !face && inr;
+    const int mo = inr ? ml : m;  // in range for the address below
     const AxisCoefs<double>& ac = (AXIS == 1) ? p.ay : p.az;
     const DR* __restrict__ drp = ac.dr + static_cast<size_t>(s) * ac.npad;
     const double c1 = p.c1[s];
@@ -153,8 +203,8 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
       staged_s = s;
       __syncwarp();
     }
-    double* out = p.f + ((AXIS == 1) ? ((static_cast<size_t>(s) * p.nz + m) * p.ny) * p.nxp
-                                     : (static_cast<size_t>(s) * p.nz * p.ny + m) * p.nxp) + i;
+    double* out = p.f + ((AXIS == 1) ? ((static_cast<size_t>(s) * p.nz + mo) * p.ny) * p.nxp
+                                     : (static_cast<size_t>(s) * p.nz * p.ny + mo) * p.nxp) + (inr ? i : i0);
     // forward pairs of chunk c (staged, or from global where the plan had no room)
     auto load_cf = [&](int c, DR (&cf)[R]) {
 #pragma unroll
@@ -167,9 +217,10 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
     const bool edge_tile = __any_sync(kAll, !lane_on);
     long long nxt = ntiles;
     int ni0 = 0, nm_ = 0, ns_ = 0;  // the next tile, decoded when taken
+    bool np_ = false;
     auto take_next = [&]() {
       nxt = grab();
-      if (nxt < ntiles) decode(nxt, ni0, nm_, ns_);
+      if (nxt < ntiles) decode(nxt, ni0, nm_, ns_, np_);
     };
 
     // ---- forward elimination ----
@@ -208,9 +259,9 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
         if (c == T - KF && NR == 0) take_next();
         const int cn = c + KF;
         if (cn < T)
-          issue(i0, m, s, cn, sl, fpar ^ 1u);
+          issue(i0, m, s, pk, cn, sl, fpar ^ 1u);
         else if (NR == 0 && nxt < ntiles)
-          issue(ni0, nm_, ns_, cn - T, sl, fpar ^ 1u);
+          issue(ni0, nm_, ns_, np_, cn - T, sl, fpar ^ 1u);
         if (++fsl == KF) {
           fsl = 0;
           fpar ^= 1u;
@@ -264,7 +315,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
       // the next tile's first inputs take the (now idle) input slots
       if (TM && nxt < ntiles) {
         for (int c = 0; c < KF; ++c) {
-          issue(ni0, nm_, ns_, c, fsl, fpar);
+          issue(ni0, nm_, ns_, np_, c, fsl, fpar);
           if (++fsl == KF) {
             fsl = 0;
             fpar ^= 1u;
@@ -338,7 +389,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
         fence_async_smem();  // this lane's forward results in the slot precede the refill
         __syncwarp();        // every lane has read the slot
         // the next tile's resident chunk for this slot (slot order flips)
-        if (nxt < ntiles) issue(ni0, nm_, ns_, T + (NR - 1 - (c - T)), rslot(flip, c), (k + 1) & 1u);
+        if (nxt < ntiles) issue(ni0, nm_, ns_, np_, T + (NR - 1 - (c - T)), rslot(flip, c), (k + 1) & 1u);
       }
     };
     if (edge_tile) {
@@ -350,13 +401,15 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const Sweep
     ti0 = ni0;
     tm_ = nm_;
     ts = ns_;
+    tp = np_;
   }
 }
 
 template <int AXIS>
 __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
-    sweep_yz_tmem_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<double> p,
-                         uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns, int stage_dr) {
+    sweep_yz_tmem_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap pmap,
+                         const SweepParams<double> p, uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf,
+                         int ns, int stage_dr, int pw) {
   constexpr int CH = kRingRows;
   constexpr int TI = 32;
   constexpr int kSlotElems = CH * TI;
@@ -367,9 +420,7 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   g.n = (AXIS == 1) ? p.ny : p.nz;
   g.nm = (AXIS == 1) ? p.nz : p.ny;  // the line's other coordinate (k for y, j for z)
   g.C = (g.n + CH - 1) / CH;
-  g.ntx = (g.nx + TI - 1) / TI;
-  g.per_s = static_cast<long long>(g.ntx) * g.nm;
-  g.ntiles = g.per_s * p.S;
+  yz_shape_tiles(g, pw, p.s_hi - p.s_lo);
   g.row_stride = (AXIS == 1) ? static_cast<size_t>(p.nxp) : static_cast<size_t>(p.nxp) * p.ny;
   const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
   const int nt = static_cast<int>(blockDim.x >> 5) - ns;  // TMEM rings (warps ns..ns+nt-1)
@@ -387,7 +438,10 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   double2* drs = stage_dr ? reinterpret_cast<double2*>(cus + static_cast<size_t>(g.C) * CH) : nullptr;
 
   if (t == 0) {
-    if (warp == 0) prefetch_tmap(&map);
+    if (warp == 0) {
+      prefetch_tmap(&map);
+      if (pw > 0) prefetch_tmap(&pmap);
+    }
     for (int c = 0; c < nslots; ++c) mbar_init(smem_u32(&full[c]), 1);
     fence_barrier_init();
   }
@@ -404,20 +458,20 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
     if (g.C <= kTmemMaxChunks) {
       if (stage_dr)
-        yz_tmem_ring<AXIS, 1, true>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+        yz_tmem_ring<AXIS, 1, true>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
       else
-        yz_tmem_ring<AXIS, 1, false>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+        yz_tmem_ring<AXIS, 1, false>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
     } else {
       if (stage_dr)
-        yz_tmem_ring<AXIS, 2, true>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+        yz_tmem_ring<AXIS, 2, true>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
       else
-        yz_tmem_ring<AXIS, 2, false>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+        yz_tmem_ring<AXIS, 2, false>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
     }
   } else {
     if (stage_dr)
-      yz_tmem_ring<AXIS, 0, true>(&map, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
+      yz_tmem_ring<AXIS, 0, true>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
     else
-      yz_tmem_ring<AXIS, 0, false>(&map, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
+      yz_tmem_ring<AXIS, 0, false>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
   }
 
   // Loads still in flight (only after a wait gave up) land before the CTA
@@ -450,20 +504,26 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
 // source kernel, lines of 2 to 46 chunks).  The same plan as the y/z TMEM
 // sweep: one CTA per SM of ns shared-memory rings and nt <= 4 TMEM rings,
 // each one warp issuing its own TMA loads, tiles handed out by the per-solve
-// counter.  A tile is 32 x-lines of one (k, s); chunk c is the 128-byte
-// column [16c, 16c + 16) of the 32 lines, staged with the 128B swizzle, and
-// lane t owns line j0 + t.  A shared-memory ring stages the whole tile
-// (forward results in place); a TMEM ring streams a line's first 16 chunks
-// through kf input slots and keeps their forward results in its TMEM lanes,
-// the chunks past 16 resident in shared-memory slots.  The back substitution
-// leaves each chunk's results as 32 swizzled rows (in the slot, or in the
-// TMEM ring's staging chunk) and the warp writes them out transposed: each
-// store instruction covers two lines' 128-byte segments.
+// counter.  A tile is 32 consecutive x-lines of one substrate in row order
+// (row k * ny + j, the planes being contiguous in the field), so tiles run on
+// across the ends of y rows and only a substrate's last tile is partial (with
+// tiles of 32 lines of one (k, s), 200 lines took 7 tiles, the last 8 lines
+// wide, at the cost of 7 full ones: the recurrence is latency bound).  Chunk c
+// is the 128-byte column [16c, 16c + 16) of the 32 lines, staged with the
+// 128B swizzle by one 3-D box, and lane t owns row r0 + t.  A shared-memory
+// ring stages the whole tile (forward results in place); a TMEM ring streams
+// a line's first 16 chunks through kf input slots and keeps their forward
+// results in its TMEM lanes, the chunks past 16 resident in shared-memory
+// slots.  The back substitution leaves each chunk's results as 32 swizzled
+// rows (in the slot, or in the TMEM ring's staging chunk), which leave in one
+// bulk tensor store (rows past the substrate's last are clipped by the map).
 constexpr int kXTmemBarrierBytes = 256;  // at the end of a ring
 
 // The shape of one x persistent sweep, shared by its rings.
 struct XShape {
-  int nx, ny, nz, C, ntj;
+  int nx, ny, nz, C;
+  int rows;  // x-lines per substrate, ny * nz: row k * ny + j
+  int ntj;   // 32-row tiles per substrate
   long long ntiles;
 };
 
@@ -491,11 +551,11 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
   const int RB = TM ? KF : 0;                                       // first resident slot
   auto rslot = [&](bool fl, int c) { return RB + ring_slot(fl, NR, c - T); };
 
-  auto decode = [&](long long tile, int& j0, int& k, int& s) {
-    const long long r = tile / ntj;
-    j0 = static_cast<int>(tile - r * ntj) * 32;
-    s = static_cast<int>(r / nz);
-    k = static_cast<int>(r - static_cast<long long>(s) * nz);
+  // a tile is 32 consecutive rows (k * ny + j) of one substrate
+  auto decode = [&](long long tile, int& r0, int& s) {
+    const int sg = static_cast<int>(tile / ntj);
+    r0 = static_cast<int>(tile - static_cast<long long>(sg) * ntj) * 32;
+    s = p.s_lo + sg;
   };
   auto grab = [&]() -> long long {
     long long v = 0;
@@ -505,11 +565,11 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
     }
     return __shfl_sync(kAll, v, 0);
   };
-  auto issue = [&](int j0, int k, int s, int c, int sl, uint32_t par) {
+  auto issue = [&](int r0, int s, int c, int sl, uint32_t par) {
     if (t == 0) {
       const uint32_t bar = smem_u32(&full[sl]);
       mbar_expect_tx(bar, kChunkBytes);
-      tma_load_4d(smem_u32(slots + static_cast<size_t>(sl) * kChunkBytes), map, bar, c * W, j0, k, s);
+      tma_load_3d(smem_u32(slots + static_cast<size_t>(sl) * kChunkBytes), map, bar, c * W, r0, s);
     }
     pend |= 1u << sl;
     ppar = (ppar & ~(1u << sl)) | (par << sl);
@@ -517,21 +577,28 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
 
   bool ok = true;
   long long tile = grab();
-  int tj0 = 0, tk = 0, ts = 0;
+  int tr0 = 0, ts = 0;
   if (tile < ntiles) {
-    decode(tile, tj0, tk, ts);
-    for (int c = 0; c < (TM ? KF : 0); ++c) issue(tj0, tk, ts, c, c, 0u);
-    for (int c = T; c < C; ++c) issue(tj0, tk, ts, c, rslot(false, c), 0u);
+    decode(tile, tr0, ts);
+    for (int c = 0; c < (TM ? KF : 0); ++c) issue(tr0, ts, c, c, 0u);
+    for (int c = T; c < C; ++c) issue(tr0, ts, c, rslot(false, c), 0u);
   }
   const int screen = p.screen;
   int staged_s = -1;
+  // chunks kc0..kc1 of the staged substrate lie in its converged range
+  // (AxisCoefs::conv): their forward pairs are dk and upper diagonals ck
+  int kc0 = INT_MAX, kc1 = -1;
+  DR dk = make_double2(0.0, 0.0);
+  double ck = 0.0;
   int fsl = 0;
   uint32_t fpar = 0;
   for (uint32_t it = 0; tile < ntiles; ++it) {
-    const int j0 = tj0, k = tk, s = ts;
+    const int r0 = tr0, s = ts;
     const bool flip = (it & 1u) != 0;
-    const int j = j0 + t;
-    const bool valid = j < ny;
+    const int rl = r0 + t;  // this lane's line: row rl = k * ny + j
+    const bool valid = rl < g.rows;
+    const int k = valid ? rl / ny : 0;
+    const int j = valid ? rl - k * ny : 0;
     const bool act = p.active[s] != 0;
     const bool face = act && (j == 0 || j == ny - 1 || k == 0 || k == nz - 1);
     const bool lane_on = valid && !face;
@@ -539,6 +606,14 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
     const double c1 = p.c1[s];
     if (s != staged_s) {
       stage_row(cus, p.ax.cu + static_cast<size_t>(s) * p.ax.npad, C * W);
+      kc0 = INT_MAX;
+      kc1 = -1;
+      if (p.ax.conv != nullptr && nx >= 3) {
+        kc0 = (__ldg(p.ax.conv + s) + W - 1) / W;
+        kc1 = (nx - 1) / W - 1;  // chunks ending at element nx - 2 or before
+        dk = __ldg(drp + nx - 2);
+        ck = __ldg(p.ax.cu + static_cast<size_t>(s) * p.ax.npad + nx - 2);
+      }
       staged_s = s;
       __syncwarp();
     }
@@ -555,25 +630,32 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
         fv = p.yface + ((static_cast<size_t>(j == 0 ? 0 : 1) * S + s) * nz + k) * nx;
     }
     double* plane = p.f + (static_cast<size_t>(s) * nz + k) * ny * static_cast<size_t>(p.nxp);
-    DR cf[W];
-#pragma unroll
-    for (int q = 0; q < W; ++q) cf[q] = __ldg(drp + q);
     double y = -0.0;
     int hwmin = INT_MAX;
     const bool edge_tile = __any_sync(kAll, !lane_on);
+    // constant-coefficient chunks of this tile (edge tiles read every chunk's)
+    const int k0 = edge_tile ? INT_MAX : kc0, k1 = edge_tile ? -1 : kc1;
     long long nxt = ntiles;
-    int nj0 = 0, nk = 0, ns_ = 0;
+    int nr0 = 0, ns_ = 0;
     auto take_next = [&]() {
       nxt = grab();
-      if (nxt < ntiles) decode(nxt, nj0, nk, ns_);
+      if (nxt < ntiles) decode(nxt, nr0, ns_);
     };
 
     // ---- forward elimination ----
-    auto fwd_chunk = [&](bool edge, int c) {
+    // kconst: std::true_type for a chunk in the converged range
+    auto fwd_chunk = [&](auto kconst, bool edge, int c) {
+      constexpr bool K = decltype(kconst)::value;
       const int i0 = c * W;
       const bool flow = MODE == 1 || (MODE == 2 && c < T);
       const int sl = flow ? fsl : rslot(flip, c);
       const uint32_t par = flow ? fpar : (it & 1u);
+      // the chunk's forward pairs, loading while the slot's barrier is awaited
+      DR cf[W];
+      if constexpr (!K) {
+#pragma unroll
+        for (int q = 0; q < W; ++q) cf[q] = __ldg(drp + i0 + q);
+      }
       if (ok) ok = mbar_wait(smem_u32(&full[sl]), par);
       pend &= ~(1u << sl);
       unsigned char* crow = slots + static_cast<size_t>(sl) * kChunkBytes + t * 128;
@@ -594,13 +676,23 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
           for (int q = 0; q < W; ++q)
             if (i0 + q >= nx) v[q] = 1.0;
         }
-        if (flow) {
-          y = forward_any<W>(screen, v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
-        } else {
-          RowPut<double> put{crow, sw};
-          y = forward_any<W>(screen, v, cf, c1, y, put);
-        }
+        // the screen reads the inputs before the chain
         if (screen != kScreenFast) hwmin = min(hwmin, batch_min_hi<W>(v));
+        if constexpr (K) {
+          if (flow) {
+            y = forward_any_const<W>(screen, v, dk, c1, y, [&](int q, double val) { yv[q] = val; });
+          } else {
+            RowPut<double> put{crow, sw};
+            y = forward_any_const<W>(screen, v, dk, c1, y, put);
+          }
+        } else {
+          if (flow) {
+            y = forward_any<W>(screen, v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
+          } else {
+            RowPut<double> put{crow, sw};
+            y = forward_any<W>(screen, v, cf, c1, y, put);
+          }
+        }
       } else if (flow) {
 #pragma unroll
         for (int q = 0; q < W; ++q) yv[q] = 0.0;  // lanes with no line: anything, never read
@@ -612,21 +704,24 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
         if (MODE == 1 && c == T - KF) take_next();
         const int cn = c + KF;
         if (cn < T)
-          issue(j0, k, s, cn, sl, fpar ^ 1u);
+          issue(r0, s, cn, sl, fpar ^ 1u);
         else if (MODE == 1 && nxt < ntiles)
-          issue(nj0, nk, ns_, cn - T, sl, fpar ^ 1u);
+          issue(nr0, ns_, cn - T, sl, fpar ^ 1u);
         if (++fsl == KF) {
           fsl = 0;
           fpar ^= 1u;
         }
       }
-#pragma unroll
-      for (int q = 0; q < W; ++q) cf[q] = __ldg(drp + (c + 1) * W + q);
     };
     if (edge_tile) {
-      for (int c = 0; c < C; ++c) fwd_chunk(true, c);
+      for (int c = 0; c < C; ++c) fwd_chunk(std::false_type{}, true, c);
     } else {
-      for (int c = 0; c < C; ++c) fwd_chunk(false, c);
+      for (int c = 0; c < C; ++c) {
+        if (c >= k0 && c <= k1)
+          fwd_chunk(std::true_type{}, false, c);
+        else
+          fwd_chunk(std::false_type{}, false, c);
+      }
     }
     __syncwarp();
     if constexpr (TM) tmem_wait_st();
@@ -684,9 +779,10 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
     }
     int pend_refill = -1;  // a resident chunk whose slot waits for its store to be read
     auto refill = [&](int cc) {
-      if (nxt < ntiles) issue(nj0, nk, ns_, T + (NR - 1 - (cc - T)), rslot(flip, cc), (it + 1) & 1u);
+      if (nxt < ntiles) issue(nr0, ns_, T + (NR - 1 - (cc - T)), rslot(flip, cc), (it + 1) & 1u);
     };
-    auto back_chunk = [&](bool edge, int c) {
+    auto back_chunk = [&](auto kconst, bool edge, int c) {
+      constexpr bool K = decltype(kconst)::value;
       const int i0 = c * W;
       const bool flow = MODE == 1 || (MODE == 2 && c < T);
       unsigned char* cbase = flow ? stage : slots + static_cast<size_t>(rslot(flip, c)) * kChunkBytes;
@@ -707,13 +803,18 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
           for (int q = 0; q < W; ++q) v[q] = (i0 + q < nx) ? fv[i0 + q] : 0.0;
         }
       } else if (!edge || valid) {
-        const double2* cwp = reinterpret_cast<const double2*>(cus + i0);  // 16-byte pairs
         double cw[W];
+        if constexpr (K) {
 #pragma unroll
-        for (int q = 0; q < W / 2; ++q) {
-          const double2 pr = cwp[q];
-          cw[2 * q] = pr.x;
-          cw[2 * q + 1] = pr.y;
+          for (int q = 0; q < W; ++q) cw[q] = ck;
+        } else {
+          const double2* cwp = reinterpret_cast<const double2*>(cus + i0);  // 16-byte pairs
+#pragma unroll
+          for (int q = 0; q < W / 2; ++q) {
+            const double2 pr = cwp[q];
+            cw[2 * q] = pr.x;
+            cw[2 * q + 1] = pr.y;
+          }
         }
         if (i0 + W > nx) {
 #pragma unroll
@@ -754,7 +855,7 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
       fence_async_smem();
       __syncwarp();
       if (t == 0) {
-        tma_store_4d(map, smem_u32(cbase), i0, j0, k, s);
+        tma_store_3d(map, smem_u32(cbase), i0, r0, s);
         tma_store_commit();
       }
       if (!flow) {
@@ -770,9 +871,14 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
       }
     };
     if (edge_tile) {
-      for (int c = C - 1; c >= 0; --c) back_chunk(true, c);
+      for (int c = C - 1; c >= 0; --c) back_chunk(std::false_type{}, true, c);
     } else {
-      for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
+      for (int c = C - 1; c >= 0; --c) {
+        if (c >= k0 && c <= k1)
+          back_chunk(std::true_type{}, false, c);
+        else
+          back_chunk(std::false_type{}, false, c);
+      }
     }
     if (pend_refill >= 0) {
       if (t == 0) tma_store_wait_read();
@@ -786,7 +892,7 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
       fence_async_smem();
       __syncwarp();
       for (int c = 0; c < KF; ++c) {
-        issue(nj0, nk, ns_, c, fsl, fpar);
+        issue(nr0, ns_, c, fsl, fpar);
         if (++fsl == KF) {
           fsl = 0;
           fpar ^= 1u;
@@ -802,8 +908,7 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
       }
     }
     tile = nxt;
-    tj0 = nj0;
-    tk = nk;
+    tr0 = nr0;
     ts = ns_;
   }
 }
@@ -819,8 +924,9 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   g.ny = p.ny;
   g.nz = p.nz;
   g.C = (g.nx + 15) / 16;
-  g.ntj = (g.ny + 31) / 32;
-  g.ntiles = static_cast<long long>(g.ntj) * g.nz * p.S;
+  g.rows = g.ny * g.nz;
+  g.ntj = (g.rows + 31) / 32;
+  g.ntiles = static_cast<long long>(g.ntj) * (p.s_hi - p.s_lo);
   const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
   const int nt = static_cast<int>(blockDim.x >> 5) - ns;  // TMEM rings (warps ns..ns+nt-1)
   const bool tm = warp >= ns;
@@ -901,7 +1007,7 @@ constexpr int kTmemRingSmemF32 = 3;  // most shared-memory rings (warps 0..ns-1;
 constexpr int kTmemRingTmemF32 = 8;  // most TMEM rings, two per lane quarter
 
 template <int AXIS, int MODE>
-__device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const SweepParams<float>& p,
+__device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const CUtensorMap* pmap, const SweepParams<float>& p,
                                                  const YzShape& g, int KF, uint64_t* full, float* slots, double* cus,
                                                  double* drs, uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
   constexpr int R = kRowBatch;
@@ -911,7 +1017,7 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
   constexpr uint32_t kSlotBytes = kSlotElems * sizeof(float);
   constexpr unsigned kAll = 0xffffffffu;
   const int t = threadIdx.x & 31;
-  const int nx = g.nx, n = g.n, nm = g.nm, C = g.C, ntx = g.ntx;
+  const int nx = g.nx, n = g.n, nm = g.nm, C = g.C, ntr = g.ntr;
   constexpr bool TM = MODE != 0;
   const int T = MODE == 0 ? 0 : (MODE == 1 ? C : kTmemMaxChunks);  // chunks kept in TMEM
   const int NR = MODE == 1 ? 0 : C - T;                             // chunks resident in shared memory
@@ -919,16 +1025,26 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
   const long long ntiles = g.ntiles;
   unsigned long long* counter = p.tile_counter;
 
-  auto decode = [&](long long tile, int& i0, int& m, int& s) {
-    s = static_cast<int>(tile / g.per_s);
-    const long long r = tile - s * g.per_s;
-    m = static_cast<int>(r / ntx);
-    i0 = static_cast<int>(r - static_cast<long long>(m) * ntx) * TI;
+  // tile -> (i0, m, s, packed): regular tiles first, then packed ones (m the
+  // first plane of the group)
+  auto decode = [&](long long tile, int& i0, int& m, int& s, bool& pk) {
+    const int sg = static_cast<int>(tile / g.per_s);
+    const long long r = tile - sg * g.per_s;
+    s = p.s_lo + sg;
+    pk = r >= g.nreg;
+    if (pk) {
+      m = static_cast<int>(r - g.nreg) * g.P;
+      i0 = g.ntr * TI;
+    } else {
+      m = static_cast<int>(r / ntr);
+      i0 = static_cast<int>(r - static_cast<long long>(m) * ntr) * TI;
+    }
   };
   auto skip = [&](long long tile) {  // every line of the tile in an activated face: final already
     int i0, m, s;
-    decode(tile, i0, m, s);
-    return p.active[s] != 0 && (m == 0 || m == nm - 1);
+    bool pk;
+    decode(tile, i0, m, s, pk);
+    return !pk && p.active[s] != 0 && (m == 0 || m == nm - 1);
   };
   auto grab = [&]() -> long long {
     long long v = 0;
@@ -940,12 +1056,14 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
     }
     return __shfl_sync(kAll, v, 0);
   };
-  auto issue = [&](int i0, int m, int s, int c, int sl, uint32_t par) {
+  auto issue = [&](int i0, int m, int s, bool pk, int c, int sl, uint32_t par) {
     if (t == 0) {
       const uint32_t bar = smem_u32(&full[sl]);
       mbar_expect_tx(bar, kSlotBytes);
       const uint32_t dst = smem_u32(slots + static_cast<size_t>(sl) * kSlotElems);
-      if (AXIS == 1)
+      if (pk)  // the packed map's dimensions: x, planes, rows along the line, substrate
+        tma_load_4d(dst, pmap, bar, i0, m, c * CH, s);
+      else if (AXIS == 1)
         tma_load_4d(dst, map, bar, i0, c * CH, m, s);
       else
         tma_load_4d(dst, map, bar, i0, m, c * CH, s);
@@ -958,10 +1076,11 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
   bool ok = true;
   long long tile = grab();
   int ti0 = 0, tm_ = 0, ts = 0;
+  bool tp = false;
   if (tile < ntiles) {
-    decode(tile, ti0, tm_, ts);
-    for (int c = 0; c < (TM ? KF : 0); ++c) issue(ti0, tm_, ts, c, c, 0u);
-    for (int c = T; c < C; ++c) issue(ti0, tm_, ts, c, rslot(false, c), 0u);
+    decode(tile, ti0, tm_, ts, tp);
+    for (int c = 0; c < (TM ? KF : 0); ++c) issue(ti0, tm_, ts, tp, c, c, 0u);
+    for (int c = T; c < C; ++c) issue(ti0, tm_, ts, tp, c, rslot(false, c), 0u);
   }
   const int screen = p.screen;
   int staged_s = -1;
@@ -969,11 +1088,17 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
   uint32_t fpar = 0;
   for (uint32_t k = 0; tile < ntiles; ++k) {
     const int i0 = ti0, m = tm_, s = ts;
+    const bool pk = tp;
     const bool flip = (k & 1u) != 0;
     const bool act = p.active[s] != 0;
-    const int i = i0 + t;
-    const bool face = act && (i == 0 || i == nx - 1);  // lines in an x face keep their (pinned) input
-    const bool lane_on = !face && i < nx;
+    // this lane's line (x = i, plane ml); lines in an activated face keep
+    // their (pinned) input
+    const int i = pk ? i0 + (t & (g.pw - 1)) : i0 + t;
+    const int ml = pk ? m + (t >> g.pw_log) : m;
+    const bool inr = i < nx && ml < nm;
+    const bool face = act && (i == 0 || i == nx - 1 || ml == 0 || ml == nm - 1);
+    const bool lane_on = !face && inr;
+    const int mo = inr ? ml : m;  // in range for the address below
     const AxisCoefs<float>& ac = (AXIS == 1) ? p.ay : p.az;
     const double* __restrict__ drp = ac.dr + static_cast<size_t>(s) * ac.npad;  // RN(1/d)
     const double c1 = p.c1[s];
@@ -984,8 +1109,8 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
       staged_s = s;
       __syncwarp();
     }
-    float* out = p.f + ((AXIS == 1) ? ((static_cast<size_t>(s) * p.nz + m) * p.ny) * p.nxp
-                                    : (static_cast<size_t>(s) * p.nz * p.ny + m) * p.nxp) + i;
+    float* out = p.f + ((AXIS == 1) ? ((static_cast<size_t>(s) * p.nz + mo) * p.ny) * p.nxp
+                                    : (static_cast<size_t>(s) * p.nz * p.ny + mo) * p.nxp) + (inr ? i : i0);
     auto load_cf = [&](int c, double (&cf)[R]) {
       if (drs) {
 #pragma unroll
@@ -1001,9 +1126,10 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
     const bool edge_tile = __any_sync(kAll, !lane_on);
     long long nxt = ntiles;
     int ni0 = 0, nm_ = 0, ns_ = 0;
+    bool np_ = false;
     auto take_next = [&]() {
       nxt = grab();
-      if (nxt < ntiles) decode(nxt, ni0, nm_, ns_);
+      if (nxt < ntiles) decode(nxt, ni0, nm_, ns_, np_);
     };
 
     // ---- forward elimination (FP64 recurrence, results rounded to FP32) ----
@@ -1040,9 +1166,9 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
         if (c == T - KF && NR == 0) take_next();
         const int cn = c + KF;
         if (cn < T)
-          issue(i0, m, s, cn, sl, fpar ^ 1u);
+          issue(i0, m, s, pk, cn, sl, fpar ^ 1u);
         else if (NR == 0 && nxt < ntiles)
-          issue(ni0, nm_, ns_, cn - T, sl, fpar ^ 1u);
+          issue(ni0, nm_, ns_, np_, cn - T, sl, fpar ^ 1u);
         if (++fsl == KF) {
           fsl = 0;
           fpar ^= 1u;
@@ -1065,7 +1191,7 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
       take_next();
       if (TM && nxt < ntiles) {
         for (int c = 0; c < KF; ++c) {
-          issue(ni0, nm_, ns_, c, fsl, fpar);
+          issue(ni0, nm_, ns_, np_, c, fsl, fpar);
           if (++fsl == KF) {
             fsl = 0;
             fpar ^= 1u;
@@ -1136,7 +1262,7 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
       }
       if (!flow) {
         __syncwarp();  // every lane has read the slot
-        if (nxt < ntiles) issue(ni0, nm_, ns_, T + (NR - 1 - (c - T)), rslot(flip, c), (k + 1) & 1u);
+        if (nxt < ntiles) issue(ni0, nm_, ns_, np_, T + (NR - 1 - (c - T)), rslot(flip, c), (k + 1) & 1u);
       }
     };
     if (edge_tile) {
@@ -1148,13 +1274,15 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const S
     ti0 = ni0;
     tm_ = nm_;
     ts = ns_;
+    tp = np_;
   }
 }
 
 template <int AXIS>
 __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
-    sweep_yz_tmem_f32_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<float> p,
-                             uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns, int stage_dr) {
+    sweep_yz_tmem_f32_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap pmap,
+                             const SweepParams<float> p, uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf,
+                             int ns, int stage_dr, int pw) {
   constexpr int CH = kRingRows;
   constexpr int TI = 32;
   constexpr int kSlotElems = CH * TI;
@@ -1165,9 +1293,7 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
   g.n = (AXIS == 1) ? p.ny : p.nz;
   g.nm = (AXIS == 1) ? p.nz : p.ny;
   g.C = (g.n + CH - 1) / CH;
-  g.ntx = (g.nx + TI - 1) / TI;
-  g.per_s = static_cast<long long>(g.ntx) * g.nm;
-  g.ntiles = g.per_s * p.S;
+  yz_shape_tiles(g, pw, p.s_hi - p.s_lo);
   g.row_stride = (AXIS == 1) ? static_cast<size_t>(p.nxp) : static_cast<size_t>(p.nxp) * p.ny;
   const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
   const int nt = static_cast<int>(blockDim.x >> 5) - ns;  // TMEM rings (warps ns..ns+nt-1)
@@ -1185,7 +1311,10 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
   double* drs = stage_dr ? cus + static_cast<size_t>(g.C) * CH : nullptr;
 
   if (t == 0) {
-    if (warp == 0) prefetch_tmap(&map);
+    if (warp == 0) {
+      prefetch_tmap(&map);
+      if (pw > 0) prefetch_tmap(&pmap);
+    }
     for (int c = 0; c < nslots; ++c) mbar_init(smem_u32(&full[c]), 1);
     fence_barrier_init();
   }
@@ -1203,11 +1332,11 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
     const uint32_t half = static_cast<uint32_t>((warp - ns) >= 4 ? 256 : 0);
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + half;
     if (g.C <= kTmemMaxChunks)
-      yz_tmem_ring_f32<AXIS, 1>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+      yz_tmem_ring_f32<AXIS, 1>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
     else
-      yz_tmem_ring_f32<AXIS, 2>(&map, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+      yz_tmem_ring_f32<AXIS, 2>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
   } else {
-    yz_tmem_ring_f32<AXIS, 0>(&map, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
+    yz_tmem_ring_f32<AXIS, 0>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
   }
   if (pend != 0) {
     for (int sl = 0; sl < nslots; ++sl)
@@ -1237,8 +1366,9 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
 //
 // The FP64 x sweep's plan above for the FP32 form: values stored in FP32,
 // the recurrence in FP64, the pins and face values as the per-tile FP32 x
-// sweep of bfvm_sweeps.cu applies them, so results are its bits.  A chunk is
-// the 128-byte column [32c, 32c + 32) of the tile's 32 lines; its forward
+// sweep of bfvm_sweeps.cu applies them, so results are its bits.  Tiles are
+// 32 consecutive rows (k * ny + j) of one substrate, as in the FP64 sweep.  A
+// chunk is the 128-byte column [32c, 32c + 32) of the tile's 32 lines; its forward
 // results take 32 TMEM columns, so a ring keeps 8 chunks (lines of up to 256)
 // in 256 columns and two rings share each lane quarter.
 constexpr int kXTmemRingSmemF32 = 0;   // shared-memory rings (none: measured slower, see use_tmem_x_f32)
@@ -1267,11 +1397,11 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
   const int RB = TM ? KF : 0;                                           // first resident slot
   auto rslot = [&](bool fl, int c) { return RB + ring_slot(fl, NR, c - T); };
 
-  auto decode = [&](long long tile, int& j0, int& k, int& s) {
-    const long long r = tile / ntj;
-    j0 = static_cast<int>(tile - r * ntj) * 32;
-    s = static_cast<int>(r / nz);
-    k = static_cast<int>(r - static_cast<long long>(s) * nz);
+  // a tile is 32 consecutive rows (k * ny + j) of one substrate
+  auto decode = [&](long long tile, int& r0, int& s) {
+    const int sg = static_cast<int>(tile / ntj);
+    r0 = static_cast<int>(tile - static_cast<long long>(sg) * ntj) * 32;
+    s = p.s_lo + sg;
   };
   auto grab = [&]() -> long long {
     long long v = 0;
@@ -1281,11 +1411,11 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
     }
     return __shfl_sync(kAll, v, 0);
   };
-  auto issue = [&](int j0, int k, int s, int c, int sl, uint32_t par) {
+  auto issue = [&](int r0, int s, int c, int sl, uint32_t par) {
     if (t == 0) {
       const uint32_t bar = smem_u32(&full[sl]);
       mbar_expect_tx(bar, kChunkBytes);
-      tma_load_4d(smem_u32(slots + static_cast<size_t>(sl) * kChunkBytes), map, bar, c * W, j0, k, s);
+      tma_load_3d(smem_u32(slots + static_cast<size_t>(sl) * kChunkBytes), map, bar, c * W, r0, s);
     }
     pend |= 1u << sl;
     ppar = (ppar & ~(1u << sl)) | (par << sl);
@@ -1293,21 +1423,23 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
 
   bool ok = true;
   long long tile = grab();
-  int tj0 = 0, tk = 0, ts = 0;
+  int tr0 = 0, ts = 0;
   if (tile < ntiles) {
-    decode(tile, tj0, tk, ts);
-    for (int c = 0; c < (TM ? KF : 0); ++c) issue(tj0, tk, ts, c, c, 0u);
-    for (int c = T; c < C; ++c) issue(tj0, tk, ts, c, rslot(false, c), 0u);
+    decode(tile, tr0, ts);
+    for (int c = 0; c < (TM ? KF : 0); ++c) issue(tr0, ts, c, c, 0u);
+    for (int c = T; c < C; ++c) issue(tr0, ts, c, rslot(false, c), 0u);
   }
   const int screen = p.screen;
   int staged_s = -1;
   int fsl = 0;
   uint32_t fpar = 0;
   for (uint32_t it = 0; tile < ntiles; ++it) {
-    const int j0 = tj0, k = tk, s = ts;
+    const int r0 = tr0, s = ts;
     const bool flip = (it & 1u) != 0;
-    const int j = j0 + t;
-    const bool valid = j < ny;
+    const int rl = r0 + t;  // this lane's line: row rl = k * ny + j
+    const bool valid = rl < g.rows;
+    const int k = valid ? rl / ny : 0;
+    const int j = valid ? rl - k * ny : 0;
     const bool act = p.active[s] != 0;
     const bool face = act && (j == 0 || j == ny - 1 || k == 0 || k == nz - 1);
     const bool lane_on = valid && !face;
@@ -1339,10 +1471,10 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
     double y = -0.0;
     const bool edge_tile = __any_sync(kAll, !lane_on);
     long long nxt = ntiles;
-    int nj0 = 0, nk = 0, ns_ = 0;
+    int nr0 = 0, ns_ = 0;
     auto take_next = [&]() {
       nxt = grab();
-      if (nxt < ntiles) decode(nxt, nj0, nk, ns_);
+      if (nxt < ntiles) decode(nxt, nr0, ns_);
     };
 
     // ---- forward elimination (FP64 recurrence, results rounded to FP32) ----
@@ -1402,9 +1534,9 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
         if (MODE == 1 && c == T - KF) take_next();
         const int cn = c + KF;
         if (cn < T)
-          issue(j0, k, s, cn, sl, fpar ^ 1u);
+          issue(r0, s, cn, sl, fpar ^ 1u);
         else if (MODE == 1 && nxt < ntiles)
-          issue(nj0, nk, ns_, cn - T, sl, fpar ^ 1u);
+          issue(nr0, ns_, cn - T, sl, fpar ^ 1u);
         if (++fsl == KF) {
           fsl = 0;
           fpar ^= 1u;
@@ -1433,7 +1565,7 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
     }
     int pend_refill = -1;  // a resident chunk whose slot waits for its store to be read
     auto refill = [&](int cc) {
-      if (nxt < ntiles) issue(nj0, nk, ns_, T + (NR - 1 - (cc - T)), rslot(flip, cc), (it + 1) & 1u);
+      if (nxt < ntiles) issue(nr0, ns_, T + (NR - 1 - (cc - T)), rslot(flip, cc), (it + 1) & 1u);
     };
     auto back_chunk = [&](bool edge, int c) {
       const int i0 = c * W;
@@ -1521,7 +1653,7 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
       fence_async_smem();
       __syncwarp();
       if (t == 0) {
-        tma_store_4d(map, smem_u32(cbase), i0, j0, k, s);
+        tma_store_3d(map, smem_u32(cbase), i0, r0, s);
         tma_store_commit();
       }
       if (!flow) {
@@ -1553,7 +1685,7 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
       fence_async_smem();
       __syncwarp();
       for (int c = 0; c < KF; ++c) {
-        issue(nj0, nk, ns_, c, fsl, fpar);
+        issue(nr0, ns_, c, fsl, fpar);
         if (++fsl == KF) {
           fsl = 0;
           fpar ^= 1u;
@@ -1569,8 +1701,7 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
       }
     }
     tile = nxt;
-    tj0 = nj0;
-    tk = nk;
+    tr0 = nr0;
     ts = ns_;
   }
 }
@@ -1586,8 +1717,9 @@ __global__ void __launch_bounds__(32 * (kXTmemRingSmemF32 + kXTmemRingTmemF32), 
   g.ny = p.ny;
   g.nz = p.nz;
   g.C = (g.nx + 31) / 32;
-  g.ntj = (g.ny + 31) / 32;
-  g.ntiles = static_cast<long long>(g.ntj) * g.nz * p.S;
+  g.rows = g.ny * g.nz;
+  g.ntj = (g.rows + 31) / 32;
+  g.ntiles = static_cast<long long>(g.ntj) * (p.s_hi - p.s_lo);
   const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
   const int nt = static_cast<int>(blockDim.x >> 5) - ns;  // TMEM rings (warps ns..ns+nt-1)
   const bool tm = warp >= ns;
@@ -1783,9 +1915,17 @@ static bool use_tmem_yz(int eb, int n_line, const SweepConfig& cfg, int* ns, int
   return best > 0;
 }
 
+// Tiles of a y/z sweep over nx columns and nm planes per substrate, with
+// partial x tiles packed pw wide (pw = 0: none).
+static long long yz_tiles(int nx, int nm, int S, int pw) {
+  if (pw <= 0) return static_cast<long long>((nx + 31) / 32) * nm * S;
+  const int P = 32 / pw;
+  return (static_cast<long long>(nx / 32) * nm + (nm + P - 1) / P) * S;
+}
+
 template <int AXIS>
-cudaError_t launch_tmem_yz(const CUtensorMap& ring_map, const SweepParams<double>& p, const SweepConfig& cfg,
-                           cudaStream_t st, bool* launched) {
+cudaError_t launch_tmem_yz(const CUtensorMap& ring_map, const CUtensorMap& pmap, int pw,
+                           const SweepParams<double>& p, const SweepConfig& cfg, cudaStream_t st, bool* launched) {
   *launched = false;
   const int n = (AXIS == 1) ? p.ny : p.nz;
   int ns = 0, nt = 0, kf = 0;
@@ -1793,14 +1933,14 @@ cudaError_t launch_tmem_yz(const CUtensorMap& ring_map, const SweepParams<double
   if (!use_tmem_yz(8, n, cfg, &ns, &nt, &kf, &dr)) return cudaSuccess;
   const int rings = ns + nt;
   const size_t smem = tmem_yz_smem(n, ns, nt, kf, dr);
-  const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * p.S;
+  const long long tiles = yz_tiles(p.nx, (AXIS == 1) ? p.nz : p.ny, p.s_hi - p.s_lo, pw);
   int grid = 0;
   cudaError_t e = persistent_grid(sweep_yz_tmem_kernel<AXIS>, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
   sweep_yz_tmem_kernel<AXIS><<<grid, 32 * rings, smem, st>>>(
-      ring_map, p, static_cast<uint32_t>(tmem_yz_smem_ring_bytes(n, dr)),
-      static_cast<uint32_t>(tmem_yz_ring_bytes(n, kf, dr)), kf, ns, dr ? 1 : 0);
+      ring_map, pmap, p, static_cast<uint32_t>(tmem_yz_smem_ring_bytes(n, dr)),
+      static_cast<uint32_t>(tmem_yz_ring_bytes(n, kf, dr)), kf, ns, dr ? 1 : 0, pw);
   *launched = true;
   return cudaGetLastError();
 }
@@ -1812,7 +1952,7 @@ cudaError_t launch_tmem_x(const CUtensorMap& map, const SweepParams<double>& p, 
   if (!use_tmem_x(8, p.nx, p.line_off != nullptr, cfg, &ns, &nt, &kf)) return cudaSuccess;
   const int rings = ns + nt;
   const size_t smem = x_tmem_smem(p.nx, ns, nt, kf);
-  const long long tiles = static_cast<long long>((p.ny + 31) / 32) * p.nz * p.S;
+  const long long tiles = (static_cast<long long>(p.ny) * p.nz + 31) / 32 * (p.s_hi - p.s_lo);
   int grid = 0;
   cudaError_t e = persistent_grid(sweep_x_tmem_kernel, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;
@@ -1824,9 +1964,9 @@ cudaError_t launch_tmem_x(const CUtensorMap& map, const SweepParams<double>& p, 
   return cudaGetLastError();
 }
 
-template cudaError_t launch_tmem_yz<1>(const CUtensorMap&, const SweepParams<double>&, const SweepConfig&,
+template cudaError_t launch_tmem_yz<1>(const CUtensorMap&, const CUtensorMap&, int, const SweepParams<double>&, const SweepConfig&,
                                        cudaStream_t, bool*);
-template cudaError_t launch_tmem_yz<2>(const CUtensorMap&, const SweepParams<double>&, const SweepConfig&,
+template cudaError_t launch_tmem_yz<2>(const CUtensorMap&, const CUtensorMap&, int, const SweepParams<double>&, const SweepConfig&,
                                        cudaStream_t, bool*);
 
 // The staged FP64 coefficient rows of one FP32 ring: the upper diagonal
@@ -1887,8 +2027,8 @@ static bool use_tmem_yz_f32(int eb, int n_line, const SweepConfig& cfg, int* ns,
 }
 
 template <int AXIS>
-cudaError_t launch_tmem_yz_f32(const CUtensorMap& ring_map, const SweepParams<float>& p, const SweepConfig& cfg,
-                               cudaStream_t st, bool* launched) {
+cudaError_t launch_tmem_yz_f32(const CUtensorMap& ring_map, const CUtensorMap& pmap, int pw,
+                               const SweepParams<float>& p, const SweepConfig& cfg, cudaStream_t st, bool* launched) {
   *launched = false;
   const int n = (AXIS == 1) ? p.ny : p.nz;
   int ns = 0, nt = 0, kf = 0;
@@ -1896,22 +2036,22 @@ cudaError_t launch_tmem_yz_f32(const CUtensorMap& ring_map, const SweepParams<fl
   if (!use_tmem_yz_f32(4, n, cfg, &ns, &nt, &kf, &dr)) return cudaSuccess;
   const int rings = ns + nt;
   const size_t smem = tmem_yz_f32_smem(n, ns, nt, kf, dr);
-  const long long tiles = static_cast<long long>((p.nx + 31) / 32) * ((AXIS == 1) ? p.nz : p.ny) * p.S;
+  const long long tiles = yz_tiles(p.nx, (AXIS == 1) ? p.nz : p.ny, p.s_hi - p.s_lo, pw);
   int grid = 0;
   cudaError_t e =
       persistent_grid(sweep_yz_tmem_f32_kernel<AXIS>, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
   sweep_yz_tmem_f32_kernel<AXIS><<<grid, 32 * rings, smem, st>>>(
-      ring_map, p, static_cast<uint32_t>(tmem_yz_f32_smem_ring_bytes(n, dr)),
-      static_cast<uint32_t>(tmem_yz_f32_ring_bytes(n, kf, dr)), kf, ns, dr ? 1 : 0);
+      ring_map, pmap, p, static_cast<uint32_t>(tmem_yz_f32_smem_ring_bytes(n, dr)),
+      static_cast<uint32_t>(tmem_yz_f32_ring_bytes(n, kf, dr)), kf, ns, dr ? 1 : 0, pw);
   *launched = true;
   return cudaGetLastError();
 }
 
-template cudaError_t launch_tmem_yz_f32<1>(const CUtensorMap&, const SweepParams<float>&, const SweepConfig&,
+template cudaError_t launch_tmem_yz_f32<1>(const CUtensorMap&, const CUtensorMap&, int, const SweepParams<float>&, const SweepConfig&,
                                            cudaStream_t, bool*);
-template cudaError_t launch_tmem_yz_f32<2>(const CUtensorMap&, const SweepParams<float>&, const SweepConfig&,
+template cudaError_t launch_tmem_yz_f32<2>(const CUtensorMap&, const CUtensorMap&, int, const SweepParams<float>&, const SweepConfig&,
                                            cudaStream_t, bool*);
 
 // One ring of the FP32 TMEM x sweep (a multiple of 1024 bytes, so every chunk
@@ -1979,7 +2119,7 @@ cudaError_t launch_tmem_x_f32(const CUtensorMap& map, const SweepParams<float>& 
   if (!use_tmem_x_f32(4, p.nx, p.line_off != nullptr, cfg, &ns, &nt, &kf, &dr)) return cudaSuccess;
   const int rings = ns + nt;
   const size_t smem = x_tmem_f32_smem(p.nx, ns, nt, kf, dr);
-  const long long tiles = static_cast<long long>((p.ny + 31) / 32) * p.nz * p.S;
+  const long long tiles = (static_cast<long long>(p.ny) * p.nz + 31) / 32 * (p.s_hi - p.s_lo);
   int grid = 0;
   cudaError_t e = persistent_grid(sweep_x_tmem_f32_kernel, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;

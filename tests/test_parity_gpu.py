@@ -392,3 +392,62 @@ def test_tmem_sweeps_fp32_bitwise(shape, chain):
         assert np.array_equal(got, base), (shape, chain, key)
     err = _normwise(base, Port.run(wl), S)
     assert np.all(err <= FP32_TOL), err
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_substrate_streams_give_the_same_bits(precision):
+    """Runs of steps with the substrates split over two streams (the default)
+    equal one sequence of launches bit for bit: an odd substrate count (groups
+    of 2 and 1), stacked agents with internalized-substrate tracking, fused
+    and standalone sources, a run long enough to replay the captured graph
+    plus a remainder, and a short uncaptured run.  FP64 equals the oracle."""
+    wl = W.small_random(37, nx=200, ny=64, nz=40, S=3, n_agents=6000, steps=21, agent_mode="gauss", stack=True)
+    c1, c2, e2 = Port.workload_constants(wl)
+    f = wl.field0.copy()
+    internal = np.zeros((wl.n_agents, wl.S))
+    V = wl.dx * wl.dx * wl.dx
+    for _ in range(wl.steps + 3):
+        Port.sources_tracked(f, wl.S, wl.agent_voxel, c1, c2, e2, wl.net_export * wl.dt, V, internal)
+        Port.lod_step(f, wl.shape, wl.D, wl.decay, wl.dt, wl.dx, wl.dirichlet_active, wl.dirichlet_values)
+    for fused in (False, True):
+        outs = []
+        for streams in (1, 2):
+            me = Microenvironment.from_workload(wl, precision)
+            me.set_substrate_streams(streams)
+            assert me.substrate_streams() == streams
+            me.set_fused_sources(fused)
+            me.set_track_internalized_substrates(True)
+            me.simulate_diffusion_decay(wl.steps, sources=True)
+            me.simulate_diffusion_decay(3, sources=True)
+            outs.append((me.download_field(), me.internalized_substrates()))
+            me.close()
+        assert np.array_equal(outs[0][0], outs[1][0]), (precision, fused)
+        assert np.array_equal(outs[0][1], outs[1][1]), (precision, fused)
+        if precision == "fp64":
+            assert np.array_equal(outs[1][0], f), fused
+            assert np.array_equal(outs[1][1], internal), fused
+        else:
+            assert np.all(_normwise(outs[1][0], f, wl.S) <= FP32_TOL), fused
+
+
+@pytest.mark.parametrize("shape", [(42, 70, 45, 2), (48, 40, 37, 1), (81, 50, 33, 2), (100, 36, 70, 3)])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_packed_partial_tiles(shape, precision):
+    """The y/z sweeps pack the partial x tiles of several planes into one
+    tile (x extents whose remainder mod 32 is 10, 16, 17 -- not packed -- and
+    4), and the x sweep runs its lines in row order across y-row ends: FP64
+    bit for bit against the oracle, FP32 within its tolerance, both with the
+    sweeps in tensor memory forced on every axis."""
+    nx, ny, nz, S = shape
+    wl = W.small_random(38 + nx, nx=nx, ny=ny, nz=nz, S=S, n_agents=1500, steps=3, stack=True)
+    me = Microenvironment.from_workload(wl, precision)
+    me.set_sweep_schedule(2)
+    me.set_sweep_tmem(2)
+    me.simulate_diffusion_decay(wl.steps, sources=True)
+    got = me.download_field()
+    me.close()
+    expect = Port.run(wl)
+    if precision == "fp64":
+        assert np.array_equal(got, expect)
+    else:
+        assert np.all(_normwise(got, expect, S) <= FP32_TOL)

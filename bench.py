@@ -79,9 +79,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
-    ap.add_argument("--substrate-streams", type=int, choices=[1, 2], default=2,
-                    help="bfvm_set_substrate_streams of the timed solve: 2 (default) sweeps the two halves of the "
-                         "substrates on two streams, 1 in one sequence of launches")
+    ap.add_argument("--substrate-streams", type=int, choices=[1, 2], default=1,
+                    help="bfvm_set_substrate_streams of the timed solve: 1 (default) one sequence of launches, 2 "
+                         "the two halves of the substrates on two streams")
     ap.add_argument("--fp64-chain", type=int, choices=[0, 1, 2], default=0,
                     help="arithmetic of the timed solve (bfvm_set_fp64_chain): 0 the reference's (default)")
     ap.add_argument("--workload", choices=["cube200", "uneven_batch", "serve", "accuracy"], default="cube200",

@@ -350,9 +350,9 @@ class Microenvironment:
         source kernel ahead of the sweeps (False, the default)."""
         check(self.L.bfvm_set_fused_sources(self.h, 1 if fused else 0), "bfvm_set_fused_sources")
 
-    def set_substrate_streams(self, streams=2):
-        """Runs of steps sweep the two halves of the substrates on two streams
-        (2, the default) or every substrate in one sequence of launches (1);
+    def set_substrate_streams(self, streams=1):
+        """Runs of steps sweep every substrate in one sequence of launches (1,
+        the default) or the two halves of the substrates on two streams (2);
         the same bits either way."""
         check(self.L.bfvm_set_substrate_streams(self.h, int(streams)), "bfvm_set_substrate_streams")
 

@@ -20,10 +20,10 @@ struct bfvm_ctx {
   // voxel ids are sorted on stream (fork: stream -> copy_stream, join back)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  // substrate groups (bfvm_set_substrate_streams): runs of steps sweep the
-  // second half of the substrates on group_stream, forked from stream and
-  // joined back, so each group's kernels fill the other's idle SMs
-  int sub_streams = 2;
+  // substrate groups (bfvm_set_substrate_streams): with 2, runs of steps
+  // sweep the second half of the substrates on group_stream, forked from
+  // stream and joined back (measured slower at cube200: default 1)
+  int sub_streams = 1;
   cudaStream_t group_stream = nullptr;
   cudaEvent_t ev_gfork = nullptr, ev_gjoin = nullptr;
   void* f = nullptr;           // field, device layout

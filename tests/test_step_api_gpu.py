@@ -26,7 +26,8 @@ def test_graph_replay_equals_single_steps(precision, fused):
     before = kernel_launches()
     b.simulate_diffusion_decay(wl.steps, sources=True)
     b.synchronize()
-    per_step = 3 if fused else 4
+    # sources and three sweeps per substrate group (two groups by default)
+    per_step = (3 if fused else 4) * b.substrate_streams()
     assert kernel_launches() - before == wl.steps * per_step
     np.testing.assert_array_equal(b.download_field(), a.download_field())
     if precision == "fp64":

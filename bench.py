@@ -63,10 +63,10 @@ WORKLOAD = ("cube200: 200x200x200 voxels (dx=10 um), 4 substrates, 100000 agents
 # current kernels; profiles/sweeps_cube200_fp64.txt gives the commands and
 # the raw figures.  Keys: (precision, kernel index 0=sources 1=x 2=y 3=z).
 NCU_TRAFFIC = {
-    ("fp64", 0): 56552448 + 1760768,
-    ("fp64", 1): 271819776 + 198265856,
-    ("fp64", 2): 266214656 + 198479872,
-    ("fp64", 3): 266218240 + 195012864,
+    ("fp64", 0): 56553472 + 1718528,
+    ("fp64", 1): 273038080 + 199272448,
+    ("fp64", 2): 271641856 + 199482880,
+    ("fp64", 3): 271166208 + 195453184,
 }
 
 

@@ -93,7 +93,8 @@ def uneven_batch(n_envs=256, steps=200, trial_steps=5, device=0, chain=0):
         e1.record(bs)
         b.synchronize()
         t = e0.elapsed_time(e1) * 1e-3
-        res = {"s": t, "updates_per_s": tot * steps / t, "schedule": b.get_schedule(), "autotune_ms_per_step": tuned_ms}
+        res = {"s": t, "updates_per_s": tot * steps / t, "schedule": b.get_schedule(),
+               "direct_threshold": b.get_direct_threshold(), "autotune_ms_per_step": tuned_ms}
         if prec == "fp64":
             res["bitwise_equal_to_plain"] = all(bool(torch.equal(_device_field(me, device), r))
                                                 for me, r in zip(mes, ref))

@@ -38,6 +38,14 @@ struct bfvm_batch {
   long long direct_min = 2097152;  // mode 2: N*S (voxel-substrate values) from which a member steps directly
   std::vector<bfvm_ctx*> direct;  // mode 2: the members stepped directly (set with the tables)
   int direct_launches = 0;        // their kernels per step
+  // mode 2: the direct members run on up to kSideStreams side streams, forked
+  // from the batch stream and joined back around each run of steps, so that
+  // the members' own persistent kernels share the GPU; direct_lane[i] is the
+  // side stream of direct[i] (members balanced by size)
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_ev;
+  cudaEvent_t fork_ev = nullptr;
+  std::vector<int> direct_lane;
   int yz_chunk = 32;
   int order = 0;        // 0: members in insertion order; 1: largest first
   int ctas_per_sm = 0;  // 0: as many as fit
@@ -63,6 +71,8 @@ struct bfvm_batch {
 };
 
 namespace {
+
+constexpr int kSideStreams = 8;
 
 int sm_count_dev(int dev) {
   int n = 0;
@@ -116,6 +126,37 @@ int build_tables(bfvm_batch* b, bool sources) {
       b->direct_launches += 3 + ((sources && c->n_agents > 0 && !c->cfg.fuse_sources) ? 1 : 0);
     } else {
       idx.push_back(q);
+    }
+  }
+  // the direct members' side streams: the largest member first onto the
+  // least loaded stream
+  {
+    const int K = std::min(static_cast<int>(b->direct.size()), kSideStreams);
+    while (static_cast<int>(b->side.size()) < K) {
+      cudaStream_t st = nullptr;
+      cudaEvent_t ev = nullptr;
+      BFVM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaStreamDestroy(st);
+        return BFVM_ERR_CUDA;
+      }
+      b->side.push_back(st);
+      b->side_ev.push_back(ev);
+    }
+    if (K > 0 && !b->fork_ev) BFVM_CUDA(cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming));
+    std::vector<int> order(b->direct.size());
+    for (size_t q = 0; q < order.size(); ++q) order[q] = static_cast<int>(q);
+    auto work = [&](int q) {
+      const bfvm_ctx* c = b->direct[q];
+      return 1LL * c->nx * c->ny * c->nz * c->S;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return work(a) > work(c); });
+    std::vector<long long> load(K, 0);
+    b->direct_lane.assign(b->direct.size(), 0);
+    for (int q : order) {
+      const int k = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+      b->direct_lane[q] = k;
+      load[k] += work(q);
     }
   }
   const int nb = static_cast<int>(idx.size());
@@ -197,20 +238,9 @@ int build_tables(bfvm_batch* b, bool sources) {
   return BFVM_OK;
 }
 
-// Launches of one step on the batch stream (also used while capturing).
-// stall_env >= 0 (fault injection, fused schedule only): that table entry's
-// finished-x-tile counter starts far below zero, so its y tiles wait on x
-// tiles that never count up and their bounded waits run out.
+// One step of the fused schedule (schedule 0) on the batch stream.
 template <typename T>
-cudaError_t enqueue_step(bfvm_batch* b, int stall_env = -1) {
-  if (b->mode >= 1) {
-    cudaError_t e = launch_batch_sweeps<T>(b->d_hdr, static_cast<const BatchEnv<T>*>(b->d_envs), b->d_pre, b->cap,
-                                           b->items, b->axis_smem, b->stream);
-    if (e != cudaSuccess) return e;
-    for (bfvm_ctx* c : b->direct)
-      if (enqueue_step_on(c, b->built_sources, b->stream) != BFVM_OK) return cudaErrorLaunchFailure;
-    return cudaSuccess;
-  }
+cudaError_t enqueue_fused_step(bfvm_batch* b, int stall_env) {
   cudaError_t e = cudaMemsetAsync(b->d_counters, 0, sizeof(int) * (1 + 3 * b->cap), b->stream);
   if (e != cudaSuccess) return e;
   if (stall_env >= 0) {
@@ -219,6 +249,45 @@ cudaError_t enqueue_step(bfvm_batch* b, int stall_env = -1) {
   }
   return launch_batch_step<T>(b->d_hdr, static_cast<const BatchEnv<T>*>(b->d_envs), b->d_pre, b->cap, b->d_counters,
                               b->d_status, b->grid, b->smem, b->stream);
+}
+
+// Launches of nsteps steps on the batch stream (also used while capturing).
+// Schedules 1 and 2: the batched sweeps on the batch stream; the direct
+// members (schedule 2), each with all of its steps in order, on their side
+// streams, forked from the batch stream before the first step and joined
+// back after the last (the members are independent solves).
+// stall_env >= 0 (fault injection, fused schedule only): that table entry's
+// finished-x-tile counter starts far below zero, so its y tiles wait on x
+// tiles that never count up and their bounded waits run out.
+template <typename T>
+cudaError_t enqueue_steps(bfvm_batch* b, int nsteps, int stall_env = -1) {
+  if (b->mode >= 1) {
+    const int K = std::min(static_cast<int>(b->direct.size()), static_cast<int>(b->side.size()));
+    cudaError_t e = cudaSuccess;
+    if (K > 0) {
+      if ((e = cudaEventRecord(b->fork_ev, b->stream)) != cudaSuccess) return e;
+      for (int k = 0; k < K; ++k)
+        if ((e = cudaStreamWaitEvent(b->side[k], b->fork_ev, 0)) != cudaSuccess) return e;
+    }
+    for (int s = 0; s < nsteps && e == cudaSuccess; ++s)
+      e = launch_batch_sweeps<T>(b->d_hdr, static_cast<const BatchEnv<T>*>(b->d_envs), b->d_pre, b->cap, b->items,
+                                 b->axis_smem, b->stream);
+    for (size_t q = 0; q < b->direct.size() && e == cudaSuccess; ++q) {
+      cudaStream_t st = K > 0 ? b->side[b->direct_lane[q] % K] : b->stream;
+      for (int s = 0; s < nsteps && e == cudaSuccess; ++s)
+        if (enqueue_step_on(b->direct[q], b->built_sources, st) != BFVM_OK) e = cudaErrorLaunchFailure;
+    }
+    // joined even after a failed launch, so that a capture can end
+    for (int k = 0; k < K; ++k) {
+      cudaError_t e2 = cudaEventRecord(b->side_ev[k], b->side[k]);
+      if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(b->stream, b->side_ev[k], 0);
+      if (e == cudaSuccess) e = e2;
+    }
+    return e;
+  }
+  cudaError_t e = cudaSuccess;
+  for (int s = 0; s < nsteps && e == cudaSuccess; ++s) e = enqueue_fused_step<T>(b, s == 0 ? stall_env : -1);
+  return e;
 }
 
 // The batched kernels of one step (the directly stepped members count their
@@ -230,7 +299,7 @@ int kernels_per_step(const bfvm_batch* b) {
 
 template <typename T>
 int launch_one(bfvm_batch* b, int stall_env = -1) {
-  BFVM_CUDA(enqueue_step<T>(b, stall_env));
+  BFVM_CUDA(enqueue_steps<T>(b, 1, stall_env));
   note_launches(kernels_per_step(b));
   b->launches += kernels_per_step(b) + b->direct_launches;
   return BFVM_OK;
@@ -242,8 +311,8 @@ int capture_graph(bfvm_batch* b) {
   cudaGraph_t g = nullptr;
   BFVM_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   set_launch_capture(true);  // the replays count the launches
-  for (int s = 0; s < b->graph_steps; ++s) {
-    const cudaError_t e2 = enqueue_step<T>(b);
+  {
+    const cudaError_t e2 = enqueue_steps<T>(b, b->graph_steps);
     if (e2 != cudaSuccess) {
       set_launch_capture(false);
       cudaStreamEndCapture(b->stream, &g);
@@ -370,6 +439,12 @@ int bfvm_batch_destroy(bfvm_batch* b) {
   if (b->d_hdr) cudaFree(b->d_hdr);
   if (b->d_status) cudaFree(b->d_status);
   if (b->ev) cudaEventDestroy(b->ev);
+  for (size_t k = 0; k < b->side.size(); ++k) {
+    cudaStreamSynchronize(b->side[k]);
+    cudaStreamDestroy(b->side[k]);
+    cudaEventDestroy(b->side_ev[k]);
+  }
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return BFVM_OK;
@@ -516,8 +591,9 @@ int bfvm_batch_autotune(bfvm_batch* b, int flags, int trial_steps, double* best_
     for (int ord : {0, 1})
       for (int ctas : {0, 8, 4}) cands.push_back({0, ch, ord, ctas, b->direct_min});
   }
-  // mode 2: members from 32^3, 64^3 or 128^3 voxel-substrate values step directly
-  for (long long dm : {32768LL, 262144LL, 2097152LL})
+  // mode 2: every member, or members from 32^3, 64^3 or 128^3 voxel-substrate
+  // values, step directly (their own kernels on the side streams)
+  for (long long dm : {1LL, 32768LL, 262144LL, 2097152LL})
     for (int ch : {32, 64}) cands.push_back({2, ch, 0, 0, dm});
   const int keep_graph = b->graph_steps;
   const long long keep_direct = b->direct_min;

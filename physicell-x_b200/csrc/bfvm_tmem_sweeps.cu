@@ -92,7 +92,7 @@ __device__ __forceinline__ void yz_shape_tiles(YzShape& g, int pw, int S) {
 // resident chunks (C > 16).
 // STAGED: the forward pairs read from the ring's copy `drs` in shared
 // memory, else from global memory.
-template <int AXIS, int MODE, bool STAGED>
+template <int AXIS, int MODE, bool STAGED, bool FAST>
 __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUtensorMap* pmap, const SweepParams<double>& p, const YzShape& g,
                                              int KF, uint64_t* full, double* slots, double* cus, double2* drs,
                                              uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
@@ -176,6 +176,11 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
   }
   const int screen = p.screen;
   int staged_s = -1;
+  // chunks kc0..kc1 of the staged substrate lie in its converged range
+  // (AxisCoefs::conv): their forward pairs are dk and upper diagonals ck
+  int kc0 = INT_MAX, kc1 = -1;
+  DR dk = make_double2(0.0, 0.0);
+  double ck = 0.0;
   int fsl = 0;        // TMEM chunks: slot of the next input to consume
   uint32_t fpar = 0;  // and the phase it completes
   for (uint32_t k = 0; tile < ntiles; ++k) {
@@ -200,6 +205,14 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
       // prefetch) -- read as shared-memory broadcasts
       stage_row(cus, ac.cu + static_cast<size_t>(s) * ac.npad, C * CH);
       if (STAGED) stage_row(reinterpret_cast<double*>(drs), reinterpret_cast<const double*>(drp), 2 * (C + 1) * CH);
+      kc0 = INT_MAX;
+      kc1 = -1;
+      if (FAST && ac.conv != nullptr && n >= 3) {
+        kc0 = (__ldg(ac.conv + s) + CH - 1) / CH;
+        kc1 = (n - 1) / CH - 1;  // chunks ending at row n - 2 or before
+        dk = __ldg(drp + n - 2);
+        ck = __ldg(ac.cu + static_cast<size_t>(s) * ac.npad + n - 2);
+      }
       staged_s = s;
       __syncwarp();
     }
@@ -210,11 +223,11 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
 #pragma unroll
       for (int q = 0; q < R; ++q) cf[q] = STAGED ? drs[c * R + q] : __ldg(drp + c * R + q);
     };
-    DR cf[R];
-    load_cf(0, cf);
     double y = -0.0;
     int hwmin = INT_MAX;
     const bool edge_tile = __any_sync(kAll, !lane_on);
+    // constant-coefficient chunks of this tile (edge tiles read every chunk's)
+    const int k0 = edge_tile ? INT_MAX : kc0, k1 = edge_tile ? -1 : kc1;
     long long nxt = ntiles;
     int ni0 = 0, nm_ = 0, ns_ = 0;  // the next tile, decoded when taken
     bool np_ = false;
@@ -224,11 +237,16 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
     };
 
     // ---- forward elimination ----
-    auto fwd_chunk = [&](bool edge, int c) {
+    // kconst: std::true_type for a chunk in the converged range
+    auto fwd_chunk = [&](auto kconst, bool edge, int c) {
+      constexpr bool K = decltype(kconst)::value;
       const int rb = c * CH;
       const bool flow = MODE == 1 || (MODE == 2 && c < T);
       const int sl = flow ? fsl : rslot(flip, c);
       const uint32_t par = flow ? fpar : (k & 1u);
+      // the chunk's forward pairs, loading while the slot's barrier is awaited
+      DR cf[R];
+      if constexpr (!K) load_cf(c, cf);
       if (ok) ok = mbar_wait(smem_u32(&full[sl]), par);
       pend &= ~(1u << sl);
       double* cb = slots + static_cast<size_t>(sl) * kSlotElems + t;
@@ -242,11 +260,25 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
           for (int q = 0; q < R; ++q)
             if (rb + q >= n) v[q] = 1.0;
         }
-        if (flow)
-          y = forward_any<R>(screen, v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
-        else
-          y = forward_any<R>(screen, v, cf, c1, y, [&](int q, double val) { cb[q * TI] = val; });
-        if (screen != kScreenFast) hwmin = min(hwmin, batch_min_hi<R>(v));
+        if constexpr (K) {
+          if (!FAST) hwmin = min(hwmin, batch_min_hi<R>(v));
+          if (flow)
+            y = forward_any_const<R>(FAST ? kScreenFast : 1, v, dk, c1, y, [&](int q, double val) { yv[q] = val; });
+          else
+            y = forward_any_const<R>(FAST ? kScreenFast : 1, v, dk, c1, y,
+                                     [&](int q, double val) { cb[q * TI] = val; });
+        } else if constexpr (FAST) {
+          if (flow)
+            y = forward_fast<R>(v, cf, y, [&](int q, double val) { yv[q] = val; });
+          else
+            y = forward_fast<R>(v, cf, y, [&](int q, double val) { cb[q * TI] = val; });
+        } else {
+          if (flow)
+            y = forward_bare<R>(v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
+          else
+            y = forward_bare<R>(v, cf, c1, y, [&](int q, double val) { cb[q * TI] = val; });
+          hwmin = min(hwmin, batch_min_hi<R>(v));
+        }
       } else if (flow) {
 #pragma unroll
         for (int q = 0; q < R; ++q) yv[q] = 0.0;  // lanes with no line: anything, never read
@@ -267,12 +299,16 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
           fpar ^= 1u;
         }
       }
-      load_cf(c + 1, cf);
     };
     if (edge_tile) {
-      for (int c = 0; c < C; ++c) fwd_chunk(true, c);
+      for (int c = 0; c < C; ++c) fwd_chunk(std::false_type{}, true, c);
     } else {
-      for (int c = 0; c < C; ++c) fwd_chunk(false, c);
+      for (int c = 0; c < C; ++c) {
+        if (c >= k0 && c <= k1)
+          fwd_chunk(std::true_type{}, false, c);
+        else
+          fwd_chunk(std::false_type{}, false, c);
+      }
     }
     __syncwarp();
     if constexpr (TM) tmem_wait_st();
@@ -283,7 +319,7 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
     // The screen, once per tile: a line with an input below 2^-960 (or
     // negative) anywhere is redone from its inputs, which are still in the
     // field (this tile's results are stored only by the back substitution).
-    if (__any_sync(kAll, !screen_clean(screen, hwmin))) {
+    if (!FAST && __any_sync(kAll, !screen_clean(screen, hwmin))) {
       y = -0.0;
       for (int c = 0; c < C; ++c) {
         const int rb = c * CH;
@@ -340,7 +376,8 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
       __syncwarp();
       tmem_ld32_issue(tbase + 32u * (T - 1), tr);
     }
-    auto back_chunk = [&](bool edge, int c) {
+    auto back_chunk = [&](auto kconst, bool edge, int c) {
+      constexpr bool K = decltype(kconst)::value;
       const int rb = c * CH;
       const bool flow = MODE == 1 || (MODE == 2 && c < T);
       double v[R];
@@ -356,13 +393,18 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
         for (int q = 0; q < R; ++q) v[q] = cb[q * TI];
       }
       if (!edge || lane_on) {
-        const double2* cwp = reinterpret_cast<const double2*>(cus + rb);  // 16-byte pairs
         double cw[R];
+        if constexpr (K) {
 #pragma unroll
-        for (int q = 0; q < R / 2; ++q) {
-          const double2 pr = cwp[q];
-          cw[2 * q] = pr.x;
-          cw[2 * q + 1] = pr.y;
+          for (int q = 0; q < R; ++q) cw[q] = ck;
+        } else {
+          const double2* cwp = reinterpret_cast<const double2*>(cus + rb);  // 16-byte pairs
+#pragma unroll
+          for (int q = 0; q < R / 2; ++q) {
+            const double2 pr = cwp[q];
+            cw[2 * q] = pr.x;
+            cw[2 * q + 1] = pr.y;
+          }
         }
         double* o = out + static_cast<size_t>(rb) * g.row_stride;
         if (c == C - 1 || (act && c == 0)) {
@@ -393,9 +435,14 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
       }
     };
     if (edge_tile) {
-      for (int c = C - 1; c >= 0; --c) back_chunk(true, c);
+      for (int c = C - 1; c >= 0; --c) back_chunk(std::false_type{}, true, c);
     } else {
-      for (int c = C - 1; c >= 0; --c) back_chunk(false, c);
+      for (int c = C - 1; c >= 0; --c) {
+        if (c >= k0 && c <= k1)
+          back_chunk(std::true_type{}, false, c);
+        else
+          back_chunk(std::false_type{}, false, c);
+      }
     }
     tile = nxt;
     ti0 = ni0;
@@ -405,7 +452,9 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
   }
 }
 
-template <int AXIS>
+// FAST: the short FP64 chain (SweepParams::screen == kScreenFast), compiled
+// apart from the reference-exact one so that each carries one chain.
+template <int AXIS, bool FAST>
 __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
     sweep_yz_tmem_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap pmap,
                          const SweepParams<double> p, uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf,
@@ -458,20 +507,20 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
     if (g.C <= kTmemMaxChunks) {
       if (stage_dr)
-        yz_tmem_ring<AXIS, 1, true>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+        yz_tmem_ring<AXIS, 1, true, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
       else
-        yz_tmem_ring<AXIS, 1, false>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+        yz_tmem_ring<AXIS, 1, false, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
     } else {
       if (stage_dr)
-        yz_tmem_ring<AXIS, 2, true>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+        yz_tmem_ring<AXIS, 2, true, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
       else
-        yz_tmem_ring<AXIS, 2, false>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+        yz_tmem_ring<AXIS, 2, false, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
     }
   } else {
     if (stage_dr)
-      yz_tmem_ring<AXIS, 0, true>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
+      yz_tmem_ring<AXIS, 0, true, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
     else
-      yz_tmem_ring<AXIS, 0, false>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
+      yz_tmem_ring<AXIS, 0, false, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
   }
 
   // Loads still in flight (only after a wait gave up) land before the CTA
@@ -531,7 +580,7 @@ struct XShape {
 // chunk); 2: TMEM ring with the chunks past 16 resident in shared memory (the
 // first input slot stages the TMEM chunks' results; the next tile's first
 // inputs load after the back substitution).
-template <int MODE>
+template <int MODE, bool FAST>
 __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepParams<double>& p, const XShape& g,
                                             int KF, unsigned char* slots, uint64_t* full, double* cus,
                                             unsigned char* stage, uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
@@ -677,20 +726,20 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
             if (i0 + q >= nx) v[q] = 1.0;
         }
         // the screen reads the inputs before the chain
-        if (screen != kScreenFast) hwmin = min(hwmin, batch_min_hi<W>(v));
+        if constexpr (!FAST) hwmin = min(hwmin, batch_min_hi<W>(v));
         if constexpr (K) {
           if (flow) {
-            y = forward_any_const<W>(screen, v, dk, c1, y, [&](int q, double val) { yv[q] = val; });
+            y = forward_any_const<W>(FAST ? kScreenFast : 1, v, dk, c1, y, [&](int q, double val) { yv[q] = val; });
           } else {
             RowPut<double> put{crow, sw};
-            y = forward_any_const<W>(screen, v, dk, c1, y, put);
+            y = forward_any_const<W>(FAST ? kScreenFast : 1, v, dk, c1, y, put);
           }
         } else {
           if (flow) {
-            y = forward_any<W>(screen, v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
+            y = forward_any<W>(FAST ? kScreenFast : 1, v, cf, c1, y, [&](int q, double val) { yv[q] = val; });
           } else {
             RowPut<double> put{crow, sw};
-            y = forward_any<W>(screen, v, cf, c1, y, put);
+            y = forward_any<W>(FAST ? kScreenFast : 1, v, cf, c1, y, put);
           }
         }
       } else if (flow) {
@@ -733,7 +782,7 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
     // anywhere is redone from its inputs -- the field still holds them (this
     // tile's results are stored only by the back substitution) -- pinned as
     // above, with every numerator checked.
-    if (__any_sync(kAll, !screen_clean(screen, hwmin))) {
+    if (!FAST && __any_sync(kAll, !screen_clean(screen, hwmin))) {
       const double* src = plane + static_cast<size_t>(lane_on ? j : 0) * p.nxp;
       y = -0.0;
       for (int c = 0; c < C; ++c) {
@@ -913,6 +962,9 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
   }
 }
 
+// FAST: the short FP64 chain (SweepParams::screen == kScreenFast), compiled
+// apart from the reference-exact one.
+template <bool FAST>
 __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
     sweep_x_tmem_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<double> p,
                         uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns) {
@@ -962,11 +1014,11 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
     tmem_fence_after();
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
     if (own_stage)
-      x_tmem_ring<1>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+      x_tmem_ring<1, FAST>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
     else
-      x_tmem_ring<2>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+      x_tmem_ring<2, FAST>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
   } else {
-    x_tmem_ring<0>(&map, p, g, kf, slots, full, cus, nullptr, 0u, pend, ppar);
+    x_tmem_ring<0, FAST>(&map, p, g, kf, slots, full, cus, nullptr, 0u, pend, ppar);
   }
   if (pend != 0) {
     for (int sl = 0; sl < nslots; ++sl)
@@ -1006,7 +1058,7 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
 constexpr int kTmemRingSmemF32 = 3;  // most shared-memory rings (warps 0..ns-1; 3 measured best of 0-5)
 constexpr int kTmemRingTmemF32 = 8;  // most TMEM rings, two per lane quarter
 
-template <int AXIS, int MODE>
+template <int AXIS, int MODE, bool FAST>
 __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const CUtensorMap* pmap, const SweepParams<float>& p,
                                                  const YzShape& g, int KF, uint64_t* full, float* slots, double* cus,
                                                  double* drs, uint32_t tbase, uint32_t& pend, uint32_t& ppar) {
@@ -1082,7 +1134,6 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const C
     for (int c = 0; c < (TM ? KF : 0); ++c) issue(ti0, tm_, ts, tp, c, c, 0u);
     for (int c = T; c < C; ++c) issue(ti0, tm_, ts, tp, c, rslot(false, c), 0u);
   }
-  const int screen = p.screen;
   int staged_s = -1;
   int fsl = 0;
   uint32_t fpar = 0;
@@ -1152,9 +1203,10 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const C
             if (rb + q >= n) v[q] = 1.0f;
         }
         if (flow)
-          y = forward_store<R>(v, cf, c1, shift, screen, y, [&](int q, float val) { yv[q] = val; });
+          y = forward_store<R>(v, cf, c1, shift, FAST ? kScreenFast : 0, y, [&](int q, float val) { yv[q] = val; });
         else
-          y = forward_store<R>(v, cf, c1, shift, screen, y, [&](int q, float val) { cb[q * TI] = val; });
+          y = forward_store<R>(v, cf, c1, shift, FAST ? kScreenFast : 0, y,
+                               [&](int q, float val) { cb[q * TI] = val; });
       } else if (flow) {
 #pragma unroll
         for (int q = 0; q < R; ++q) yv[q] = 0.0f;  // lanes with no line: anything, never read
@@ -1278,7 +1330,9 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const C
   }
 }
 
-template <int AXIS>
+// FAST: the FP32 form's short chain (SweepParams::screen == kScreenFast),
+// compiled apart from the default one.
+template <int AXIS, bool FAST>
 __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
     sweep_yz_tmem_f32_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap pmap,
                              const SweepParams<float> p, uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf,
@@ -1332,11 +1386,11 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
     const uint32_t half = static_cast<uint32_t>((warp - ns) >= 4 ? 256 : 0);
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + half;
     if (g.C <= kTmemMaxChunks)
-      yz_tmem_ring_f32<AXIS, 1>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+      yz_tmem_ring_f32<AXIS, 1, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
     else
-      yz_tmem_ring_f32<AXIS, 2>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+      yz_tmem_ring_f32<AXIS, 2, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
   } else {
-    yz_tmem_ring_f32<AXIS, 0>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
+    yz_tmem_ring_f32<AXIS, 0, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
   }
   if (pend != 0) {
     for (int sl = 0; sl < nslots; ++sl)
@@ -1377,7 +1431,7 @@ constexpr int kXTmemMaxChunksF32 = 8;  // chunks of a TMEM ring in its 256 colum
 
 // STAGED: RN(1/d) read from the ring's copy `drs` in shared memory, else
 // from global memory.
-template <int MODE, bool STAGED>
+template <int MODE, bool STAGED, bool FAST>
 __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const SweepParams<float>& p,
                                                 const XShape& g, int KF, unsigned char* slots, uint64_t* full,
                                                 double* cus, double* drs, unsigned char* stage, uint32_t tbase,
@@ -1429,7 +1483,6 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
     for (int c = 0; c < (TM ? KF : 0); ++c) issue(tr0, ts, c, c, 0u);
     for (int c = T; c < C; ++c) issue(tr0, ts, c, rslot(false, c), 0u);
   }
-  const int screen = p.screen;
   int staged_s = -1;
   int fsl = 0;
   uint32_t fpar = 0;
@@ -1512,10 +1565,11 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
             }
           }
           if (flow) {
-            y = forward_store<16>(vh, cf, c1, shift, screen, y, [&](int q, float val) { yh[q] = val; });
+            y = forward_store<16>(vh, cf, c1, shift, FAST ? kScreenFast : 0, y, [&](int q, float val) { yh[q] = val; });
           } else {
             RowPut<float> put{crow, sw};
-            y = forward_store<16>(vh, cf, c1, shift, screen, y, [&](int q, float val) { put(16 * h + q, val); });
+            y = forward_store<16>(vh, cf, c1, shift, FAST ? kScreenFast : 0, y,
+                                  [&](int q, float val) { put(16 * h + q, val); });
           }
         } else if (flow) {
 #pragma unroll
@@ -1706,6 +1760,8 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
   }
 }
 
+// FAST: the FP32 form's short chain, compiled apart from the default one.
+template <bool FAST>
 __global__ void __launch_bounds__(32 * (kXTmemRingSmemF32 + kXTmemRingTmemF32), 1)
     sweep_x_tmem_f32_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<float> p,
                             uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns, int stage_dr) {
@@ -1759,16 +1815,16 @@ __global__ void __launch_bounds__(32 * (kXTmemRingSmemF32 + kXTmemRingTmemF32), 
     const uint32_t half = static_cast<uint32_t>((warp - ns) >= 4 ? 256 : 0);
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + half;
     if (own_stage && stage_dr)
-      x_tmem_ring_f32<1, true>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
+      x_tmem_ring_f32<1, true, FAST>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
     else if (own_stage)
-      x_tmem_ring_f32<1, false>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
+      x_tmem_ring_f32<1, false, FAST>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
     else if (stage_dr)
-      x_tmem_ring_f32<2, true>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
+      x_tmem_ring_f32<2, true, FAST>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
     else
-      x_tmem_ring_f32<2, false>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
+      x_tmem_ring_f32<2, false, FAST>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
   } else {
     // no shared-memory rings are planned (kXTmemRingSmemF32 = 0); kept for the plan's range
-    x_tmem_ring_f32<0, false>(&map, p, g, kf, slots, full, cus, drs, nullptr, 0u, pend, ppar);
+    x_tmem_ring_f32<0, false, FAST>(&map, p, g, kf, slots, full, cus, drs, nullptr, 0u, pend, ppar);
   }
   if (pend != 0) {
     for (int sl = 0; sl < nslots; ++sl)
@@ -1935,12 +1991,16 @@ cudaError_t launch_tmem_yz(const CUtensorMap& ring_map, const CUtensorMap& pmap,
   const size_t smem = tmem_yz_smem(n, ns, nt, kf, dr);
   const long long tiles = yz_tiles(p.nx, (AXIS == 1) ? p.nz : p.ny, p.s_hi - p.s_lo, pw);
   int grid = 0;
-  cudaError_t e = persistent_grid(sweep_yz_tmem_kernel<AXIS>, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
+  cudaError_t e = p.screen == kScreenFast
+                      ? persistent_grid(sweep_yz_tmem_kernel<AXIS, true>, smem, (tiles + rings - 1) / rings, &grid,
+                                        32 * rings)
+                      : persistent_grid(sweep_yz_tmem_kernel<AXIS, false>, smem, (tiles + rings - 1) / rings, &grid,
+                                        32 * rings);
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
-  sweep_yz_tmem_kernel<AXIS><<<grid, 32 * rings, smem, st>>>(
-      ring_map, pmap, p, static_cast<uint32_t>(tmem_yz_smem_ring_bytes(n, dr)),
-      static_cast<uint32_t>(tmem_yz_ring_bytes(n, kf, dr)), kf, ns, dr ? 1 : 0, pw);
+  auto kern = p.screen == kScreenFast ? sweep_yz_tmem_kernel<AXIS, true> : sweep_yz_tmem_kernel<AXIS, false>;
+  kern<<<grid, 32 * rings, smem, st>>>(ring_map, pmap, p, static_cast<uint32_t>(tmem_yz_smem_ring_bytes(n, dr)),
+                                       static_cast<uint32_t>(tmem_yz_ring_bytes(n, kf, dr)), kf, ns, dr ? 1 : 0, pw);
   *launched = true;
   return cudaGetLastError();
 }
@@ -1954,12 +2014,12 @@ cudaError_t launch_tmem_x(const CUtensorMap& map, const SweepParams<double>& p, 
   const size_t smem = x_tmem_smem(p.nx, ns, nt, kf);
   const long long tiles = (static_cast<long long>(p.ny) * p.nz + 31) / 32 * (p.s_hi - p.s_lo);
   int grid = 0;
-  cudaError_t e = persistent_grid(sweep_x_tmem_kernel, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
+  auto kern = p.screen == kScreenFast ? sweep_x_tmem_kernel<true> : sweep_x_tmem_kernel<false>;
+  cudaError_t e = persistent_grid(kern, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
-  sweep_x_tmem_kernel<<<grid, 32 * rings, smem, st>>>(map, p, static_cast<uint32_t>(x_tmem_ring_bytes(p.nx, false, kf)),
-                                                      static_cast<uint32_t>(x_tmem_ring_bytes(p.nx, true, kf)), kf,
-                                                      ns);
+  kern<<<grid, 32 * rings, smem, st>>>(map, p, static_cast<uint32_t>(x_tmem_ring_bytes(p.nx, false, kf)),
+                                       static_cast<uint32_t>(x_tmem_ring_bytes(p.nx, true, kf)), kf, ns);
   *launched = true;
   return cudaGetLastError();
 }
@@ -2038,13 +2098,13 @@ cudaError_t launch_tmem_yz_f32(const CUtensorMap& ring_map, const CUtensorMap& p
   const size_t smem = tmem_yz_f32_smem(n, ns, nt, kf, dr);
   const long long tiles = yz_tiles(p.nx, (AXIS == 1) ? p.nz : p.ny, p.s_hi - p.s_lo, pw);
   int grid = 0;
-  cudaError_t e =
-      persistent_grid(sweep_yz_tmem_f32_kernel<AXIS>, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
+  auto kern = p.screen == kScreenFast ? sweep_yz_tmem_f32_kernel<AXIS, true> : sweep_yz_tmem_f32_kernel<AXIS, false>;
+  cudaError_t e = persistent_grid(kern, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
-  sweep_yz_tmem_f32_kernel<AXIS><<<grid, 32 * rings, smem, st>>>(
-      ring_map, pmap, p, static_cast<uint32_t>(tmem_yz_f32_smem_ring_bytes(n, dr)),
-      static_cast<uint32_t>(tmem_yz_f32_ring_bytes(n, kf, dr)), kf, ns, dr ? 1 : 0, pw);
+  kern<<<grid, 32 * rings, smem, st>>>(ring_map, pmap, p, static_cast<uint32_t>(tmem_yz_f32_smem_ring_bytes(n, dr)),
+                                       static_cast<uint32_t>(tmem_yz_f32_ring_bytes(n, kf, dr)), kf, ns, dr ? 1 : 0,
+                                       pw);
   *launched = true;
   return cudaGetLastError();
 }
@@ -2121,12 +2181,13 @@ cudaError_t launch_tmem_x_f32(const CUtensorMap& map, const SweepParams<float>& 
   const size_t smem = x_tmem_f32_smem(p.nx, ns, nt, kf, dr);
   const long long tiles = (static_cast<long long>(p.ny) * p.nz + 31) / 32 * (p.s_hi - p.s_lo);
   int grid = 0;
-  cudaError_t e = persistent_grid(sweep_x_tmem_f32_kernel, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
+  auto kern = p.screen == kScreenFast ? sweep_x_tmem_f32_kernel<true> : sweep_x_tmem_f32_kernel<false>;
+  cudaError_t e = persistent_grid(kern, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
-  sweep_x_tmem_f32_kernel<<<grid, 32 * rings, smem, st>>>(
-      map, p, static_cast<uint32_t>(x_tmem_f32_ring_bytes(p.nx, false, kf, dr)),
-      static_cast<uint32_t>(x_tmem_f32_ring_bytes(p.nx, true, kf, dr)), kf, ns, dr ? 1 : 0);
+  kern<<<grid, 32 * rings, smem, st>>>(map, p, static_cast<uint32_t>(x_tmem_f32_ring_bytes(p.nx, false, kf, dr)),
+                                       static_cast<uint32_t>(x_tmem_f32_ring_bytes(p.nx, true, kf, dr)), kf, ns,
+                                       dr ? 1 : 0);
   *launched = true;
   return cudaGetLastError();
 }

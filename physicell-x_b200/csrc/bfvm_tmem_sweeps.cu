@@ -453,8 +453,11 @@ __device__ __forceinline__ void yz_tmem_ring(const CUtensorMap* map, const CUten
 }
 
 // FAST: the short FP64 chain (SweepParams::screen == kScreenFast), compiled
-// apart from the reference-exact one so that each carries one chain.
-template <int AXIS, bool FAST>
+// apart from the reference-exact one so that each carries one chain; STAGED:
+// the forward pairs staged per ring (stage_dr); LONG: lines of more than
+// kTmemMaxChunks chunks (TMEM rings with resident chunks).  Each kernel holds
+// the two ring bodies it runs and no others.
+template <int AXIS, bool FAST, bool STAGED, bool LONG>
 __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
     sweep_yz_tmem_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap pmap,
                          const SweepParams<double> p, uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf,
@@ -505,22 +508,9 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   if (tm) {
     tmem_fence_after();
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
-    if (g.C <= kTmemMaxChunks) {
-      if (stage_dr)
-        yz_tmem_ring<AXIS, 1, true, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
-      else
-        yz_tmem_ring<AXIS, 1, false, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
-    } else {
-      if (stage_dr)
-        yz_tmem_ring<AXIS, 2, true, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
-      else
-        yz_tmem_ring<AXIS, 2, false, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
-    }
+    yz_tmem_ring<AXIS, LONG ? 2 : 1, STAGED, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
   } else {
-    if (stage_dr)
-      yz_tmem_ring<AXIS, 0, true, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
-    else
-      yz_tmem_ring<AXIS, 0, false, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
+    yz_tmem_ring<AXIS, 0, STAGED, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
   }
 
   // Loads still in flight (only after a wait gave up) land before the CTA
@@ -963,8 +953,10 @@ __device__ __forceinline__ void x_tmem_ring(const CUtensorMap* map, const SweepP
 }
 
 // FAST: the short FP64 chain (SweepParams::screen == kScreenFast), compiled
-// apart from the reference-exact one.
-template <bool FAST>
+// apart from the reference-exact one; OWN: lines of at most kTmemMaxChunks
+// chunks (TMEM rings with their own staging chunk), else TMEM rings with
+// resident chunks.
+template <bool FAST, bool OWN>
 __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
     sweep_x_tmem_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<double> p,
                         uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns) {
@@ -1013,10 +1005,7 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmem + kTmemRingTmem), 1)
   if (tm) {
     tmem_fence_after();
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16);
-    if (own_stage)
-      x_tmem_ring<1, FAST>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
-    else
-      x_tmem_ring<2, FAST>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
+    x_tmem_ring<OWN ? 1 : 2, FAST>(&map, p, g, kf, slots, full, cus, stage, tbase, pend, ppar);
   } else {
     x_tmem_ring<0, FAST>(&map, p, g, kf, slots, full, cus, nullptr, 0u, pend, ppar);
   }
@@ -1331,8 +1320,9 @@ __device__ __forceinline__ void yz_tmem_ring_f32(const CUtensorMap* map, const C
 }
 
 // FAST: the FP32 form's short chain (SweepParams::screen == kScreenFast),
-// compiled apart from the default one.
-template <int AXIS, bool FAST>
+// compiled apart from the default one; LONG: lines of more than
+// kTmemMaxChunks chunks.
+template <int AXIS, bool FAST, bool LONG>
 __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
     sweep_yz_tmem_f32_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap pmap,
                              const SweepParams<float> p, uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf,
@@ -1385,10 +1375,7 @@ __global__ void __launch_bounds__(32 * (kTmemRingSmemF32 + kTmemRingTmemF32), 1)
     // lane quarter warp % 4; the second ring on a quarter takes columns 256..511
     const uint32_t half = static_cast<uint32_t>((warp - ns) >= 4 ? 256 : 0);
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + half;
-    if (g.C <= kTmemMaxChunks)
-      yz_tmem_ring_f32<AXIS, 1, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
-    else
-      yz_tmem_ring_f32<AXIS, 2, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
+    yz_tmem_ring_f32<AXIS, LONG ? 2 : 1, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, tbase, pend, ppar);
   } else {
     yz_tmem_ring_f32<AXIS, 0, FAST>(&map, &pmap, p, g, kf, full, slots, cus, drs, 0u, pend, ppar);
   }
@@ -1760,8 +1747,10 @@ __device__ __forceinline__ void x_tmem_ring_f32(const CUtensorMap* map, const Sw
   }
 }
 
-// FAST: the FP32 form's short chain, compiled apart from the default one.
-template <bool FAST>
+// FAST: the FP32 form's short chain, compiled apart from the default one;
+// STAGED: RN(1/d) staged per ring (stage_dr); OWN: lines of at most
+// kXTmemMaxChunksF32 chunks.
+template <bool FAST, bool STAGED, bool OWN>
 __global__ void __launch_bounds__(32 * (kXTmemRingSmemF32 + kXTmemRingTmemF32), 1)
     sweep_x_tmem_f32_kernel(const __grid_constant__ CUtensorMap map, const SweepParams<float> p,
                             uint32_t smem_ring_bytes, uint32_t tmem_ring_bytes, int kf, int ns, int stage_dr) {
@@ -1814,14 +1803,7 @@ __global__ void __launch_bounds__(32 * (kXTmemRingSmemF32 + kXTmemRingTmemF32), 
     // lane quarter warp % 4; the second ring on a quarter takes columns 256..511
     const uint32_t half = static_cast<uint32_t>((warp - ns) >= 4 ? 256 : 0);
     const uint32_t tbase = *tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + half;
-    if (own_stage && stage_dr)
-      x_tmem_ring_f32<1, true, FAST>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
-    else if (own_stage)
-      x_tmem_ring_f32<1, false, FAST>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
-    else if (stage_dr)
-      x_tmem_ring_f32<2, true, FAST>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
-    else
-      x_tmem_ring_f32<2, false, FAST>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
+    x_tmem_ring_f32<OWN ? 1 : 2, STAGED, FAST>(&map, p, g, kf, slots, full, cus, drs, stage, tbase, pend, ppar);
   } else {
     // no shared-memory rings are planned (kXTmemRingSmemF32 = 0); kept for the plan's range
     x_tmem_ring_f32<0, false, FAST>(&map, p, g, kf, slots, full, cus, drs, nullptr, 0u, pend, ppar);
@@ -1991,14 +1973,15 @@ cudaError_t launch_tmem_yz(const CUtensorMap& ring_map, const CUtensorMap& pmap,
   const size_t smem = tmem_yz_smem(n, ns, nt, kf, dr);
   const long long tiles = yz_tiles(p.nx, (AXIS == 1) ? p.nz : p.ny, p.s_hi - p.s_lo, pw);
   int grid = 0;
-  cudaError_t e = p.screen == kScreenFast
-                      ? persistent_grid(sweep_yz_tmem_kernel<AXIS, true>, smem, (tiles + rings - 1) / rings, &grid,
-                                        32 * rings)
-                      : persistent_grid(sweep_yz_tmem_kernel<AXIS, false>, smem, (tiles + rings - 1) / rings, &grid,
-                                        32 * rings);
+  const bool fast = p.screen == kScreenFast, lng = (n + kRingRows - 1) / kRingRows > kTmemMaxChunks;
+  auto kern = fast ? (dr ? (lng ? sweep_yz_tmem_kernel<AXIS, true, true, true> : sweep_yz_tmem_kernel<AXIS, true, true, false>)
+                         : (lng ? sweep_yz_tmem_kernel<AXIS, true, false, true> : sweep_yz_tmem_kernel<AXIS, true, false, false>))
+                   : (dr ? (lng ? sweep_yz_tmem_kernel<AXIS, false, true, true> : sweep_yz_tmem_kernel<AXIS, false, true, false>)
+                         : (lng ? sweep_yz_tmem_kernel<AXIS, false, false, true>
+                                : sweep_yz_tmem_kernel<AXIS, false, false, false>));
+  cudaError_t e = persistent_grid(kern, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
-  auto kern = p.screen == kScreenFast ? sweep_yz_tmem_kernel<AXIS, true> : sweep_yz_tmem_kernel<AXIS, false>;
   kern<<<grid, 32 * rings, smem, st>>>(ring_map, pmap, p, static_cast<uint32_t>(tmem_yz_smem_ring_bytes(n, dr)),
                                        static_cast<uint32_t>(tmem_yz_ring_bytes(n, kf, dr)), kf, ns, dr ? 1 : 0, pw);
   *launched = true;
@@ -2014,7 +1997,9 @@ cudaError_t launch_tmem_x(const CUtensorMap& map, const SweepParams<double>& p, 
   const size_t smem = x_tmem_smem(p.nx, ns, nt, kf);
   const long long tiles = (static_cast<long long>(p.ny) * p.nz + 31) / 32 * (p.s_hi - p.s_lo);
   int grid = 0;
-  auto kern = p.screen == kScreenFast ? sweep_x_tmem_kernel<true> : sweep_x_tmem_kernel<false>;
+  const bool own = (p.nx + 15) / 16 <= kTmemMaxChunks;
+  auto kern = p.screen == kScreenFast ? (own ? sweep_x_tmem_kernel<true, true> : sweep_x_tmem_kernel<true, false>)
+                                      : (own ? sweep_x_tmem_kernel<false, true> : sweep_x_tmem_kernel<false, false>);
   cudaError_t e = persistent_grid(kern, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
@@ -2098,7 +2083,10 @@ cudaError_t launch_tmem_yz_f32(const CUtensorMap& ring_map, const CUtensorMap& p
   const size_t smem = tmem_yz_f32_smem(n, ns, nt, kf, dr);
   const long long tiles = yz_tiles(p.nx, (AXIS == 1) ? p.nz : p.ny, p.s_hi - p.s_lo, pw);
   int grid = 0;
-  auto kern = p.screen == kScreenFast ? sweep_yz_tmem_f32_kernel<AXIS, true> : sweep_yz_tmem_f32_kernel<AXIS, false>;
+  const bool lng = (n + kRingRows - 1) / kRingRows > kTmemMaxChunks;
+  auto kern = p.screen == kScreenFast
+                  ? (lng ? sweep_yz_tmem_f32_kernel<AXIS, true, true> : sweep_yz_tmem_f32_kernel<AXIS, true, false>)
+                  : (lng ? sweep_yz_tmem_f32_kernel<AXIS, false, true> : sweep_yz_tmem_f32_kernel<AXIS, false, false>);
   cudaError_t e = persistent_grid(kern, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
@@ -2181,7 +2169,13 @@ cudaError_t launch_tmem_x_f32(const CUtensorMap& map, const SweepParams<float>& 
   const size_t smem = x_tmem_f32_smem(p.nx, ns, nt, kf, dr);
   const long long tiles = (static_cast<long long>(p.ny) * p.nz + 31) / 32 * (p.s_hi - p.s_lo);
   int grid = 0;
-  auto kern = p.screen == kScreenFast ? sweep_x_tmem_f32_kernel<true> : sweep_x_tmem_f32_kernel<false>;
+  const bool own = (p.nx + 31) / 32 <= kXTmemMaxChunksF32;
+  auto kern =
+      p.screen == kScreenFast
+          ? (dr ? (own ? sweep_x_tmem_f32_kernel<true, true, true> : sweep_x_tmem_f32_kernel<true, true, false>)
+                : (own ? sweep_x_tmem_f32_kernel<true, false, true> : sweep_x_tmem_f32_kernel<true, false, false>))
+          : (dr ? (own ? sweep_x_tmem_f32_kernel<false, true, true> : sweep_x_tmem_f32_kernel<false, true, false>)
+                : (own ? sweep_x_tmem_f32_kernel<false, false, true> : sweep_x_tmem_f32_kernel<false, false, false>));
   cudaError_t e = persistent_grid(kern, smem, (tiles + rings - 1) / rings, &grid, 32 * rings);
   if (e != cudaSuccess) return e;
   if (cfg.persistent < 2 && tiles < kTmemMinTilesPerRing * grid * rings) return cudaSuccess;
